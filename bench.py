@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 DIVA velocity solver.
+
+Metric: DIVA solves/s on the 321 x 561 x 15 synthetic ice cap (the 1600 x 2800 km,
+5 km configuration), each solve a cold start run to a relative nonlinear
+residual of 1e-6, followed by the SIA 3D velocities ("DIVA plus SIA").
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One process per GPU (torchrun for N > 1).  A single solve does not shard:
+each rank runs an independent replica of the workload, so per-GPU work is
+fixed as N grows ("scaling": "weak") and there is no data-path collective;
+the only collectives are the timing barrier and the max over ranks.
+
+value : solves/s of the whole job, device-timed with CUDA events on the
+        library's stream, inputs (geometry, masks, rheology) resident in HBM;
+        each step restores the cold-start state (device copy), solves and
+        computes the SIA velocities.
+e2e   : the same through the public API with host buffers: every step uploads
+        the inputs and the cold-start state from pinned host memory, prepares
+        them on the GPU (update_general_ice_model_data, rheology), solves, and
+        downloads the velocity fields.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_package():
+    import importlib.util
+    if "imau_ice_b200" in sys.modules:
+        return sys.modules["imau_ice_b200"]
+    d = os.path.join(ROOT, "imau-ice_b200")
+    spec = importlib.util.spec_from_file_location("imau_ice_b200", os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["imau_ice_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+METRIC = "DIVA solves/s at 321x561x15 to rel-res 1e-6"
+UNIT = "solves/s"
+INPUT_FIELDS = ["Hi_a", "Hb_a", "SL_a", "dHb_dt_a", "Ti_a", "beta_sq_a"]
+STATE_FIELDS = ["u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "taub_cx", "taub_cy", "u_3D_a", "v_3D_a"]
+OUTPUT_FIELDS = ["u_vav_cx", "v_vav_cy", "u_3D_cx", "v_3D_cy", "w_3D_a", "u_3D_SIA_cx", "v_3D_SIA_cy"]
+KERNEL_NAMES = {0: "k_column_coefficients", 1: "k_gs (fine level, 4 colours)", 2: "k_matvec"}
+
+
+def workload(seed=2):
+    from imau_ice_b200 import synth
+    g, cfg, fields = synth.ice_cap(seed=seed)
+    cfg = dict(cfg)
+    cfg.update(picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1, lin_rtol=1e-10)
+    return g, cfg, fields
+
+
+def config_json(g, extra=None):
+    c = {"workload": "DIVA+SIA cold-start solve, synthetic ice cap 1600x2800 km @5 km",
+         "nx": g["nx"], "ny": g["ny"], "nz": len(g["zeta"]), "stop": "nonlinear rel-res <= 1e-6",
+         "linear_solver": "BiCGStab + geometric multigrid V(2,2), adaptive tolerance",
+         "l2": "inputs larger than L2 (working set ~0.6 GB > 126 MB)"}
+    c.update(extra or {})
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_traffic(kernel_key):
+    """dram bytes per launch of a kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_key}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("dram_bytes_per_launch_scaled:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(sample_picard_its, n_picard_full, threads=1, timeout_s=60.0):
+    """The oracle (a CPU port of the reference path) on the same workload: the first
+    `sample_picard_its` viscosity iterations of one cold solve, timed, scaled to one full
+    solve of `n_picard_full` iterations.  Linear solves: GMRES(30) + ILU(0) from the
+    current iterate with the same adaptive tolerance rule as the GPU path."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_backend
+    from imau_ice_b200 import diva
+    orc = oracle_backend.oracle_backend()
+    g, cfg, fields = workload()
+    cfg = dict(cfg)
+    cfg["DIVA_visc_it_nit"] = sample_picard_its
+    grid = diva.Grid(**g)
+    ctx = diva.Context(grid, cfg, orc)
+    oracle_backend.set_linear_solver(ctx, oracle_backend.LIN_GMRES_WARM, rtol=1e-10, abstol=0.0)
+    ctx.upload(fields)
+    ctx.update_general_ice_model_data()
+    ctx.calc_pressure_melting_point()
+    ctx.calc_ice_rheology()
+    ctx.update_general_ice_model_data()
+    t0 = time.perf_counter()
+    rep = ctx.solve_DIVA()
+    ctx.calc_sia_3d_velocities()
+    t = time.perf_counter() - t0
+    ctx.close()
+    its = max(1, rep["picard_iterations"])
+    per_solve = t / its * n_picard_full
+    return {"value": 1.0 / per_solve, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"first {its} of {n_picard_full} viscosity iterations of one cold solve at 321x561x15 "
+                       f"({t:.1f} s), scaled to a full solve; early iterations use looser linear tolerances, "
+                       f"so this overestimates CPU speed")}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    load_package()
+    g, _, _ = workload()
+    n_full = args.ref_picard_full
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(args.ref_sample_its, n_full)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(args.ref_sample_its, n_full)["value"])
+    v = statistics.mean(vals)
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ice cap)",
+           "config": config_json(g, {"parallelism": "none (CPU oracle port, 1 thread)"}),
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                            "sample": f"first {args.ref_sample_its} of {n_full} viscosity iterations per step"},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    load_package()
+    from imau_ice_b200 import build, diva
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    build.build()
+
+    g, cfg, fields = workload()
+    grid = diva.Grid(**g)
+    ctx = diva.Context(grid, cfg)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload(fields)
+    ctx.update_general_ice_model_data()
+    ctx.calc_pressure_melting_point()
+    ctx.calc_ice_rheology()
+    ctx.update_general_ice_model_data()
+    ctx.state_save()
+
+    def step():
+        ctx.state_restore()          # cold start: the initial state of the solve, a device copy
+        r = ctx.solve_DIVA()
+        ctx.calc_sia_3d_velocities()
+        return r
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = ctx.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    reps = [step() for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = ctx.kernel_launches() - l0
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": world * args.steps / (ms / 1000.0), "unit": UNIT,
+                              "quick": True, "gpu_launches": int(launches)}))
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1000.0)
+    picard = [r["picard_iterations"] for r in reps]
+    mg = [r["mg_cycles"] for r in reps]
+
+    # roofline of the dominant kernel: time share = launches per solve x time per launch
+    prof = {}
+    for which in (0, 1, 2):
+        prof[which] = ctx.profile_kernel(which, reps=30 if which else 10)
+    t_col = prof[0][0] * statistics.mean(picard)
+    t_gs = prof[1][0] * statistics.mean(mg) * 4      # V(2,2): four fine-level sweeps per cycle
+    dom = 0 if t_col >= t_gs else 1
+    ms_l, bytes_l = prof[dom]
+    hbm_peak = None
+    peak_src = "fallback 6650 GB/s"
+    try:
+        hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        hbm_peak = 6650.0
+    achieved = bytes_l / (ms_l * 1e-3) / 1e9
+    traffic_key = "k_column_coefficients" if dom == 0 else "k_gs"
+    roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": read_traffic(traffic_key),
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": bytes_l, "ms_per_launch": ms_l,
+                "other_kernels": {KERNEL_NAMES[w]: {"ms_per_launch": prof[w][0],
+                                                    "GB/s": prof[w][1] / (prof[w][0] * 1e-3) / 1e9}
+                                  for w in prof}}
+
+    # end to end through the public API with pinned host buffers
+    def pinned(a):
+        t_ = torch.empty(a.shape[::-1], dtype=torch.float64 if a.dtype == np.float64 else torch.int32,
+                         pin_memory=True)
+        h = t_.numpy().T            # Fortran-ordered view of the pinned buffer
+        h[...] = a
+        return h, t_
+
+    keep = []
+    host_in = {}
+    for n in INPUT_FIELDS:
+        h, t_ = pinned(np.asarray(fields[n]))
+        host_in[n] = h
+        keep.append(t_)
+    for n in STATE_FIELDS:
+        h, t_ = pinned(ctx.empty(n))
+        host_in[n] = h
+        keep.append(t_)
+    h2d = sum(a.nbytes for a in host_in.values())
+    e2e_steps = max(1, min(args.steps, 3))
+
+    def e2e_step():
+        ctx.upload(host_in)
+        ctx.update_general_ice_model_data()
+        ctx.calc_pressure_melting_point()
+        ctx.calc_ice_rheology()
+        ctx.update_general_ice_model_data()
+        ctx.solve_DIVA()
+        ctx.calc_sia_3d_velocities()
+        return ctx.download(OUTPUT_FIELDS)
+
+    out = e2e_step()
+    d2h = sum(a.nbytes for a in out.values())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    te = torch.tensor([time.perf_counter() - t0], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    e2e_val = world * e2e_steps / float(te.item())
+
+    if rank == 0:
+        res = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ice cap)",
+               "config": config_json(g, {"parallelism": f"replicas x{world} (a single solve does not shard)",
+                                         "picard_iterations": picard, "mg_cycles": mg,
+                                         "relres": [r["relres"] for r in reps]}),
+               "roofline": roofline, "clocks": clk,
+               "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                       "timing": "host wall clock with device synchronisation, max over ranks"},
+               "gpu_launches": int(launches)}
+        if not args.no_cpu_baseline:
+            try:
+                res["cpu_baseline"] = cpu_baseline(args.cpu_sample_its, int(round(statistics.mean(picard))))
+            except Exception as ex:   # the baseline is reported, never required
+                res["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
+        print(json.dumps(res))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--cpu-sample-its", type=int, default=8, help="viscosity iterations timed for the CPU baseline")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--quick", action="store_true",
+                   help="timed solves only (no roofline, e2e or CPU legs): the command profiled with ncu")
+    p.add_argument("--ref-sample-its", type=int, default=4)
+    p.add_argument("--ref-picard-full", type=int, default=89,
+                   help="viscosity iterations of a full solve (as measured on the GPU path)")
+    args = p.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

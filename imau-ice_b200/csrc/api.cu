@@ -1,0 +1,640 @@
+// api.cu -- the C ABI of libdiva_b200.so (include/diva.h): context, device
+// memory, Fortran-order upload/download, and the host-side sequencing of
+// solve_SIA / solve_SSA / solve_DIVA (ice_velocity_module.f90:36-374).
+//
+// All device memory of a context is one cudaMalloc'd arena carved at create
+// time; no call after diva_create allocates.  Every kernel runs on the
+// context's stream.  Host synchronisation happens once per viscosity
+// iteration (to read the step norm) and once per Krylov half-step.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include "ctx.hpp"
+
+using namespace diva;
+
+struct diva_ctx {
+  Ctx c;
+};
+
+namespace diva {
+
+int set_error(Ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+int check_cuda(Ctx* c, cudaError_t e, const char* what) {
+  return set_error(c, DIVA_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace diva
+
+namespace {
+
+const diva_field_info_t g_info[DIVA_NUM_FIELDS] = {
+#define X(ID, name, grid, type) {#name, DIVA_GRID_##grid, DIVA_DTYPE_##type},
+    DIVA_FIELD_LIST(X)
+#undef X
+};
+
+bool is3d(int kind) { return kind >= DIVA_GRID_A3; }
+int base_kind(int kind) { return is3d(kind) ? kind - DIVA_GRID_A3 : kind; }
+
+int64_t host_numel(int nx, int ny, int nz, int kind) {
+  const int64_t n2[4] = {(int64_t)ny * nx, (int64_t)ny * (nx - 1), (int64_t)(ny - 1) * nx, (int64_t)(ny - 1) * (nx - 1)};
+  return (is3d(kind) ? nz : 1) * n2[base_kind(kind)];
+}
+
+// Fortran-order host array <-> padded, layer-major device layout
+template <typename T>
+__global__ void k_unpack(Dims d, int kind, const T* __restrict__ src, T* __restrict__ dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  const int bk = kind >= DIVA_GRID_A3 ? kind - DIVA_GRID_A3 : kind;
+  const int hny = (bk == DIVA_GRID_CY || bk == DIVA_GRID_B) ? d.ny - 1 : d.ny;
+  const int hnx = (bk == DIVA_GRID_CX || bk == DIVA_GRID_B) ? d.nx - 1 : d.nx;
+  if (j >= hny || i >= hnx) return;
+  const long long col = (long long)i * hny + j;
+  if (kind >= DIVA_GRID_A3) {
+    for (int k = 0; k < d.nz; ++k) dst[(long long)k * d.plane + d.at(j, i)] = src[col * d.nz + k];
+  } else {
+    dst[d.at(j, i)] = src[col];
+  }
+}
+template <typename T>
+__global__ void k_pack(Dims d, int kind, const T* __restrict__ src, T* __restrict__ dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  const int bk = kind >= DIVA_GRID_A3 ? kind - DIVA_GRID_A3 : kind;
+  const int hny = (bk == DIVA_GRID_CY || bk == DIVA_GRID_B) ? d.ny - 1 : d.ny;
+  const int hnx = (bk == DIVA_GRID_CX || bk == DIVA_GRID_B) ? d.nx - 1 : d.nx;
+  if (j >= hny || i >= hnx) return;
+  const long long col = (long long)i * hny + j;
+  if (kind >= DIVA_GRID_A3) {
+    for (int k = 0; k < d.nz; ++k) dst[col * d.nz + k] = src[(long long)k * d.plane + d.at(j, i)];
+  } else {
+    dst[col] = src[d.at(j, i)];
+  }
+}
+
+__global__ void k_fill(double* p, long long n, double v) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) p[t] = v;
+}
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+struct Carver {
+  char* base;
+  size_t off = 0;
+  bool dry;
+  void* take(size_t bytes) {
+    void* p = dry ? nullptr : base + off;
+    off += align256(bytes);
+    return p;
+  }
+};
+
+void config_defaults(diva_config_t* c) {
+  // configuration_module.f90:271-367, 424-426, 702
+  memset(c, 0, sizeof(*c));
+  c->choice_ice_dynamics = DIVA_DYN_DIVA;
+  c->n_flow = 3.0; c->m_enh_sheet = 1.0; c->m_enh_shelf = 1.0;
+  c->choice_ice_margin = DIVA_MARGIN_INFINITE_SLAB;
+  c->include_SSADIVA_crossterms = 1; c->do_GL_subgrid_friction = 1;
+  c->DIVA_visc_it_norm_dUV_tol = 1E-2; c->DIVA_visc_it_nit = 50; c->DIVA_visc_it_relax = 0.4;
+  c->DIVA_epsilon_sq_0 = 1E-15; c->DIVA_visc_eff_min = 1E3; c->DIVA_beta_max = 1E20; c->DIVA_vel_max = 5000.0;
+  c->choice_sliding_law = DIVA_SLIDING_COULOMB_REGULARISED;
+  c->slid_delta_v = 1.0E-3; c->slid_Weertman_m = 3.0; c->slid_Coulomb_reg_q_plastic = 0.3;
+  c->slid_Coulomb_reg_u_threshold = 100.0; c->slid_ZI_ut = 200.0; c->slid_ZI_p = 5.0;
+  c->include_basal_freezing = 1; c->deltaT_basal_freezing = 2.0;
+  c->choice_basal_hydrology = DIVA_HYDRO_MARTIN2011; c->Martin2011_hydro_Hb_min = 0.0; c->Martin2011_hydro_Hb_max = 1000.0;
+  c->choice_ice_rheology = DIVA_RHEO_HUYBRECHTS1992; c->uniform_flow_factor = 1E-16;
+  c->do_ocean_floodfill = 1;
+  c->lin_rtol = 1E-8; c->lin_maxit = 500;
+  c->picard_stop = DIVA_STOP_RESID_UV; c->picard_relres_tol = 1E-6; c->lin_adaptive = 0;
+  c->precision = DIVA_PREC_FP64;
+}
+
+int validate_config(Ctx* c, const diva_config_t* cfg) {
+  if (cfg->choice_ice_dynamics < 0 || cfg->choice_ice_dynamics > 3) return set_error(c, DIVA_BAD_INPUT, "choice_ice_dynamics");
+  if (cfg->choice_ice_margin < 0 || cfg->choice_ice_margin > 1) return set_error(c, DIVA_BAD_INPUT, "choice_ice_margin");
+  if (cfg->choice_sliding_law < 0 || cfg->choice_sliding_law > 6) return set_error(c, DIVA_BAD_INPUT, "choice_sliding_law");
+  if (cfg->DIVA_visc_it_nit < 1) return set_error(c, DIVA_BAD_INPUT, "DIVA_visc_it_nit must be >= 1");
+  if (!(cfg->n_flow > 0.0)) return set_error(c, DIVA_BAD_INPUT, "n_flow must be > 0");
+  if (cfg->lin_maxit < 1) return set_error(c, DIVA_BAD_INPUT, "lin_maxit must be >= 1");
+  const int bcs[8] = {cfg->BC_u_west, cfg->BC_u_east, cfg->BC_u_south, cfg->BC_u_north,
+                      cfg->BC_v_west, cfg->BC_v_east, cfg->BC_v_south, cfg->BC_v_north};
+  for (int b : bcs)
+    if (b < 0 || b > 2) return set_error(c, DIVA_BAD_INPUT, "boundary condition code");
+  return DIVA_OK;
+}
+
+void apply_config(Ctx* c, const diva_config_t* cfg) {
+  c->c = *cfg;
+  c->bc = BCs{cfg->BC_u_west, cfg->BC_u_east, cfg->BC_u_south, cfg->BC_u_north,
+              cfg->BC_v_west, cfg->BC_v_east, cfg->BC_v_south, cfg->BC_v_north};
+  for (int k = 0; k < c->zt.nz; ++k) c->zt.zn[k] = pow(c->zt.z[k], cfg->n_flow);
+}
+
+// multigrid hierarchy: halve every direction with at least 9 points
+void plan_levels(Ctx* c) {
+  int nx = c->d.nx, ny = c->d.ny;
+  double dx = c->d.dx;
+  c->nlev = 0;
+  for (;;) {
+    Dims L;
+    L.nx = nx; L.ny = ny; L.nz = c->d.nz;
+    L.ld = c->nlev == 0 ? c->d.ld : ((ny + 15) / 16) * 16;
+    L.plane = (long long)L.nx * L.ld;
+    L.dx = dx;
+    c->lv[c->nlev].d = L;
+    c->nlev++;
+    if (c->nlev == kMaxLevels) break;
+    const bool cx = nx >= 9, cy = ny >= 9;
+    if (!cx && !cy) break;
+    if (cx) { nx = (nx + 2) / 2; dx *= 2.0; }
+    if (cy) ny = (ny + 2) / 2;
+  }
+}
+
+size_t carve(Ctx* c, Carver& cv) {
+  const Dims& d = c->d;
+  for (int f = 0; f < DIVA_NUM_FIELDS; ++f) {
+    const size_t es = g_info[f].dtype == DIVA_DTYPE_D ? sizeof(double) : sizeof(int);
+    c->f[f] = cv.take((is3d(g_info[f].grid) ? d.nz : 1) * d.plane * es);
+  }
+  c->visc_prev = (double*)cv.take(sizeof(double) * d.nz * d.plane);
+  c->afac = (double*)cv.take(sizeof(double) * d.nz * d.plane);
+  for (int q = 0; q < 4; ++q) c->quad[q] = (double*)cv.take(sizeof(double) * d.plane);
+  for (int q = 0; q < 2; ++q) c->err_cand[q] = (double*)cv.take(sizeof(double) * d.plane);
+  c->staging = (double*)cv.take(sizeof(double) * d.nz * d.plane);
+  c->ff_ocean = (int*)cv.take(sizeof(int) * 2 * d.plane);
+  c->ff_flag = (int*)cv.take(sizeof(int) * 4);
+  c->scal = (double*)cv.take(sizeof(double) * SC_COUNT);
+  const dim3 g = grid2d(d.ny, d.nx);
+  c->max_blocks = g.x * g.y;
+  c->partials = (double*)cv.take(sizeof(double) * 4 * c->max_blocks);
+  for (int k = 0; k < KV_COUNT; ++k)
+    for (int q = 0; q < 2; ++q) c->kv[k][q] = (double*)cv.take(sizeof(double) * d.plane);
+  for (int l = 0; l < c->nlev; ++l) {
+    Level& L = c->lv[l];
+    const size_t pb = sizeof(double) * L.d.plane;
+    L.Na = (double*)cv.take(pb); L.Nb = (double*)cv.take(pb); L.Bx = (double*)cv.take(pb); L.By = (double*)cv.take(pb);
+    L.idu = (double*)cv.take(pb); L.idv = (double*)cv.take(pb);
+    L.xu = (double*)cv.take(pb); L.xv = (double*)cv.take(pb); L.bu = (double*)cv.take(pb); L.bv = (double*)cv.take(pb);
+    L.ru = (double*)cv.take(pb); L.rv = (double*)cv.take(pb);
+  }
+  return cv.off;
+}
+
+size_t field_dev_bytes(const Ctx* c, int f) {
+  const size_t es = g_info[f].dtype == DIVA_DTYPE_D ? sizeof(double) : sizeof(int);
+  return (is3d(g_info[f].grid) ? c->d.nz : 1) * c->d.plane * es;
+}
+
+int begin(Ctx* c) {
+  c->lin_iters = 0;
+  c->mg_cycles = 0;
+  c->fine_passes = 0.0;
+  c->err.clear();
+  DIVA_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  return DIVA_OK;
+}
+int finish(Ctx* c, diva_report_t* rep) {
+  DIVA_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  DIVA_CUDA(c, cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  DIVA_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  if (rep) {
+    rep->elapsed_ms = ms;
+    rep->linear_iterations = (int32_t)c->lin_iters;
+    rep->mg_cycles = (int32_t)c->mg_cycles;
+    rep->fine_passes = c->fine_passes;
+  }
+  return DIVA_OK;
+}
+
+int fill_const(Ctx* c, double* p, double v) {
+  const long long n = c->d.plane;
+  k_fill<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(p, n, v); c->launches++;
+  DIVA_LAUNCHED(c, "k_fill");
+  return DIVA_OK;
+}
+
+// the viscosity iteration shared by solve_SSA (:180-240) and solve_DIVA (:307-363)
+int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
+  const diva_config_t& C = c->c;
+  const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
+  int it = 0, st = DIVA_OK, lin_fail = 0;
+  double resid = 0.0, relres = -1.0;
+  for (;;) {
+    ++it;
+    if ((st = launch_diva_coefficients(c, u, v, diva))) return st;
+    if ((st = solver_setup(c))) return st;
+    if (relmode) {
+      if ((st = solver_relres(c, u, v, &relres))) return st;
+      if (!std::isfinite(relres)) return set_error(c, DIVA_NAN_DETECTED, "NaN in the nonlinear residual");
+      if (relres <= C.picard_relres_tol) {
+        if (diva && (st = launch_basal_stress_velocities(c))) return st;
+        break;
+      }
+    }
+    double rtol = C.lin_rtol;
+    if (relmode && C.lin_adaptive) rtol = std::max(C.lin_rtol, std::min(0.1, 0.05 * relres));
+    int iters = 0;
+    st = solver_solve(c, u, v, rtol, C.lin_maxit, &iters, nullptr);
+    if (st == DIVA_LINEAR_NOT_CONVERGED) {
+      ++lin_fail;   // the reference does not check PETSc/SOR convergence either; keep iterating
+    } else if (st) {
+      return st;
+    }
+    if ((st = launch_picard_update(c, u, v, c->kv[KV_X][0], c->kv[KV_X][1], diva))) return st;
+    DIVA_CUDA(c, cudaMemcpyAsync(c->h_scal + SC_RES1, c->scal + SC_RES1, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+    const double r1 = c->h_scal[SC_RES1], r2 = c->h_scal[SC_RES2], cnt = c->h_scal[SC_RES1 + 2];
+    if (!std::isfinite(r1) || !std::isfinite(r2)) return set_error(c, DIVA_NAN_DETECTED, "NaN in the velocities");
+    resid = (cnt > 0.0) ? 2.0 * sqrt(r1) / std::max(sqrt(r2), 1E-8) : 0.0;
+    bool converged = false;
+    if (!relmode && resid < C.DIVA_visc_it_norm_dUV_tol) converged = true;
+    else if (it >= C.DIVA_visc_it_nit) converged = true;
+    if (!converged) launch_commit_err(c);
+    if (converged) break;
+  }
+  int status = DIVA_OK;
+  if (it >= C.DIVA_visc_it_nit && ((relmode && !(relres >= 0.0 && relres <= C.picard_relres_tol)) ||
+                                   (!relmode && resid >= C.DIVA_visc_it_norm_dUV_tol)))
+    status = DIVA_MAX_PICARD;
+  if (rep) {
+    rep->picard_iterations = it;
+    rep->resid_UV = resid;
+    rep->relres = relres;
+    rep->status = status;
+    rep->reserved[0] = lin_fail;
+  }
+  return status;
+}
+
+int prepare_velocity_solve(Ctx* c) {
+  int st;
+  if ((st = launch_driving_stress(c))) return st;
+  if ((st = launch_basal_conditions(c))) return st;
+  if ((st = launch_grounded_fractions(c))) return st;
+  if ((st = fill_const(c, c->D(DIVA_F_DIVA_ERR_CX), 1E5))) return st;
+  if ((st = fill_const(c, c->D(DIVA_F_DIVA_ERR_CY), 1E5))) return st;
+  if ((st = launch_prepare_afac(c))) return st;
+  // set_sico_masks (:1678) depends only on TAF and Hi, which do not change
+  // during the viscosity iteration: once per solve gives the same masks
+  if ((st = launch_sico_masks(c))) return st;
+  return DIVA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void diva_config_defaults(diva_config_t* cfg) {
+  if (cfg) config_defaults(cfg);
+}
+
+void diva_grid_init(diva_grid_t* g, int32_t nx, int32_t ny, double dx, double xmin, double ymin) {
+  if (!g) return;
+  memset(g, 0, sizeof(*g));
+  g->nx = nx; g->ny = ny; g->nz = 15; g->dx = dx; g->xmin = xmin; g->ymin = ymin;
+  const double z[15] = {0.00, 0.10, 0.20, 0.30, 0.40, 0.50, 0.60, 0.70, 0.80, 0.90, 0.925, 0.95, 0.975, 0.99, 1.00};
+  for (int k = 0; k < 15; ++k) g->zeta[k] = z[k];
+}
+
+int diva_field_info(int32_t id, diva_field_info_t* out) {
+  if (id < 0 || id >= DIVA_NUM_FIELDS || !out) return DIVA_BAD_INPUT;
+  *out = g_info[id];
+  return DIVA_OK;
+}
+
+int64_t diva_field_numel(const diva_grid_t* g, int32_t id) {
+  if (!g || id < 0 || id >= DIVA_NUM_FIELDS) return -1;
+  return host_numel(g->nx, g->ny, g->nz, g_info[id].grid);
+}
+
+int diva_create(diva_ctx_t** out, const diva_grid_t* g, const diva_config_t* cfg) {
+  if (!out || !g || !cfg) return DIVA_BAD_INPUT;
+  *out = nullptr;
+  if (g->nx < 5 || g->ny < 5 || g->nz < 2 || g->nz > kMaxNz || !(g->dx > 0.0)) return DIVA_BAD_INPUT;
+  for (int k = 1; k < g->nz; ++k)
+    if (!(g->zeta[k] > g->zeta[k - 1])) return DIVA_BAD_INPUT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DIVA_CUDA_ERROR;
+  diva_ctx* h = new diva_ctx();
+  Ctx* c = &h->c;
+  int st = validate_config(c, cfg);
+  if (st) { delete h; return st; }
+  c->g = *g;
+  c->d.nx = g->nx; c->d.ny = g->ny; c->d.nz = g->nz;
+  c->d.ld = ((g->ny + 15) / 16) * 16;
+  c->d.plane = (long long)c->d.nx * c->d.ld;
+  c->d.dx = g->dx;
+  c->zt.nz = g->nz;
+  for (int k = 0; k < g->nz; ++k) {
+    c->zt.z[k] = g->zeta[k];
+    c->zt.z2[k] = pow(g->zeta[k], 2.0);
+  }
+  apply_config(c, cfg);
+  plan_levels(c);
+  Carver dry{nullptr, 0, true};
+  const size_t bytes = carve(c, dry);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return DIVA_CUDA_ERROR; }
+  c->own_stream = true;
+  if (cudaMalloc(&c->arena, bytes) != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete h;
+    return DIVA_CUDA_ERROR;
+  }
+  c->arena_bytes = bytes;
+  Carver real{c->arena, 0, false};
+  carve(c, real);
+  if (cudaMallocHost(&c->h_scal, sizeof(double) * SC_COUNT) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaMemsetAsync(c->arena, 0, bytes, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    diva_destroy(h);
+    return DIVA_CUDA_ERROR;
+  }
+  *out = h;
+  return DIVA_OK;
+}
+
+int diva_destroy(diva_ctx_t* h) {
+  if (!h) return DIVA_OK;
+  Ctx* c = &h->c;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int f = 0; f < DIVA_NUM_FIELDS; ++f)
+    if (c->saved[f]) cudaFree(c->saved[f]);
+  if (c->arena) cudaFree(c->arena);
+  if (c->h_scal) cudaFreeHost(c->h_scal);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete h;
+  return DIVA_OK;
+}
+
+int diva_set_config(diva_ctx_t* h, const diva_config_t* cfg) {
+  if (!h || !cfg) return DIVA_BAD_INPUT;
+  int st = validate_config(&h->c, cfg);
+  if (st) return st;
+  apply_config(&h->c, cfg);
+  return DIVA_OK;
+}
+
+int diva_set_stream(diva_ctx_t* h, void* stream) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (stream) {
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    c->stream = static_cast<cudaStream_t>(stream);
+    c->own_stream = false;
+  }
+  return DIVA_OK;
+}
+
+int diva_upload_field(diva_ctx_t* h, int32_t id, const void* host) {
+  if (!h || !host || id < 0 || id >= DIVA_NUM_FIELDS) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  const int kind = g_info[id].grid;
+  const size_t es = g_info[id].dtype == DIVA_DTYPE_D ? sizeof(double) : sizeof(int);
+  const size_t n = (size_t)host_numel(c->d.nx, c->d.ny, c->d.nz, kind);
+  DIVA_CUDA(c, cudaMemcpyAsync(c->staging, host, n * es, cudaMemcpyHostToDevice, c->stream));
+  if (g_info[id].dtype == DIVA_DTYPE_D) {
+    k_unpack<double><<<grid2d(c->d.ny, c->d.nx), block2d(), 0, c->stream>>>(c->d, kind, c->staging, c->D(id)); c->launches++;
+  } else {
+    k_unpack<int><<<grid2d(c->d.ny, c->d.nx), block2d(), 0, c->stream>>>(c->d, kind, (const int*)c->staging, c->I(id)); c->launches++;
+  }
+  DIVA_LAUNCHED(c, "k_unpack");
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_download_field(diva_ctx_t* h, int32_t id, void* host) {
+  if (!h || !host || id < 0 || id >= DIVA_NUM_FIELDS) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  const int kind = g_info[id].grid;
+  const size_t es = g_info[id].dtype == DIVA_DTYPE_D ? sizeof(double) : sizeof(int);
+  const size_t n = (size_t)host_numel(c->d.nx, c->d.ny, c->d.nz, kind);
+  if (g_info[id].dtype == DIVA_DTYPE_D) {
+    k_pack<double><<<grid2d(c->d.ny, c->d.nx), block2d(), 0, c->stream>>>(c->d, kind, c->D(id), c->staging); c->launches++;
+  } else {
+    k_pack<int><<<grid2d(c->d.ny, c->d.nx), block2d(), 0, c->stream>>>(c->d, kind, c->I(id), (int*)c->staging); c->launches++;
+  }
+  DIVA_LAUNCHED(c, "k_pack");
+  DIVA_CUDA(c, cudaMemcpyAsync(host, c->staging, n * es, cudaMemcpyDeviceToHost, c->stream));
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_upload(diva_ctx_t* h, const diva_fields_t* f) {
+  if (!h || !f) return DIVA_BAD_INPUT;
+  for (int q = 0; q < DIVA_NUM_FIELDS; ++q)
+    if (f->ptr[q]) {
+      int st = diva_upload_field(h, q, f->ptr[q]);
+      if (st) return st;
+    }
+  return DIVA_OK;
+}
+
+int diva_download(diva_ctx_t* h, const diva_fields_t* f) {
+  if (!h || !f) return DIVA_BAD_INPUT;
+  for (int q = 0; q < DIVA_NUM_FIELDS; ++q)
+    if (f->ptr[q]) {
+      int st = diva_download_field(h, q, f->ptr[q]);
+      if (st) return st;
+    }
+  return DIVA_OK;
+}
+
+int diva_update_general_ice_model_data(diva_ctx_t* h) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  int st = launch_update_general_ice_model_data(c);
+  if (st) return st;
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_calc_pressure_melting_point(diva_ctx_t* h) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  int st = launch_pressure_melting_point(c);
+  if (st) return st;
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_calc_ice_rheology(diva_ctx_t* h) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  int st = launch_ice_rheology(c);
+  if (st) return st;
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_calc_sia_3d_velocities(diva_ctx_t* h) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  int st = launch_sia(c);
+  if (st) return st;
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_solve_sia(diva_ctx_t* h, diva_report_t* rep) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  if (rep) { memset(rep, 0, sizeof(*rep)); rep->relres = -1.0; }
+  if (!(c->c.choice_ice_dynamics == DIVA_DYN_SIA || c->c.choice_ice_dynamics == DIVA_DYN_SIA_SSA))
+    return set_error(c, DIVA_BAD_INPUT, "solve_SIA should only be called when choice_ice_dynamics is SIA or SIA/SSA");
+  int st;
+  if ((st = begin(c))) return st;
+  if ((st = launch_sia(c))) return st;
+  if ((st = launch_secondary_velocities(c))) return st;
+  return finish(c, rep);
+}
+
+int diva_solve_diva(diva_ctx_t* h, diva_report_t* rep) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  if (rep) { memset(rep, 0, sizeof(*rep)); rep->relres = -1.0; }
+  if (c->c.choice_ice_dynamics != DIVA_DYN_DIVA)
+    return set_error(c, DIVA_BAD_INPUT, "solve_DIVA should only be called when choice_ice_dynamics is DIVA");
+  if (c->c.choice_ice_margin == DIVA_MARGIN_BC)
+    return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
+  int st;
+  if ((st = begin(c))) return st;
+  int any = 0;
+  if ((st = launch_any_sheet(c, &any))) return st;
+  if (!any) {
+    if ((st = launch_zero_velocities(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY)))) return st;
+    return finish(c, rep);
+  }
+  if ((st = prepare_velocity_solve(c))) return st;
+  const int pst = picard(c, true, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), rep);
+  if (pst != DIVA_OK && pst != DIVA_MAX_PICARD) return pst;
+  if ((st = launch_visc_b_output(c))) return st;
+  if ((st = launch_3d_horizontal_velocities(c))) return st;
+  if ((st = launch_secondary_velocities(c))) return st;
+  if ((st = finish(c, rep))) return st;
+  return pst;
+}
+
+int diva_solve_ssa(diva_ctx_t* h, diva_report_t* rep) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  if (rep) { memset(rep, 0, sizeof(*rep)); rep->relres = -1.0; }
+  if (!(c->c.choice_ice_dynamics == DIVA_DYN_SSA || c->c.choice_ice_dynamics == DIVA_DYN_SIA_SSA))
+    return set_error(c, DIVA_BAD_INPUT, "solve_SSA should only be called when choice_ice_dynamics is SSA or SIA/SSA");
+  if (c->c.choice_ice_margin == DIVA_MARGIN_BC)
+    return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
+  int st;
+  if ((st = begin(c))) return st;
+  int any = 0;
+  if ((st = launch_any_sheet(c, &any))) return st;
+  if (!any || c->c.choice_sliding_law == DIVA_SLIDING_NONE) {
+    if ((st = launch_zero_velocities(c, c->D(DIVA_F_U_SSA_CX), c->D(DIVA_F_V_SSA_CY)))) return st;
+    return finish(c, rep);
+  }
+  if ((st = prepare_velocity_solve(c))) return st;
+  const int pst = picard(c, false, c->D(DIVA_F_U_SSA_CX), c->D(DIVA_F_V_SSA_CY), rep);
+  if (pst != DIVA_OK && pst != DIVA_MAX_PICARD) return pst;
+  if ((st = launch_visc_b_output(c))) return st;
+  if ((st = launch_secondary_velocities(c))) return st;
+  if ((st = finish(c, rep))) return st;
+  return pst;
+}
+
+int diva_nonlinear_residual(diva_ctx_t* h, double* relres) {
+  if (!h || !relres) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  if (c->c.choice_ice_margin == DIVA_MARGIN_BC)
+    return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
+  int st;
+  if ((st = launch_driving_stress(c))) return st;
+  if ((st = launch_basal_conditions(c))) return st;
+  if ((st = launch_grounded_fractions(c))) return st;
+  if ((st = launch_prepare_afac(c))) return st;
+  if ((st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true))) return st;
+  if ((st = solver_setup(c))) return st;
+  return solver_relres(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), relres);
+}
+
+int diva_state_save(diva_ctx_t* h) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  for (int f = 0; f < DIVA_NUM_FIELDS; ++f) {
+    const size_t nb = field_dev_bytes(c, f);
+    if (!c->saved[f]) DIVA_CUDA(c, cudaMalloc(&c->saved[f], nb));
+    DIVA_CUDA(c, cudaMemcpyAsync(c->saved[f], c->f[f], nb, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  c->have_saved = true;
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_state_restore(diva_ctx_t* h) {
+  if (!h) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  if (!c->have_saved) return set_error(c, DIVA_BAD_INPUT, "no saved state");
+  for (int f = 0; f < DIVA_NUM_FIELDS; ++f)
+    DIVA_CUDA(c, cudaMemcpyAsync(c->f[f], c->saved[f], field_dev_bytes(c, f), cudaMemcpyDeviceToDevice, c->stream));
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, double* bytes) {
+  if (!h || !ms || !bytes || reps < 1 || which < 0 || which > 2) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  const double nc = (double)c->d.nx * c->d.ny, w = sizeof(double), nz = c->d.nz;
+  int st = DIVA_OK;
+  DIVA_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  for (int r = 0; r < reps && !st; ++r) {
+    switch (which) {
+      case 0: st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true); break;
+      case 1: st = solver_smooth_fine(c, 1); break;
+      case 2: st = solver_matvec_fine(c, 1); break;
+    }
+  }
+  if (st) return st;
+  DIVA_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  DIVA_CUDA(c, cudaEventSynchronize(c->ev1));
+  float t = 0.f;
+  DIVA_CUDA(c, cudaEventElapsedTime(&t, c->ev0, c->ev1));
+  *ms = t / reps;
+  // algorithmic bytes per launch (compulsory traffic per column, FP64):
+  //  0: read A-factor and the previous viscosity, write the new one (3 nz) + 15 2D fields
+  //  1: one sweep over both colours: u, v, N_a, N_b, beta_x, beta_y, b_u, b_v read, u, v written (10)
+  //  2: operator application: u, v, N_a, N_b, beta_x, beta_y read, A u, A v written (8)
+  const double per_col[3] = {(3 * nz + 15) * w, 10 * w, 8 * w};
+  *bytes = per_col[which] * nc;
+  return DIVA_OK;
+}
+
+int64_t diva_kernel_launches(const diva_ctx_t* h) { return h ? (int64_t)h->c.launches : -1; }
+
+const char* diva_last_error(const diva_ctx_t* h) { return h ? h->c.err.c_str() : ""; }
+
+const char* diva_status_string(int32_t s) {
+  switch (s) {
+    case DIVA_OK: return "OK";
+    case DIVA_MAX_PICARD: return "MAX_PICARD";
+    case DIVA_LINEAR_NOT_CONVERGED: return "LINEAR_NOT_CONVERGED";
+    case DIVA_NAN_DETECTED: return "NAN_DETECTED";
+    case DIVA_BAD_INPUT: return "BAD_INPUT";
+    case DIVA_CUDA_ERROR: return "CUDA_ERROR";
+    case DIVA_TIMEOUT: return "TIMEOUT";
+    case DIVA_UNSUPPORTED: return "UNSUPPORTED";
+  }
+  return "UNKNOWN";
+}
+
+}  // extern "C"

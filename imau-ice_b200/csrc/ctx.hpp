@@ -1,0 +1,121 @@
+// ctx.hpp -- device-resident state of one grid and the launchers shared by
+// the translation units of libdiva_b200.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include "common.cuh"
+
+namespace diva {
+
+constexpr int kMaxLevels = 12;
+
+// One multigrid level of the staggered DIVA operator.  Coefficients are the
+// rediscretised Na (a-grid), Nb (b-grid) and the reaction terms Bx = beta_eff_cx*dx^2
+// (cx) and By (cy) of the level's grid; idu/idv are the inverse effective
+// diagonals used by the Gauss-Seidel smoother.
+struct Level {
+  Dims d;
+  double *Na, *Nb, *Bx, *By, *idu, *idv;
+  double *xu, *xv, *bu, *bv, *ru, *rv;
+};
+
+// Boundary condition codes of the velocity unknowns (diva_bc_t), per side.
+struct BCs {
+  int uW, uE, uS, uN, vW, vE, vS, vN;
+};
+
+// Krylov vectors on the fine level, each a (u,v) pair of planes.
+enum { KV_X = 0, KV_R, KV_RHAT, KV_P, KV_PHAT, KV_V, KV_S, KV_SHAT, KV_T, KV_B, KV_COUNT };
+
+// Device scalars of the linear solver and of the Picard bookkeeping.
+enum {
+  SC_RHO = 0, SC_ALPHA, SC_OMEGA, SC_BETA, SC_RNORM2, SC_BNORM2, SC_SNORM2, SC_TMP0, SC_TMP1, SC_TMP2,
+  SC_RES1, SC_RES2, SC_NCNT, SC_RR, SC_BB, SC_NANFLAG, SC_FLAG, SC_COUNT = 32
+};
+
+struct Ctx {
+  diva_grid_t g;
+  diva_config_t c;
+  Dims d;
+  Zeta zt;
+  BCs bc;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  void* f[DIVA_NUM_FIELDS] = {};      // device pointer of each field
+  void* saved[DIVA_NUM_FIELDS] = {};  // state snapshot (diva_state_save)
+  bool have_saved = false;
+  // work buffers
+  double* visc_prev = nullptr;        // second buffer of visc_eff_3D_a (Picard double buffering)
+  double* afac = nullptr;             // 0.5 * A^(-1/n), per solve
+  double* quad[4] = {};               // grounded fractions of the four quadrants (NW, NE, SW, SE)
+  double* err_cand[2] = {};           // DIVA_err candidates (cx, cy)
+  double* staging = nullptr;          // upload/download staging (largest field)
+  int* ff_ocean = nullptr;            // flood-fill state
+  int* ff_flag = nullptr;
+  double* scal = nullptr;             // device scalars (SC_*)
+  double* h_scal = nullptr;           // pinned host mirror
+  double* partials = nullptr;         // block partial sums
+  int max_blocks = 0;
+  double* kv[KV_COUNT][2] = {};       // Krylov vectors (u,v)
+  Level lv[kMaxLevels];
+  int nlev = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // counters of the last solve
+  long lin_iters = 0, mg_cycles = 0;
+  long long launches = 0;            // kernels launched since create
+  double fine_passes = 0.0;
+  std::string err;
+
+  template <class T> T* F(int id) const { return static_cast<T*>(f[id]); }
+  double* D(int id) const { return static_cast<double*>(f[id]); }
+  int* I(int id) const { return static_cast<int*>(f[id]); }
+};
+
+// status helpers
+int set_error(Ctx* c, int code, const std::string& msg);
+int check_cuda(Ctx* c, cudaError_t e, const char* what);
+#define DIVA_CUDA(ctx, call)                                       \
+  do {                                                             \
+    cudaError_t e__ = (call);                                      \
+    if (e__ != cudaSuccess) return check_cuda((ctx), e__, #call);  \
+  } while (0)
+#define DIVA_LAUNCHED(ctx, what)                                   \
+  do {                                                             \
+    cudaError_t e__ = cudaGetLastError();                          \
+    if (e__ != cudaSuccess) return check_cuda((ctx), e__, (what)); \
+  } while (0)
+
+// geometry.cu
+int launch_update_general_ice_model_data(Ctx* c);
+int launch_pressure_melting_point(Ctx* c);
+int launch_ice_rheology(Ctx* c);
+int launch_basal_conditions(Ctx* c);
+int launch_grounded_fractions(Ctx* c);
+int launch_driving_stress(Ctx* c);
+int launch_sico_masks(Ctx* c);
+
+// picard.cu
+int launch_prepare_afac(Ctx* c);
+int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva);
+int launch_picard_update(Ctx* c, double* u, double* v, const double* xu, const double* xv, bool diva);
+int launch_commit_err(Ctx* c);
+int launch_basal_stress_velocities(Ctx* c);
+int launch_visc_b_output(Ctx* c);
+int launch_3d_horizontal_velocities(Ctx* c);
+int launch_secondary_velocities(Ctx* c);
+int launch_sia(Ctx* c);
+int launch_ssa_beta_eff(Ctx* c);
+int launch_zero_velocities(Ctx* c, double* u, double* v);
+int launch_any_sheet(Ctx* c, int* result);
+
+// solver.cu
+int solver_setup(Ctx* c);     // coefficients of all levels from N_a, N_b, beta_eff, taud
+int solver_solve(Ctx* c, const double* u0, const double* v0, double rtol, int maxit, int* iters, double* relres0);
+int solver_relres(Ctx* c, const double* u, const double* v, double* relres);
+int solver_fill_boundary(Ctx* c, double* u, double* v);
+int solver_smooth_fine(Ctx* c, int sweeps);
+int solver_matvec_fine(Ctx* c, int reps);
+
+}  // namespace diva

@@ -1,0 +1,300 @@
+"""Host-side mirror of IMAU-ICE's velocity interface.
+
+The reference exposes ``solve_SIA(grid, ice)``, ``solve_SSA(grid, ice)`` and
+``solve_DIVA(grid, ice)`` (src/ice_velocity_module.f90:36, :115, :249), which
+read TYPE(type_grid), update TYPE(type_ice_model) in place and take their
+settings from the global ``C%``.  This module keeps that shape:
+
+* ``Grid`` describes the square grid (nx, ny, dx, zeta);
+* an ice model is a ``dict`` of NumPy arrays named after the reference's
+  components (``ice["Hi_a"]``, ``ice["u_vav_cx"]``, ...), Fortran-ordered with
+  the reference's shapes, e.g. ``(ny, nx-1)`` for a cx-grid field and
+  ``(nz, ny, nx)`` for a 3D a-grid field, so ``ice["Hi_a"][j, i]`` is
+  ``ice%Hi_a(j+1, i+1)``;
+* ``solve_DIVA(grid, ice, config)`` etc. copy the inputs to the GPU, run the
+  solve there and write the outputs back into ``ice``.
+
+For repeated solves on one grid, ``Context`` keeps the whole state resident on
+the GPU between calls (upload once, solve many times, download on request),
+which is how the Fortran shim in INTEGRATION.md drives the library.
+
+The product backend is ``libdiva_b200.so`` (CUDA, sm_100a).  There is no CPU
+fallback: if the library or a GPU is missing, creating a context raises.
+"""
+import ctypes as C
+import os
+import numpy as np
+
+from . import _abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libdiva_b200.so")
+
+ZETA_DEFAULT = [0.00, 0.10, 0.20, 0.30, 0.40, 0.50, 0.60, 0.70, 0.80, 0.90,
+                0.925, 0.95, 0.975, 0.99, 1.00]   # configuration_module.f90:168-170
+
+
+class DivaError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Backend:
+    """A loaded implementation of the diva.h entry points (``prefix`` + name)."""
+
+    def __init__(self, path, prefix, name):
+        if not os.path.exists(path):
+            raise DivaError(_abi.BAD_INPUT, f"library not built: {path}")
+        self.lib = C.CDLL(path)
+        self.fns = _abi.bind(self.lib, prefix)
+        self.prefix = prefix
+        self.name = name
+        self.path = path
+        self._fields = None
+
+    def fields(self):
+        if self._fields is None:
+            out, info, i = [], _abi.FieldInfo(), 0
+            while self.fns["field_info"](i, C.byref(info)) == 0:
+                out.append((info.name.decode(), _abi.GRID_KINDS[info.grid], "f8" if info.dtype == 0 else "i4"))
+                i += 1
+            self._fields = out
+        return self._fields
+
+    def default_config(self):
+        cfg = _abi.Config()
+        self.fns["config_defaults"](C.byref(cfg))
+        return cfg
+
+
+_CUDA = None
+
+
+def cuda_backend():
+    """The product backend; loads ``lib/libdiva_b200.so`` once."""
+    global _CUDA
+    if _CUDA is None:
+        _CUDA = Backend(LIB_PATH, "diva_", "cuda")
+    return _CUDA
+
+
+class Grid:
+    """TYPE(type_grid) (data_types_module.f90:13-29): a regular square grid."""
+
+    def __init__(self, nx, ny, dx, zeta=None, xmin=0.0, ymin=0.0):
+        self.nx, self.ny, self.dx = int(nx), int(ny), float(dx)
+        self.zeta = np.asarray(ZETA_DEFAULT if zeta is None else zeta, dtype=np.float64)
+        self.nz = len(self.zeta)
+        self.xmin, self.ymin = float(xmin), float(ymin)
+        if self.nz > _abi.MAX_NZ or self.nz < 2:
+            raise DivaError(_abi.BAD_INPUT, f"nz={self.nz} outside 2..{_abi.MAX_NZ}")
+
+    @property
+    def x(self):
+        return self.xmin + self.dx * np.arange(self.nx)
+
+    @property
+    def y(self):
+        return self.ymin + self.dx * np.arange(self.ny)
+
+    def to_c(self):
+        g = _abi.Grid()
+        g.nx, g.ny, g.nz, g.dx, g.xmin, g.ymin = self.nx, self.ny, self.nz, self.dx, self.xmin, self.ymin
+        for k, z in enumerate(self.zeta):
+            g.zeta[k] = z
+        return g
+
+    def shape(self, kind):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        return {"A": (ny, nx), "CX": (ny, nx - 1), "CY": (ny - 1, nx), "B": (ny - 1, nx - 1),
+                "A3": (nz, ny, nx), "CX3": (nz, ny, nx - 1), "CY3": (nz, ny - 1, nx),
+                "B3": (nz, ny - 1, nx - 1)}[kind]
+
+
+def make_config(backend, overrides=None):
+    """Reference defaults with ``overrides`` (strings for the string options)."""
+    cfg = backend.default_config()
+    for k, v in (overrides or {}).items():
+        if k in _abi.ENUM_OPTIONS and isinstance(v, str):
+            v = _abi.ENUM_OPTIONS[k][v]
+        if not hasattr(cfg, k):
+            raise DivaError(_abi.BAD_INPUT, f"unknown config option {k}")
+        setattr(cfg, k, v)
+    return cfg
+
+
+class Context:
+    """Device-resident state of one grid (allocate_ice_model + solution matrix)."""
+
+    def __init__(self, grid, config=None, backend=None):
+        self.backend = backend or cuda_backend()
+        self.grid = grid
+        self.fields = {name: (kind, dt) for name, kind, dt in self.backend.fields()}
+        self.ids = {name: i for i, (name, _, _) in enumerate(self.backend.fields())}
+        self.cfg = config if isinstance(config, _abi.Config) else make_config(self.backend, config)
+        self._g = grid.to_c()
+        h = C.c_void_p()
+        st = self.backend.fns["create"](C.byref(h), C.byref(self._g), C.byref(self.cfg))
+        if st != 0:
+            raise DivaError(st, f"{self.backend.prefix}create failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.backend.fns["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st not in (0, _abi.MAX_PICARD):
+            err = self.backend.fns["last_error"](self.h)
+            raise DivaError(st, f"{what}: {err.decode() if err else ''}")
+        return st
+
+    def set_config(self, overrides):
+        self.cfg = make_config(self.backend, overrides) if not isinstance(overrides, _abi.Config) else overrides
+        self._check(self.backend.fns["set_config"](self.h, C.byref(self.cfg)), "set_config")
+
+    # ---- field I/O ---------------------------------------------------------
+    def empty(self, name):
+        kind, dt = self.fields[name]
+        return np.zeros(self.grid.shape(kind), dtype=dt, order="F")
+
+    def upload(self, ice):
+        for name, arr in ice.items():
+            if name not in self.fields:
+                continue
+            kind, dt = self.fields[name]
+            a = np.asfortranarray(arr, dtype=dt)
+            if a.shape != self.grid.shape(kind):
+                raise DivaError(_abi.BAD_INPUT, f"{name}: shape {a.shape} != {self.grid.shape(kind)}")
+            self._check(self.backend.fns["upload_field"](self.h, self.ids[name], a.ctypes.data), f"upload {name}")
+
+    def download(self, names=None):
+        out = {}
+        for name in (names or self.fields.keys()):
+            a = self.empty(name)
+            self._check(self.backend.fns["download_field"](self.h, self.ids[name], a.ctypes.data), f"download {name}")
+            out[name] = a
+        return out
+
+    # ---- the reference's routines ---------------------------------------------
+    def update_general_ice_model_data(self):
+        self._check(self.backend.fns["update_general_ice_model_data"](self.h), "update_general_ice_model_data")
+
+    def calc_pressure_melting_point(self):
+        self._check(self.backend.fns["calc_pressure_melting_point"](self.h), "calc_pressure_melting_point")
+
+    def calc_ice_rheology(self):
+        self._check(self.backend.fns["calc_ice_rheology"](self.h), "calc_ice_rheology")
+
+    def _solve(self, fn, what):
+        rep = _abi.Report()
+        self._check(self.backend.fns[fn](self.h, C.byref(rep)), what)
+        return rep.as_dict()
+
+    def solve_SIA(self):
+        return self._solve("solve_sia", "solve_SIA")
+
+    def solve_SSA(self):
+        return self._solve("solve_ssa", "solve_SSA")
+
+    def solve_DIVA(self):
+        return self._solve("solve_diva", "solve_DIVA")
+
+    def calc_sia_3d_velocities(self):
+        self._check(self.backend.fns["calc_sia_3d_velocities"](self.h), "calc_sia_3d_velocities")
+
+    def nonlinear_residual(self):
+        r = C.c_double()
+        self._check(self.backend.fns["nonlinear_residual"](self.h, C.byref(r)), "nonlinear_residual")
+        return r.value
+
+    def state_save(self):
+        self._check(self.backend.fns["state_save"](self.h), "state_save")
+
+    def state_restore(self):
+        self._check(self.backend.fns["state_restore"](self.h), "state_restore")
+
+    # ---- CUDA-library extras ---------------------------------------------------
+    def set_stream(self, stream_handle):
+        """Run all of this context's work on a caller's CUDA stream (cudaStream_t as int)."""
+        f = self.backend.lib.diva_set_stream
+        f.argtypes = [C.c_void_p, C.c_void_p]
+        self._check(f(self.h, C.c_void_p(stream_handle)), "set_stream")
+
+    def kernel_launches(self):
+        """Kernels this context has launched since creation (diva_kernel_launches)."""
+        f = self.backend.lib.diva_kernel_launches
+        f.argtypes = [C.c_void_p]
+        f.restype = C.c_int64
+        return int(f(self.h))
+
+    def profile_kernel(self, which, reps=20):
+        """(ms per launch, algorithmic bytes per launch) of one hot kernel (diva_profile_kernel)."""
+        f = self.backend.lib.diva_profile_kernel
+        f.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        ms, nb = C.c_double(), C.c_double()
+        self._check(f(self.h, which, reps, C.byref(ms), C.byref(nb)), "profile_kernel")
+        return ms.value, nb.value
+
+
+# Fields each routine writes (downloaded back into the caller's dict).
+OUT_UPDATE = ["Hs_a", "TAF_a", "mask_land_a", "mask_ocean_a", "mask_ice_a", "mask_sheet_a", "mask_shelf_a",
+              "mask_coast_a", "mask_margin_a", "mask_gl_a", "mask_cf_a", "mask_a", "Hi_cx", "Hi_cy", "Hi_b",
+              "dHi_dx_a", "dHi_dy_a", "dHs_dx_a", "dHs_dy_a", "dHs_dx_cx", "dHs_dy_cx", "dHs_dx_cy", "dHs_dy_cy",
+              "A_flow_3D_cx", "A_flow_3D_cy", "A_flow_vav_cx", "A_flow_vav_cy"]
+OUT_RHEOLOGY = ["A_flow_3D_a", "A_flow_vav_a", "A_flow_3D_cx", "A_flow_3D_cy", "A_flow_vav_cx", "A_flow_vav_cy"]
+OUT_SECONDARY = ["u_3D_cx", "v_3D_cy", "w_3D_a", "u_3D_a", "v_3D_a", "u_vav_cx", "v_vav_cy",
+                 "u_surf_cx", "v_surf_cy", "u_base_cx", "v_base_cy", "u_vav_a", "v_vav_a", "u_surf_a", "v_surf_a",
+                 "u_base_a", "v_base_a", "uabs_vav_a", "uabs_surf_a", "uabs_base_a", "w_surf_a", "w_base_a", "R_shear"]
+OUT_PICARD = ["taudx_cx", "taudy_cy", "f_grnd_a", "f_grnd_cx", "f_grnd_cy", "f_grnd_b", "Neff_a",
+              "pore_water_pressure_a", "overburden_pressure_a", "tauc_a",
+              "visc_eff_3D_a", "visc_eff_int_a", "visc_eff_3D_b", "visc_eff_int_b", "N_a", "N_b", "N_cx", "N_cy",
+              "beta_a", "beta_eff_a", "beta_eff_cx", "beta_eff_cy", "u_cx_prev", "v_cy_prev",
+              "DIVA_err_cx", "DIVA_err_cy", "DIVA_mask_combi", "DIVA_isfront_inner", "DIVA_isfront_outer"]
+OUT_DIVA = OUT_PICARD + ["du_dz_3D_cx", "dv_dz_3D_cy", "F2_a", "F1_3D_a", "taub_cx", "taub_cy"] + OUT_SECONDARY
+OUT_SSA = OUT_PICARD + ["u_SSA_cx", "v_SSA_cy"] + OUT_SECONDARY
+OUT_SIA = ["u_3D_SIA_cx", "v_3D_SIA_cy"] + OUT_SECONDARY
+
+
+def _run(grid, ice, config, backend, fn, outputs):
+    ctx = Context(grid, config, backend)
+    try:
+        ctx.upload(ice)
+        rep = getattr(ctx, fn)()
+        ice.update(ctx.download(outputs) if outputs is not None else ctx.download())
+        return rep
+    finally:
+        ctx.close()
+
+
+def update_general_ice_model_data(grid, ice, config=None, backend=None):
+    """general_ice_model_data_module.f90:30-86 on the GPU; updates ``ice`` in place."""
+    return _run(grid, ice, config, backend, "update_general_ice_model_data", OUT_UPDATE)
+
+
+def calc_ice_rheology(grid, ice, config=None, backend=None):
+    """thermodynamics_module.f90:641-753 on the GPU; updates ``ice`` in place."""
+    return _run(grid, ice, config, backend, "calc_ice_rheology", OUT_RHEOLOGY)
+
+
+def solve_SIA(grid, ice, config=None, backend=None):
+    """ice_velocity_module.f90:36-114 on the GPU; updates ``ice`` in place."""
+    return _run(grid, ice, config, backend, "solve_SIA", OUT_SIA)
+
+
+def solve_SSA(grid, ice, config=None, backend=None):
+    """ice_velocity_module.f90:115-248 on the GPU; updates ``ice`` in place."""
+    return _run(grid, ice, config, backend, "solve_SSA", OUT_SSA)
+
+
+def solve_DIVA(grid, ice, config=None, backend=None):
+    """ice_velocity_module.f90:249-374 on the GPU; updates ``ice`` in place."""
+    return _run(grid, ice, config, backend, "solve_DIVA", OUT_DIVA)

@@ -1,0 +1,225 @@
+/*
+ * diva.h -- C ABI of the B200 ice-velocity library (libdiva_b200.so).
+ *
+ * Drop-in replacement for the velocity hot path of IMAU-ICE:
+ *   SUBROUTINE solve_SIA ( grid, ice)   src/ice_velocity_module.f90:36-114
+ *   SUBROUTINE solve_SSA ( grid, ice)   src/ice_velocity_module.f90:115-248
+ *   SUBROUTINE solve_DIVA( grid, ice)   src/ice_velocity_module.f90:249-374
+ * plus the routines that prepare their inputs on the same device-resident
+ * state:
+ *   update_general_ice_model_data       src/general_ice_model_data_module.f90:30-86
+ *   calc_pressure_melting_point         src/thermodynamics_module.f90:609-640
+ *   calc_ice_rheology                   src/thermodynamics_module.f90:641-753
+ *
+ * The Fortran reference passes TYPE(type_grid) and TYPE(type_ice_model) and
+ * reads its settings from the global C%.  Here the grid and the settings are
+ * given once to diva_create(), the ice fields are copied in and out through
+ * diva_upload()/diva_download() (host arrays in Fortran order, shapes as in
+ * diva_fields.h), and everything in between stays resident in GPU memory.
+ *
+ * All entry points return a diva_status_t; 0 is success.  No entry point
+ * terminates the process (the reference calls crash() -> MPI_ABORT).
+ */
+#ifndef DIVA_H
+#define DIVA_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "diva_fields.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DIVA_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum {
+  DIVA_OK = 0,
+  DIVA_MAX_PICARD = 1,          /* viscosity iteration hit its cap (non-fatal, as in the reference) */
+  DIVA_LINEAR_NOT_CONVERGED = 2,/* linear solve missed its tolerance within its iteration cap */
+  DIVA_NAN_DETECTED = 3,        /* NaN/Inf in the solution (check_for_NaN_dp_* analogue) */
+  DIVA_BAD_INPUT = 4,           /* invalid argument, size, option or calling mode */
+  DIVA_CUDA_ERROR = 5,          /* a CUDA runtime call failed */
+  DIVA_TIMEOUT = 6,             /* a bounded device-side loop ran out of iterations */
+  DIVA_UNSUPPORTED = 7          /* option not implemented by this backend */
+} diva_status_t;
+
+/* ---- field identifiers (diva_fields.h) --------------------------------- */
+typedef enum {
+#define DIVA_X_ENUM(ID, name, grid, type) DIVA_F_##ID,
+  DIVA_FIELD_LIST(DIVA_X_ENUM)
+#undef DIVA_X_ENUM
+  DIVA_NUM_FIELDS
+} diva_field_id_t;
+
+typedef enum { DIVA_GRID_A = 0, DIVA_GRID_CX, DIVA_GRID_CY, DIVA_GRID_B,
+               DIVA_GRID_A3, DIVA_GRID_CX3, DIVA_GRID_CY3, DIVA_GRID_B3 } diva_grid_kind_t;
+typedef enum { DIVA_DTYPE_D = 0, DIVA_DTYPE_I = 1 } diva_dtype_t;
+
+typedef struct {
+  const char* name;   /* reference component name, e.g. "u_vav_cx" */
+  int grid;           /* diva_grid_kind_t */
+  int dtype;          /* diva_dtype_t */
+} diva_field_info_t;
+
+/* ---- option enums (string options of the reference's C%) ---------------- */
+typedef enum { DIVA_DYN_SIA = 0, DIVA_DYN_SSA = 1, DIVA_DYN_SIA_SSA = 2, DIVA_DYN_DIVA = 3 } diva_dynamics_t;
+typedef enum { DIVA_MARGIN_INFINITE_SLAB = 0, DIVA_MARGIN_BC = 1 } diva_margin_t;
+typedef enum { DIVA_BC_INFINITE = 0, DIVA_BC_ZERO = 1, DIVA_BC_PERIODIC = 2 } diva_bc_t;
+typedef enum { DIVA_SLIDING_NONE = 0, DIVA_SLIDING_WEERTMAN = 1, DIVA_SLIDING_COULOMB = 2,
+               DIVA_SLIDING_COULOMB_REGULARISED = 3, DIVA_SLIDING_TSAI2015 = 4,
+               DIVA_SLIDING_SCHOOF2005 = 5, DIVA_SLIDING_ZOET_IVERSON = 6 } diva_sliding_t;
+typedef enum { DIVA_HYDRO_DRY = 0, DIVA_HYDRO_SATURATED = 1, DIVA_HYDRO_MARTIN2011 = 2 } diva_hydro_t;
+typedef enum { DIVA_RHEO_UNIFORM = 0, DIVA_RHEO_HUYBRECHTS1992 = 1 } diva_rheology_t;
+/* Picard stop test: the reference's step norm resid_UV (ice_velocity_module.f90:1530-1601),
+ * or the FP64 nonlinear residual ||b(u) - A(u) u|| / ||b(u)||. */
+typedef enum { DIVA_STOP_RESID_UV = 0, DIVA_STOP_RELRES = 1 } diva_stop_t;
+/* Arithmetic of the linear solves: plain FP64, or FP32 multigrid inside FP64 defect correction. */
+typedef enum { DIVA_PREC_FP64 = 0, DIVA_PREC_MIXED = 1 } diva_precision_t;
+
+/* ---- grid (TYPE(type_grid), data_types_module.f90:13-29) --------------- */
+typedef struct {
+  int32_t nx, ny, nz;     /* a-grid size; number of scaled-zeta layers */
+  double dx;              /* square cells, dx = dy [m] */
+  double xmin, ymin;      /* x(1), y(1) [m] (informational) */
+  double zeta[64];        /* C%zeta(1:nz), 0 at the surface, 1 at the base */
+} diva_grid_t;
+
+/* ---- configuration (the C% fields the path reads) ----------------------- */
+typedef struct {
+  int32_t choice_ice_dynamics;          /* diva_dynamics_t        configuration_module.f90:271 */
+  double  n_flow;                       /* Glen exponent                                   :272 */
+  double  m_enh_sheet, m_enh_shelf;     /* enhancement factors                         :273-274 */
+  int32_t choice_ice_margin;            /* diva_margin_t                                   :275 */
+  int32_t include_SSADIVA_crossterms;   /*                                                 :276 */
+  int32_t do_GL_subgrid_friction;       /*                                                 :277 */
+  double  DIVA_visc_it_norm_dUV_tol;    /*                                                 :282 */
+  int32_t DIVA_visc_it_nit;             /*                                                 :283 */
+  double  DIVA_visc_it_relax;           /*                                                 :284 */
+  double  DIVA_epsilon_sq_0;            /*                                                 :285 */
+  double  DIVA_visc_eff_min;            /*                                                 :286 */
+  double  DIVA_beta_max;                /*                                                 :287 */
+  double  DIVA_vel_max;                 /*                                                 :288 */
+  int32_t BC_u_west, BC_u_east, BC_u_south, BC_u_north;   /* diva_bc_t               :289-292 */
+  int32_t BC_v_west, BC_v_east, BC_v_south, BC_v_north;   /* diva_bc_t               :293-296 */
+  int32_t choice_sliding_law;           /* diva_sliding_t                                  :349 */
+  double  slid_delta_v;                 /*                                                 :351 */
+  double  slid_Weertman_m;              /*                                                 :352 */
+  double  slid_Coulomb_reg_q_plastic;   /*                                                 :353 */
+  double  slid_Coulomb_reg_u_threshold; /*                                                 :354 */
+  double  slid_ZI_ut, slid_ZI_p;        /*                                             :355-356 */
+  int32_t include_basal_freezing;       /*                                                 :357 */
+  double  deltaT_basal_freezing;        /*                                                 :358 */
+  int32_t choice_basal_hydrology;       /* diva_hydro_t                                    :361 */
+  double  Martin2011_hydro_Hb_min, Martin2011_hydro_Hb_max;  /*                       :362-363 */
+  int32_t choice_ice_rheology;          /* diva_rheology_t                                 :424 */
+  double  uniform_flow_factor;          /*                                                 :425 */
+  int32_t do_ocean_floodfill;           /*                                                 :702 */
+  /* Coulomb law with tauc_a given as input (choice_param_basal_roughness 'SSA_icestream',
+   * basal_conditions_and_sliding_module.f90:1021-1023) instead of tan(phi_fric) * Neff */
+  int32_t prescribed_tauc;
+  /* linear solve: replaces DIVA_PETSc_rtol/abstol (:301-302) and DIVA_SOR_* (:298-300) */
+  double  lin_rtol;                     /* relative residual target of every linear solve */
+  int32_t lin_maxit;                    /* Krylov iteration cap per linear solve */
+  /* Picard stop rule */
+  int32_t picard_stop;                  /* diva_stop_t */
+  double  picard_relres_tol;            /* used when picard_stop == DIVA_STOP_RELRES */
+  int32_t lin_adaptive;                 /* RELRES mode: linear rtol tied to the current nonlinear residual */
+  int32_t precision;                    /* diva_precision_t */
+  int32_t reserved[8];
+} diva_config_t;
+
+/* ---- per-solve report --------------------------------------------------- */
+typedef struct {
+  int32_t status;                 /* diva_status_t of the solve */
+  int32_t picard_iterations;      /* viscosity iterations taken */
+  int32_t linear_iterations;      /* Krylov iterations summed over the solve */
+  int32_t mg_cycles;              /* multigrid V-cycles summed over the solve */
+  double  resid_UV;               /* last step norm (ice_velocity_module.f90:1530-1601) */
+  double  relres;                 /* last FP64 nonlinear relative residual (-1 if not evaluated) */
+  double  fine_passes;            /* fine-grid-equivalent stencil passes (for byte counting) */
+  double  elapsed_ms;             /* device time of the call (CUDA events); 0 for the CPU oracle */
+  int32_t reserved[8];
+} diva_report_t;
+
+/* Host pointers for upload/download, indexed by diva_field_id_t; NULL = skip. */
+typedef struct { void* ptr[DIVA_NUM_FIELDS]; } diva_fields_t;
+
+typedef struct diva_ctx diva_ctx_t;
+
+/* Defaults of configuration_module.f90:271-367, 424-426, 702 (with the velocity
+ * options of the reference's default run: DIVA, infinite slab, cross terms). */
+void diva_config_defaults(diva_config_t* cfg);
+/* C%zeta default (configuration_module.f90:168-170) and nz = 15. */
+void diva_grid_init(diva_grid_t* grid, int32_t nx, int32_t ny, double dx, double xmin, double ymin);
+
+int  diva_field_info(int32_t id, diva_field_info_t* out);
+/* Number of elements of a field on this grid (e.g. nz*ny*(nx-1) for CX3). */
+int64_t diva_field_numel(const diva_grid_t* grid, int32_t id);
+
+/* Allocate all device state for one grid; replaces allocate_ice_model
+ * (ice_dynamics_module.f90:1034-1251) and initialise_SSADIVA_solution_matrix
+ * (ice_velocity_module.f90:2814-2860).  All fields start at zero. */
+int  diva_create(diva_ctx_t** ctx, const diva_grid_t* grid, const diva_config_t* cfg);
+int  diva_destroy(diva_ctx_t* ctx);
+int  diva_set_config(diva_ctx_t* ctx, const diva_config_t* cfg);
+/* Bind a CUDA stream (cudaStream_t as void*; NULL = the library's own stream). */
+int  diva_set_stream(diva_ctx_t* ctx, void* stream);
+
+int  diva_upload(diva_ctx_t* ctx, const diva_fields_t* host);
+int  diva_download(diva_ctx_t* ctx, const diva_fields_t* host);
+int  diva_upload_field(diva_ctx_t* ctx, int32_t id, const void* host);
+int  diva_download_field(diva_ctx_t* ctx, int32_t id, void* host);
+
+/* update_general_ice_model_data (general_ice_model_data_module.f90:30-86). */
+int  diva_update_general_ice_model_data(diva_ctx_t* ctx);
+/* calc_pressure_melting_point (thermodynamics_module.f90:609-640). */
+int  diva_calc_pressure_melting_point(diva_ctx_t* ctx);
+/* calc_ice_rheology (thermodynamics_module.f90:641-753). */
+int  diva_calc_ice_rheology(diva_ctx_t* ctx);
+
+/* solve_SIA (ice_velocity_module.f90:36-114); needs choice_ice_dynamics SIA or SIA/SSA. */
+int  diva_solve_sia(diva_ctx_t* ctx, diva_report_t* rep);
+/* solve_SSA (ice_velocity_module.f90:115-248); needs SSA or SIA/SSA. */
+int  diva_solve_ssa(diva_ctx_t* ctx, diva_report_t* rep);
+/* solve_DIVA (ice_velocity_module.f90:249-374); needs DIVA. */
+int  diva_solve_diva(diva_ctx_t* ctx, diva_report_t* rep);
+/* The SIA 3D velocity loop of solve_SIA (ice_velocity_module.f90:60-105) alone,
+ * in any dynamics mode (used for "DIVA plus SIA" diagnostics). */
+int  diva_calc_sia_3d_velocities(diva_ctx_t* ctx);
+
+/* FP64 nonlinear residual of the current (u_vav_cx, v_vav_cy): evaluates the
+ * coefficients of the next viscosity iteration (A3-A7) and returns
+ * ||b - A u||_2 / ||b||_2 over the interior rows.  Leaves the state unchanged
+ * except for the coefficient fields. */
+int  diva_nonlinear_residual(diva_ctx_t* ctx, double* relres);
+
+/* Snapshot / restore of the Picard state that persists across calls
+ * (velocities, visc_eff_3D_a, taub, u_3D_a, v_3D_a, u_3D_cx, v_3D_cy ...):
+ * a device-side checkpoint, replacing a cold restart from u = 0. */
+int  diva_state_save(diva_ctx_t* ctx);
+int  diva_state_restore(diva_ctx_t* ctx);
+
+/* Time one hot kernel of the current state in isolation: `which` selects
+ *   0  the fused column-coefficient kernel (viscosity, F2, beta, beta_eff) + face kernel
+ *   1  one full Gauss-Seidel sweep (4 colours) of the fine-level operator
+ *   2  one fine-level operator application (matrix-free A x with dot products)
+ * `reps` launches are bracketed by CUDA events on the context's stream;
+ * returns the mean device time per launch and the algorithmic bytes one launch
+ * must move.  Needs a context that has completed a solve; kind 0 leaves the
+ * coefficient fields of the next viscosity iteration behind, kinds 1-2 touch
+ * only solver scratch vectors. */
+int  diva_profile_kernel(diva_ctx_t* ctx, int32_t which, int32_t reps, double* ms_per_launch,
+                         double* bytes_per_launch);
+
+/* Number of kernels this context has launched since diva_create. */
+int64_t diva_kernel_launches(const diva_ctx_t* ctx);
+
+const char* diva_last_error(const diva_ctx_t* ctx);
+const char* diva_status_string(int32_t status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DIVA_H */

@@ -1,0 +1,117 @@
+"""Behaviour of the C ABI on the GPU: determinism, checkpoint/restore, the
+reference-shaped Python API, error codes, and failure handling without any
+device fault (bad inputs are injected on the host)."""
+import numpy as np
+import pytest
+
+from imau_ice_b200 import _abi, diva
+import helpers
+
+pytestmark = pytest.mark.gpu
+
+
+def small():
+    return helpers.make_case(2, dx=40e3, overrides={"lin_rtol": 1e-10})
+
+
+def test_bitwise_deterministic(cuda):
+    g, cfg, f = small()
+    r1, o1 = helpers.run(cuda, g, cfg, f)
+    r2, o2 = helpers.run(cuda, g, cfg, f)
+    assert r1["picard_iterations"] == r2["picard_iterations"]
+    for k in ("u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "w_3D_a"):
+        assert np.array_equal(o1[k], o2[k]), k
+
+
+def test_state_save_restore_reproduces_a_solve(cuda):
+    g, cfg, f = small()
+    ctx = diva.Context(g, cfg, cuda)
+    helpers.prepare(ctx, f)
+    ctx.state_save()
+    r1 = ctx.solve_DIVA()
+    a = ctx.download(["u_vav_cx", "v_vav_cy", "u_3D_a"])
+    ctx.state_restore()
+    r2 = ctx.solve_DIVA()
+    b = ctx.download(["u_vav_cx", "v_vav_cy", "u_3D_a"])
+    ctx.close()
+    assert r1["picard_iterations"] == r2["picard_iterations"]
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_warm_start_converges_faster(cuda):
+    g, cfg, f = helpers.make_case(2, dx=40e3, overrides={"picard_stop": "relres", "picard_relres_tol": 1e-6,
+                                                         "DIVA_visc_it_nit": 300, "lin_adaptive": 1})
+    ctx = diva.Context(g, cfg, cuda)
+    helpers.prepare(ctx, f)
+    cold = ctx.solve_DIVA()
+    warm = ctx.solve_DIVA()          # second call starts from the converged state
+    ctx.close()
+    assert cold["relres"] <= 1e-6 and warm["relres"] <= 1e-6
+    assert warm["picard_iterations"] < cold["picard_iterations"]
+
+
+def test_reference_shaped_functions(cuda):
+    g, cfg, f = small()
+    ice = dict(f)
+    diva.update_general_ice_model_data(g, ice, cfg, cuda)
+    assert "mask_sheet_a" in ice and ice["mask_sheet_a"].sum() > 0
+    rep = diva.solve_DIVA(g, ice, cfg, cuda)
+    assert rep["picard_iterations"] >= 1
+    assert ice["u_vav_cx"].shape == (g.ny, g.nx - 1) and ice["u_3D_cx"].shape == (g.nz, g.ny, g.nx - 1)
+    assert np.isfinite(ice["u_vav_cx"]).all()
+
+
+def test_wrong_dynamics_mode_is_rejected(cuda):
+    g, cfg, f = small()
+    ctx = diva.Context(g, cfg, cuda)
+    with pytest.raises(diva.DivaError) as e:
+        ctx.solve_SIA()
+    assert e.value.status == _abi.BAD_INPUT
+    ctx.close()
+
+
+def test_bc_margins_are_reported_unsupported(cuda):
+    g, cfg, f = small()
+    ctx = diva.Context(g, dict(cfg, choice_ice_margin="BC"), cuda)
+    helpers.prepare(ctx, f)
+    with pytest.raises(diva.DivaError) as e:
+        ctx.solve_DIVA()
+    assert e.value.status == _abi.UNSUPPORTED
+    ctx.close()
+
+
+def test_bad_grid_rejected(cuda):
+    with pytest.raises(diva.DivaError) as e:
+        diva.Context(diva.Grid(3, 3, 1e3), {}, cuda)
+    assert e.value.status == _abi.BAD_INPUT
+
+
+def test_nan_input_is_reported_not_faulted(cuda):
+    """A corrupt input (NaN thickness) ends the solve with NAN_DETECTED; the context stays usable."""
+    g, cfg, f = small()
+    bad = dict(f)
+    H = np.array(f["Hi_a"])
+    H[g.ny // 2, g.nx // 2] = np.nan
+    bad["Hi_a"] = np.asfortranarray(H)
+    ctx = diva.Context(g, cfg, cuda)
+    helpers.prepare(ctx, bad)
+    with pytest.raises(diva.DivaError) as e:
+        ctx.solve_DIVA()
+    assert e.value.status == _abi.NAN_DETECTED
+    zeros = {k: ctx.empty(k) for k in ("u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "taub_cx", "taub_cy",
+                                       "u_3D_a", "v_3D_a")}
+    ctx.upload(zeros)                        # recover on the same context from a cold state
+    helpers.prepare(ctx, f)
+    rep = ctx.solve_DIVA()
+    ctx.close()
+    assert rep["status"] in (_abi.OK, _abi.MAX_PICARD)
+
+
+def test_linear_iteration_cap_is_bounded(cuda):
+    g, cfg, f = helpers.make_case(2, dx=40e3, overrides={"lin_maxit": 1, "lin_rtol": 1e-14, "DIVA_visc_it_nit": 5})
+    ctx = diva.Context(g, cfg, cuda)
+    helpers.prepare(ctx, f)
+    rep = ctx.solve_DIVA()
+    ctx.close()
+    assert rep["picard_iterations"] == 5 and rep["linear_iterations"] == 5
