@@ -241,6 +241,7 @@ def run_b200(args):
         dist.barrier()
     clk = clocks.stop()
     launches = ctx.kernel_launches() - l0
+    ms = e0.elapsed_time(e1)
     if args.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": world * args.steps / (ms / 1000.0), "unit": UNIT,
@@ -249,7 +250,6 @@ def run_b200(args):
         if world > 1:
             dist.destroy_process_group()
         return 0
-    ms = e0.elapsed_time(e1)
     t = torch.tensor([ms], device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -42,6 +42,13 @@ struct Zeta {
   double zn[kMaxNz];   // zeta**n_flow
 };
 
+// MAX and MIN as gfortran expands them for the reference (mvar = a; if (b > mvar
+// .OR. isnan(mvar)) mvar = b): a NaN argument never wins.  Written out with an
+// explicit NaN test so that the result does not depend on how min/max
+// instructions are selected for NaN operands.
+__host__ __device__ __forceinline__ double max_ref(double a, double b) { return (b > a || a != a) ? b : a; }
+__host__ __device__ __forceinline__ double min_ref(double a, double b) { return (b < a || a != a) ? b : a; }
+
 __device__ __forceinline__ double stag_margin(double v0, double v1, double H0, double H1) {
   // calc_staggered_margin, ice_velocity_module.f90:1300-1319
   if (H0 > 0.0 && H1 == 0.0) return v0;

@@ -30,8 +30,8 @@ __global__ void k_surface_taf(Dims d, const double* Hi, const double* Hb, const 
   if (j >= d.ny || i >= d.nx) return;
   const long long q = d.at(j, i);
   const double h = Hi[q], b = Hb[q], s = SL[q];
-  Hs[q] = h + fmax(s - kRhoI / kRhoSW * h, b);              // surface_elevation :138-148
-  TAF[q] = h - fmax(0.0, (s - b) * (kRhoSW / kRhoI));       // thickness_above_floatation :149-159
+  Hs[q] = h + max_ref(s - kRhoI / kRhoSW * h, b);              // surface_elevation :138-148
+  TAF[q] = h - max_ref(0.0, (s - b) * (kRhoSW / kRhoI));       // thickness_above_floatation :149-159
   const int fl = is_floating(h, b, s) ? 1 : 0;
   cand[q] = fl;
   const bool edge = (i == 0 || i == d.nx - 1 || j == 0 || j == d.ny - 1);
@@ -249,13 +249,13 @@ __global__ void k_basal_hydro(Dims d, int choice, double hb_min, double hb_max, 
   if (choice == DIVA_HYDRO_DRY) p = 0.0;
   else if (choice == DIVA_HYDRO_SATURATED) p = -kRhoSW * kGrav * (SL[q] - Hb[q]);
   else {
-    const double lam = fmin(1.0, fmax(0.0, 1.0 - (Hb[q] - SL[q] - hb_min) / (hb_max - hb_min)));
+    const double lam = min_ref(1.0, max_ref(0.0, 1.0 - (Hb[q] - SL[q] - hb_min) / (hb_max - hb_min)));
     p = 0.96 * kRhoI * kGrav * Hi[q] * lam;
   }
   pwp[q] = p;
   const double o = kRhoI * kGrav * Hi[q];
   ob[q] = o;
-  Neff[q] = fmax(0.0, o - p);
+  Neff[q] = max_ref(0.0, o - p);
 }
 
 // calc_fraction_above_zero :521-711 with rotate_quad(_until_match) :712-783
@@ -265,8 +265,8 @@ __device__ __forceinline__ void rotate_quad(double& NW, double& NE, double& SW, 
 }
 __device__ __forceinline__ double nudge(double f, double t) {
   if (f == 0.0) return t;
-  if (f > 0.0) return fmax(t, f);
-  if (f < 0.0) return fmin(-t, f);
+  if (f > 0.0) return max_ref(t, f);
+  if (f < 0.0) return min_ref(-t, f);
   return f;
 }
 __device__ double fraction_above_zero(double fNW, double fNE, double fSW, double fSE) {
@@ -330,7 +330,7 @@ __device__ double fraction_above_zero(double fNW, double fNE, double fSW, double
       phi = CUDART_NAN;
     }
   }
-  return fmax(0.0, fmin(1.0, phi));
+  return max_ref(0.0, min_ref(1.0, phi));
 }
 
 // determine_grounded_fractions_CISM_quads :420-520 (TAF edge-extended by one cell)

@@ -112,7 +112,7 @@ __device__ __forceinline__ double sliding_beta(const CoefArgs& a, long long q, d
       return tc * pow(uabs, a.q_plastic - 1.0) / pow(a.u_thr, a.q_plastic);
     }
     case DIVA_SLIDING_TSAI2015:
-      return fmin(a.alpha_sq[q] * a.Neff[q], a.beta_sq[q] * pow(uabs, 1.0 / a.wm)) * pow(uabs, -1.0);
+      return min_ref(a.alpha_sq[q] * a.Neff[q], a.beta_sq[q] * pow(uabs, 1.0 / a.wm)) * pow(uabs, -1.0);
     case DIVA_SLIDING_SCHOOF2005: {
       const double a2 = a.alpha_sq[q], b2 = a.beta_sq[q], m = a.wm;
       return ((b2 * pow(uabs, 1.0 / m) * a2 * a.Neff[q]) / (pow(pow(b2, m) * uabs + pow(a2 * a.Neff[q], m), 1.0 / m))) *
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(256) k_column_coefficients(CoefArgs a) {
       }
       const double eps_sq = eps_h + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
       const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
-      eta = fmax(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
+      eta = max_ref(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
     }
     a.visc[off + q] = eta;
     if (k > 0) vint = vint + 0.5 * (eta + vprev) * (a.zt.z[k] - a.zt.z[k - 1]);
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(256) k_column_coefficients(CoefArgs a) {
   }
   if (!skip_visc) {
     a.visc_int[q] = vint;
-    a.Na[q] = a.bc_margin ? vint * H : vint * fmax(0.1, H);
+    a.Na[q] = a.bc_margin ? vint * H : vint * max_ref(0.1, H);
   }
   // sliding (calc_sliding_term_beta :924-951)
   double ua, va;
@@ -201,12 +201,12 @@ __global__ void __launch_bounds__(256) k_column_coefficients(CoefArgs a) {
   if (j == 0) va = a.v[d.at(0, i)];
   else if (j == ny - 1) va = a.v[d.at(ny - 2, i)];
   else va = (a.v[d.at(j - 1, i)] + a.v[q]) / 2.0;
-  double beta = fmin(sliding_beta(a, q, ua, va), a.beta_max);
+  double beta = min_ref(sliding_beta(a, q, ua, va), a.beta_max);
   if (!a.gl_subgrid && a.mask_ocean[q] == 1) beta = 0.0;
   a.beta[q] = beta;
   if (a.diva) {
     double F2;
-    if (ice) F2 = fmax(a.Fmin, fint);
+    if (ice) F2 = max_ref(a.Fmin, fint);
     else F2 = a.bc_margin ? 0.0 : a.Fmin;
     a.F2[q] = F2;
     double be;
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(256) k_face_coefficients(FaceArgs a) {
       prev = vb;
     }
     a.visc_int_b[q] = s;
-    const double nb = a.bc_margin ? s * a.Hb_i[q] : s * fmax(0.1, a.Hb_i[q]);
+    const double nb = a.bc_margin ? s * a.Hb_i[q] : s * max_ref(0.1, a.Hb_i[q]);
     a.Nb[q] = nb;
     a.lvNb[q] = a.crossterms ? nb : 1.0;
   }
@@ -644,7 +644,7 @@ __global__ void __launch_bounds__(256) k_secondary(SecArgs a) {
     // x and y index pairs of the divergence stencil (:603-622)
     const int ia = (i == 0) ? 1 : (i == nx - 1 ? nx - 2 : i), ib = ia - 1;
     const int ja = (j == 0) ? 1 : (j == ny - 1 ? ny - 2 : j), jb = ja - 1;
-    const double H = a.Hi[q], Hm = fmax(0.1, H);
+    const double H = a.Hi[q], Hm = max_ref(0.1, H);
     const double gsx = a.dHs_dx[q], gsy = a.dHs_dy[q], gix = a.dHi_dx[q], giy = a.dHi_dy[q];
     double du_kp1 = (a.u3[ob + d.at(j, ia)] - a.u3[ob + d.at(j, ib)]) / dx;
     double dv_kp1 = (a.v3[ob + d.at(ja, i)] - a.v3[ob + d.at(jb, i)]) / dx;
@@ -681,7 +681,7 @@ __global__ void __launch_bounds__(256) k_secondary(SecArgs a) {
   double R;
   if (a.dyn == DIVA_DYN_SIA) R = 1.0;
   else if (a.dyn == DIVA_DYN_SSA) R = 0.0;
-  else R = (a.ice[q] == 1) ? fmax(0.0, fmin(1.0, (1.0 - ab / as))) : 0.0;
+  else R = (a.ice[q] == 1) ? max_ref(0.0, min_ref(1.0, (1.0 - ab / as))) : 0.0;
   a.Rs[q] = R;
 }
 
@@ -709,11 +709,11 @@ __global__ void k_sia(Dims d, Zeta zt, double n, const int* sheet, const double*
     const double D0 = pow(kRhoI * kGrav * H, n) * pow((sx * sx + sy * sy), (n - 1.0) / 2.0);
     // D(zeta) = 2 H int_base^zeta A zeta^n (vertical_integration_from_bottom_to_zeta)
     double acc = 0.0, fk1 = A[(long long)(nz - 1) * P + q] * zt.zn[nz - 1];
-    out[(long long)(nz - 1) * P + q] = fmax(D0 * (2.0 * H * 0.0), -1E5) * slope;
+    out[(long long)(nz - 1) * P + q] = max_ref(D0 * (2.0 * H * 0.0), -1E5) * slope;
     for (int k = nz - 2; k >= 0; --k) {
       const double fk = A[(long long)k * P + q] * zt.zn[k];
       acc = acc - 0.5 * (fk1 + fk) * (zt.z[k + 1] - zt.z[k]);
-      out[(long long)k * P + q] = fmax(D0 * (2.0 * H * acc), -1E5) * slope;
+      out[(long long)k * P + q] = max_ref(D0 * (2.0 * H * acc), -1E5) * slope;
       fk1 = fk;
     }
   }

@@ -55,7 +55,9 @@ def test_reference_shaped_functions(cuda):
     g, cfg, f = small()
     ice = dict(f)
     diva.update_general_ice_model_data(g, ice, cfg, cuda)
-    assert "mask_sheet_a" in ice and ice["mask_sheet_a"].sum() > 0
+    diva.calc_ice_rheology(g, ice, cfg, cuda)
+    diva.update_general_ice_model_data(g, ice, cfg, cuda)
+    assert "mask_sheet_a" in ice and ice["mask_sheet_a"].sum() > 0 and ice["A_flow_3D_a"].min() > 0
     rep = diva.solve_DIVA(g, ice, cfg, cuda)
     assert rep["picard_iterations"] >= 1
     assert ice["u_vav_cx"].shape == (g.ny, g.nx - 1) and ice["u_3D_cx"].shape == (g.nz, g.ny, g.nx - 1)

@@ -149,6 +149,7 @@ def test_full_size_icecap_against_the_oracle(cuda, oracle):
     octx = diva.Context(g, cfg, oracle)
     helpers.prepare(octx, f)
     octx.calc_sia_3d_velocities()
+    oracle.lib.orc_prepare_diva(octx.h)      # driving stress, basal conditions, grounded fractions
     ref = octx.download()
     for m in MASKS[:10]:
         assert np.array_equal(gpu[m], ref[m]), m
