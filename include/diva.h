@@ -213,6 +213,31 @@ int  diva_state_restore(diva_ctx_t* ctx);
 int  diva_profile_kernel(diva_ctx_t* ctx, int32_t which, int32_t reps, double* ms_per_launch,
                          double* bytes_per_launch);
 
+/* Allocation-free step norm of one viscosity iteration.
+ * No counterpart in the reference: it exists for callers that cannot let a
+ * library allocate GPU memory -- a host model that budgets all device memory
+ * through its own pool, or code that must not trigger cudaMalloc while other
+ * work shares the device.  It computes resid_UV exactly as the reference's
+ * calc_visc_iter_UV_resid does (2 ||u - u_prev|| / max(||u + u_prev||, 1e-8)
+ * over cx and cy points with |u| above 1e-6 m/yr, 0 if there are none) from
+ * device arrays the caller owns, and writes it to resid_uv (one double in
+ * device memory).  Layout: u arrays (j,i) at i*ld_cx + j for i < nx-1,
+ * j < ny (ld_cx >= ny); v arrays (j,i) at i*ld_cy + j for j < ny-1 (ld_cy >=
+ * ny-1); Fortran arrays u_vav_cx(ny,nx-1) and v_vav_cy(ny-1,nx) copied to the
+ * device as they are fit with ld_cx = ny, ld_cy = ny-1.  Runs on `stream`
+ * (cudaStream_t; NULL = legacy default stream) and does not synchronise.
+ * It allocates nothing: its scratch is a static 384 KiB device array that
+ * every GPU loading the library holds until exit, enough for grids of at most
+ * 16384 thread blocks of 32 x 8 columns, i.e. ceil(ny/32) * ceil(nx/8) <=
+ * 16384 (2048 x 2048 fits); larger grids return DIVA_BAD_INPUT.  The first
+ * call on a device looks up the scratch array's device address (with that
+ * device current) and caches it, so make the first call before any stream
+ * capture.  All calls share the scratch array: calls that overlap on the GPU
+ * race, so serialise them. */
+int  diva_visc_iter_uv_resid_noalloc(int32_t nx, int32_t ny, const double* u_cx, const double* u_cx_prev,
+                                     int32_t ld_cx, const double* v_cy, const double* v_cy_prev, int32_t ld_cy,
+                                     double* resid_uv, void* stream);
+
 /* Number of kernels this context has launched since diva_create. */
 int64_t diva_kernel_launches(const diva_ctx_t* ctx);
 
