@@ -227,7 +227,8 @@ def run_b200(args):
     for _ in range(args.warmup):
         step()
     clocks = ClockSampler(local)
-    clocks.start()
+    if not args.quick:            # no NVML polling while a profiler owns the counters
+        clocks.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -239,13 +240,13 @@ def run_b200(args):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clk = clocks.stop()
+    clk = clocks.stop() if not args.quick else {}
     launches = ctx.kernel_launches() - l0
     ms = e0.elapsed_time(e1)
     if args.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": world * args.steps / (ms / 1000.0), "unit": UNIT,
-                              "quick": True, "gpu_launches": int(launches)}))
+                              "quick": True, "gpu_launches": int(launches), "reports": reps}))
         ctx.close()
         if world > 1:
             dist.destroy_process_group()

@@ -83,7 +83,10 @@ class Report(C.Structure):
                 ("reserved", C.c_int32 * 8)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d["linear_not_converged"] = self.reserved[0]   # linear solves that missed their tolerance
+        d["graph_launched"] = self.reserved[1]         # 1 if the iterations ran as CUDA graphs
+        return d
 
 
 class FieldInfo(C.Structure):

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include "ctx.hpp"
@@ -222,8 +223,65 @@ int fill_const(Ctx* c, double* p, double v) {
   return DIVA_OK;
 }
 
+// The viscosity iteration as one graph launch per iteration (see solver.cu):
+// the Krylov loop and the skip of a converged iteration run on the device;
+// the host reads one status block per iteration and mirrors the viscosity
+// buffer swap the graph performed.
+int picard_graph(Ctx* c, bool diva, diva_report_t* rep) {
+  const diva_config_t& C = c->c;
+  const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
+  PicardGraphs& G = c->graphs[diva ? 1 : 0];
+  double init[SC_COUNT - SC_TARGET2] = {};
+  init[SC_RELRES - SC_TARGET2] = -1.0;
+  DIVA_CUDA(c, cudaMemcpyAsync(c->scal + SC_TARGET2, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  int it = 0;
+  double resid = 0.0, relres = -1.0;
+  bool by_relres = false;
+  for (;;) {
+    int parity;
+    if (c->f[DIVA_F_VISC_EFF_3D_A] == G.visc_buf[0]) parity = 0;
+    else if (c->f[DIVA_F_VISC_EFF_3D_A] == G.visc_buf[1]) parity = 1;
+    else return set_error(c, DIVA_CUDA_ERROR, "viscosity buffers out of step with the captured graphs");
+    DIVA_CUDA(c, cudaGraphLaunch(G.exec[parity], c->stream));
+    std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
+    DIVA_CUDA(c, cudaMemcpyAsync(c->h_scal + SC_TARGET2, c->scal + SC_TARGET2,
+                                 sizeof(double) * (SC_COUNT - SC_TARGET2), cudaMemcpyDeviceToHost, c->stream));
+    DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+    const double* h = c->h_scal;
+    it = (int)h[SC_PIC_IT];
+    const bool solved = h[SC_SOLVED] != 0.0;
+    const long lin = (long)h[SC_LIN_IT], full = (long)h[SC_LIN_FULL];
+    c->lin_iters += lin;
+    c->mg_cycles += lin + full;
+    c->launches += G.n_pre + G.n_post + (solved ? G.n_head + G.n_tail + lin * G.n_first + full * G.n_second : 0);
+    c->fine_passes += G.p_pre + (solved ? G.p_head + G.p_tail + lin * G.p_first + full * G.p_second : 0.0);
+    relres = h[SC_RELRES];
+    if (h[SC_NAN] != 0.0) return set_error(c, DIVA_NAN_DETECTED, "NaN in the viscosity iteration");
+    if (h[SC_EXIT_RELRES] != 0.0) { by_relres = true; break; }
+    resid = h[SC_RESID];
+    if (h[SC_CONVERGED] != 0.0) break;
+    if (it > C.DIVA_visc_it_nit + 1) return set_error(c, DIVA_TIMEOUT, "viscosity iteration did not stop");
+  }
+  int status = DIVA_OK;
+  if (!by_relres && it >= C.DIVA_visc_it_nit && (relmode || resid >= C.DIVA_visc_it_norm_dUV_tol))
+    status = DIVA_MAX_PICARD;
+  if (rep) {
+    rep->picard_iterations = it;
+    rep->resid_UV = resid;
+    rep->relres = relres;
+    rep->status = status;
+    rep->reserved[0] = (int32_t)c->h_scal[SC_LIN_FAILED];
+    rep->reserved[1] = 1;   // graph-launched
+  }
+  return status;
+}
+
 // the viscosity iteration shared by solve_SSA (:180-240) and solve_DIVA (:307-363)
 int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
+  if (!c->graphs_disabled && c->c.choice_ice_margin != DIVA_MARGIN_BC) {
+    if (solver_build_picard_graphs(c, diva) == DIVA_OK) return picard_graph(c, diva, rep);
+    c->graphs_disabled = true;   // conditional graph nodes unavailable: host-driven loop below
+  }
   const diva_config_t& C = c->c;
   const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
   int it = 0, st = DIVA_OK, lin_fail = 0;
@@ -272,6 +330,7 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
     rep->relres = relres;
     rep->status = status;
     rep->reserved[0] = lin_fail;
+    rep->reserved[1] = 0;   // host-driven
   }
   return status;
 }
@@ -341,6 +400,9 @@ int diva_create(diva_ctx_t** out, const diva_grid_t* g, const diva_config_t* cfg
   }
   apply_config(c, cfg);
   plan_levels(c);
+  // DIVA_NO_GRAPHS=1 launches the same kernels one by one instead of from
+  // CUDA graphs (kernel-level profilers list them individually that way)
+  if (const char* e = getenv("DIVA_NO_GRAPHS")) c->graphs_disabled = (e[0] == '1');
   Carver dry{nullptr, 0, true};
   const size_t bytes = carve(c, dry);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return DIVA_CUDA_ERROR; }
@@ -368,6 +430,7 @@ int diva_destroy(diva_ctx_t* h) {
   if (!h) return DIVA_OK;
   Ctx* c = &h->c;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  solver_destroy_graphs(c);
   for (int f = 0; f < DIVA_NUM_FIELDS; ++f)
     if (c->saved[f]) cudaFree(c->saved[f]);
   if (c->arena) cudaFree(c->arena);
@@ -384,6 +447,7 @@ int diva_set_config(diva_ctx_t* h, const diva_config_t* cfg) {
   int st = validate_config(&h->c, cfg);
   if (st) return st;
   apply_config(&h->c, cfg);
+  solver_destroy_graphs(&h->c);   // captured kernel arguments carry the configuration
   return DIVA_OK;
 }
 

@@ -30,7 +30,21 @@ enum { KV_X = 0, KV_R, KV_RHAT, KV_P, KV_PHAT, KV_V, KV_S, KV_SHAT, KV_T, KV_B, 
 // Device scalars of the linear solver and of the Picard bookkeeping.
 enum {
   SC_RHO = 0, SC_ALPHA, SC_OMEGA, SC_BETA, SC_RNORM2, SC_BNORM2, SC_SNORM2, SC_TMP0, SC_TMP1, SC_TMP2,
-  SC_RES1, SC_RES2, SC_NCNT, SC_RR, SC_BB, SC_NANFLAG, SC_FLAG, SC_COUNT = 32
+  SC_RES1, SC_RES2, SC_NCNT, SC_RR, SC_BB, SC_NANFLAG, SC_FLAG,
+  // device-side control of a graph-launched viscosity iteration
+  SC_TARGET2, SC_LIN_IT, SC_LIN_FULL, SC_LIN_FAILED, SC_PIC_IT, SC_EXIT_RELRES, SC_CONVERGED, SC_RESID,
+  SC_RELRES, SC_NAN, SC_SOLVED, SC_HALFDONE,
+  SC_COUNT = 40
+};
+
+// One instantiated graph per parity of the viscosity double buffer; the launch
+// and pass counts of each captured region turn executed iterations into totals.
+struct PicardGraphs {
+  bool valid = false;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  void* visc_buf[2] = {nullptr, nullptr};   // buffer holding the current viscosity when exec[p] starts
+  long long n_pre = 0, n_head = 0, n_first = 0, n_second = 0, n_tail = 0, n_post = 0;
+  double p_pre = 0, p_head = 0, p_first = 0, p_second = 0, p_tail = 0;
 };
 
 struct Ctx {
@@ -62,6 +76,8 @@ struct Ctx {
   Level lv[kMaxLevels];
   int nlev = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  PicardGraphs graphs[2];               // [0] solve_SSA, [1] solve_DIVA
+  bool graphs_disabled = false;         // set if graph construction failed: host-driven loop
   // counters of the last solve
   long lin_iters = 0, mg_cycles = 0;
   long long launches = 0;            // kernels launched since create
@@ -108,6 +124,9 @@ int launch_secondary_velocities(Ctx* c);
 int launch_sia(Ctx* c);
 int launch_ssa_beta_eff(Ctx* c);
 int launch_zero_velocities(Ctx* c, double* u, double* v);
+int launch_ctl_end(Ctx* c, bool relmode);
+int launch_err_commit_pred(Ctx* c);
+int launch_basal_pred(Ctx* c);
 int launch_any_sheet(Ctx* c, int* result);
 
 // solver.cu
@@ -117,5 +136,7 @@ int solver_relres(Ctx* c, const double* u, const double* v, double* relres);
 int solver_fill_boundary(Ctx* c, double* u, double* v);
 int solver_smooth_fine(Ctx* c, int sweeps);
 int solver_matvec_fine(Ctx* c, int reps);
+int solver_build_picard_graphs(Ctx* c, bool diva);
+void solver_destroy_graphs(Ctx* c);
 
 }  // namespace diva

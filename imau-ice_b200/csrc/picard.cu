@@ -429,9 +429,10 @@ __global__ void k_sum_partials(const double* partials, int nblocks, int width, d
 __global__ void k_basal_stress_velocities(Dims d, int sliding_none, int basal_freezing, double dT, const double* u,
                                           const double* v, const double* bex, const double* bey, const double* F2,
                                           const double* Hi, const double* Ti, const double* Tpmp, double* tbx,
-                                          double* tby, double* ubx, double* vby) {
+                                          double* tby, double* ubx, double* vby, const double* pred) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
   if (j >= d.ny || i >= d.nx) return;
+  if (pred && *pred == 0.0) return;   // graph launch: only when the iteration stopped on the nonlinear residual
   const long long q = d.at(j, i);
   bool frozen = false;
   if (basal_freezing) {
@@ -855,8 +856,56 @@ int launch_basal_stress_velocities(Ctx* c) {
                                     c->D(DIVA_F_BETA_EFF_CX), c->D(DIVA_F_BETA_EFF_CY), c->D(DIVA_F_F2_A),
                                     c->D(DIVA_F_HI_A), c->D(DIVA_F_TI_A), c->D(DIVA_F_TI_PMP_A),
                                     c->D(DIVA_F_TAUB_CX), c->D(DIVA_F_TAUB_CY), c->D(DIVA_F_U_BASE_CX),
-                                    c->D(DIVA_F_V_BASE_CY)); c->launches++;
+                                    c->D(DIVA_F_V_BASE_CY), nullptr); c->launches++;
   DIVA_LAUNCHED(c, "k_basal_stress_velocities");
+  return DIVA_OK;
+}
+
+int launch_basal_pred(Ctx* c) {
+  const diva_config_t& C = c->c;
+  k_basal_stress_velocities<<<G2>>>(c->d, C.choice_sliding_law == DIVA_SLIDING_NONE, C.include_basal_freezing,
+                                    C.deltaT_basal_freezing, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY),
+                                    c->D(DIVA_F_BETA_EFF_CX), c->D(DIVA_F_BETA_EFF_CY), c->D(DIVA_F_F2_A),
+                                    c->D(DIVA_F_HI_A), c->D(DIVA_F_TI_A), c->D(DIVA_F_TI_PMP_A),
+                                    c->D(DIVA_F_TAUB_CX), c->D(DIVA_F_TAUB_CY), c->D(DIVA_F_U_BASE_CX),
+                                    c->D(DIVA_F_V_BASE_CY), c->scal + SC_EXIT_RELRES); c->launches++;
+  DIVA_LAUNCHED(c, "k_basal_stress_velocities");
+  return DIVA_OK;
+}
+
+// end of a graph-launched viscosity iteration: the step norm from the summed
+// partials (calc_visc_iter_UV_resid :1588-1596) and the stop test (:346-351)
+__global__ void k_ctl_end(double* sc, int relmode, double tol, int nit) {
+  const double r1 = sc[SC_RES1], r2 = sc[SC_RES2], cnt = sc[SC_RES1 + 2];
+  if (!isfinite(r1) || !isfinite(r2)) sc[SC_NAN] = 1.0;
+  const double resid = (cnt > 0.0) ? 2.0 * sqrt(r1) / max_ref(sqrt(r2), 1E-8) : 0.0;
+  sc[SC_RESID] = resid;
+  bool conv = false;
+  if (!relmode && resid < tol) conv = true;
+  else if (sc[SC_PIC_IT] >= (double)nit) conv = true;
+  sc[SC_CONVERGED] = conv ? 1.0 : 0.0;
+}
+
+// DIVA_err of this iteration becomes the field unless the iteration converged (:353-355)
+__global__ void k_err_commit(Dims d, const double* sc, const double* cx, const double* cy, double* fx, double* fy) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= d.ny || i >= d.nx) return;
+  if (sc[SC_CONVERGED] != 0.0) return;
+  const long long q = d.at(j, i);
+  fx[q] = cx[q];
+  fy[q] = cy[q];
+}
+
+int launch_ctl_end(Ctx* c, bool relmode) {
+  k_ctl_end<<<1, 1, 0, c->stream>>>(c->scal, relmode, c->c.DIVA_visc_it_norm_dUV_tol, c->c.DIVA_visc_it_nit); c->launches++;
+  DIVA_LAUNCHED(c, "k_ctl_end");
+  return DIVA_OK;
+}
+
+int launch_err_commit_pred(Ctx* c) {
+  k_err_commit<<<G2>>>(c->d, c->scal, c->err_cand[0], c->err_cand[1], c->D(DIVA_F_DIVA_ERR_CX),
+                       c->D(DIVA_F_DIVA_ERR_CY)); c->launches++;
+  DIVA_LAUNCHED(c, "k_err_commit");
   return DIVA_OK;
 }
 

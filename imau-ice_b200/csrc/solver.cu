@@ -172,6 +172,17 @@ __global__ void k_rhs(Dims d, int crossterms, const double* tdx, const double* t
   bv[q] = v_int(d, j, i) ? (crossterms ? -tdy[q] * dx2 : -tdy[q] * dx2 / Ncy[q]) : 0.0;
 }
 
+// Gauss-Seidel update of one point of one component (comp 0 = u, 1 = v)
+__device__ __forceinline__ void gs_point(const Op& o, double* xu, double* xv, const double* bu, const double* bv,
+                                         const double* idu, const double* idv, int comp, int j, int i) {
+  const long long q = o.d.at(j, i);
+  if (comp == 0) {
+    if (u_int(o.d, j, i)) xu[q] += (bu[q] - Au(o, xu, xv, j, i)) * idu[q];
+  } else {
+    if (v_int(o.d, j, i)) xv[q] += (bv[q] - Av(o, xu, xv, j, i)) * idv[q];
+  }
+}
+
 // one colour of Gauss-Seidel: comp 0 = u, 1 = v; colour = (i+j) parity
 __global__ void k_gs(Op o, double* xu, double* xv, const double* bu, const double* bv, const double* idu,
                      const double* idv, int comp, int color) {
@@ -179,49 +190,51 @@ __global__ void k_gs(Op o, double* xu, double* xv, const double* bu, const doubl
   const int i = blockIdx.y * blockDim.y + threadIdx.y;
   const int j = 2 * jj + ((i + color) & 1);
   if (j >= o.d.ny || i >= o.d.nx) return;
-  const long long q = o.d.at(j, i);
-  if (comp == 0) {
-    if (!u_int(o.d, j, i)) return;
-    xu[q] += (bu[q] - Au(o, xu, xv, j, i)) * idu[q];
-  } else {
-    if (!v_int(o.d, j, i)) return;
-    xv[q] += (bv[q] - Av(o, xu, xv, j, i)) * idv[q];
+  gs_point(o, xu, xv, bu, bv, idu, idv, comp, j, i);
+}
+
+// block-wide pass over all points of one colour (the caller synchronises)
+__device__ __forceinline__ void block_gs_pass(const Op& o, double* xu, double* xv, const double* bu, const double* bv,
+                                              const double* idu, const double* idv, int comp, int color) {
+  const Dims& d = o.d;
+  const int n = d.nx * d.ny;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int j = t % d.ny, i = t / d.ny;
+    if (((i + j) & 1) != color) continue;
+    gs_point(o, xu, xv, bu, bv, idu, idv, comp, j, i);
   }
 }
 
-// relaxation of the coarsest level by one block (bounded number of sweeps)
-__global__ void k_coarse_solve(Op o, double* xu, double* xv, const double* bu, const double* bv, const double* idu,
-                               const double* idv, int sweeps) {
-  const Dims& d = o.d;
-  const int n = d.nx * d.ny;
+// relaxation of the coarsest level by one block: `sweeps` symmetric sweeps u0 u1 v0 v1 | v1 v0 u1 u0
+__device__ __forceinline__ void block_coarse_relax(const Op& o, double* xu, double* xv, const double* bu,
+                                                   const double* bv, const double* idu, const double* idv,
+                                                   int sweeps) {
   for (int s = 0; s < sweeps; ++s) {
     for (int pass = 0; pass < 8; ++pass) {
-      // symmetric order: u0 u1 v0 v1 | v1 v0 u1 u0
       const int p = pass < 4 ? pass : 7 - pass;
-      const int comp = p >> 1, color = p & 1;
-      for (int t = threadIdx.x; t < n; t += blockDim.x) {
-        const int j = t % d.ny, i = t / d.ny;
-        if (((i + j) & 1) != color) continue;
-        const long long q = d.at(j, i);
-        if (comp == 0) {
-          if (u_int(d, j, i)) xu[q] += (bu[q] - Au(o, xu, xv, j, i)) * idu[q];
-        } else {
-          if (v_int(d, j, i)) xv[q] += (bv[q] - Av(o, xu, xv, j, i)) * idv[q];
-        }
-      }
+      block_gs_pass(o, xu, xv, bu, bv, idu, idv, p >> 1, p & 1);
       __syncthreads();
     }
   }
 }
 
+__global__ void k_coarse_solve(Op o, double* xu, double* xv, const double* bu, const double* bv, const double* idu,
+                               const double* idv, int sweeps) {
+  block_coarse_relax(o, xu, xv, bu, bv, idu, idv, sweeps);
+}
+
 // r = b - A x on the interior (zero elsewhere)
+__device__ __forceinline__ void residual_point(const Op& o, const double* xu, const double* xv, const double* bu,
+                                               const double* bv, double* ru, double* rv, int j, int i) {
+  const long long q = o.d.at(j, i);
+  ru[q] = u_int(o.d, j, i) ? bu[q] - Au(o, xu, xv, j, i) : 0.0;
+  rv[q] = v_int(o.d, j, i) ? bv[q] - Av(o, xu, xv, j, i) : 0.0;
+}
 __global__ void k_residual(Op o, const double* xu, const double* xv, const double* bu, const double* bv, double* ru,
                            double* rv) {
   IDX2D
   if (j >= o.d.ny || i >= o.d.nx) return;
-  const long long q = o.d.at(j, i);
-  ru[q] = u_int(o.d, j, i) ? bu[q] - Au(o, xu, xv, j, i) : 0.0;
-  rv[q] = v_int(o.d, j, i) ? bv[q] - Av(o, xu, xv, j, i) : 0.0;
+  residual_point(o, xu, xv, bu, bv, ru, rv, j, i);
 }
 
 // 1D transfer weights.  "cell" direction: u along x, v along y; "node": u along y, v along x.
@@ -253,10 +266,9 @@ __device__ __forceinline__ int scatter_node(int f, int f2, int* C, double* w) {
 }
 
 // b_c = P^T r_f on coarse interior points; x_c = 0
-__global__ void k_restrict(Dims df, Dims dc, int fx, int fy, const double* ru, const double* rv, double* bu,
-                           double* bv, double* xu, double* xv) {
-  IDX2D
-  if (j >= dc.ny || i >= dc.nx) return;
+__device__ __forceinline__ void restrict_point(const Dims& df, const Dims& dc, int fx, int fy, const double* ru,
+                                               const double* rv, double* bu, double* bv, double* xu, double* xv,
+                                               int j, int i) {
   const long long q = dc.at(j, i);
   int fi[4], fj[4];
   double wi[4], wj[4];
@@ -279,12 +291,16 @@ __global__ void k_restrict(Dims df, Dims dc, int fx, int fy, const double* ru, c
   xu[q] = 0.0;
   xv[q] = 0.0;
 }
+__global__ void k_restrict(Dims df, Dims dc, int fx, int fy, const double* ru, const double* rv, double* bu,
+                           double* bv, double* xu, double* xv) {
+  IDX2D
+  if (j >= dc.ny || i >= dc.nx) return;
+  restrict_point(df, dc, fx, fy, ru, rv, bu, bv, xu, xv, j, i);
+}
 
 // x_f += P x_c on fine interior points (coarse values read through the coarse boundary mapping)
-__global__ void k_prolong(Op oc, Dims df, int fx, int fy, const double* xcu, const double* xcv, double* xu,
-                          double* xv) {
-  IDX2D
-  if (j >= df.ny || i >= df.nx) return;
+__device__ __forceinline__ void prolong_point(const Op& oc, const Dims& df, int fx, int fy, const double* xcu,
+                                              const double* xcv, double* xu, double* xv, int j, int i) {
   const long long q = df.at(j, i);
   int Ci[2], Cj[2];
   double wi[2], wj[2];
@@ -308,6 +324,76 @@ __global__ void k_prolong(Op oc, Dims df, int fx, int fy, const double* xcu, con
         s += wj[a] * wi[b] * LV(oc, xcv, J, I);
       }
     xv[q] += s;
+  }
+}
+__global__ void k_prolong(Op oc, Dims df, int fx, int fy, const double* xcu, const double* xcv, double* xu,
+                          double* xv) {
+  IDX2D
+  if (j >= df.ny || i >= df.nx) return;
+  prolong_point(oc, df, fx, fy, xcu, xcv, xu, xv, j, i);
+}
+
+// The levels from `first` down, run by one thread block with barriers between
+// the phases: the same per-point operations in the same order as the per-level
+// kernels of vcycle(), without a launch per phase.
+struct SubLevel {
+  Op o;
+  double *xu, *xv, *bu, *bv, *ru, *rv;
+  const double *idu, *idv;
+  int fx, fy;   // coarsening factors to the next level
+};
+struct SubCycle {
+  int first, last, nu1, nu2, coarse_sweeps;
+  SubLevel L[kMaxLevels];
+};
+
+template <class F>
+__device__ __forceinline__ void block_for_points(const Dims& d, F f) {
+  const int n = d.nx * d.ny;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) f(t % d.ny, t / d.ny);
+}
+
+__global__ void __launch_bounds__(512) k_subcycle(SubCycle sc, double* xu0, double* xv0, const double* bu0,
+                                                  const double* bv0) {
+  // descend
+  for (int l = sc.first; l <= sc.last; ++l) {
+    const SubLevel& L = sc.L[l];
+    double* xu = l == sc.first ? xu0 : L.xu;
+    double* xv = l == sc.first ? xv0 : L.xv;
+    const double* bu = l == sc.first ? bu0 : L.bu;
+    const double* bv = l == sc.first ? bv0 : L.bv;
+    if (l == sc.last) {
+      block_coarse_relax(L.o, xu, xv, bu, bv, L.idu, L.idv, sc.coarse_sweeps);
+      break;
+    }
+    for (int s = 0; s < sc.nu1; ++s)
+      for (int p = 0; p < 4; ++p) {
+        block_gs_pass(L.o, xu, xv, bu, bv, L.idu, L.idv, p >> 1, p & 1);
+        __syncthreads();
+      }
+    block_for_points(L.o.d, [&](int j, int i) { residual_point(L.o, xu, xv, bu, bv, L.ru, L.rv, j, i); });
+    __syncthreads();
+    const SubLevel& K = sc.L[l + 1];
+    block_for_points(K.o.d, [&](int j, int i) {
+      restrict_point(L.o.d, K.o.d, L.fx, L.fy, L.ru, L.rv, K.bu, K.bv, K.xu, K.xv, j, i);
+    });
+    __syncthreads();
+  }
+  // ascend
+  for (int l = sc.last - 1; l >= sc.first; --l) {
+    const SubLevel& L = sc.L[l];
+    const SubLevel& K = sc.L[l + 1];
+    double* xu = l == sc.first ? xu0 : L.xu;
+    double* xv = l == sc.first ? xv0 : L.xv;
+    const double* bu = l == sc.first ? bu0 : L.bu;
+    const double* bv = l == sc.first ? bv0 : L.bv;
+    block_for_points(L.o.d, [&](int j, int i) { prolong_point(K.o, L.o.d, L.fx, L.fy, K.xu, K.xv, xu, xv, j, i); });
+    __syncthreads();
+    for (int s = 0; s < sc.nu2; ++s)
+      for (int p = 3; p >= 0; --p) {
+        block_gs_pass(L.o, xu, xv, bu, bv, L.idu, L.idv, p >> 1, p & 1);
+        __syncthreads();
+      }
   }
 }
 
@@ -565,6 +651,124 @@ __global__ void k_relres(Op o, const double* u, const double* v, const double* b
   store_partials(acc, partials, nbx);
 }
 
+// ---- device-side control of a graph-launched viscosity iteration ------------------
+// Single-thread kernels that finish a reduction and set the conditional-node
+// handles, so the Krylov loop and the skip of a converged iteration are
+// decided on the device without a host round trip.
+__device__ __forceinline__ void sum_partials4(const double* partials, int nblocks, double (&out)[kPW]) {
+  __shared__ double sh[kPW][256];
+  double s[kPW] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int q = 0; q < kPW; ++q) s[q] += partials[kPW * b + q];
+  for (int q = 0; q < kPW; ++q) sh[q][threadIdx.x] = s[q];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int q = 0; q < kPW; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + o];
+    __syncthreads();
+  }
+  for (int q = 0; q < kPW; ++q) out[q] = sh[q][0];
+}
+
+__global__ void k_ctl_begin(double* sc) {
+  sc[SC_PIC_IT] += 1.0;
+  sc[SC_EXIT_RELRES] = 0.0;
+  sc[SC_LIN_IT] = 0.0;
+  sc[SC_LIN_FULL] = 0.0;
+  sc[SC_SOLVED] = 0.0;
+  sc[SC_CONVERGED] = 0.0;
+}
+
+// nonlinear residual of the current iterate; skip the solve when it meets the tolerance
+__global__ void k_ctl_relres(const double* partials, int nblocks, double* sc, cudaGraphConditionalHandle h_solve,
+                             double tol) {
+  double v[kPW];
+  sum_partials4(partials, nblocks, v);
+  if (threadIdx.x != 0) return;
+  const double rr = v[0], bb = v[1];
+  const double relres = bb > 0.0 ? sqrt(rr / bb) : sqrt(rr);
+  sc[SC_RELRES] = relres;
+  bool stop = false;
+  if (!isfinite(relres)) { sc[SC_NAN] = 1.0; stop = true; }
+  else if (relres <= tol) { sc[SC_EXIT_RELRES] = 1.0; stop = true; }
+  cudaGraphSetConditional(h_solve, stop ? 0u : 1u);
+}
+
+// initial Krylov residual and the target of this linear solve
+__global__ void k_ctl_lin_init(const double* partials, int nblocks, double* sc, cudaGraphConditionalHandle h_while,
+                               int adaptive, double lin_rtol, int maxit) {
+  double v[kPW];
+  sum_partials4(partials, nblocks, v);
+  if (threadIdx.x != 0) return;
+  const double rr = v[0], bb = v[1];
+  sc[SC_RNORM2] = rr;
+  sc[SC_BNORM2] = bb;
+  sc[SC_RHO] = rr;
+  double rtol = lin_rtol;
+  if (adaptive) rtol = max_ref(lin_rtol, min_ref(0.1, 0.05 * sc[SC_RELRES]));
+  const double t = rtol * (bb > 0.0 ? sqrt(bb) : 1.0);
+  sc[SC_TARGET2] = t * t;
+  sc[SC_SOLVED] = 1.0;
+  if (!isfinite(rr)) sc[SC_NAN] = 1.0;
+  cudaGraphSetConditional(h_while, (isfinite(rr) && rr > t * t && maxit > 0) ? 1u : 0u);
+}
+
+// after s = r - alpha v: stop at the half step if |s| meets the target
+__global__ void k_ctl_half(const double* partials, int nblocks, double* sc, cudaGraphConditionalHandle h_while,
+                           cudaGraphConditionalHandle h_half) {
+  double v[kPW];
+  sum_partials4(partials, nblocks, v);
+  if (threadIdx.x != 0) return;
+  const double ss = v[0];
+  sc[SC_SNORM2] = ss;
+  sc[SC_LIN_IT] += 1.0;
+  if (!isfinite(ss)) {
+    sc[SC_NAN] = 1.0;
+    sc[SC_HALFDONE] = 0.0;
+    cudaGraphSetConditional(h_half, 0u);
+    cudaGraphSetConditional(h_while, 0u);
+  } else if (ss <= sc[SC_TARGET2]) {
+    sc[SC_HALFDONE] = 1.0;
+    sc[SC_RNORM2] = ss;
+    cudaGraphSetConditional(h_half, 0u);
+    cudaGraphSetConditional(h_while, 0u);
+  } else {
+    sc[SC_HALFDONE] = 0.0;
+    cudaGraphSetConditional(h_half, 1u);
+  }
+}
+
+__global__ void k_x_half_pred(Dims d, const double* sc, double* xu, double* xv, const double* phu, const double* phv) {
+  IDX2D
+  if (j >= d.ny || i >= d.nx) return;
+  if (sc[SC_HALFDONE] == 0.0) return;
+  const long long q = d.at(j, i);
+  const double alpha = sc[SC_ALPHA];
+  if (u_int(d, j, i)) xu[q] += alpha * phu[q];
+  if (v_int(d, j, i)) xv[q] += alpha * phv[q];
+}
+
+// after the full step: rho, beta and the continue test
+__global__ void k_ctl_full(const double* partials, int nblocks, double* sc, cudaGraphConditionalHandle h_while,
+                           int maxit) {
+  double v[kPW];
+  sum_partials4(partials, nblocks, v);
+  if (threadIdx.x != 0) return;
+  const double rho_new = v[0], rr = v[1];
+  const double om = sc[SC_OMEGA], al = sc[SC_ALPHA], rho = sc[SC_RHO];
+  sc[SC_BETA] = (rho != 0.0 && om != 0.0) ? (rho_new / rho) * (al / om) : 0.0;
+  sc[SC_RHO] = rho_new;
+  sc[SC_RNORM2] = rr;
+  sc[SC_LIN_FULL] += 1.0;
+  const bool fin = isfinite(rr);
+  if (!fin) sc[SC_NAN] = 1.0;
+  cudaGraphSetConditional(h_while, (fin && rr > sc[SC_TARGET2] && sc[SC_LIN_IT] < (double)maxit) ? 1u : 0u);
+}
+
+__global__ void k_ctl_lin_finish(double* sc) {
+  if (sc[SC_RNORM2] > sc[SC_TARGET2]) sc[SC_LIN_FAILED] += 1.0;
+}
+
 // ---- host side --------------------------------------------------------------------
 Op op_of(const Ctx* c, int l) {
   Op o;
@@ -635,8 +839,38 @@ static int gs_sweep(Ctx* c, int l, double* xu, double* xv, const double* bu, con
   return DIVA_OK;
 }
 
+// levels with at most this many points are handled by one k_subcycle block
+constexpr long long kSubMaxPoints = 4096;
+
+static int sub_first_level(const Ctx* c) {
+  for (int l = 0; l < c->nlev; ++l)
+    if ((long long)c->lv[l].d.nx * c->lv[l].d.ny <= kSubMaxPoints) return l;
+  return c->nlev - 1;
+}
+
 static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv) {
   const int nu1 = 2, nu2 = 2, coarse_sweeps = 64;
+  if (l == sub_first_level(c)) {
+    SubCycle sc;
+    sc.first = l;
+    sc.last = c->nlev - 1;
+    sc.nu1 = nu1;
+    sc.nu2 = nu2;
+    sc.coarse_sweeps = coarse_sweeps;
+    for (int q = l; q < c->nlev; ++q) {
+      const Level& L = c->lv[q];
+      SubLevel& S = sc.L[q];
+      S.o = make_op(c, q);
+      S.xu = L.xu; S.xv = L.xv; S.bu = L.bu; S.bv = L.bv; S.ru = L.ru; S.rv = L.rv;
+      S.idu = L.idu; S.idv = L.idv;
+      S.fx = 1; S.fy = 1;
+      if (q + 1 < c->nlev) factors(c, q, &S.fx, &S.fy);
+    }
+    k_subcycle<<<1, 512, 0, c->stream>>>(sc, xu, xv, bu, bv); c->launches++;
+    DIVA_LAUNCHED(c, "k_subcycle");
+    for (int q = l; q < c->nlev; ++q) c->fine_passes += 8.0 * (double)c->lv[q].d.plane / (double)c->d.plane;
+    return DIVA_OK;
+  }
   if (l == c->nlev - 1) {
     k_coarse_solve<<<1, 256, 0, c->stream>>>(make_op(c, l), xu, xv, bu, bv, c->lv[l].idu, c->lv[l].idv,
                                              coarse_sweeps); c->launches++;
@@ -785,6 +1019,236 @@ int solver_matvec_fine(Ctx* c, int reps) {
 int solver_fill_boundary(Ctx* c, double* u, double* v) {
   k_fill_boundary<<<grid2d(c->d.ny, c->d.nx), block2d(), 0, c->stream>>>(c->d, c->bc, u, v); c->launches++;
   DIVA_LAUNCHED(c, "k_fill_boundary");
+  return DIVA_OK;
+}
+
+// ---- one viscosity iteration as one CUDA graph ------------------------------------
+//
+//   pre   : k_ctl_begin, coefficients (K1 + faces), operator set-up of all levels,
+//           [relres stop rule] nonlinear residual -> k_ctl_relres sets IF(solve)
+//   IF(solve):
+//     head  : x <- (u,v), initial residual, k_ctl_lin_init sets WHILE(krylov)
+//     WHILE(krylov):
+//       first : V-cycle p -> phat, v = A phat, alpha, s, k_ctl_half sets IF(second)
+//               and may end the loop; x += alpha phat if it did
+//       IF(second): V-cycle s -> shat, t = A shat, omega, x and r, k_ctl_full
+//                   sets WHILE(krylov), p update
+//     tail  : boundary fill, Picard update (limits, relaxation, step norm, basal
+//             stress and velocity), stop test, DIVA_err commit
+//   post  : [DIVA] basal stress/velocity when the residual stopped the iteration
+//
+// Two instances are built, one per parity of the viscosity double buffer.
+namespace {
+
+struct CaptureCtx {
+  Ctx* c;
+  cudaStream_t s[4] = {};
+  bool capturing[4] = {};
+  long long l0 = 0;
+  double p0 = 0.0;
+  void mark() { l0 = c->launches; p0 = c->fine_passes; }
+  long long dl() const { return c->launches - l0; }
+  double dp() const { return c->fine_passes - p0; }
+};
+
+int add_conditional(Ctx* c, cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    cudaGraph_t* body) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  DIVA_CUDA(c, cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  if (st != cudaStreamCaptureStatusActive) return set_error(c, DIVA_CUDA_ERROR, "stream is not capturing");
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = type;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  DIVA_CUDA(c, cudaGraphAddNode(&node, g, deps, nd, &p));
+  *body = p.conditional.phGraph_out[0];
+  DIVA_CUDA(c, cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  return DIVA_OK;
+}
+
+int capture_graph_of(Ctx* c, cudaStream_t s, cudaGraph_t* g) {
+  cudaStreamCaptureStatus st;
+  DIVA_CUDA(c, cudaStreamGetCaptureInfo(s, &st, nullptr, g, nullptr, nullptr));
+  return DIVA_OK;
+}
+
+int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
+  const diva_config_t& C = c->c;
+  const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
+  const Dims d = c->d;
+  const Op o = make_op(c, 0);
+  dim3 g2 = grid2d(d.ny, d.nx);
+  const int nb = g2.x * g2.y;
+  auto U_ = [&](int k) { return c->kv[k][0]; };
+  auto V_ = [&](int k) { return c->kv[k][1]; };
+  double* u = c->D(diva ? DIVA_F_U_VAV_CX : DIVA_F_U_SSA_CX);
+  double* v = c->D(diva ? DIVA_F_V_VAV_CY : DIVA_F_V_SSA_CY);
+  int st;
+
+  cudaGraph_t graph;
+  DIVA_CUDA(c, cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle h_solve;
+  DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_solve, graph, 1, cudaGraphCondAssignDefault));
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[0], graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cc.capturing[0] = true;
+  c->stream = cc.s[0];
+  // ---- pre
+  cc.mark();
+  G.visc_buf[parity] = c->f[DIVA_F_VISC_EFF_3D_A];
+  k_ctl_begin<<<1, 1, 0, c->stream>>>(c->scal); c->launches++;
+  if ((st = launch_diva_coefficients(c, u, v, diva))) return st;   // swaps the viscosity buffers
+  if ((st = solver_setup(c))) return st;
+  if (relmode) {
+    k_relres<<<g2, block2d(), 0, c->stream>>>(o, u, v, U_(KV_B), V_(KV_B), c->partials, g2.x); c->launches++;
+    k_ctl_relres<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, h_solve, C.picard_relres_tol); c->launches++;
+    c->fine_passes += 1.0;
+  }
+  DIVA_LAUNCHED(c, "graph pre");
+  G.n_pre = cc.dl(); G.p_pre = cc.dp();
+  // ---- IF(solve)
+  cudaGraph_t body_solve;
+  if ((st = add_conditional(c, cc.s[0], h_solve, cudaGraphCondTypeIf, &body_solve))) return st;
+  cudaGraphConditionalHandle h_while;
+  DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_while, body_solve, 0, cudaGraphCondAssignDefault));
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[1], body_solve, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+  cc.capturing[1] = true;
+  c->stream = cc.s[1];
+  cc.mark();
+  DIVA_CUDA(c, cudaMemcpyAsync(U_(KV_X), u, sizeof(double) * d.plane, cudaMemcpyDeviceToDevice, c->stream));
+  DIVA_CUDA(c, cudaMemcpyAsync(V_(KV_X), v, sizeof(double) * d.plane, cudaMemcpyDeviceToDevice, c->stream));
+  k_init_residual<<<g2, block2d(), 0, c->stream>>>(o, U_(KV_X), V_(KV_X), U_(KV_B), V_(KV_B), U_(KV_R), V_(KV_R),
+                                                   U_(KV_RHAT), V_(KV_RHAT), U_(KV_P), V_(KV_P), c->partials, g2.x); c->launches++;
+  k_ctl_lin_init<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, h_while, relmode && C.lin_adaptive, C.lin_rtol,
+                                           C.lin_maxit); c->launches++;
+  c->fine_passes += 1.0;
+  DIVA_LAUNCHED(c, "graph head");
+  G.n_head = cc.dl(); G.p_head = cc.dp();
+  // ---- WHILE(krylov)
+  cudaGraph_t body_while;
+  if ((st = add_conditional(c, cc.s[1], h_while, cudaGraphCondTypeWhile, &body_while))) return st;
+  cudaGraphConditionalHandle h_half;
+  DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_half, body_while, 1, cudaGraphCondAssignDefault));
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[2], body_while, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+  cc.capturing[2] = true;
+  c->stream = cc.s[2];
+  cc.mark();
+  if ((st = precond(c, U_(KV_P), V_(KV_P), U_(KV_PHAT), V_(KV_PHAT)))) return st;
+  k_matvec<<<g2, block2d(), 0, c->stream>>>(o, U_(KV_PHAT), V_(KV_PHAT), U_(KV_V), V_(KV_V), U_(KV_RHAT), V_(KV_RHAT),
+                                            nullptr, nullptr, c->partials, g2.x); c->launches++;
+  k_reduce<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, ST_ALPHA); c->launches++;
+  k_update_s<<<g2, block2d(), 0, c->stream>>>(d, c->scal, U_(KV_R), V_(KV_R), U_(KV_V), V_(KV_V), U_(KV_S), V_(KV_S),
+                                              c->partials, g2.x); c->launches++;
+  k_ctl_half<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, h_while, h_half); c->launches++;
+  k_x_half_pred<<<g2, block2d(), 0, c->stream>>>(d, c->scal, U_(KV_X), V_(KV_X), U_(KV_PHAT), V_(KV_PHAT)); c->launches++;
+  c->fine_passes += 3.0;
+  DIVA_LAUNCHED(c, "graph first half");
+  G.n_first = cc.dl(); G.p_first = cc.dp();
+  // ---- IF(second half)
+  cudaGraph_t body_half;
+  if ((st = add_conditional(c, cc.s[2], h_half, cudaGraphCondTypeIf, &body_half))) return st;
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[3], body_half, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+  cc.capturing[3] = true;
+  c->stream = cc.s[3];
+  cc.mark();
+  if ((st = precond(c, U_(KV_S), V_(KV_S), U_(KV_SHAT), V_(KV_SHAT)))) return st;
+  k_matvec<<<g2, block2d(), 0, c->stream>>>(o, U_(KV_SHAT), V_(KV_SHAT), U_(KV_T), V_(KV_T), U_(KV_S), V_(KV_S),
+                                            nullptr, nullptr, c->partials, g2.x); c->launches++;
+  k_reduce<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, ST_OMEGA); c->launches++;
+  k_update_xr<<<g2, block2d(), 0, c->stream>>>(d, c->scal, U_(KV_X), V_(KV_X), U_(KV_PHAT), V_(KV_PHAT), U_(KV_SHAT),
+                                               V_(KV_SHAT), U_(KV_S), V_(KV_S), U_(KV_T), V_(KV_T), U_(KV_R),
+                                               V_(KV_R), U_(KV_RHAT), V_(KV_RHAT), c->partials, g2.x); c->launches++;
+  k_ctl_full<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, h_while, C.lin_maxit); c->launches++;
+  k_update_p<<<g2, block2d(), 0, c->stream>>>(d, c->scal, U_(KV_R), V_(KV_R), U_(KV_V), V_(KV_V), U_(KV_P), V_(KV_P)); c->launches++;
+  c->fine_passes += 3.0;
+  DIVA_LAUNCHED(c, "graph second half");
+  G.n_second = cc.dl(); G.p_second = cc.dp();
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[3], &body_half));
+  cc.capturing[3] = false;
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[2], &body_while));
+  cc.capturing[2] = false;
+  // ---- tail
+  c->stream = cc.s[1];
+  cc.mark();
+  k_ctl_lin_finish<<<1, 1, 0, c->stream>>>(c->scal); c->launches++;
+  k_fill_boundary<<<g2, block2d(), 0, c->stream>>>(d, c->bc, U_(KV_X), V_(KV_X)); c->launches++;
+  DIVA_LAUNCHED(c, "graph tail");
+  if ((st = launch_picard_update(c, u, v, U_(KV_X), V_(KV_X), diva))) return st;
+  if ((st = launch_ctl_end(c, relmode))) return st;
+  if ((st = launch_err_commit_pred(c))) return st;
+  G.n_tail = cc.dl(); G.p_tail = cc.dp();
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[1], &body_solve));
+  cc.capturing[1] = false;
+  // ---- post
+  c->stream = cc.s[0];
+  cc.mark();
+  if (diva && relmode && (st = launch_basal_pred(c))) return st;
+  G.n_post = cc.dl();
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[0], &graph));
+  cc.capturing[0] = false;
+  cudaGraphExec_t exec = nullptr;
+  DIVA_CUDA(c, cudaGraphInstantiate(&exec, graph, 0));
+  cudaGraphDestroy(graph);
+  G.exec[parity] = exec;
+  return DIVA_OK;
+}
+
+}  // namespace
+
+void solver_destroy_graphs(Ctx* c) {
+  for (auto& G : c->graphs) {
+    for (auto& e : G.exec)
+      if (e) cudaGraphExecDestroy(e), e = nullptr;
+    G.valid = false;
+  }
+}
+
+int solver_build_picard_graphs(Ctx* c, bool diva) {
+  PicardGraphs& G = c->graphs[diva ? 1 : 0];
+  if (G.valid) return DIVA_OK;
+  CaptureCtx cc;
+  cc.c = c;
+  cudaStream_t user = c->stream;
+  const long long launches0 = c->launches;
+  const double passes0 = c->fine_passes;
+  const long mg0 = c->mg_cycles;
+  void* visc0 = c->f[DIVA_F_VISC_EFF_3D_A];
+  double* prev0 = c->visc_prev;
+  int st = DIVA_OK;
+  for (int q = 0; q < 4 && !st; ++q)
+    if (cudaStreamCreateWithFlags(&cc.s[q], cudaStreamNonBlocking) != cudaSuccess) st = DIVA_CUDA_ERROR;
+  // parity 0 starts from the current buffer, parity 1 from the other; the two
+  // captures swap the viscosity buffers twice, so the host state is unchanged
+  for (int parity = 0; parity < 2 && !st; ++parity) st = build_one(c, cc, diva, G, parity);
+  for (int q = 3; q >= 0; --q) {
+    if (cc.capturing[q]) {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(cc.s[q], &junk);
+      if (junk) cudaGraphDestroy(junk);
+    }
+  }
+  cudaGetLastError();   // clear any capture error so the host path can proceed
+  for (int q = 0; q < 4; ++q)
+    if (cc.s[q]) cudaStreamDestroy(cc.s[q]);
+  c->stream = user;
+  c->launches = launches0;
+  c->fine_passes = passes0;
+  c->mg_cycles = mg0;
+  c->f[DIVA_F_VISC_EFF_3D_A] = visc0;   // the captures swap these without running anything
+  c->visc_prev = prev0;
+  if (st) {
+    for (auto& e : G.exec)
+      if (e) cudaGraphExecDestroy(e), e = nullptr;
+    return st;
+  }
+  G.valid = true;
   return DIVA_OK;
 }
 

@@ -117,3 +117,18 @@ def test_linear_iteration_cap_is_bounded(cuda):
     rep = ctx.solve_DIVA()
     ctx.close()
     assert rep["picard_iterations"] == 5 and rep["linear_iterations"] == 5
+
+
+def test_graph_launched_iterations_match_direct_launches(cuda, monkeypatch):
+    """Each viscosity iteration runs as one CUDA graph (device-side Krylov loop);
+    launching the same kernels one by one gives bit-identical results."""
+    g, cfg, f = helpers.make_case(2, dx=40e3, overrides={"picard_stop": "relres", "picard_relres_tol": 1e-6,
+                                                         "DIVA_visc_it_nit": 300, "lin_adaptive": 1})
+    rg, og = helpers.run(cuda, g, cfg, f)
+    monkeypatch.setenv("DIVA_NO_GRAPHS", "1")
+    rd, od = helpers.run(cuda, g, cfg, f)
+    assert rg["graph_launched"] == 1 and rd["graph_launched"] == 0
+    assert rg["picard_iterations"] == rd["picard_iterations"]
+    assert rg["linear_iterations"] == rd["linear_iterations"] and rg["mg_cycles"] == rd["mg_cycles"]
+    for k in ("u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "DIVA_err_cx", "taub_cx", "u_3D_cx"):
+        assert np.array_equal(og[k], od[k]), k
