@@ -51,7 +51,9 @@ UNIT = "solves/s"
 INPUT_FIELDS = ["Hi_a", "Hb_a", "SL_a", "dHb_dt_a", "Ti_a", "beta_sq_a"]
 STATE_FIELDS = ["u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "taub_cx", "taub_cy", "u_3D_a", "v_3D_a"]
 OUTPUT_FIELDS = ["u_vav_cx", "v_vav_cy", "u_3D_cx", "v_3D_cy", "w_3D_a", "u_3D_SIA_cx", "v_3D_SIA_cy"]
-KERNEL_NAMES = {0: "k_column_coefficients", 1: "k_gs (fine level, 4 colours)", 2: "k_matvec"}
+KERNEL_NAMES = {0: "k_column_coefficients", 1: "k_gs (fine level, 4 colours)", 2: "k_matvec",
+                3: "V-cycle (all levels)", 4: "k_subcycle (coarse levels, one block)"}
+TRAFFIC_KEYS = {0: "k_column_coefficients", 1: "k_gs", 4: "k_subcycle"}
 
 
 def workload(seed=2):
@@ -261,11 +263,13 @@ def run_b200(args):
 
     # roofline of the dominant kernel: time share = launches per solve x time per launch
     prof = {}
-    for which in (0, 1, 2):
+    for which in (0, 1, 2, 3, 4):
         prof[which] = ctx.profile_kernel(which, reps=30 if which else 10)
-    t_col = prof[0][0] * statistics.mean(picard)
-    t_gs = prof[1][0] * statistics.mean(mg) * 4      # V(2,2): four fine-level sweeps per cycle
-    dom = 0 if t_col >= t_gs else 1
+    # device time per solve of each part, from its in-situ time per launch x launches per solve
+    per_solve = {0: prof[0][0] * statistics.mean(picard),
+                 1: prof[1][0] * statistics.mean(mg) * 4,      # V(2,2): four fine-level sweeps per cycle
+                 4: prof[4][0] * statistics.mean(mg)}
+    dom = max(per_solve, key=per_solve.get)
     ms_l, bytes_l = prof[dom]
     hbm_peak = None
     peak_src = "fallback 6650 GB/s"
@@ -275,13 +279,15 @@ def run_b200(args):
     except Exception:
         hbm_peak = 6650.0
     achieved = bytes_l / (ms_l * 1e-3) / 1e9
-    traffic_key = "k_column_coefficients" if dom == 0 else "k_gs"
+    traffic_key = TRAFFIC_KEYS[dom]
     roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": read_traffic(traffic_key),
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": bytes_l, "ms_per_launch": ms_l,
                 "other_kernels": {KERNEL_NAMES[w]: {"ms_per_launch": prof[w][0],
                                                     "GB/s": prof[w][1] / (prof[w][0] * 1e-3) / 1e9}
-                                  for w in prof}}
+                                  for w in prof},
+                "ms_per_solve": {KERNEL_NAMES[w]: per_solve[w] for w in per_solve} |
+                                {KERNEL_NAMES[3]: prof[3][0] * statistics.mean(mg)}}
 
     # end to end through the public API with pinned host buffers
     def pinned(a):

@@ -173,6 +173,9 @@ size_t carve(Ctx* c, Carver& cv) {
   c->ff_ocean = (int*)cv.take(sizeof(int) * 2 * d.plane);
   c->ff_flag = (int*)cv.take(sizeof(int) * 4);
   c->scal = (double*)cv.take(sizeof(double) * SC_COUNT);
+  c->coarse_A = (double*)cv.take(sizeof(double) * kCoarseDirectMax * kCoarseDirectMax);
+  c->coarse_inv = (double*)cv.take(sizeof(double) * kCoarseDirectMax * kCoarseDirectMax);
+  c->coarse_singular = (int*)cv.take(sizeof(int) * 4);
   const dim3 g = grid2d(d.ny, d.nx);
   c->max_blocks = g.x * g.y;
   c->partials = (double*)cv.take(sizeof(double) * 4 * c->max_blocks);
@@ -656,7 +659,7 @@ int diva_state_restore(diva_ctx_t* h) {
 }
 
 int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, double* bytes) {
-  if (!h || !ms || !bytes || reps < 1 || which < 0 || which > 2) return DIVA_BAD_INPUT;
+  if (!h || !ms || !bytes || reps < 1 || which < 0 || which > 4) return DIVA_BAD_INPUT;
   Ctx* c = &h->c;
   const double nc = (double)c->d.nx * c->d.ny, w = sizeof(double), nz = c->d.nz;
   int st = DIVA_OK;
@@ -666,6 +669,8 @@ int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, 
       case 0: st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true); break;
       case 1: st = solver_smooth_fine(c, 1); break;
       case 2: st = solver_matvec_fine(c, 1); break;
+      case 3: st = solver_vcycle_fine(c, 1); break;
+      case 4: st = solver_subcycle(c, 1); break;
     }
   }
   if (st) return st;
@@ -678,8 +683,10 @@ int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, 
   //  0: read A-factor and the previous viscosity, write the new one (3 nz) + 15 2D fields
   //  1: one sweep over both colours: u, v, N_a, N_b, beta_x, beta_y, b_u, b_v read, u, v written (10)
   //  2: operator application: u, v, N_a, N_b, beta_x, beta_y read, A u, A v written (8)
+  //  3: one V-cycle: per level 4 sweeps, a residual and the transfers, weighted by its points
+  //  4: the one-block coarse levels of a V-cycle (latency-bound; bytes as for 3 over those levels)
   const double per_col[3] = {(3 * nz + 15) * w, 10 * w, 8 * w};
-  *bytes = per_col[which] * nc;
+  *bytes = which < 3 ? per_col[which] * nc : (which == 3 ? solver_vcycle_bytes(c) : 0.0);
   return DIVA_OK;
 }
 

@@ -8,6 +8,7 @@
 namespace diva {
 
 constexpr int kMaxLevels = 12;
+constexpr int kCoarseDirectMax = 64;    // unknowns of a coarsest level solved directly
 
 // One multigrid level of the staggered DIVA operator.  Coefficients are the
 // rediscretised Na (a-grid), Nb (b-grid) and the reaction terms Bx = beta_eff_cx*dx^2
@@ -75,6 +76,12 @@ struct Ctx {
   double* kv[KV_COUNT][2] = {};       // Krylov vectors (u,v)
   Level lv[kMaxLevels];
   int nlev = 0;
+  // inverse of the coarsest level's reduced matrix (when it has few enough unknowns)
+  bool coarse_direct = false;
+  int coarse_n = 0;
+  double* coarse_A = nullptr;         // probed matrix, row-major n x n
+  double* coarse_inv = nullptr;       // its inverse
+  int* coarse_singular = nullptr;     // set by the inversion: relax instead
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   PicardGraphs graphs[2];               // [0] solve_SSA, [1] solve_DIVA
   bool graphs_disabled = false;         // set if graph construction failed: host-driven loop
@@ -136,6 +143,9 @@ int solver_relres(Ctx* c, const double* u, const double* v, double* relres);
 int solver_fill_boundary(Ctx* c, double* u, double* v);
 int solver_smooth_fine(Ctx* c, int sweeps);
 int solver_matvec_fine(Ctx* c, int reps);
+int solver_vcycle_fine(Ctx* c, int reps);
+int solver_subcycle(Ctx* c, int reps);
+double solver_vcycle_bytes(const Ctx* c);
 int solver_build_picard_graphs(Ctx* c, bool diva);
 void solver_destroy_graphs(Ctx* c);
 

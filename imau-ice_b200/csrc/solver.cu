@@ -20,7 +20,9 @@
 //     restriction = transpose of prolongation;
 //   * smoothing is 4-colour Gauss-Seidel (u red/black, v red/black), with the
 //     exact diagonal of the reduced system;
-//   * the coarsest level is relaxed by one thread block with many sweeps.
+//   * the levels below 4096 points run inside one thread block (one launch per
+//     V-cycle), and the coarsest level is solved directly with its inverse,
+//     formed once per viscosity iteration.
 // All reductions are two-stage (block partials, then one fixed-order sum) so
 // results are bit-reproducible from run to run.
 #include <cmath>
@@ -29,6 +31,8 @@
 
 namespace diva {
 namespace {
+
+constexpr int kSubThreads = 1024;       // threads of the one-block coarse-level kernel
 
 struct Op {
   Dims d;
@@ -197,11 +201,10 @@ __global__ void k_gs(Op o, double* xu, double* xv, const double* bu, const doubl
 __device__ __forceinline__ void block_gs_pass(const Op& o, double* xu, double* xv, const double* bu, const double* bv,
                                               const double* idu, const double* idv, int comp, int color) {
   const Dims& d = o.d;
-  const int n = d.nx * d.ny;
+  const int hj = (d.ny + 1) / 2, n = hj * d.nx;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    const int j = t % d.ny, i = t / d.ny;
-    if (((i + j) & 1) != color) continue;
-    gs_point(o, xu, xv, bu, bv, idu, idv, comp, j, i);
+    const int i = t / hj, j = 2 * (t % hj) + ((i + color) & 1);
+    if (j < d.ny) gs_point(o, xu, xv, bu, bv, idu, idv, comp, j, i);
   }
 }
 
@@ -333,6 +336,141 @@ __global__ void k_prolong(Op oc, Dims df, int fx, int fy, const double* xcu, con
   prolong_point(oc, df, fx, fy, xcu, xcv, xu, xv, j, i);
 }
 
+// ---- direct solve of the coarsest level ------------------------------------------------
+// The coarsest level has at most kCoarseDirectMax interior unknowns, numbered u first,
+// then v, each in plane order (i outer, j inner).  Its reduced matrix is probed column
+// by column with the smoother's own operator (Au/Av through the boundary elimination)
+// and inverted by Gauss-Jordan elimination with partial pivoting once per viscosity
+// iteration, so the coarse step of every V-cycle is one matrix-vector product.  A pivot
+// below 1e-13 of the largest entry (a singular coarse operator, e.g. a free-floating
+// shelf with no fixed boundary) raises the flag and the coarse step relaxes instead.
+struct CoarseMap {
+  int ny, nu, nv;
+  __device__ __forceinline__ int n() const { return nu + nv; }
+  __device__ __forceinline__ void point(int r, int& comp, int& j, int& i) const {
+    if (r < nu) { comp = 0; i = 1 + r / (ny - 2); j = 1 + r % (ny - 2); }
+    else { const int q = r - nu; comp = 1; i = 1 + q / (ny - 3); j = 1 + q % (ny - 3); }
+  }
+};
+
+// column c = blockIdx.x of the coarse matrix: A e_c evaluated at every row
+__global__ void k_coarse_probe(Op o, CoarseMap m, double* A) {
+  extern __shared__ double sx[];   // unit vector e_c: u plane, then v plane
+  const int plane = (int)o.d.plane, n = m.n(), c = blockIdx.x;
+  for (int t = threadIdx.x; t < 2 * plane; t += blockDim.x) sx[t] = 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int comp, j, i;
+    m.point(c, comp, j, i);
+    sx[comp * plane + o.d.at(j, i)] = 1.0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    int comp, j, i;
+    m.point(r, comp, j, i);
+    A[r * n + c] = comp == 0 ? Au(o, sx, sx + plane, j, i) : Av(o, sx, sx + plane, j, i);
+  }
+}
+
+// Ainv = A^{-1} by in-place Gauss-Jordan with row pivoting (columns unscrambled at the end)
+__global__ void __launch_bounds__(256) k_coarse_invert(int n, const double* A, double* Ainv, int* singular) {
+  constexpr int M = kCoarseDirectMax;
+  __shared__ double a[M][M + 1];
+  __shared__ double fcol[M];
+  __shared__ int perm[M];
+  __shared__ double red[256];
+  __shared__ int s_p, s_bad;
+  const int tid = threadIdx.x;
+  double amax = 0.0;
+  for (int e = tid; e < n * n; e += blockDim.x) {
+    const double v = A[e];
+    a[e / n][e % n] = v;
+    amax = (fabs(v) > amax || v != v) ? fabs(v) : amax;
+  }
+  red[tid] = amax;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (tid < o) red[tid] = (red[tid + o] > red[tid] || red[tid + o] != red[tid + o]) ? red[tid + o] : red[tid];
+    __syncthreads();
+  }
+  const double tiny = 1e-13 * red[0];
+  if (tid == 0) s_bad = !(red[0] > 0.0) || red[0] != red[0];
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {   // s_bad is read only between barriers that follow its last write
+    if (tid < 32) {   // pivot: largest |a[r][k]|, r >= k, lowest r on ties
+      double best = -1.0;
+      int br = k;
+      for (int r = k + tid; r < n; r += 32)
+        if (fabs(a[r][k]) > best) { best = fabs(a[r][k]); br = r; }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int orr = __shfl_down_sync(0xffffffffu, br, o);
+        if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
+      }
+      if (tid == 0) {
+        s_p = br;
+        if (!(best > tiny)) s_bad = 1;
+      }
+    }
+    __syncthreads();
+    if (s_bad) break;
+    const int p = s_p;
+    if (p != k)
+      for (int c = tid; c < n; c += blockDim.x) {
+        const double t = a[k][c];
+        a[k][c] = a[p][c];
+        a[p][c] = t;
+      }
+    if (tid == 0) perm[k] = p;
+    __syncthreads();
+    const double piv = a[k][k];
+    for (int r = tid; r < n; r += blockDim.x) fcol[r] = a[r][k];
+    __syncthreads();
+    for (int c = tid; c < n; c += blockDim.x) a[k][c] = (c == k ? 1.0 : a[k][c]) / piv;
+    __syncthreads();
+    for (int e = tid; e < n * n; e += blockDim.x) {
+      const int r = e / n, c = e % n;
+      if (r != k) a[r][c] = (c == k ? 0.0 : a[r][c]) - fcol[r] * a[k][c];
+    }
+    __syncthreads();
+  }
+  if (!s_bad) {
+    for (int k = n - 1; k >= 0; --k) {
+      const int p = perm[k];
+      if (p != k)
+        for (int r = tid; r < n; r += blockDim.x) {
+          const double t = a[r][k];
+          a[r][k] = a[r][p];
+          a[r][p] = t;
+        }
+      __syncthreads();
+    }
+    for (int e = tid; e < n * n; e += blockDim.x) Ainv[e] = a[e / n][e % n];
+  }
+  if (tid == 0) *singular = s_bad;
+}
+
+// x += Ainv (b - A x) on the coarsest level, by one block (the caller synchronises)
+__device__ __forceinline__ void block_coarse_direct(const Op& o, const CoarseMap& m, const double* Ainv, double* xu,
+                                                    double* xv, const double* bu, const double* bv) {
+  __shared__ double sr[kCoarseDirectMax];
+  const int n = m.n();
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    int comp, j, i;
+    m.point(r, comp, j, i);
+    const long long q = o.d.at(j, i);
+    sr[r] = comp == 0 ? bu[q] - Au(o, xu, xv, j, i) : bv[q] - Av(o, xu, xv, j, i);
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    double s = 0.0;
+    for (int c = 0; c < n; ++c) s += Ainv[r * n + c] * sr[c];
+    int comp, j, i;
+    m.point(r, comp, j, i);
+    (comp == 0 ? xu : xv)[o.d.at(j, i)] += s;
+  }
+}
+
 // The levels from `first` down, run by one thread block with barriers between
 // the phases: the same per-point operations in the same order as the per-level
 // kernels of vcycle(), without a launch per phase.
@@ -344,6 +482,10 @@ struct SubLevel {
 };
 struct SubCycle {
   int first, last, nu1, nu2, coarse_sweeps;
+  int direct;                  // coarsest level solved with Ainv unless *singular
+  CoarseMap map;
+  const double* Ainv;
+  const int* singular;
   SubLevel L[kMaxLevels];
 };
 
@@ -353,8 +495,8 @@ __device__ __forceinline__ void block_for_points(const Dims& d, F f) {
   for (int t = threadIdx.x; t < n; t += blockDim.x) f(t % d.ny, t / d.ny);
 }
 
-__global__ void __launch_bounds__(512) k_subcycle(SubCycle sc, double* xu0, double* xv0, const double* bu0,
-                                                  const double* bv0) {
+__global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* xu0, double* xv0,
+                                                          const double* bu0, const double* bv0) {
   // descend
   for (int l = sc.first; l <= sc.last; ++l) {
     const SubLevel& L = sc.L[l];
@@ -363,7 +505,12 @@ __global__ void __launch_bounds__(512) k_subcycle(SubCycle sc, double* xu0, doub
     const double* bu = l == sc.first ? bu0 : L.bu;
     const double* bv = l == sc.first ? bv0 : L.bv;
     if (l == sc.last) {
-      block_coarse_relax(L.o, xu, xv, bu, bv, L.idu, L.idv, sc.coarse_sweeps);
+      if (sc.direct && *sc.singular == 0) {
+        block_coarse_direct(L.o, sc.map, sc.Ainv, xu, xv, bu, bv);
+        __syncthreads();
+      } else {
+        block_coarse_relax(L.o, xu, xv, bu, bv, L.idu, L.idv, sc.coarse_sweeps);
+      }
       break;
     }
     for (int s = 0; s < sc.nu1; ++s)
@@ -804,6 +951,15 @@ static void factors(const Ctx* c, int l, int* fx, int* fy) {
 
 #define GL(l) grid2d(c->lv[l].d.ny, c->lv[l].d.nx), block2d(), 0, c->stream
 
+static CoarseMap coarse_map(const Ctx* c) {
+  const Dims& d = c->lv[c->nlev - 1].d;
+  CoarseMap m;
+  m.ny = d.ny;
+  m.nu = (d.nx > 3 && d.ny > 2) ? (d.nx - 3) * (d.ny - 2) : 0;
+  m.nv = (d.nx > 2 && d.ny > 3) ? (d.nx - 2) * (d.ny - 3) : 0;
+  return m;
+}
+
 int solver_setup(Ctx* c) {
   const diva_config_t& C = c->c;
   if (C.choice_ice_margin == DIVA_MARGIN_BC)
@@ -822,6 +978,16 @@ int solver_setup(Ctx* c) {
   for (int l = 0; l < c->nlev; ++l) {
     k_diag<<<GL(l)>>>(make_op(c, l), c->lv[l].idu, c->lv[l].idv); c->launches++;
     DIVA_LAUNCHED(c, "k_diag");
+  }
+  const CoarseMap m = coarse_map(c);
+  const Dims& dc = c->lv[c->nlev - 1].d;
+  c->coarse_n = m.nu + m.nv;
+  c->coarse_direct = c->coarse_n > 0 && c->coarse_n <= kCoarseDirectMax && 2 * dc.plane * sizeof(double) <= 32768;
+  if (c->coarse_direct) {
+    k_coarse_probe<<<c->coarse_n, 128, 2 * dc.plane * sizeof(double), c->stream>>>(make_op(c, c->nlev - 1), m,
+                                                                                    c->coarse_A); c->launches++;
+    k_coarse_invert<<<1, 256, 0, c->stream>>>(c->coarse_n, c->coarse_A, c->coarse_inv, c->coarse_singular); c->launches++;
+    DIVA_LAUNCHED(c, "coarse inverse");
   }
   return DIVA_OK;
 }
@@ -857,6 +1023,10 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
     sc.nu1 = nu1;
     sc.nu2 = nu2;
     sc.coarse_sweeps = coarse_sweeps;
+    sc.direct = c->coarse_direct ? 1 : 0;
+    sc.map = coarse_map(c);
+    sc.Ainv = c->coarse_inv;
+    sc.singular = c->coarse_singular;
     for (int q = l; q < c->nlev; ++q) {
       const Level& L = c->lv[q];
       SubLevel& S = sc.L[q];
@@ -866,7 +1036,7 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
       S.fx = 1; S.fy = 1;
       if (q + 1 < c->nlev) factors(c, q, &S.fx, &S.fy);
     }
-    k_subcycle<<<1, 512, 0, c->stream>>>(sc, xu, xv, bu, bv); c->launches++;
+    k_subcycle<<<1, kSubThreads, 0, c->stream>>>(sc, xu, xv, bu, bv); c->launches++;
     DIVA_LAUNCHED(c, "k_subcycle");
     for (int q = l; q < c->nlev; ++q) c->fine_passes += 8.0 * (double)c->lv[q].d.plane / (double)c->d.plane;
     return DIVA_OK;
@@ -1014,6 +1184,35 @@ int solver_matvec_fine(Ctx* c, int reps) {
   }
   DIVA_LAUNCHED(c, "k_matvec");
   return DIVA_OK;
+}
+
+// one preconditioner application (V-cycle from zero) on the current Krylov residual
+int solver_vcycle_fine(Ctx* c, int reps) {
+  for (int r = 0; r < reps; ++r) {
+    int st = precond(c, c->kv[KV_R][0], c->kv[KV_R][1], c->kv[KV_PHAT][0], c->kv[KV_PHAT][1]);
+    if (st) return st;
+  }
+  return DIVA_OK;
+}
+
+// the one-block part of the V-cycle alone, on the arrays of its first level
+int solver_subcycle(Ctx* c, int reps) {
+  const int l = sub_first_level(c);
+  const Level& L = c->lv[l];
+  for (int r = 0; r < reps; ++r) {
+    int st = vcycle(c, l, L.xu, L.xv, L.bu, L.bv);
+    if (st) return st;
+  }
+  return DIVA_OK;
+}
+
+// algorithmic bytes of one V-cycle (FP64, compulsory traffic per point and level):
+// each sweep 10 values, the residual 8, the transfers 6, weighted by the level's points
+double solver_vcycle_bytes(const Ctx* c) {
+  double b = 0.0;
+  for (int l = 0; l < c->nlev; ++l)
+    b += (double)c->lv[l].d.nx * c->lv[l].d.ny * sizeof(double) * (4 * 10 + 8 + 6);
+  return b;
 }
 
 int solver_fill_boundary(Ctx* c, double* u, double* v) {
