@@ -406,6 +406,8 @@ int diva_create(diva_ctx_t** out, const diva_grid_t* g, const diva_config_t* cfg
   // DIVA_NO_GRAPHS=1 launches the same kernels one by one instead of from
   // CUDA graphs (kernel-level profilers list them individually that way)
   if (const char* e = getenv("DIVA_NO_GRAPHS")) c->graphs_disabled = (e[0] == '1');
+  // DIVA_NO_TILES=1 smooths every level with the per-colour kernels (same results)
+  if (const char* e = getenv("DIVA_NO_TILES")) c->tiles_disabled = (e[0] == '1');
   Carver dry{nullptr, 0, true};
   const size_t bytes = carve(c, dry);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return DIVA_CUDA_ERROR; }
@@ -421,7 +423,7 @@ int diva_create(diva_ctx_t** out, const diva_grid_t* g, const diva_config_t* cfg
   if (cudaMallocHost(&c->h_scal, sizeof(double) * SC_COUNT) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaMemsetAsync(c->arena, 0, bytes, c->stream) != cudaSuccess ||
-      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+      cudaStreamSynchronize(c->stream) != cudaSuccess || solver_init(c) != DIVA_OK) {
     diva_destroy(h);
     return DIVA_CUDA_ERROR;
   }
@@ -451,7 +453,7 @@ int diva_set_config(diva_ctx_t* h, const diva_config_t* cfg) {
   if (st) return st;
   apply_config(&h->c, cfg);
   solver_destroy_graphs(&h->c);   // captured kernel arguments carry the configuration
-  return DIVA_OK;
+  return solver_init(&h->c);
 }
 
 int diva_set_stream(diva_ctx_t* h, void* stream) {

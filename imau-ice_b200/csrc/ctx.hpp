@@ -85,6 +85,8 @@ struct Ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   PicardGraphs graphs[2];               // [0] solve_SSA, [1] solve_DIVA
   bool graphs_disabled = false;         // set if graph construction failed: host-driven loop
+  bool tiled = false;                   // large levels smoothed by the tiled kernels
+  bool tiles_disabled = false;          // per-colour kernels on every level
   // counters of the last solve
   long lin_iters = 0, mg_cycles = 0;
   long long launches = 0;            // kernels launched since create
@@ -137,6 +139,7 @@ int launch_basal_pred(Ctx* c);
 int launch_any_sheet(Ctx* c, int* result);
 
 // solver.cu
+int solver_init(Ctx* c);      // per-context solver choices (after the configuration is known)
 int solver_setup(Ctx* c);     // coefficients of all levels from N_a, N_b, beta_eff, taud
 int solver_solve(Ctx* c, const double* u0, const double* v0, double rtol, int maxit, int* iters, double* relres0);
 int solver_relres(Ctx* c, const double* u, const double* v, double* relres);

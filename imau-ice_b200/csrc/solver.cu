@@ -20,8 +20,10 @@
 //     restriction = transpose of prolongation;
 //   * smoothing is 4-colour Gauss-Seidel (u red/black, v red/black), with the
 //     exact diagonal of the reduced system;
-//   * the levels below 4096 points run inside one thread block (one launch per
-//     V-cycle), and the coarsest level is solved directly with its inverse,
+//   * the larger levels are smoothed by tile kernels (two launches per level and
+//     V-cycle, halo recomputed instead of exchanged), the coarse levels whose
+//     data fit in 200 KB run out of one thread block's shared memory (one launch
+//     per V-cycle), and the coarsest level is solved directly with its inverse,
 //     formed once per viscosity iteration.
 // All reductions are two-stage (block partials, then one fixed-order sum) so
 // results are bit-reproducible from run to run.
@@ -88,44 +90,71 @@ __device__ __forceinline__ bool v_src(const Dims& d, const BCs& b, int j, int i,
   else { is = W ? d.nx - 2 : (E ? 1 : i); js = S ? d.ny - 3 : (N ? 1 : j); }
   return true;
 }
+// Where the x values of the (j,i) point live: a full plane of the level (GIx), or
+// a shared-memory tile whose origin is (j0,i0) and whose rows hold rj points (TIx).
+struct GIx {
+  Dims d;
+  __device__ __forceinline__ long long operator()(int j, int i) const { return d.at(j, i); }
+};
+struct TIx {
+  int j0, i0, rj;
+  __device__ __forceinline__ int operator()(int j, int i) const { return (i - i0) * rj + (j - j0); }
+};
+
 // Read a u (v) value through the boundary elimination (RAW = false), or as
 // stored (RAW = true: the reference's assembled rows reference stored values).
+template <bool RAW, class IX>
+__device__ __forceinline__ double LUx(const Op& o, const double* x, const IX& ix, int j, int i) {
+  if (RAW) return x[ix(j, i)];
+  int js, is;
+  return u_src(o.d, o.bc, j, i, js, is) ? x[ix(js, is)] : 0.0;
+}
+template <bool RAW, class IX>
+__device__ __forceinline__ double LVx(const Op& o, const double* x, const IX& ix, int j, int i) {
+  if (RAW) return x[ix(j, i)];
+  int js, is;
+  return v_src(o.d, o.bc, j, i, js, is) ? x[ix(js, is)] : 0.0;
+}
 template <bool RAW = false>
 __device__ __forceinline__ double LU(const Op& o, const double* x, int j, int i) {
-  if (RAW) return x[o.d.at(j, i)];
-  int js, is;
-  return u_src(o.d, o.bc, j, i, js, is) ? x[o.d.at(js, is)] : 0.0;
+  return LUx<RAW>(o, x, GIx{o.d}, j, i);
 }
 template <bool RAW = false>
 __device__ __forceinline__ double LV(const Op& o, const double* x, int j, int i) {
-  if (RAW) return x[o.d.at(j, i)];
-  int js, is;
-  return v_src(o.d, o.bc, j, i, js, is) ? x[o.d.at(js, is)] : 0.0;
+  return LVx<RAW>(o, x, GIx{o.d}, j, i);
 }
 
 // (A x) of the u row at interior (j,i) (list_DIVA_matrix_coefficients_eq_1_free :2342-2404)
-template <bool RAW = false>
-__device__ __forceinline__ double Au(const Op& o, const double* xu, const double* xv, int j, int i) {
+template <bool RAW, class IX>
+__device__ __forceinline__ double AuX(const Op& o, const double* xu, const double* xv, const IX& ix, int j, int i) {
   const Dims& d = o.d;
   const double Ae = o.Na[d.at(j, i + 1)], Aw = o.Na[d.at(j, i)], Bn = o.Nb[d.at(j, i)], Bs = o.Nb[d.at(j - 1, i)];
   const double cE = 4.0 * o.ax * Ae, cW = 4.0 * o.ax * Aw, cN = o.ay * Bn, cS = o.ay * Bs;
   const double diag = -(cE + cW + cN + cS) - o.Bx[d.at(j, i)];
-  return cE * LU<RAW>(o, xu, j, i + 1) + cW * LU<RAW>(o, xu, j, i - 1) + cN * LU<RAW>(o, xu, j + 1, i) +
-         cS * LU<RAW>(o, xu, j - 1, i) + diag * xu[d.at(j, i)] + (-2.0 * Aw - Bn) * LV<RAW>(o, xv, j, i) +
-         (2.0 * Ae + Bn) * LV<RAW>(o, xv, j, i + 1) + (2.0 * Aw + Bs) * LV<RAW>(o, xv, j - 1, i) +
-         (-2.0 * Ae - Bs) * LV<RAW>(o, xv, j - 1, i + 1);
+  return cE * LUx<RAW>(o, xu, ix, j, i + 1) + cW * LUx<RAW>(o, xu, ix, j, i - 1) +
+         cN * LUx<RAW>(o, xu, ix, j + 1, i) + cS * LUx<RAW>(o, xu, ix, j - 1, i) + diag * xu[ix(j, i)] +
+         (-2.0 * Aw - Bn) * LVx<RAW>(o, xv, ix, j, i) + (2.0 * Ae + Bn) * LVx<RAW>(o, xv, ix, j, i + 1) +
+         (2.0 * Aw + Bs) * LVx<RAW>(o, xv, ix, j - 1, i) + (-2.0 * Ae - Bs) * LVx<RAW>(o, xv, ix, j - 1, i + 1);
 }
 // (A x) of the v row at interior (j,i) (list_DIVA_matrix_coefficients_eq_2_free :2405-2467)
-template <bool RAW = false>
-__device__ __forceinline__ double Av(const Op& o, const double* xu, const double* xv, int j, int i) {
+template <bool RAW, class IX>
+__device__ __forceinline__ double AvX(const Op& o, const double* xu, const double* xv, const IX& ix, int j, int i) {
   const Dims& d = o.d;
   const double An = o.Na[d.at(j + 1, i)], As = o.Na[d.at(j, i)], Be = o.Nb[d.at(j, i)], Bw = o.Nb[d.at(j, i - 1)];
   const double cN = 4.0 * o.ay * An, cS = 4.0 * o.ay * As, cE = o.ax * Be, cW = o.ax * Bw;
   const double diag = -(cN + cS + cE + cW) - o.By[d.at(j, i)];
-  return cN * LV<RAW>(o, xv, j + 1, i) + cS * LV<RAW>(o, xv, j - 1, i) + cE * LV<RAW>(o, xv, j, i + 1) +
-         cW * LV<RAW>(o, xv, j, i - 1) + diag * xv[d.at(j, i)] + (-2.0 * An - Bw) * LU<RAW>(o, xu, j + 1, i - 1) +
-         (2.0 * An + Be) * LU<RAW>(o, xu, j + 1, i) + (2.0 * As + Bw) * LU<RAW>(o, xu, j, i - 1) +
-         (-2.0 * As - Be) * LU<RAW>(o, xu, j, i);
+  return cN * LVx<RAW>(o, xv, ix, j + 1, i) + cS * LVx<RAW>(o, xv, ix, j - 1, i) +
+         cE * LVx<RAW>(o, xv, ix, j, i + 1) + cW * LVx<RAW>(o, xv, ix, j, i - 1) + diag * xv[ix(j, i)] +
+         (-2.0 * An - Bw) * LUx<RAW>(o, xu, ix, j + 1, i - 1) + (2.0 * An + Be) * LUx<RAW>(o, xu, ix, j + 1, i) +
+         (2.0 * As + Bw) * LUx<RAW>(o, xu, ix, j, i - 1) + (-2.0 * As - Be) * LUx<RAW>(o, xu, ix, j, i);
+}
+template <bool RAW = false>
+__device__ __forceinline__ double Au(const Op& o, const double* xu, const double* xv, int j, int i) {
+  return AuX<RAW>(o, xu, xv, GIx{o.d}, j, i);
+}
+template <bool RAW = false>
+__device__ __forceinline__ double Av(const Op& o, const double* xu, const double* xv, int j, int i) {
+  return AvX<RAW>(o, xu, xv, GIx{o.d}, j, i);
 }
 // effective diagonal of the reduced system: couplings to boundary unknowns whose source is the row itself fold in
 __device__ __forceinline__ double diag_u(const Op& o, int j, int i) {
@@ -301,13 +330,15 @@ __global__ void k_restrict(Dims df, Dims dc, int fx, int fy, const double* ru, c
   restrict_point(df, dc, fx, fy, ru, rv, bu, bv, xu, xv, j, i);
 }
 
-// x_f += P x_c on fine interior points (coarse values read through the coarse boundary mapping)
-__device__ __forceinline__ void prolong_point(const Op& oc, const Dims& df, int fx, int fy, const double* xcu,
-                                              const double* xcv, double* xu, double* xv, int j, int i) {
-  const long long q = df.at(j, i);
+// P x_c at the fine point (j,i): increments of u and v (coarse values read through the
+// coarse boundary mapping); zero off the fine interior
+__device__ __forceinline__ void prolong_delta(const Op& oc, const Dims& df, int fx, int fy, const double* xcu,
+                                              const double* xcv, int j, int i, double& du, double& dv) {
   int Ci[2], Cj[2];
   double wi[2], wj[2];
   const Dims& dc = oc.d;
+  du = 0.0;
+  dv = 0.0;
   if (u_int(df, j, i)) {
     const int ni = scatter_cell(i, fx, Ci, wi), nj = scatter_node(j, fy, Cj, wj);
     double s = 0.0;
@@ -316,7 +347,7 @@ __device__ __forceinline__ void prolong_point(const Op& oc, const Dims& df, int 
         const int J = min(max(Cj[a], 0), dc.ny - 1), I = min(max(Ci[b], 0), dc.nx - 2);
         s += wj[a] * wi[b] * LU(oc, xcu, J, I);
       }
-    xu[q] += s;
+    du = s;
   }
   if (v_int(df, j, i)) {
     const int ni = scatter_node(i, fx, Ci, wi), nj = scatter_cell(j, fy, Cj, wj);
@@ -326,14 +357,161 @@ __device__ __forceinline__ void prolong_point(const Op& oc, const Dims& df, int 
         const int J = min(max(Cj[a], 0), dc.ny - 2), I = min(max(Ci[b], 0), dc.nx - 1);
         s += wj[a] * wi[b] * LV(oc, xcv, J, I);
       }
-    xv[q] += s;
+    dv = s;
   }
+}
+// x_f += P x_c on fine interior points
+__device__ __forceinline__ void prolong_point(const Op& oc, const Dims& df, int fx, int fy, const double* xcu,
+                                              const double* xcv, double* xu, double* xv, int j, int i) {
+  const long long q = df.at(j, i);
+  double du, dv;
+  prolong_delta(oc, df, fx, fy, xcu, xcv, j, i, du, dv);
+  if (u_int(df, j, i)) xu[q] += du;
+  if (v_int(df, j, i)) xv[q] += dv;
 }
 __global__ void k_prolong(Op oc, Dims df, int fx, int fy, const double* xcu, const double* xcv, double* xu,
                           double* xv) {
   IDX2D
   if (j >= df.ny || i >= df.nx) return;
   prolong_point(oc, df, fx, fy, xcu, xcv, xu, xv, j, i);
+}
+
+// ---- tiled smoothing of the large levels ---------------------------------------------
+// One block owns a TJ x TI tile of a level and keeps x and b of the tile plus a
+// halo of kHalo points on every side in shared memory.  Colour pass q of a
+// smoothing phase updates the points within kHalo-1-q of the tile.  Every value
+// a row reads -- its stencil neighbours and, on an 'infinite' or 'zero' side, the
+// inner point a boundary unknown is mapped to -- lies within one point of the row,
+// so after the 8 passes of V(2,2)'s pre- or post-smoothing the tile and one ring
+// around it hold exactly what the level-wide colour sweeps produce, and the
+// residual of the tile follows from them.  The halo is recomputed by the
+// neighbouring blocks instead of exchanged.  A periodic side maps a boundary
+// unknown across the domain, so such grids use the per-colour kernels.
+constexpr int kHalo = 9;
+constexpr int kTileThreads = 512;
+
+template <int TJ, int TI>
+struct TileGeom {
+  static constexpr int RJ = TJ + 2 * kHalo, RI = TI + 2 * kHalo, N = RJ * RI;
+  static constexpr size_t smem = 4 * N * sizeof(double);   // xu, xv, bu, bv of the region
+};
+
+// Chebyshev distance of (j,i) from the tile [tj0, tj0+TJ) x [ti0, ti0+TI)
+__device__ __forceinline__ int tile_dist(int j, int i, int tj0, int ti0, int TJ, int TI) {
+  const int dj = max(max(tj0 - j, j - (tj0 + TJ - 1)), 0);
+  const int di = max(max(ti0 - i, i - (ti0 + TI - 1)), 0);
+  return max(dj, di);
+}
+
+// one colour pass over the region points within `reach` of the tile
+template <int TJ, int TI>
+__device__ __forceinline__ void tile_pass(const Op& o, const TIx& ix, double* xu, double* xv, const double* bu,
+                                          const double* bv, const double* idu, const double* idv, int tj0, int ti0,
+                                          int comp, int color, int reach) {
+  using G = TileGeom<TJ, TI>;
+  const Dims& d = o.d;
+  constexpr int hj = (G::RJ + 1) / 2;
+  for (int t = threadIdx.x; t < hj * G::RI; t += blockDim.x) {
+    const int i = ix.i0 + t / hj;
+    const int j = ix.j0 + 2 * (t % hj) + ((color + i + ix.j0) & 1);   // (i + j) & 1 == color
+    if (j >= ix.j0 + G::RJ || j < 0 || j >= d.ny || i < 0 || i >= d.nx) continue;
+    if (tile_dist(j, i, tj0, ti0, TJ, TI) > reach) continue;
+    const long long q = d.at(j, i);
+    const int k = ix(j, i);
+    if (comp == 0) {
+      if (u_int(d, j, i)) xu[k] += (bu[k] - AuX<false>(o, xu, xv, ix, j, i)) * idu[q];
+    } else {
+      if (v_int(d, j, i)) xv[k] += (bv[k] - AvX<false>(o, xu, xv, ix, j, i)) * idv[q];
+    }
+  }
+}
+
+// pre-smoothing: `sweeps` forward sweeps (u0 u1 v0 v1) from x, then x and r = b - A x of the tile
+template <int TJ, int TI>
+__global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, const double* gbu, const double* gbv,
+                                                              double* gxu, double* gxv, double* gru, double* grv,
+                                                              const double* idu, const double* idv, int sweeps) {
+  using G = TileGeom<TJ, TI>;
+  extern __shared__ double sm[];
+  double *xu = sm, *xv = sm + G::N, *bu = sm + 2 * G::N, *bv = sm + 3 * G::N;
+  const Dims& d = o.d;
+  const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
+  const TIx ix{tj0 - kHalo, ti0 - kHalo, G::RJ};
+  for (int t = threadIdx.x; t < G::N; t += blockDim.x) {
+    const int j = ix.j0 + t % G::RJ, i = ix.i0 + t / G::RJ;
+    const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
+    const long long q = in ? d.at(j, i) : 0;
+    xu[t] = in ? gxu[q] : 0.0;
+    xv[t] = in ? gxv[q] : 0.0;
+    bu[t] = in ? gbu[q] : 0.0;
+    bv[t] = in ? gbv[q] : 0.0;
+  }
+  __syncthreads();
+  int pass = 0;
+  for (int s = 0; s < sweeps; ++s)
+    for (int p = 0; p < 4; ++p, ++pass) {
+      tile_pass<TJ, TI>(o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      __syncthreads();
+    }
+  for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
+    const int j = tj0 + t % TJ, i = ti0 + t / TJ;
+    if (j >= d.ny || i >= d.nx) continue;
+    const long long q = d.at(j, i);
+    const int k = ix(j, i);
+    gxu[q] = xu[k];
+    gxv[q] = xv[k];
+    gru[q] = u_int(d, j, i) ? bu[k] - AuX<false>(o, xu, xv, ix, j, i) : 0.0;
+    grv[q] = v_int(d, j, i) ? bv[k] - AvX<false>(o, xu, xv, ix, j, i) : 0.0;
+  }
+}
+
+// post-smoothing: x += P x_c, then `sweeps` backward sweeps (v1 v0 u1 u0); x of the tile
+template <int TJ, int TI>
+__global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx, int fy, const double* xcu,
+                                                            const double* xcv, const double* gbu, const double* gbv,
+                                                            double* gxu, double* gxv, const double* idu,
+                                                            const double* idv, int sweeps) {
+  using G = TileGeom<TJ, TI>;
+  extern __shared__ double sm[];
+  double *xu = sm, *xv = sm + G::N, *bu = sm + 2 * G::N, *bv = sm + 3 * G::N;
+  const Dims& d = o.d;
+  const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
+  const TIx ix{tj0 - kHalo, ti0 - kHalo, G::RJ};
+  for (int t = threadIdx.x; t < G::N; t += blockDim.x) {
+    const int j = ix.j0 + t % G::RJ, i = ix.i0 + t / G::RJ;
+    const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
+    double xa = 0.0, xb = 0.0, ba = 0.0, bb = 0.0;
+    if (in) {
+      const long long q = d.at(j, i);
+      double du, dv;
+      prolong_delta(oc, d, fx, fy, xcu, xcv, j, i, du, dv);
+      xa = gxu[q];
+      xb = gxv[q];
+      if (u_int(d, j, i)) xa += du;
+      if (v_int(d, j, i)) xb += dv;
+      ba = gbu[q];
+      bb = gbv[q];
+    }
+    xu[t] = xa;
+    xv[t] = xb;
+    bu[t] = ba;
+    bv[t] = bb;
+  }
+  __syncthreads();
+  int pass = 0;
+  for (int s = 0; s < sweeps; ++s)
+    for (int p = 3; p >= 0; --p, ++pass) {
+      tile_pass<TJ, TI>(o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      __syncthreads();
+    }
+  for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
+    const int j = tj0 + t % TJ, i = ti0 + t / TJ;
+    if (j >= d.ny || i >= d.nx) continue;
+    const long long q = d.at(j, i);
+    const int k = ix(j, i);
+    gxu[q] = xu[k];
+    gxv[q] = xv[k];
+  }
 }
 
 // ---- direct solve of the coarsest level ------------------------------------------------
@@ -471,14 +649,21 @@ __device__ __forceinline__ void block_coarse_direct(const Op& o, const CoarseMap
   }
 }
 
-// The levels from `first` down, run by one thread block with barriers between
-// the phases: the same per-point operations in the same order as the per-level
-// kernels of vcycle(), without a launch per phase.
+// The levels from `first` down, run by one thread block out of shared memory with
+// barriers between the phases: the same per-point operations in the same order
+// as the per-level kernels of vcycle(), without a launch per phase and without a
+// global-memory round trip per phase.  Each level keeps kSubArrays compact planes
+// (row length ny) in the block's dynamic shared memory; the coefficients of every
+// level and x, b of the first are staged in at the start, x of the first level is
+// written back at the end.
+enum { SA_NA, SA_NB, SA_BX, SA_BY, SA_IDU, SA_IDV, SA_XU, SA_XV, SA_BU, SA_BV, SA_RU, SA_RV, kSubArrays };
+constexpr size_t kSubSmemBudget = 200 * 1024;   // dynamic shared memory of the sub-cycle
+
 struct SubLevel {
-  Op o;
-  double *xu, *xv, *bu, *bv, *ru, *rv;
-  const double *idu, *idv;
-  int fx, fy;   // coarsening factors to the next level
+  Op o;                      // global-memory operator of the level
+  const double *idu, *idv;   // global inverse diagonals
+  int fx, fy;                // coarsening factors to the next level
+  int soff;                  // offset of the level's planes in shared memory (doubles)
 };
 struct SubCycle {
   int first, last, nu1, nu2, coarse_sweeps;
@@ -497,50 +682,99 @@ __device__ __forceinline__ void block_for_points(const Dims& d, F f) {
 
 __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* xu0, double* xv0,
                                                           const double* bu0, const double* bv0) {
-  // descend
+  extern __shared__ double sm[];
+  __shared__ Op so[kMaxLevels];   // operators of the staged levels
+  if (threadIdx.x == 0)
+    for (int l = sc.first; l <= sc.last; ++l) {
+      Op o = sc.L[l].o;
+      const int P = o.d.nx * o.d.ny;
+      o.d.ld = o.d.ny;
+      o.d.plane = P;
+      double* a = sm + sc.L[l].soff;
+      o.Na = a + SA_NA * P;
+      o.Nb = a + SA_NB * P;
+      o.Bx = a + SA_BX * P;
+      o.By = a + SA_BY * P;
+      so[l] = o;
+    }
   for (int l = sc.first; l <= sc.last; ++l) {
     const SubLevel& L = sc.L[l];
-    double* xu = l == sc.first ? xu0 : L.xu;
-    double* xv = l == sc.first ? xv0 : L.xv;
-    const double* bu = l == sc.first ? bu0 : L.bu;
-    const double* bv = l == sc.first ? bv0 : L.bv;
+    const Dims& g = L.o.d;
+    const int P = g.nx * g.ny;
+    double* a = sm + L.soff;
+    for (int t = threadIdx.x; t < P; t += blockDim.x) {
+      const long long q = g.at(t % g.ny, t / g.ny);
+      a[SA_NA * P + t] = L.o.Na[q];
+      a[SA_NB * P + t] = L.o.Nb[q];
+      a[SA_BX * P + t] = L.o.Bx[q];
+      a[SA_BY * P + t] = L.o.By[q];
+      a[SA_IDU * P + t] = L.idu[q];
+      a[SA_IDV * P + t] = L.idv[q];
+      if (l == sc.first) {
+        a[SA_XU * P + t] = xu0[q];
+        a[SA_XV * P + t] = xv0[q];
+        a[SA_BU * P + t] = bu0[q];
+        a[SA_BV * P + t] = bv0[q];
+      }
+    }
+  }
+  __syncthreads();
+  auto arr = [&](int l, int k) { return sm + sc.L[l].soff + k * (sc.L[l].o.d.nx * sc.L[l].o.d.ny); };
+  // descend
+  for (int l = sc.first; l <= sc.last; ++l) {
+    const Op& o = so[l];
+    double *xu = arr(l, SA_XU), *xv = arr(l, SA_XV), *bu = arr(l, SA_BU), *bv = arr(l, SA_BV);
+    const double *idu = arr(l, SA_IDU), *idv = arr(l, SA_IDV);
     if (l == sc.last) {
       if (sc.direct && *sc.singular == 0) {
-        block_coarse_direct(L.o, sc.map, sc.Ainv, xu, xv, bu, bv);
+        block_coarse_direct(o, sc.map, sc.Ainv, xu, xv, bu, bv);
         __syncthreads();
       } else {
-        block_coarse_relax(L.o, xu, xv, bu, bv, L.idu, L.idv, sc.coarse_sweeps);
+        block_coarse_relax(o, xu, xv, bu, bv, idu, idv, sc.coarse_sweeps);
       }
       break;
     }
     for (int s = 0; s < sc.nu1; ++s)
       for (int p = 0; p < 4; ++p) {
-        block_gs_pass(L.o, xu, xv, bu, bv, L.idu, L.idv, p >> 1, p & 1);
+        block_gs_pass(o, xu, xv, bu, bv, idu, idv, p >> 1, p & 1);
         __syncthreads();
       }
-    block_for_points(L.o.d, [&](int j, int i) { residual_point(L.o, xu, xv, bu, bv, L.ru, L.rv, j, i); });
+    double *ru = arr(l, SA_RU), *rv = arr(l, SA_RV);
+    block_for_points(o.d, [&](int j, int i) { residual_point(o, xu, xv, bu, bv, ru, rv, j, i); });
     __syncthreads();
-    const SubLevel& K = sc.L[l + 1];
-    block_for_points(K.o.d, [&](int j, int i) {
-      restrict_point(L.o.d, K.o.d, L.fx, L.fy, L.ru, L.rv, K.bu, K.bv, K.xu, K.xv, j, i);
+    const Op& k = so[l + 1];
+    double *kxu = arr(l + 1, SA_XU), *kxv = arr(l + 1, SA_XV), *kbu = arr(l + 1, SA_BU), *kbv = arr(l + 1, SA_BV);
+    const int fx = sc.L[l].fx, fy = sc.L[l].fy;
+    block_for_points(k.d, [&](int j, int i) {
+      restrict_point(o.d, k.d, fx, fy, ru, rv, kbu, kbv, kxu, kxv, j, i);
     });
     __syncthreads();
   }
   // ascend
   for (int l = sc.last - 1; l >= sc.first; --l) {
-    const SubLevel& L = sc.L[l];
-    const SubLevel& K = sc.L[l + 1];
-    double* xu = l == sc.first ? xu0 : L.xu;
-    double* xv = l == sc.first ? xv0 : L.xv;
-    const double* bu = l == sc.first ? bu0 : L.bu;
-    const double* bv = l == sc.first ? bv0 : L.bv;
-    block_for_points(L.o.d, [&](int j, int i) { prolong_point(K.o, L.o.d, L.fx, L.fy, K.xu, K.xv, xu, xv, j, i); });
+    const Op& o = so[l];
+    const Op& k = so[l + 1];
+    double *xu = arr(l, SA_XU), *xv = arr(l, SA_XV), *bu = arr(l, SA_BU), *bv = arr(l, SA_BV);
+    const double *idu = arr(l, SA_IDU), *idv = arr(l, SA_IDV);
+    const double *kxu = arr(l + 1, SA_XU), *kxv = arr(l + 1, SA_XV);
+    const int fx = sc.L[l].fx, fy = sc.L[l].fy;
+    block_for_points(o.d, [&](int j, int i) { prolong_point(k, o.d, fx, fy, kxu, kxv, xu, xv, j, i); });
     __syncthreads();
     for (int s = 0; s < sc.nu2; ++s)
       for (int p = 3; p >= 0; --p) {
-        block_gs_pass(L.o, xu, xv, bu, bv, L.idu, L.idv, p >> 1, p & 1);
+        block_gs_pass(o, xu, xv, bu, bv, idu, idv, p >> 1, p & 1);
         __syncthreads();
       }
+  }
+  {
+    const Dims& g = sc.L[sc.first].o.d;
+    const int P = g.nx * g.ny;
+    const double *xu = arr(sc.first, SA_XU), *xv = arr(sc.first, SA_XV);
+    for (int t = threadIdx.x; t < P; t += blockDim.x) {
+      const long long q = g.at(t % g.ny, t / g.ny);
+      xu0[q] = xu[t];
+      xv0[q] = xv[t];
+    }
   }
 }
 
@@ -1005,13 +1239,78 @@ static int gs_sweep(Ctx* c, int l, double* xu, double* xv, const double* bu, con
   return DIVA_OK;
 }
 
-// levels with at most this many points are handled by one k_subcycle block
-constexpr long long kSubMaxPoints = 4096;
+// shared memory the sub-cycle needs from level l down
+static size_t sub_bytes(const Ctx* c, int l) {
+  size_t b = 0;
+  for (int q = l; q < c->nlev; ++q) b += (size_t)kSubArrays * c->lv[q].d.nx * c->lv[q].d.ny * sizeof(double);
+  return b;
+}
 
+// first level of the one-block sub-cycle: the largest whose levels all fit in shared memory
 static int sub_first_level(const Ctx* c) {
   for (int l = 0; l < c->nlev; ++l)
-    if ((long long)c->lv[l].d.nx * c->lv[l].d.ny <= kSubMaxPoints) return l;
+    if (sub_bytes(c, l) <= kSubSmemBudget) return l;
   return c->nlev - 1;
+}
+
+static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv);
+
+// tile edge of level l's smoothing kernels: 32 x 32 while that still fills the GPU, else 16 x 16
+static int tile_edge(const Ctx* c, int l) {
+  const Dims& d = c->lv[l].d;
+  const long long b32 = (long long)((d.ny + 31) / 32) * ((d.nx + 31) / 32);
+  return b32 >= 148 ? 32 : 16;
+}
+
+template <int T>
+static int vcycle_tiled_t(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv, int nu1,
+                          int nu2) {
+  using G = TileGeom<T, T>;
+  const Level& L = c->lv[l];
+  const Level& K = c->lv[l + 1];
+  const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
+  const Op o = make_op(c, l);
+  k_smooth_down<T, T><<<grid, kTileThreads, G::smem, c->stream>>>(o, bu, bv, xu, xv, L.ru, L.rv, L.idu, L.idv,
+                                                                   nu1); c->launches++;
+  DIVA_LAUNCHED(c, "k_smooth_down");
+  int fx, fy;
+  factors(c, l, &fx, &fy);
+  k_restrict<<<GL(l + 1)>>>(L.d, K.d, fx, fy, L.ru, L.rv, K.bu, K.bv, K.xu, K.xv); c->launches++;
+  DIVA_LAUNCHED(c, "k_restrict");
+  int st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv);
+  if (st) return st;
+  k_smooth_up<T, T><<<grid, kTileThreads, G::smem, c->stream>>>(o, make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv,
+                                                                 xu, xv, L.idu, L.idv, nu2); c->launches++;
+  DIVA_LAUNCHED(c, "k_smooth_up");
+  c->fine_passes += (nu1 + nu2 + 1) * (double)L.d.plane / (double)c->d.plane;
+  return DIVA_OK;
+}
+
+// V-cycle step of a tiled level: 2 launches for the smoothing and the residual instead of 4 per sweep
+static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv, int nu1,
+                        int nu2) {
+  if (4 * nu1 > kHalo - 1 || 4 * nu2 > kHalo - 1) return set_error(c, DIVA_UNSUPPORTED, "tiled smoothing depth");
+  return tile_edge(c, l) == 32 ? vcycle_tiled_t<32>(c, l, xu, xv, bu, bv, nu1, nu2)
+                               : vcycle_tiled_t<16>(c, l, xu, xv, bu, bv, nu1, nu2);
+}
+
+// Shared-memory limits of the tiled kernels (the 32 x 32 tiles need 80 KB) and of
+// the sub-cycle, and whether the grid's boundary conditions allow tiles at all.
+int solver_init(Ctx* c) {
+  if (sub_bytes(c, c->nlev - 1) > kSubSmemBudget)
+    return set_error(c, DIVA_UNSUPPORTED, "coarsest multigrid level too large for the one-block sub-cycle");
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kSubSmemBudget));
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TileGeom<32, 32>::smem));
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_up<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TileGeom<32, 32>::smem));
+  const BCs& b = c->bc;
+  const int all[8] = {b.uW, b.uE, b.uS, b.uN, b.vW, b.vE, b.vS, b.vN};
+  bool periodic = false;
+  for (int q = 0; q < 8; ++q) periodic = periodic || all[q] == DIVA_BC_PERIODIC;
+  c->tiled = !periodic && !c->tiles_disabled;
+  return DIVA_OK;
 }
 
 static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv) {
@@ -1027,16 +1326,18 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
     sc.map = coarse_map(c);
     sc.Ainv = c->coarse_inv;
     sc.singular = c->coarse_singular;
+    int soff = 0;
     for (int q = l; q < c->nlev; ++q) {
       const Level& L = c->lv[q];
       SubLevel& S = sc.L[q];
       S.o = make_op(c, q);
-      S.xu = L.xu; S.xv = L.xv; S.bu = L.bu; S.bv = L.bv; S.ru = L.ru; S.rv = L.rv;
       S.idu = L.idu; S.idv = L.idv;
       S.fx = 1; S.fy = 1;
       if (q + 1 < c->nlev) factors(c, q, &S.fx, &S.fy);
+      S.soff = soff;
+      soff += kSubArrays * L.d.nx * L.d.ny;
     }
-    k_subcycle<<<1, kSubThreads, 0, c->stream>>>(sc, xu, xv, bu, bv); c->launches++;
+    k_subcycle<<<1, kSubThreads, sub_bytes(c, l), c->stream>>>(sc, xu, xv, bu, bv); c->launches++;
     DIVA_LAUNCHED(c, "k_subcycle");
     for (int q = l; q < c->nlev; ++q) c->fine_passes += 8.0 * (double)c->lv[q].d.plane / (double)c->d.plane;
     return DIVA_OK;
@@ -1050,6 +1351,7 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
   int st;
+  if (c->tiled) return vcycle_tiled(c, l, xu, xv, bu, bv, nu1, nu2);
   for (int s = 0; s < nu1; ++s)
     if ((st = gs_sweep(c, l, xu, xv, bu, bv, true))) return st;
   k_residual<<<GL(l)>>>(make_op(c, l), xu, xv, bu, bv, L.ru, L.rv); c->launches++;
@@ -1267,12 +1569,6 @@ int add_conditional(Ctx* c, cudaStream_t s, cudaGraphConditionalHandle h, cudaGr
   DIVA_CUDA(c, cudaGraphAddNode(&node, g, deps, nd, &p));
   *body = p.conditional.phGraph_out[0];
   DIVA_CUDA(c, cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
-  return DIVA_OK;
-}
-
-int capture_graph_of(Ctx* c, cudaStream_t s, cudaGraph_t* g) {
-  cudaStreamCaptureStatus st;
-  DIVA_CUDA(c, cudaStreamGetCaptureInfo(s, &st, nullptr, g, nullptr, nullptr));
   return DIVA_OK;
 }
 
