@@ -683,11 +683,12 @@ int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, 
   *ms = t / reps;
   // algorithmic bytes per launch (compulsory traffic per column, FP64):
   //  0: read A-factor and the previous viscosity, write the new one (3 nz) + 15 2D fields
-  //  1: one sweep over both colours: u, v, N_a, N_b, beta_x, beta_y, b_u, b_v read, u, v written (10)
+  //  1: fine-level smoothing of one V-cycle: the tiled pre- and post-smoothing kernels (24 values,
+  //     solver_smooth_fine_values), or one per-colour sweep on untiled grids (10)
   //  2: operator application: u, v, N_a, N_b, beta_x, beta_y read, A u, A v written (8)
   //  3: one V-cycle: per level 4 sweeps, a residual and the transfers, weighted by its points
   //  4: the one-block coarse levels of a V-cycle (latency-bound; bytes as for 3 over those levels)
-  const double per_col[3] = {(3 * nz + 15) * w, 10 * w, 8 * w};
+  const double per_col[3] = {(3 * nz + 15) * w, solver_smooth_fine_values(c) * w, 8 * w};
   *bytes = which < 3 ? per_col[which] * nc : (which == 3 ? solver_vcycle_bytes(c) : 0.0);
   return DIVA_OK;
 }

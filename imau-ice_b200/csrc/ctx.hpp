@@ -145,6 +145,7 @@ int solver_solve(Ctx* c, const double* u0, const double* v0, double rtol, int ma
 int solver_relres(Ctx* c, const double* u, const double* v, double* relres);
 int solver_fill_boundary(Ctx* c, double* u, double* v);
 int solver_smooth_fine(Ctx* c, int sweeps);
+int solver_smooth_fine_values(const Ctx* c);
 int solver_matvec_fine(Ctx* c, int reps);
 int solver_vcycle_fine(Ctx* c, int reps);
 int solver_subcycle(Ctx* c, int reps);

@@ -20,6 +20,7 @@
 // One thread owns one a-grid column (j,i) and, with it, the cx face (j,i) east
 // of it and the cy face (j,i) north of it.  Column loops run over the zeta
 // layers, each a coalesced plane.
+#include <algorithm>
 #include <cmath>
 #include <math_constants.h>
 #include "ctx.hpp"
@@ -80,22 +81,6 @@ __device__ __forceinline__ double ddx_cy_to_a(const Dims& d, const double* v, in
   return (V(jc, nx - 1) - V(jc, nx - 2)) / dx;
 }
 
-// du/dz on the cx face (j,f) (calc_vertical_shear_strain_rates :685-695)
-__device__ __forceinline__ double dudz_face(const CoefArgs& a, int j, int f, int k, long long off) {
-  const Dims& d = a.d;
-  const long long q0 = d.at(j, f), q1 = d.at(j, f + 1);
-  if (a.mask_ice[q0] == 0 && a.mask_ice[q1] == 0) return 0.0;
-  const double vc = stag_margin(a.visc_prev[off + q0], a.visc_prev[off + q1], a.Hi[q0], a.Hi[q1]);
-  return (a.taub_cx[q0] / vc) * a.zt.z[k];
-}
-__device__ __forceinline__ double dvdz_face(const CoefArgs& a, int g, int i, int k, long long off) {
-  const Dims& d = a.d;
-  const long long q0 = d.at(g, i), q1 = d.at(g + 1, i);
-  if (a.mask_ice[q0] == 0 && a.mask_ice[q1] == 0) return 0.0;
-  const double vc = stag_margin(a.visc_prev[off + q0], a.visc_prev[off + q1], a.Hi[q0], a.Hi[q1]);
-  return (a.taub_cy[q0] / vc) * a.zt.z[k];
-}
-
 __device__ __forceinline__ double sliding_beta(const CoefArgs& a, long long q, double ua, double va) {
   const double uabs = sqrt(a.delta_v * a.delta_v + ua * ua + va * va);
   switch (a.sliding) {
@@ -125,69 +110,124 @@ __device__ __forceinline__ double sliding_beta(const CoefArgs& a, long long q, d
   return CUDART_NAN;
 }
 
-__global__ void __launch_bounds__(256) k_column_coefficients(CoefArgs a) {
+// Layer-parallel: a block covers 32 columns of one grid column i (lane = j) and
+// every layer (threadIdx.y = k, strided when nz > 32), so each warp streams one
+// zeta layer of 32 neighbouring columns.  The threads of layer 0 first evaluate
+// the column's 2D quantities once (strain rates of the mean flow, the inputs of
+// its four shear faces) and pass them through shared memory.  Each thread then
+// computes its column's own east and north shear faces in its layer; the north
+// face of the lane below is the south face of this lane (shuffle), only the west
+// face is recomputed.  The column integrals are summed in layer order by the
+// threads of layer 0, exactly as the sequential quadrature does.
+constexpr int kColLanes = 32;
+enum { FACE_E, FACE_W, FACE_N, FACE_S };
+
+__global__ void __launch_bounds__(1024) k_column_coefficients(CoefArgs a) {
+  __shared__ double s_eta[kMaxNz][kColLanes];
+  __shared__ double s_f[kMaxNz][kColLanes];
+  __shared__ double s_eps[kColLanes];
+  __shared__ double s_H0[4][kColLanes], s_H1[4][kColLanes], s_tb[4][kColLanes];
+  __shared__ int s_act[4][kColLanes];
   const Dims d = a.d;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
-  if (j >= d.ny || i >= d.nx) return;
+  const int lane = threadIdx.x;
+  const int j = blockIdx.x * kColLanes + lane, i = blockIdx.y;
+  const bool col = j < d.ny;   // lanes past the last row stay for the shuffles
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const long long q = d.at(j, i);
-  const double H = a.Hi[q];
-  const bool ice = a.mask_ice[q] == 1;
-  // strain rates of the depth-averaged flow (calc_effective_viscosity :751-754)
-  const double du_dx = ddx_cx_to_a(d, a.u, j, i), dv_dy = ddy_cy_to_a(d, a.v, j, i);
-  const double du_dy = ddy_cx_to_a(d, a.u, j, i), dv_dx = ddx_cy_to_a(d, a.v, j, i);
-  const double eps_h = du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((du_dy + dv_dx) * (du_dy + dv_dx));
+  const long long q = d.at(col ? j : ny - 1, i);
+  const int* __restrict__ mask = a.mask_ice;
+  const double* __restrict__ Hi = a.Hi;
+  const double* __restrict__ vp = a.visc_prev;
+  const double* __restrict__ afac = a.afac;
+  double* __restrict__ visc = a.visc;
+  double* __restrict__ dudz = a.dudz;
+  double* __restrict__ dvdz = a.dvdz;
+  const double H = Hi[q];
+  const bool ice = mask[q] == 1;
   const bool skip_visc = a.bc_margin && !ice;  // BC margins: no viscosity outside the ice (:759-764)
-  double vint = 0.0, fint = 0.0, vprev = 0.0, fprev = 0.0;
-  for (int k = 0; k < nz; ++k) {
-    const long long off = (long long)k * d.plane;
-    double dudz_e = 0.0, dvdz_n = 0.0;
-    if (a.diva) {
-      // own faces (written), then the faces west/south of the column
-      if (i < nx - 1) {
-        dudz_e = dudz_face(a, j, i, k, off);
-        a.dudz[off + q] = dudz_e;
-      }
-      if (j < ny - 1) {
-        dvdz_n = dvdz_face(a, j, i, k, off);
-        a.dvdz[off + q] = dvdz_n;
-      }
+  // the faces of the column (calc_vertical_shear_strain_rates :685-721); a column on
+  // the last row/column uses the face before it alone
+  const bool has_e = col && i < nx - 1, has_w = col && i > 0, has_n = col && j < ny - 1, has_s = col && j > 0;
+  const long long qe = has_e ? d.at(j, i + 1) : q, qw = has_w ? d.at(j, i - 1) : q;
+  const long long qn = has_n ? d.at(j + 1, i) : q, qs = has_s ? d.at(j - 1, i) : q;
+  if (threadIdx.y == 0) {
+    // strain rates of the depth-averaged flow (calc_effective_viscosity :751-754)
+    double eps_h = 0.0;
+    if (col && !skip_visc) {
+      const double du_dx = ddx_cx_to_a(d, a.u, j, i), dv_dy = ddy_cy_to_a(d, a.v, j, i);
+      const double du_dy = ddy_cx_to_a(d, a.u, j, i), dv_dx = ddx_cy_to_a(d, a.v, j, i);
+      eps_h = du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((du_dy + dv_dx) * (du_dy + dv_dx));
     }
-    double eta;
-    if (skip_visc) {
-      eta = 0.0;
-    } else {
+    s_eps[lane] = eps_h;
+    // face f joins p0 and p1; it has ice if either side has (:685-695)
+    const bool has[4] = {has_e, has_w, has_n, has_s};
+    const long long p0[4] = {q, qw, q, qs}, p1[4] = {qe, q, qn, q};
+    for (int f = 0; f < 4; ++f) {
+      const bool on = a.diva && has[f];
+      s_act[f][lane] = on && !(mask[p0[f]] == 0 && mask[p1[f]] == 0);
+      s_H0[f][lane] = on ? Hi[p0[f]] : 0.0;
+      s_H1[f][lane] = on ? Hi[p1[f]] : 0.0;
+      s_tb[f][lane] = on ? (f < 2 ? a.taub_cx : a.taub_cy)[p0[f]] : 0.0;
+    }
+  }
+  __syncthreads();
+  const double eps_h = s_eps[lane];
+  const double Hw = has_w ? Hi[qw] : 0.0, Hs = has_s ? Hi[qs] : 0.0;
+  // du/dz on face f in layer k: (taub / staggered viscosity) * zeta (:685-695)
+  auto face_dz = [&](int f, long long p0, long long p1, long long off, double zk) {
+    if (!s_act[f][lane]) return 0.0;
+    const double vc = stag_margin(vp[off + p0], vp[off + p1], s_H0[f][lane], s_H1[f][lane]);
+    return (s_tb[f][lane] / vc) * zk;
+  };
+  for (int k = threadIdx.y; k < nz; k += blockDim.y) {
+    const long long off = (long long)k * d.plane;
+    const double zk = a.zt.z[k];
+    double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0;
+    if (a.diva) {
+      if (has_e) {
+        dudz_e = face_dz(FACE_E, q, qe, off, zk);
+        dudz[off + q] = dudz_e;
+      }
+      if (has_n) {
+        dvdz_n = face_dz(FACE_N, q, qn, off, zk);
+        dvdz[off + q] = dvdz_n;
+      }
+      dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
+      if (lane == 0 && has_s) dvdz_s = face_dz(FACE_S, qs, q, off, zk);
+    }
+    double eta = 0.0;
+    if (col && !skip_visc) {
       double du_dz_a = 0.0, dv_dz_a = 0.0;
       if (a.diva) {
         if (i == 0) du_dz_a = dudz_e;
-        else if (i == nx - 1) du_dz_a = dudz_face(a, j, nx - 2, k, off);
-        else du_dz_a = stag_margin(dudz_face(a, j, i - 1, k, off), dudz_e, a.Hi[d.at(j, i - 1)], H);
+        else if (i == nx - 1) du_dz_a = face_dz(FACE_W, qw, q, off, zk);
+        else du_dz_a = stag_margin(face_dz(FACE_W, qw, q, off, zk), dudz_e, Hw, H);
         if (j == 0) dv_dz_a = dvdz_n;
-        else if (j == ny - 1) dv_dz_a = dvdz_face(a, ny - 2, i, k, off);
-        else dv_dz_a = stag_margin(dvdz_face(a, j - 1, i, k, off), dvdz_n, a.Hi[d.at(j - 1, i)], H);
+        else if (j == ny - 1) dv_dz_a = dvdz_s;
+        else dv_dz_a = stag_margin(dvdz_s, dvdz_n, Hs, H);
       } else {
         // solve_SSA calls calc_effective_viscosity without refreshing du/dz: use the stored fields
-        const double* dz_u = a.dudz;
-        const double* dz_v = a.dvdz;
-        if (i == 0) du_dz_a = dz_u[off + d.at(j, 0)];
-        else if (i == nx - 1) du_dz_a = dz_u[off + d.at(j, nx - 2)];
-        else du_dz_a = stag_margin(dz_u[off + d.at(j, i - 1)], dz_u[off + q], a.Hi[d.at(j, i - 1)], H);
-        if (j == 0) dv_dz_a = dz_v[off + d.at(0, i)];
-        else if (j == ny - 1) dv_dz_a = dz_v[off + d.at(ny - 2, i)];
-        else dv_dz_a = stag_margin(dz_v[off + d.at(j - 1, i)], dz_v[off + q], a.Hi[d.at(j - 1, i)], H);
+        if (i == 0) du_dz_a = dudz[off + d.at(j, 0)];
+        else if (i == nx - 1) du_dz_a = dudz[off + d.at(j, nx - 2)];
+        else du_dz_a = stag_margin(dudz[off + qw], dudz[off + q], Hw, H);
+        if (j == 0) dv_dz_a = dvdz[off + d.at(0, i)];
+        else if (j == ny - 1) dv_dz_a = dvdz[off + d.at(ny - 2, i)];
+        else dv_dz_a = stag_margin(dvdz[off + qs], dvdz[off + q], Hs, H);
       }
       const double eps_sq = eps_h + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
       const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
-      eta = max_ref(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
+      eta = max_ref(afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
     }
-    a.visc[off + q] = eta;
-    if (k > 0) vint = vint + 0.5 * (eta + vprev) * (a.zt.z[k] - a.zt.z[k - 1]);
-    vprev = eta;
-    if (a.diva) {
-      const double fk = (H / eta) * a.zt.z2[k];
-      if (k > 0) fint = fint + 0.5 * (fk + fprev) * (a.zt.z[k] - a.zt.z[k - 1]);
-      fprev = fk;
-    }
+    if (col) visc[off + q] = eta;
+    s_eta[k][lane] = eta;
+    if (a.diva) s_f[k][lane] = (H / eta) * a.zt.z2[k];
+  }
+  __syncthreads();
+  if (threadIdx.y != 0 || !col) return;
+  double vint = 0.0, fint = 0.0;
+  for (int k = 1; k < nz; ++k) {
+    const double dz = a.zt.z[k] - a.zt.z[k - 1];
+    vint = vint + 0.5 * (s_eta[k][lane] + s_eta[k - 1][lane]) * dz;
+    if (a.diva) fint = fint + 0.5 * (s_f[k][lane] + s_f[k - 1][lane]) * dz;
   }
   if (!skip_visc) {
     a.visc_int[q] = vint;
@@ -795,7 +835,10 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
     DIVA_CUDA(c, cudaMemcpyAsync(c->D(DIVA_F_VISC_EFF_3D_A), c->visc_prev, sizeof(double) * c->d.plane * c->d.nz,
                                  cudaMemcpyDeviceToDevice, c->stream));
   }
-  k_column_coefficients<<<G2>>>(a); c->launches++;
+  {
+    const dim3 block(kColLanes, std::min(c->d.nz, 32)), grid((c->d.ny + kColLanes - 1) / kColLanes, c->d.nx);
+    k_column_coefficients<<<grid, block, 0, c->stream>>>(a); c->launches++;
+  }
   DIVA_LAUNCHED(c, "k_column_coefficients");
   FaceArgs fa{};
   fa.d = c->d;

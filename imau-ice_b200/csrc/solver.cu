@@ -298,10 +298,9 @@ __device__ __forceinline__ int scatter_node(int f, int f2, int* C, double* w) {
 }
 
 // b_c = P^T r_f on coarse interior points; x_c = 0
-__device__ __forceinline__ void restrict_point(const Dims& df, const Dims& dc, int fx, int fy, const double* ru,
-                                               const double* rv, double* bu, double* bv, double* xu, double* xv,
-                                               int j, int i) {
-  const long long q = dc.at(j, i);
+// (P^T r_f) at the coarse point (j,i): the restricted u and v residuals (zero off the coarse interior)
+__device__ __forceinline__ void restrict_values(const Dims& df, const Dims& dc, int fx, int fy, const double* ru,
+                                                const double* rv, int j, int i, double& bu, double& bv) {
   int fi[4], fj[4];
   double wi[4], wj[4];
   double s = 0.0;
@@ -311,7 +310,7 @@ __device__ __forceinline__ void restrict_point(const Dims& df, const Dims& dc, i
       for (int b = 0; b < ni; ++b)
         if (u_int(df, fj[a], fi[b])) s += wj[a] * wi[b] * ru[df.at(fj[a], fi[b])];
   }
-  bu[q] = s;
+  bu = s;
   s = 0.0;
   if (v_int(dc, j, i)) {
     const int ni = gather_node(i, fx, fi, wi), nj = gather_cell(j, fy, fj, wj);
@@ -319,7 +318,14 @@ __device__ __forceinline__ void restrict_point(const Dims& df, const Dims& dc, i
       for (int b = 0; b < ni; ++b)
         if (v_int(df, fj[a], fi[b])) s += wj[a] * wi[b] * rv[df.at(fj[a], fi[b])];
   }
-  bv[q] = s;
+  bv = s;
+}
+// b_c = P^T r_f on coarse interior points; x_c = 0
+__device__ __forceinline__ void restrict_point(const Dims& df, const Dims& dc, int fx, int fy, const double* ru,
+                                               const double* rv, double* bu, double* bv, double* xu, double* xv,
+                                               int j, int i) {
+  const long long q = dc.at(j, i);
+  restrict_values(df, dc, fx, fy, ru, rv, j, i, bu[q], bv[q]);
   xu[q] = 0.0;
   xv[q] = 0.0;
 }
@@ -426,9 +432,19 @@ __device__ __forceinline__ void tile_pass(const Op& o, const TIx& ix, double* xu
   }
 }
 
-// pre-smoothing: `sweeps` forward sweeps (u0 u1 v0 v1) from x, then x and r = b - A x of the tile
+// Source of b for a pre-smoothing kernel: given on the level (the finest), or the
+// restriction of the finer level's residual, computed where it is needed.
+struct Restriction {
+  int on;              // 0: b given in gbu/gbv
+  Dims df;             // finer level
+  int fx, fy;          // coarsening factors from it
+  const double *ru, *rv;
+};
+
+// pre-smoothing from x = 0 (the descent of a V-cycle enters every level with x = 0):
+// `sweeps` forward sweeps (u0 u1 v0 v1), then x, b and r = b - A x of the tile
 template <int TJ, int TI>
-__global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, const double* gbu, const double* gbv,
+__global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction rs, double* gbu, double* gbv,
                                                               double* gxu, double* gxv, double* gru, double* grv,
                                                               const double* idu, const double* idv, int sweeps) {
   using G = TileGeom<TJ, TI>;
@@ -440,11 +456,20 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, const double
   for (int t = threadIdx.x; t < G::N; t += blockDim.x) {
     const int j = ix.j0 + t % G::RJ, i = ix.i0 + t / G::RJ;
     const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
-    const long long q = in ? d.at(j, i) : 0;
-    xu[t] = in ? gxu[q] : 0.0;
-    xv[t] = in ? gxv[q] : 0.0;
-    bu[t] = in ? gbu[q] : 0.0;
-    bv[t] = in ? gbv[q] : 0.0;
+    double b0 = 0.0, b1 = 0.0;
+    if (in) {
+      if (rs.on) {
+        restrict_values(rs.df, d, rs.fx, rs.fy, rs.ru, rs.rv, j, i, b0, b1);
+      } else {
+        const long long q = d.at(j, i);
+        b0 = gbu[q];
+        b1 = gbv[q];
+      }
+    }
+    xu[t] = 0.0;
+    xv[t] = 0.0;
+    bu[t] = b0;
+    bv[t] = b1;
   }
   __syncthreads();
   int pass = 0;
@@ -460,6 +485,10 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, const double
     const int k = ix(j, i);
     gxu[q] = xu[k];
     gxv[q] = xv[k];
+    if (rs.on) {
+      gbu[q] = bu[k];
+      gbv[q] = bv[k];
+    }
     gru[q] = u_int(d, j, i) ? bu[k] - AuX<false>(o, xu, xv, ix, j, i) : 0.0;
     grv[q] = v_int(d, j, i) ? bv[k] - AvX<false>(o, xu, xv, ix, j, i) : 0.0;
   }
@@ -671,6 +700,7 @@ struct SubCycle {
   CoarseMap map;
   const double* Ainv;
   const int* singular;
+  Restriction rs;              // b of the first level: given, or restricted from the finer residual
   SubLevel L[kMaxLevels];
 };
 
@@ -710,11 +740,18 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
       a[SA_BY * P + t] = L.o.By[q];
       a[SA_IDU * P + t] = L.idu[q];
       a[SA_IDV * P + t] = L.idv[q];
-      if (l == sc.first) {
-        a[SA_XU * P + t] = xu0[q];
-        a[SA_XV * P + t] = xv0[q];
-        a[SA_BU * P + t] = bu0[q];
-        a[SA_BV * P + t] = bv0[q];
+      if (l == sc.first) {   // entered with x = 0
+        double b0, b1;
+        if (sc.rs.on) {
+          restrict_values(sc.rs.df, g, sc.rs.fx, sc.rs.fy, sc.rs.ru, sc.rs.rv, t % g.ny, t / g.ny, b0, b1);
+        } else {
+          b0 = bu0[q];
+          b1 = bv0[q];
+        }
+        a[SA_XU * P + t] = 0.0;
+        a[SA_XV * P + t] = 0.0;
+        a[SA_BU * P + t] = b0;
+        a[SA_BV * P + t] = b1;
       }
     }
   }
@@ -1253,7 +1290,8 @@ static int sub_first_level(const Ctx* c) {
   return c->nlev - 1;
 }
 
-static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv);
+static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
+                  const Restriction& rs);
 
 // tile edge of level l's smoothing kernels: 32 x 32 while that still fills the GPU, else 16 x 16
 static int tile_edge(const Ctx* c, int l) {
@@ -1263,35 +1301,40 @@ static int tile_edge(const Ctx* c, int l) {
 }
 
 template <int T>
-static int vcycle_tiled_t(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv, int nu1,
-                          int nu2) {
+static int vcycle_tiled_t(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
+                          const Restriction& rs, int nu1, int nu2) {
   using G = TileGeom<T, T>;
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
   const Op o = make_op(c, l);
-  k_smooth_down<T, T><<<grid, kTileThreads, G::smem, c->stream>>>(o, bu, bv, xu, xv, L.ru, L.rv, L.idu, L.idv,
-                                                                   nu1); c->launches++;
+  // b is written only when it is restricted here (rs.on), which never happens on the finest level
+  k_smooth_down<T, T><<<grid, kTileThreads, G::smem, c->stream>>>(o, rs, const_cast<double*>(bu),
+                                                                   const_cast<double*>(bv), xu, xv, L.ru, L.rv,
+                                                                   L.idu, L.idv, nu1); c->launches++;
   DIVA_LAUNCHED(c, "k_smooth_down");
-  int fx, fy;
-  factors(c, l, &fx, &fy);
-  k_restrict<<<GL(l + 1)>>>(L.d, K.d, fx, fy, L.ru, L.rv, K.bu, K.bv, K.xu, K.xv); c->launches++;
-  DIVA_LAUNCHED(c, "k_restrict");
-  int st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv);
+  Restriction next;
+  next.on = 1;
+  next.df = L.d;
+  factors(c, l, &next.fx, &next.fy);
+  next.ru = L.ru;
+  next.rv = L.rv;
+  int st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv, next);
   if (st) return st;
-  k_smooth_up<T, T><<<grid, kTileThreads, G::smem, c->stream>>>(o, make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv,
-                                                                 xu, xv, L.idu, L.idv, nu2); c->launches++;
+  k_smooth_up<T, T><<<grid, kTileThreads, G::smem, c->stream>>>(o, make_op(c, l + 1), next.fx, next.fy, K.xu,
+                                                                 K.xv, bu, bv, xu, xv, L.idu, L.idv, nu2); c->launches++;
   DIVA_LAUNCHED(c, "k_smooth_up");
   c->fine_passes += (nu1 + nu2 + 1) * (double)L.d.plane / (double)c->d.plane;
   return DIVA_OK;
 }
 
-// V-cycle step of a tiled level: 2 launches for the smoothing and the residual instead of 4 per sweep
-static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv, int nu1,
-                        int nu2) {
+// V-cycle step of a tiled level: 2 launches for the smoothing, the residual and the
+// restriction instead of 4 per sweep and 2 more
+static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
+                        const Restriction& rs, int nu1, int nu2) {
   if (4 * nu1 > kHalo - 1 || 4 * nu2 > kHalo - 1) return set_error(c, DIVA_UNSUPPORTED, "tiled smoothing depth");
-  return tile_edge(c, l) == 32 ? vcycle_tiled_t<32>(c, l, xu, xv, bu, bv, nu1, nu2)
-                               : vcycle_tiled_t<16>(c, l, xu, xv, bu, bv, nu1, nu2);
+  return tile_edge(c, l) == 32 ? vcycle_tiled_t<32>(c, l, xu, xv, bu, bv, rs, nu1, nu2)
+                               : vcycle_tiled_t<16>(c, l, xu, xv, bu, bv, rs, nu1, nu2);
 }
 
 // Shared-memory limits of the tiled kernels (the 32 x 32 tiles need 80 KB) and of
@@ -1313,7 +1356,10 @@ int solver_init(Ctx* c) {
   return DIVA_OK;
 }
 
-static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv) {
+// One V-cycle from level l down, entered with x = 0.  b is given in bu/bv, or (rs.on)
+// restricted from the finer level's residual by the level's first kernel.
+static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
+                  const Restriction& rs) {
   const int nu1 = 2, nu2 = 2, coarse_sweeps = 64;
   if (l == sub_first_level(c)) {
     SubCycle sc;
@@ -1337,6 +1383,7 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
       S.soff = soff;
       soff += kSubArrays * L.d.nx * L.d.ny;
     }
+    sc.rs = rs;
     k_subcycle<<<1, kSubThreads, sub_bytes(c, l), c->stream>>>(sc, xu, xv, bu, bv); c->launches++;
     DIVA_LAUNCHED(c, "k_subcycle");
     for (int q = l; q < c->nlev; ++q) c->fine_passes += 8.0 * (double)c->lv[q].d.plane / (double)c->d.plane;
@@ -1351,7 +1398,7 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
   int st;
-  if (c->tiled) return vcycle_tiled(c, l, xu, xv, bu, bv, nu1, nu2);
+  if (c->tiled) return vcycle_tiled(c, l, xu, xv, bu, bv, rs, nu1, nu2);
   for (int s = 0; s < nu1; ++s)
     if ((st = gs_sweep(c, l, xu, xv, bu, bv, true))) return st;
   k_residual<<<GL(l)>>>(make_op(c, l), xu, xv, bu, bv, L.ru, L.rv); c->launches++;
@@ -1360,7 +1407,7 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
   factors(c, l, &fx, &fy);
   k_restrict<<<GL(l + 1)>>>(L.d, K.d, fx, fy, L.ru, L.rv, K.bu, K.bv, K.xu, K.xv); c->launches++;
   DIVA_LAUNCHED(c, "k_restrict");
-  if ((st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv))) return st;
+  if ((st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv, Restriction{}))) return st;
   k_prolong<<<GL(l)>>>(make_op(c, l + 1), L.d, fx, fy, K.xu, K.xv, xu, xv); c->launches++;
   DIVA_LAUNCHED(c, "k_prolong");
   for (int s = 0; s < nu2; ++s)
@@ -1370,10 +1417,14 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
 
 // z = M^{-1} r: one V-cycle from zero
 static int precond(Ctx* c, const double* ru, const double* rv, double* zu, double* zv) {
-  DIVA_CUDA(c, cudaMemsetAsync(zu, 0, sizeof(double) * c->d.plane, c->stream));
-  DIVA_CUDA(c, cudaMemsetAsync(zv, 0, sizeof(double) * c->d.plane, c->stream));
+  // the tiled kernels and the sub-cycle start from x = 0 themselves and write every
+  // point of z; the per-colour sweeps read x
+  if (!c->tiled && sub_first_level(c) > 0) {
+    DIVA_CUDA(c, cudaMemsetAsync(zu, 0, sizeof(double) * c->d.plane, c->stream));
+    DIVA_CUDA(c, cudaMemsetAsync(zv, 0, sizeof(double) * c->d.plane, c->stream));
+  }
   c->mg_cycles++;
-  return vcycle(c, 0, zu, zv, ru, rv);
+  return vcycle(c, 0, zu, zv, ru, rv, Restriction{});
 }
 
 static int read_scalars(Ctx* c) {
@@ -1467,13 +1518,51 @@ int solver_relres(Ctx* c, const double* u, const double* v, double* relres) {
   return DIVA_OK;
 }
 
-// fine-level smoothing sweeps on the Krylov solution vector (used to time the smoother)
+// Fine-level smoothing as the V-cycle runs it (used to time the smoother): the tiled
+// pre- and post-smoothing kernels (V(2,2), residual included) when the grid is tiled,
+// else `sweeps` per-colour sweeps.  x, b and the coarse correction are the solver's
+// scratch vectors.
 int solver_smooth_fine(Ctx* c, int sweeps) {
+  if (c->tiled && c->nlev > 1 && sub_first_level(c) > 0) {
+    const Level& L = c->lv[0];
+    const Level& K = c->lv[1];
+    const int nu = 2;
+    int fx, fy;
+    factors(c, 0, &fx, &fy);
+    const Op o = make_op(c, 0);
+    double *xu = c->kv[KV_X][0], *xv = c->kv[KV_X][1];
+    double *bu = c->kv[KV_B][0], *bv = c->kv[KV_B][1];   // not written: the restriction is off
+    if (tile_edge(c, 0) == 32) {
+      using G = TileGeom<32, 32>;
+      const dim3 grid((L.d.ny + 31) / 32, (L.d.nx + 31) / 32);
+      k_smooth_down<32, 32><<<grid, kTileThreads, G::smem, c->stream>>>(o, Restriction{}, bu, bv, xu, xv, L.ru,
+                                                                         L.rv, L.idu, L.idv, nu); c->launches++;
+      k_smooth_up<32, 32><<<grid, kTileThreads, G::smem, c->stream>>>(o, make_op(c, 1), fx, fy, K.xu, K.xv, bu, bv,
+                                                                       xu, xv, L.idu, L.idv, nu); c->launches++;
+    } else {
+      using G = TileGeom<16, 16>;
+      const dim3 grid((L.d.ny + 15) / 16, (L.d.nx + 15) / 16);
+      k_smooth_down<16, 16><<<grid, kTileThreads, G::smem, c->stream>>>(o, Restriction{}, bu, bv, xu, xv, L.ru,
+                                                                         L.rv, L.idu, L.idv, nu); c->launches++;
+      k_smooth_up<16, 16><<<grid, kTileThreads, G::smem, c->stream>>>(o, make_op(c, 1), fx, fy, K.xu, K.xv, bu, bv,
+                                                                       xu, xv, L.idu, L.idv, nu); c->launches++;
+    }
+    DIVA_LAUNCHED(c, "fine-level tiled smoothing");
+    return DIVA_OK;
+  }
   for (int s = 0; s < sweeps; ++s) {
     int st = gs_sweep(c, 0, c->kv[KV_X][0], c->kv[KV_X][1], c->kv[KV_B][0], c->kv[KV_B][1], true);
     if (st) return st;
   }
   return DIVA_OK;
+}
+
+// compulsory FP64 values per fine-level point moved by one solver_smooth_fine(c, 1)
+int solver_smooth_fine_values(const Ctx* c) {
+  // tiled, per point and component pair: pre reads b_u, b_v and N_a, N_b, beta_x, beta_y
+  // and the two inverse diagonals (8) and writes x_u, x_v, r_u, r_v (4); post reads x_u,
+  // x_v, b_u, b_v and the same 6 coefficients (10) and writes x_u, x_v (2)
+  return (c->tiled && c->nlev > 1 && sub_first_level(c) > 0) ? 24 : 10;
 }
 
 int solver_matvec_fine(Ctx* c, int reps) {
@@ -1502,7 +1591,7 @@ int solver_subcycle(Ctx* c, int reps) {
   const int l = sub_first_level(c);
   const Level& L = c->lv[l];
   for (int r = 0; r < reps; ++r) {
-    int st = vcycle(c, l, L.xu, L.xv, L.bu, L.bv);
+    int st = vcycle(c, l, L.xu, L.xv, L.bu, L.bv, Restriction{});
     if (st) return st;
   }
   return DIVA_OK;
