@@ -110,27 +110,40 @@ __device__ __forceinline__ double sliding_beta(const CoefArgs& a, long long q, d
   return CUDART_NAN;
 }
 
-// Layer-parallel: a block covers 32 columns of one grid column i (lane = j) and
-// every layer (threadIdx.y = k, strided when nz > 32), so each warp streams one
-// zeta layer of 32 neighbouring columns.  The threads of layer 0 first evaluate
-// the column's 2D quantities once (strain rates of the mean flow, the inputs of
-// its four shear faces) and pass them through shared memory.  Each thread then
-// computes its column's own east and north shear faces in its layer; the north
-// face of the lane below is the south face of this lane (shuffle), only the west
-// face is recomputed.  The column integrals are summed in layer order by the
-// threads of layer 0, exactly as the sequential quadrature does.
-constexpr int kColLanes = 32;
-enum { FACE_E, FACE_W, FACE_N, FACE_S };
+// One thread per column, a warp over 32 neighbouring rows j of one grid column i.
+// The 2D inputs of the column's four shear faces are read once, before the layer
+// loop; each layer loads the previous viscosity once per point (centre, east,
+// north, west) and the A-factor, and the north face of the lane below is this
+// lane's south face (shuffle), so a layer costs three face divisions.
+constexpr int kColLanes = 32, kColRows = 4;
 
-__global__ void __launch_bounds__(1024) k_column_coefficients(CoefArgs a) {
-  __shared__ double s_eta[kMaxNz][kColLanes];
-  __shared__ double s_f[kMaxNz][kColLanes];
-  __shared__ double s_eps[kColLanes];
-  __shared__ double s_H0[4][kColLanes], s_H1[4][kColLanes], s_tb[4][kColLanes];
-  __shared__ int s_act[4][kColLanes];
+struct FaceIn {
+  bool act;        // ice on at least one side (:685-695)
+  double H0, H1;   // thickness either side, for the staggered margin viscosity
+  double tb;       // basal stress on the face
+};
+__device__ __forceinline__ FaceIn face_in(bool has, const int* __restrict__ mask, const double* __restrict__ Hi,
+                                          const double* __restrict__ taub, long long p0, long long p1) {
+  FaceIn f{false, 0.0, 0.0, 0.0};
+  if (!has) return f;
+  f.act = !(mask[p0] == 0 && mask[p1] == 0);
+  f.H0 = Hi[p0];
+  f.H1 = Hi[p1];
+  f.tb = taub[p0];
+  return f;
+}
+// du/dz on a face in one layer: (taub / staggered viscosity) * zeta
+__device__ __forceinline__ double face_dz(const FaceIn& f, double v0, double v1, double zk) {
+  if (!f.act) return 0.0;
+  const double vc = stag_margin(v0, v1, f.H0, f.H1);
+  return (f.tb / vc) * zk;
+}
+
+__global__ void __launch_bounds__(kColLanes * kColRows, 6) k_column_coefficients(CoefArgs a) {
   const Dims d = a.d;
   const int lane = threadIdx.x;
-  const int j = blockIdx.x * kColLanes + lane, i = blockIdx.y;
+  const int j = blockIdx.x * kColLanes + lane, i = blockIdx.y * kColRows + threadIdx.y;
+  if (i >= d.nx) return;       // whole warps: i is uniform across a warp
   const bool col = j < d.ny;   // lanes past the last row stay for the shuffles
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   const long long q = d.at(col ? j : ny - 1, i);
@@ -144,63 +157,49 @@ __global__ void __launch_bounds__(1024) k_column_coefficients(CoefArgs a) {
   const double H = Hi[q];
   const bool ice = mask[q] == 1;
   const bool skip_visc = a.bc_margin && !ice;  // BC margins: no viscosity outside the ice (:759-764)
+  // strain rates of the depth-averaged flow (calc_effective_viscosity :751-754)
+  double eps_h = 0.0;
+  if (col && !skip_visc) {
+    const double du_dx = ddx_cx_to_a(d, a.u, j, i), dv_dy = ddy_cy_to_a(d, a.v, j, i);
+    const double du_dy = ddy_cx_to_a(d, a.u, j, i), dv_dx = ddx_cy_to_a(d, a.v, j, i);
+    eps_h = du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((du_dy + dv_dx) * (du_dy + dv_dx));
+  }
   // the faces of the column (calc_vertical_shear_strain_rates :685-721); a column on
   // the last row/column uses the face before it alone
   const bool has_e = col && i < nx - 1, has_w = col && i > 0, has_n = col && j < ny - 1, has_s = col && j > 0;
   const long long qe = has_e ? d.at(j, i + 1) : q, qw = has_w ? d.at(j, i - 1) : q;
   const long long qn = has_n ? d.at(j + 1, i) : q, qs = has_s ? d.at(j - 1, i) : q;
-  if (threadIdx.y == 0) {
-    // strain rates of the depth-averaged flow (calc_effective_viscosity :751-754)
-    double eps_h = 0.0;
-    if (col && !skip_visc) {
-      const double du_dx = ddx_cx_to_a(d, a.u, j, i), dv_dy = ddy_cy_to_a(d, a.v, j, i);
-      const double du_dy = ddy_cx_to_a(d, a.u, j, i), dv_dx = ddx_cy_to_a(d, a.v, j, i);
-      eps_h = du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((du_dy + dv_dx) * (du_dy + dv_dx));
-    }
-    s_eps[lane] = eps_h;
-    // face f joins p0 and p1; it has ice if either side has (:685-695)
-    const bool has[4] = {has_e, has_w, has_n, has_s};
-    const long long p0[4] = {q, qw, q, qs}, p1[4] = {qe, q, qn, q};
-    for (int f = 0; f < 4; ++f) {
-      const bool on = a.diva && has[f];
-      s_act[f][lane] = on && !(mask[p0[f]] == 0 && mask[p1[f]] == 0);
-      s_H0[f][lane] = on ? Hi[p0[f]] : 0.0;
-      s_H1[f][lane] = on ? Hi[p1[f]] : 0.0;
-      s_tb[f][lane] = on ? (f < 2 ? a.taub_cx : a.taub_cy)[p0[f]] : 0.0;
-    }
-  }
-  __syncthreads();
-  const double eps_h = s_eps[lane];
+  const FaceIn fe = face_in(a.diva && has_e, mask, Hi, a.taub_cx, q, qe);
+  const FaceIn fw = face_in(a.diva && has_w, mask, Hi, a.taub_cx, qw, q);
+  const FaceIn fn = face_in(a.diva && has_n, mask, Hi, a.taub_cy, q, qn);
+  const FaceIn fs = face_in(a.diva && has_s && lane == 0, mask, Hi, a.taub_cy, qs, q);
   const double Hw = has_w ? Hi[qw] : 0.0, Hs = has_s ? Hi[qs] : 0.0;
-  // du/dz on face f in layer k: (taub / staggered viscosity) * zeta (:685-695)
-  auto face_dz = [&](int f, long long p0, long long p1, long long off, double zk) {
-    if (!s_act[f][lane]) return 0.0;
-    const double vc = stag_margin(vp[off + p0], vp[off + p1], s_H0[f][lane], s_H1[f][lane]);
-    return (s_tb[f][lane] / vc) * zk;
-  };
-  for (int k = threadIdx.y; k < nz; k += blockDim.y) {
+  double vint = 0.0, fint = 0.0, vprev = 0.0, fprev = 0.0;
+  for (int k = 0; k < nz; ++k) {
     const long long off = (long long)k * d.plane;
     const double zk = a.zt.z[k];
-    double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0;
+    double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0, dudz_w = 0.0;
     if (a.diva) {
+      const double vq = vp[off + q];
       if (has_e) {
-        dudz_e = face_dz(FACE_E, q, qe, off, zk);
+        dudz_e = face_dz(fe, vq, vp[off + qe], zk);
         dudz[off + q] = dudz_e;
       }
       if (has_n) {
-        dvdz_n = face_dz(FACE_N, q, qn, off, zk);
+        dvdz_n = face_dz(fn, vq, vp[off + qn], zk);
         dvdz[off + q] = dvdz_n;
       }
+      if (has_w) dudz_w = face_dz(fw, vp[off + qw], vq, zk);
       dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
-      if (lane == 0 && has_s) dvdz_s = face_dz(FACE_S, qs, q, off, zk);
+      if (lane == 0 && has_s) dvdz_s = face_dz(fs, vp[off + qs], vq, zk);
     }
     double eta = 0.0;
     if (col && !skip_visc) {
       double du_dz_a = 0.0, dv_dz_a = 0.0;
       if (a.diva) {
         if (i == 0) du_dz_a = dudz_e;
-        else if (i == nx - 1) du_dz_a = face_dz(FACE_W, qw, q, off, zk);
-        else du_dz_a = stag_margin(face_dz(FACE_W, qw, q, off, zk), dudz_e, Hw, H);
+        else if (i == nx - 1) du_dz_a = dudz_w;
+        else du_dz_a = stag_margin(dudz_w, dudz_e, Hw, H);
         if (j == 0) dv_dz_a = dvdz_n;
         else if (j == ny - 1) dv_dz_a = dvdz_s;
         else dv_dz_a = stag_margin(dvdz_s, dvdz_n, Hs, H);
@@ -218,17 +217,15 @@ __global__ void __launch_bounds__(1024) k_column_coefficients(CoefArgs a) {
       eta = max_ref(afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
     }
     if (col) visc[off + q] = eta;
-    s_eta[k][lane] = eta;
-    if (a.diva) s_f[k][lane] = (H / eta) * a.zt.z2[k];
+    if (k > 0) vint = vint + 0.5 * (eta + vprev) * (zk - a.zt.z[k - 1]);
+    vprev = eta;
+    if (a.diva) {
+      const double fk = (H / eta) * a.zt.z2[k];
+      if (k > 0) fint = fint + 0.5 * (fk + fprev) * (zk - a.zt.z[k - 1]);
+      fprev = fk;
+    }
   }
-  __syncthreads();
-  if (threadIdx.y != 0 || !col) return;
-  double vint = 0.0, fint = 0.0;
-  for (int k = 1; k < nz; ++k) {
-    const double dz = a.zt.z[k] - a.zt.z[k - 1];
-    vint = vint + 0.5 * (s_eta[k][lane] + s_eta[k - 1][lane]) * dz;
-    if (a.diva) fint = fint + 0.5 * (s_f[k][lane] + s_f[k - 1][lane]) * dz;
-  }
+  if (!col) return;
   if (!skip_visc) {
     a.visc_int[q] = vint;
     a.Na[q] = a.bc_margin ? vint * H : vint * max_ref(0.1, H);
@@ -836,7 +833,8 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
                                  cudaMemcpyDeviceToDevice, c->stream));
   }
   {
-    const dim3 block(kColLanes, std::min(c->d.nz, 32)), grid((c->d.ny + kColLanes - 1) / kColLanes, c->d.nx);
+    const dim3 block(kColLanes, kColRows);
+    const dim3 grid((c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
     k_column_coefficients<<<grid, block, 0, c->stream>>>(a); c->launches++;
   }
   DIVA_LAUNCHED(c, "k_column_coefficients");
