@@ -186,25 +186,6 @@ __device__ __forceinline__ double diag_v(const Op& o, int j, int i) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;                   \
   const int i = blockIdx.y * blockDim.y + threadIdx.y;
 
-__global__ void k_diag(Op o, double* idu, double* idv) {
-  IDX2D
-  if (j >= o.d.ny || i >= o.d.nx) return;
-  const long long q = o.d.at(j, i);
-  idu[q] = u_int(o.d, j, i) ? 1.0 / diag_u(o, j, i) : 0.0;
-  idv[q] = v_int(o.d, j, i) ? 1.0 / diag_v(o, j, i) : 0.0;
-}
-
-// rhs of the free rows: b = -taud * dx^2 (divided by N_cx/N_cy without cross terms)
-__global__ void k_rhs(Dims d, int crossterms, const double* tdx, const double* tdy, const double* Ncx,
-                      const double* Ncy, double* bu, double* bv) {
-  IDX2D
-  if (j >= d.ny || i >= d.nx) return;
-  const long long q = d.at(j, i);
-  const double dx2 = d.dx * d.dx;
-  bu[q] = u_int(d, j, i) ? (crossterms ? -tdx[q] * dx2 : -tdx[q] * dx2 / Ncx[q]) : 0.0;
-  bv[q] = v_int(d, j, i) ? (crossterms ? -tdy[q] * dx2 : -tdy[q] * dx2 / Ncy[q]) : 0.0;
-}
-
 // Gauss-Seidel update of one point of one component (comp 0 = u, 1 = v)
 __device__ __forceinline__ void gs_point(const Op& o, double* xu, double* xv, const double* bu, const double* bv,
                                          const double* idu, const double* idv, int comp, int j, int i) {
@@ -579,82 +560,82 @@ __global__ void k_coarse_probe(Op o, CoarseMap m, double* A) {
   }
 }
 
-// Ainv = A^{-1} by in-place Gauss-Jordan with row pivoting (columns unscrambled at the end)
-__global__ void __launch_bounds__(256) k_coarse_invert(int n, const double* A, double* Ainv, int* singular) {
-  constexpr int M = kCoarseDirectMax;
-  __shared__ double a[M][M + 1];
-  __shared__ double fcol[M];
+// Ainv = A^{-1} by Gauss-Jordan elimination with row pivoting (columns unscrambled at
+// the end).  Step k maps the matrix of step k-1 (buffer k&1) to the next one (buffer
+// (k+1)&1) in one pass, with one barrier per step: every warp finds the pivot row p of
+// column k itself, and every element takes its value from the old matrix with rows k
+// and p exchanged -- the pivot row divided by the pivot, the others eliminated with it.
+constexpr int kInvThreads = 256;
+constexpr size_t kInvSmem = 2 * kCoarseDirectMax * (kCoarseDirectMax + 1) * sizeof(double);
+
+__global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int n, const double* A, double* Ainv, int* singular) {
+  constexpr int M = kCoarseDirectMax, LD = M + 1;
+  extern __shared__ double inv_buf[];   // two n x n matrices, row stride LD
   __shared__ int perm[M];
-  __shared__ double red[256];
-  __shared__ int s_p, s_bad;
-  const int tid = threadIdx.x;
+  __shared__ double wmax[kInvThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double amax = 0.0;
   for (int e = tid; e < n * n; e += blockDim.x) {
     const double v = A[e];
-    a[e / n][e % n] = v;
+    inv_buf[(e / n) * LD + e % n] = v;
     amax = (fabs(v) > amax || v != v) ? fabs(v) : amax;
   }
-  red[tid] = amax;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (tid < o) red[tid] = (red[tid + o] > red[tid] || red[tid + o] != red[tid + o]) ? red[tid + o] : red[tid];
-    __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) {   // largest magnitude; a NaN wins
+    const double w = __shfl_xor_sync(0xffffffffu, amax, o);
+    amax = (w > amax || w != w) ? w : amax;
   }
-  const double tiny = 1e-13 * red[0];
-  if (tid == 0) s_bad = !(red[0] > 0.0) || red[0] != red[0];
+  if (lane == 0) wmax[warp] = amax;
   __syncthreads();
-  for (int k = 0; k < n; ++k) {   // s_bad is read only between barriers that follow its last write
-    if (tid < 32) {   // pivot: largest |a[r][k]|, r >= k, lowest r on ties
-      double best = -1.0;
-      int br = k;
-      for (int r = k + tid; r < n; r += 32)
-        if (fabs(a[r][k]) > best) { best = fabs(a[r][k]); br = r; }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_down_sync(0xffffffffu, best, o);
-        const int orr = __shfl_down_sync(0xffffffffu, br, o);
-        if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
-      }
-      if (tid == 0) {
-        s_p = br;
-        if (!(best > tiny)) s_bad = 1;
-      }
+  amax = wmax[0];
+  for (int w = 1; w < (int)(blockDim.x >> 5); ++w) amax = (wmax[w] > amax || wmax[w] != wmax[w]) ? wmax[w] : amax;
+  const double tiny = 1e-13 * amax;
+  bool bad = !(amax > 0.0) || amax != amax;
+  int cur = 0;
+  for (int k = 0; k < n && !bad; ++k) {
+    const double* a = inv_buf + cur * M * LD;
+    double* b = inv_buf + (cur ^ 1) * M * LD;
+    // pivot: largest |a[r][k]|, r >= k, lowest r on ties (the same in every warp)
+    double best = -1.0;
+    int br = k;
+    for (int r = k + lane; r < n; r += 32)
+      if (fabs(a[r * LD + k]) > best) { best = fabs(a[r * LD + k]); br = r; }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+      if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
     }
-    __syncthreads();
-    if (s_bad) break;
-    const int p = s_p;
-    if (p != k)
-      for (int c = tid; c < n; c += blockDim.x) {
-        const double t = a[k][c];
-        a[k][c] = a[p][c];
-        a[p][c] = t;
-      }
+    if (!(best > tiny)) { bad = true; break; }
+    const int p = br;
     if (tid == 0) perm[k] = p;
-    __syncthreads();
-    const double piv = a[k][k];
-    for (int r = tid; r < n; r += blockDim.x) fcol[r] = a[r][k];
-    __syncthreads();
-    for (int c = tid; c < n; c += blockDim.x) a[k][c] = (c == k ? 1.0 : a[k][c]) / piv;
-    __syncthreads();
+    const double piv = a[p * LD + k];
     for (int e = tid; e < n * n; e += blockDim.x) {
       const int r = e / n, c = e % n;
-      if (r != k) a[r][c] = (c == k ? 0.0 : a[r][c]) - fcol[r] * a[k][c];
+      const double pk = (c == k ? 1.0 : a[p * LD + c]) / piv;   // normalised pivot row
+      if (r == k) {
+        b[r * LD + c] = pk;
+      } else {
+        const int src = r == p ? k : r;   // the row that sits at r after the exchange
+        b[r * LD + c] = (c == k ? 0.0 : a[src * LD + c]) - a[src * LD + k] * pk;
+      }
     }
+    cur ^= 1;
     __syncthreads();
   }
-  if (!s_bad) {
+  if (!bad) {
+    double* a = inv_buf + cur * M * LD;
     for (int k = n - 1; k >= 0; --k) {
       const int p = perm[k];
       if (p != k)
         for (int r = tid; r < n; r += blockDim.x) {
-          const double t = a[r][k];
-          a[r][k] = a[r][p];
-          a[r][p] = t;
+          const double t = a[r * LD + k];
+          a[r * LD + k] = a[r * LD + p];
+          a[r * LD + p] = t;
         }
       __syncthreads();
     }
-    for (int e = tid; e < n * n; e += blockDim.x) Ainv[e] = a[e / n][e % n];
+    for (int e = tid; e < n * n; e += blockDim.x) Ainv[e] = a[(e / n) * LD + e % n];
   }
-  if (tid == 0) *singular = s_bad;
+  if (tid == 0) *singular = bad ? 1 : 0;
 }
 
 // x += Ainv (b - A x) on the coarsest level, by one block (the caller synchronises)
@@ -816,10 +797,9 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
 }
 
 // rediscretised coarse coefficients (averages of the fine ones; B scales with the cell area)
-__global__ void k_coarsen(Dims df, Dims dc, int fx, int fy, const double* Na, const double* Nb, const double* Bx,
-                          const double* By, double* cNa, double* cNb, double* cBx, double* cBy) {
-  IDX2D
-  if (j >= dc.ny || i >= dc.nx) return;
+__device__ __forceinline__ void coarsen_point(const Dims& df, const Dims& dc, int fx, int fy, const double* Na,
+                                              const double* Nb, const double* Bx, const double* By, double* cNa,
+                                              double* cNb, double* cBx, double* cBy, int j, int i) {
   const long long q = dc.at(j, i);
   auto cl = [](int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); };
   const double w3[3] = {0.25, 0.5, 0.25};
@@ -862,6 +842,32 @@ __global__ void k_coarsen(Dims df, Dims dc, int fx, int fy, const double* Na, co
         s += wb * (1.0 / fy) * By[df.at(cl(fy * j + a, 0, df.ny - 2), cl(fx * i + b, 0, df.nx - 1))];
     }
     cBy[q] = area * s;
+  }
+}
+
+// rhs of the free rows of the finest level (k_rhs), folded into the first set-up launch
+struct RhsArgs {
+  int on, crossterms;
+  const double *tdx, *tdy, *Ncx, *Ncy;
+  double *bu, *bv;
+};
+
+// Operator set-up of one level in one launch over its points: the inverse diagonals of
+// level l, the rediscretised coefficients of level l+1 (coarse points are a subset of
+// the fine index range) and, on the finest level, the right-hand side.
+__global__ void k_level_setup(Op o, int coarsen, Dims dc, int fx, int fy, double* cNa, double* cNb, double* cBx,
+                              double* cBy, double* idu, double* idv, RhsArgs rhs) {
+  IDX2D
+  if (j >= o.d.ny || i >= o.d.nx) return;
+  const long long q = o.d.at(j, i);
+  idu[q] = u_int(o.d, j, i) ? 1.0 / diag_u(o, j, i) : 0.0;
+  idv[q] = v_int(o.d, j, i) ? 1.0 / diag_v(o, j, i) : 0.0;
+  if (coarsen && j < dc.ny && i < dc.nx)
+    coarsen_point(o.d, dc, fx, fy, o.Na, o.Nb, o.Bx, o.By, cNa, cNb, cBx, cBy, j, i);
+  if (rhs.on) {
+    const double dx2 = o.d.dx * o.d.dx;
+    rhs.bu[q] = u_int(o.d, j, i) ? (rhs.crossterms ? -rhs.tdx[q] * dx2 : -rhs.tdx[q] * dx2 / rhs.Ncx[q]) : 0.0;
+    rhs.bv[q] = v_int(o.d, j, i) ? (rhs.crossterms ? -rhs.tdy[q] * dx2 : -rhs.tdy[q] * dx2 / rhs.Ncy[q]) : 0.0;
   }
 }
 
@@ -1235,20 +1241,25 @@ int solver_setup(Ctx* c) {
   const diva_config_t& C = c->c;
   if (C.choice_ice_margin == DIVA_MARGIN_BC)
     return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
-  k_rhs<<<GL(0)>>>(c->d, C.include_SSADIVA_crossterms, c->D(DIVA_F_TAUDX_CX), c->D(DIVA_F_TAUDY_CY),
-                   c->D(DIVA_F_N_CX), c->D(DIVA_F_N_CY), c->kv[KV_B][0], c->kv[KV_B][1]); c->launches++;
-  DIVA_LAUNCHED(c, "k_rhs");
-  for (int l = 0; l + 1 < c->nlev; ++l) {
-    int fx, fy;
-    factors(c, l, &fx, &fy);
-    const Level& F = c->lv[l];
-    const Level& K = c->lv[l + 1];
-    k_coarsen<<<GL(l + 1)>>>(F.d, K.d, fx, fy, F.Na, F.Nb, F.Bx, F.By, K.Na, K.Nb, K.Bx, K.By); c->launches++;
-    DIVA_LAUNCHED(c, "k_coarsen");
-  }
+  // level l's diagonal and level l+1's coefficients in one launch; the finest level's
+  // launch also forms the right-hand side
   for (int l = 0; l < c->nlev; ++l) {
-    k_diag<<<GL(l)>>>(make_op(c, l), c->lv[l].idu, c->lv[l].idv); c->launches++;
-    DIVA_LAUNCHED(c, "k_diag");
+    const Level& F = c->lv[l];
+    const bool coarsen = l + 1 < c->nlev;
+    const Level& K = c->lv[coarsen ? l + 1 : l];
+    int fx = 1, fy = 1;
+    if (coarsen) factors(c, l, &fx, &fy);
+    RhsArgs rhs{};
+    if (l == 0) {
+      rhs.on = 1;
+      rhs.crossterms = C.include_SSADIVA_crossterms;
+      rhs.tdx = c->D(DIVA_F_TAUDX_CX); rhs.tdy = c->D(DIVA_F_TAUDY_CY);
+      rhs.Ncx = c->D(DIVA_F_N_CX); rhs.Ncy = c->D(DIVA_F_N_CY);
+      rhs.bu = c->kv[KV_B][0]; rhs.bv = c->kv[KV_B][1];
+    }
+    k_level_setup<<<GL(l)>>>(make_op(c, l), coarsen ? 1 : 0, K.d, fx, fy, K.Na, K.Nb, K.Bx, K.By, F.idu, F.idv,
+                             rhs); c->launches++;
+    DIVA_LAUNCHED(c, "k_level_setup");
   }
   const CoarseMap m = coarse_map(c);
   const Dims& dc = c->lv[c->nlev - 1].d;
@@ -1257,7 +1268,7 @@ int solver_setup(Ctx* c) {
   if (c->coarse_direct) {
     k_coarse_probe<<<c->coarse_n, 128, 2 * dc.plane * sizeof(double), c->stream>>>(make_op(c, c->nlev - 1), m,
                                                                                     c->coarse_A); c->launches++;
-    k_coarse_invert<<<1, 256, 0, c->stream>>>(c->coarse_n, c->coarse_A, c->coarse_inv, c->coarse_singular); c->launches++;
+    k_coarse_invert<<<1, kInvThreads, kInvSmem, c->stream>>>(c->coarse_n, c->coarse_A, c->coarse_inv, c->coarse_singular); c->launches++;
     DIVA_LAUNCHED(c, "coarse inverse");
   }
   return DIVA_OK;
@@ -1342,6 +1353,7 @@ static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu,
 int solver_init(Ctx* c) {
   if (sub_bytes(c, c->nlev - 1) > kSubSmemBudget)
     return set_error(c, DIVA_UNSUPPORTED, "coarsest multigrid level too large for the one-block sub-cycle");
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
