@@ -68,7 +68,7 @@ def workload(seed=2):
 def config_json(g, extra=None):
     c = {"workload": "DIVA+SIA cold-start solve, synthetic ice cap 1600x2800 km @5 km",
          "nx": g["nx"], "ny": g["ny"], "nz": len(g["zeta"]), "stop": "nonlinear rel-res <= 1e-6",
-         "linear_solver": "BiCGStab + geometric multigrid V(2,2), adaptive tolerance",
+         "linear_solver": "BiCGStab + geometric multigrid V(2,2), adaptive tolerance 0.5 min(1, rel-res)",
          "l2": "inputs larger than L2 (working set ~0.6 GB > 126 MB)"}
     c.update(extra or {})
     return c

@@ -70,6 +70,7 @@ class Config(C.Structure):
         ("picard_stop", C.c_int32),
         ("picard_relres_tol", C.c_double),
         ("lin_adaptive", C.c_int32),
+        ("lin_adaptive_eta", C.c_double),
         ("precision", C.c_int32),
         ("reserved", C.c_int32 * 8),
     ]

@@ -113,7 +113,7 @@ void config_defaults(diva_config_t* c) {
   c->choice_ice_rheology = DIVA_RHEO_HUYBRECHTS1992; c->uniform_flow_factor = 1E-16;
   c->do_ocean_floodfill = 1;
   c->lin_rtol = 1E-8; c->lin_maxit = 500;
-  c->picard_stop = DIVA_STOP_RESID_UV; c->picard_relres_tol = 1E-6; c->lin_adaptive = 0;
+  c->picard_stop = DIVA_STOP_RESID_UV; c->picard_relres_tol = 1E-6; c->lin_adaptive = 0; c->lin_adaptive_eta = 0.5;
   c->precision = DIVA_PREC_FP64;
 }
 
@@ -124,6 +124,8 @@ int validate_config(Ctx* c, const diva_config_t* cfg) {
   if (cfg->DIVA_visc_it_nit < 1) return set_error(c, DIVA_BAD_INPUT, "DIVA_visc_it_nit must be >= 1");
   if (!(cfg->n_flow > 0.0)) return set_error(c, DIVA_BAD_INPUT, "n_flow must be > 0");
   if (cfg->lin_maxit < 1) return set_error(c, DIVA_BAD_INPUT, "lin_maxit must be >= 1");
+  if (cfg->lin_adaptive && !(cfg->lin_adaptive_eta > 0.0 && cfg->lin_adaptive_eta < 1.0))
+    return set_error(c, DIVA_BAD_INPUT, "lin_adaptive_eta must lie in (0, 1)");
   const int bcs[8] = {cfg->BC_u_west, cfg->BC_u_east, cfg->BC_u_south, cfg->BC_u_north,
                       cfg->BC_v_west, cfg->BC_v_east, cfg->BC_v_south, cfg->BC_v_north};
   for (int b : bcs)
@@ -302,7 +304,7 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
       }
     }
     double rtol = C.lin_rtol;
-    if (relmode && C.lin_adaptive) rtol = std::max(C.lin_rtol, std::min(0.1, 0.05 * relres));
+    if (relmode && C.lin_adaptive) rtol = std::max(C.lin_rtol, C.lin_adaptive_eta * std::min(1.0, relres));
     int iters = 0;
     st = solver_solve(c, u, v, rtol, C.lin_maxit, &iters, nullptr);
     if (st == DIVA_LINEAR_NOT_CONVERGED) {

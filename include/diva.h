@@ -126,6 +126,7 @@ typedef struct {
   int32_t picard_stop;                  /* diva_stop_t */
   double  picard_relres_tol;            /* used when picard_stop == DIVA_STOP_RELRES */
   int32_t lin_adaptive;                 /* RELRES mode: linear rtol tied to the current nonlinear residual */
+  double  lin_adaptive_eta;             /* that rtol: max(lin_rtol, eta * min(1, rel-res)); default 0.5 */
   int32_t precision;                    /* diva_precision_t */
   int32_t reserved[8];
 } diva_config_t;

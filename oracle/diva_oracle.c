@@ -1889,7 +1889,7 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
     memcpy(FD(c, V_CY_PREV), v, sizeof(double) * ncy);
     /* same adaptive linear tolerance rule as the GPU library (iterative solvers only) */
     if (relmode && C->lin_adaptive && (c->lin_solver == ORC_LIN_GMRES_ILU || c->lin_solver == ORC_LIN_GMRES_WARM))
-      c->petsc_rtol = fmax(C->lin_rtol, fmin(0.1, 0.05 * relres));
+      c->petsc_rtol = fmax(C->lin_rtol, C->lin_adaptive_eta * fmin(1.0, relres));
     int st = solve_stag_linearised(c, u, v);
     if (st != DIVA_OK) status = st;
     apply_velocity_limits(c, u, v);
@@ -1996,7 +1996,7 @@ void orc_config_defaults(diva_config_t* c) {
   c->choice_ice_rheology = DIVA_RHEO_HUYBRECHTS1992; c->uniform_flow_factor = 1E-16;
   c->do_ocean_floodfill = 1;
   c->lin_rtol = 1E-8; c->lin_maxit = 2000;
-  c->picard_stop = DIVA_STOP_RESID_UV; c->picard_relres_tol = 1E-6; c->lin_adaptive = 0;
+  c->picard_stop = DIVA_STOP_RESID_UV; c->picard_relres_tol = 1E-6; c->lin_adaptive = 0; c->lin_adaptive_eta = 0.5;
   c->precision = DIVA_PREC_FP64;
 }
 
