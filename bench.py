@@ -311,6 +311,11 @@ def run_b200(args):
         host_in[n] = h
         keep.append(t_)
     h2d = sum(a.nbytes for a in host_in.values())
+    host_out = {}
+    for n in OUTPUT_FIELDS:
+        h, t_ = pinned(ctx.empty(n))
+        host_out[n] = h
+        keep.append(t_)
     e2e_steps = max(1, min(args.steps, 3))
 
     def e2e_step():
@@ -321,7 +326,7 @@ def run_b200(args):
         ctx.update_general_ice_model_data()
         ctx.solve_DIVA()
         ctx.calc_sia_3d_velocities()
-        return ctx.download(OUTPUT_FIELDS)
+        return ctx.download(OUTPUT_FIELDS, out=host_out)
 
     out = e2e_step()
     d2h = sum(a.nbytes for a in out.values())

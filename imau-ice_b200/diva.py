@@ -176,13 +176,22 @@ class Context:
                 raise DivaError(_abi.BAD_INPUT, f"{name}: shape {a.shape} != {self.grid.shape(kind)}")
             self._check(self.backend.fns["upload_field"](self.h, self.ids[name], a.ctypes.data), f"upload {name}")
 
-    def download(self, names=None):
-        out = {}
+    def download(self, names=None, out=None):
+        """Fields as Fortran-ordered host arrays.  ``out`` may hold preallocated arrays
+        (e.g. views of pinned memory) to fill instead of allocating new ones."""
+        res = {}
         for name in (names or self.fields.keys()):
-            a = self.empty(name)
+            a = None if out is None else out.get(name)
+            if a is None:
+                a = self.empty(name)
+            else:
+                kind, dt = self.fields[name]
+                if a.dtype != dt or a.shape != self.grid.shape(kind) or not a.flags.f_contiguous:
+                    raise DivaError(_abi.BAD_INPUT, f"{name}: output array must be Fortran-ordered {dt} "
+                                                   f"{self.grid.shape(kind)}")
             self._check(self.backend.fns["download_field"](self.h, self.ids[name], a.ctypes.data), f"download {name}")
-            out[name] = a
-        return out
+            res[name] = a
+        return res
 
     # ---- the reference's routines ---------------------------------------------
     def update_general_ice_model_data(self):
