@@ -178,6 +178,7 @@ size_t carve(Ctx* c, Carver& cv) {
   c->coarse_A = (double*)cv.take(sizeof(double) * kCoarseDirectMax * kCoarseDirectMax);
   c->coarse_inv = (double*)cv.take(sizeof(double) * kCoarseDirectMax * kCoarseDirectMax);
   c->coarse_singular = (int*)cv.take(sizeof(int) * 4);
+  c->sub_tab = (uint16_t*)cv.take(sizeof(uint16_t) * (solver_table_entries(c) + 8));
   const dim3 g = grid2d(d.ny, d.nx);
   c->max_blocks = g.x * g.y;
   c->partials = (double*)cv.take(sizeof(double) * 4 * c->max_blocks);

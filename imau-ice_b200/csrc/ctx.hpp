@@ -82,6 +82,10 @@ struct Ctx {
   double* coarse_A = nullptr;         // probed matrix, row-major n x n
   double* coarse_inv = nullptr;       // its inverse
   int* coarse_singular = nullptr;     // set by the inversion: relax instead
+  // row tables of the one-block sub-cycle levels (grid and boundary conditions only)
+  uint16_t* sub_tab = nullptr;
+  size_t sub_tab_off[kMaxLevels] = {};
+  int sub_cls[kMaxLevels][5] = {};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   PicardGraphs graphs[2];               // [0] solve_SSA, [1] solve_DIVA
   bool graphs_disabled = false;         // set if graph construction failed: host-driven loop
@@ -139,7 +143,8 @@ int launch_basal_pred(Ctx* c);
 int launch_any_sheet(Ctx* c, int* result);
 
 // solver.cu
-int solver_init(Ctx* c);      // per-context solver choices (after the configuration is known)
+int solver_init(Ctx* c);
+size_t solver_table_entries(const Ctx* c);   // uint16 entries of the sub-cycle row tables      // per-context solver choices (after the configuration is known)
 int solver_setup(Ctx* c);     // coefficients of all levels from N_a, N_b, beta_eff, taud
 int solver_solve(Ctx* c, const double* u0, const double* v0, double rtol, int maxit, int* iters, double* relres0);
 int solver_relres(Ctx* c, const double* u, const double* v, double* relres);

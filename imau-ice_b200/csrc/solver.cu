@@ -29,6 +29,7 @@
 // results are bit-reproducible from run to run.
 #include <cmath>
 #include <cstdio>
+#include <vector>
 #include "ctx.hpp"
 
 namespace diva {
@@ -43,19 +44,19 @@ struct Op {
   const double *Na, *Nb, *Bx, *By;
 };
 
-__device__ __forceinline__ bool u_int(const Dims& d, int j, int i) {
+__host__ __device__ __forceinline__ bool u_int(const Dims& d, int j, int i) {
   return i >= 1 && i <= d.nx - 3 && j >= 1 && j <= d.ny - 2;
 }
-__device__ __forceinline__ bool v_int(const Dims& d, int j, int i) {
+__host__ __device__ __forceinline__ bool v_int(const Dims& d, int j, int i) {
   return i >= 1 && i <= d.nx - 2 && j >= 1 && j <= d.ny - 3;
 }
-__device__ __forceinline__ int bc_pick(int a, int b) {
+__host__ __device__ __forceinline__ int bc_pick(int a, int b) {
   if (a == DIVA_BC_ZERO || b == DIVA_BC_ZERO) return DIVA_BC_ZERO;
   if (a == DIVA_BC_INFINITE || b == DIVA_BC_INFINITE) return DIVA_BC_INFINITE;
   return DIVA_BC_PERIODIC;
 }
 // Source of u(j,i) (list_DIVA_matrix_coefficients_eq_1_boundary :1932-2061); false = zero.
-__device__ __forceinline__ bool u_src(const Dims& d, const BCs& b, int j, int i, int& js, int& is) {
+__host__ __device__ __forceinline__ bool u_src(const Dims& d, const BCs& b, int j, int i, int& js, int& is) {
   if (u_int(d, j, i)) { js = j; is = i; return true; }
   const bool W = i == 0, E = i == d.nx - 2, S = j == 0, N = j == d.ny - 1;
   int t;
@@ -73,7 +74,7 @@ __device__ __forceinline__ bool u_src(const Dims& d, const BCs& b, int j, int i,
   return true;
 }
 // Source of v(j,i) (list_DIVA_matrix_coefficients_eq_2_boundary :2062-2191).
-__device__ __forceinline__ bool v_src(const Dims& d, const BCs& b, int j, int i, int& js, int& is) {
+__host__ __device__ __forceinline__ bool v_src(const Dims& d, const BCs& b, int j, int i, int& js, int& is) {
   if (v_int(d, j, i)) { js = j; is = i; return true; }
   const bool W = i == 0, E = i == d.nx - 1, S = j == 0, N = j == d.ny - 2;
   int t;
@@ -663,17 +664,29 @@ __device__ __forceinline__ void block_coarse_direct(const Op& o, const CoarseMap
 // barriers between the phases: the same per-point operations in the same order
 // as the per-level kernels of vcycle(), without a launch per phase and without a
 // global-memory round trip per phase.  Each level keeps kSubArrays compact planes
-// (row length ny) in the block's dynamic shared memory; the coefficients of every
-// level and x, b of the first are staged in at the start, x of the first level is
-// written back at the end.
+// (row length ny, one extra element that stays 0) in the block's dynamic shared
+// memory; the coefficients of every level and b of the first are staged in at the
+// start, x of the first level is written back at the end.
+//
+// The Gauss-Seidel passes and residuals run from row tables built once on the host
+// (they depend on the grid and the boundary conditions only): for each level the
+// interior rows grouped by (component, colour), each with its plane position and the
+// positions its eight off-diagonal stencil reads map to (boundary unknowns resolved
+// to their sources, 'zero' sides to the zero element).  A row update is then table
+// reads and the operator's arithmetic, without per-read boundary logic.
 enum { SA_NA, SA_NB, SA_BX, SA_BY, SA_IDU, SA_IDV, SA_XU, SA_XV, SA_BU, SA_BV, SA_RU, SA_RV, kSubArrays };
 constexpr size_t kSubSmemBudget = 200 * 1024;   // dynamic shared memory of the sub-cycle
+constexpr int kTabCols = 9;                      // a row's position and its eight mapped reads
 
 struct SubLevel {
   Op o;                      // global-memory operator of the level
   const double *idu, *idv;   // global inverse diagonals
   int fx, fy;                // coarsening factors to the next level
   int soff;                  // offset of the level's planes in shared memory (doubles)
+  int rows;                  // interior rows (u then v)
+  int cls[5];                // row ranges of the classes u colour 0, u 1, v 0, v 1
+  int toff;                  // offset of the level's row table in the shared table area (uint16)
+  const uint16_t* gtab;      // the table in global memory: kTabCols columns of `rows` entries
 };
 struct SubCycle {
   int first, last, nu1, nu2, coarse_sweeps;
@@ -682,6 +695,7 @@ struct SubCycle {
   const double* Ainv;
   const int* singular;
   Restriction rs;              // b of the first level: given, or restricted from the finer residual
+  int dbl;                     // doubles of all levels' planes (the table area follows)
   SubLevel L[kMaxLevels];
 };
 
@@ -691,36 +705,63 @@ __device__ __forceinline__ void block_for_points(const Dims& d, F f) {
   for (int t = threadIdx.x; t < n; t += blockDim.x) f(t % d.ny, t / d.ny);
 }
 
+// (A x) of table row r: same terms in the same order as AuX / AvX
+__device__ __forceinline__ double table_row_apply(const uint16_t* tab, int R, int r, bool urow, int ny, double ax,
+                                                  double ay, const double* Na, const double* Nb, const double* Bx,
+                                                  const double* By, const double* xu, const double* xv, int& q) {
+  q = tab[r];
+  const int s0 = tab[R + r], s1 = tab[2 * R + r], s2 = tab[3 * R + r], s3 = tab[4 * R + r];
+  const int s4 = tab[5 * R + r], s5 = tab[6 * R + r], s6 = tab[7 * R + r], s7 = tab[8 * R + r];
+  if (urow) {
+    const double Ae = Na[q + ny], Aw = Na[q], Bn = Nb[q], Bs = Nb[q - 1];
+    const double cE = 4.0 * ax * Ae, cW = 4.0 * ax * Aw, cN = ay * Bn, cS = ay * Bs;
+    const double diag = -(cE + cW + cN + cS) - Bx[q];
+    return cE * xu[s0] + cW * xu[s1] + cN * xu[s2] + cS * xu[s3] + diag * xu[q] + (-2.0 * Aw - Bn) * xv[s4] +
+           (2.0 * Ae + Bn) * xv[s5] + (2.0 * Aw + Bs) * xv[s6] + (-2.0 * Ae - Bs) * xv[s7];
+  }
+  const double An = Na[q + 1], As = Na[q], Be = Nb[q], Bw = Nb[q - ny];
+  const double cN = 4.0 * ay * An, cS = 4.0 * ay * As, cE = ax * Be, cW = ax * Bw;
+  const double diag = -(cN + cS + cE + cW) - By[q];
+  return cN * xv[s0] + cS * xv[s1] + cE * xv[s2] + cW * xv[s3] + diag * xv[q] + (-2.0 * An - Bw) * xu[s4] +
+         (2.0 * An + Be) * xu[s5] + (2.0 * As + Bw) * xu[s6] + (-2.0 * As - Be) * xu[s7];
+}
+
 __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* xu0, double* xv0,
                                                           const double* bu0, const double* bv0) {
   extern __shared__ double sm[];
   __shared__ Op so[kMaxLevels];   // operators of the staged levels
+  uint16_t* tabs = reinterpret_cast<uint16_t*>(sm + sc.dbl);
   if (threadIdx.x == 0)
     for (int l = sc.first; l <= sc.last; ++l) {
       Op o = sc.L[l].o;
-      const int P = o.d.nx * o.d.ny;
+      const int P1 = o.d.nx * o.d.ny + 1;
       o.d.ld = o.d.ny;
-      o.d.plane = P;
+      o.d.plane = P1 - 1;
       double* a = sm + sc.L[l].soff;
-      o.Na = a + SA_NA * P;
-      o.Nb = a + SA_NB * P;
-      o.Bx = a + SA_BX * P;
-      o.By = a + SA_BY * P;
+      o.Na = a + SA_NA * P1;
+      o.Nb = a + SA_NB * P1;
+      o.Bx = a + SA_BX * P1;
+      o.By = a + SA_BY * P1;
       so[l] = o;
     }
   for (int l = sc.first; l <= sc.last; ++l) {
     const SubLevel& L = sc.L[l];
     const Dims& g = L.o.d;
-    const int P = g.nx * g.ny;
+    const int P = g.nx * g.ny, P1 = P + 1;
     double* a = sm + L.soff;
-    for (int t = threadIdx.x; t < P; t += blockDim.x) {
+    for (int t = threadIdx.x; t < P1; t += blockDim.x) {
+      if (t == P) {   // the zero element read by 'zero' boundary sides
+        a[SA_XU * P1 + t] = 0.0;
+        a[SA_XV * P1 + t] = 0.0;
+        continue;
+      }
       const long long q = g.at(t % g.ny, t / g.ny);
-      a[SA_NA * P + t] = L.o.Na[q];
-      a[SA_NB * P + t] = L.o.Nb[q];
-      a[SA_BX * P + t] = L.o.Bx[q];
-      a[SA_BY * P + t] = L.o.By[q];
-      a[SA_IDU * P + t] = L.idu[q];
-      a[SA_IDV * P + t] = L.idv[q];
+      a[SA_NA * P1 + t] = L.o.Na[q];
+      a[SA_NB * P1 + t] = L.o.Nb[q];
+      a[SA_BX * P1 + t] = L.o.Bx[q];
+      a[SA_BY * P1 + t] = L.o.By[q];
+      a[SA_IDU * P1 + t] = L.idu[q];
+      a[SA_IDV * P1 + t] = L.idv[q];
       if (l == sc.first) {   // entered with x = 0
         double b0, b1;
         if (sc.rs.on) {
@@ -729,15 +770,34 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
           b0 = bu0[q];
           b1 = bv0[q];
         }
-        a[SA_XU * P + t] = 0.0;
-        a[SA_XV * P + t] = 0.0;
-        a[SA_BU * P + t] = b0;
-        a[SA_BV * P + t] = b1;
+        a[SA_XU * P1 + t] = 0.0;
+        a[SA_XV * P1 + t] = 0.0;
+        a[SA_BU * P1 + t] = b0;
+        a[SA_BV * P1 + t] = b1;
       }
     }
+    for (int t = threadIdx.x; t < kTabCols * L.rows; t += blockDim.x) tabs[L.toff + t] = L.gtab[t];
   }
   __syncthreads();
-  auto arr = [&](int l, int k) { return sm + sc.L[l].soff + k * (sc.L[l].o.d.nx * sc.L[l].o.d.ny); };
+  auto arr = [&](int l, int k) { return sm + sc.L[l].soff + k * (sc.L[l].o.d.nx * sc.L[l].o.d.ny + 1); };
+  // one Gauss-Seidel pass over the rows of class p (0/1: u colours, 2/3: v colours)
+  auto gs_pass = [&](int l, int p) {
+    const SubLevel& L = sc.L[l];
+    const Op& o = so[l];
+    const int P1 = L.o.d.nx * L.o.d.ny + 1, ny = L.o.d.ny;
+    const double* a = sm + L.soff;
+    double* xu = sm + L.soff + SA_XU * P1;
+    double* xv = sm + L.soff + SA_XV * P1;
+    const uint16_t* tab = tabs + L.toff;
+    const bool urow = p < 2;
+    for (int r = L.cls[p] + threadIdx.x; r < L.cls[p + 1]; r += blockDim.x) {
+      int q;
+      const double Ax = table_row_apply(tab, L.rows, r, urow, ny, o.ax, o.ay, a + SA_NA * P1, a + SA_NB * P1,
+                                        a + SA_BX * P1, a + SA_BY * P1, xu, xv, q);
+      if (urow) xu[q] += (a[SA_BU * P1 + q] - Ax) * a[SA_IDU * P1 + q];
+      else xv[q] += (a[SA_BV * P1 + q] - Ax) * a[SA_IDV * P1 + q];
+    }
+  };
   // descend
   for (int l = sc.first; l <= sc.last; ++l) {
     const Op& o = so[l];
@@ -754,11 +814,25 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
     }
     for (int s = 0; s < sc.nu1; ++s)
       for (int p = 0; p < 4; ++p) {
-        block_gs_pass(o, xu, xv, bu, bv, idu, idv, p >> 1, p & 1);
+        gs_pass(l, p);
         __syncthreads();
       }
+    // residual of the interior rows (the restriction reads interior rows only)
     double *ru = arr(l, SA_RU), *rv = arr(l, SA_RV);
-    block_for_points(o.d, [&](int j, int i) { residual_point(o, xu, xv, bu, bv, ru, rv, j, i); });
+    {
+      const SubLevel& L = sc.L[l];
+      const int P1 = L.o.d.nx * L.o.d.ny + 1;
+      const double* a = sm + L.soff;
+      const uint16_t* tab = tabs + L.toff;
+      for (int r = threadIdx.x; r < L.rows; r += blockDim.x) {
+        const bool urow = r < L.cls[2];
+        int q;
+        const double Ax = table_row_apply(tab, L.rows, r, urow, L.o.d.ny, o.ax, o.ay, a + SA_NA * P1,
+                                          a + SA_NB * P1, a + SA_BX * P1, a + SA_BY * P1, xu, xv, q);
+        if (urow) ru[q] = bu[q] - Ax;
+        else rv[q] = bv[q] - Ax;
+      }
+    }
     __syncthreads();
     const Op& k = so[l + 1];
     double *kxu = arr(l + 1, SA_XU), *kxv = arr(l + 1, SA_XV), *kbu = arr(l + 1, SA_BU), *kbv = arr(l + 1, SA_BV);
@@ -772,15 +846,14 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
   for (int l = sc.last - 1; l >= sc.first; --l) {
     const Op& o = so[l];
     const Op& k = so[l + 1];
-    double *xu = arr(l, SA_XU), *xv = arr(l, SA_XV), *bu = arr(l, SA_BU), *bv = arr(l, SA_BV);
-    const double *idu = arr(l, SA_IDU), *idv = arr(l, SA_IDV);
+    double *xu = arr(l, SA_XU), *xv = arr(l, SA_XV);
     const double *kxu = arr(l + 1, SA_XU), *kxv = arr(l + 1, SA_XV);
     const int fx = sc.L[l].fx, fy = sc.L[l].fy;
     block_for_points(o.d, [&](int j, int i) { prolong_point(k, o.d, fx, fy, kxu, kxv, xu, xv, j, i); });
     __syncthreads();
     for (int s = 0; s < sc.nu2; ++s)
       for (int p = 3; p >= 0; --p) {
-        block_gs_pass(o, xu, xv, bu, bv, idu, idv, p >> 1, p & 1);
+        gs_pass(l, p);
         __syncthreads();
       }
   }
@@ -1287,11 +1360,26 @@ static int gs_sweep(Ctx* c, int l, double* xu, double* xv, const double* bu, con
   return DIVA_OK;
 }
 
-// shared memory the sub-cycle needs from level l down
+// interior rows (u then v) of a level
+static int level_rows(const Dims& d) {
+  const int nu = (d.nx > 3 && d.ny > 2) ? (d.nx - 3) * (d.ny - 2) : 0;
+  const int nv = (d.nx > 2 && d.ny > 3) ? (d.nx - 2) * (d.ny - 3) : 0;
+  return nu + nv;
+}
+
+// shared memory the sub-cycle needs from level l down: the planes, then the row tables
+static size_t sub_dbl(const Ctx* c, int l) {
+  size_t n = 0;
+  for (int q = l; q < c->nlev; ++q) n += (size_t)kSubArrays * ((size_t)c->lv[q].d.nx * c->lv[q].d.ny + 1);
+  return n;
+}
+static size_t sub_tab_entries(const Ctx* c, int l) {
+  size_t n = 0;
+  for (int q = l; q < c->nlev; ++q) n += (size_t)kTabCols * level_rows(c->lv[q].d);
+  return n;
+}
 static size_t sub_bytes(const Ctx* c, int l) {
-  size_t b = 0;
-  for (int q = l; q < c->nlev; ++q) b += (size_t)kSubArrays * c->lv[q].d.nx * c->lv[q].d.ny * sizeof(double);
-  return b;
+  return sub_dbl(c, l) * sizeof(double) + ((sub_tab_entries(c, l) * sizeof(uint16_t) + 15) / 16) * 16;
 }
 
 // first level of the one-block sub-cycle: the largest whose levels all fit in shared memory
@@ -1350,9 +1438,56 @@ static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu,
 
 // Shared-memory limits of the tiled kernels (the 32 x 32 tiles need 80 KB) and of
 // the sub-cycle, and whether the grid's boundary conditions allow tiles at all.
+// Row tables of the sub-cycle levels (see k_subcycle), built on the host from the
+// level sizes and the boundary conditions and copied to the context's table area.
+static int build_sub_tables(Ctx* c) {
+  const int first = sub_first_level(c);
+  std::vector<uint16_t> tab(sub_tab_entries(c, first));
+  size_t off = 0;
+  for (int l = first; l < c->nlev; ++l) {
+    Dims d = c->lv[l].d;
+    d.ld = d.ny;   // compact planes in shared memory
+    const int P = d.nx * d.ny, R = level_rows(d);
+    if (P >= 65535) return set_error(c, DIVA_UNSUPPORTED, "sub-cycle level too large for 16-bit row tables");
+    c->sub_tab_off[l] = off;
+    int r = 0;
+    auto put = [&](int j, int i, bool urow) {
+      const int js_[4] = {urow ? j : j + 1, urow ? j : j - 1, urow ? j + 1 : j, urow ? j - 1 : j};
+      const int is_[4] = {urow ? i + 1 : i, urow ? i - 1 : i, urow ? i : i + 1, urow ? i : i - 1};
+      const int jc_[4] = {urow ? j : j + 1, urow ? j : j + 1, urow ? j - 1 : j, urow ? j - 1 : j};
+      const int ic_[4] = {urow ? i : i - 1, urow ? i + 1 : i, urow ? i : i - 1, urow ? i + 1 : i};
+      tab[off + r] = (uint16_t)d.at(j, i);
+      for (int k = 0; k < 4; ++k) {   // same-component neighbours, then the cross-coupled reads
+        int js, is;
+        const bool on = urow ? u_src(d, c->bc, js_[k], is_[k], js, is) : v_src(d, c->bc, js_[k], is_[k], js, is);
+        tab[off + (size_t)(1 + k) * R + r] = on ? (uint16_t)d.at(js, is) : (uint16_t)P;
+        const bool on2 = urow ? v_src(d, c->bc, jc_[k], ic_[k], js, is) : u_src(d, c->bc, jc_[k], ic_[k], js, is);
+        tab[off + (size_t)(5 + k) * R + r] = on2 ? (uint16_t)d.at(js, is) : (uint16_t)P;
+      }
+      ++r;
+    };
+    for (int p = 0; p < 4; ++p) {
+      c->sub_cls[l][p] = r;
+      const bool urow = p < 2;
+      for (int i = 0; i < d.nx; ++i)
+        for (int j = 0; j < d.ny; ++j)
+          if (((i + j) & 1) == (p & 1) && (urow ? u_int(d, j, i) : v_int(d, j, i))) put(j, i, urow);
+    }
+    c->sub_cls[l][4] = r;
+    if (r != R) return set_error(c, DIVA_CUDA_ERROR, "sub-cycle row table size");
+    off += (size_t)kTabCols * R;
+  }
+  if (!tab.empty())
+    DIVA_CUDA(c, cudaMemcpy(c->sub_tab, tab.data(), tab.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  return DIVA_OK;
+}
+
+size_t solver_table_entries(const Ctx* c) { return sub_tab_entries(c, sub_first_level(c)); }
+
 int solver_init(Ctx* c) {
   if (sub_bytes(c, c->nlev - 1) > kSubSmemBudget)
     return set_error(c, DIVA_UNSUPPORTED, "coarsest multigrid level too large for the one-block sub-cycle");
+  if (int st = build_sub_tables(c)) return st;
   DIVA_CUDA(c, cudaFuncSetAttribute(k_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
@@ -1384,7 +1519,7 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
     sc.map = coarse_map(c);
     sc.Ainv = c->coarse_inv;
     sc.singular = c->coarse_singular;
-    int soff = 0;
+    int soff = 0, toff = 0;
     for (int q = l; q < c->nlev; ++q) {
       const Level& L = c->lv[q];
       SubLevel& S = sc.L[q];
@@ -1393,8 +1528,14 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
       S.fx = 1; S.fy = 1;
       if (q + 1 < c->nlev) factors(c, q, &S.fx, &S.fy);
       S.soff = soff;
-      soff += kSubArrays * L.d.nx * L.d.ny;
+      soff += kSubArrays * (L.d.nx * L.d.ny + 1);
+      S.rows = level_rows(L.d);
+      for (int k = 0; k < 5; ++k) S.cls[k] = c->sub_cls[q][k];
+      S.toff = toff;
+      S.gtab = c->sub_tab + c->sub_tab_off[q];
+      toff += kTabCols * S.rows;
     }
+    sc.dbl = soff;
     sc.rs = rs;
     k_subcycle<<<1, kSubThreads, sub_bytes(c, l), c->stream>>>(sc, xu, xv, bu, bv); c->launches++;
     DIVA_LAUNCHED(c, "k_subcycle");
