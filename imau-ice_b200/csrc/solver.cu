@@ -125,6 +125,23 @@ __device__ __forceinline__ double LV(const Op& o, const double* x, int j, int i)
   return LVx<RAW>(o, x, GIx{o.d}, j, i);
 }
 
+// Sum of the nine stencil terms, accumulated with explicit fused multiply-adds in a
+// fixed order, so every code path (boundary-mapped reads, plain reads, the row
+// tables of the sub-cycle) rounds identically whatever the compiler would contract.
+__device__ __forceinline__ double stencil9(double c0, double x0, double c1, double x1, double c2, double x2,
+                                           double c3, double x3, double c4, double x4, double c5, double x5,
+                                           double c6, double x6, double c7, double x7, double c8, double x8) {
+  double s = c0 * x0;
+  s = fma(c1, x1, s);
+  s = fma(c2, x2, s);
+  s = fma(c3, x3, s);
+  s = fma(c4, x4, s);
+  s = fma(c5, x5, s);
+  s = fma(c6, x6, s);
+  s = fma(c7, x7, s);
+  return fma(c8, x8, s);
+}
+
 // (A x) of the u row at interior (j,i) (list_DIVA_matrix_coefficients_eq_1_free :2342-2404)
 template <bool RAW, class IX>
 __device__ __forceinline__ double AuX(const Op& o, const double* xu, const double* xv, const IX& ix, int j, int i) {
@@ -132,10 +149,10 @@ __device__ __forceinline__ double AuX(const Op& o, const double* xu, const doubl
   const double Ae = o.Na[d.at(j, i + 1)], Aw = o.Na[d.at(j, i)], Bn = o.Nb[d.at(j, i)], Bs = o.Nb[d.at(j - 1, i)];
   const double cE = 4.0 * o.ax * Ae, cW = 4.0 * o.ax * Aw, cN = o.ay * Bn, cS = o.ay * Bs;
   const double diag = -(cE + cW + cN + cS) - o.Bx[d.at(j, i)];
-  return cE * LUx<RAW>(o, xu, ix, j, i + 1) + cW * LUx<RAW>(o, xu, ix, j, i - 1) +
-         cN * LUx<RAW>(o, xu, ix, j + 1, i) + cS * LUx<RAW>(o, xu, ix, j - 1, i) + diag * xu[ix(j, i)] +
-         (-2.0 * Aw - Bn) * LVx<RAW>(o, xv, ix, j, i) + (2.0 * Ae + Bn) * LVx<RAW>(o, xv, ix, j, i + 1) +
-         (2.0 * Aw + Bs) * LVx<RAW>(o, xv, ix, j - 1, i) + (-2.0 * Ae - Bs) * LVx<RAW>(o, xv, ix, j - 1, i + 1);
+  return stencil9(cE, LUx<RAW>(o, xu, ix, j, i + 1), cW, LUx<RAW>(o, xu, ix, j, i - 1), cN,
+                  LUx<RAW>(o, xu, ix, j + 1, i), cS, LUx<RAW>(o, xu, ix, j - 1, i), diag, xu[ix(j, i)],
+                  -2.0 * Aw - Bn, LVx<RAW>(o, xv, ix, j, i), 2.0 * Ae + Bn, LVx<RAW>(o, xv, ix, j, i + 1),
+                  2.0 * Aw + Bs, LVx<RAW>(o, xv, ix, j - 1, i), -2.0 * Ae - Bs, LVx<RAW>(o, xv, ix, j - 1, i + 1));
 }
 // (A x) of the v row at interior (j,i) (list_DIVA_matrix_coefficients_eq_2_free :2405-2467)
 template <bool RAW, class IX>
@@ -144,10 +161,10 @@ __device__ __forceinline__ double AvX(const Op& o, const double* xu, const doubl
   const double An = o.Na[d.at(j + 1, i)], As = o.Na[d.at(j, i)], Be = o.Nb[d.at(j, i)], Bw = o.Nb[d.at(j, i - 1)];
   const double cN = 4.0 * o.ay * An, cS = 4.0 * o.ay * As, cE = o.ax * Be, cW = o.ax * Bw;
   const double diag = -(cN + cS + cE + cW) - o.By[d.at(j, i)];
-  return cN * LVx<RAW>(o, xv, ix, j + 1, i) + cS * LVx<RAW>(o, xv, ix, j - 1, i) +
-         cE * LVx<RAW>(o, xv, ix, j, i + 1) + cW * LVx<RAW>(o, xv, ix, j, i - 1) + diag * xv[ix(j, i)] +
-         (-2.0 * An - Bw) * LUx<RAW>(o, xu, ix, j + 1, i - 1) + (2.0 * An + Be) * LUx<RAW>(o, xu, ix, j + 1, i) +
-         (2.0 * As + Bw) * LUx<RAW>(o, xu, ix, j, i - 1) + (-2.0 * As - Be) * LUx<RAW>(o, xu, ix, j, i);
+  return stencil9(cN, LVx<RAW>(o, xv, ix, j + 1, i), cS, LVx<RAW>(o, xv, ix, j - 1, i), cE,
+                  LVx<RAW>(o, xv, ix, j, i + 1), cW, LVx<RAW>(o, xv, ix, j, i - 1), diag, xv[ix(j, i)],
+                  -2.0 * An - Bw, LUx<RAW>(o, xu, ix, j + 1, i - 1), 2.0 * An + Be, LUx<RAW>(o, xu, ix, j + 1, i),
+                  2.0 * As + Bw, LUx<RAW>(o, xu, ix, j, i - 1), -2.0 * As - Be, LUx<RAW>(o, xu, ix, j, i));
 }
 template <bool RAW = false>
 __device__ __forceinline__ double Au(const Op& o, const double* xu, const double* xv, int j, int i) {
@@ -392,7 +409,18 @@ __device__ __forceinline__ int tile_dist(int j, int i, int tj0, int ti0, int TJ,
 }
 
 // one colour pass over the region points within `reach` of the tile
+// A block whose whole region lies in the interior of both components (u: 1 <= i <=
+// nx-3, 1 <= j <= ny-2; v: 1 <= i <= nx-2, 1 <= j <= ny-3) reads every stencil value
+// as stored: the boundary mapping is the identity there, so DEEP blocks skip it and
+// the interior tests (the same values, decided once per block).
+constexpr bool kTileDeepPath = true;
 template <int TJ, int TI>
+__device__ __forceinline__ bool tile_deep(const TIx& ix, const Dims& d) {
+  using G = TileGeom<TJ, TI>;
+  return kTileDeepPath && ix.i0 >= 1 && ix.i0 + G::RI - 1 <= d.nx - 3 && ix.j0 >= 1 && ix.j0 + G::RJ - 1 <= d.ny - 3;
+}
+
+template <int TJ, int TI, bool DEEP>
 __device__ __forceinline__ void tile_pass(const Op& o, const TIx& ix, double* xu, double* xv, const double* bu,
                                           const double* bv, const double* idu, const double* idv, int tj0, int ti0,
                                           int comp, int color, int reach) {
@@ -402,16 +430,24 @@ __device__ __forceinline__ void tile_pass(const Op& o, const TIx& ix, double* xu
   for (int t = threadIdx.x; t < hj * G::RI; t += blockDim.x) {
     const int i = ix.i0 + t / hj;
     const int j = ix.j0 + 2 * (t % hj) + ((color + i + ix.j0) & 1);   // (i + j) & 1 == color
-    if (j >= ix.j0 + G::RJ || j < 0 || j >= d.ny || i < 0 || i >= d.nx) continue;
+    if (j >= ix.j0 + G::RJ) continue;
+    if (!DEEP && (j < 0 || j >= d.ny || i < 0 || i >= d.nx)) continue;
     if (tile_dist(j, i, tj0, ti0, TJ, TI) > reach) continue;
     const long long q = d.at(j, i);
     const int k = ix(j, i);
     if (comp == 0) {
-      if (u_int(d, j, i)) xu[k] += (bu[k] - AuX<false>(o, xu, xv, ix, j, i)) * idu[q];
+      if (DEEP || u_int(d, j, i)) xu[k] += (bu[k] - AuX<DEEP>(o, xu, xv, ix, j, i)) * idu[q];
     } else {
-      if (v_int(d, j, i)) xv[k] += (bv[k] - AvX<false>(o, xu, xv, ix, j, i)) * idv[q];
+      if (DEEP || v_int(d, j, i)) xv[k] += (bv[k] - AvX<DEEP>(o, xu, xv, ix, j, i)) * idv[q];
     }
   }
+}
+template <int TJ, int TI>
+__device__ __forceinline__ void tile_pass_any(bool deep, const Op& o, const TIx& ix, double* xu, double* xv,
+                                              const double* bu, const double* bv, const double* idu,
+                                              const double* idv, int tj0, int ti0, int comp, int color, int reach) {
+  if (deep) tile_pass<TJ, TI, true>(o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, comp, color, reach);
+  else tile_pass<TJ, TI, false>(o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, comp, color, reach);
 }
 
 // Source of b for a pre-smoothing kernel: given on the level (the finest), or the
@@ -435,6 +471,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
   const TIx ix{tj0 - kHalo, ti0 - kHalo, G::RJ};
+  const bool deep = tile_deep<TJ, TI>(ix, d);
   for (int t = threadIdx.x; t < G::N; t += blockDim.x) {
     const int j = ix.j0 + t % G::RJ, i = ix.i0 + t / G::RJ;
     const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
@@ -457,7 +494,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 0; p < 4; ++p, ++pass) {
-      tile_pass<TJ, TI>(o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI>(deep, o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -471,8 +508,13 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
       gbu[q] = bu[k];
       gbv[q] = bv[k];
     }
-    gru[q] = u_int(d, j, i) ? bu[k] - AuX<false>(o, xu, xv, ix, j, i) : 0.0;
-    grv[q] = v_int(d, j, i) ? bv[k] - AvX<false>(o, xu, xv, ix, j, i) : 0.0;
+    if (deep) {
+      gru[q] = bu[k] - AuX<true>(o, xu, xv, ix, j, i);
+      grv[q] = bv[k] - AvX<true>(o, xu, xv, ix, j, i);
+    } else {
+      gru[q] = u_int(d, j, i) ? bu[k] - AuX<false>(o, xu, xv, ix, j, i) : 0.0;
+      grv[q] = v_int(d, j, i) ? bv[k] - AvX<false>(o, xu, xv, ix, j, i) : 0.0;
+    }
   }
 }
 
@@ -488,6 +530,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
   const TIx ix{tj0 - kHalo, ti0 - kHalo, G::RJ};
+  const bool deep = tile_deep<TJ, TI>(ix, d);
   for (int t = threadIdx.x; t < G::N; t += blockDim.x) {
     const int j = ix.j0 + t % G::RJ, i = ix.i0 + t / G::RJ;
     const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
@@ -512,7 +555,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 3; p >= 0; --p, ++pass) {
-      tile_pass<TJ, TI>(o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI>(deep, o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -716,14 +759,14 @@ __device__ __forceinline__ double table_row_apply(const uint16_t* tab, int R, in
     const double Ae = Na[q + ny], Aw = Na[q], Bn = Nb[q], Bs = Nb[q - 1];
     const double cE = 4.0 * ax * Ae, cW = 4.0 * ax * Aw, cN = ay * Bn, cS = ay * Bs;
     const double diag = -(cE + cW + cN + cS) - Bx[q];
-    return cE * xu[s0] + cW * xu[s1] + cN * xu[s2] + cS * xu[s3] + diag * xu[q] + (-2.0 * Aw - Bn) * xv[s4] +
-           (2.0 * Ae + Bn) * xv[s5] + (2.0 * Aw + Bs) * xv[s6] + (-2.0 * Ae - Bs) * xv[s7];
+    return stencil9(cE, xu[s0], cW, xu[s1], cN, xu[s2], cS, xu[s3], diag, xu[q], -2.0 * Aw - Bn, xv[s4],
+                    2.0 * Ae + Bn, xv[s5], 2.0 * Aw + Bs, xv[s6], -2.0 * Ae - Bs, xv[s7]);
   }
   const double An = Na[q + 1], As = Na[q], Be = Nb[q], Bw = Nb[q - ny];
   const double cN = 4.0 * ay * An, cS = 4.0 * ay * As, cE = ax * Be, cW = ax * Bw;
   const double diag = -(cN + cS + cE + cW) - By[q];
-  return cN * xv[s0] + cS * xv[s1] + cE * xv[s2] + cW * xv[s3] + diag * xv[q] + (-2.0 * An - Bw) * xu[s4] +
-         (2.0 * An + Be) * xu[s5] + (2.0 * As + Bw) * xu[s6] + (-2.0 * As - Be) * xu[s7];
+  return stencil9(cN, xv[s0], cS, xv[s1], cE, xv[s2], cW, xv[s3], diag, xv[q], -2.0 * An - Bw, xu[s4],
+                  2.0 * An + Be, xu[s5], 2.0 * As + Bw, xu[s6], -2.0 * As - Be, xu[s7]);
 }
 
 __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* xu0, double* xv0,
