@@ -143,28 +143,37 @@ __device__ __forceinline__ double stencil9(double c0, double x0, double c1, doub
 }
 
 // (A x) of the u row at interior (j,i) (list_DIVA_matrix_coefficients_eq_1_free :2342-2404)
-template <bool RAW, class IX>
-__device__ __forceinline__ double AuX(const Op& o, const double* xu, const double* xv, const IX& ix, int j, int i) {
-  const Dims& d = o.d;
-  const double Ae = o.Na[d.at(j, i + 1)], Aw = o.Na[d.at(j, i)], Bn = o.Nb[d.at(j, i)], Bs = o.Nb[d.at(j - 1, i)];
+// IX places x values, CX the coefficients N_a, N_b, B (a level plane or a shared-memory tile)
+template <bool RAW, class IX, class CX>
+__device__ __forceinline__ double AuXC(const Op& o, const double* xu, const double* xv, const IX& ix, const CX& cx,
+                                       int j, int i) {
+  const double Ae = o.Na[cx(j, i + 1)], Aw = o.Na[cx(j, i)], Bn = o.Nb[cx(j, i)], Bs = o.Nb[cx(j - 1, i)];
   const double cE = 4.0 * o.ax * Ae, cW = 4.0 * o.ax * Aw, cN = o.ay * Bn, cS = o.ay * Bs;
-  const double diag = -(cE + cW + cN + cS) - o.Bx[d.at(j, i)];
+  const double diag = -(cE + cW + cN + cS) - o.Bx[cx(j, i)];
   return stencil9(cE, LUx<RAW>(o, xu, ix, j, i + 1), cW, LUx<RAW>(o, xu, ix, j, i - 1), cN,
                   LUx<RAW>(o, xu, ix, j + 1, i), cS, LUx<RAW>(o, xu, ix, j - 1, i), diag, xu[ix(j, i)],
                   -2.0 * Aw - Bn, LVx<RAW>(o, xv, ix, j, i), 2.0 * Ae + Bn, LVx<RAW>(o, xv, ix, j, i + 1),
                   2.0 * Aw + Bs, LVx<RAW>(o, xv, ix, j - 1, i), -2.0 * Ae - Bs, LVx<RAW>(o, xv, ix, j - 1, i + 1));
 }
 // (A x) of the v row at interior (j,i) (list_DIVA_matrix_coefficients_eq_2_free :2405-2467)
-template <bool RAW, class IX>
-__device__ __forceinline__ double AvX(const Op& o, const double* xu, const double* xv, const IX& ix, int j, int i) {
-  const Dims& d = o.d;
-  const double An = o.Na[d.at(j + 1, i)], As = o.Na[d.at(j, i)], Be = o.Nb[d.at(j, i)], Bw = o.Nb[d.at(j, i - 1)];
+template <bool RAW, class IX, class CX>
+__device__ __forceinline__ double AvXC(const Op& o, const double* xu, const double* xv, const IX& ix, const CX& cx,
+                                       int j, int i) {
+  const double An = o.Na[cx(j + 1, i)], As = o.Na[cx(j, i)], Be = o.Nb[cx(j, i)], Bw = o.Nb[cx(j, i - 1)];
   const double cN = 4.0 * o.ay * An, cS = 4.0 * o.ay * As, cE = o.ax * Be, cW = o.ax * Bw;
-  const double diag = -(cN + cS + cE + cW) - o.By[d.at(j, i)];
+  const double diag = -(cN + cS + cE + cW) - o.By[cx(j, i)];
   return stencil9(cN, LVx<RAW>(o, xv, ix, j + 1, i), cS, LVx<RAW>(o, xv, ix, j - 1, i), cE,
                   LVx<RAW>(o, xv, ix, j, i + 1), cW, LVx<RAW>(o, xv, ix, j, i - 1), diag, xv[ix(j, i)],
                   -2.0 * An - Bw, LUx<RAW>(o, xu, ix, j + 1, i - 1), 2.0 * An + Be, LUx<RAW>(o, xu, ix, j + 1, i),
                   2.0 * As + Bw, LUx<RAW>(o, xu, ix, j, i - 1), -2.0 * As - Be, LUx<RAW>(o, xu, ix, j, i));
+}
+template <bool RAW, class IX>
+__device__ __forceinline__ double AuX(const Op& o, const double* xu, const double* xv, const IX& ix, int j, int i) {
+  return AuXC<RAW>(o, xu, xv, ix, GIx{o.d}, j, i);
+}
+template <bool RAW, class IX>
+__device__ __forceinline__ double AvX(const Op& o, const double* xu, const double* xv, const IX& ix, int j, int i) {
+  return AvXC<RAW>(o, xu, xv, ix, GIx{o.d}, j, i);
 }
 template <bool RAW = false>
 __device__ __forceinline__ double Au(const Op& o, const double* xu, const double* xv, int j, int i) {
@@ -395,20 +404,14 @@ __global__ void k_prolong(Op oc, Dims df, int fx, int fy, const double* xcu, con
 constexpr int kHalo = 9;
 constexpr int kTileThreads = 512;
 
-template <int TJ, int TI>
+// STAGE: the region's coefficients (N_a, N_b, B_x, B_y and the inverse diagonals)
+// are staged in shared memory too, so the colour passes touch no global memory.
+template <int TJ, int TI, bool STAGE>
 struct TileGeom {
   static constexpr int RJ = TJ + 2 * kHalo, RI = TI + 2 * kHalo, N = RJ * RI;
-  static constexpr size_t smem = 4 * N * sizeof(double);   // xu, xv, bu, bv of the region
+  static constexpr size_t smem = (STAGE ? 10 : 4) * N * sizeof(double);   // x, b (+ 6 coefficient planes)
 };
 
-// Chebyshev distance of (j,i) from the tile [tj0, tj0+TJ) x [ti0, ti0+TI)
-__device__ __forceinline__ int tile_dist(int j, int i, int tj0, int ti0, int TJ, int TI) {
-  const int dj = max(max(tj0 - j, j - (tj0 + TJ - 1)), 0);
-  const int di = max(max(ti0 - i, i - (ti0 + TI - 1)), 0);
-  return max(dj, di);
-}
-
-// one colour pass over the region points within `reach` of the tile
 // A block whose whole region lies in the interior of both components (u: 1 <= i <=
 // nx-3, 1 <= j <= ny-2; v: 1 <= i <= nx-2, 1 <= j <= ny-3) reads every stencil value
 // as stored: the boundary mapping is the identity there, so DEEP blocks skip it and
@@ -416,38 +419,83 @@ __device__ __forceinline__ int tile_dist(int j, int i, int tj0, int ti0, int TJ,
 constexpr bool kTileDeepPath = true;
 template <int TJ, int TI>
 __device__ __forceinline__ bool tile_deep(const TIx& ix, const Dims& d) {
-  using G = TileGeom<TJ, TI>;
-  return kTileDeepPath && ix.i0 >= 1 && ix.i0 + G::RI - 1 <= d.nx - 3 && ix.j0 >= 1 && ix.j0 + G::RJ - 1 <= d.ny - 3;
+  constexpr int RJ = TJ + 2 * kHalo, RI = TI + 2 * kHalo;
+  return kTileDeepPath && ix.i0 >= 1 && ix.i0 + RI - 1 <= d.nx - 3 && ix.j0 >= 1 && ix.j0 + RJ - 1 <= d.ny - 3;
 }
 
-template <int TJ, int TI, bool DEEP>
-__device__ __forceinline__ void tile_pass(const Op& o, const TIx& ix, double* xu, double* xv, const double* bu,
-                                          const double* bv, const double* idu, const double* idv, int tj0, int ti0,
-                                          int comp, int color, int reach) {
-  using G = TileGeom<TJ, TI>;
-  const Dims& d = o.d;
-  constexpr int hj = (G::RJ + 1) / 2;
-  for (int t = threadIdx.x; t < hj * G::RI; t += blockDim.x) {
-    const int i = ix.i0 + t / hj;
-    const int j = ix.j0 + 2 * (t % hj) + ((color + i + ix.j0) & 1);   // (i + j) & 1 == color
-    if (j >= ix.j0 + G::RJ) continue;
+// The shared-memory planes of a tile kernel and the operator reading from them.
+template <int TJ, int TI, bool STAGE>
+struct TileMem {
+  double *xu, *xv, *bu, *bv;
+  const double *iu, *iv;   // inverse diagonals: staged plane or the level's
+  Op os;                   // the level's operator, coefficients staged when STAGE
+  __device__ TileMem(double* sm, const Op& o, const double* idu, const double* idv) {
+    using G = TileGeom<TJ, TI, STAGE>;
+    xu = sm; xv = sm + G::N; bu = sm + 2 * G::N; bv = sm + 3 * G::N;
+    os = o;
+    iu = idu; iv = idv;
+    if (STAGE) {
+      os.Na = sm + 4 * G::N; os.Nb = sm + 5 * G::N; os.Bx = sm + 6 * G::N; os.By = sm + 7 * G::N;
+      iu = sm + 8 * G::N; iv = sm + 9 * G::N;
+    }
+  }
+  // stage the region's coefficients (out-of-domain points are never read)
+  __device__ void stage(const Op& o, const double* idu, const double* idv, const TIx& ix, int t, bool in,
+                        long long q) {
+    if (!STAGE) return;
+    using G = TileGeom<TJ, TI, STAGE>;
+    double* sm = xu;
+    sm[4 * G::N + t] = in ? o.Na[q] : 0.0;
+    sm[5 * G::N + t] = in ? o.Nb[q] : 0.0;
+    sm[6 * G::N + t] = in ? o.Bx[q] : 0.0;
+    sm[7 * G::N + t] = in ? o.By[q] : 0.0;
+    sm[8 * G::N + t] = in ? idu[q] : 0.0;
+    sm[9 * G::N + t] = in ? idv[q] : 0.0;
+  }
+  template <bool RAW>
+  __device__ __forceinline__ double Au(const TIx& ix, int j, int i) const {
+    if (STAGE) return AuXC<RAW>(os, xu, xv, ix, ix, j, i);
+    return AuXC<RAW>(os, xu, xv, ix, GIx{os.d}, j, i);
+  }
+  template <bool RAW>
+  __device__ __forceinline__ double Av(const TIx& ix, int j, int i) const {
+    if (STAGE) return AvXC<RAW>(os, xu, xv, ix, ix, j, i);
+    return AvXC<RAW>(os, xu, xv, ix, GIx{os.d}, j, i);
+  }
+  __device__ __forceinline__ double idu(const TIx& ix, int j, int i) const {
+    return STAGE ? iu[ix(j, i)] : iu[os.d.at(j, i)];
+  }
+  __device__ __forceinline__ double idv(const TIx& ix, int j, int i) const {
+    return STAGE ? iv[ix(j, i)] : iv[os.d.at(j, i)];
+  }
+};
+
+// one colour pass over the region points within `reach` of the tile
+template <int TJ, int TI, bool STAGE, bool DEEP>
+__device__ __forceinline__ void tile_pass(TileMem<TJ, TI, STAGE>& m, const TIx& ix, int tj0, int ti0, int comp,
+                                          int color, int reach) {
+  const Dims& d = m.os.d;
+  // the box of points within `reach` of the tile, one colour of it
+  const int bj0 = tj0 - reach, bi0 = ti0 - reach, BJ = TJ + 2 * reach, BI = TI + 2 * reach;
+  const int hj = (BJ + 1) / 2;
+  for (int t = threadIdx.x; t < hj * BI; t += blockDim.x) {
+    const int i = bi0 + t / hj;
+    const int j = bj0 + 2 * (t % hj) + ((color + i + bj0) & 1);   // (i + j) & 1 == color
+    if (j >= bj0 + BJ) continue;
     if (!DEEP && (j < 0 || j >= d.ny || i < 0 || i >= d.nx)) continue;
-    if (tile_dist(j, i, tj0, ti0, TJ, TI) > reach) continue;
-    const long long q = d.at(j, i);
     const int k = ix(j, i);
     if (comp == 0) {
-      if (DEEP || u_int(d, j, i)) xu[k] += (bu[k] - AuX<DEEP>(o, xu, xv, ix, j, i)) * idu[q];
+      if (DEEP || u_int(d, j, i)) m.xu[k] += (m.bu[k] - m.template Au<DEEP>(ix, j, i)) * m.idu(ix, j, i);
     } else {
-      if (DEEP || v_int(d, j, i)) xv[k] += (bv[k] - AvX<DEEP>(o, xu, xv, ix, j, i)) * idv[q];
+      if (DEEP || v_int(d, j, i)) m.xv[k] += (m.bv[k] - m.template Av<DEEP>(ix, j, i)) * m.idv(ix, j, i);
     }
   }
 }
-template <int TJ, int TI>
-__device__ __forceinline__ void tile_pass_any(bool deep, const Op& o, const TIx& ix, double* xu, double* xv,
-                                              const double* bu, const double* bv, const double* idu,
-                                              const double* idv, int tj0, int ti0, int comp, int color, int reach) {
-  if (deep) tile_pass<TJ, TI, true>(o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, comp, color, reach);
-  else tile_pass<TJ, TI, false>(o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, comp, color, reach);
+template <int TJ, int TI, bool STAGE>
+__device__ __forceinline__ void tile_pass_any(bool deep, TileMem<TJ, TI, STAGE>& m, const TIx& ix, int tj0, int ti0,
+                                              int comp, int color, int reach) {
+  if (deep) tile_pass<TJ, TI, STAGE, true>(m, ix, tj0, ti0, comp, color, reach);
+  else tile_pass<TJ, TI, STAGE, false>(m, ix, tj0, ti0, comp, color, reach);
 }
 
 // Source of b for a pre-smoothing kernel: given on the level (the finest), or the
@@ -461,40 +509,41 @@ struct Restriction {
 
 // pre-smoothing from x = 0 (the descent of a V-cycle enters every level with x = 0):
 // `sweeps` forward sweeps (u0 u1 v0 v1), then x, b and r = b - A x of the tile
-template <int TJ, int TI>
+template <int TJ, int TI, bool STAGE>
 __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction rs, double* gbu, double* gbv,
                                                               double* gxu, double* gxv, double* gru, double* grv,
                                                               const double* idu, const double* idv, int sweeps) {
-  using G = TileGeom<TJ, TI>;
+  constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
   extern __shared__ double sm[];
-  double *xu = sm, *xv = sm + G::N, *bu = sm + 2 * G::N, *bv = sm + 3 * G::N;
+  TileMem<TJ, TI, STAGE> m(sm, o, idu, idv);
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
-  const TIx ix{tj0 - kHalo, ti0 - kHalo, G::RJ};
+  const TIx ix{tj0 - kHalo, ti0 - kHalo, RJ};
   const bool deep = tile_deep<TJ, TI>(ix, d);
-  for (int t = threadIdx.x; t < G::N; t += blockDim.x) {
-    const int j = ix.j0 + t % G::RJ, i = ix.i0 + t / G::RJ;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    const int j = ix.j0 + t % RJ, i = ix.i0 + t / RJ;
     const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
+    const long long q = in ? d.at(j, i) : 0;
     double b0 = 0.0, b1 = 0.0;
     if (in) {
       if (rs.on) {
         restrict_values(rs.df, d, rs.fx, rs.fy, rs.ru, rs.rv, j, i, b0, b1);
       } else {
-        const long long q = d.at(j, i);
         b0 = gbu[q];
         b1 = gbv[q];
       }
     }
-    xu[t] = 0.0;
-    xv[t] = 0.0;
-    bu[t] = b0;
-    bv[t] = b1;
+    m.xu[t] = 0.0;
+    m.xv[t] = 0.0;
+    m.bu[t] = b0;
+    m.bv[t] = b1;
+    m.stage(o, idu, idv, ix, t, in, q);
   }
   __syncthreads();
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 0; p < 4; ++p, ++pass) {
-      tile_pass_any<TJ, TI>(deep, o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI, STAGE>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -502,41 +551,41 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
     if (j >= d.ny || i >= d.nx) continue;
     const long long q = d.at(j, i);
     const int k = ix(j, i);
-    gxu[q] = xu[k];
-    gxv[q] = xv[k];
+    gxu[q] = m.xu[k];
+    gxv[q] = m.xv[k];
     if (rs.on) {
-      gbu[q] = bu[k];
-      gbv[q] = bv[k];
+      gbu[q] = m.bu[k];
+      gbv[q] = m.bv[k];
     }
     if (deep) {
-      gru[q] = bu[k] - AuX<true>(o, xu, xv, ix, j, i);
-      grv[q] = bv[k] - AvX<true>(o, xu, xv, ix, j, i);
+      gru[q] = m.bu[k] - m.template Au<true>(ix, j, i);
+      grv[q] = m.bv[k] - m.template Av<true>(ix, j, i);
     } else {
-      gru[q] = u_int(d, j, i) ? bu[k] - AuX<false>(o, xu, xv, ix, j, i) : 0.0;
-      grv[q] = v_int(d, j, i) ? bv[k] - AvX<false>(o, xu, xv, ix, j, i) : 0.0;
+      gru[q] = u_int(d, j, i) ? m.bu[k] - m.template Au<false>(ix, j, i) : 0.0;
+      grv[q] = v_int(d, j, i) ? m.bv[k] - m.template Av<false>(ix, j, i) : 0.0;
     }
   }
 }
 
 // post-smoothing: x += P x_c, then `sweeps` backward sweeps (v1 v0 u1 u0); x of the tile
-template <int TJ, int TI>
+template <int TJ, int TI, bool STAGE>
 __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx, int fy, const double* xcu,
                                                             const double* xcv, const double* gbu, const double* gbv,
                                                             double* gxu, double* gxv, const double* idu,
                                                             const double* idv, int sweeps) {
-  using G = TileGeom<TJ, TI>;
+  constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
   extern __shared__ double sm[];
-  double *xu = sm, *xv = sm + G::N, *bu = sm + 2 * G::N, *bv = sm + 3 * G::N;
+  TileMem<TJ, TI, STAGE> m(sm, o, idu, idv);
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
-  const TIx ix{tj0 - kHalo, ti0 - kHalo, G::RJ};
+  const TIx ix{tj0 - kHalo, ti0 - kHalo, RJ};
   const bool deep = tile_deep<TJ, TI>(ix, d);
-  for (int t = threadIdx.x; t < G::N; t += blockDim.x) {
-    const int j = ix.j0 + t % G::RJ, i = ix.i0 + t / G::RJ;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    const int j = ix.j0 + t % RJ, i = ix.i0 + t / RJ;
     const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
+    const long long q = in ? d.at(j, i) : 0;
     double xa = 0.0, xb = 0.0, ba = 0.0, bb = 0.0;
     if (in) {
-      const long long q = d.at(j, i);
       double du, dv;
       prolong_delta(oc, d, fx, fy, xcu, xcv, j, i, du, dv);
       xa = gxu[q];
@@ -546,16 +595,17 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
       ba = gbu[q];
       bb = gbv[q];
     }
-    xu[t] = xa;
-    xv[t] = xb;
-    bu[t] = ba;
-    bv[t] = bb;
+    m.xu[t] = xa;
+    m.xv[t] = xb;
+    m.bu[t] = ba;
+    m.bv[t] = bb;
+    m.stage(o, idu, idv, ix, t, in, q);
   }
   __syncthreads();
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 3; p >= 0; --p, ++pass) {
-      tile_pass_any<TJ, TI>(deep, o, ix, xu, xv, bu, bv, idu, idv, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI, STAGE>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -563,8 +613,8 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
     if (j >= d.ny || i >= d.nx) continue;
     const long long q = d.at(j, i);
     const int k = ix(j, i);
-    gxu[q] = xu[k];
-    gxv[q] = xv[k];
+    gxu[q] = m.xu[k];
+    gxv[q] = m.xv[k];
   }
 }
 
@@ -1442,31 +1492,44 @@ static int tile_edge(const Ctx* c, int l) {
   return b32 >= 148 ? 32 : 16;
 }
 
-template <int T>
-static int vcycle_tiled_t(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
-                          const Restriction& rs, int nu1, int nu2) {
-  using G = TileGeom<T, T>;
+// Which tile kernels a level uses: the edge (tile_edge), and whether the region's
+// coefficients are staged in shared memory (16 x 16 tiles: 92 KB, two blocks per SM;
+// 32 x 32 tiles would need 200 KB, one block per SM, so they read the coefficients
+// from L2 instead).
+constexpr bool kStage16 = true, kStage32 = false;
+
+template <int T, bool S>
+static void tile_down_t(Ctx* c, int l, const Restriction& rs, const double* bu, const double* bv, double* xu,
+                        double* xv, int nu) {
+  const Level& L = c->lv[l];
+  const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
+  // b is written only when it is restricted here (rs.on), which never happens on the finest level
+  k_smooth_down<T, T, S><<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
+      make_op(c, l), rs, const_cast<double*>(bu), const_cast<double*>(bv), xu, xv, L.ru, L.rv, L.idu, L.idv, nu);
+  c->launches++;
+}
+template <int T, bool S>
+static void tile_up_t(Ctx* c, int l, int fx, int fy, const double* bu, const double* bv, double* xu, double* xv,
+                      int nu) {
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
-  const Op o = make_op(c, l);
-  // b is written only when it is restricted here (rs.on), which never happens on the finest level
-  k_smooth_down<T, T><<<grid, kTileThreads, G::smem, c->stream>>>(o, rs, const_cast<double*>(bu),
-                                                                   const_cast<double*>(bv), xu, xv, L.ru, L.rv,
-                                                                   L.idu, L.idv, nu1); c->launches++;
+  k_smooth_up<T, T, S><<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
+      make_op(c, l), make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, xu, xv, L.idu, L.idv, nu);
+  c->launches++;
+}
+static int tile_down(Ctx* c, int l, const Restriction& rs, const double* bu, const double* bv, double* xu,
+                     double* xv, int nu) {
+  if (tile_edge(c, l) == 32) tile_down_t<32, kStage32>(c, l, rs, bu, bv, xu, xv, nu);
+  else tile_down_t<16, kStage16>(c, l, rs, bu, bv, xu, xv, nu);
   DIVA_LAUNCHED(c, "k_smooth_down");
-  Restriction next;
-  next.on = 1;
-  next.df = L.d;
-  factors(c, l, &next.fx, &next.fy);
-  next.ru = L.ru;
-  next.rv = L.rv;
-  int st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv, next);
-  if (st) return st;
-  k_smooth_up<T, T><<<grid, kTileThreads, G::smem, c->stream>>>(o, make_op(c, l + 1), next.fx, next.fy, K.xu,
-                                                                 K.xv, bu, bv, xu, xv, L.idu, L.idv, nu2); c->launches++;
+  return DIVA_OK;
+}
+static int tile_up(Ctx* c, int l, int fx, int fy, const double* bu, const double* bv, double* xu, double* xv,
+                   int nu) {
+  if (tile_edge(c, l) == 32) tile_up_t<32, kStage32>(c, l, fx, fy, bu, bv, xu, xv, nu);
+  else tile_up_t<16, kStage16>(c, l, fx, fy, bu, bv, xu, xv, nu);
   DIVA_LAUNCHED(c, "k_smooth_up");
-  c->fine_passes += (nu1 + nu2 + 1) * (double)L.d.plane / (double)c->d.plane;
   return DIVA_OK;
 }
 
@@ -1475,8 +1538,20 @@ static int vcycle_tiled_t(Ctx* c, int l, double* xu, double* xv, const double* b
 static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
                         const Restriction& rs, int nu1, int nu2) {
   if (4 * nu1 > kHalo - 1 || 4 * nu2 > kHalo - 1) return set_error(c, DIVA_UNSUPPORTED, "tiled smoothing depth");
-  return tile_edge(c, l) == 32 ? vcycle_tiled_t<32>(c, l, xu, xv, bu, bv, rs, nu1, nu2)
-                               : vcycle_tiled_t<16>(c, l, xu, xv, bu, bv, rs, nu1, nu2);
+  const Level& L = c->lv[l];
+  const Level& K = c->lv[l + 1];
+  int st = tile_down(c, l, rs, bu, bv, xu, xv, nu1);
+  if (st) return st;
+  Restriction next;
+  next.on = 1;
+  next.df = L.d;
+  factors(c, l, &next.fx, &next.fy);
+  next.ru = L.ru;
+  next.rv = L.rv;
+  if ((st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv, next))) return st;
+  if ((st = tile_up(c, l, next.fx, next.fy, bu, bv, xu, xv, nu2))) return st;
+  c->fine_passes += (nu1 + nu2 + 1) * (double)L.d.plane / (double)c->d.plane;
+  return DIVA_OK;
 }
 
 // Shared-memory limits of the tiled kernels (the 32 x 32 tiles need 80 KB) and of
@@ -1534,10 +1609,14 @@ int solver_init(Ctx* c) {
   DIVA_CUDA(c, cudaFuncSetAttribute(k_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
-  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)TileGeom<32, 32>::smem));
-  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_up<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)TileGeom<32, 32>::smem));
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<32, 32, kStage32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TileGeom<32, 32, kStage32>::smem));
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_up<32, 32, kStage32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TileGeom<32, 32, kStage32>::smem));
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<16, 16, kStage16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TileGeom<16, 16, kStage16>::smem));
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_up<16, 16, kStage16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TileGeom<16, 16, kStage16>::smem));
   const BCs& b = c->bc;
   const int all[8] = {b.uW, b.uE, b.uS, b.uN, b.vW, b.vE, b.vS, b.vN};
   bool periodic = false;
@@ -1720,31 +1799,14 @@ int solver_relres(Ctx* c, const double* u, const double* v, double* relres) {
 // scratch vectors.
 int solver_smooth_fine(Ctx* c, int sweeps) {
   if (c->tiled && c->nlev > 1 && sub_first_level(c) > 0) {
-    const Level& L = c->lv[0];
-    const Level& K = c->lv[1];
     const int nu = 2;
     int fx, fy;
     factors(c, 0, &fx, &fy);
-    const Op o = make_op(c, 0);
     double *xu = c->kv[KV_X][0], *xv = c->kv[KV_X][1];
     double *bu = c->kv[KV_B][0], *bv = c->kv[KV_B][1];   // not written: the restriction is off
-    if (tile_edge(c, 0) == 32) {
-      using G = TileGeom<32, 32>;
-      const dim3 grid((L.d.ny + 31) / 32, (L.d.nx + 31) / 32);
-      k_smooth_down<32, 32><<<grid, kTileThreads, G::smem, c->stream>>>(o, Restriction{}, bu, bv, xu, xv, L.ru,
-                                                                         L.rv, L.idu, L.idv, nu); c->launches++;
-      k_smooth_up<32, 32><<<grid, kTileThreads, G::smem, c->stream>>>(o, make_op(c, 1), fx, fy, K.xu, K.xv, bu, bv,
-                                                                       xu, xv, L.idu, L.idv, nu); c->launches++;
-    } else {
-      using G = TileGeom<16, 16>;
-      const dim3 grid((L.d.ny + 15) / 16, (L.d.nx + 15) / 16);
-      k_smooth_down<16, 16><<<grid, kTileThreads, G::smem, c->stream>>>(o, Restriction{}, bu, bv, xu, xv, L.ru,
-                                                                         L.rv, L.idu, L.idv, nu); c->launches++;
-      k_smooth_up<16, 16><<<grid, kTileThreads, G::smem, c->stream>>>(o, make_op(c, 1), fx, fy, K.xu, K.xv, bu, bv,
-                                                                       xu, xv, L.idu, L.idv, nu); c->launches++;
-    }
-    DIVA_LAUNCHED(c, "fine-level tiled smoothing");
-    return DIVA_OK;
+    int st = tile_down(c, 0, Restriction{}, bu, bv, xu, xv, nu);
+    if (!st) st = tile_up(c, 0, fx, fy, bu, bv, xu, xv, nu);
+    return st;
   }
   for (int s = 0; s < sweeps; ++s) {
     int st = gs_sweep(c, 0, c->kv[KV_X][0], c->kv[KV_X][1], c->kv[KV_B][0], c->kv[KV_B][1], true);
