@@ -116,27 +116,22 @@ def marine_channel(seed=1, dx=5e3, zeta=ZETA):
     return grid, config, _fortran(fields)
 
 
-def ice_cap(seed=2, dx=5e3, zeta=ZETA):
-    """Config 2: 1600 x 2800 km ice cap (321 x 561 at 5 km).
-
-    Bed: Gaussian random field (correlation length ~150 km) rescaled to
-    [-500, 2500] m.  Surface: a smooth elliptical dome whose margin radius is
-    perturbed by a second random field; thickness = surface - bed, clipped to
-    [0, 3200] m, so margins are ragged where the bed rises through the dome.
-    Temperature 240-273 K; Weertman friction coefficient lognormal.
-    """
+def _dome(seed, dx, zeta, half_x, half_y, rx, ry, bed_corr, margin_corr, t_corr, s_max, h_max):
+    """A dome on Gaussian random topography (bed rescaled to [-500, 2500] m) whose margin
+    radius is perturbed by a second random field; thickness = surface - bed, clipped to
+    [0, h_max], so margins are ragged where the bed rises through the dome."""
     rng = np.random.default_rng(seed)
-    x, y = _axis(800e3, dx), _axis(1400e3, dx)
+    x, y = _axis(half_x, dx), _axis(half_y, dx)
     nx, ny = len(x), len(y)
     X, Y = np.meshgrid(x, y)
-    g = _grf(rng, ny, nx, dx, 150e3)
+    g = _grf(rng, ny, nx, dx, bed_corr)
     Hb = -500.0 + 3000.0 * (g - g.min()) / (g.max() - g.min())
-    r = np.sqrt((X / 760e3) ** 2 + (Y / 1340e3) ** 2)
-    rm = 1.0 + 0.05 * np.clip(_grf(rng, ny, nx, dx, 40e3), -2.0, 2.0)
-    Hs = 3400.0 * np.clip(1.0 - (r / rm) ** 2, 0.0, None)
-    H = np.clip(Hs - Hb, 0.0, 3200.0)
+    r = np.sqrt((X / rx) ** 2 + (Y / ry) ** 2)
+    rm = 1.0 + 0.05 * np.clip(_grf(rng, ny, nx, dx, margin_corr), -2.0, 2.0)
+    Hs = s_max * np.clip(1.0 - (r / rm) ** 2, 0.0, None)
+    H = np.clip(Hs - Hb, 0.0, h_max)
     H = np.where(Hs > 0.0, H, 0.0)
-    T = _temperature(rng, zeta, ny, nx, 240.0, 273.0, dx, 200e3)
+    T = _temperature(rng, zeta, ny, nx, 240.0, 273.0, dx, t_corr)
     fields = {
         "Hi_a": H, "Hb_a": Hb, "SL_a": np.zeros((ny, nx)), "dHb_dt_a": np.zeros((ny, nx)),
         "Ti_a": T, "beta_sq_a": _lognormal_friction(rng, ny, nx),
@@ -151,6 +146,44 @@ def ice_cap(seed=2, dx=5e3, zeta=ZETA):
     }
     grid = dict(nx=nx, ny=ny, dx=dx, zeta=zeta, xmin=x[0], ymin=y[0])
     return grid, config, _fortran(fields)
+
+
+def ice_cap(seed=2, dx=5e3, zeta=ZETA):
+    """Config 2: 1600 x 2800 km ice cap (321 x 561 at 5 km).
+
+    Bed correlation length ~150 km, dome 3400 m high, thickness at most 3200 m;
+    temperature 240-273 K; Weertman friction coefficient lognormal.
+    """
+    return _dome(seed, dx, zeta, 800e3, 1400e3, 760e3, 1340e3, 150e3, 40e3, 200e3, 3400.0, 3200.0)
+
+
+def ice_sheet(seed=5, dx=4e3, zeta=ZETA):
+    """Config 5's large member: a 6000 x 6000 km continental ice sheet (1501 x 1501 at
+    4 km), the same construction as the ice cap at continental scale (bed correlation
+    length ~300 km, dome 4200 m high, thickness at most 4000 m)."""
+    return _dome(seed, dx, zeta, 3000e3, 3000e3, 2850e3, 2850e3, 300e3, 80e3, 400e3, 4200.0, 4000.0)
+
+
+def ensemble(n=64, seed=0, sizes=("channel", "icecap", "sheet")):
+    """Config 5: n members with sizes drawn (seeded) from the marine channel (129 x 17),
+    the ice cap (321 x 561) and the continental sheet (1501 x 1501); per member the
+    friction coefficient is scaled by a log-uniform factor in [0.3, 3] and the flow
+    factor (through the enhancement factor) by one in [0.5, 2].  Returns a list of
+    (name, grid, config, fields)."""
+    rng = np.random.default_rng(seed)
+    gens = {"channel": marine_channel, "icecap": ice_cap, "sheet": ice_sheet}
+    out = []
+    for k in range(n):
+        kind = sizes[int(rng.integers(len(sizes)))]
+        fb = float(np.exp(rng.uniform(np.log(0.3), np.log(3.0))))
+        fa = float(np.exp(rng.uniform(np.log(0.5), np.log(2.0))))
+        g, cfg, f = gens[kind](seed=1000 + k)
+        f = dict(f)
+        if "beta_sq_a" in f:
+            f["beta_sq_a"] = np.asfortranarray(f["beta_sq_a"] * fb)
+        cfg = dict(cfg, m_enh_sheet=fa, m_enh_shelf=fa)
+        out.append((f"{kind}-{k}", g, cfg, f))
+    return out
 
 
 def schoof_icestream(dx=10e3, half_width=400e3, zeta=ZETA, A=1e-17, L=100e3, m=0.5,
@@ -182,4 +215,4 @@ def schoof_icestream(dx=10e3, half_width=400e3, zeta=ZETA, A=1e-17, L=100e3, m=0
     return grid, config, _fortran(fields)
 
 
-CONFIGS = {1: marine_channel, 2: ice_cap}
+CONFIGS = {1: marine_channel, 2: ice_cap, 5: ice_sheet}
