@@ -191,6 +191,7 @@ size_t carve(Ctx* c, Carver& cv) {
     L.idu = (double*)cv.take(pb); L.idv = (double*)cv.take(pb);
     L.xu = (double*)cv.take(pb); L.xv = (double*)cv.take(pb); L.bu = (double*)cv.take(pb); L.bv = (double*)cv.take(pb);
     L.ru = (double*)cv.take(pb); L.rv = (double*)cv.take(pb);
+    L.tu = (double*)cv.take(pb); L.tv = (double*)cv.take(pb);
   }
   return cv.off;
 }

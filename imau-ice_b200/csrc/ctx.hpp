@@ -18,6 +18,7 @@ struct Level {
   Dims d;
   double *Na, *Nb, *Bx, *By, *idu, *idv;
   double *xu, *xv, *bu, *bv, *ru, *rv;
+  double *tu, *tv;   // x after pre-smoothing (tiled levels): read over halos by the post-smoothing kernel
 };
 
 // Boundary condition codes of the velocity unknowns (diva_bc_t), per side.

@@ -567,12 +567,16 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
   }
 }
 
-// post-smoothing: x += P x_c, then `sweeps` backward sweeps (v1 v0 u1 u0); x of the tile
+// post-smoothing: x += P x_c, then `sweeps` backward sweeps (v1 v0 u1 u0); x of the tile.
+// The pre-smoothed x is read over the halo from (gxu, gxv) and the result written to
+// (oxu, oxv): separate arrays, since blocks of other tiles may still be reading the
+// halo when this block writes (the grid runs in several waves on large levels).
 template <int TJ, int TI, bool STAGE>
 __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx, int fy, const double* xcu,
                                                             const double* xcv, const double* gbu, const double* gbv,
-                                                            double* gxu, double* gxv, const double* idu,
-                                                            const double* idv, int sweeps) {
+                                                            const double* gxu, const double* gxv, double* oxu,
+                                                            double* oxv, const double* idu, const double* idv,
+                                                            int sweeps) {
   constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
   extern __shared__ double sm[];
   TileMem<TJ, TI, STAGE> m(sm, o, idu, idv);
@@ -613,8 +617,8 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
     if (j >= d.ny || i >= d.nx) continue;
     const long long q = d.at(j, i);
     const int k = ix(j, i);
-    gxu[q] = m.xu[k];
-    gxv[q] = m.xv[k];
+    oxu[q] = m.xu[k];
+    oxv[q] = m.xv[k];
   }
 }
 
@@ -1505,7 +1509,8 @@ static void tile_down_t(Ctx* c, int l, const Restriction& rs, const double* bu, 
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
   // b is written only when it is restricted here (rs.on), which never happens on the finest level
   k_smooth_down<T, T, S><<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
-      make_op(c, l), rs, const_cast<double*>(bu), const_cast<double*>(bv), xu, xv, L.ru, L.rv, L.idu, L.idv, nu);
+      make_op(c, l), rs, const_cast<double*>(bu), const_cast<double*>(bv), L.tu, L.tv, L.ru, L.rv, L.idu, L.idv,
+      nu);
   c->launches++;
 }
 template <int T, bool S>
@@ -1515,7 +1520,7 @@ static void tile_up_t(Ctx* c, int l, int fx, int fy, const double* bu, const dou
   const Level& K = c->lv[l + 1];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
   k_smooth_up<T, T, S><<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
-      make_op(c, l), make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, xu, xv, L.idu, L.idv, nu);
+      make_op(c, l), make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, L.tu, L.tv, xu, xv, L.idu, L.idv, nu);
   c->launches++;
 }
 static int tile_down(Ctx* c, int l, const Restriction& rs, const double* bu, const double* bv, double* xu,
