@@ -51,9 +51,9 @@ UNIT = "solves/s"
 INPUT_FIELDS = ["Hi_a", "Hb_a", "SL_a", "dHb_dt_a", "Ti_a", "beta_sq_a"]
 STATE_FIELDS = ["u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "taub_cx", "taub_cy", "u_3D_a", "v_3D_a"]
 OUTPUT_FIELDS = ["u_vav_cx", "v_vav_cy", "u_3D_cx", "v_3D_cy", "w_3D_a", "u_3D_SIA_cx", "v_3D_SIA_cy"]
-KERNEL_NAMES = {0: "k_column_coefficients", 1: "k_smooth_down+k_smooth_up (fine level)", 2: "k_matvec",
+KERNEL_NAMES = {0: "column coefficients (k_column_prep, k_layer_viscosity, k_column_integrals, k_face_coefficients)", 1: "k_smooth_down+k_smooth_up (fine level)", 2: "k_matvec",
                 3: "V-cycle (all levels)", 4: "k_subcycle (coarse levels, one block)"}
-TRAFFIC_KEYS = {0: "k_column_coefficients_icecap321x561", 1: "k_smooth_down_icecap321x561",
+TRAFFIC_KEYS = {0: "k_layer_viscosity_icecap321x561", 1: "k_smooth_down_icecap321x561",
                 4: "k_subcycle_icecap321x561"}
 
 

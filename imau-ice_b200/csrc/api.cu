@@ -172,6 +172,8 @@ size_t carve(Ctx* c, Carver& cv) {
   for (int q = 0; q < 4; ++q) c->quad[q] = (double*)cv.take(sizeof(double) * d.plane);
   for (int q = 0; q < 2; ++q) c->err_cand[q] = (double*)cv.take(sizeof(double) * d.plane);
   c->staging = (double*)cv.take(sizeof(double) * d.nz * d.plane);
+  c->col_eps = (double*)cv.take(sizeof(double) * d.plane);
+  c->col_flags = (int*)cv.take(sizeof(int) * d.plane);
   c->ff_ocean = (int*)cv.take(sizeof(int) * 2 * d.plane);
   c->ff_flag = (int*)cv.take(sizeof(int) * 4);
   c->scal = (double*)cv.take(sizeof(double) * SC_COUNT);

@@ -68,6 +68,8 @@ struct Ctx {
   double* quad[4] = {};               // grounded fractions of the four quadrants (NW, NE, SW, SE)
   double* err_cand[2] = {};           // DIVA_err candidates (cx, cy)
   double* staging = nullptr;          // upload/download staging (largest field)
+  double* col_eps = nullptr;          // column coefficients: mean-flow strain rate per column
+  int* col_flags = nullptr;           // column coefficients: shear faces with ice
   int* ff_ocean = nullptr;            // flood-fill state
   int* ff_flag = nullptr;
   double* scal = nullptr;             // device scalars (SC_*)

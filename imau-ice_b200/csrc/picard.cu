@@ -1,7 +1,8 @@
 // picard.cu -- the per-iteration physics of solve_DIVA / solve_SSA and the
 // velocity fields computed after the viscosity iteration.
 //
-//   K1 k_column_coefficients  calc_vertical_shear_strain_rates   ice_velocity_module.f90:664-721
+//   K1 k_column_prep, k_layer_viscosity, k_column_integrals
+//                             calc_vertical_shear_strain_rates   ice_velocity_module.f90:664-721
 //                             calc_effective_viscosity (a-grid)   :722-818
 //                             calc_sliding_term_beta + laws       :900-959, basal_conditions_and_sliding_module.f90:908-1236
 //                             calc_F_integral(n=2)                :960-1013
@@ -40,6 +41,9 @@ struct CoefArgs {
   const double *beta_sq, *phi_fric, *alpha_sq, *Neff, *Ti, *Tpmp;
   // outputs
   double *dudz, *dvdz, *visc, *visc_int, *Na, *beta, *F2, *beta_eff, *tauc;
+  // per-column scratch between the three launches
+  double* col_eps;
+  int* col_flags;
 };
 
 // strain rates of the depth-averaged velocity on the a-grid,
@@ -110,113 +114,142 @@ __device__ __forceinline__ double sliding_beta(const CoefArgs& a, long long q, d
   return CUDART_NAN;
 }
 
-// One thread per column, a warp over 32 neighbouring rows j of one grid column i.
-// The 2D inputs of the column's four shear faces are read once, before the layer
-// loop; each layer loads the previous viscosity once per point (centre, east,
-// north, west) and the A-factor, and the north face of the lane below is this
-// lane's south face (shuffle), so a layer costs three face divisions.
+// K1 in three launches.  (a) k_column_prep, one thread per column: the strain rates
+// of the depth-averaged flow and which of the column's four shear faces have ice.
+// (b) k_layer_viscosity, one thread per (column, layer), a warp over 32 neighbouring
+// rows j of one grid column i and one layer: the shear of the column's own east and
+// north faces (written), the west face, and the south face as the north face of the
+// lane below (shuffle), then the viscosity of the layer.  (c) k_column_integrals, one
+// thread per column: the vertical integrals in layer order (as the sequential
+// quadrature does), N_a, the sliding law, F2 and beta_eff.  The split costs one more
+// read of the viscosity and buys a layer-parallel, dependency-free middle step.
 constexpr int kColLanes = 32, kColRows = 4;
 
-struct FaceIn {
-  bool act;        // ice on at least one side (:685-695)
-  double H0, H1;   // thickness either side, for the staggered margin viscosity
-  double tb;       // basal stress on the face
-};
-__device__ __forceinline__ FaceIn face_in(bool has, const int* __restrict__ mask, const double* __restrict__ Hi,
-                                          const double* __restrict__ taub, long long p0, long long p1) {
-  FaceIn f{false, 0.0, 0.0, 0.0};
-  if (!has) return f;
-  f.act = !(mask[p0] == 0 && mask[p1] == 0);
-  f.H0 = Hi[p0];
-  f.H1 = Hi[p1];
-  f.tb = taub[p0];
-  return f;
+// Per-column decisions of the layer step, packed by k_column_prep:
+//   bits 0-3   the E, W, N, S shear face carries ice (FACE_*)
+//   bits 4-11  per face, which side the staggered viscosity takes (calc_staggered_margin
+//              :1300-1319): 0 the mean of both, 1 the first (west/south) side, 2 the second
+//   bits 12-15 the same choice for the column's own x and y staggering of du/dz, dv/dz,
+//              including the first/last grid column and row, which take one face only
+//   bit 16     no viscosity in this column (BC margins outside the ice)
+enum { FACE_E = 1, FACE_W = 2, FACE_N = 4, FACE_S = 8, COL_SKIP = 1 << 16 };
+constexpr int kModeShift = 4, kStagXShift = 12, kStagYShift = 14;
+
+__device__ __forceinline__ int margin_mode(double H0, double H1) {
+  if (H0 > 0.0 && H1 == 0.0) return 1;
+  if (H0 == 0.0 && H1 > 0.0) return 2;
+  return 0;
 }
-// du/dz on a face in one layer: (taub / staggered viscosity) * zeta
-__device__ __forceinline__ double face_dz(const FaceIn& f, double v0, double v1, double zk) {
-  if (!f.act) return 0.0;
-  const double vc = stag_margin(v0, v1, f.H0, f.H1);
-  return (f.tb / vc) * zk;
+// calc_staggered_margin with the side choice made beforehand (same values as stag_margin)
+__device__ __forceinline__ double stag_mode(int mode, double v0, double v1) {
+  return mode == 1 ? v0 : (mode == 2 ? v1 : 0.5 * (v0 + v1));
 }
 
-__global__ void __launch_bounds__(kColLanes * kColRows, 6) k_column_coefficients(CoefArgs a) {
+__global__ void __launch_bounds__(256) k_column_prep(CoefArgs a) {
   const Dims d = a.d;
-  const int lane = threadIdx.x;
-  const int j = blockIdx.x * kColLanes + lane, i = blockIdx.y * kColRows + threadIdx.y;
-  if (i >= d.nx) return;       // whole warps: i is uniform across a warp
-  const bool col = j < d.ny;   // lanes past the last row stay for the shuffles
-  const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const long long q = d.at(col ? j : ny - 1, i);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= d.ny || i >= d.nx) return;
+  const int nx = d.nx, ny = d.ny;
+  const long long q = d.at(j, i);
   const int* __restrict__ mask = a.mask_ice;
   const double* __restrict__ Hi = a.Hi;
-  const double* __restrict__ vp = a.visc_prev;
-  const double* __restrict__ afac = a.afac;
-  double* __restrict__ visc = a.visc;
-  double* __restrict__ dudz = a.dudz;
-  double* __restrict__ dvdz = a.dvdz;
-  const double H = Hi[q];
   const bool ice = mask[q] == 1;
   const bool skip_visc = a.bc_margin && !ice;  // BC margins: no viscosity outside the ice (:759-764)
   // strain rates of the depth-averaged flow (calc_effective_viscosity :751-754)
   double eps_h = 0.0;
-  if (col && !skip_visc) {
+  if (!skip_visc) {
     const double du_dx = ddx_cx_to_a(d, a.u, j, i), dv_dy = ddy_cy_to_a(d, a.v, j, i);
     const double du_dy = ddy_cx_to_a(d, a.u, j, i), dv_dx = ddx_cy_to_a(d, a.v, j, i);
     eps_h = du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((du_dy + dv_dx) * (du_dy + dv_dx));
   }
-  // the faces of the column (calc_vertical_shear_strain_rates :685-721); a column on
-  // the last row/column uses the face before it alone
+  const double H = Hi[q];
+  int flags = skip_visc ? COL_SKIP : 0;
+  auto face = [&](int bit, int f, long long p0, long long p1) {
+    // a face carries shear if either side has ice (calc_vertical_shear_strain_rates :685-695)
+    if (a.diva && !(mask[p0] == 0 && mask[p1] == 0)) flags |= bit;
+    flags |= margin_mode(Hi[p0], Hi[p1]) << (kModeShift + 2 * f);
+  };
+  if (i < nx - 1) face(FACE_E, 0, q, d.at(j, i + 1));
+  if (i > 0) face(FACE_W, 1, d.at(j, i - 1), q);
+  if (j < ny - 1) face(FACE_N, 2, q, d.at(j + 1, i));
+  if (j > 0) face(FACE_S, 3, d.at(j - 1, i), q);
+  // a-grid staggering of the face values: first column/row the east/north face alone (2),
+  // last column/row the west/south face alone (1), else the margin rule
+  const int mx = i == 0 ? 2 : (i == nx - 1 ? 1 : margin_mode(Hi[d.at(j, i - 1)], H));
+  const int my = j == 0 ? 2 : (j == ny - 1 ? 1 : margin_mode(Hi[d.at(j - 1, i)], H));
+  flags |= (mx << kStagXShift) | (my << kStagYShift);
+  a.col_eps[q] = eps_h;
+  a.col_flags[q] = flags;
+}
+
+__global__ void __launch_bounds__(kColLanes * kColRows) k_layer_viscosity(CoefArgs a) {
+  const Dims d = a.d;
+  const int lane = threadIdx.x;
+  // the layer is the fastest grid index: blocks running together share their columns'
+  // 2D inputs in L1/L2 instead of streaming them once per layer
+  const int k = blockIdx.x, j = blockIdx.y * kColLanes + lane, i = blockIdx.z * kColRows + threadIdx.y;
+  if (i >= d.nx) return;       // whole warps: i is uniform across a warp
+  const bool col = j < d.ny;   // lanes past the last row stay for the shuffle
+  const int nx = d.nx, ny = d.ny, ld = d.ld;
+  const int q = i * ld + (col ? j : ny - 1);   // plane index (planes hold < 2^31 points)
+  const long long off = (long long)k * d.plane;
+  const double* __restrict__ vp = a.visc_prev + off;
+  const double zk = a.zt.z[k];
+  const int flags = a.col_flags[q];
   const bool has_e = col && i < nx - 1, has_w = col && i > 0, has_n = col && j < ny - 1, has_s = col && j > 0;
-  const long long qe = has_e ? d.at(j, i + 1) : q, qw = has_w ? d.at(j, i - 1) : q;
-  const long long qn = has_n ? d.at(j + 1, i) : q, qs = has_s ? d.at(j - 1, i) : q;
-  const FaceIn fe = face_in(a.diva && has_e, mask, Hi, a.taub_cx, q, qe);
-  const FaceIn fw = face_in(a.diva && has_w, mask, Hi, a.taub_cx, qw, q);
-  const FaceIn fn = face_in(a.diva && has_n, mask, Hi, a.taub_cy, q, qn);
-  const FaceIn fs = face_in(a.diva && has_s && lane == 0, mask, Hi, a.taub_cy, qs, q);
-  const double Hw = has_w ? Hi[qw] : 0.0, Hs = has_s ? Hi[qs] : 0.0;
+  auto mode = [&](int f) { return (flags >> (kModeShift + 2 * f)) & 3; };
+  double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0, dudz_w = 0.0;
+  if (a.diva) {
+    const double vq = vp[q];
+    if (has_e) {
+      if (flags & FACE_E) dudz_e = (a.taub_cx[q] / stag_mode(mode(0), vq, vp[q + ld])) * zk;
+      a.dudz[off + q] = dudz_e;
+    }
+    if (has_n) {
+      if (flags & FACE_N) dvdz_n = (a.taub_cy[q] / stag_mode(mode(2), vq, vp[q + 1])) * zk;
+      a.dvdz[off + q] = dvdz_n;
+    }
+    if (has_w && (flags & FACE_W)) dudz_w = (a.taub_cx[q - ld] / stag_mode(mode(1), vp[q - ld], vq)) * zk;
+    dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
+    if (lane == 0 && has_s)
+      dvdz_s = (flags & FACE_S) ? (a.taub_cy[q - 1] / stag_mode(mode(3), vp[q - 1], vq)) * zk : 0.0;
+  }
+  if (!col) return;
+  double eta = 0.0;
+  if (!(flags & COL_SKIP)) {
+    const int mx = (flags >> kStagXShift) & 3, my = (flags >> kStagYShift) & 3;
+    double du_dz_a, dv_dz_a;
+    if (a.diva) {
+      du_dz_a = stag_mode(mx, dudz_w, dudz_e);
+      dv_dz_a = stag_mode(my, dvdz_s, dvdz_n);
+    } else {
+      // solve_SSA calls calc_effective_viscosity without refreshing du/dz: use the stored fields
+      const double* dudz = a.dudz + off;
+      const double* dvdz = a.dvdz + off;
+      du_dz_a = stag_mode(mx, i > 0 ? dudz[q - ld] : 0.0, i < nx - 1 ? dudz[q] : 0.0);
+      dv_dz_a = stag_mode(my, j > 0 ? dvdz[q - 1] : 0.0, j < ny - 1 ? dvdz[q] : 0.0);
+    }
+    const double eps_sq = a.col_eps[q] + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
+    const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
+    eta = max_ref(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
+  }
+  a.visc[off + q] = eta;
+}
+
+__global__ void __launch_bounds__(256) k_column_integrals(CoefArgs a) {
+  const Dims d = a.d;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= d.ny || i >= d.nx) return;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const long long q = d.at(j, i);
+  const double H = a.Hi[q];
+  const bool ice = a.mask_ice[q] == 1;
+  const bool skip_visc = a.bc_margin && !ice;
+  const double* __restrict__ visc = a.visc;
   double vint = 0.0, fint = 0.0, vprev = 0.0, fprev = 0.0;
   for (int k = 0; k < nz; ++k) {
-    const long long off = (long long)k * d.plane;
+    const double eta = visc[(long long)k * d.plane + q];
     const double zk = a.zt.z[k];
-    double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0, dudz_w = 0.0;
-    if (a.diva) {
-      const double vq = vp[off + q];
-      if (has_e) {
-        dudz_e = face_dz(fe, vq, vp[off + qe], zk);
-        dudz[off + q] = dudz_e;
-      }
-      if (has_n) {
-        dvdz_n = face_dz(fn, vq, vp[off + qn], zk);
-        dvdz[off + q] = dvdz_n;
-      }
-      if (has_w) dudz_w = face_dz(fw, vp[off + qw], vq, zk);
-      dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
-      if (lane == 0 && has_s) dvdz_s = face_dz(fs, vp[off + qs], vq, zk);
-    }
-    double eta = 0.0;
-    if (col && !skip_visc) {
-      double du_dz_a = 0.0, dv_dz_a = 0.0;
-      if (a.diva) {
-        if (i == 0) du_dz_a = dudz_e;
-        else if (i == nx - 1) du_dz_a = dudz_w;
-        else du_dz_a = stag_margin(dudz_w, dudz_e, Hw, H);
-        if (j == 0) dv_dz_a = dvdz_n;
-        else if (j == ny - 1) dv_dz_a = dvdz_s;
-        else dv_dz_a = stag_margin(dvdz_s, dvdz_n, Hs, H);
-      } else {
-        // solve_SSA calls calc_effective_viscosity without refreshing du/dz: use the stored fields
-        if (i == 0) du_dz_a = dudz[off + d.at(j, 0)];
-        else if (i == nx - 1) du_dz_a = dudz[off + d.at(j, nx - 2)];
-        else du_dz_a = stag_margin(dudz[off + qw], dudz[off + q], Hw, H);
-        if (j == 0) dv_dz_a = dvdz[off + d.at(0, i)];
-        else if (j == ny - 1) dv_dz_a = dvdz[off + d.at(ny - 2, i)];
-        else dv_dz_a = stag_margin(dvdz[off + qs], dvdz[off + q], Hs, H);
-      }
-      const double eps_sq = eps_h + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
-      const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
-      eta = max_ref(afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
-    }
-    if (col) visc[off + q] = eta;
     if (k > 0) vint = vint + 0.5 * (eta + vprev) * (zk - a.zt.z[k - 1]);
     vprev = eta;
     if (a.diva) {
@@ -225,7 +258,6 @@ __global__ void __launch_bounds__(kColLanes * kColRows, 6) k_column_coefficients
       fprev = fk;
     }
   }
-  if (!col) return;
   if (!skip_visc) {
     a.visc_int[q] = vint;
     a.Na[q] = a.bc_margin ? vint * H : vint * max_ref(0.1, H);
@@ -832,12 +864,16 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
     DIVA_CUDA(c, cudaMemcpyAsync(c->D(DIVA_F_VISC_EFF_3D_A), c->visc_prev, sizeof(double) * c->d.plane * c->d.nz,
                                  cudaMemcpyDeviceToDevice, c->stream));
   }
+  a.col_eps = c->col_eps;
+  a.col_flags = c->col_flags;
+  k_column_prep<<<G2>>>(a); c->launches++;
   {
     const dim3 block(kColLanes, kColRows);
-    const dim3 grid((c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
-    k_column_coefficients<<<grid, block, 0, c->stream>>>(a); c->launches++;
+    const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
+    k_layer_viscosity<<<grid, block, 0, c->stream>>>(a); c->launches++;
   }
-  DIVA_LAUNCHED(c, "k_column_coefficients");
+  k_column_integrals<<<G2>>>(a); c->launches++;
+  DIVA_LAUNCHED(c, "column coefficients");
   FaceArgs fa{};
   fa.d = c->d;
   fa.zt = c->zt;
