@@ -667,7 +667,7 @@ int diva_state_restore(diva_ctx_t* h) {
 }
 
 int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, double* bytes) {
-  if (!h || !ms || !bytes || reps < 1 || which < 0 || which > 4) return DIVA_BAD_INPUT;
+  if (!h || !ms || !bytes || reps < 1 || which < 0 || which > 5) return DIVA_BAD_INPUT;
   Ctx* c = &h->c;
   const double nc = (double)c->d.nx * c->d.ny, w = sizeof(double), nz = c->d.nz;
   int st = DIVA_OK;
@@ -679,6 +679,7 @@ int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, 
       case 2: st = solver_matvec_fine(c, 1); break;
       case 3: st = solver_vcycle_fine(c, 1); break;
       case 4: st = solver_subcycle(c, 1); break;
+      case 5: st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true, true); break;
     }
   }
   if (st) return st;
@@ -695,7 +696,10 @@ int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, 
   //  3: one V-cycle: per level 4 sweeps, a residual and the transfers, weighted by its points
   //  4: the one-block coarse levels of a V-cycle (latency-bound; bytes as for 3 over those levels)
   const double per_col[3] = {(3 * nz + 15) * w, solver_smooth_fine_values(c) * w, 8 * w};
-  *bytes = which < 3 ? per_col[which] * nc : (which == 3 ? solver_vcycle_bytes(c) : 0.0);
+  //  5: the layer-parallel viscosity step alone: previous viscosity and A-factor read, viscosity
+  //     and the two shear fields written (5 nz)
+  *bytes = which < 3 ? per_col[which] * nc
+                     : (which == 3 ? solver_vcycle_bytes(c) : (which == 5 ? 5 * nz * w * nc : 0.0));
   return DIVA_OK;
 }
 

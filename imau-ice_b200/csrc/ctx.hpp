@@ -130,7 +130,7 @@ int launch_sico_masks(Ctx* c);
 
 // picard.cu
 int launch_prepare_afac(Ctx* c);
-int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva);
+int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva, bool layer_only = false);
 int launch_picard_update(Ctx* c, double* u, double* v, const double* xu, const double* xv, bool diva);
 int launch_commit_err(Ctx* c);
 int launch_basal_stress_velocities(Ctx* c);

@@ -812,7 +812,7 @@ int launch_prepare_afac(Ctx* c) {
   return DIVA_OK;
 }
 
-int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva) {
+int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva, bool layer_only) {
   const diva_config_t& C = c->c;
   // Picard double buffering of visc_eff_3D_a: read the previous, write the new
   std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
@@ -866,11 +866,17 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
   }
   a.col_eps = c->col_eps;
   a.col_flags = c->col_flags;
-  k_column_prep<<<G2>>>(a); c->launches++;
+  if (!layer_only) {
+    k_column_prep<<<G2>>>(a); c->launches++;
+  }
   {
     const dim3 block(kColLanes, kColRows);
     const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
     k_layer_viscosity<<<grid, block, 0, c->stream>>>(a); c->launches++;
+  }
+  if (layer_only) {   // timing of the layer step alone (diva_profile_kernel), per-column data of the last call
+    DIVA_LAUNCHED(c, "k_layer_viscosity");
+    return DIVA_OK;
   }
   k_column_integrals<<<G2>>>(a); c->launches++;
   DIVA_LAUNCHED(c, "column coefficients");

@@ -208,10 +208,11 @@ int  diva_state_restore(diva_ctx_t* ctx);
  *   2  one fine-level operator application (matrix-free A x with dot products)
  *   3  one multigrid V-cycle (the preconditioner of one Krylov half-step)
  *   4  the one-block coarse-level part of a V-cycle alone
+ *   5  the layer-parallel viscosity step of 0 alone (k_layer_viscosity)
  * `reps` launches are bracketed by CUDA events on the context's stream;
  * returns the mean device time per launch and the algorithmic bytes one launch
  * must move.  Needs a context that has completed a solve; kind 0 leaves the
- * coefficient fields of the next viscosity iteration behind, kinds 1-4 touch
+ * coefficient fields of the next viscosity iteration behind (5 too), kinds 1-4 touch
  * only solver scratch vectors. */
 int  diva_profile_kernel(diva_ctx_t* ctx, int32_t which, int32_t reps, double* ms_per_launch,
                          double* bytes_per_launch);
