@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 #include <string>
 #include "ctx.hpp"
 
@@ -235,54 +236,90 @@ int fill_const(Ctx* c, double* p, double v) {
 // The viscosity iteration as one graph launch per iteration (see solver.cu):
 // the Krylov loop and the skip of a converged iteration run on the device;
 // the host reads one status block per iteration and mirrors the viscosity
-// buffer swap the graph performed.
-int picard_graph(Ctx* c, bool diva, diva_report_t* rep) {
-  const diva_config_t& C = c->c;
-  const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
-  PicardGraphs& G = c->graphs[diva ? 1 : 0];
+// buffer swap the graph performed.  In steps, so that a batch of contexts can
+// keep one iteration of each in flight on its own stream (diva_solve_diva_batch).
+struct GraphLoop {
+  bool diva = true;
+  int it = 0;
+  double resid = 0.0, relres = -1.0;
+  bool by_relres = false, done = false;
+};
+
+int graph_loop_begin(Ctx* c, GraphLoop& L) {
   double init[SC_COUNT - SC_TARGET2] = {};
   init[SC_RELRES - SC_TARGET2] = -1.0;
   DIVA_CUDA(c, cudaMemcpyAsync(c->scal + SC_TARGET2, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
-  int it = 0;
-  double resid = 0.0, relres = -1.0;
-  bool by_relres = false;
-  for (;;) {
-    int parity;
-    if (c->f[DIVA_F_VISC_EFF_3D_A] == G.visc_buf[0]) parity = 0;
-    else if (c->f[DIVA_F_VISC_EFF_3D_A] == G.visc_buf[1]) parity = 1;
-    else return set_error(c, DIVA_CUDA_ERROR, "viscosity buffers out of step with the captured graphs");
-    DIVA_CUDA(c, cudaGraphLaunch(G.exec[parity], c->stream));
-    std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
-    DIVA_CUDA(c, cudaMemcpyAsync(c->h_scal + SC_TARGET2, c->scal + SC_TARGET2,
-                                 sizeof(double) * (SC_COUNT - SC_TARGET2), cudaMemcpyDeviceToHost, c->stream));
-    DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
-    const double* h = c->h_scal;
-    it = (int)h[SC_PIC_IT];
-    const bool solved = h[SC_SOLVED] != 0.0;
-    const long lin = (long)h[SC_LIN_IT], full = (long)h[SC_LIN_FULL];
-    c->lin_iters += lin;
-    c->mg_cycles += lin + full;
-    c->launches += G.n_pre + G.n_post + (solved ? G.n_head + G.n_tail + lin * G.n_first + full * G.n_second : 0);
-    c->fine_passes += G.p_pre + (solved ? G.p_head + G.p_tail + lin * G.p_first + full * G.p_second : 0.0);
-    relres = h[SC_RELRES];
-    if (h[SC_NAN] != 0.0) return set_error(c, DIVA_NAN_DETECTED, "NaN in the viscosity iteration");
-    if (h[SC_EXIT_RELRES] != 0.0) { by_relres = true; break; }
-    resid = h[SC_RESID];
-    if (h[SC_CONVERGED] != 0.0) break;
-    if (it > C.DIVA_visc_it_nit + 1) return set_error(c, DIVA_TIMEOUT, "viscosity iteration did not stop");
+  L.it = 0; L.resid = 0.0; L.relres = -1.0; L.by_relres = false; L.done = false;
+  return DIVA_OK;
+}
+
+// enqueue one iteration and the copy of its status block (pinned host mirror)
+int graph_loop_launch(Ctx* c, GraphLoop& L) {
+  PicardGraphs& G = c->graphs[L.diva ? 1 : 0];
+  int parity;
+  if (c->f[DIVA_F_VISC_EFF_3D_A] == G.visc_buf[0]) parity = 0;
+  else if (c->f[DIVA_F_VISC_EFF_3D_A] == G.visc_buf[1]) parity = 1;
+  else return set_error(c, DIVA_CUDA_ERROR, "viscosity buffers out of step with the captured graphs");
+  DIVA_CUDA(c, cudaGraphLaunch(G.exec[parity], c->stream));
+  std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
+  DIVA_CUDA(c, cudaMemcpyAsync(c->h_scal + SC_TARGET2, c->scal + SC_TARGET2,
+                               sizeof(double) * (SC_COUNT - SC_TARGET2), cudaMemcpyDeviceToHost, c->stream));
+  return DIVA_OK;
+}
+
+// wait for the iteration launched last and account for it; L.done when the loop stops
+int graph_loop_collect(Ctx* c, GraphLoop& L) {
+  const diva_config_t& C = c->c;
+  PicardGraphs& G = c->graphs[L.diva ? 1 : 0];
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  const double* h = c->h_scal;
+  L.it = (int)h[SC_PIC_IT];
+  const bool solved = h[SC_SOLVED] != 0.0;
+  const long lin = (long)h[SC_LIN_IT], full = (long)h[SC_LIN_FULL];
+  c->lin_iters += lin;
+  c->mg_cycles += lin + full;
+  c->launches += G.n_pre + G.n_post + (solved ? G.n_head + G.n_tail + lin * G.n_first + full * G.n_second : 0);
+  c->fine_passes += G.p_pre + (solved ? G.p_head + G.p_tail + lin * G.p_first + full * G.p_second : 0.0);
+  L.relres = h[SC_RELRES];
+  if (h[SC_NAN] != 0.0) return set_error(c, DIVA_NAN_DETECTED, "NaN in the viscosity iteration");
+  if (h[SC_EXIT_RELRES] != 0.0) {
+    L.by_relres = true;
+    L.done = true;
+    return DIVA_OK;
   }
+  L.resid = h[SC_RESID];
+  if (h[SC_CONVERGED] != 0.0) L.done = true;
+  else if (L.it > C.DIVA_visc_it_nit + 1) return set_error(c, DIVA_TIMEOUT, "viscosity iteration did not stop");
+  return DIVA_OK;
+}
+
+int graph_loop_end(Ctx* c, const GraphLoop& L, diva_report_t* rep) {
+  const diva_config_t& C = c->c;
+  const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
   int status = DIVA_OK;
-  if (!by_relres && it >= C.DIVA_visc_it_nit && (relmode || resid >= C.DIVA_visc_it_norm_dUV_tol))
+  if (!L.by_relres && L.it >= C.DIVA_visc_it_nit && (relmode || L.resid >= C.DIVA_visc_it_norm_dUV_tol))
     status = DIVA_MAX_PICARD;
   if (rep) {
-    rep->picard_iterations = it;
-    rep->resid_UV = resid;
-    rep->relres = relres;
+    rep->picard_iterations = L.it;
+    rep->resid_UV = L.resid;
+    rep->relres = L.relres;
     rep->status = status;
     rep->reserved[0] = (int32_t)c->h_scal[SC_LIN_FAILED];
     rep->reserved[1] = 1;   // graph-launched
   }
   return status;
+}
+
+int picard_graph(Ctx* c, bool diva, diva_report_t* rep) {
+  GraphLoop L;
+  L.diva = diva;
+  int st = graph_loop_begin(c, L);
+  while (!st && !L.done) {
+    if ((st = graph_loop_launch(c, L))) break;
+    st = graph_loop_collect(c, L);
+  }
+  if (st) return st;
+  return graph_loop_end(c, L, rep);
 }
 
 // the viscosity iteration shared by solve_SSA (:180-240) and solve_DIVA (:307-363)
@@ -601,6 +638,99 @@ int diva_solve_diva(diva_ctx_t* h, diva_report_t* rep) {
   if ((st = launch_secondary_velocities(c))) return st;
   if ((st = finish(c, rep))) return st;
   return pst;
+}
+
+// solve_DIVA for several contexts at once.  Each context runs on its own stream; one
+// viscosity iteration of every unfinished context is kept in flight, so the
+// iterations of different members overlap on the GPU.  A context that cannot use
+// graph-launched iterations (graph construction unavailable) is solved on its own
+// after the others.  reports[k] receives the report of ctxs[k]; the return value is
+// DIVA_OK if every member returned OK, else the first other status.
+int diva_solve_diva_batch(diva_ctx_t** hs, int32_t n, diva_report_t* reports) {
+  if (!hs || n < 1 || !reports) return DIVA_BAD_INPUT;
+  for (int k = 0; k < n; ++k) {
+    if (!hs[k]) return DIVA_BAD_INPUT;
+    for (int m = 0; m < k; ++m)
+      if (hs[m] == hs[k]) return set_error(&hs[k]->c, DIVA_BAD_INPUT, "a context appears twice in the batch");
+  }
+  std::vector<int> status(n, DIVA_OK);
+  std::vector<GraphLoop> loops(n);
+  std::vector<char> active(n, 0), sequential(n, 0);
+  // set-up of every member up to its first iteration
+  for (int k = 0; k < n; ++k) {
+    Ctx* c = &hs[k]->c;
+    diva_report_t* rep = &reports[k];
+    memset(rep, 0, sizeof(*rep));
+    rep->relres = -1.0;
+    int st = DIVA_OK;
+    if (c->c.choice_ice_dynamics != DIVA_DYN_DIVA) {
+      st = set_error(c, DIVA_BAD_INPUT, "solve_DIVA should only be called when choice_ice_dynamics is DIVA");
+    } else if (c->c.choice_ice_margin == DIVA_MARGIN_BC) {
+      st = set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
+    } else if (!(st = begin(c))) {
+      int any = 0;
+      if (!(st = launch_any_sheet(c, &any))) {
+        if (!any) {
+          if (!(st = launch_zero_velocities(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY)))) st = finish(c, rep);
+        } else if (!(st = prepare_velocity_solve(c))) {
+          if (!c->graphs_disabled && solver_build_picard_graphs(c, true) == DIVA_OK) {
+            loops[k].diva = true;
+            if (!(st = graph_loop_begin(c, loops[k]))) active[k] = 1;
+          } else {
+            c->graphs_disabled = true;
+            sequential[k] = 1;
+          }
+        }
+      }
+    }
+    status[k] = st;
+    if (st) rep->status = st;
+  }
+  // iterations: launch one of every active member, then collect them in turn
+  for (;;) {
+    bool any = false;
+    for (int k = 0; k < n; ++k)
+      if (active[k]) {
+        int st = graph_loop_launch(&hs[k]->c, loops[k]);
+        if (st) { status[k] = st; active[k] = 0; reports[k].status = st; }
+        else any = true;
+      }
+    if (!any) break;
+    for (int k = 0; k < n; ++k)
+      if (active[k]) {
+        int st = graph_loop_collect(&hs[k]->c, loops[k]);
+        if (st) { status[k] = st; active[k] = 0; reports[k].status = st; }
+        else if (loops[k].done) {
+          active[k] = 0;
+          status[k] = graph_loop_end(&hs[k]->c, loops[k], &reports[k]);
+          Ctx* c = &hs[k]->c;
+          int s2;
+          if ((s2 = launch_visc_b_output(c)) || (s2 = launch_3d_horizontal_velocities(c)) ||
+              (s2 = launch_secondary_velocities(c)) || (s2 = finish(c, &reports[k]))) {
+            status[k] = s2;
+          }
+          reports[k].status = status[k];
+        }
+      }
+  }
+  // members without graph-launched iterations
+  for (int k = 0; k < n; ++k)
+    if (sequential[k]) {
+      Ctx* c = &hs[k]->c;
+      const int pst = picard(c, true, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), &reports[k]);
+      int st = pst;
+      if (pst == DIVA_OK || pst == DIVA_MAX_PICARD) {
+        int s2;
+        if ((s2 = launch_visc_b_output(c)) || (s2 = launch_3d_horizontal_velocities(c)) ||
+            (s2 = launch_secondary_velocities(c)) || (s2 = finish(c, &reports[k])))
+          st = s2;
+      }
+      status[k] = st;
+      reports[k].status = st;
+    }
+  for (int k = 0; k < n; ++k)
+    if (status[k] != DIVA_OK) return status[k];
+  return DIVA_OK;
 }
 
 int diva_solve_ssa(diva_ctx_t* h, diva_report_t* rep) {

@@ -304,6 +304,33 @@ def solve_SSA(grid, ice, config=None, backend=None):
     return _run(grid, ice, config, backend, "solve_SSA", OUT_SSA)
 
 
+def solve_DIVA_batch(contexts):
+    """solve_DIVA for several contexts at once (diva_solve_diva_batch): each on its own
+    stream, one viscosity iteration of every unfinished member in flight, so small
+    members share the GPU.  Returns the reports in order; raises DivaError naming the
+    first member whose status is neither OK nor MAX_PICARD."""
+    if not contexts:
+        return []
+    be = contexts[0].backend
+    if any(c.backend is not be for c in contexts):
+        raise DivaError(_abi.BAD_INPUT, "all contexts of a batch must use the same backend")
+    f = getattr(be.lib, be.prefix + "solve_diva_batch", None)
+    if f is None:
+        raise DivaError(_abi.UNSUPPORTED, f"{be.name} backend has no batched solve")
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(_abi.Report)]
+    n = len(contexts)
+    hs = (C.c_void_p * n)(*[c.h for c in contexts])
+    reps = (_abi.Report * n)()
+    f(hs, n, reps)
+    out = [r.as_dict() for r in reps]
+    for k, (c, r) in enumerate(zip(contexts, out)):
+        if r["status"] not in (0, _abi.MAX_PICARD):
+            err = be.fns["last_error"](c.h)
+            raise DivaError(r["status"], f"solve_DIVA_batch member {k}: {err.decode() if err else ''}")
+    return out
+
+
 def solve_DIVA(grid, ice, config=None, backend=None):
     """ice_velocity_module.f90:249-374 on the GPU; updates ``ice`` in place."""
     return _run(grid, ice, config, backend, "solve_DIVA", OUT_DIVA)

@@ -186,6 +186,13 @@ int  diva_solve_sia(diva_ctx_t* ctx, diva_report_t* rep);
 int  diva_solve_ssa(diva_ctx_t* ctx, diva_report_t* rep);
 /* solve_DIVA (ice_velocity_module.f90:249-374); needs DIVA. */
 int  diva_solve_diva(diva_ctx_t* ctx, diva_report_t* rep);
+/* solve_DIVA for n contexts at once (an ensemble; no single routine of the reference:
+ * its members would be separate solve_DIVA calls).  Each context runs on its own
+ * stream and one viscosity iteration of every unfinished member is kept in flight,
+ * so the iterations of different members overlap on the GPU.  reports[k] is the report
+ * of ctxs[k] (its status included); returns DIVA_OK if every member is OK, else the
+ * first other status.  Contexts must be distinct. */
+int  diva_solve_diva_batch(diva_ctx_t** ctxs, int32_t n, diva_report_t* reports);
 /* The SIA 3D velocity loop of solve_SIA (ice_velocity_module.f90:60-105) alone,
  * in any dynamics mode (used for "DIVA plus SIA" diagnostics). */
 int  diva_calc_sia_3d_velocities(diva_ctx_t* ctx);

@@ -149,3 +149,37 @@ def test_tiled_smoothing_matches_per_colour_kernels(cuda, monkeypatch, dx):
     assert rt["linear_iterations"] == rp["linear_iterations"] and rt["mg_cycles"] == rp["mg_cycles"]
     for k in ("u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "u_3D_cx"):
         assert np.array_equal(ot[k], op[k]), k
+
+
+def test_batch_solve_matches_individual_solves(cuda):
+    """diva_solve_diva_batch keeps one iteration of every member in flight on its own
+    stream; each member's result is bit-identical to solving it alone."""
+    ov = {"picard_stop": "relres", "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 300, "lin_adaptive": 1}
+    cases = [helpers.make_case(1, overrides=ov), helpers.make_case(2, dx=40e3, overrides=ov),
+             helpers.make_case(2, dx=10e3, overrides=dict(ov, DIVA_visc_it_nit=40))]
+    names = ("u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "u_3D_cx", "w_3D_a")
+    alone = [helpers.run(cuda, g, cfg, f, post=None) for g, cfg, f in cases]
+    ctxs = []
+    for g, cfg, f in cases:
+        ctx = diva.Context(g, cfg, cuda)
+        helpers.prepare(ctx, f)
+        ctxs.append(ctx)
+    reps = diva.solve_DIVA_batch(ctxs)
+    outs = [ctx.download(list(names)) for ctx in ctxs]
+    for ctx in ctxs:
+        ctx.close()
+    for (ra, oa), rb, ob in zip(alone, reps, outs):
+        assert ra["status"] == rb["status"] and ra["picard_iterations"] == rb["picard_iterations"]
+        assert ra["mg_cycles"] == rb["mg_cycles"]
+        for k in names:
+            assert np.array_equal(oa[k], ob[k]), k
+    assert reps[2]["status"] == _abi.MAX_PICARD   # the capped member ends like the lone solve
+
+
+def test_batch_solve_rejects_repeated_context(cuda):
+    g, cfg, f = helpers.make_case(2, dx=40e3)
+    ctx = diva.Context(g, cfg, cuda)
+    helpers.prepare(ctx, f)
+    with pytest.raises(diva.DivaError):
+        diva.solve_DIVA_batch([ctx, ctx])
+    ctx.close()
