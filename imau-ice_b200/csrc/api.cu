@@ -651,7 +651,7 @@ int diva_solve_diva_batch(diva_ctx_t** hs, int32_t n, diva_report_t* reports) {
   for (int k = 0; k < n; ++k) {
     if (!hs[k]) return DIVA_BAD_INPUT;
     for (int m = 0; m < k; ++m)
-      if (hs[m] == hs[k]) return set_error(&hs[k]->c, DIVA_BAD_INPUT, "a context appears twice in the batch");
+      if (hs[m] == hs[k]) return set_error(&hs[0]->c, DIVA_BAD_INPUT, "a context appears twice in the batch");
   }
   std::vector<int> status(n, DIVA_OK);
   std::vector<GraphLoop> loops(n);

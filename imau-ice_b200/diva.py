@@ -322,8 +322,11 @@ def solve_DIVA_batch(contexts):
     n = len(contexts)
     hs = (C.c_void_p * n)(*[c.h for c in contexts])
     reps = (_abi.Report * n)()
-    f(hs, n, reps)
+    st = f(hs, n, reps)
     out = [r.as_dict() for r in reps]
+    if st not in (0, _abi.MAX_PICARD) and all(r["status"] in (0, _abi.MAX_PICARD) for r in out):
+        err = be.fns["last_error"](contexts[0].h)   # rejected before any member ran
+        raise DivaError(st, f"solve_DIVA_batch: {err.decode() if err else ''}")
     for k, (c, r) in enumerate(zip(contexts, out)):
         if r["status"] not in (0, _abi.MAX_PICARD):
             err = be.fns["last_error"](c.h)
