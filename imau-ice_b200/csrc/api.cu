@@ -248,6 +248,7 @@ struct GraphLoop {
 int graph_loop_begin(Ctx* c, GraphLoop& L) {
   double init[SC_COUNT - SC_TARGET2] = {};
   init[SC_RELRES - SC_TARGET2] = -1.0;
+  init[SC_ETA - SC_TARGET2] = c->c.lin_adaptive_eta;
   DIVA_CUDA(c, cudaMemcpyAsync(c->scal + SC_TARGET2, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
   L.it = 0; L.resid = 0.0; L.relres = -1.0; L.by_relres = false; L.done = false;
   return DIVA_OK;
@@ -331,13 +332,15 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
   const diva_config_t& C = c->c;
   const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
   int it = 0, st = DIVA_OK, lin_fail = 0;
-  double resid = 0.0, relres = -1.0;
+  double resid = 0.0, relres = -1.0, eta = C.lin_adaptive_eta, relres_prev = 0.0;
   for (;;) {
     ++it;
     if ((st = launch_diva_coefficients(c, u, v, diva))) return st;
     if ((st = solver_setup(c))) return st;
     if (relmode) {
       if ((st = solver_relres(c, u, v, &relres))) return st;
+      eta = eta_after(eta, relres, relres_prev, C.picard_relres_tol);   // as the graph's k_ctl_relres does
+      relres_prev = relres;
       if (!std::isfinite(relres)) return set_error(c, DIVA_NAN_DETECTED, "NaN in the nonlinear residual");
       if (relres <= C.picard_relres_tol) {
         if (diva && (st = launch_basal_stress_velocities(c))) return st;
@@ -345,7 +348,7 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
       }
     }
     double rtol = C.lin_rtol;
-    if (relmode && C.lin_adaptive) rtol = std::max(C.lin_rtol, C.lin_adaptive_eta * std::min(1.0, relres));
+    if (relmode && C.lin_adaptive) rtol = std::max(C.lin_rtol, eta * std::min(1.0, relres));
     int iters = 0;
     st = solver_solve(c, u, v, rtol, C.lin_maxit, &iters, nullptr);
     if (st == DIVA_LINEAR_NOT_CONVERGED) {

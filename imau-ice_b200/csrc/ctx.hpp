@@ -8,7 +8,17 @@
 namespace diva {
 
 constexpr int kMaxLevels = 12;
-constexpr int kCoarseDirectMax = 64;    // unknowns of a coarsest level solved directly
+constexpr int kCoarseDirectMax = 64;
+// Adaptive linear tolerance (lin_adaptive): rtol = max(lin_rtol, eta * min(1, rel-res)),
+// eta starting at lin_adaptive_eta and halved, down to kEtaFloor, whenever a viscosity
+// iteration within kEtaWindow x the stop tolerance fails to lower the nonlinear residual:
+// near the target a loose solve can stall a relaxed Picard iteration at the noise its own
+// linear error injects, while early iterations are often non-monotone and left alone.
+constexpr double kEtaFloor = 0.05, kEtaWindow = 100.0;
+__host__ __device__ inline double eta_after(double eta, double relres, double prev, double tol) {
+  const bool stalled = prev > 0.0 && relres >= prev && relres < kEtaWindow * tol;
+  return stalled ? (0.5 * eta > kEtaFloor ? 0.5 * eta : kEtaFloor) : eta;
+}    // unknowns of a coarsest level solved directly
 
 // One multigrid level of the staggered DIVA operator.  Coefficients are the
 // rediscretised Na (a-grid), Nb (b-grid) and the reaction terms Bx = beta_eff_cx*dx^2
@@ -36,6 +46,7 @@ enum {
   // device-side control of a graph-launched viscosity iteration
   SC_TARGET2, SC_LIN_IT, SC_LIN_FULL, SC_LIN_FAILED, SC_PIC_IT, SC_EXIT_RELRES, SC_CONVERGED, SC_RESID,
   SC_RELRES, SC_NAN, SC_SOLVED, SC_HALFDONE,
+  SC_ETA, SC_RELRES_PREV,   // adaptive linear tolerance factor and the previous nonlinear residual
   SC_COUNT = 40
 };
 

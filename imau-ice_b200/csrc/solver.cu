@@ -1282,6 +1282,8 @@ __global__ void k_ctl_relres(const double* partials, int nblocks, double* sc, cu
   const double rr = v[0], bb = v[1];
   const double relres = bb > 0.0 ? sqrt(rr / bb) : sqrt(rr);
   sc[SC_RELRES] = relres;
+  sc[SC_ETA] = eta_after(sc[SC_ETA], relres, sc[SC_RELRES_PREV], tol);
+  sc[SC_RELRES_PREV] = relres;
   bool stop = false;
   if (!isfinite(relres)) { sc[SC_NAN] = 1.0; stop = true; }
   else if (relres <= tol) { sc[SC_EXIT_RELRES] = 1.0; stop = true; }
@@ -1290,7 +1292,7 @@ __global__ void k_ctl_relres(const double* partials, int nblocks, double* sc, cu
 
 // initial Krylov residual and the target of this linear solve
 __global__ void k_ctl_lin_init(const double* partials, int nblocks, double* sc, cudaGraphConditionalHandle h_while,
-                               int adaptive, double lin_rtol, double eta, int maxit) {
+                               int adaptive, double lin_rtol, int maxit) {
   double v[kPW];
   sum_partials4(partials, nblocks, v);
   if (threadIdx.x != 0) return;
@@ -1299,7 +1301,7 @@ __global__ void k_ctl_lin_init(const double* partials, int nblocks, double* sc, 
   sc[SC_BNORM2] = bb;
   sc[SC_RHO] = rr;
   double rtol = lin_rtol;
-  if (adaptive) rtol = max_ref(lin_rtol, eta * min_ref(1.0, sc[SC_RELRES]));
+  if (adaptive) rtol = max_ref(lin_rtol, sc[SC_ETA] * min_ref(1.0, sc[SC_RELRES]));
   const double t = rtol * (bb > 0.0 ? sqrt(bb) : 1.0);
   sc[SC_TARGET2] = t * t;
   sc[SC_SOLVED] = 1.0;
@@ -1972,7 +1974,7 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
   k_init_residual<<<g2, block2d(), 0, c->stream>>>(o, U_(KV_X), V_(KV_X), U_(KV_B), V_(KV_B), U_(KV_R), V_(KV_R),
                                                    U_(KV_RHAT), V_(KV_RHAT), U_(KV_P), V_(KV_P), c->partials, g2.x); c->launches++;
   k_ctl_lin_init<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, h_while, relmode && C.lin_adaptive, C.lin_rtol,
-                                           C.lin_adaptive_eta, C.lin_maxit); c->launches++;
+                                           C.lin_maxit); c->launches++;
   c->fine_passes += 1.0;
   DIVA_LAUNCHED(c, "graph head");
   G.n_head = cc.dl(); G.p_head = cc.dp();

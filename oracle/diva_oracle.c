@@ -1857,6 +1857,7 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
   long lin0 = c->lin_iters_total;
   const int relmode = (C->picard_stop == DIVA_STOP_RELRES);
   int exited_by_relres = 0;
+  double eta = C->lin_adaptive_eta, relres_prev = 0.0;
   for (;;) {
     ++it;
     if (diva) calc_vertical_shear_strain_rates(c);
@@ -1879,6 +1880,11 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
       set_sico_masks(c);
       assemble(c, u, v);
       relres = relres_current(c, u, v);
+      /* adaptive tolerance factor: halved (floor 0.05) when, within 100 x the stop
+       * tolerance, the residual did not fall */
+      if (relres_prev > 0.0 && relres >= relres_prev && relres < 100.0 * C->picard_relres_tol)
+        eta = fmax(0.05, 0.5 * eta);
+      relres_prev = relres;
       if (relres <= C->picard_relres_tol) { exited_by_relres = 1; }
     }
     if (exited_by_relres) {
@@ -1889,7 +1895,7 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
     memcpy(FD(c, V_CY_PREV), v, sizeof(double) * ncy);
     /* same adaptive linear tolerance rule as the GPU library (iterative solvers only) */
     if (relmode && C->lin_adaptive && (c->lin_solver == ORC_LIN_GMRES_ILU || c->lin_solver == ORC_LIN_GMRES_WARM))
-      c->petsc_rtol = fmax(C->lin_rtol, C->lin_adaptive_eta * fmin(1.0, relres));
+      c->petsc_rtol = fmax(C->lin_rtol, eta * fmin(1.0, relres));
     int st = solve_stag_linearised(c, u, v);
     if (st != DIVA_OK) status = st;
     apply_velocity_limits(c, u, v);
