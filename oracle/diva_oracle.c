@@ -30,6 +30,7 @@
  * on the first Picard iteration of a cold start (0/0 in du/dz).
  * Build with -ffp-contract=off: no fused multiply-adds, as in the reference.
  */
+#define _POSIX_C_SOURCE 200809L   /* pthread barriers under -std=c11 */
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -37,9 +38,7 @@
 #include <string.h>
 #include <float.h>
 #include <time.h>
-#ifdef _OPENMP
-#include <omp.h>
-#endif
+#include <pthread.h>
 
 #include "../include/diva.h"
 
@@ -57,6 +56,8 @@ enum { TYPE_LAND = 0, TYPE_OCEAN = 1, TYPE_LAKE = 2, TYPE_SHEET = 3, TYPE_SHELF 
        TYPE_COAST = 5, TYPE_MARGIN = 6, TYPE_GL = 7, TYPE_CF = 8 };
 
 /* linear solvers of the oracle */
+#define ORC_MAX_THREADS 64
+struct orc_pool;
 enum { ORC_LIN_DIRECT = 0, ORC_LIN_SOR = 1, ORC_LIN_GMRES_ILU = 2, ORC_LIN_GMRES_WARM = 3 };
 
 typedef struct {
@@ -82,6 +83,8 @@ typedef struct orc_ctx {
   int SOR_nit; double SOR_tol, SOR_omega;
   double petsc_rtol, petsc_abstol;
   int lin_iters_last;
+  int threads;              /* threads of the timed CPU baseline (1: the sequential algorithm) */
+  struct orc_pool* pool;    /* their workers (NULL with one thread) */
   long lin_iters_total;
   char err[512];
 } orc_ctx;
@@ -783,24 +786,80 @@ static void calc_vertical_shear_strain_rates(orc_ctx* c) {
 }
 
 /* calc_effective_viscosity :722-899 */
-static void calc_effective_viscosity(orc_ctx* c, const double* u_cx, const double* v_cy) {
+/* rows of block b of nb (contiguous, balanced by row count) */
+static void block_rows(int n, int nb, int b, int* lo, int* hi) {
+  *lo = (int)((long long)n * b / nb);
+  *hi = (int)((long long)n * (b + 1) / nb);
+}
+
+/* ---- worker pool of the timed CPU baseline (pthreads; one per context with threads > 1) ----
+ * pool_run(P, fn, arg) runs fn(arg, t, T) on T threads (the caller is thread 0) and returns
+ * when all have finished; with T = 1 it is a plain call. */
+typedef void (*task_fn)(void* arg, int t, int T);
+struct worker_arg { struct orc_pool* P; int t; };
+struct orc_pool {
+  int T, quit;
+  pthread_t th[ORC_MAX_THREADS];
+  struct worker_arg wa[ORC_MAX_THREADS];
+  pthread_barrier_t start, done;
+  task_fn fn;
+  void* arg;
+};
+static void* pool_worker(void* wa) {
+  struct orc_pool* P = ((struct worker_arg*)wa)->P;
+  const int t = ((struct worker_arg*)wa)->t;
+  for (;;) {
+    pthread_barrier_wait(&P->start);
+    if (P->quit) break;
+    P->fn(P->arg, t, P->T);
+    pthread_barrier_wait(&P->done);
+  }
+  return NULL;
+}
+static void pool_run(struct orc_pool* P, task_fn fn, void* arg) {
+  if (!P || P->T <= 1) { fn(arg, 0, 1); return; }
+  P->fn = fn;
+  P->arg = arg;
+  pthread_barrier_wait(&P->start);
+  fn(arg, 0, P->T);
+  pthread_barrier_wait(&P->done);
+}
+static struct orc_pool* pool_create(int T) {
+  struct orc_pool* P = (struct orc_pool*)calloc(1, sizeof(struct orc_pool));
+  P->T = T;
+  pthread_barrier_init(&P->start, NULL, (unsigned)T);
+  pthread_barrier_init(&P->done, NULL, (unsigned)T);
+  for (int t = 1; t < T; ++t) {
+    P->wa[t].P = P;
+    P->wa[t].t = t;
+    pthread_create(&P->th[t], NULL, pool_worker, &P->wa[t]);
+  }
+  return P;
+}
+static void pool_destroy(struct orc_pool* P) {
+  if (!P) return;
+  if (P->T > 1) {
+    P->quit = 1;
+    pthread_barrier_wait(&P->start);
+    for (int t = 1; t < P->T; ++t) pthread_join(P->th[t], NULL);
+  }
+  pthread_barrier_destroy(&P->start);
+  pthread_barrier_destroy(&P->done);
+  free(P);
+}
+
+/* the columns [i0, i1) of calc_effective_viscosity (one slice per baseline thread) */
+static void visc_columns_range(orc_ctx* c, const double* du_dx, const double* du_dy, const double* dv_dx,
+                               const double* dv_dy, int i0, int i1) {
   DECL_DIMS(c);
   const diva_config_t* C = &c->c;
   const double* zeta = c->g.zeta;
-  const double dx = c->dx;
-  const size_t na = (size_t)nx * ny;
-  double *du_dx = (double*)malloc(na * sizeof(double)), *du_dy = (double*)malloc(na * sizeof(double));
-  double *dv_dx = (double*)malloc(na * sizeof(double)), *dv_dy = (double*)malloc(na * sizeof(double));
-  ddx_cx_to_a(nx, ny, dx, u_cx, du_dx);
-  ddy_cx_to_a(nx, ny, dx, u_cx, du_dy);
-  ddx_cy_to_a(nx, ny, dx, v_cy, dv_dx);
-  ddy_cy_to_a(nx, ny, dx, v_cy, dv_dy);
   const int32_t* ice = FI(c, MASK_ICE_A);
   const double *Hi = FD(c, HI_A), *A = FD(c, A_FLOW_3D_A), *dudz = FD(c, DU_DZ_3D_CX), *dvdz = FD(c, DV_DZ_3D_CY);
   double *visc = FD(c, VISC_EFF_3D_A), *vint_a = FD(c, VISC_EFF_INT_A), *Na = FD(c, N_A);
   const double e_A = -1.0 / C->n_flow, e_eps = (1.0 - C->n_flow) / (2.0 * C->n_flow);
   const int bc = (C->choice_ice_margin == DIVA_MARGIN_BC);
-  for (int i = 0; i < nx; ++i)
+  for (int i = i0; i < i1; ++i)
     for (int j = 0; j < ny; ++j) {
       if (bc && ice[IA(j, i)] == 0) {
         for (int k = 0; k < nz; ++k) visc[IA3(k, j, i)] = 0.0;
@@ -824,9 +883,58 @@ static void calc_effective_viscosity(orc_ctx* c, const double* u_cx, const doubl
       vint_a[IA(j, i)] = vint(zeta, nz, &visc[IA3(0, j, i)]);
       Na[IA(j, i)] = bc ? vint_a[IA(j, i)] * Hi[IA(j, i)] : vint_a[IA(j, i)] * fmax(0.1, Hi[IA(j, i)]);
     }
+}
+
+struct visc_cols { orc_ctx* c; const double *du_dx, *du_dy, *dv_dx, *dv_dy; };
+static void visc_b_range(orc_ctx* c, int i0, int i1);
+static void visc_b_columns(void* arg, int t, int T) {
+  struct visc_cols* v = (struct visc_cols*)arg;
+  int i0, i1;
+  block_rows(v->c->nx - 1, T, t, &i0, &i1);
+  visc_b_range(v->c, i0, i1);
+}
+static void visc_columns(void* arg, int t, int T) {
+  struct visc_cols* v = (struct visc_cols*)arg;
+  int i0, i1;
+  block_rows(v->c->nx, T, t, &i0, &i1);
+  visc_columns_range(v->c, v->du_dx, v->du_dy, v->dv_dx, v->dv_dy, i0, i1);
+}
+
+static void calc_effective_viscosity(orc_ctx* c, const double* u_cx, const double* v_cy) {
+  DECL_DIMS(c);
+  const diva_config_t* C = &c->c;
+  const double dx = c->dx;
+  const size_t na = (size_t)nx * ny;
+  double *du_dx = (double*)malloc(na * sizeof(double)), *du_dy = (double*)malloc(na * sizeof(double));
+  double *dv_dx = (double*)malloc(na * sizeof(double)), *dv_dy = (double*)malloc(na * sizeof(double));
+  ddx_cx_to_a(nx, ny, dx, u_cx, du_dx);
+  ddy_cx_to_a(nx, ny, dx, u_cx, du_dy);
+  ddx_cy_to_a(nx, ny, dx, v_cy, dv_dx);
+  ddy_cy_to_a(nx, ny, dx, v_cy, dv_dy);
+  double* Na = FD(c, N_A);
+  /* the a-grid columns, in column strips over the baseline's threads */
+  struct visc_cols a = {c, du_dx, du_dy, dv_dx, dv_dy};
+  pool_run(c->pool, visc_columns, &a);
+  struct visc_cols bb = {c, NULL, NULL, NULL, NULL};
+  pool_run(c->pool, visc_b_columns, &bb);
+  if (!C->include_SSADIVA_crossterms) {
+    map_a_to_cx(nx, ny, Na, FD(c, N_CX));
+    map_a_to_cy(nx, ny, Na, FD(c, N_CY));
+  }
+  free(du_dx); free(du_dy); free(dv_dx); free(dv_dy);
+}
+
+/* the b-grid columns [i0, i1) of calc_effective_viscosity (:820-874) */
+static void visc_b_range(orc_ctx* c, int i0, int i1) {
+  DECL_DIMS(c);
+  const diva_config_t* C = &c->c;
+  const double* zeta = c->g.zeta;
+  const int32_t* ice = FI(c, MASK_ICE_A);
+  const double* visc = FD(c, VISC_EFF_3D_A);
+  const int bc = (C->choice_ice_margin == DIVA_MARGIN_BC);
   double *visc_b = FD(c, VISC_EFF_3D_B), *vint_b = FD(c, VISC_EFF_INT_B), *Nb = FD(c, N_B);
   const double* Hi_b = FD(c, HI_B);
-  for (int i = 0; i < nx - 1; ++i)
+  for (int i = i0; i < i1; ++i)
     for (int j = 0; j < ny - 1; ++j) {
       double* vb = &visc_b[IB3(0, j, i)];
       if (bc) {
@@ -844,11 +952,6 @@ static void calc_effective_viscosity(orc_ctx* c, const double* u_cx, const doubl
       vint_b[IB(j, i)] = vint(zeta, nz, vb);
       Nb[IB(j, i)] = bc ? vint_b[IB(j, i)] * Hi_b[IB(j, i)] : vint_b[IB(j, i)] * fmax(0.1, Hi_b[IB(j, i)]);
     }
-  if (!C->include_SSADIVA_crossterms) {
-    map_a_to_cx(nx, ny, Na, FD(c, N_CX));
-    map_a_to_cy(nx, ny, Na, FD(c, N_CY));
-  }
-  free(du_dx); free(du_dy); free(dv_dx); free(dv_dy);
 }
 
 /* calc_sliding_term_beta :900-959 */
@@ -1422,18 +1525,23 @@ static int solve_direct(orc_ctx* c) {
  * PETSc defaults that KSPSetFromOptions picks without options
  * (petsc_module.F90:49-69; PETSc is not vendored, this restates its
  * published algorithm).  Classical Gram-Schmidt, Givens rotations. */
-static void ilu0_factor(const csr_t* m, double* lu, int* diag) {
-  const int n = m->m;
-  memcpy(lu, m->val, sizeof(double) * m->nnz);
-  int* pos = (int*)malloc(sizeof(int) * n);
-  for (int q = 0; q < n; ++q) pos[q] = -1;
-  for (int i = 0; i < n; ++i) {
+/* ILU(0) of the rows [lo, hi) restricted to the columns [lo, hi): with one block this is
+ * ILU(0) of the whole matrix; with T blocks it is block-Jacobi ILU(0), the
+ * preconditioner PETSc's KSPSetFromOptions picks when the matrix is split over T
+ * ranks.  Entries outside the block are kept in lu but never used. */
+static void ilu0_factor_block(const csr_t* m, double* lu, int* diag, int* pos, int lo, int hi) {
+  for (int i = lo; i < hi; ++i) {
     diag[i] = -1;
-    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k) { pos[m->idx[k]] = k; if (m->idx[k] == i) diag[i] = k; }
+    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k) {
+      const int col = m->idx[k];
+      if (col < lo || col >= hi) continue;
+      pos[col] = k;
+      if (col == i) diag[i] = k;
+    }
     /* eliminate the row's lower entries in increasing column order (IKJ variant) */
-    int cnt = m->ptr[i + 1] - m->ptr[i];
-    int order[64];
-    for (int t = 0; t < cnt; ++t) order[t] = m->ptr[i] + t;
+    int cnt = 0, order[64];
+    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k)
+      if (m->idx[k] >= lo && m->idx[k] < hi) order[cnt++] = k;
     for (int a = 1; a < cnt; ++a) { int v = order[a], b = a - 1; while (b >= 0 && m->idx[order[b]] > m->idx[v]) { order[b + 1] = order[b]; --b; } order[b + 1] = v; }
     for (int t = 0; t < cnt; ++t) {
       int kk = order[t], col = m->idx[kk];
@@ -1441,79 +1549,150 @@ static void ilu0_factor(const csr_t* m, double* lu, int* diag) {
       lu[kk] = lu[kk] / lu[diag[col]];
       for (int k2 = m->ptr[col]; k2 < m->ptr[col + 1]; ++k2) {
         int c2 = m->idx[k2];
-        if (c2 > col && pos[c2] >= 0) lu[pos[c2]] -= lu[kk] * lu[k2];
+        if (c2 > col && c2 >= lo && c2 < hi && pos[c2] >= 0) lu[pos[c2]] -= lu[kk] * lu[k2];
       }
     }
-    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k) pos[m->idx[k]] = -1;
+    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k)
+      if (m->idx[k] >= lo && m->idx[k] < hi) pos[m->idx[k]] = -1;
   }
-  free(pos);
 }
-static void ilu0_apply(const csr_t* m, const double* lu, const int* diag, const double* r, double* z) {
-  const int n = m->m;
-  for (int i = 0; i < n; ++i) {
+static void ilu0_apply_block(const csr_t* m, const double* lu, const int* diag, const double* r, double* z, int lo,
+                             int hi) {
+  for (int i = lo; i < hi; ++i) {
     double s = r[i];
-    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k) if (m->idx[k] < i) s -= lu[k] * z[m->idx[k]];
+    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k) {
+      const int col = m->idx[k];
+      if (col < i && col >= lo) s -= lu[k] * z[col];
+    }
     z[i] = s;
   }
-  for (int i = n - 1; i >= 0; --i) {
+  for (int i = hi - 1; i >= lo; --i) {
     double s = z[i];
-    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k) if (m->idx[k] > i) s -= lu[k] * z[m->idx[k]];
+    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k) {
+      const int col = m->idx[k];
+      if (col > i && col < hi) s -= lu[k] * z[col];
+    }
     z[i] = s / lu[diag[i]];
   }
 }
-static void spmv(const csr_t* m, const double* x, double* y) {
-  for (int i = 0; i < m->m; ++i) {
-    double s = 0.0;
-    for (int k = m->ptr[i]; k < m->ptr[i + 1]; ++k) s += m->val[k] * x[m->idx[k]];
-    y[i] = s;
+/* the parallel pieces of GMRES: thread t of T takes the t-th contiguous slice of rows */
+struct vec_task {
+  const csr_t* m;
+  const double *lu, *r, *x, *a, *b;
+  const int* diag;
+  double *z, *y, *out;
+  double s;
+  int n, op;
+  double part[ORC_MAX_THREADS];
+};
+enum { VT_ILU_FACTOR, VT_ILU_APPLY, VT_SPMV, VT_DOT, VT_AXPY, VT_SCALE };
+static void vec_task_run(void* arg, int t, int T) {
+  struct vec_task* v = (struct vec_task*)arg;
+  int lo, hi;
+  block_rows(v->n, T, t, &lo, &hi);
+  switch (v->op) {
+    case VT_ILU_FACTOR: {
+      int* pos = (int*)malloc(sizeof(int) * v->n);
+      for (int q = lo; q < hi; ++q) pos[q] = -1;
+      ilu0_factor_block(v->m, v->z, (int*)v->diag, pos, lo, hi);
+      free(pos);
+      break;
+    }
+    case VT_ILU_APPLY: ilu0_apply_block(v->m, v->lu, v->diag, v->r, v->z, lo, hi); break;
+    case VT_SPMV:
+      for (int i = lo; i < hi; ++i) {
+        double s = 0.0;
+        for (int k = v->m->ptr[i]; k < v->m->ptr[i + 1]; ++k) s += v->m->val[k] * v->x[v->m->idx[k]];
+        v->y[i] = s;
+      }
+      break;
+    case VT_DOT: { double s = 0.0; for (int q = lo; q < hi; ++q) s += v->a[q] * v->b[q]; v->part[t] = s; break; }
+    case VT_AXPY: for (int q = lo; q < hi; ++q) v->out[q] += v->s * v->a[q]; break;         /* out += s a */
+    case VT_SCALE: for (int q = lo; q < hi; ++q) v->out[q] = v->s != 0.0 ? v->a[q] / v->s : 0.0; break;
   }
 }
+/* ILU(0) over as many row blocks as the pool has threads (one block: plain ILU(0)) */
+static void ilu0_factor(struct orc_pool* P, const csr_t* m, double* lu, int* diag) {
+  memcpy(lu, m->val, sizeof(double) * m->nnz);
+  struct vec_task v = {0};
+  v.m = m; v.z = lu; v.diag = diag; v.n = m->m; v.op = VT_ILU_FACTOR;
+  pool_run(P, vec_task_run, &v);
+}
+static void ilu0_apply(struct orc_pool* P, const csr_t* m, const double* lu, const int* diag, const double* r,
+                       double* z) {
+  struct vec_task v = {0};
+  v.m = m; v.lu = lu; v.diag = diag; v.r = r; v.z = z; v.n = m->m; v.op = VT_ILU_APPLY;
+  pool_run(P, vec_task_run, &v);
+}
+static void spmv_p(struct orc_pool* P, const csr_t* m, const double* x, double* y) {
+  struct vec_task v = {0};
+  v.m = m; v.x = x; v.y = y; v.n = m->m; v.op = VT_SPMV;
+  pool_run(P, vec_task_run, &v);
+}
+static void spmv(const csr_t* m, const double* x, double* y) { spmv_p(NULL, m, x, y); }
+/* sums of the per-thread slices in thread order: deterministic for a given thread count,
+ * and with one thread the plain sequential sum */
+static double dot_p(struct orc_pool* P, int n, const double* a, const double* b) {
+  struct vec_task v = {0};
+  v.a = a; v.b = b; v.n = n; v.op = VT_DOT;
+  pool_run(P, vec_task_run, &v);
+  const int T = (P && P->T > 1) ? P->T : 1;
+  double s = v.part[0];
+  for (int t = 1; t < T; ++t) s += v.part[t];
+  return s;
+}
 static double nrm2(int n, const double* a) { double s = 0.0; for (int q = 0; q < n; ++q) s += a[q] * a[q]; return sqrt(s); }
+static double nrm2_p(struct orc_pool* P, int n, const double* a) {
+  return (P && P->T > 1) ? sqrt(dot_p(P, n, a, a)) : nrm2(n, a);
+}
+static void axpy_p(struct orc_pool* P, int n, double s, const double* a, double* out) {
+  struct vec_task v = {0};
+  v.a = a; v.out = out; v.s = s; v.n = n; v.op = VT_AXPY;
+  pool_run(P, vec_task_run, &v);
+}
+static void scale_p(struct orc_pool* P, int n, const double* a, double s, double* out) {   /* out = a / s */
+  struct vec_task v = {0};
+  v.a = a; v.out = out; v.s = s; v.n = n; v.op = VT_SCALE;
+  pool_run(P, vec_task_run, &v);
+}
 
 static int solve_gmres(orc_ctx* c, double rtol, double abstol, int maxit, int zero_guess) {
   csr_t* m = &c->m;
+  struct orc_pool* P = c->pool;   /* NULL: one thread, the sequential algorithm */
   const int n = m->m, R = 30;
   double* lu = (double*)malloc(sizeof(double) * m->nnz);
   int* diag = (int*)calloc((size_t)n, sizeof(int));
-  ilu0_factor(m, lu, diag);
+  ilu0_factor(P, m, lu, diag);
   double* V = (double*)malloc(sizeof(double) * (size_t)n * (R + 1));
   double *w = (double*)malloc(sizeof(double) * n), *t = (double*)malloc(sizeof(double) * n);
   double H[31 * 30], cs[30], sn[30], g[31], y[30];
   double* x = m->x;
   if (zero_guess) memset(x, 0, sizeof(double) * n);
-  ilu0_apply(m, lu, diag, m->b, t);
-  double bnorm = nrm2(n, t);
-  spmv(m, x, w);
+  ilu0_apply(P, m, lu, diag, m->b, t);
+  double bnorm = nrm2_p(P, n, t);
+  spmv_p(P, m, x, w);
   for (int q = 0; q < n; ++q) w[q] = m->b[q] - w[q];
-  ilu0_apply(m, lu, diag, w, t);
-  double rnorm = nrm2(n, t);
+  ilu0_apply(P, m, lu, diag, w, t);
+  double rnorm = nrm2_p(P, n, t);
   /* PETSc's default test is relative to the initial residual, which is ||B b|| from a zero guess;
    * a warm start is measured against ||B b|| as well */
   double r0 = bnorm;
   double target = fmax(rtol * r0, abstol);
   int it = 0, status = DIVA_OK;
   while (rnorm > target && it < maxit) {
-    for (int q = 0; q < n; ++q) V[q] = t[q] / rnorm;
+    scale_p(P, n, t, rnorm, V);
     memset(g, 0, sizeof(g));
     g[0] = rnorm;
     int kk = 0;
     for (; kk < R && it < maxit; ++kk) {
       ++it;
-      spmv(m, &V[(size_t)kk * n], w);
-      ilu0_apply(m, lu, diag, w, t);
-      for (int l = 0; l <= kk; ++l) {
-        double s = 0.0; const double* vl = &V[(size_t)l * n];
-        for (int q = 0; q < n; ++q) s += t[q] * vl[q];
-        H[l * R + kk] = s;
-      }
-      for (int l = 0; l <= kk; ++l) {
-        const double* vl = &V[(size_t)l * n]; double h = H[l * R + kk];
-        for (int q = 0; q < n; ++q) t[q] -= h * vl[q];
-      }
-      double hn = nrm2(n, t);
+      spmv_p(P, m, &V[(size_t)kk * n], w);
+      ilu0_apply(P, m, lu, diag, w, t);
+      for (int l = 0; l <= kk; ++l) H[l * R + kk] = dot_p(P, n, t, &V[(size_t)l * n]);
+      for (int l = 0; l <= kk; ++l) axpy_p(P, n, -H[l * R + kk], &V[(size_t)l * n], t);
+      double hn = nrm2_p(P, n, t);
       H[(kk + 1) * R + kk] = hn;
-      double* vn = &V[(size_t)(kk + 1) * n];
-      for (int q = 0; q < n; ++q) vn[q] = (hn != 0.0) ? t[q] / hn : 0.0;
+      scale_p(P, n, t, hn, &V[(size_t)(kk + 1) * n]);
       for (int l = 0; l < kk; ++l) {
         double a = H[l * R + kk], b = H[(l + 1) * R + kk];
         H[l * R + kk] = cs[l] * a + sn[l] * b;
@@ -1531,11 +1710,11 @@ static int solve_gmres(orc_ctx* c, double rtol, double abstol, int maxit, int ze
       for (int q = l + 1; q < kk; ++q) s -= H[l * R + q] * y[q];
       y[l] = s / H[l * R + l];
     }
-    for (int l = 0; l < kk; ++l) { const double* vl = &V[(size_t)l * n]; for (int q = 0; q < n; ++q) x[q] += y[l] * vl[q]; }
-    spmv(m, x, w);
+    for (int l = 0; l < kk; ++l) axpy_p(P, n, y[l], &V[(size_t)l * n], x);
+    spmv_p(P, m, x, w);
     for (int q = 0; q < n; ++q) w[q] = m->b[q] - w[q];
-    ilu0_apply(m, lu, diag, w, t);
-    rnorm = nrm2(n, t);
+    ilu0_apply(P, m, lu, diag, w, t);
+    rnorm = nrm2_p(P, n, t);
   }
   if (rnorm > target) status = DIVA_LINEAR_NOT_CONVERGED;
   c->lin_iters_last = it;
@@ -2056,6 +2235,7 @@ int orc_destroy(orc_ctx* c) {
   for (int f = 0; f < DIVA_NUM_FIELDS; ++f) { free(c->F[f]); free(c->S[f]); }
   free(c->ij2n_u); free(c->ij2n_v); free(c->n2ij);
   free(c->m.ptr); free(c->m.idx); free(c->m.val); free(c->m.b); free(c->m.x);
+  pool_destroy(c->pool);
   free(c);
   return DIVA_OK;
 }
@@ -2163,10 +2343,14 @@ void orc_vertical_integration_from_bottom_to_zeta(const double* zeta, int nz, co
   vint_bottom_to_zeta(zeta, nz, f, out);
 }
 
-int orc_num_threads(void) {
-#ifdef _OPENMP
-  return omp_get_max_threads();
-#else
-  return 1;
-#endif
+/* Threads of this context's GMRES (timed CPU baseline only; 1 keeps the sequential
+ * algorithm the parity tests use, more splits ILU(0) into block-Jacobi over row blocks). */
+int orc_set_threads(orc_ctx* c, int32_t threads) {
+  if (!c || threads < 1 || threads > ORC_MAX_THREADS) return DIVA_BAD_INPUT;
+  pool_destroy(c->pool);
+  c->pool = threads > 1 ? pool_create(threads) : NULL;
+  c->threads = threads;
+  return DIVA_OK;
 }
+
+int orc_num_threads(void) { return ORC_MAX_THREADS; }

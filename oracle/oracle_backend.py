@@ -47,7 +47,15 @@ def oracle_backend():
     lib.orc_vertical_average.restype = C.c_double
     lib.orc_vertical_integration_from_bottom_to_zeta.argtypes = [dp, C.c_int, dp, dp]
     lib.orc_num_threads.restype = C.c_int
+    lib.orc_set_threads.argtypes = [C.c_void_p, C.c_int32]
+    lib.orc_set_threads.restype = C.c_int
     return b
+
+
+def set_threads(ctx, threads):
+    """OpenMP threads of the oracle's GMRES and column loops (1: the sequential algorithm
+    of the parity tests; more: block-Jacobi ILU(0) over that many row blocks)."""
+    ctx.backend.lib.orc_set_threads(ctx.h, int(threads))
 
 
 def set_linear_solver(ctx, kind=LIN_DIRECT, rtol=1e-2, abstol=2.5, sor_nit=10000, sor_tol=2.5, sor_omega=1.3):
