@@ -624,12 +624,14 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
 
 // ---- direct solve of the coarsest level ------------------------------------------------
 // The coarsest level has at most kCoarseDirectMax interior unknowns, numbered u first,
-// then v, each in plane order (i outer, j inner).  Its reduced matrix is probed column
-// by column with the smoother's own operator (Au/Av through the boundary elimination)
-// and inverted by Gauss-Jordan elimination with partial pivoting once per viscosity
-// iteration, so the coarse step of every V-cycle is one matrix-vector product.  A pivot
-// below 1e-13 of the largest entry (a singular coarse operator, e.g. a free-floating
-// shelf with no fixed boundary) raises the flag and the coarse step relaxes instead.
+// then v, each in plane order (i outer, j inner).  Once per viscosity iteration its
+// reduced matrix is assembled from the sub-cycle's row tables (the operator's nine
+// terms per row, boundary reads already mapped to their sources, duplicates summed in
+// the operator's own term order) and inverted by Gauss-Jordan elimination with partial
+// pivoting, in one launch; the coarse step of every V-cycle is then one matrix-vector
+// product.  A pivot below 1e-13 of the largest entry (a singular coarse operator, e.g.
+// a free-floating shelf with no fixed boundary) raises the flag and the coarse step
+// relaxes instead.
 struct CoarseMap {
   int ny, nu, nv;
   __device__ __forceinline__ int n() const { return nu + nv; }
@@ -639,47 +641,67 @@ struct CoarseMap {
   }
 };
 
-// column c = blockIdx.x of the coarse matrix: A e_c evaluated at every row
-__global__ void k_coarse_probe(Op o, CoarseMap m, double* A) {
-  extern __shared__ double sx[];   // unit vector e_c: u plane, then v plane
-  const int plane = (int)o.d.plane, n = m.n(), c = blockIdx.x;
-  for (int t = threadIdx.x; t < 2 * plane; t += blockDim.x) sx[t] = 0.0;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int comp, j, i;
-    m.point(c, comp, j, i);
-    sx[comp * plane + o.d.at(j, i)] = 1.0;
-  }
-  __syncthreads();
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
-    int comp, j, i;
-    m.point(r, comp, j, i);
-    A[r * n + c] = comp == 0 ? Au(o, sx, sx + plane, j, i) : Av(o, sx, sx + plane, j, i);
-  }
-}
-
-// Ainv = A^{-1} by Gauss-Jordan elimination with row pivoting (columns unscrambled at
-// the end).  Step k maps the matrix of step k-1 (buffer k&1) to the next one (buffer
-// (k+1)&1) in one pass, with one barrier per step: every warp finds the pivot row p of
-// column k itself, and every element takes its value from the old matrix with rows k
-// and p exchanged -- the pivot row divided by the pivot, the others eliminated with it.
-constexpr int kInvThreads = 256;
+// Assembly and inversion of the coarsest level's matrix by one block.  tab is the level's
+// row table (kTabCols columns of R = n rows: plane position, 4 same-component and 4
+// cross-component mapped reads; the zero element P = nx*ny stands for 'zero' sides).
+// Gauss-Jordan step k maps the matrix of step k-1 (buffer k&1) to the next one in one
+// pass with one barrier: every warp finds the pivot row p of column k itself, and every
+// element takes its value from the old matrix with rows k and p exchanged.
+constexpr int kInvThreads = 1024;
 constexpr size_t kInvSmem = 2 * kCoarseDirectMax * (kCoarseDirectMax + 1) * sizeof(double);
 
-__global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int n, const double* A, double* Ainv, int* singular) {
+__global__ void __launch_bounds__(kInvThreads) k_coarse_setup(Op o, CoarseMap m, const uint16_t* tab, double* Ainv,
+                                                              int* singular) {
   constexpr int M = kCoarseDirectMax, LD = M + 1;
   extern __shared__ double inv_buf[];   // two n x n matrices, row stride LD
   __shared__ int perm[M];
   __shared__ double wmax[kInvThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n = m.n(), ny = m.ny, P = o.d.nx * ny;
+  const Dims& d = o.d;
+  for (int e = tid; e < n * n; e += blockDim.x) inv_buf[(e / n) * LD + e % n] = 0.0;
+  __syncthreads();
+  // the unknown of a plane position (compact rows of length ny) of a u or v point
+  auto unknown = [&](int pos, bool ucomp) {
+    const int i = pos / ny, j = pos % ny;
+    return ucomp ? (i - 1) * (ny - 2) + (j - 1) : m.nu + (i - 1) * (ny - 3) + (j - 1);
+  };
+  for (int r = tid; r < n; r += blockDim.x) {
+    const int pos = tab[r], i = pos / ny, j = pos % ny;
+    int src[8];
+    for (int t = 0; t < 8; ++t) src[t] = tab[(1 + t) * n + r];
+    double cf[9];
+    if (r < m.nu) {
+      const double Ae = o.Na[d.at(j, i + 1)], Aw = o.Na[d.at(j, i)], Bn = o.Nb[d.at(j, i)], Bs = o.Nb[d.at(j - 1, i)];
+      const double cE = 4.0 * o.ax * Ae, cW = 4.0 * o.ax * Aw, cN = o.ay * Bn, cS = o.ay * Bs;
+      cf[0] = cE; cf[1] = cW; cf[2] = cN; cf[3] = cS;
+      cf[4] = -(cE + cW + cN + cS) - o.Bx[d.at(j, i)];
+      cf[5] = -2.0 * Aw - Bn; cf[6] = 2.0 * Ae + Bn; cf[7] = 2.0 * Aw + Bs; cf[8] = -2.0 * Ae - Bs;
+    } else {
+      const double An = o.Na[d.at(j + 1, i)], As = o.Na[d.at(j, i)], Be = o.Nb[d.at(j, i)], Bw = o.Nb[d.at(j, i - 1)];
+      const double cN = 4.0 * o.ay * An, cS = 4.0 * o.ay * As, cE = o.ax * Be, cW = o.ax * Bw;
+      cf[0] = cN; cf[1] = cS; cf[2] = cE; cf[3] = cW;
+      cf[4] = -(cN + cS + cE + cW) - o.By[d.at(j, i)];
+      cf[5] = -2.0 * An - Bw; cf[6] = 2.0 * An + Be; cf[7] = 2.0 * As + Bw; cf[8] = -2.0 * As - Be;
+    }
+    const bool u = r < m.nu;
+    const int row = unknown(pos, u);
+    double* a = inv_buf + row * LD;
+    // the terms in the operator's order: 4 same-component reads, the diagonal, 4 cross reads
+    for (int t = 0; t < 4; ++t)
+      if (src[t] != P) a[unknown(src[t], u)] += cf[t];
+    a[row] += cf[4];
+    for (int t = 4; t < 8; ++t)
+      if (src[t] != P) a[unknown(src[t], !u)] += cf[t + 1];
+  }
+  __syncthreads();
   double amax = 0.0;
   for (int e = tid; e < n * n; e += blockDim.x) {
-    const double v = A[e];
-    inv_buf[(e / n) * LD + e % n] = v;
+    const double v = inv_buf[(e / n) * LD + e % n];
     amax = (fabs(v) > amax || v != v) ? fabs(v) : amax;
   }
-  for (int o = 16; o > 0; o >>= 1) {   // largest magnitude; a NaN wins
-    const double w = __shfl_xor_sync(0xffffffffu, amax, o);
+  for (int o2 = 16; o2 > 0; o2 >>= 1) {   // largest magnitude; a NaN wins
+    const double w = __shfl_xor_sync(0xffffffffu, amax, o2);
     amax = (w > amax || w != w) ? w : amax;
   }
   if (lane == 0) wmax[warp] = amax;
@@ -697,9 +719,9 @@ __global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int n, const doub
     int br = k;
     for (int r = k + lane; r < n; r += 32)
       if (fabs(a[r * LD + k]) > best) { best = fabs(a[r * LD + k]); br = r; }
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+    for (int o2 = 16; o2 > 0; o2 >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o2);
+      const int orr = __shfl_xor_sync(0xffffffffu, br, o2);
       if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
     }
     if (!(best > tiny)) { bad = true; break; }
@@ -1438,9 +1460,9 @@ int solver_setup(Ctx* c) {
   c->coarse_n = m.nu + m.nv;
   c->coarse_direct = c->coarse_n > 0 && c->coarse_n <= kCoarseDirectMax && 2 * dc.plane * sizeof(double) <= 32768;
   if (c->coarse_direct) {
-    k_coarse_probe<<<c->coarse_n, 128, 2 * dc.plane * sizeof(double), c->stream>>>(make_op(c, c->nlev - 1), m,
-                                                                                    c->coarse_A); c->launches++;
-    k_coarse_invert<<<1, kInvThreads, kInvSmem, c->stream>>>(c->coarse_n, c->coarse_A, c->coarse_inv, c->coarse_singular); c->launches++;
+    k_coarse_setup<<<1, kInvThreads, kInvSmem, c->stream>>>(make_op(c, c->nlev - 1), m,
+                                                            c->sub_tab + c->sub_tab_off[c->nlev - 1], c->coarse_inv,
+                                                            c->coarse_singular); c->launches++;
     DIVA_LAUNCHED(c, "coarse inverse");
   }
   return DIVA_OK;
@@ -1613,7 +1635,7 @@ int solver_init(Ctx* c) {
   if (sub_bytes(c, c->nlev - 1) > kSubSmemBudget)
     return set_error(c, DIVA_UNSUPPORTED, "coarsest multigrid level too large for the one-block sub-cycle");
   if (int st = build_sub_tables(c)) return st;
-  DIVA_CUDA(c, cudaFuncSetAttribute(k_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_coarse_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<32, 32, kStage32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
