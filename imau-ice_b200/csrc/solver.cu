@@ -650,8 +650,8 @@ struct CoarseMap {
 constexpr int kInvThreads = 1024;
 constexpr size_t kInvSmem = 2 * kCoarseDirectMax * (kCoarseDirectMax + 1) * sizeof(double);
 
-__global__ void __launch_bounds__(kInvThreads) k_coarse_setup(Op o, CoarseMap m, const uint16_t* tab, double* Ainv,
-                                                              int* singular) {
+__device__ __forceinline__ void coarse_setup_block(const Op& o, const CoarseMap& m, const uint16_t* tab,
+                                                   double* Ainv, int* singular) {
   constexpr int M = kCoarseDirectMax, LD = M + 1;
   extern __shared__ double inv_buf[];   // two n x n matrices, row stride LD
   __shared__ int perm[M];
@@ -757,6 +757,7 @@ __global__ void __launch_bounds__(kInvThreads) k_coarse_setup(Op o, CoarseMap m,
   }
   if (tid == 0) *singular = bad ? 1 : 0;
 }
+
 
 // x += Ainv (b - A x) on the coarsest level, by one block (the caller synchronises)
 __device__ __forceinline__ void block_coarse_direct(const Op& o, const CoarseMap& m, const double* Ainv, double* xu,
@@ -1061,6 +1062,42 @@ __global__ void k_level_setup(Op o, int coarsen, Dims dc, int fx, int fy, double
     rhs.bu[q] = u_int(o.d, j, i) ? (rhs.crossterms ? -rhs.tdx[q] * dx2 : -rhs.tdx[q] * dx2 / rhs.Ncx[q]) : 0.0;
     rhs.bv[q] = v_int(o.d, j, i) ? (rhs.crossterms ? -rhs.tdy[q] * dx2 : -rhs.tdy[q] * dx2 / rhs.Ncy[q]) : 0.0;
   }
+}
+
+// Operator set-up of the sub-cycle levels in one block: per level (one barrier each) the
+// inverse diagonals and the coefficients of the next level, then the coarsest level's
+// matrix and its inverse.  The same per-point operations as k_level_setup and
+// k_coarse_setup.
+struct SmallSetup {
+  int first, last;           // the levels handled
+  int direct;                // assemble and invert the coarsest level's matrix
+  CoarseMap map;
+  const uint16_t* tab;       // the coarsest level's row table
+  double* Ainv;
+  int* singular;
+  Op o[kMaxLevels];
+  double *idu[kMaxLevels], *idv[kMaxLevels];
+  int fx[kMaxLevels], fy[kMaxLevels];
+};
+
+__global__ void __launch_bounds__(kInvThreads) k_small_setup(SmallSetup a) {
+  for (int l = a.first; l <= a.last; ++l) {
+    const Op& o = a.o[l];
+    const bool coarsen = l < a.last;
+    const Op& k = a.o[coarsen ? l + 1 : l];
+    const int n = o.d.nx * o.d.ny;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      const int j = t % o.d.ny, i = t / o.d.ny;
+      const long long q = o.d.at(j, i);
+      a.idu[l][q] = u_int(o.d, j, i) ? 1.0 / diag_u(o, j, i) : 0.0;
+      a.idv[l][q] = v_int(o.d, j, i) ? 1.0 / diag_v(o, j, i) : 0.0;
+      if (coarsen && j < k.d.ny && i < k.d.nx)
+        coarsen_point(o.d, k.d, a.fx[l], a.fy[l], o.Na, o.Nb, o.Bx, o.By, const_cast<double*>(k.Na),
+                      const_cast<double*>(k.Nb), const_cast<double*>(k.Bx), const_cast<double*>(k.By), j, i);
+    }
+    __syncthreads();
+  }
+  if (a.direct) coarse_setup_block(a.o[a.last], a.map, a.tab, a.Ainv, a.singular);
 }
 
 // ---- Krylov kernels (fine level) --------------------------------------------------
@@ -1431,13 +1468,17 @@ static CoarseMap coarse_map(const Ctx* c) {
   return m;
 }
 
+static int sub_first_level(const Ctx* c);
+
 int solver_setup(Ctx* c) {
   const diva_config_t& C = c->c;
   if (C.choice_ice_margin == DIVA_MARGIN_BC)
     return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
   // level l's diagonal and level l+1's coefficients in one launch; the finest level's
   // launch also forms the right-hand side
-  for (int l = 0; l < c->nlev; ++l) {
+  // the finest level's launch also forms the right-hand side, so it always runs on its own
+  const int first_small = sub_first_level(c) > 1 ? sub_first_level(c) : 1;
+  for (int l = 0; l < first_small && l < c->nlev; ++l) {
     const Level& F = c->lv[l];
     const bool coarsen = l + 1 < c->nlev;
     const Level& K = c->lv[coarsen ? l + 1 : l];
@@ -1456,15 +1497,25 @@ int solver_setup(Ctx* c) {
     DIVA_LAUNCHED(c, "k_level_setup");
   }
   const CoarseMap m = coarse_map(c);
-  const Dims& dc = c->lv[c->nlev - 1].d;
   c->coarse_n = m.nu + m.nv;
-  c->coarse_direct = c->coarse_n > 0 && c->coarse_n <= kCoarseDirectMax && 2 * dc.plane * sizeof(double) <= 32768;
-  if (c->coarse_direct) {
-    k_coarse_setup<<<1, kInvThreads, kInvSmem, c->stream>>>(make_op(c, c->nlev - 1), m,
-                                                            c->sub_tab + c->sub_tab_off[c->nlev - 1], c->coarse_inv,
-                                                            c->coarse_singular); c->launches++;
-    DIVA_LAUNCHED(c, "coarse inverse");
+  c->coarse_direct = c->coarse_n > 0 && c->coarse_n <= kCoarseDirectMax;
+  SmallSetup a;
+  a.first = first_small;
+  a.last = c->nlev - 1;
+  a.direct = c->coarse_direct ? 1 : 0;
+  a.map = m;
+  a.tab = c->sub_tab + c->sub_tab_off[c->nlev - 1];
+  a.Ainv = c->coarse_inv;
+  a.singular = c->coarse_singular;
+  for (int l = a.first < a.last ? a.first : a.last; l <= a.last; ++l) {   // (first > last on a one-level grid)
+    a.o[l] = make_op(c, l);
+    a.idu[l] = c->lv[l].idu;
+    a.idv[l] = c->lv[l].idv;
+    a.fx[l] = a.fy[l] = 1;
+    if (l < a.last) factors(c, l, &a.fx[l], &a.fy[l]);
   }
+  k_small_setup<<<1, kInvThreads, kInvSmem, c->stream>>>(a); c->launches++;
+  DIVA_LAUNCHED(c, "k_small_setup");
   return DIVA_OK;
 }
 
@@ -1635,7 +1686,7 @@ int solver_init(Ctx* c) {
   if (sub_bytes(c, c->nlev - 1) > kSubSmemBudget)
     return set_error(c, DIVA_UNSUPPORTED, "coarsest multigrid level too large for the one-block sub-cycle");
   if (int st = build_sub_tables(c)) return st;
-  DIVA_CUDA(c, cudaFuncSetAttribute(k_coarse_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
+  DIVA_CUDA(c, cudaFuncSetAttribute(k_small_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<32, 32, kStage32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
