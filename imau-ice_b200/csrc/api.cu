@@ -175,6 +175,8 @@ size_t carve(Ctx* c, Carver& cv) {
   c->staging = (double*)cv.take(sizeof(double) * d.nz * d.plane);
   c->col_eps = (double*)cv.take(sizeof(double) * d.plane);
   c->col_flags = (int*)cv.take(sizeof(int) * d.plane);
+  c->rtu = (int8_t*)cv.take(d.plane);
+  c->rtv = (int8_t*)cv.take(d.plane);
   c->ff_ocean = (int*)cv.take(sizeof(int) * 2 * d.plane);
   c->ff_flag = (int*)cv.take(sizeof(int) * 4);
   c->scal = (double*)cv.take(sizeof(double) * SC_COUNT);
@@ -325,7 +327,7 @@ int picard_graph(Ctx* c, bool diva, diva_report_t* rep) {
 
 // the viscosity iteration shared by solve_SSA (:180-240) and solve_DIVA (:307-363)
 int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
-  if (!c->graphs_disabled && c->c.choice_ice_margin != DIVA_MARGIN_BC) {
+  if (!c->graphs_disabled) {
     if (solver_build_picard_graphs(c, diva) == DIVA_OK) return picard_graph(c, diva, rep);
     c->graphs_disabled = true;   // conditional graph nodes unavailable: host-driven loop below
   }
@@ -395,6 +397,7 @@ int prepare_velocity_solve(Ctx* c) {
   // set_sico_masks (:1678) depends only on TAF and Hi, which do not change
   // during the viscosity iteration: once per solve gives the same masks
   if ((st = launch_sico_masks(c))) return st;
+  if ((st = solver_row_types(c))) return st;
   return DIVA_OK;
 }
 
@@ -623,8 +626,6 @@ int diva_solve_diva(diva_ctx_t* h, diva_report_t* rep) {
   if (rep) { memset(rep, 0, sizeof(*rep)); rep->relres = -1.0; }
   if (c->c.choice_ice_dynamics != DIVA_DYN_DIVA)
     return set_error(c, DIVA_BAD_INPUT, "solve_DIVA should only be called when choice_ice_dynamics is DIVA");
-  if (c->c.choice_ice_margin == DIVA_MARGIN_BC)
-    return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
   int st;
   if ((st = begin(c))) return st;
   int any = 0;
@@ -668,8 +669,6 @@ int diva_solve_diva_batch(diva_ctx_t** hs, int32_t n, diva_report_t* reports) {
     int st = DIVA_OK;
     if (c->c.choice_ice_dynamics != DIVA_DYN_DIVA) {
       st = set_error(c, DIVA_BAD_INPUT, "solve_DIVA should only be called when choice_ice_dynamics is DIVA");
-    } else if (c->c.choice_ice_margin == DIVA_MARGIN_BC) {
-      st = set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
     } else if (!(st = begin(c))) {
       int any = 0;
       if (!(st = launch_any_sheet(c, &any))) {
@@ -742,8 +741,6 @@ int diva_solve_ssa(diva_ctx_t* h, diva_report_t* rep) {
   if (rep) { memset(rep, 0, sizeof(*rep)); rep->relres = -1.0; }
   if (!(c->c.choice_ice_dynamics == DIVA_DYN_SSA || c->c.choice_ice_dynamics == DIVA_DYN_SIA_SSA))
     return set_error(c, DIVA_BAD_INPUT, "solve_SSA should only be called when choice_ice_dynamics is SSA or SIA/SSA");
-  if (c->c.choice_ice_margin == DIVA_MARGIN_BC)
-    return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
   int st;
   if ((st = begin(c))) return st;
   int any = 0;
@@ -764,14 +761,14 @@ int diva_solve_ssa(diva_ctx_t* h, diva_report_t* rep) {
 int diva_nonlinear_residual(diva_ctx_t* h, double* relres) {
   if (!h || !relres) return DIVA_BAD_INPUT;
   Ctx* c = &h->c;
-  if (c->c.choice_ice_margin == DIVA_MARGIN_BC)
-    return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
   int st;
   if ((st = launch_driving_stress(c))) return st;
   if ((st = launch_basal_conditions(c))) return st;
   if ((st = launch_grounded_fractions(c))) return st;
   if ((st = launch_prepare_afac(c))) return st;
   if ((st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true))) return st;
+  if ((st = launch_sico_masks(c))) return st;
+  if ((st = solver_row_types(c))) return st;
   if ((st = solver_setup(c))) return st;
   return solver_relres(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), relres);
 }

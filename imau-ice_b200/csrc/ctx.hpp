@@ -81,6 +81,8 @@ struct Ctx {
   double* staging = nullptr;          // upload/download staging (largest field)
   double* col_eps = nullptr;          // column coefficients: mean-flow strain rate per column
   int* col_flags = nullptr;           // column coefficients: shear faces with ice
+  int8_t* rtu = nullptr;              // finest-level row types ('BC' ice margins)
+  int8_t* rtv = nullptr;
   int* ff_ocean = nullptr;            // flood-fill state
   int* ff_flag = nullptr;
   double* scal = nullptr;             // device scalars (SC_*)
@@ -163,6 +165,7 @@ int solver_setup(Ctx* c);     // coefficients of all levels from N_a, N_b, beta_
 int solver_solve(Ctx* c, const double* u0, const double* v0, double rtol, int maxit, int* iters, double* relres0);
 int solver_relres(Ctx* c, const double* u, const double* v, double* relres);
 int solver_fill_boundary(Ctx* c, double* u, double* v);
+int solver_row_types(Ctx* c);   // finest-level row types of choice_ice_margin 'BC' (after the SICO masks)
 int solver_smooth_fine(Ctx* c, int sweeps);
 int solver_smooth_fine_values(const Ctx* c);
 int solver_matvec_fine(Ctx* c, int reps);

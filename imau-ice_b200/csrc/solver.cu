@@ -42,7 +42,17 @@ struct Op {
   BCs bc;
   double ax, ay;   // hy/hx and hx/hy of the level's cells (1 on the fine grid)
   const double *Na, *Nb, *Bx, *By;
+  // 'BC' ice margins (finest level only, else null): the type of each u and v row
+  const int8_t *rtu, *rtv;
+  double inv_dx;
 };
+
+// Row types of the finest level with choice_ice_margin 'BC' (solve_DIVA_stag_linearised
+// :1683-1727): a free row, u = 0 (shelf next to land, or a front cell with ocean on both
+// sides), or the calving-front stress row of list_DIVA_matrix_coefficients_eq_1_margin
+// (:2192-2266) / eq_2_margin (:2267-2341) with the ice on the lower (west/south) or upper
+// side of the face.
+enum : int8_t { RT_FREE = 0, RT_IDENT = 1, RT_MARGIN_LO = 2, RT_MARGIN_HI = 3 };
 
 __host__ __device__ __forceinline__ bool u_int(const Dims& d, int j, int i) {
   return i >= 1 && i <= d.nx - 3 && j >= 1 && j <= d.ny - 2;
@@ -142,11 +152,30 @@ __device__ __forceinline__ double stencil9(double c0, double x0, double c1, doub
   return fma(c8, x8, s);
 }
 
+__device__ __forceinline__ double stencil4(double c0, double x0, double c1, double x1, double c2, double x2,
+                                           double c3, double x3) {
+  double s = c0 * x0;
+  s = fma(c1, x1, s);
+  s = fma(c2, x2, s);
+  return fma(c3, x3, s);
+}
+
 // (A x) of the u row at interior (j,i) (list_DIVA_matrix_coefficients_eq_1_free :2342-2404)
 // IX places x values, CX the coefficients N_a, N_b, B (a level plane or a shared-memory tile)
-template <bool RAW, class IX, class CX>
+template <bool RAW, bool FRONT = true, class IX, class CX>
 __device__ __forceinline__ double AuXC(const Op& o, const double* xu, const double* xv, const IX& ix, const CX& cx,
                                        int j, int i) {
+  if (FRONT && o.rtu) {
+    const int t = o.rtu[o.d.at(j, i)];
+    if (t == RT_IDENT) return xu[ix(j, i)];
+    if (t != RT_FREE) {   // front row: -4N u(i1-1) + 4N u(i1) - 2N v(j-1,i1) + 2N v(j,i1), N = N_a(i1)/dx
+      const int i1 = t == RT_MARGIN_LO ? i : i + 1;
+      const double N = o.Na[cx(j, i1)];
+      return stencil4(-4.0 * o.inv_dx * N, LUx<RAW>(o, xu, ix, j, i1 - 1), 4.0 * o.inv_dx * N,
+                      LUx<RAW>(o, xu, ix, j, i1), -2.0 * o.inv_dx * N, LVx<RAW>(o, xv, ix, j - 1, i1),
+                      2.0 * o.inv_dx * N, LVx<RAW>(o, xv, ix, j, i1));
+    }
+  }
   const double Ae = o.Na[cx(j, i + 1)], Aw = o.Na[cx(j, i)], Bn = o.Nb[cx(j, i)], Bs = o.Nb[cx(j - 1, i)];
   const double cE = 4.0 * o.ax * Ae, cW = 4.0 * o.ax * Aw, cN = o.ay * Bn, cS = o.ay * Bs;
   const double diag = -(cE + cW + cN + cS) - o.Bx[cx(j, i)];
@@ -156,9 +185,20 @@ __device__ __forceinline__ double AuXC(const Op& o, const double* xu, const doub
                   2.0 * Aw + Bs, LVx<RAW>(o, xv, ix, j - 1, i), -2.0 * Ae - Bs, LVx<RAW>(o, xv, ix, j - 1, i + 1));
 }
 // (A x) of the v row at interior (j,i) (list_DIVA_matrix_coefficients_eq_2_free :2405-2467)
-template <bool RAW, class IX, class CX>
+template <bool RAW, bool FRONT = true, class IX, class CX>
 __device__ __forceinline__ double AvXC(const Op& o, const double* xu, const double* xv, const IX& ix, const CX& cx,
                                        int j, int i) {
+  if (FRONT && o.rtv) {
+    const int t = o.rtv[o.d.at(j, i)];
+    if (t == RT_IDENT) return xv[ix(j, i)];
+    if (t != RT_FREE) {   // front row: -4N v(j1-1) + 4N v(j1) - 2N u(j1,i-1) + 2N u(j1,i), N = N_a(j1)/dx
+      const int j1 = t == RT_MARGIN_LO ? j : j + 1;
+      const double N = o.Na[cx(j1, i)];
+      return stencil4(-4.0 * o.inv_dx * N, LVx<RAW>(o, xv, ix, j1 - 1, i), 4.0 * o.inv_dx * N,
+                      LVx<RAW>(o, xv, ix, j1, i), -2.0 * o.inv_dx * N, LUx<RAW>(o, xu, ix, j1, i - 1),
+                      2.0 * o.inv_dx * N, LUx<RAW>(o, xu, ix, j1, i));
+    }
+  }
   const double An = o.Na[cx(j + 1, i)], As = o.Na[cx(j, i)], Be = o.Nb[cx(j, i)], Bw = o.Nb[cx(j, i - 1)];
   const double cN = 4.0 * o.ay * An, cS = 4.0 * o.ay * As, cE = o.ax * Be, cW = o.ax * Bw;
   const double diag = -(cN + cS + cE + cW) - o.By[cx(j, i)];
@@ -186,6 +226,19 @@ __device__ __forceinline__ double Av(const Op& o, const double* xu, const double
 // effective diagonal of the reduced system: couplings to boundary unknowns whose source is the row itself fold in
 __device__ __forceinline__ double diag_u(const Op& o, int j, int i) {
   const Dims& d = o.d;
+  if (o.rtu) {
+    const int t = o.rtu[d.at(j, i)];
+    if (t == RT_IDENT) return 1.0;
+    if (t != RT_FREE) {   // the u terms of the front row whose source is this row
+      const int i1 = t == RT_MARGIN_LO ? i : i + 1;
+      const double N = o.Na[d.at(j, i1)];
+      double dg = 0.0;
+      int js, is;
+      if (u_src(d, o.bc, j, i1 - 1, js, is) && js == j && is == i) dg += -4.0 * o.inv_dx * N;
+      if (u_src(d, o.bc, j, i1, js, is) && js == j && is == i) dg += 4.0 * o.inv_dx * N;
+      return dg;
+    }
+  }
   const double Ae = o.Na[d.at(j, i + 1)], Aw = o.Na[d.at(j, i)], Bn = o.Nb[d.at(j, i)], Bs = o.Nb[d.at(j - 1, i)];
   const double cE = 4.0 * o.ax * Ae, cW = 4.0 * o.ax * Aw, cN = o.ay * Bn, cS = o.ay * Bs;
   double dg = -(cE + cW + cN + cS) - o.Bx[d.at(j, i)];
@@ -198,6 +251,19 @@ __device__ __forceinline__ double diag_u(const Op& o, int j, int i) {
 }
 __device__ __forceinline__ double diag_v(const Op& o, int j, int i) {
   const Dims& d = o.d;
+  if (o.rtv) {
+    const int t = o.rtv[d.at(j, i)];
+    if (t == RT_IDENT) return 1.0;
+    if (t != RT_FREE) {
+      const int j1 = t == RT_MARGIN_LO ? j : j + 1;
+      const double N = o.Na[d.at(j1, i)];
+      double dg = 0.0;
+      int js, is;
+      if (v_src(d, o.bc, j1 - 1, i, js, is) && js == j && is == i) dg += -4.0 * o.inv_dx * N;
+      if (v_src(d, o.bc, j1, i, js, is) && js == j && is == i) dg += 4.0 * o.inv_dx * N;
+      return dg;
+    }
+  }
   const double An = o.Na[d.at(j + 1, i)], As = o.Na[d.at(j, i)], Be = o.Nb[d.at(j, i)], Bw = o.Nb[d.at(j, i - 1)];
   const double cN = 4.0 * o.ay * An, cS = 4.0 * o.ay * As, cE = o.ax * Be, cW = o.ax * Bw;
   double dg = -(cN + cS + cE + cW) - o.By[d.at(j, i)];
@@ -424,7 +490,9 @@ __device__ __forceinline__ bool tile_deep(const TIx& ix, const Dims& d) {
 }
 
 // The shared-memory planes of a tile kernel and the operator reading from them.
-template <int TJ, int TI, bool STAGE>
+// FRONT: the operator may carry 'BC' front rows (only the finest level's kernels with
+// choice_ice_margin 'BC'); without it the row-type test is compiled out.
+template <int TJ, int TI, bool STAGE, bool FRONT>
 struct TileMem {
   double *xu, *xv, *bu, *bv;
   const double *iu, *iv;   // inverse diagonals: staged plane or the level's
@@ -454,13 +522,13 @@ struct TileMem {
   }
   template <bool RAW>
   __device__ __forceinline__ double Au(const TIx& ix, int j, int i) const {
-    if (STAGE) return AuXC<RAW>(os, xu, xv, ix, ix, j, i);
-    return AuXC<RAW>(os, xu, xv, ix, GIx{os.d}, j, i);
+    if (STAGE) return AuXC<RAW, FRONT>(os, xu, xv, ix, ix, j, i);
+    return AuXC<RAW, FRONT>(os, xu, xv, ix, GIx{os.d}, j, i);
   }
   template <bool RAW>
   __device__ __forceinline__ double Av(const TIx& ix, int j, int i) const {
-    if (STAGE) return AvXC<RAW>(os, xu, xv, ix, ix, j, i);
-    return AvXC<RAW>(os, xu, xv, ix, GIx{os.d}, j, i);
+    if (STAGE) return AvXC<RAW, FRONT>(os, xu, xv, ix, ix, j, i);
+    return AvXC<RAW, FRONT>(os, xu, xv, ix, GIx{os.d}, j, i);
   }
   __device__ __forceinline__ double idu(const TIx& ix, int j, int i) const {
     return STAGE ? iu[ix(j, i)] : iu[os.d.at(j, i)];
@@ -471,8 +539,8 @@ struct TileMem {
 };
 
 // one colour pass over the region points within `reach` of the tile
-template <int TJ, int TI, bool STAGE, bool DEEP>
-__device__ __forceinline__ void tile_pass(TileMem<TJ, TI, STAGE>& m, const TIx& ix, int tj0, int ti0, int comp,
+template <int TJ, int TI, bool STAGE, bool FRONT, bool DEEP>
+__device__ __forceinline__ void tile_pass(TileMem<TJ, TI, STAGE, FRONT>& m, const TIx& ix, int tj0, int ti0, int comp,
                                           int color, int reach) {
   const Dims& d = m.os.d;
   // the box of points within `reach` of the tile, one colour of it
@@ -491,11 +559,11 @@ __device__ __forceinline__ void tile_pass(TileMem<TJ, TI, STAGE>& m, const TIx& 
     }
   }
 }
-template <int TJ, int TI, bool STAGE>
-__device__ __forceinline__ void tile_pass_any(bool deep, TileMem<TJ, TI, STAGE>& m, const TIx& ix, int tj0, int ti0,
+template <int TJ, int TI, bool STAGE, bool FRONT>
+__device__ __forceinline__ void tile_pass_any(bool deep, TileMem<TJ, TI, STAGE, FRONT>& m, const TIx& ix, int tj0, int ti0,
                                               int comp, int color, int reach) {
-  if (deep) tile_pass<TJ, TI, STAGE, true>(m, ix, tj0, ti0, comp, color, reach);
-  else tile_pass<TJ, TI, STAGE, false>(m, ix, tj0, ti0, comp, color, reach);
+  if (deep) tile_pass<TJ, TI, STAGE, FRONT, true>(m, ix, tj0, ti0, comp, color, reach);
+  else tile_pass<TJ, TI, STAGE, FRONT, false>(m, ix, tj0, ti0, comp, color, reach);
 }
 
 // Source of b for a pre-smoothing kernel: given on the level (the finest), or the
@@ -509,13 +577,13 @@ struct Restriction {
 
 // pre-smoothing from x = 0 (the descent of a V-cycle enters every level with x = 0):
 // `sweeps` forward sweeps (u0 u1 v0 v1), then x, b and r = b - A x of the tile
-template <int TJ, int TI, bool STAGE>
+template <int TJ, int TI, bool STAGE, bool FRONT>
 __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction rs, double* gbu, double* gbv,
                                                               double* gxu, double* gxv, double* gru, double* grv,
                                                               const double* idu, const double* idv, int sweeps) {
   constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
   extern __shared__ double sm[];
-  TileMem<TJ, TI, STAGE> m(sm, o, idu, idv);
+  TileMem<TJ, TI, STAGE, FRONT> m(sm, o, idu, idv);
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
   const TIx ix{tj0 - kHalo, ti0 - kHalo, RJ};
@@ -543,7 +611,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 0; p < 4; ++p, ++pass) {
-      tile_pass_any<TJ, TI, STAGE>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI, STAGE, FRONT>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -571,7 +639,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
 // The pre-smoothed x is read over the halo from (gxu, gxv) and the result written to
 // (oxu, oxv): separate arrays, since blocks of other tiles may still be reading the
 // halo when this block writes (the grid runs in several waves on large levels).
-template <int TJ, int TI, bool STAGE>
+template <int TJ, int TI, bool STAGE, bool FRONT>
 __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx, int fy, const double* xcu,
                                                             const double* xcv, const double* gbu, const double* gbv,
                                                             const double* gxu, const double* gxv, double* oxu,
@@ -579,7 +647,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
                                                             int sweeps) {
   constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
   extern __shared__ double sm[];
-  TileMem<TJ, TI, STAGE> m(sm, o, idu, idv);
+  TileMem<TJ, TI, STAGE, FRONT> m(sm, o, idu, idv);
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
   const TIx ix{tj0 - kHalo, ti0 - kHalo, RJ};
@@ -609,7 +677,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 3; p >= 0; --p, ++pass) {
-      tile_pass_any<TJ, TI, STAGE>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI, STAGE, FRONT>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -1038,12 +1106,55 @@ __device__ __forceinline__ void coarsen_point(const Dims& df, const Dims& dc, in
   }
 }
 
-// rhs of the free rows of the finest level (k_rhs), folded into the first set-up launch
+// the row types of the finest level from the SICO masks (assembly loop :1683-1727)
+__global__ void k_row_types(Dims d, const int* combi, const int* inner, const int* outer, int8_t* rtu,
+                            int8_t* rtv) {
+  IDX2D
+  if (j >= d.ny || i >= d.nx) return;
+  const long long q = d.at(j, i);
+  int8_t t = RT_FREE;
+  if (u_int(d, j, i)) {
+    const long long q1 = d.at(j, i + 1);
+    if ((combi[q] == 3 && combi[q1] == 1) || (combi[q] == 1 && combi[q1] == 3)) {
+      t = RT_IDENT;   // shelf next to land
+    } else if ((inner[q] == 1 && outer[q1] == 1) || (outer[q] == 1 && inner[q1] == 1)) {
+      const int i1 = inner[q] == 1 ? i : i + 1;
+      if (outer[d.at(j, i1 - 1)] == 1 && outer[d.at(j, i1 + 1)] == 1) t = RT_IDENT;
+      else t = i1 == i ? RT_MARGIN_LO : RT_MARGIN_HI;
+    }
+  }
+  rtu[q] = t;
+  t = RT_FREE;
+  if (v_int(d, j, i)) {
+    const long long q1 = d.at(j + 1, i);
+    if ((combi[q] == 3 && combi[q1] == 1) || (combi[q] == 1 && combi[q1] == 3)) {
+      t = RT_IDENT;
+    } else if ((inner[q] == 1 && outer[q1] == 1) || (outer[q] == 1 && inner[q1] == 1)) {
+      const int j1 = inner[q] == 1 ? j : j + 1;
+      if (outer[d.at(j1 - 1, i)] == 1 && outer[d.at(j1 + 1, i)] == 1) t = RT_IDENT;
+      else t = j1 == j ? RT_MARGIN_LO : RT_MARGIN_HI;
+    }
+  }
+  rtv[q] = t;
+}
+
+// rhs of the free rows of the finest level (k_rhs), folded into the first set-up launch;
+// with 'BC' margins, 0 for u = 0 rows and the front stress for front rows
 struct RhsArgs {
   int on, crossterms;
   const double *tdx, *tdy, *Ncx, *Ncy;
   double *bu, *bv;
+  const int8_t *rtu, *rtv;
+  const double *Hi, *SL, *Hb;
 };
+
+// vertically integrated stress difference across a calving front at the ice cell q
+// (0.5 rho_i g H^2 - 0.5 rho_sw g H_ocean^2, :2251-2262)
+__device__ __forceinline__ double front_stress(const RhsArgs& r, long long q) {
+  const double H = r.Hi[q];
+  const double Ho = r.SL[q] > r.Hb[q] ? min_ref(kRhoI / kRhoSW * H, r.SL[q] - r.Hb[q]) : 0.0;
+  return 0.5 * kRhoI * kGrav * H * H - 0.5 * kRhoSW * kGrav * Ho * Ho;
+}
 
 // Operator set-up of one level in one launch over its points: the inverse diagonals of
 // level l, the rediscretised coefficients of level l+1 (coarse points are a subset of
@@ -1061,6 +1172,13 @@ __global__ void k_level_setup(Op o, int coarsen, Dims dc, int fx, int fy, double
     const double dx2 = o.d.dx * o.d.dx;
     rhs.bu[q] = u_int(o.d, j, i) ? (rhs.crossterms ? -rhs.tdx[q] * dx2 : -rhs.tdx[q] * dx2 / rhs.Ncx[q]) : 0.0;
     rhs.bv[q] = v_int(o.d, j, i) ? (rhs.crossterms ? -rhs.tdy[q] * dx2 : -rhs.tdy[q] * dx2 / rhs.Ncy[q]) : 0.0;
+    if (rhs.rtu) {
+      const int tu = rhs.rtu[q], tv = rhs.rtv[q];
+      if (tu == RT_IDENT) rhs.bu[q] = 0.0;
+      else if (tu != RT_FREE) rhs.bu[q] = front_stress(rhs, o.d.at(j, tu == RT_MARGIN_LO ? i : i + 1));
+      if (tv == RT_IDENT) rhs.bv[q] = 0.0;
+      else if (tv != RT_FREE) rhs.bv[q] = front_stress(rhs, o.d.at(tv == RT_MARGIN_LO ? j : j + 1, i));
+    }
   }
 }
 
@@ -1432,6 +1550,13 @@ Op op_of(const Ctx* c, int l) {
   o.ax = c->lv[l].d.dx;   // placeholders, set below
   o.ay = 1.0;
   o.Na = c->lv[l].Na; o.Nb = c->lv[l].Nb; o.Bx = c->lv[l].Bx; o.By = c->lv[l].By;
+  o.inv_dx = 1.0 / c->lv[l].d.dx;
+  o.rtu = nullptr;
+  o.rtv = nullptr;
+  if (l == 0 && c->c.choice_ice_margin == DIVA_MARGIN_BC) {
+    o.rtu = c->rtu;
+    o.rtv = c->rtv;
+  }
   return o;
 }
 
@@ -1472,11 +1597,12 @@ static int sub_first_level(const Ctx* c);
 
 int solver_setup(Ctx* c) {
   const diva_config_t& C = c->c;
-  if (C.choice_ice_margin == DIVA_MARGIN_BC)
-    return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' is not implemented by the GPU solver");
+  // the 'BC' front rows live on the finest level only; a grid too small to coarsen
+  // would hand that level to the coarse direct solve, whose matrix has no front rows
+  if (C.choice_ice_margin == DIVA_MARGIN_BC && c->nlev < 2)
+    return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' needs nx or ny of at least 9");
   // level l's diagonal and level l+1's coefficients in one launch; the finest level's
-  // launch also forms the right-hand side
-  // the finest level's launch also forms the right-hand side, so it always runs on its own
+  // launch also forms the right-hand side, so it always runs on its own
   const int first_small = sub_first_level(c) > 1 ? sub_first_level(c) : 1;
   for (int l = 0; l < first_small && l < c->nlev; ++l) {
     const Level& F = c->lv[l];
@@ -1491,6 +1617,10 @@ int solver_setup(Ctx* c) {
       rhs.tdx = c->D(DIVA_F_TAUDX_CX); rhs.tdy = c->D(DIVA_F_TAUDY_CY);
       rhs.Ncx = c->D(DIVA_F_N_CX); rhs.Ncy = c->D(DIVA_F_N_CY);
       rhs.bu = c->kv[KV_B][0]; rhs.bv = c->kv[KV_B][1];
+      if (C.choice_ice_margin == DIVA_MARGIN_BC) {
+        rhs.rtu = c->rtu; rhs.rtv = c->rtv;
+        rhs.Hi = c->D(DIVA_F_HI_A); rhs.SL = c->D(DIVA_F_SL_A); rhs.Hb = c->D(DIVA_F_HB_A);
+      }
     }
     k_level_setup<<<GL(l)>>>(make_op(c, l), coarsen ? 1 : 0, K.d, fx, fy, K.Na, K.Nb, K.Bx, K.By, F.idu, F.idv,
                              rhs); c->launches++;
@@ -1556,7 +1686,9 @@ static size_t sub_bytes(const Ctx* c, int l) {
 
 // first level of the one-block sub-cycle: the largest whose levels all fit in shared memory
 static int sub_first_level(const Ctx* c) {
-  for (int l = 0; l < c->nlev; ++l)
+  // the finest level's 'BC' front rows are not in the sub-cycle's row tables
+  const int l0 = (c->c.choice_ice_margin == DIVA_MARGIN_BC && c->nlev > 1) ? 1 : 0;
+  for (int l = l0; l < c->nlev; ++l)
     if (sub_bytes(c, l) <= kSubSmemBudget) return l;
   return c->nlev - 1;
 }
@@ -1583,9 +1715,10 @@ static void tile_down_t(Ctx* c, int l, const Restriction& rs, const double* bu, 
   const Level& L = c->lv[l];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
   // b is written only when it is restricted here (rs.on), which never happens on the finest level
-  k_smooth_down<T, T, S><<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
-      make_op(c, l), rs, const_cast<double*>(bu), const_cast<double*>(bv), L.tu, L.tv, L.ru, L.rv, L.idu, L.idv,
-      nu);
+  const Op o = make_op(c, l);
+  auto kern = o.rtu ? k_smooth_down<T, T, S, true> : k_smooth_down<T, T, S, false>;
+  kern<<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
+      o, rs, const_cast<double*>(bu), const_cast<double*>(bv), L.tu, L.tv, L.ru, L.rv, L.idu, L.idv, nu);
   c->launches++;
 }
 template <int T, bool S>
@@ -1594,8 +1727,10 @@ static void tile_up_t(Ctx* c, int l, int fx, int fy, const double* bu, const dou
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
-  k_smooth_up<T, T, S><<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
-      make_op(c, l), make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, L.tu, L.tv, xu, xv, L.idu, L.idv, nu);
+  const Op o = make_op(c, l);
+  auto kern = o.rtu ? k_smooth_up<T, T, S, true> : k_smooth_up<T, T, S, false>;
+  kern<<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
+      o, make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, L.tu, L.tv, xu, xv, L.idu, L.idv, nu);
   c->launches++;
 }
 static int tile_down(Ctx* c, int l, const Restriction& rs, const double* bu, const double* bv, double* xu,
@@ -1689,14 +1824,20 @@ int solver_init(Ctx* c) {
   DIVA_CUDA(c, cudaFuncSetAttribute(k_small_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
-  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<32, 32, kStage32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)TileGeom<32, 32, kStage32>::smem));
-  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_up<32, 32, kStage32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)TileGeom<32, 32, kStage32>::smem));
-  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_down<16, 16, kStage16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)TileGeom<16, 16, kStage16>::smem));
-  DIVA_CUDA(c, cudaFuncSetAttribute(k_smooth_up<16, 16, kStage16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)TileGeom<16, 16, kStage16>::smem));
+  const void* tile32[4] = {(const void*)k_smooth_down<32, 32, kStage32, false>,
+                           (const void*)k_smooth_down<32, 32, kStage32, true>,
+                           (const void*)k_smooth_up<32, 32, kStage32, false>,
+                           (const void*)k_smooth_up<32, 32, kStage32, true>};
+  const void* tile16[4] = {(const void*)k_smooth_down<16, 16, kStage16, false>,
+                           (const void*)k_smooth_down<16, 16, kStage16, true>,
+                           (const void*)k_smooth_up<16, 16, kStage16, false>,
+                           (const void*)k_smooth_up<16, 16, kStage16, true>};
+  for (int k = 0; k < 4; ++k) {
+    DIVA_CUDA(c, cudaFuncSetAttribute(tile32[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)TileGeom<32, 32, kStage32>::smem));
+    DIVA_CUDA(c, cudaFuncSetAttribute(tile16[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)TileGeom<16, 16, kStage16>::smem));
+  }
   const BCs& b = c->bc;
   const int all[8] = {b.uW, b.uE, b.uS, b.uN, b.vW, b.vE, b.vS, b.vN};
   bool periodic = false;
@@ -1942,6 +2083,15 @@ double solver_vcycle_bytes(const Ctx* c) {
   for (int l = 0; l < c->nlev; ++l)
     b += (double)c->lv[l].d.nx * c->lv[l].d.ny * sizeof(double) * (4 * 10 + 8 + 6);
   return b;
+}
+
+// row types of the finest level (choice_ice_margin 'BC'), from the SICO masks of this solve
+int solver_row_types(Ctx* c) {
+  if (c->c.choice_ice_margin != DIVA_MARGIN_BC) return DIVA_OK;
+  k_row_types<<<GL(0)>>>(c->d, c->I(DIVA_F_DIVA_MASK_COMBI), c->I(DIVA_F_DIVA_ISFRONT_INNER),
+                         c->I(DIVA_F_DIVA_ISFRONT_OUTER), c->rtu, c->rtv); c->launches++;
+  DIVA_LAUNCHED(c, "k_row_types");
+  return DIVA_OK;
 }
 
 int solver_fill_boundary(Ctx* c, double* u, double* v) {

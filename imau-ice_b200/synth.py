@@ -62,7 +62,7 @@ ZETA = np.array([0.00, 0.10, 0.20, 0.30, 0.40, 0.50, 0.60, 0.70, 0.80, 0.90,
                  0.925, 0.95, 0.975, 0.99, 1.00])
 
 
-def marine_channel(seed=1, dx=5e3, zeta=ZETA):
+def marine_channel(seed=1, dx=5e3, zeta=ZETA, calving_front=False):
     """Config 1: 640 x 80 km channel (129 x 17 at 5 km), grounding line near x = 450 km.
 
     Bed: a trough from +100 m to -700 m along flow with a seeded low-order
@@ -70,6 +70,15 @@ def marine_channel(seed=1, dx=5e3, zeta=ZETA):
     thinning to flotation at x_gl = 450 km, then a thinning floating shelf.
     Temperature 243-273 K; Weertman friction coefficient lognormal
     (median 1e4, sigma 0.5).
+
+    ``calving_front=True`` cuts the shelf for the 'BC' ice-margin rows: open
+    ocean in the last column, every third interior row one column shorter (a
+    ragged front, so v rows meet it too), one open-ocean cell inside the shelf
+    (fronts facing both ways) and one ice-free land cell inside the shelf
+    (shelf-next-to-land rows).  No velocity point lies between two ocean cells
+    away from the domain boundary on purpose: with 'BC' the reference gives
+    ice-free cells zero viscosity and zero friction, so such rows keep only
+    b-grid shear terms (or none) and the matrix becomes singular.
     """
     rng = np.random.default_rng(seed)
     x, y = _axis(320e3, dx), _axis(40e3, dx)
@@ -97,6 +106,13 @@ def marine_channel(seed=1, dx=5e3, zeta=ZETA):
     H = np.minimum(H_center, np.maximum(0.0, Hs_center - Hb))
     H = H * (1.0 + 0.02 * _grf(rng, ny, nx, dx, 30e3))
     H = np.maximum(H, 0.0)
+    if calving_front:
+        H[:, nx - 1] = 0.0
+        H[2:ny - 2:3, nx - 2] = 0.0
+        H[ny // 2 - 2, nx - 20] = 0.0
+        jl, il = ny // 2 + 1, nx - 12
+        H[jl, il] = 0.0
+        Hb[jl, il] = 50.0
     T = _temperature(rng, zeta, ny, nx, 243.0, 273.0, dx, 60e3)
     fields = {
         "Hi_a": H, "Hb_a": Hb, "SL_a": np.zeros((ny, nx)), "dHb_dt_a": np.zeros((ny, nx)),

@@ -8,9 +8,9 @@ INT_FIELDS = {"mask_land_a", "mask_ocean_a", "mask_ice_a", "mask_sheet_a", "mask
               "DIVA_isfront_outer"}
 
 
-def make_case(cfg_id, dx=None, seed=None, overrides=None):
+def make_case(cfg_id, dx=None, seed=None, overrides=None, **gen_kw):
     gen = synth.CONFIGS[cfg_id]
-    kw = {}
+    kw = dict(gen_kw)
     if dx is not None:
         kw["dx"] = dx
     if seed is not None:

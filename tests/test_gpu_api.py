@@ -73,14 +73,40 @@ def test_wrong_dynamics_mode_is_rejected(cuda):
     ctx.close()
 
 
-def test_bc_margins_are_reported_unsupported(cuda):
-    g, cfg, f = small()
-    ctx = diva.Context(g, dict(cfg, choice_ice_margin="BC"), cuda)
-    helpers.prepare(ctx, f)
+def test_bc_margins_need_a_coarser_level(cuda):
+    """The 'BC' front rows live on the finest multigrid level; a grid below 9 points in
+    both directions has no coarser level and is refused instead of solved without them."""
+    n = 8
+    g = diva.Grid(n, n, 5e3)
+    f = {"Hi_a": np.full((n, n), 300.0), "Hb_a": np.full((n, n), -600.0), "SL_a": np.zeros((n, n)),
+         "Ti_a": np.full((g.nz, n, n), 260.0), "beta_sq_a": np.full((n, n), 1e4)}
+    f["Hb_a"][:, :3] = 100.0        # grounded ice upstream (a solve without sheet ice returns early)
+    f["Hi_a"][:, -2:] = 0.0
+    ctx = diva.Context(g, {"choice_ice_margin": "BC"}, cuda)
+    helpers.prepare(ctx, {k: np.asfortranarray(v) for k, v in f.items()})
     with pytest.raises(diva.DivaError) as e:
         ctx.solve_DIVA()
     assert e.value.status == _abi.UNSUPPORTED
     ctx.close()
+
+
+@pytest.mark.parametrize("dx", [5e3, 2.5e3])
+def test_bc_margins_same_result_on_every_launch_path(cuda, monkeypatch, dx):
+    """The cut shelf with 'BC' margins through the graph-launched viscosity loop, the
+    host-driven loop (DIVA_NO_GRAPHS=1) and the per-colour smoothing kernels
+    (DIVA_NO_TILES=1): the same iterations, bit for bit."""
+    g, cfg, f = helpers.make_case(1, dx=dx, overrides={"choice_ice_margin": "BC", "lin_rtol": 1e-10},
+                                  calving_front=True)
+    r1, o1 = helpers.run(cuda, g, cfg, f)
+    monkeypatch.setenv("DIVA_NO_GRAPHS", "1")
+    r2, o2 = helpers.run(cuda, g, cfg, f)
+    monkeypatch.setenv("DIVA_NO_TILES", "1")
+    r3, o3 = helpers.run(cuda, g, cfg, f)
+    assert r1["graph_launched"] == 1 and r2["graph_launched"] == 0
+    assert r1["picard_iterations"] == r2["picard_iterations"] == r3["picard_iterations"]
+    for k in ("u_vav_cx", "v_vav_cy", "u_3D_cx"):
+        assert np.array_equal(o1[k], o2[k]) and np.array_equal(o1[k], o3[k]), k
+    assert np.abs(o1["u_vav_cx"]).max() > 100.0
 
 
 def test_bad_grid_rejected(cuda):

@@ -173,6 +173,52 @@ def test_assembled_matrix_structure():
     assert np.all(A.diagonal()[bnd] == 1.0) and np.all(b[bnd] == 0.0)
 
 
+def test_bc_margin_rows():
+    """choice_ice_margin = 'BC' on the cut shelf: stress rows at every ice/ocean face
+    (ice_velocity_module.f90:2192-2341, 4 entries, rhs = the depth-integrated pressure
+    imbalance), identity rows where shelf meets ice-free land (:1787-1796), and a
+    non-singular matrix."""
+    g, cfg, f = synth.marine_channel(calving_front=True)
+    grid = diva.Grid(**g)
+    ctx = diva.Context(grid, dict(cfg, choice_ice_margin="BC"), ob.oracle_backend())
+    helpers.prepare(ctx, f)
+    lib = ctx.backend.lib
+    lib.orc_prepare_diva(ctx.h)
+    lib.orc_diva_coefficients(ctx.h)
+    lib.orc_assemble_current(ctx.h)
+    ptr, idx, val, b, x = ob.matrix(ctx)
+    m = ctx.download(["Hi_a", "DIVA_mask_combi"])
+    H, combi = m["Hi_a"], m["DIVA_mask_combi"]
+    nx, ny = grid.nx, grid.ny
+    eq = {}
+    n = 0
+    for i in range(nx):                                     # ice_velocity_module.f90:2840-2855
+        for j in range(ny):
+            if i < nx - 1:
+                eq[("u", j, i)] = n; n += 1
+            if j < ny - 1:
+                eq[("v", j, i)] = n; n += 1
+    nnz = np.diff(ptr)
+    fronts = idents = 0
+    for (kind, j, i), r in eq.items():
+        j2, i2 = (j, i + 1) if kind == "u" else (j + 1, i)
+        if (kind == "u" and i in (0, nx - 2)) or (kind == "v" and j in (0, ny - 2)) or j == 0 or j == ny - 1 \
+                or i == 0 or i == nx - 1:
+            continue
+        if {combi[j, i], combi[j2, i2]} == {1, 3}:
+            assert nnz[r] == 1 and val[ptr[r]] == 1.0 and b[r] == 0.0
+            idents += 1
+        elif (H[j, i] > 0) != (H[j2, i2] > 0) and 3 in (combi[j, i], combi[j2, i2]):
+            Hf = max(H[j, i], H[j2, i2])
+            assert nnz[r] == 4 and b[r] > 0.0 and b[r] < 0.5 * 910.0 * 9.81 * Hf ** 2
+            fronts += 1
+    assert idents == 4 and fronts == 19      # 5 notches x (1 u + 2 v) + 4 around the open cell
+    import scipy.sparse as sp
+    A = sp.csr_matrix((val, idx, ptr), shape=(len(b), len(b))).toarray()
+    s = np.linalg.svd(A, compute_uv=False)
+    assert s[-1] > 1e-3
+
+
 # ---- the Schoof (2006) SSA ice stream: known answer of the SSA path ----------------
 def test_ssa_matches_schoof2006():
     g, cfg, f = synth.schoof_icestream(dx=10e3)
