@@ -83,6 +83,7 @@ typedef struct orc_ctx {
   int SOR_nit; double SOR_tol, SOR_omega;
   double petsc_rtol, petsc_abstol;
   int lin_iters_last;
+  int true_residual;        /* GMRES tests the true residual (right preconditioning) */
   int threads;              /* threads of the timed CPU baseline (1: the sequential algorithm) */
   struct orc_pool* pool;    /* their workers (NULL with one thread) */
   long lin_iters_total;
@@ -1656,23 +1657,41 @@ static void scale_p(struct orc_pool* P, int n, const double* a, double s, double
   pool_run(P, vec_task_run, &v);
 }
 
-static int solve_gmres(orc_ctx* c, double rtol, double abstol, int maxit, int zero_guess) {
+/* right = 1: right preconditioning, A M^-1 y = b, x = M^-1 y; the Arnoldi residual is
+ * then the true residual ||b - A x||, tested against rtol ||b|| -- the test of the
+ * adaptive tolerance rule (the GPU's BiCGStab measures the true residual too).
+ * right = 0: left preconditioning with PETSc's default test on ||M^-1 (b - A x)||. */
+static int solve_gmres(orc_ctx* c, double rtol, double abstol, int maxit, int zero_guess, int right) {
   csr_t* m = &c->m;
   struct orc_pool* P = c->pool;   /* NULL: one thread, the sequential algorithm */
   const int n = m->m, R = 30;
   double* lu = (double*)malloc(sizeof(double) * m->nnz);
   int* diag = (int*)calloc((size_t)n, sizeof(int));
   ilu0_factor(P, m, lu, diag);
+  /* a zero pivot ends the solve, as PETSc's factorisation does ("zero pivot in LU
+   * factorization"); it arises from empty rows, e.g. between ocean cells with 'BC' margins */
+  for (int q = 0; q < n; ++q)
+    if (diag[q] < 0 || !(fabs(lu[diag[q]]) > 0.0) || !isfinite(lu[diag[q]])) {
+      free(lu); free(diag);
+      snprintf(c->err, sizeof(c->err), "ILU(0): zero pivot in row %d", q);
+      return DIVA_LINEAR_NOT_CONVERGED;
+    }
   double* V = (double*)malloc(sizeof(double) * (size_t)n * (R + 1));
   double *w = (double*)malloc(sizeof(double) * n), *t = (double*)malloc(sizeof(double) * n);
   double H[31 * 30], cs[30], sn[30], g[31], y[30];
   double* x = m->x;
+  double* z = right ? (double*)malloc(sizeof(double) * n) : NULL;
   if (zero_guess) memset(x, 0, sizeof(double) * n);
-  ilu0_apply(P, m, lu, diag, m->b, t);
-  double bnorm = nrm2_p(P, n, t);
+  double bnorm;
+  if (right) bnorm = nrm2_p(P, n, m->b);
+  else {
+    ilu0_apply(P, m, lu, diag, m->b, t);
+    bnorm = nrm2_p(P, n, t);
+  }
   spmv_p(P, m, x, w);
   for (int q = 0; q < n; ++q) w[q] = m->b[q] - w[q];
-  ilu0_apply(P, m, lu, diag, w, t);
+  if (right) memcpy(t, w, sizeof(double) * n);
+  else ilu0_apply(P, m, lu, diag, w, t);
   double rnorm = nrm2_p(P, n, t);
   /* PETSc's default test is relative to the initial residual, which is ||B b|| from a zero guess;
    * a warm start is measured against ||B b|| as well */
@@ -1686,8 +1705,13 @@ static int solve_gmres(orc_ctx* c, double rtol, double abstol, int maxit, int ze
     int kk = 0;
     for (; kk < R && it < maxit; ++kk) {
       ++it;
-      spmv_p(P, m, &V[(size_t)kk * n], w);
-      ilu0_apply(P, m, lu, diag, w, t);
+      if (right) {
+        ilu0_apply(P, m, lu, diag, &V[(size_t)kk * n], z);
+        spmv_p(P, m, z, t);
+      } else {
+        spmv_p(P, m, &V[(size_t)kk * n], w);
+        ilu0_apply(P, m, lu, diag, w, t);
+      }
       for (int l = 0; l <= kk; ++l) H[l * R + kk] = dot_p(P, n, t, &V[(size_t)l * n]);
       for (int l = 0; l <= kk; ++l) axpy_p(P, n, -H[l * R + kk], &V[(size_t)l * n], t);
       double hn = nrm2_p(P, n, t);
@@ -1710,24 +1734,32 @@ static int solve_gmres(orc_ctx* c, double rtol, double abstol, int maxit, int ze
       for (int q = l + 1; q < kk; ++q) s -= H[l * R + q] * y[q];
       y[l] = s / H[l * R + l];
     }
-    for (int l = 0; l < kk; ++l) axpy_p(P, n, y[l], &V[(size_t)l * n], x);
+    if (right) {   /* x += M^-1 (V y) */
+      memset(w, 0, sizeof(double) * n);
+      for (int l = 0; l < kk; ++l) axpy_p(P, n, y[l], &V[(size_t)l * n], w);
+      ilu0_apply(P, m, lu, diag, w, z);
+      axpy_p(P, n, 1.0, z, x);
+    } else {
+      for (int l = 0; l < kk; ++l) axpy_p(P, n, y[l], &V[(size_t)l * n], x);
+    }
     spmv_p(P, m, x, w);
     for (int q = 0; q < n; ++q) w[q] = m->b[q] - w[q];
-    ilu0_apply(P, m, lu, diag, w, t);
+    if (right) memcpy(t, w, sizeof(double) * n);
+    else ilu0_apply(P, m, lu, diag, w, t);
     rnorm = nrm2_p(P, n, t);
   }
-  if (rnorm > target) status = DIVA_LINEAR_NOT_CONVERGED;
+  if (!(rnorm <= target)) status = DIVA_LINEAR_NOT_CONVERGED;   /* NaN included */
   c->lin_iters_last = it;
   c->lin_iters_total += it;
-  free(lu); free(diag); free(V); free(w); free(t);
+  free(lu); free(diag); free(V); free(w); free(t); free(z);
   return status;
 }
 
 static int linear_solve(orc_ctx* c) {
   switch (c->lin_solver) {
     case ORC_LIN_SOR: return solve_sor(c);
-    case ORC_LIN_GMRES_ILU: return solve_gmres(c, c->petsc_rtol, c->petsc_abstol, 100000, 1);
-    case ORC_LIN_GMRES_WARM: return solve_gmres(c, c->petsc_rtol, c->petsc_abstol, 100000, 0);
+    case ORC_LIN_GMRES_ILU: return solve_gmres(c, c->petsc_rtol, c->petsc_abstol, 100000, 1, c->true_residual);
+    case ORC_LIN_GMRES_WARM: return solve_gmres(c, c->petsc_rtol, c->petsc_abstol, 100000, 0, c->true_residual);
     default: return solve_direct(c);
   }
 }
@@ -2073,9 +2105,12 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
     memcpy(FD(c, U_CX_PREV), u, sizeof(double) * ncx);
     memcpy(FD(c, V_CY_PREV), v, sizeof(double) * ncy);
     /* same adaptive linear tolerance rule as the GPU library (iterative solvers only) */
-    if (relmode && C->lin_adaptive && (c->lin_solver == ORC_LIN_GMRES_ILU || c->lin_solver == ORC_LIN_GMRES_WARM))
-      c->petsc_rtol = fmax(C->lin_rtol, eta * fmin(1.0, relres));
+    const int adaptive = relmode && C->lin_adaptive &&
+                         (c->lin_solver == ORC_LIN_GMRES_ILU || c->lin_solver == ORC_LIN_GMRES_WARM);
+    if (adaptive) c->petsc_rtol = fmax(C->lin_rtol, eta * fmin(1.0, relres));
+    c->true_residual = adaptive;
     int st = solve_stag_linearised(c, u, v);
+    c->true_residual = 0;
     if (st != DIVA_OK) status = st;
     apply_velocity_limits(c, u, v);
     relax_visc_iterations(c, u, v, C->DIVA_visc_it_relax);

@@ -109,6 +109,22 @@ def test_bc_margins_same_result_on_every_launch_path(cuda, monkeypatch, dx):
     assert np.abs(o1["u_vav_cx"]).max() > 100.0
 
 
+def test_bc_margins_singular_geometry_is_reported(cuda):
+    """'BC' with a wide open-ocean strip: rows between ocean cells are empty in the
+    reference's matrix (zero viscosity and friction there), so the system is singular;
+    the solve ends with an error status instead of returning velocities."""
+    g, cfg, f = helpers.make_case(1, overrides={"choice_ice_margin": "BC", "DIVA_visc_it_nit": 20})
+    H = np.array(f["Hi_a"])
+    H[:, -12:] = 0.0
+    f = dict(f, Hi_a=np.asfortranarray(H))
+    ctx = diva.Context(g, cfg, cuda)
+    helpers.prepare(ctx, f)
+    with pytest.raises(diva.DivaError) as e:
+        ctx.solve_DIVA()
+    assert e.value.status in (_abi.NAN_DETECTED, _abi.LINEAR_NOT_CONVERGED)
+    ctx.close()
+
+
 def test_bad_grid_rejected(cuda):
     with pytest.raises(diva.DivaError) as e:
         diva.Context(diva.Grid(3, 3, 1e3), {}, cuda)
@@ -209,3 +225,20 @@ def test_batch_solve_rejects_repeated_context(cuda):
     with pytest.raises(diva.DivaError):
         diva.solve_DIVA_batch([ctx, ctx])
     ctx.close()
+
+
+def test_ensemble_members_equal_lone_solves(cuda):
+    """An ensemble solved through the partition/batch driver on one rank gives each
+    member exactly its lone solve (same iterations, bit-identical velocities)."""
+    import dist_worker
+    from imau_ice_b200 import ensemble
+    members = dist_worker.small_channel_members(3)
+    g, cfg, f = helpers.make_case(2, dx=40e3, overrides={"lin_rtol": 1e-10})
+    members.append(("icecap-3", g, cfg, f))
+    res, parts = ensemble.solve_ensemble(members, cuda)
+    assert parts == [[0, 1, 2, 3]] and sorted(res) == [0, 1, 2, 3]
+    for k, (name, grid, c, fields) in enumerate(members):
+        r, o = helpers.run(cuda, grid, c, fields)
+        assert res[k]["report"]["picard_iterations"] == r["picard_iterations"], name
+        assert np.array_equal(res[k]["u_vav_cx"], o["u_vav_cx"]), name
+        assert np.array_equal(res[k]["v_vav_cy"], o["v_vav_cy"]), name
