@@ -58,11 +58,12 @@ TRAFFIC_KEYS = {5: "k_layer_viscosity_icecap321x561", 1: "k_smooth_down_icecap32
                 4: "k_subcycle_icecap321x561"}
 
 
-def workload(seed=2):
+def workload(seed=2, precision="fp64"):
     from imau_ice_b200 import synth
     g, cfg, fields = synth.ice_cap(seed=seed)
     cfg = dict(cfg)
-    cfg.update(picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1, lin_rtol=1e-10)
+    cfg.update(picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1, lin_rtol=1e-10,
+               precision=precision)
     return g, cfg, fields
 
 
@@ -219,7 +220,7 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     build.build()
 
-    g, cfg, fields = workload()
+    g, cfg, fields = workload(precision=args.precision)
     grid = diva.Grid(**g)
     ctx = diva.Context(grid, cfg)
     stream = torch.cuda.Stream()
@@ -361,6 +362,7 @@ def run_b200(args):
                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ice cap)",
                "config": config_json(g, {"parallelism": f"replicas x{world} (a single solve does not shard)",
+                                         "precision": args.precision,
                                          "picard_iterations": picard, "mg_cycles": mg,
                                          "relres": [r["relres"] for r in reps]}),
                "roofline": roofline, "clocks": clk,
@@ -474,6 +476,8 @@ def main():
     p.add_argument("--workload", choices=["icecap", "ensemble"], default="icecap",
                    help="icecap: the headline solve (default); ensemble: --members perturbed members")
     p.add_argument("--members", type=int, default=64)
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                   help="mixed: FP32 finest-level smoother inside the FP64 Krylov solve (not the default line)")
     args = p.parse_args()
     if args.impl == "b200" and args.workload == "ensemble":
         return run_ensemble(args)

@@ -125,6 +125,8 @@ int validate_config(Ctx* c, const diva_config_t* cfg) {
   if (cfg->DIVA_visc_it_nit < 1) return set_error(c, DIVA_BAD_INPUT, "DIVA_visc_it_nit must be >= 1");
   if (!(cfg->n_flow > 0.0)) return set_error(c, DIVA_BAD_INPUT, "n_flow must be > 0");
   if (cfg->lin_maxit < 1) return set_error(c, DIVA_BAD_INPUT, "lin_maxit must be >= 1");
+  if (cfg->precision != DIVA_PREC_FP64 && cfg->precision != DIVA_PREC_MIXED)
+    return set_error(c, DIVA_BAD_INPUT, "precision must be DIVA_PREC_FP64 or DIVA_PREC_MIXED");
   if (cfg->lin_adaptive && !(cfg->lin_adaptive_eta > 0.0 && cfg->lin_adaptive_eta < 1.0))
     return set_error(c, DIVA_BAD_INPUT, "lin_adaptive_eta must lie in (0, 1)");
   const int bcs[8] = {cfg->BC_u_west, cfg->BC_u_east, cfg->BC_u_south, cfg->BC_u_north,
@@ -175,6 +177,7 @@ size_t carve(Ctx* c, Carver& cv) {
   c->staging = (double*)cv.take(sizeof(double) * d.nz * d.plane);
   c->col_eps = (double*)cv.take(sizeof(double) * d.plane);
   c->col_flags = (int*)cv.take(sizeof(int) * d.plane);
+  for (int k = 0; k < 6; ++k) c->f32[k] = (float*)cv.take(sizeof(float) * d.plane);
   c->rtu = (int8_t*)cv.take(d.plane);
   c->rtv = (int8_t*)cv.take(d.plane);
   c->ff_ocean = (int*)cv.take(sizeof(int) * 2 * d.plane);

@@ -36,6 +36,9 @@ struct BCs {
   int uW, uE, uS, uN, vW, vE, vS, vN;
 };
 
+// Float planes of the finest level for the mixed-precision preconditioner.
+enum { F32_NA = 0, F32_NB, F32_BX, F32_BY, F32_IDU, F32_IDV };
+
 // Krylov vectors on the fine level, each a (u,v) pair of planes.
 enum { KV_X = 0, KV_R, KV_RHAT, KV_P, KV_PHAT, KV_V, KV_S, KV_SHAT, KV_T, KV_B, KV_COUNT };
 
@@ -81,6 +84,7 @@ struct Ctx {
   double* staging = nullptr;          // upload/download staging (largest field)
   double* col_eps = nullptr;          // column coefficients: mean-flow strain rate per column
   int* col_flags = nullptr;           // column coefficients: shear faces with ice
+  float* f32[6] = {};                 // float copies of the finest level (F32_*, precision 'mixed')
   int8_t* rtu = nullptr;              // finest-level row types ('BC' ice margins)
   int8_t* rtv = nullptr;
   int* ff_ocean = nullptr;            // flood-fill state

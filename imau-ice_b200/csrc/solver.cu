@@ -37,15 +37,20 @@ namespace {
 
 constexpr int kSubThreads = 1024;       // threads of the one-block coarse-level kernel
 
-struct Op {
+// A level's operator.  R is the type of its coefficients and of the x values it is
+// applied to: double everywhere, float for the finest level's smoother copies of the
+// mixed-precision preconditioner (precision = DIVA_PREC_MIXED).
+template <class R>
+struct OpT {
   Dims d;
   BCs bc;
   double ax, ay;   // hy/hx and hx/hy of the level's cells (1 on the fine grid)
-  const double *Na, *Nb, *Bx, *By;
+  const R *Na, *Nb, *Bx, *By;
   // 'BC' ice margins (finest level only, else null): the type of each u and v row
   const int8_t *rtu, *rtv;
   double inv_dx;
 };
+using Op = OpT<double>;
 
 // Row types of the finest level with choice_ice_margin 'BC' (solve_DIVA_stag_linearised
 // :1683-1727): a free row, u = 0 (shelf next to land, or a front cell with ocean on both
@@ -114,17 +119,17 @@ struct TIx {
 
 // Read a u (v) value through the boundary elimination (RAW = false), or as
 // stored (RAW = true: the reference's assembled rows reference stored values).
-template <bool RAW, class IX>
-__device__ __forceinline__ double LUx(const Op& o, const double* x, const IX& ix, int j, int i) {
+template <bool RAW, class R, class IX>
+__device__ __forceinline__ R LUx(const OpT<R>& o, const R* x, const IX& ix, int j, int i) {
   if (RAW) return x[ix(j, i)];
   int js, is;
-  return u_src(o.d, o.bc, j, i, js, is) ? x[ix(js, is)] : 0.0;
+  return u_src(o.d, o.bc, j, i, js, is) ? x[ix(js, is)] : R(0);
 }
-template <bool RAW, class IX>
-__device__ __forceinline__ double LVx(const Op& o, const double* x, const IX& ix, int j, int i) {
+template <bool RAW, class R, class IX>
+__device__ __forceinline__ R LVx(const OpT<R>& o, const R* x, const IX& ix, int j, int i) {
   if (RAW) return x[ix(j, i)];
   int js, is;
-  return v_src(o.d, o.bc, j, i, js, is) ? x[ix(js, is)] : 0.0;
+  return v_src(o.d, o.bc, j, i, js, is) ? x[ix(js, is)] : R(0);
 }
 template <bool RAW = false>
 __device__ __forceinline__ double LU(const Op& o, const double* x, int j, int i) {
@@ -138,74 +143,79 @@ __device__ __forceinline__ double LV(const Op& o, const double* x, int j, int i)
 // Sum of the nine stencil terms, accumulated with explicit fused multiply-adds in a
 // fixed order, so every code path (boundary-mapped reads, plain reads, the row
 // tables of the sub-cycle) rounds identically whatever the compiler would contract.
-__device__ __forceinline__ double stencil9(double c0, double x0, double c1, double x1, double c2, double x2,
-                                           double c3, double x3, double c4, double x4, double c5, double x5,
-                                           double c6, double x6, double c7, double x7, double c8, double x8) {
-  double s = c0 * x0;
-  s = fma(c1, x1, s);
-  s = fma(c2, x2, s);
-  s = fma(c3, x3, s);
-  s = fma(c4, x4, s);
-  s = fma(c5, x5, s);
-  s = fma(c6, x6, s);
-  s = fma(c7, x7, s);
-  return fma(c8, x8, s);
+__device__ __forceinline__ double fma_r(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fma_r(float a, float b, float c) { return fmaf(a, b, c); }
+
+template <class R>
+__device__ __forceinline__ R stencil9(R c0, R x0, R c1, R x1, R c2, R x2, R c3, R x3, R c4, R x4, R c5, R x5, R c6,
+                                      R x6, R c7, R x7, R c8, R x8) {
+  R s = c0 * x0;
+  s = fma_r(c1, x1, s);
+  s = fma_r(c2, x2, s);
+  s = fma_r(c3, x3, s);
+  s = fma_r(c4, x4, s);
+  s = fma_r(c5, x5, s);
+  s = fma_r(c6, x6, s);
+  s = fma_r(c7, x7, s);
+  return fma_r(c8, x8, s);
 }
 
-__device__ __forceinline__ double stencil4(double c0, double x0, double c1, double x1, double c2, double x2,
-                                           double c3, double x3) {
-  double s = c0 * x0;
-  s = fma(c1, x1, s);
-  s = fma(c2, x2, s);
-  return fma(c3, x3, s);
+template <class R>
+__device__ __forceinline__ R stencil4(R c0, R x0, R c1, R x1, R c2, R x2, R c3, R x3) {
+  R s = c0 * x0;
+  s = fma_r(c1, x1, s);
+  s = fma_r(c2, x2, s);
+  return fma_r(c3, x3, s);
 }
 
 // (A x) of the u row at interior (j,i) (list_DIVA_matrix_coefficients_eq_1_free :2342-2404)
 // IX places x values, CX the coefficients N_a, N_b, B (a level plane or a shared-memory tile)
-template <bool RAW, bool FRONT = true, class IX, class CX>
-__device__ __forceinline__ double AuXC(const Op& o, const double* xu, const double* xv, const IX& ix, const CX& cx,
-                                       int j, int i) {
+// (the constants are written R(k) so that R = double performs exactly the double
+// operations of the reference's rows and R = float stays in single precision)
+template <bool RAW, bool FRONT = true, class R, class IX, class CX>
+__device__ __forceinline__ R AuXC(const OpT<R>& o, const R* xu, const R* xv, const IX& ix, const CX& cx, int j,
+                                  int i) {
   if (FRONT && o.rtu) {
     const int t = o.rtu[o.d.at(j, i)];
     if (t == RT_IDENT) return xu[ix(j, i)];
     if (t != RT_FREE) {   // front row: -4N u(i1-1) + 4N u(i1) - 2N v(j-1,i1) + 2N v(j,i1), N = N_a(i1)/dx
       const int i1 = t == RT_MARGIN_LO ? i : i + 1;
-      const double N = o.Na[cx(j, i1)];
-      return stencil4(-4.0 * o.inv_dx * N, LUx<RAW>(o, xu, ix, j, i1 - 1), 4.0 * o.inv_dx * N,
-                      LUx<RAW>(o, xu, ix, j, i1), -2.0 * o.inv_dx * N, LVx<RAW>(o, xv, ix, j - 1, i1),
-                      2.0 * o.inv_dx * N, LVx<RAW>(o, xv, ix, j, i1));
+      const R N = o.Na[cx(j, i1)], idx = R(o.inv_dx);
+      return stencil4(R(-4) * idx * N, LUx<RAW>(o, xu, ix, j, i1 - 1), R(4) * idx * N, LUx<RAW>(o, xu, ix, j, i1),
+                      R(-2) * idx * N, LVx<RAW>(o, xv, ix, j - 1, i1), R(2) * idx * N, LVx<RAW>(o, xv, ix, j, i1));
     }
   }
-  const double Ae = o.Na[cx(j, i + 1)], Aw = o.Na[cx(j, i)], Bn = o.Nb[cx(j, i)], Bs = o.Nb[cx(j - 1, i)];
-  const double cE = 4.0 * o.ax * Ae, cW = 4.0 * o.ax * Aw, cN = o.ay * Bn, cS = o.ay * Bs;
-  const double diag = -(cE + cW + cN + cS) - o.Bx[cx(j, i)];
+  const R Ae = o.Na[cx(j, i + 1)], Aw = o.Na[cx(j, i)], Bn = o.Nb[cx(j, i)], Bs = o.Nb[cx(j - 1, i)];
+  const R ax = R(o.ax), ay = R(o.ay);
+  const R cE = R(4) * ax * Ae, cW = R(4) * ax * Aw, cN = ay * Bn, cS = ay * Bs;
+  const R diag = -(cE + cW + cN + cS) - o.Bx[cx(j, i)];
   return stencil9(cE, LUx<RAW>(o, xu, ix, j, i + 1), cW, LUx<RAW>(o, xu, ix, j, i - 1), cN,
                   LUx<RAW>(o, xu, ix, j + 1, i), cS, LUx<RAW>(o, xu, ix, j - 1, i), diag, xu[ix(j, i)],
-                  -2.0 * Aw - Bn, LVx<RAW>(o, xv, ix, j, i), 2.0 * Ae + Bn, LVx<RAW>(o, xv, ix, j, i + 1),
-                  2.0 * Aw + Bs, LVx<RAW>(o, xv, ix, j - 1, i), -2.0 * Ae - Bs, LVx<RAW>(o, xv, ix, j - 1, i + 1));
+                  R(-2) * Aw - Bn, LVx<RAW>(o, xv, ix, j, i), R(2) * Ae + Bn, LVx<RAW>(o, xv, ix, j, i + 1),
+                  R(2) * Aw + Bs, LVx<RAW>(o, xv, ix, j - 1, i), R(-2) * Ae - Bs, LVx<RAW>(o, xv, ix, j - 1, i + 1));
 }
 // (A x) of the v row at interior (j,i) (list_DIVA_matrix_coefficients_eq_2_free :2405-2467)
-template <bool RAW, bool FRONT = true, class IX, class CX>
-__device__ __forceinline__ double AvXC(const Op& o, const double* xu, const double* xv, const IX& ix, const CX& cx,
-                                       int j, int i) {
+template <bool RAW, bool FRONT = true, class R, class IX, class CX>
+__device__ __forceinline__ R AvXC(const OpT<R>& o, const R* xu, const R* xv, const IX& ix, const CX& cx, int j,
+                                  int i) {
   if (FRONT && o.rtv) {
     const int t = o.rtv[o.d.at(j, i)];
     if (t == RT_IDENT) return xv[ix(j, i)];
     if (t != RT_FREE) {   // front row: -4N v(j1-1) + 4N v(j1) - 2N u(j1,i-1) + 2N u(j1,i), N = N_a(j1)/dx
       const int j1 = t == RT_MARGIN_LO ? j : j + 1;
-      const double N = o.Na[cx(j1, i)];
-      return stencil4(-4.0 * o.inv_dx * N, LVx<RAW>(o, xv, ix, j1 - 1, i), 4.0 * o.inv_dx * N,
-                      LVx<RAW>(o, xv, ix, j1, i), -2.0 * o.inv_dx * N, LUx<RAW>(o, xu, ix, j1, i - 1),
-                      2.0 * o.inv_dx * N, LUx<RAW>(o, xu, ix, j1, i));
+      const R N = o.Na[cx(j1, i)], idx = R(o.inv_dx);
+      return stencil4(R(-4) * idx * N, LVx<RAW>(o, xv, ix, j1 - 1, i), R(4) * idx * N, LVx<RAW>(o, xv, ix, j1, i),
+                      R(-2) * idx * N, LUx<RAW>(o, xu, ix, j1, i - 1), R(2) * idx * N, LUx<RAW>(o, xu, ix, j1, i));
     }
   }
-  const double An = o.Na[cx(j + 1, i)], As = o.Na[cx(j, i)], Be = o.Nb[cx(j, i)], Bw = o.Nb[cx(j, i - 1)];
-  const double cN = 4.0 * o.ay * An, cS = 4.0 * o.ay * As, cE = o.ax * Be, cW = o.ax * Bw;
-  const double diag = -(cN + cS + cE + cW) - o.By[cx(j, i)];
+  const R An = o.Na[cx(j + 1, i)], As = o.Na[cx(j, i)], Be = o.Nb[cx(j, i)], Bw = o.Nb[cx(j, i - 1)];
+  const R ax = R(o.ax), ay = R(o.ay);
+  const R cN = R(4) * ay * An, cS = R(4) * ay * As, cE = ax * Be, cW = ax * Bw;
+  const R diag = -(cN + cS + cE + cW) - o.By[cx(j, i)];
   return stencil9(cN, LVx<RAW>(o, xv, ix, j + 1, i), cS, LVx<RAW>(o, xv, ix, j - 1, i), cE,
                   LVx<RAW>(o, xv, ix, j, i + 1), cW, LVx<RAW>(o, xv, ix, j, i - 1), diag, xv[ix(j, i)],
-                  -2.0 * An - Bw, LUx<RAW>(o, xu, ix, j + 1, i - 1), 2.0 * An + Be, LUx<RAW>(o, xu, ix, j + 1, i),
-                  2.0 * As + Bw, LUx<RAW>(o, xu, ix, j, i - 1), -2.0 * As - Be, LUx<RAW>(o, xu, ix, j, i));
+                  R(-2) * An - Bw, LUx<RAW>(o, xu, ix, j + 1, i - 1), R(2) * An + Be, LUx<RAW>(o, xu, ix, j + 1, i),
+                  R(2) * As + Bw, LUx<RAW>(o, xu, ix, j, i - 1), R(-2) * As - Be, LUx<RAW>(o, xu, ix, j, i));
 }
 template <bool RAW, class IX>
 __device__ __forceinline__ double AuX(const Op& o, const double* xu, const double* xv, const IX& ix, int j, int i) {
@@ -373,8 +383,9 @@ __device__ __forceinline__ int scatter_node(int f, int f2, int* C, double* w) {
 
 // b_c = P^T r_f on coarse interior points; x_c = 0
 // (P^T r_f) at the coarse point (j,i): the restricted u and v residuals (zero off the coarse interior)
-__device__ __forceinline__ void restrict_values(const Dims& df, const Dims& dc, int fx, int fy, const double* ru,
-                                                const double* rv, int j, int i, double& bu, double& bv) {
+template <class RR>
+__device__ __forceinline__ void restrict_values(const Dims& df, const Dims& dc, int fx, int fy, const RR* ru,
+                                                const RR* rv, int j, int i, double& bu, double& bv) {
   int fi[4], fj[4];
   double wi[4], wj[4];
   double s = 0.0;
@@ -382,7 +393,7 @@ __device__ __forceinline__ void restrict_values(const Dims& df, const Dims& dc, 
     const int ni = gather_cell(i, fx, fi, wi), nj = gather_node(j, fy, fj, wj);
     for (int a = 0; a < nj; ++a)
       for (int b = 0; b < ni; ++b)
-        if (u_int(df, fj[a], fi[b])) s += wj[a] * wi[b] * ru[df.at(fj[a], fi[b])];
+        if (u_int(df, fj[a], fi[b])) s += wj[a] * wi[b] * (double)ru[df.at(fj[a], fi[b])];
   }
   bu = s;
   s = 0.0;
@@ -390,7 +401,7 @@ __device__ __forceinline__ void restrict_values(const Dims& df, const Dims& dc, 
     const int ni = gather_node(i, fx, fi, wi), nj = gather_cell(j, fy, fj, wj);
     for (int a = 0; a < nj; ++a)
       for (int b = 0; b < ni; ++b)
-        if (v_int(df, fj[a], fi[b])) s += wj[a] * wi[b] * rv[df.at(fj[a], fi[b])];
+        if (v_int(df, fj[a], fi[b])) s += wj[a] * wi[b] * (double)rv[df.at(fj[a], fi[b])];
   }
   bv = s;
 }
@@ -472,10 +483,12 @@ constexpr int kTileThreads = 512;
 
 // STAGE: the region's coefficients (N_a, N_b, B_x, B_y and the inverse diagonals)
 // are staged in shared memory too, so the colour passes touch no global memory.
-template <int TJ, int TI, bool STAGE>
+// R: the type of the tile's values and coefficients (float on the finest level of the
+// mixed-precision preconditioner, else double).
+template <int TJ, int TI, bool STAGE, class R = double>
 struct TileGeom {
   static constexpr int RJ = TJ + 2 * kHalo, RI = TI + 2 * kHalo, N = RJ * RI;
-  static constexpr size_t smem = (STAGE ? 10 : 4) * N * sizeof(double);   // x, b (+ 6 coefficient planes)
+  static constexpr size_t smem = (STAGE ? 10 : 4) * N * sizeof(R);   // x, b (+ 6 coefficient planes)
 };
 
 // A block whose whole region lies in the interior of both components (u: 1 <= i <=
@@ -492,13 +505,13 @@ __device__ __forceinline__ bool tile_deep(const TIx& ix, const Dims& d) {
 // The shared-memory planes of a tile kernel and the operator reading from them.
 // FRONT: the operator may carry 'BC' front rows (only the finest level's kernels with
 // choice_ice_margin 'BC'); without it the row-type test is compiled out.
-template <int TJ, int TI, bool STAGE, bool FRONT>
+template <int TJ, int TI, bool STAGE, bool FRONT, class R>
 struct TileMem {
-  double *xu, *xv, *bu, *bv;
-  const double *iu, *iv;   // inverse diagonals: staged plane or the level's
-  Op os;                   // the level's operator, coefficients staged when STAGE
-  __device__ TileMem(double* sm, const Op& o, const double* idu, const double* idv) {
-    using G = TileGeom<TJ, TI, STAGE>;
+  R *xu, *xv, *bu, *bv;
+  const R *iu, *iv;   // inverse diagonals: staged plane or the level's
+  OpT<R> os;          // the level's operator, coefficients staged when STAGE
+  __device__ TileMem(R* sm, const OpT<R>& o, const R* idu, const R* idv) {
+    using G = TileGeom<TJ, TI, STAGE, R>;
     xu = sm; xv = sm + G::N; bu = sm + 2 * G::N; bv = sm + 3 * G::N;
     os = o;
     iu = idu; iv = idv;
@@ -508,40 +521,39 @@ struct TileMem {
     }
   }
   // stage the region's coefficients (out-of-domain points are never read)
-  __device__ void stage(const Op& o, const double* idu, const double* idv, const TIx& ix, int t, bool in,
-                        long long q) {
+  __device__ void stage(const OpT<R>& o, const R* idu, const R* idv, const TIx& ix, int t, bool in, long long q) {
     if (!STAGE) return;
-    using G = TileGeom<TJ, TI, STAGE>;
-    double* sm = xu;
-    sm[4 * G::N + t] = in ? o.Na[q] : 0.0;
-    sm[5 * G::N + t] = in ? o.Nb[q] : 0.0;
-    sm[6 * G::N + t] = in ? o.Bx[q] : 0.0;
-    sm[7 * G::N + t] = in ? o.By[q] : 0.0;
-    sm[8 * G::N + t] = in ? idu[q] : 0.0;
-    sm[9 * G::N + t] = in ? idv[q] : 0.0;
+    using G = TileGeom<TJ, TI, STAGE, R>;
+    R* sm = xu;
+    sm[4 * G::N + t] = in ? o.Na[q] : R(0);
+    sm[5 * G::N + t] = in ? o.Nb[q] : R(0);
+    sm[6 * G::N + t] = in ? o.Bx[q] : R(0);
+    sm[7 * G::N + t] = in ? o.By[q] : R(0);
+    sm[8 * G::N + t] = in ? idu[q] : R(0);
+    sm[9 * G::N + t] = in ? idv[q] : R(0);
   }
   template <bool RAW>
-  __device__ __forceinline__ double Au(const TIx& ix, int j, int i) const {
+  __device__ __forceinline__ R Au(const TIx& ix, int j, int i) const {
     if (STAGE) return AuXC<RAW, FRONT>(os, xu, xv, ix, ix, j, i);
     return AuXC<RAW, FRONT>(os, xu, xv, ix, GIx{os.d}, j, i);
   }
   template <bool RAW>
-  __device__ __forceinline__ double Av(const TIx& ix, int j, int i) const {
+  __device__ __forceinline__ R Av(const TIx& ix, int j, int i) const {
     if (STAGE) return AvXC<RAW, FRONT>(os, xu, xv, ix, ix, j, i);
     return AvXC<RAW, FRONT>(os, xu, xv, ix, GIx{os.d}, j, i);
   }
-  __device__ __forceinline__ double idu(const TIx& ix, int j, int i) const {
+  __device__ __forceinline__ R idu(const TIx& ix, int j, int i) const {
     return STAGE ? iu[ix(j, i)] : iu[os.d.at(j, i)];
   }
-  __device__ __forceinline__ double idv(const TIx& ix, int j, int i) const {
+  __device__ __forceinline__ R idv(const TIx& ix, int j, int i) const {
     return STAGE ? iv[ix(j, i)] : iv[os.d.at(j, i)];
   }
 };
 
 // one colour pass over the region points within `reach` of the tile
-template <int TJ, int TI, bool STAGE, bool FRONT, bool DEEP>
-__device__ __forceinline__ void tile_pass(TileMem<TJ, TI, STAGE, FRONT>& m, const TIx& ix, int tj0, int ti0, int comp,
-                                          int color, int reach) {
+template <bool DEEP, class M>
+__device__ __forceinline__ void tile_pass(M& m, const TIx& ix, int TJ, int TI, int tj0, int ti0, int comp, int color,
+                                          int reach) {
   const Dims& d = m.os.d;
   // the box of points within `reach` of the tile, one colour of it
   const int bj0 = tj0 - reach, bi0 = ti0 - reach, BJ = TJ + 2 * reach, BI = TI + 2 * reach;
@@ -559,11 +571,11 @@ __device__ __forceinline__ void tile_pass(TileMem<TJ, TI, STAGE, FRONT>& m, cons
     }
   }
 }
-template <int TJ, int TI, bool STAGE, bool FRONT>
-__device__ __forceinline__ void tile_pass_any(bool deep, TileMem<TJ, TI, STAGE, FRONT>& m, const TIx& ix, int tj0, int ti0,
-                                              int comp, int color, int reach) {
-  if (deep) tile_pass<TJ, TI, STAGE, FRONT, true>(m, ix, tj0, ti0, comp, color, reach);
-  else tile_pass<TJ, TI, STAGE, FRONT, false>(m, ix, tj0, ti0, comp, color, reach);
+template <int TJ, int TI, class M>
+__device__ __forceinline__ void tile_pass_any(bool deep, M& m, const TIx& ix, int tj0, int ti0, int comp, int color,
+                                              int reach) {
+  if (deep) tile_pass<true>(m, ix, TJ, TI, tj0, ti0, comp, color, reach);
+  else tile_pass<false>(m, ix, TJ, TI, tj0, ti0, comp, color, reach);
 }
 
 // Source of b for a pre-smoothing kernel: given on the level (the finest), or the
@@ -572,18 +584,30 @@ struct Restriction {
   int on;              // 0: b given in gbu/gbv
   Dims df;             // finer level
   int fx, fy;          // coarsening factors from it
-  const double *ru, *rv;
+  const void *ru, *rv; // its residual: double, or float (rfloat) from a mixed-precision finest level
+  int rfloat;
 };
+__device__ __forceinline__ void restrict_from(const Restriction& rs, const Dims& dc, int j, int i, double& b0,
+                                              double& b1) {
+  if (rs.rfloat)
+    restrict_values(rs.df, dc, rs.fx, rs.fy, static_cast<const float*>(rs.ru), static_cast<const float*>(rs.rv), j,
+                    i, b0, b1);
+  else
+    restrict_values(rs.df, dc, rs.fx, rs.fy, static_cast<const double*>(rs.ru), static_cast<const double*>(rs.rv),
+                    j, i, b0, b1);
+}
 
 // pre-smoothing from x = 0 (the descent of a V-cycle enters every level with x = 0):
-// `sweeps` forward sweeps (u0 u1 v0 v1), then x, b and r = b - A x of the tile
-template <int TJ, int TI, bool STAGE, bool FRONT>
-__global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction rs, double* gbu, double* gbv,
-                                                              double* gxu, double* gxv, double* gru, double* grv,
-                                                              const double* idu, const double* idv, int sweeps) {
+// `sweeps` forward sweeps (u0 u1 v0 v1), then x, b and r = b - A x of the tile.
+// b is read (and, when restricted here, stored) in double; x and r are written in R.
+template <int TJ, int TI, bool STAGE, bool FRONT, class R>
+__global__ void __launch_bounds__(kTileThreads) k_smooth_down(OpT<R> o, Restriction rs, double* gbu, double* gbv,
+                                                              R* gxu, R* gxv, R* gru, R* grv, const R* idu,
+                                                              const R* idv, int sweeps) {
   constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
-  extern __shared__ double sm[];
-  TileMem<TJ, TI, STAGE, FRONT> m(sm, o, idu, idv);
+  extern __shared__ double smd[];
+  R* sm = reinterpret_cast<R*>(smd);
+  TileMem<TJ, TI, STAGE, FRONT, R> m(sm, o, idu, idv);
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
   const TIx ix{tj0 - kHalo, ti0 - kHalo, RJ};
@@ -595,23 +619,23 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
     double b0 = 0.0, b1 = 0.0;
     if (in) {
       if (rs.on) {
-        restrict_values(rs.df, d, rs.fx, rs.fy, rs.ru, rs.rv, j, i, b0, b1);
+        restrict_from(rs, d, j, i, b0, b1);
       } else {
         b0 = gbu[q];
         b1 = gbv[q];
       }
     }
-    m.xu[t] = 0.0;
-    m.xv[t] = 0.0;
-    m.bu[t] = b0;
-    m.bv[t] = b1;
+    m.xu[t] = R(0);
+    m.xv[t] = R(0);
+    m.bu[t] = R(b0);
+    m.bv[t] = R(b1);
     m.stage(o, idu, idv, ix, t, in, q);
   }
   __syncthreads();
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 0; p < 4; ++p, ++pass) {
-      tile_pass_any<TJ, TI, STAGE, FRONT>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -629,8 +653,8 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
       gru[q] = m.bu[k] - m.template Au<true>(ix, j, i);
       grv[q] = m.bv[k] - m.template Av<true>(ix, j, i);
     } else {
-      gru[q] = u_int(d, j, i) ? m.bu[k] - m.template Au<false>(ix, j, i) : 0.0;
-      grv[q] = v_int(d, j, i) ? m.bv[k] - m.template Av<false>(ix, j, i) : 0.0;
+      gru[q] = u_int(d, j, i) ? m.bu[k] - m.template Au<false>(ix, j, i) : R(0);
+      grv[q] = v_int(d, j, i) ? m.bv[k] - m.template Av<false>(ix, j, i) : R(0);
     }
   }
 }
@@ -638,16 +662,17 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(Op o, Restriction 
 // post-smoothing: x += P x_c, then `sweeps` backward sweeps (v1 v0 u1 u0); x of the tile.
 // The pre-smoothed x is read over the halo from (gxu, gxv) and the result written to
 // (oxu, oxv): separate arrays, since blocks of other tiles may still be reading the
-// halo when this block writes (the grid runs in several waves on large levels).
-template <int TJ, int TI, bool STAGE, bool FRONT>
-__global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx, int fy, const double* xcu,
+// halo when this block writes (the grid runs in several waves on large levels).  The
+// coarse correction and b are double; the smoothing runs in R; the output is double.
+template <int TJ, int TI, bool STAGE, bool FRONT, class R>
+__global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int fx, int fy, const double* xcu,
                                                             const double* xcv, const double* gbu, const double* gbv,
-                                                            const double* gxu, const double* gxv, double* oxu,
-                                                            double* oxv, const double* idu, const double* idv,
-                                                            int sweeps) {
+                                                            const R* gxu, const R* gxv, double* oxu, double* oxv,
+                                                            const R* idu, const R* idv, int sweeps) {
   constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
-  extern __shared__ double sm[];
-  TileMem<TJ, TI, STAGE, FRONT> m(sm, o, idu, idv);
+  extern __shared__ double smd[];
+  R* sm = reinterpret_cast<R*>(smd);
+  TileMem<TJ, TI, STAGE, FRONT, R> m(sm, o, idu, idv);
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
   const TIx ix{tj0 - kHalo, ti0 - kHalo, RJ};
@@ -667,17 +692,17 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(Op o, Op oc, int fx,
       ba = gbu[q];
       bb = gbv[q];
     }
-    m.xu[t] = xa;
-    m.xv[t] = xb;
-    m.bu[t] = ba;
-    m.bv[t] = bb;
+    m.xu[t] = R(xa);
+    m.xv[t] = R(xb);
+    m.bu[t] = R(ba);
+    m.bv[t] = R(bb);
     m.stage(o, idu, idv, ix, t, in, q);
   }
   __syncthreads();
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 3; p >= 0; --p, ++pass) {
-      tile_pass_any<TJ, TI, STAGE, FRONT>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -953,7 +978,7 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
       if (l == sc.first) {   // entered with x = 0
         double b0, b1;
         if (sc.rs.on) {
-          restrict_values(sc.rs.df, g, sc.rs.fx, sc.rs.fy, sc.rs.ru, sc.rs.rv, t % g.ny, t / g.ny, b0, b1);
+          restrict_from(sc.rs, g, t % g.ny, t / g.ny, b0, b1);
         } else {
           b0 = bu0[q];
           b1 = bv0[q];
@@ -1159,13 +1184,26 @@ __device__ __forceinline__ double front_stress(const RhsArgs& r, long long q) {
 // Operator set-up of one level in one launch over its points: the inverse diagonals of
 // level l, the rediscretised coefficients of level l+1 (coarse points are a subset of
 // the fine index range) and, on the finest level, the right-hand side.
+// float copies of the finest level's coefficients and inverse diagonals (DIVA_PREC_MIXED)
+struct F32Out {
+  float *Na, *Nb, *Bx, *By, *idu, *idv;
+};
+
 __global__ void k_level_setup(Op o, int coarsen, Dims dc, int fx, int fy, double* cNa, double* cNb, double* cBx,
-                              double* cBy, double* idu, double* idv, RhsArgs rhs) {
+                              double* cBy, double* idu, double* idv, RhsArgs rhs, F32Out f32) {
   IDX2D
   if (j >= o.d.ny || i >= o.d.nx) return;
   const long long q = o.d.at(j, i);
   idu[q] = u_int(o.d, j, i) ? 1.0 / diag_u(o, j, i) : 0.0;
   idv[q] = v_int(o.d, j, i) ? 1.0 / diag_v(o, j, i) : 0.0;
+  if (f32.Na) {
+    f32.Na[q] = (float)o.Na[q];
+    f32.Nb[q] = (float)o.Nb[q];
+    f32.Bx[q] = (float)o.Bx[q];
+    f32.By[q] = (float)o.By[q];
+    f32.idu[q] = (float)idu[q];
+    f32.idv[q] = (float)idv[q];
+  }
   if (coarsen && j < dc.ny && i < dc.nx)
     coarsen_point(o.d, dc, fx, fy, o.Na, o.Nb, o.Bx, o.By, cNa, cNb, cBx, cBy, j, i);
   if (rhs.on) {
@@ -1577,6 +1615,19 @@ static Op make_op(const Ctx* c, int l) {
   o.ay = 1.0 / o.ax;
   return o;
 }
+// The finest level of the mixed-precision preconditioner (DIVA_PREC_MIXED): its smoother runs
+// in float on float copies of the coefficients and inverse diagonals (written by the
+// finest level's set-up), with the pre-smoothed x and the residual stored as float in
+// the level's tu/tv and ru/rv planes.  Everything else stays double.
+static bool level_fp32(const Ctx* c, int l) { return l == 0 && c->c.precision == DIVA_PREC_MIXED && c->tiled; }
+static OpT<float> make_op32(const Ctx* c) {
+  const Op o = make_op(c, 0);
+  OpT<float> f;
+  f.d = o.d; f.bc = o.bc; f.ax = o.ax; f.ay = o.ay; f.inv_dx = o.inv_dx; f.rtu = o.rtu; f.rtv = o.rtv;
+  f.Na = c->f32[F32_NA]; f.Nb = c->f32[F32_NB]; f.Bx = c->f32[F32_BX]; f.By = c->f32[F32_BY];
+  return f;
+}
+
 static void factors(const Ctx* c, int l, int* fx, int* fy) {
   *fx = (c->lv[l + 1].d.nx != c->lv[l].d.nx) ? 2 : 1;
   *fy = (c->lv[l + 1].d.ny != c->lv[l].d.ny) ? 2 : 1;
@@ -1601,6 +1652,9 @@ int solver_setup(Ctx* c) {
   // would hand that level to the coarse direct solve, whose matrix has no front rows
   if (C.choice_ice_margin == DIVA_MARGIN_BC && c->nlev < 2)
     return set_error(c, DIVA_UNSUPPORTED, "choice_ice_margin 'BC' needs nx or ny of at least 9");
+  if (C.precision == DIVA_PREC_MIXED && (c->nlev < 2 || !c->tiled))
+    return set_error(c, DIVA_UNSUPPORTED,
+                     "precision 'mixed' needs the tiled smoother (no periodic boundary, DIVA_NO_TILES unset) and nx or ny >= 9");
   // level l's diagonal and level l+1's coefficients in one launch; the finest level's
   // launch also forms the right-hand side, so it always runs on its own
   const int first_small = sub_first_level(c) > 1 ? sub_first_level(c) : 1;
@@ -1622,8 +1676,13 @@ int solver_setup(Ctx* c) {
         rhs.Hi = c->D(DIVA_F_HI_A); rhs.SL = c->D(DIVA_F_SL_A); rhs.Hb = c->D(DIVA_F_HB_A);
       }
     }
+    F32Out f32{};
+    if (level_fp32(c, l)) {
+      f32.Na = c->f32[F32_NA]; f32.Nb = c->f32[F32_NB]; f32.Bx = c->f32[F32_BX]; f32.By = c->f32[F32_BY];
+      f32.idu = c->f32[F32_IDU]; f32.idv = c->f32[F32_IDV];
+    }
     k_level_setup<<<GL(l)>>>(make_op(c, l), coarsen ? 1 : 0, K.d, fx, fy, K.Na, K.Nb, K.Bx, K.By, F.idu, F.idv,
-                             rhs); c->launches++;
+                             rhs, f32); c->launches++;
     DIVA_LAUNCHED(c, "k_level_setup");
   }
   const CoarseMap m = coarse_map(c);
@@ -1684,13 +1743,21 @@ static size_t sub_bytes(const Ctx* c, int l) {
   return sub_dbl(c, l) * sizeof(double) + ((sub_tab_entries(c, l) * sizeof(uint16_t) + 15) / 16) * 16;
 }
 
-// first level of the one-block sub-cycle: the largest whose levels all fit in shared memory
-static int sub_first_level(const Ctx* c) {
-  // the finest level's 'BC' front rows are not in the sub-cycle's row tables
-  const int l0 = (c->c.choice_ice_margin == DIVA_MARGIN_BC && c->nlev > 1) ? 1 : 0;
-  for (int l = l0; l < c->nlev; ++l)
+// the largest level whose levels all fit in the sub-cycle's shared memory (the row
+// tables are built from there down, whatever the configuration)
+static int sub_first_fit(const Ctx* c) {
+  for (int l = 0; l < c->nlev; ++l)
     if (sub_bytes(c, l) <= kSubSmemBudget) return l;
   return c->nlev - 1;
+}
+// first level of the one-block sub-cycle
+static int sub_first_level(const Ctx* c) {
+  // the finest level's 'BC' front rows are not in the sub-cycle's row tables, and a
+  // mixed-precision finest level is smoothed by the float tile kernels
+  const bool own0 = c->c.choice_ice_margin == DIVA_MARGIN_BC || (c->c.precision == DIVA_PREC_MIXED && c->tiled);
+  const int l0 = (own0 && c->nlev > 1) ? 1 : 0;
+  const int f = sub_first_fit(c);
+  return f > l0 ? f : l0;
 }
 
 static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
@@ -1709,41 +1776,59 @@ static int tile_edge(const Ctx* c, int l) {
 // from L2 instead).
 constexpr bool kStage16 = true, kStage32 = false;
 
-template <int T, bool S>
-static void tile_down_t(Ctx* c, int l, const Restriction& rs, const double* bu, const double* bv, double* xu,
-                        double* xv, int nu) {
+template <int T, bool S, class R>
+static void tile_down_r(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, const Restriction& rs,
+                        const double* bu, const double* bv, int nu) {
   const Level& L = c->lv[l];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
   // b is written only when it is restricted here (rs.on), which never happens on the finest level
-  const Op o = make_op(c, l);
-  auto kern = o.rtu ? k_smooth_down<T, T, S, true> : k_smooth_down<T, T, S, false>;
-  kern<<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
-      o, rs, const_cast<double*>(bu), const_cast<double*>(bv), L.tu, L.tv, L.ru, L.rv, L.idu, L.idv, nu);
+  auto kern = o.rtu ? k_smooth_down<T, T, S, true, R> : k_smooth_down<T, T, S, false, R>;
+  kern<<<grid, kTileThreads, TileGeom<T, T, S, R>::smem, c->stream>>>(
+      o, rs, const_cast<double*>(bu), const_cast<double*>(bv), reinterpret_cast<R*>(L.tu),
+      reinterpret_cast<R*>(L.tv), reinterpret_cast<R*>(L.ru), reinterpret_cast<R*>(L.rv), idu, idv, nu);
   c->launches++;
 }
-template <int T, bool S>
-static void tile_up_t(Ctx* c, int l, int fx, int fy, const double* bu, const double* bv, double* xu, double* xv,
-                      int nu) {
+template <int T, bool S, class R>
+static void tile_up_r(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, int fx, int fy, const double* bu,
+                      const double* bv, double* xu, double* xv, int nu) {
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
-  const Op o = make_op(c, l);
-  auto kern = o.rtu ? k_smooth_up<T, T, S, true> : k_smooth_up<T, T, S, false>;
-  kern<<<grid, kTileThreads, TileGeom<T, T, S>::smem, c->stream>>>(
-      o, make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, L.tu, L.tv, xu, xv, L.idu, L.idv, nu);
+  auto kern = o.rtu ? k_smooth_up<T, T, S, true, R> : k_smooth_up<T, T, S, false, R>;
+  kern<<<grid, kTileThreads, TileGeom<T, T, S, R>::smem, c->stream>>>(
+      o, make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, reinterpret_cast<const R*>(L.tu),
+      reinterpret_cast<const R*>(L.tv), xu, xv, idu, idv, nu);
   c->launches++;
 }
 static int tile_down(Ctx* c, int l, const Restriction& rs, const double* bu, const double* bv, double* xu,
                      double* xv, int nu) {
-  if (tile_edge(c, l) == 32) tile_down_t<32, kStage32>(c, l, rs, bu, bv, xu, xv, nu);
-  else tile_down_t<16, kStage16>(c, l, rs, bu, bv, xu, xv, nu);
+  const Level& L = c->lv[l];
+  if (level_fp32(c, l)) {   // float tiles stage their coefficients at both edges (100 KB at 32 x 32)
+    const OpT<float> o = make_op32(c);
+    if (tile_edge(c, l) == 32) tile_down_r<32, true>(c, l, o, c->f32[F32_IDU], c->f32[F32_IDV], rs, bu, bv, nu);
+    else tile_down_r<16, true>(c, l, o, c->f32[F32_IDU], c->f32[F32_IDV], rs, bu, bv, nu);
+  } else {
+    const Op o = make_op(c, l);
+    const double *iu = L.idu, *iv = L.idv;
+    if (tile_edge(c, l) == 32) tile_down_r<32, kStage32>(c, l, o, iu, iv, rs, bu, bv, nu);
+    else tile_down_r<16, kStage16>(c, l, o, iu, iv, rs, bu, bv, nu);
+  }
   DIVA_LAUNCHED(c, "k_smooth_down");
   return DIVA_OK;
 }
 static int tile_up(Ctx* c, int l, int fx, int fy, const double* bu, const double* bv, double* xu, double* xv,
                    int nu) {
-  if (tile_edge(c, l) == 32) tile_up_t<32, kStage32>(c, l, fx, fy, bu, bv, xu, xv, nu);
-  else tile_up_t<16, kStage16>(c, l, fx, fy, bu, bv, xu, xv, nu);
+  const Level& L = c->lv[l];
+  if (level_fp32(c, l)) {
+    const OpT<float> o = make_op32(c);
+    if (tile_edge(c, l) == 32) tile_up_r<32, true>(c, l, o, c->f32[F32_IDU], c->f32[F32_IDV], fx, fy, bu, bv, xu, xv, nu);
+    else tile_up_r<16, true>(c, l, o, c->f32[F32_IDU], c->f32[F32_IDV], fx, fy, bu, bv, xu, xv, nu);
+  } else {
+    const Op o = make_op(c, l);
+    const double *iu = L.idu, *iv = L.idv;
+    if (tile_edge(c, l) == 32) tile_up_r<32, kStage32>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
+    else tile_up_r<16, kStage16>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
+  }
   DIVA_LAUNCHED(c, "k_smooth_up");
   return DIVA_OK;
 }
@@ -1757,12 +1842,13 @@ static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu,
   const Level& K = c->lv[l + 1];
   int st = tile_down(c, l, rs, bu, bv, xu, xv, nu1);
   if (st) return st;
-  Restriction next;
+  Restriction next{};
   next.on = 1;
   next.df = L.d;
   factors(c, l, &next.fx, &next.fy);
   next.ru = L.ru;
   next.rv = L.rv;
+  next.rfloat = level_fp32(c, l) ? 1 : 0;   // the float residual of a mixed-precision finest level
   if ((st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv, next))) return st;
   if ((st = tile_up(c, l, next.fx, next.fy, bu, bv, xu, xv, nu2))) return st;
   c->fine_passes += (nu1 + nu2 + 1) * (double)L.d.plane / (double)c->d.plane;
@@ -1774,7 +1860,7 @@ static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu,
 // Row tables of the sub-cycle levels (see k_subcycle), built on the host from the
 // level sizes and the boundary conditions and copied to the context's table area.
 static int build_sub_tables(Ctx* c) {
-  const int first = sub_first_level(c);
+  const int first = sub_first_fit(c);
   std::vector<uint16_t> tab(sub_tab_entries(c, first));
   size_t off = 0;
   for (int l = first; l < c->nlev; ++l) {
@@ -1815,7 +1901,7 @@ static int build_sub_tables(Ctx* c) {
   return DIVA_OK;
 }
 
-size_t solver_table_entries(const Ctx* c) { return sub_tab_entries(c, sub_first_level(c)); }
+size_t solver_table_entries(const Ctx* c) { return sub_tab_entries(c, sub_first_fit(c)); }
 
 int solver_init(Ctx* c) {
   if (sub_bytes(c, c->nlev - 1) > kSubSmemBudget)
@@ -1824,19 +1910,31 @@ int solver_init(Ctx* c) {
   DIVA_CUDA(c, cudaFuncSetAttribute(k_small_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
-  const void* tile32[4] = {(const void*)k_smooth_down<32, 32, kStage32, false>,
-                           (const void*)k_smooth_down<32, 32, kStage32, true>,
-                           (const void*)k_smooth_up<32, 32, kStage32, false>,
-                           (const void*)k_smooth_up<32, 32, kStage32, true>};
-  const void* tile16[4] = {(const void*)k_smooth_down<16, 16, kStage16, false>,
-                           (const void*)k_smooth_down<16, 16, kStage16, true>,
-                           (const void*)k_smooth_up<16, 16, kStage16, false>,
-                           (const void*)k_smooth_up<16, 16, kStage16, true>};
+  const void* tile32[4] = {(const void*)k_smooth_down<32, 32, kStage32, false, double>,
+                           (const void*)k_smooth_down<32, 32, kStage32, true, double>,
+                           (const void*)k_smooth_up<32, 32, kStage32, false, double>,
+                           (const void*)k_smooth_up<32, 32, kStage32, true, double>};
+  const void* tile16[4] = {(const void*)k_smooth_down<16, 16, kStage16, false, double>,
+                           (const void*)k_smooth_down<16, 16, kStage16, true, double>,
+                           (const void*)k_smooth_up<16, 16, kStage16, false, double>,
+                           (const void*)k_smooth_up<16, 16, kStage16, true, double>};
+  const void* f32t32[4] = {(const void*)k_smooth_down<32, 32, true, false, float>,
+                           (const void*)k_smooth_down<32, 32, true, true, float>,
+                           (const void*)k_smooth_up<32, 32, true, false, float>,
+                           (const void*)k_smooth_up<32, 32, true, true, float>};
+  const void* f32t16[4] = {(const void*)k_smooth_down<16, 16, true, false, float>,
+                           (const void*)k_smooth_down<16, 16, true, true, float>,
+                           (const void*)k_smooth_up<16, 16, true, false, float>,
+                           (const void*)k_smooth_up<16, 16, true, true, float>};
   for (int k = 0; k < 4; ++k) {
     DIVA_CUDA(c, cudaFuncSetAttribute(tile32[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)TileGeom<32, 32, kStage32>::smem));
     DIVA_CUDA(c, cudaFuncSetAttribute(tile16[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)TileGeom<16, 16, kStage16>::smem));
+    DIVA_CUDA(c, cudaFuncSetAttribute(f32t32[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)TileGeom<32, 32, true, float>::smem));
+    DIVA_CUDA(c, cudaFuncSetAttribute(f32t16[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)TileGeom<16, 16, true, float>::smem));
   }
   const BCs& b = c->bc;
   const int all[8] = {b.uW, b.uE, b.uS, b.uN, b.vW, b.vE, b.vS, b.vN};

@@ -75,7 +75,11 @@ typedef enum { DIVA_RHEO_UNIFORM = 0, DIVA_RHEO_HUYBRECHTS1992 = 1 } diva_rheolo
 /* Picard stop test: the reference's step norm resid_UV (ice_velocity_module.f90:1530-1601),
  * or the FP64 nonlinear residual ||b(u) - A(u) u|| / ||b(u)||. */
 typedef enum { DIVA_STOP_RESID_UV = 0, DIVA_STOP_RELRES = 1 } diva_stop_t;
-/* Arithmetic of the linear solves: plain FP64, or FP32 multigrid inside FP64 defect correction. */
+/* Arithmetic of the linear solves: plain FP64, or MIXED: the finest multigrid level's
+ * smoother (tile kernels) runs in FP32 on FP32 copies of the coefficients, inside the
+ * FP64 BiCGStab whose residuals, and the nonlinear residual and Picard norms, stay FP64.
+ * MIXED needs the tiled smoother (no periodic side) and a grid of at least 9 points in one
+ * direction; otherwise the solve returns DIVA_UNSUPPORTED. */
 typedef enum { DIVA_PREC_FP64 = 0, DIVA_PREC_MIXED = 1 } diva_precision_t;
 
 /* ---- grid (TYPE(type_grid), data_types_module.f90:13-29) --------------- */

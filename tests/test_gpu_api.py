@@ -242,3 +242,35 @@ def test_ensemble_members_equal_lone_solves(cuda):
         assert res[k]["report"]["picard_iterations"] == r["picard_iterations"], name
         assert np.array_equal(res[k]["u_vav_cx"], o["u_vav_cx"]), name
         assert np.array_equal(res[k]["v_vav_cy"], o["v_vav_cy"]), name
+
+
+def test_mixed_precision_is_validated(cuda):
+    g, cfg, f = small()
+    with pytest.raises(diva.DivaError) as e:
+        diva.Context(g, dict(cfg, precision=2), cuda)
+    assert e.value.status == _abi.BAD_INPUT
+    ctx = diva.Context(g, dict(cfg, precision="mixed", BC_u_west="periodic", BC_u_east="periodic"), cuda)
+    helpers.prepare(ctx, f)
+    with pytest.raises(diva.DivaError) as e:
+        ctx.solve_DIVA()
+    assert e.value.status == _abi.UNSUPPORTED
+    ctx.close()
+
+
+@pytest.mark.parametrize("case", ["channel_5km", "icecap_5km"])
+def test_mixed_precision_matches_fp64(cuda, case):
+    """precision 'mixed' (FP32 finest-level smoother inside FP64 BiCGStab) reaches the same
+    nonlinear tolerance as the FP64 solver; the velocities agree to the tolerance's size."""
+    cfg_id = 1 if case.startswith("channel") else 2
+    ov = {"picard_stop": "relres", "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 500, "lin_adaptive": 1,
+          "lin_rtol": 1e-10}
+    g, cfg, f = helpers.make_case(cfg_id, overrides=ov)
+    r64, o64 = helpers.run(cuda, g, cfg, f)
+    r32, o32 = helpers.run(cuda, g, dict(cfg, precision="mixed"), f)
+    assert r64["status"] == 0, r64
+    assert r32["status"] == 0, r32
+    assert r32["relres"] <= 1e-6
+    a = np.concatenate([o64["u_vav_cx"].ravel(), o64["v_vav_cy"].ravel()])
+    b = np.concatenate([o32["u_vav_cx"].ravel(), o32["v_vav_cy"].ravel()])
+    assert helpers.rel_l2(b, a) <= 1e-5
+    assert abs(r32["picard_iterations"] - r64["picard_iterations"]) <= 0.1 * r64["picard_iterations"] + 2
