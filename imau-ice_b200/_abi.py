@@ -24,6 +24,7 @@ HYDRO = {"dry": 0, "saturated": 1, "Martin2011": 2}
 RHEO = {"uniform": 0, "Huybrechts1992": 1}
 STOP = {"resid_UV": 0, "relres": 1}
 PREC = {"fp64": 0, "mixed": 1}
+HBC = {"zero": 0, "infinite": 1, "periodic": 2, "fixed": 3, "none": 4}
 
 GRID_KINDS = ["A", "CX", "CY", "B", "A3", "CX3", "CY3", "B3"]
 
@@ -72,6 +73,8 @@ class Config(C.Structure):
         ("lin_adaptive", C.c_int32),
         ("lin_adaptive_eta", C.c_double),
         ("precision", C.c_int32),
+        ("ice_thickness_west_BC", C.c_int32), ("ice_thickness_east_BC", C.c_int32),
+        ("ice_thickness_south_BC", C.c_int32), ("ice_thickness_north_BC", C.c_int32),
         ("reserved", C.c_int32 * 8),
     ]
 
@@ -101,6 +104,8 @@ ENUM_OPTIONS = {
     "BC_v_west": BC, "BC_v_east": BC, "BC_v_south": BC, "BC_v_north": BC,
     "choice_sliding_law": SLIDING, "choice_basal_hydrology": HYDRO,
     "choice_ice_rheology": RHEO, "picard_stop": STOP, "precision": PREC,
+    "ice_thickness_west_BC": HBC, "ice_thickness_east_BC": HBC, "ice_thickness_south_BC": HBC,
+    "ice_thickness_north_BC": HBC,
 }
 
 
@@ -125,6 +130,12 @@ def bind(lib, prefix):
         "nonlinear_residual": (C.c_int, [vp, dp]),
         "state_save": (C.c_int, [vp]),
         "state_restore": (C.c_int, [vp]),
+        "determine_floating_margin_fraction": (C.c_int, [vp]),
+        "calc_dHi_dt": (C.c_int, [vp, C.c_double]),
+        "calc_critical_timestep_adv": (C.c_int, [vp, C.c_double, dp]),
+        "pc_predictor": (C.c_int, [vp, C.c_double, C.c_double]),
+        "pc_corrector": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, dp]),
+        "pc_finish": (C.c_int, [vp, C.c_double]),
         "last_error": (C.c_char_p, [vp]),
     }
     fns = {}

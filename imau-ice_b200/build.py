@@ -20,7 +20,8 @@ OBJ_DIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
           "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
-SOURCES = {"api.cu": [], "geometry.cu": ["--fmad=false"], "picard.cu": [], "solver.cu": [], "noalloc.cu": []}
+SOURCES = {"api.cu": [], "geometry.cu": ["--fmad=false"], "picard.cu": [], "solver.cu": [], "noalloc.cu": [],
+           "thickness.cu": ["--fmad=false"]}
 
 
 def _nvcc():

@@ -17,10 +17,6 @@
 
 using namespace diva;
 
-struct diva_ctx {
-  Ctx c;
-};
-
 namespace diva {
 
 int set_error(Ctx* c, int code, const std::string& msg) {

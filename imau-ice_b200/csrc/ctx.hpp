@@ -180,3 +180,8 @@ int solver_build_picard_graphs(Ctx* c, bool diva);
 void solver_destroy_graphs(Ctx* c);
 
 }  // namespace diva
+
+// the opaque handle of the C ABI
+struct diva_ctx {
+  diva::Ctx c;
+};

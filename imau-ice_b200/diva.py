@@ -225,6 +225,38 @@ class Context:
         self._check(self.backend.fns["nonlinear_residual"](self.h, C.byref(r)), "nonlinear_residual")
         return r.value
 
+    # ---- the ice-thickness update and the predictor/corrector stages ---------------
+    def determine_floating_margin_fraction(self):
+        """general_ice_model_data_module.f90:784-865."""
+        self._check(self.backend.fns["determine_floating_margin_fraction"](self.h),
+                    "determine_floating_margin_fraction")
+
+    def calc_dHi_dt(self, dt):
+        """ice_thickness_module.f90:26-300 ('explicit') with apply_ice_thickness_BC."""
+        self._check(self.backend.fns["calc_dHi_dt"](self.h, float(dt)), "calc_dHi_dt")
+
+    def calc_critical_timestep_adv(self, dt_max):
+        """ice_dynamics_module.f90:726-762; returns dt_crit_adv."""
+        r = C.c_double()
+        self._check(self.backend.fns["calc_critical_timestep_adv"](self.h, float(dt_max), C.byref(r)),
+                    "calc_critical_timestep_adv")
+        return r.value
+
+    def pc_predictor(self, dt, zeta):
+        """The predictor stage of run_ice_dynamics_pc (ice_dynamics_module.f90:360-377)."""
+        self._check(self.backend.fns["pc_predictor"](self.h, float(dt), float(zeta)), "pc_predictor")
+
+    def pc_corrector(self, dt, zeta, eta_min):
+        """The corrector stage and calc_pc_truncation_error (:404-421, :763-816); returns pc_eta."""
+        r = C.c_double()
+        self._check(self.backend.fns["pc_corrector"](self.h, float(dt), float(zeta), float(eta_min), C.byref(r)),
+                    "pc_corrector")
+        return r.value
+
+    def pc_finish(self, dt):
+        """Hi_tplusdt_a and the thickness update of the step (:429-431, :435-648 in part)."""
+        self._check(self.backend.fns["pc_finish"](self.h, float(dt)), "pc_finish")
+
     def state_save(self):
         self._check(self.backend.fns["state_save"](self.h), "state_save")
 

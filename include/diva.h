@@ -81,6 +81,9 @@ typedef enum { DIVA_STOP_RESID_UV = 0, DIVA_STOP_RELRES = 1 } diva_stop_t;
  * MIXED needs the tiled smoother (no periodic side) and a grid of at least 9 points in one
  * direction; otherwise the solve returns DIVA_UNSUPPORTED. */
 typedef enum { DIVA_PREC_FP64 = 0, DIVA_PREC_MIXED = 1 } diva_precision_t;
+/* Ice thickness at the domain boundary (apply_ice_thickness_BC, ice_thickness_module.f90:728-931). */
+typedef enum { DIVA_HBC_ZERO = 0, DIVA_HBC_INFINITE = 1, DIVA_HBC_PERIODIC = 2, DIVA_HBC_FIXED = 3,
+               DIVA_HBC_NONE = 4 } diva_hbc_t;
 
 /* ---- grid (TYPE(type_grid), data_types_module.f90:13-29) --------------- */
 typedef struct {
@@ -132,6 +135,8 @@ typedef struct {
   int32_t lin_adaptive;                 /* RELRES mode: linear rtol tied to the current nonlinear residual */
   double  lin_adaptive_eta;             /* that rtol: max(lin_rtol, eta * min(1, rel-res)); default 0.5 */
   int32_t precision;                    /* diva_precision_t */
+  /* ice thickness boundary conditions, diva_hbc_t (configuration_module.f90:325-328, default zero) */
+  int32_t ice_thickness_west_BC, ice_thickness_east_BC, ice_thickness_south_BC, ice_thickness_north_BC;
   int32_t reserved[8];
 } diva_config_t;
 
@@ -200,6 +205,38 @@ int  diva_solve_diva_batch(diva_ctx_t** ctxs, int32_t n, diva_report_t* reports)
 /* The SIA 3D velocity loop of solve_SIA (ice_velocity_module.f90:60-105) alone,
  * in any dynamics mode (used for "DIVA plus SIA" diagnostics). */
 int  diva_calc_sia_3d_velocities(diva_ctx_t* ctx);
+
+/* ---- ice-thickness update and the predictor/corrector step ------------------
+ * The consumers of u_vav_cx / v_vav_cy inside a time step (run_ice_dynamics_pc,
+ * ice_dynamics_module.f90:243-432), on the device; the time-step control itself
+ * (dt_crit, pc_zeta, pc_eta, the event clock) is host logic around these calls. */
+/* determine_floating_margin_fraction (general_ice_model_data_module.f90:784-865):
+ * float_margin_frac_a and Hi_eff_cf_a of rows 2..ny-1 from Hi_a and the masks. */
+int  diva_determine_floating_margin_fraction(diva_ctx_t* ctx);
+/* calc_dHi_dt with choice_ice_integration_method 'explicit' (ice_thickness_module.f90:
+ * 26-300): upwind fluxes Qx_cx/Qy_cy of u_vav, mass balance SMB_a + BMB_a (the floating
+ * fraction at calving fronts, none on open ocean), outfluxes rescaled so no cell goes
+ * negative, dHi_dt_a and Hi_tplusdt_a = Hi_a + dt dHi_dt_a, then
+ * apply_ice_thickness_BC (:728-931; west, east, south, north in that order). */
+int  diva_calc_dHi_dt(diva_ctx_t* ctx, double dt);
+/* calc_critical_timestep_adv (ice_dynamics_module.f90:726-762):
+ * min(dt_max, 0.9 min over interior a-points of dx / (|u_vav_cx| + |v_vav_cy|)). */
+int  diva_calc_critical_timestep_adv(diva_ctx_t* ctx, double dt_max, double* dt_crit_adv);
+/* The predictor of run_ice_dynamics_pc (:360-377): dHidt_Hnm1_unm1 = dHidt_Hn_un;
+ * calc_dHi_dt(dt); dHidt_Hn_un = dHi_dt_a; Hi_pred = max(0, Hi + dt ((1 + zeta/2)
+ * dHidt_Hn_un - zeta/2 dHidt_Hnm1_unm1)); Hi_old = Hi; Hi = Hi_pred;
+ * update_general_ice_model_data.  The velocity solve follows (the caller's). */
+int  diva_pc_predictor(diva_ctx_t* ctx, double dt, double zeta);
+/* The corrector (:408-421) and calc_pc_truncation_error (:763-816): calc_dHi_dt(dt);
+ * dHidt_Hstarnp1_unp1 = dHi_dt_a; Hi = Hi_old; update_general_ice_model_data;
+ * Hi_corr = max(0, Hi_old + dt/2 (dHidt_Hn_un + dHidt_Hstarnp1_unp1));
+ * dHi_dt_a = (Hi_corr - Hi) / dt; pc_tau and *eta = max(eta_min, pc_tau over interior
+ * sheet cells with no grounding line in their 3 x 3 neighbourhood). */
+int  diva_pc_corrector(diva_ctx_t* ctx, double dt, double zeta, double eta_min, double* eta);
+/* Hi_tplusdt_a = max(0, Hi_a + dt dHi_dt_a) (:429-431), then (update_ice_thickness,
+ * :435-648, without calving, fixed geometries or the no-ice mask) Hi_a = Hi_tplusdt_a,
+ * update_general_ice_model_data and determine_floating_margin_fraction. */
+int  diva_pc_finish(diva_ctx_t* ctx, double dt);
 
 /* FP64 nonlinear residual of the current (u_vav_cx, v_vav_cy): evaluates the
  * coefficients of the next viscosity iteration (A3-A7) and returns

@@ -127,6 +127,27 @@
   /* SICOPOLIS-style solver masks (set_sico_masks) */        \
   X(DIVA_MASK_COMBI,      DIVA_mask_combi,      A,   I)      \
   X(DIVA_ISFRONT_INNER,   DIVA_isfront_inner,   A,   I)      \
-  X(DIVA_ISFRONT_OUTER,   DIVA_isfront_outer,   A,   I)
+  X(DIVA_ISFRONT_OUTER,   DIVA_isfront_outer,   A,   I)      \
+  /* ice-thickness update and predictor/corrector step   */ \
+  /* (ice_thickness_module.f90:26-300, 728-931;          */ \
+  /*  ice_dynamics_module.f90:243-432, 726-816;          */ \
+  /*  general_ice_model_data_module.f90:784-865);        */ \
+  /* SMB_a is SMB%SMB_year and BMB_a is BMB%BMB          */ \
+  /* (data_types_module.f90:732, 742), m/yr of ice       */ \
+  X(SMB_A,                SMB_a,                A,   D)      \
+  X(BMB_A,                BMB_a,                A,   D)      \
+  X(FLOAT_MARGIN_FRAC_A,  float_margin_frac_a,  A,   D)      \
+  X(HI_EFF_CF_A,          Hi_eff_cf_a,          A,   D)      \
+  X(QX_CX,                Qx_cx,                CX,  D)      \
+  X(QY_CY,                Qy_cy,                CY,  D)      \
+  X(DHI_DT_A,             dHi_dt_a,             A,   D)      \
+  X(HI_TPLUSDT_A,         Hi_tplusdt_a,         A,   D)      \
+  X(HI_PRED,              Hi_pred,              A,   D)      \
+  X(HI_CORR,              Hi_corr,              A,   D)      \
+  X(HI_OLD,               Hi_old,               A,   D)      \
+  X(DHIDT_HN_UN,          dHidt_Hn_un,          A,   D)      \
+  X(DHIDT_HNM1_UNM1,      dHidt_Hnm1_unm1,      A,   D)      \
+  X(DHIDT_HSTARNP1_UNP1,  dHidt_Hstarnp1_unp1,  A,   D)      \
+  X(PC_TAU,               pc_tau,               A,   D)
 
 #endif /* DIVA_FIELDS_H */

@@ -2327,6 +2327,225 @@ int orc_prepare_diva(orc_ctx* c) {
   return DIVA_OK;
 }
 /* One set of DIVA coefficient stages (A3-A7) at the current state. */
+/* ------------------------------------------------------------------------ */
+/* Ice-thickness update and the predictor/corrector step (the consumers of   */
+/* u_vav inside a time step)                                                 */
+
+/* Hi_from_Hb_and_Hs, utilities_module.f90:160-183 */
+static double hi_from_hb_and_hs(double Hb, double Hs, double SL) {
+  const double Hs_float = Hb + (SL - Hb) * SW_DENSITY / ICE_DENSITY;
+  if (Hs > Hs_float) return Hs - Hb;
+  return (Hs - SL) / (1.0 - ICE_DENSITY / SW_DENSITY);
+}
+
+/* determine_floating_margin_fraction, general_ice_model_data_module.f90:784-865
+ * (rows 2..ny-1 only; the first and last rows keep their values) */
+static void floating_margin_fraction(orc_ctx* c) {
+  DECL_DIMS(c);
+  const double* Hi = FD(c, HI_A);
+  const int32_t *ice = FI(c, MASK_ICE_A), *cf = FI(c, MASK_CF_A), *shelf = FI(c, MASK_SHELF_A);
+  double *fmf = FD(c, FLOAT_MARGIN_FRAC_A), *Heff = FD(c, HI_EFF_CF_A);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 1; j < ny - 1; ++j) {
+      const size_t q = IA(j, i);
+      fmf[q] = ice[q] == 1 ? 1.0 : 0.0;
+      Heff[q] = ice[q] == 1 ? Hi[q] : 0.0;
+      if (!(cf[q] == 1 && shelf[q] == 1)) continue;
+      int inner_neighbours = 0;
+      double Hmax = 0.0;
+      for (int ii = (i > 0 ? i - 1 : 0); ii <= (i < nx - 1 ? i + 1 : nx - 1); ++ii)
+        for (int jj = j - 1; jj <= j + 1; ++jj) {
+          const size_t p = IA(jj, ii);
+          if (ice[p] == 1 && cf[p] == 0) { inner_neighbours = 1; Hmax = fmax(Hmax, Hi[p]); }
+        }
+      if (!inner_neighbours || Hmax < Hi[q]) { fmf[q] = 1.0; Heff[q] = Hi[q]; continue; }
+      fmf[q] = Hi[q] / Hmax;
+      Heff[q] = Hmax;
+    }
+}
+
+/* apply_ice_thickness_BC, ice_thickness_module.f90:728-931: west, east, south, north */
+static void apply_ice_thickness_bc(orc_ctx* c, double dt) {
+  DECL_DIMS(c);
+  const double *Hi = FD(c, HI_A), *Hb = FD(c, HB_A), *SL = FD(c, SL_A);
+  double *Hn = FD(c, HI_TPLUSDT_A), *dH = FD(c, DHI_DT_A);
+  const int diva = c->c.choice_ice_dynamics == DIVA_DYN_DIVA;
+  const int bc[4] = {c->c.ice_thickness_west_BC, c->c.ice_thickness_east_BC, c->c.ice_thickness_south_BC,
+                     c->c.ice_thickness_north_BC};
+  for (int side = 0; side < 4; ++side) {
+    const int xside = side < 2;
+    const int n = xside ? ny : nx;                             /* points along the side */
+    const int edge = side == 0 ? 0 : side == 1 ? nx - 1 : side == 2 ? 0 : ny - 1;
+    const int inner = side == 0 ? 1 : side == 1 ? nx - 2 : side == 2 ? 1 : ny - 2;
+    const int opposite = side == 0 ? nx - 2 : side == 1 ? 1 : side == 2 ? ny - 2 : 1;
+    for (int k = 0; k < n; ++k) {
+      const size_t q = xside ? IA(k, edge) : IA(edge, k);
+      const size_t qi = xside ? IA(k, inner) : IA(inner, k);
+      const size_t qo = xside ? IA(k, opposite) : IA(opposite, k);
+      switch (bc[side]) {
+        case DIVA_HBC_ZERO:
+          Hn[q] = 0.0; dH[q] = -Hi[q] / dt;
+          if (diva) { Hn[qi] = 0.0; dH[qi] = -Hi[qi] / dt; }
+          break;
+        case DIVA_HBC_INFINITE: {
+          const double Hs_nb = surface_elevation(Hn[qi], Hb[qi], SL[qi]);
+          Hn[q] = hi_from_hb_and_hs(Hb[q], Hs_nb, SL[q]);
+          dH[q] = (Hn[q] - Hi[q]) / dt;
+          break;
+        }
+        case DIVA_HBC_PERIODIC: Hn[q] = Hi[qo]; dH[q] = (Hn[q] - Hi[q]) / dt; break;
+        case DIVA_HBC_FIXED: Hn[q] = Hi[q]; dH[q] = 0.0; break;
+        default: break;                                        /* 'none' */
+      }
+    }
+  }
+}
+
+/* calc_dHi_dt with 'explicit' integration, ice_thickness_module.f90:26-300 */
+static void calc_dHi_dt(orc_ctx* c, double dt) {
+  DECL_DIMS(c);
+  const double dx = c->dx;
+  const double *u = FD(c, U_VAV_CX), *v = FD(c, V_VAV_CY), *Hi = FD(c, HI_A);
+  const double *smb = FD(c, SMB_A), *bmb = FD(c, BMB_A), *fmf = FD(c, FLOAT_MARGIN_FRAC_A);
+  const int32_t *cf = FI(c, MASK_CF_A), *shelf = FI(c, MASK_SHELF_A), *ocean = FI(c, MASK_OCEAN_A);
+  double *Qx = FD(c, QX_CX), *Qy = FD(c, QY_CY), *dH = FD(c, DHI_DT_A), *Hn = FD(c, HI_TPLUSDT_A);
+  /* upwind fluxes, :91-120 */
+  for (int i = 0; i < nx - 1; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const double uu = u[ICX(j, i)];
+      Qx[ICX(j, i)] = uu * (uu > 0.0 ? Hi[IA(j, i)] : Hi[IA(j, i + 1)]) * dx * dt;
+    }
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny - 1; ++j) {
+      const double vv = v[ICY(j, i)];
+      Qy[ICY(j, i)] = vv * (vv > 0.0 ? Hi[IA(j, i)] : Hi[IA(j + 1, i)]) * dx * dt;
+    }
+  /* mass balance and outflux limitation, :175-262 (in place, in the reference's order) */
+  double* mb = (double*)malloc(sizeof(double) * (size_t)nx * ny);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const size_t q = IA(j, i);
+      if (cf[q] == 1 && shelf[q] == 1) mb[q] = (smb[q] + bmb[q]) * dx * dx * dt * fmf[q];
+      else if (ocean[q] == 1 && shelf[q] == 0) mb[q] = 0.0;
+      else mb[q] = (smb[q] + bmb[q]) * dx * dx * dt;
+      const double avail = Hi[q] * dx * dx;
+      double out = 0.0;
+      if (i > 0 && !(Qx[ICX(j, i - 1)] > 0.0)) out -= Qx[ICX(j, i - 1)];
+      if (i < nx - 1 && !(Qx[ICX(j, i)] < 0.0)) out += Qx[ICX(j, i)];
+      if (j > 0 && !(Qy[ICY(j - 1, i)] > 0.0)) out -= Qy[ICY(j - 1, i)];
+      if (j < ny - 1 && !(Qy[ICY(j, i)] < 0.0)) out += Qy[ICY(j, i)];
+      double r = 1.0;
+      if (-mb[q] >= avail) { mb[q] = -avail; r = 0.0; }
+      if (out > avail + mb[q]) r = (avail + mb[q]) / out;
+      if (r < 1.0) {
+        if (i > 0 && Qx[ICX(j, i - 1)] < 0.0) Qx[ICX(j, i - 1)] *= r;
+        if (i < nx - 1 && Qx[ICX(j, i)] > 0.0) Qx[ICX(j, i)] *= r;
+        if (j > 0 && Qy[ICY(j - 1, i)] < 0.0) Qy[ICY(j - 1, i)] *= r;
+        if (j < ny - 1 && Qy[ICY(j, i)] > 0.0) Qy[ICY(j, i)] *= r;
+      }
+    }
+  /* rate of change and thickness at t + dt, :266-290 */
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const size_t q = IA(j, i);
+      double d = mb[q] / (dx * dx * dt);
+      if (i > 0) d = d + Qx[ICX(j, i - 1)] / (dx * dx * dt);
+      if (i < nx - 1) d = d - Qx[ICX(j, i)] / (dx * dx * dt);
+      if (j > 0) d = d + Qy[ICY(j - 1, i)] / (dx * dx * dt);
+      if (j < ny - 1) d = d - Qy[ICY(j, i)] / (dx * dx * dt);
+      d = fmax(d, -Hi[q] / dt);
+      dH[q] = d;
+      Hn[q] = Hi[q] + d * dt;
+    }
+  free(mb);
+  apply_ice_thickness_bc(c, dt);
+}
+
+int orc_determine_floating_margin_fraction(orc_ctx* c) { floating_margin_fraction(c); return DIVA_OK; }
+
+int orc_calc_dHi_dt(orc_ctx* c, double dt) {
+  if (!(dt > 0.0)) return DIVA_BAD_INPUT;
+  calc_dHi_dt(c, dt);
+  DECL_DIMS(c);
+  if (check_nan(c, FD(c, DHI_DT_A), (size_t)nx * ny)) return DIVA_NAN_DETECTED;
+  return DIVA_OK;
+}
+
+/* calc_critical_timestep_adv, ice_dynamics_module.f90:726-762 */
+int orc_calc_critical_timestep_adv(orc_ctx* c, double dt_max, double* dt_crit_adv) {
+  DECL_DIMS(c);
+  const double *u = FD(c, U_VAV_CX), *v = FD(c, V_VAV_CY);
+  double dtc = 2.0 * dt_max;
+  for (int i = 1; i < nx - 1; ++i)
+    for (int j = 1; j < ny - 1; ++j) dtc = fmin(dtc, c->dx / (fabs(u[ICX(j, i)]) + fabs(v[ICY(j, i)])));
+  *dt_crit_adv = fmin(dt_max, dtc * 0.9);
+  return DIVA_OK;
+}
+
+/* the predictor of run_ice_dynamics_pc, ice_dynamics_module.f90:360-377 */
+int orc_pc_predictor(orc_ctx* c, double dt, double zeta) {
+  DECL_DIMS(c);
+  const size_t n = (size_t)nx * ny;
+  if (!(dt > 0.0)) return DIVA_BAD_INPUT;
+  memcpy(FD(c, DHIDT_HNM1_UNM1), FD(c, DHIDT_HN_UN), sizeof(double) * n);
+  calc_dHi_dt(c, dt);
+  memcpy(FD(c, DHIDT_HN_UN), FD(c, DHI_DT_A), sizeof(double) * n);
+  double *Hi = FD(c, HI_A), *pred = FD(c, HI_PRED), *old = FD(c, HI_OLD);
+  const double *hn = FD(c, DHIDT_HN_UN), *hm = FD(c, DHIDT_HNM1_UNM1);
+  for (size_t q = 0; q < n; ++q)
+    pred[q] = fmax(0.0, Hi[q] + dt * ((1.0 + zeta / 2.0) * hn[q] - (zeta / 2.0) * hm[q]));
+  memcpy(old, Hi, sizeof(double) * n);
+  memcpy(Hi, pred, sizeof(double) * n);
+  return orc_update_general_ice_model_data(c);
+}
+
+/* the corrector, :404-421, and calc_pc_truncation_error, :763-816 */
+int orc_pc_corrector(orc_ctx* c, double dt, double zeta, double eta_min, double* eta) {
+  DECL_DIMS(c);
+  const size_t n = (size_t)nx * ny;
+  if (!(dt > 0.0)) return DIVA_BAD_INPUT;
+  calc_dHi_dt(c, dt);
+  memcpy(FD(c, DHIDT_HSTARNP1_UNP1), FD(c, DHI_DT_A), sizeof(double) * n);
+  double *Hi = FD(c, HI_A), *old = FD(c, HI_OLD), *corr = FD(c, HI_CORR), *dH = FD(c, DHI_DT_A);
+  memcpy(Hi, old, sizeof(double) * n);
+  int st = orc_update_general_ice_model_data(c);
+  if (st) return st;
+  const double *hn = FD(c, DHIDT_HN_UN), *hs = FD(c, DHIDT_HSTARNP1_UNP1), *pred = FD(c, HI_PRED);
+  for (size_t q = 0; q < n; ++q) {
+    corr[q] = fmax(0.0, old[q] + 0.5 * dt * (hn[q] + hs[q]));
+    dH[q] = (corr[q] - Hi[q]) / dt;
+  }
+  double* tau = FD(c, PC_TAU);
+  const int32_t *sheet = FI(c, MASK_SHEET_A), *gl = FI(c, MASK_GL_A);
+  double e = eta_min;
+  for (int i = 1; i < nx - 1; ++i)
+    for (int j = 1; j < ny - 1; ++j) {
+      const size_t q = IA(j, i);
+      tau[q] = fabs(zeta * (corr[q] - pred[q]) / ((3.0 * zeta + 3.0) * dt));
+      int near_gl = 0;
+      for (int ii = i - 1; ii <= i + 1; ++ii)
+        for (int jj = j - 1; jj <= j + 1; ++jj) near_gl |= gl[IA(jj, ii)] != 0;
+      if (sheet[q] == 1 && !near_gl) e = fmax(e, tau[q]);
+    }
+  *eta = e;
+  return DIVA_OK;
+}
+
+/* Hi_tplusdt_a (:429-431) and the geometry update of update_ice_thickness (:435-648
+ * without calving, fixed geometries, shelf removal or the no-ice mask) */
+int orc_pc_finish(orc_ctx* c, double dt) {
+  DECL_DIMS(c);
+  const size_t n = (size_t)nx * ny;
+  double *Hi = FD(c, HI_A), *Hn = FD(c, HI_TPLUSDT_A);
+  const double* dH = FD(c, DHI_DT_A);
+  for (size_t q = 0; q < n; ++q) Hn[q] = fmax(0.0, Hi[q] + dt * dH[q]);
+  for (size_t q = 0; q < n; ++q) Hi[q] = fmax(0.0, Hn[q]);
+  int st = orc_update_general_ice_model_data(c);
+  if (st) return st;
+  floating_margin_fraction(c);
+  return DIVA_OK;
+}
+
 int orc_diva_coefficients(orc_ctx* c) {
   double *u = FD(c, U_VAV_CX), *v = FD(c, V_VAV_CY);
   calc_vertical_shear_strain_rates(c);

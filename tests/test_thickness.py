@@ -1,0 +1,188 @@
+"""The explicit ice-thickness update and the predictor/corrector stages on the CPU
+oracle: an independent NumPy restatement of calc_dHi_dt_explicit
+(ice_thickness_module.f90:65-300), known answers of the boundary conditions
+(:728-931) and of the advective time-step limit (ice_dynamics_module.f90:726-762),
+mass conservation, and a few predictor/corrector steps (:243-432)."""
+import numpy as np
+import pytest
+
+from imau_ice_b200 import diva, dynamics, synth
+import helpers
+import oracle_backend as ob
+
+RHO_I, RHO_SW = 910.0, 1028.0
+
+
+def small_case(seed=0, nx=11, ny=9, dx=10e3, bc="none", dyn="DIVA"):
+    rng = np.random.default_rng(seed)
+    g = diva.Grid(nx, ny, dx)
+    Hb = rng.uniform(-600.0, 400.0, (ny, nx))
+    H = np.where(rng.random((ny, nx)) < 0.8, rng.uniform(50.0, 1500.0, (ny, nx)), 0.0)
+    f = {"Hi_a": H, "Hb_a": Hb, "SL_a": np.zeros((ny, nx)), "Ti_a": np.full((g.nz, ny, nx), 260.0),
+         "SMB_a": rng.uniform(-2.0, 1.0, (ny, nx)), "BMB_a": rng.uniform(-3.0, 0.5, (ny, nx)),
+         "u_vav_cx": rng.uniform(-400.0, 400.0, (ny, nx - 1)), "v_vav_cy": rng.uniform(-400.0, 400.0, (ny - 1, nx))}
+    cfg = {"choice_ice_dynamics": dyn, "ice_thickness_west_BC": bc, "ice_thickness_east_BC": bc,
+           "ice_thickness_south_BC": bc, "ice_thickness_north_BC": bc}
+    ctx = diva.Context(g, cfg, ob.oracle_backend())
+    ctx.upload({k: np.asfortranarray(v) for k, v in f.items()})
+    ctx.update_general_ice_model_data()
+    ctx.determine_floating_margin_fraction()
+    return ctx, g
+
+
+def numpy_dHi_dt(o, dx, dt):
+    """calc_dHi_dt_explicit restated with NumPy (the outflux limitation as the reference's
+    sequential in-place loop, i outer and j inner)."""
+    H, u, v = o["Hi_a"], o["u_vav_cx"], o["v_vav_cy"]
+    ny, nx = H.shape
+    Qx = u * np.where(u > 0, H[:, :-1], H[:, 1:]) * dx * dt
+    Qy = v * np.where(v > 0, H[:-1, :], H[1:, :]) * dx * dt
+    msmb = o["SMB_a"] + o["BMB_a"]
+    cf_shelf = (o["mask_cf_a"] == 1) & (o["mask_shelf_a"] == 1)
+    open_ocean = (o["mask_ocean_a"] == 1) & (o["mask_shelf_a"] == 0)
+    mb = np.where(cf_shelf, msmb * dx * dx * dt * o["float_margin_frac_a"],
+                  np.where(open_ocean, 0.0, msmb * dx * dx * dt))
+    for i in range(nx):
+        for j in range(ny):
+            avail = H[j, i] * dx * dx
+            out = 0.0
+            if i > 0 and not Qx[j, i - 1] > 0: out -= Qx[j, i - 1]
+            if i < nx - 1 and not Qx[j, i] < 0: out += Qx[j, i]
+            if j > 0 and not Qy[j - 1, i] > 0: out -= Qy[j - 1, i]
+            if j < ny - 1 and not Qy[j, i] < 0: out += Qy[j, i]
+            r = 1.0
+            if -mb[j, i] >= avail:
+                mb[j, i] = -avail
+                r = 0.0
+            if out > avail + mb[j, i]:
+                r = (avail + mb[j, i]) / out
+            if r < 1.0:
+                if i > 0 and Qx[j, i - 1] < 0: Qx[j, i - 1] *= r
+                if i < nx - 1 and Qx[j, i] > 0: Qx[j, i] *= r
+                if j > 0 and Qy[j - 1, i] < 0: Qy[j - 1, i] *= r
+                if j < ny - 1 and Qy[j, i] > 0: Qy[j, i] *= r
+    den = dx * dx * dt
+    d = mb / den
+    d[:, 1:] = d[:, 1:] + Qx / den
+    d[:, :-1] = d[:, :-1] - Qx / den
+    d[1:, :] = d[1:, :] + Qy / den
+    d[:-1, :] = d[:-1, :] - Qy / den
+    d = np.maximum(d, -H / dt)
+    return Qx, Qy, d, H + d * dt
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_explicit_update_matches_a_numpy_restatement(seed):
+    ctx, g = small_case(seed)
+    dt = 2.5
+    ctx.calc_dHi_dt(dt)
+    o = ctx.download()
+    Qx, Qy, d, Hn = numpy_dHi_dt(o, g.dx, dt)
+    # the column sums in d are accumulated in the reference's term order only up to
+    # reassociation, so 1e-12; fluxes are elementwise and exact
+    np.testing.assert_array_equal(o["Qx_cx"], Qx)
+    np.testing.assert_array_equal(o["Qy_cy"], Qy)
+    np.testing.assert_allclose(o["dHi_dt_a"], d, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(o["Hi_tplusdt_a"], Hn, rtol=1e-12, atol=1e-9)
+    assert o["Hi_tplusdt_a"].min() >= -1e-9                    # outfluxes were limited
+
+
+def test_explicit_update_conserves_mass():
+    ctx, g = small_case(5)
+    dt = 1.0
+    ctx.calc_dHi_dt(dt)
+    o = ctx.download()
+    # fluxes only cross interior faces: the volume change is the applied mass balance,
+    # wherever the -Hi/dt floor did not act
+    Qx, Qy, d, Hn = numpy_dHi_dt(o, g.dx, dt)
+    floor = np.isclose(o["dHi_dt_a"], -o["Hi_a"] / dt)
+    vol = (o["Hi_tplusdt_a"] - o["Hi_a"]).sum() * g.dx ** 2
+    div = np.zeros_like(o["Hi_a"])
+    div[:, 1:] += o["Qx_cx"]; div[:, :-1] -= o["Qx_cx"]; div[1:, :] += o["Qy_cy"]; div[:-1, :] -= o["Qy_cy"]
+    mb = (o["dHi_dt_a"] * dt * g.dx ** 2 - div)
+    assert abs(div.sum()) <= 1e-6 * np.abs(o["Qx_cx"]).sum()
+    assert np.isclose(vol, mb.sum() + div.sum(), rtol=1e-10)
+    assert floor.sum() < floor.size
+
+
+def test_thickness_boundary_conditions():
+    ny, nx = 9, 11
+    for bc, check in [
+        ("zero", lambda o: np.all(o["Hi_tplusdt_a"][:, :2] == 0) and np.all(o["Hi_tplusdt_a"][:2, :] == 0)
+         and np.all(o["Hi_tplusdt_a"][:, -2:] == 0) and np.all(o["Hi_tplusdt_a"][-2:, :] == 0)),
+        ("fixed", lambda o: np.all(o["Hi_tplusdt_a"][:, 0] == o["Hi_a"][:, 0]) and np.all(o["dHi_dt_a"][0, :] == 0)),
+        ("periodic", lambda o: np.all(o["Hi_tplusdt_a"][1:-1, 0] == o["Hi_a"][1:-1, nx - 2])
+         and np.all(o["Hi_tplusdt_a"][-1, :] == o["Hi_a"][1, :])),
+    ]:
+        ctx, g = small_case(1, nx=nx, ny=ny, bc=bc)
+        ctx.calc_dHi_dt(1.0)
+        assert check(ctx.download()), bc
+    # 'infinite': the edge cell takes the surface of its inner neighbour at t + dt
+    ctx, g = small_case(2, nx=nx, ny=ny, bc="none")
+    ctx.set_config({"choice_ice_dynamics": "DIVA", "ice_thickness_west_BC": "infinite", "ice_thickness_east_BC": "none",
+                    "ice_thickness_south_BC": "none", "ice_thickness_north_BC": "none"})
+    ctx.calc_dHi_dt(1.0)
+    o = ctx.download()
+    Hn, Hb, SL = o["Hi_tplusdt_a"], o["Hb_a"], o["SL_a"]
+    Hs_in = Hn[:, 1] + np.maximum(SL[:, 1] - RHO_I / RHO_SW * Hn[:, 1], Hb[:, 1])
+    Hs_float = Hb[:, 0] + (SL[:, 0] - Hb[:, 0]) * RHO_SW / RHO_I
+    expect = np.where(Hs_in > Hs_float, Hs_in - Hb[:, 0], (Hs_in - SL[:, 0]) / (1.0 - RHO_I / RHO_SW))
+    np.testing.assert_allclose(Hn[:, 0], expect, rtol=1e-14)
+    # with SIA dynamics only the edge row/column is zeroed
+    ctx, g = small_case(1, nx=nx, ny=ny, bc="zero", dyn="SIA")
+    ctx.calc_dHi_dt(1.0)
+    o = ctx.download()
+    assert np.all(o["Hi_tplusdt_a"][:, 0] == 0) and np.any(o["Hi_tplusdt_a"][2:-2, 1] != 0)
+
+
+def test_critical_timestep_known_answer():
+    ctx, g = small_case(0)
+    u = np.full((g.ny, g.nx - 1), 100.0)
+    v = np.zeros((g.ny - 1, g.nx))
+    v[3, 4] = -300.0
+    ctx.upload({"u_vav_cx": u, "v_vav_cy": v})
+    assert ctx.calc_critical_timestep_adv(10.0) == min(10.0, 0.9 * g.dx / 400.0)
+    assert ctx.calc_critical_timestep_adv(1e-3) == 1e-3                    # capped at dt_max
+
+
+def test_floating_margin_fraction_known_answer():
+    ny, nx = 7, 7
+    g = diva.Grid(nx, ny, 1e3)
+    H = np.zeros((ny, nx))
+    H[:, :3] = 400.0            # a shelf ...
+    H[3, 3] = 100.0             # ... and a thin calving-front cell beyond it
+    f = {"Hi_a": H, "Hb_a": np.full((ny, nx), -1000.0), "SL_a": np.zeros((ny, nx)),
+         "Ti_a": np.full((g.nz, ny, nx), 260.0)}
+    ctx = diva.Context(g, {}, ob.oracle_backend())
+    ctx.upload({k: np.asfortranarray(v) for k, v in f.items()})
+    ctx.update_general_ice_model_data()
+    ctx.determine_floating_margin_fraction()
+    o = ctx.download(["float_margin_frac_a", "Hi_eff_cf_a", "mask_cf_a"])
+    assert o["mask_cf_a"][3, 3] == 1
+    # its non-front ice neighbours are the interior shelf cells of column 1 (400 m)
+    assert o["float_margin_frac_a"][3, 3] == 100.0 / 400.0 and o["Hi_eff_cf_a"][3, 3] == 400.0
+    assert o["float_margin_frac_a"][3, 5] == 0.0 and o["float_margin_frac_a"][3, 1] == 1.0
+
+
+def test_predictor_corrector_steps_on_the_oracle():
+    g, cfg, f = synth.marine_channel(dx=20e3)
+    f = dict(f)
+    f["SMB_a"] = np.asfortranarray(np.full_like(f["Hi_a"], 0.3))
+    f["BMB_a"] = np.asfortranarray(np.where(f["Hb_a"] < -400.0, -1.0, 0.0))
+    cfg = dict(cfg, lin_rtol=1e-10, ice_thickness_west_BC="infinite", ice_thickness_east_BC="zero",
+               ice_thickness_south_BC="infinite", ice_thickness_north_BC="infinite")
+    ctx = diva.Context(diva.Grid(**g), cfg, ob.oracle_backend())
+    ob.set_linear_solver(ctx, ob.LIN_GMRES_WARM, 1e-10, 0.0)
+    helpers.prepare(ctx, f)
+    ctx.determine_floating_margin_fraction()
+    pc = dynamics.PCTimeStepper(ctx, start_time=0.0, end_time=1000.0)
+    H0 = ctx.download(["Hi_a"])["Hi_a"].copy()
+    n = pc.run(max_steps=4)
+    o = ctx.download(["Hi_a", "pc_tau", "dHi_dt_a"])
+    assert n == 4 and len(pc.reports) == 4
+    assert pc.time > 0.0 and pc.dt_crit_ice >= pc.dt_min
+    assert o["Hi_a"].min() >= 0.0 and np.isfinite(o["Hi_a"]).all()
+    change = np.abs(o["Hi_a"] - H0)
+    assert np.all(o["Hi_a"][:, -2:] == 0.0)                        # the 'zero' east edge (two columns, DIVA)
+    assert 0.0 < change[2:-2, 2:-2].max() < 50.0                    # a few years of flow inside
+    assert pc.pc_eta >= pc.pc_eta_min and np.isfinite(pc.pc_eta)
