@@ -4,8 +4,9 @@
 //
 // All device memory of a context is one cudaMalloc'd arena carved at create
 // time; no call after diva_create allocates.  Every kernel runs on the
-// context's stream.  Host synchronisation happens once per viscosity
-// iteration (to read the step norm) and once per Krylov half-step.
+// context's stream.  The viscosity loop is one CUDA graph launch per solve
+// (device-side loop; the host waits once, at its end); the host-driven fallback
+// synchronises once per viscosity iteration and once per Krylov half-step.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -255,7 +256,7 @@ int graph_loop_begin(Ctx* c, GraphLoop& L) {
   return DIVA_OK;
 }
 
-// enqueue one iteration and the copy of its status block (pinned host mirror)
+// enqueue the whole viscosity loop (one graph launch) and the copy of its status block
 int graph_loop_launch(Ctx* c, GraphLoop& L) {
   PicardGraphs& G = c->graphs[L.diva ? 1 : 0];
   int parity;
@@ -263,35 +264,33 @@ int graph_loop_launch(Ctx* c, GraphLoop& L) {
   else if (c->f[DIVA_F_VISC_EFF_3D_A] == G.visc_buf[1]) parity = 1;
   else return set_error(c, DIVA_CUDA_ERROR, "viscosity buffers out of step with the captured graphs");
   DIVA_CUDA(c, cudaGraphLaunch(G.exec[parity], c->stream));
-  std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
   DIVA_CUDA(c, cudaMemcpyAsync(c->h_scal + SC_TARGET2, c->scal + SC_TARGET2,
                                sizeof(double) * (SC_COUNT - SC_TARGET2), cudaMemcpyDeviceToHost, c->stream));
   return DIVA_OK;
 }
 
-// wait for the iteration launched last and account for it; L.done when the loop stops
+// wait for the loop and account for it: every iteration swapped the viscosity buffers
 int graph_loop_collect(Ctx* c, GraphLoop& L) {
-  const diva_config_t& C = c->c;
   PicardGraphs& G = c->graphs[L.diva ? 1 : 0];
   DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
   const double* h = c->h_scal;
   L.it = (int)h[SC_PIC_IT];
-  const bool solved = h[SC_SOLVED] != 0.0;
-  const long lin = (long)h[SC_LIN_IT], full = (long)h[SC_LIN_FULL];
+  if (L.it & 1) std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
+  const long lin = (long)h[SC_SUM_LIN], full = (long)h[SC_SUM_FULL], solved = (long)h[SC_N_SOLVED];
   c->lin_iters += lin;
   c->mg_cycles += lin + full;
-  c->launches += G.n_pre + G.n_post + (solved ? G.n_head + G.n_tail + lin * G.n_first + full * G.n_second : 0);
-  c->fine_passes += G.p_pre + (solved ? G.p_head + G.p_tail + lin * G.p_first + full * G.p_second : 0.0);
+  c->launches += (long long)L.it * (G.n_pre + G.n_post) + solved * (G.n_head + G.n_tail) + lin * G.n_first +
+                 full * G.n_second;
+  c->fine_passes += L.it * G.p_pre + solved * (G.p_head + G.p_tail) + lin * G.p_first + full * G.p_second;
   L.relres = h[SC_RELRES];
+  L.done = true;
   if (h[SC_NAN] != 0.0) return set_error(c, DIVA_NAN_DETECTED, "NaN in the viscosity iteration");
   if (h[SC_EXIT_RELRES] != 0.0) {
     L.by_relres = true;
-    L.done = true;
     return DIVA_OK;
   }
   L.resid = h[SC_RESID];
-  if (h[SC_CONVERGED] != 0.0) L.done = true;
-  else if (L.it > C.DIVA_visc_it_nit + 1) return set_error(c, DIVA_TIMEOUT, "viscosity iteration did not stop");
+  if (h[SC_CONVERGED] == 0.0) return set_error(c, DIVA_TIMEOUT, "viscosity iteration did not stop");
   return DIVA_OK;
 }
 
@@ -316,10 +315,8 @@ int picard_graph(Ctx* c, bool diva, diva_report_t* rep) {
   GraphLoop L;
   L.diva = diva;
   int st = graph_loop_begin(c, L);
-  while (!st && !L.done) {
-    if ((st = graph_loop_launch(c, L))) break;
-    st = graph_loop_collect(c, L);
-  }
+  if (!st) st = graph_loop_launch(c, L);
+  if (!st) st = graph_loop_collect(c, L);
   if (st) return st;
   return graph_loop_end(c, L, rep);
 }
@@ -643,11 +640,11 @@ int diva_solve_diva(diva_ctx_t* h, diva_report_t* rep) {
   return pst;
 }
 
-// solve_DIVA for several contexts at once.  Each context runs on its own stream; one
-// viscosity iteration of every unfinished context is kept in flight, so the
-// iterations of different members overlap on the GPU.  A context that cannot use
-// graph-launched iterations (graph construction unavailable) is solved on its own
-// after the others.  reports[k] receives the report of ctxs[k]; the return value is
+// solve_DIVA for several contexts at once.  Each context runs its graph-launched
+// viscosity loop on its own stream, all launched before any is waited for, so the
+// iterations of different members overlap on the GPU.  A context that cannot use the
+// graph-launched loop (graph construction unavailable) is solved on its own after
+// the others.  reports[k] receives the report of ctxs[k]; the return value is
 // DIVA_OK if every member returned OK, else the first other status.
 int diva_solve_diva_batch(diva_ctx_t** hs, int32_t n, diva_report_t* reports) {
   if (!hs || n < 1 || !reports) return DIVA_BAD_INPUT;
@@ -687,7 +684,7 @@ int diva_solve_diva_batch(diva_ctx_t** hs, int32_t n, diva_report_t* reports) {
     status[k] = st;
     if (st) rep->status = st;
   }
-  // iterations: launch one of every active member, then collect them in turn
+  // launch every active member's loop, then collect them in turn (one pass)
   for (;;) {
     bool any = false;
     for (int k = 0; k < n; ++k)

@@ -50,11 +50,13 @@ enum {
   SC_TARGET2, SC_LIN_IT, SC_LIN_FULL, SC_LIN_FAILED, SC_PIC_IT, SC_EXIT_RELRES, SC_CONVERGED, SC_RESID,
   SC_RELRES, SC_NAN, SC_SOLVED, SC_HALFDONE,
   SC_ETA, SC_RELRES_PREV,   // adaptive linear tolerance factor and the previous nonlinear residual
+  SC_SUM_LIN, SC_SUM_FULL, SC_N_SOLVED,   // totals of a graph-launched viscosity loop
   SC_COUNT = 40
 };
 
-// One instantiated graph per parity of the viscosity double buffer; the launch
-// and pass counts of each captured region turn executed iterations into totals.
+// The graph-launched viscosity loop: one instantiated graph per starting buffer of
+// the viscosity double buffer; the launch and pass counts of each captured region of
+// one iteration turn the loop's totals into launches and passes.
 struct PicardGraphs {
   bool valid = false;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};

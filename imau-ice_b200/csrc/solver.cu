@@ -29,6 +29,7 @@
 // results are bit-reproducible from run to run.
 #include <cmath>
 #include <cstdio>
+#include <utility>
 #include <vector>
 #include "ctx.hpp"
 
@@ -2198,8 +2199,9 @@ int solver_fill_boundary(Ctx* c, double* u, double* v) {
   return DIVA_OK;
 }
 
-// ---- one viscosity iteration as one CUDA graph ------------------------------------
+// ---- the viscosity iteration loop as one CUDA graph -------------------------------
 //
+// One viscosity iteration (ITER):
 //   pre   : k_ctl_begin, coefficients (K1 + faces), operator set-up of all levels,
 //           [relres stop rule] nonlinear residual -> k_ctl_relres sets IF(solve)
 //   IF(solve):
@@ -2211,15 +2213,22 @@ int solver_fill_boundary(Ctx* c, double* u, double* v) {
 //                   sets WHILE(krylov), p update
 //     tail  : boundary fill, Picard update (limits, relaxation, step norm, basal
 //             stress and velocity), stop test, DIVA_err commit
-//   post  : [DIVA] basal stress/velocity when the residual stopped the iteration
+//   post  : [DIVA] basal stress/velocity when the residual stopped the iteration;
+//           k_ctl_loop: continue unless the iteration converged, the residual met
+//           its tolerance, a NaN appeared or the iteration budget is spent
 //
-// Two instances are built, one per parity of the viscosity double buffer.
+// The whole loop: WHILE(picard) { ITER(parity p); IF(odd) { ITER(parity 1 - p) } }.
+// The viscosity is double-buffered (each iteration reads one buffer and writes the
+// other), and captured kernel arguments are fixed pointers, so the body holds two
+// iterations, one per buffer order; the first sets IF(odd) to its continue flag.
+// Two instances are built, one per starting buffer; one launch runs a whole solve
+// with no host round trip between iterations.
 namespace {
 
 struct CaptureCtx {
   Ctx* c;
-  cudaStream_t s[4] = {};
-  bool capturing[4] = {};
+  cudaStream_t s[6] = {};
+  bool capturing[6] = {};
   long long l0 = 0;
   double p0 = 0.0;
   void mark() { l0 = c->launches; p0 = c->fine_passes; }
@@ -2247,7 +2256,30 @@ int add_conditional(Ctx* c, cudaStream_t s, cudaGraphConditionalHandle h, cudaGr
   return DIVA_OK;
 }
 
-int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
+// the graph a capturing stream records into
+int capture_graph(Ctx* c, cudaStream_t s, cudaGraph_t* g) {
+  cudaStreamCaptureStatus st;
+  DIVA_CUDA(c, cudaStreamGetCaptureInfo(s, &st, nullptr, g, nullptr, nullptr));
+  if (st != cudaStreamCaptureStatusActive) return set_error(c, DIVA_CUDA_ERROR, "stream is not capturing");
+  return DIVA_OK;
+}
+
+// end of an iteration: totals of the loop, and whether it goes on (sets h_a, and h_b if given)
+__global__ void k_ctl_loop(double* sc, cudaGraphConditionalHandle h_a, cudaGraphConditionalHandle h_b, int has_b,
+                           int nit) {
+  sc[SC_SUM_LIN] += sc[SC_LIN_IT];
+  sc[SC_SUM_FULL] += sc[SC_LIN_FULL];
+  sc[SC_N_SOLVED] += sc[SC_SOLVED];
+  const bool stop = sc[SC_CONVERGED] != 0.0 || sc[SC_EXIT_RELRES] != 0.0 || sc[SC_NAN] != 0.0 ||
+                    sc[SC_PIC_IT] > (double)nit;
+  cudaGraphSetConditional(h_a, stop ? 0u : 1u);
+  if (has_b) cudaGraphSetConditional(h_b, stop ? 0u : 1u);
+}
+
+// One viscosity iteration recorded into the graph that stream `top` is capturing; its
+// conditional bodies use cc.s[3..5].  `count`: record the launches and passes of its parts.
+int capture_iteration(Ctx* c, CaptureCtx& cc, cudaStream_t top, bool diva, PicardGraphs& G, bool count,
+                      cudaGraphConditionalHandle h_a, cudaGraphConditionalHandle h_b, int has_b) {
   const diva_config_t& C = c->c;
   const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
   const Dims d = c->d;
@@ -2259,17 +2291,13 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
   double* u = c->D(diva ? DIVA_F_U_VAV_CX : DIVA_F_U_SSA_CX);
   double* v = c->D(diva ? DIVA_F_V_VAV_CY : DIVA_F_V_SSA_CY);
   int st;
-
   cudaGraph_t graph;
-  DIVA_CUDA(c, cudaGraphCreate(&graph, 0));
+  if ((st = capture_graph(c, top, &graph))) return st;
   cudaGraphConditionalHandle h_solve;
   DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_solve, graph, 1, cudaGraphCondAssignDefault));
-  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[0], graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  cc.capturing[0] = true;
-  c->stream = cc.s[0];
+  c->stream = top;
   // ---- pre
   cc.mark();
-  G.visc_buf[parity] = c->f[DIVA_F_VISC_EFF_3D_A];
   k_ctl_begin<<<1, 1, 0, c->stream>>>(c->scal); c->launches++;
   if ((st = launch_diva_coefficients(c, u, v, diva))) return st;   // swaps the viscosity buffers
   if ((st = solver_setup(c))) return st;
@@ -2279,16 +2307,16 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
     c->fine_passes += 1.0;
   }
   DIVA_LAUNCHED(c, "graph pre");
-  G.n_pre = cc.dl(); G.p_pre = cc.dp();
+  if (count) { G.n_pre = cc.dl(); G.p_pre = cc.dp(); }
   // ---- IF(solve)
   cudaGraph_t body_solve;
-  if ((st = add_conditional(c, cc.s[0], h_solve, cudaGraphCondTypeIf, &body_solve))) return st;
+  if ((st = add_conditional(c, top, h_solve, cudaGraphCondTypeIf, &body_solve))) return st;
   cudaGraphConditionalHandle h_while;
   DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_while, body_solve, 0, cudaGraphCondAssignDefault));
-  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[1], body_solve, nullptr, nullptr, 0,
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[3], body_solve, nullptr, nullptr, 0,
                                              cudaStreamCaptureModeThreadLocal));
-  cc.capturing[1] = true;
-  c->stream = cc.s[1];
+  cc.capturing[3] = true;
+  c->stream = cc.s[3];
   cc.mark();
   DIVA_CUDA(c, cudaMemcpyAsync(U_(KV_X), u, sizeof(double) * d.plane, cudaMemcpyDeviceToDevice, c->stream));
   DIVA_CUDA(c, cudaMemcpyAsync(V_(KV_X), v, sizeof(double) * d.plane, cudaMemcpyDeviceToDevice, c->stream));
@@ -2298,16 +2326,16 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
                                            C.lin_maxit); c->launches++;
   c->fine_passes += 1.0;
   DIVA_LAUNCHED(c, "graph head");
-  G.n_head = cc.dl(); G.p_head = cc.dp();
+  if (count) { G.n_head = cc.dl(); G.p_head = cc.dp(); }
   // ---- WHILE(krylov)
   cudaGraph_t body_while;
-  if ((st = add_conditional(c, cc.s[1], h_while, cudaGraphCondTypeWhile, &body_while))) return st;
+  if ((st = add_conditional(c, cc.s[3], h_while, cudaGraphCondTypeWhile, &body_while))) return st;
   cudaGraphConditionalHandle h_half;
   DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_half, body_while, 1, cudaGraphCondAssignDefault));
-  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[2], body_while, nullptr, nullptr, 0,
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[4], body_while, nullptr, nullptr, 0,
                                              cudaStreamCaptureModeThreadLocal));
-  cc.capturing[2] = true;
-  c->stream = cc.s[2];
+  cc.capturing[4] = true;
+  c->stream = cc.s[4];
   cc.mark();
   if ((st = precond(c, U_(KV_P), V_(KV_P), U_(KV_PHAT), V_(KV_PHAT)))) return st;
   k_matvec<<<g2, block2d(), 0, c->stream>>>(o, U_(KV_PHAT), V_(KV_PHAT), U_(KV_V), V_(KV_V), U_(KV_RHAT), V_(KV_RHAT),
@@ -2319,14 +2347,14 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
   k_x_half_pred<<<g2, block2d(), 0, c->stream>>>(d, c->scal, U_(KV_X), V_(KV_X), U_(KV_PHAT), V_(KV_PHAT)); c->launches++;
   c->fine_passes += 3.0;
   DIVA_LAUNCHED(c, "graph first half");
-  G.n_first = cc.dl(); G.p_first = cc.dp();
+  if (count) { G.n_first = cc.dl(); G.p_first = cc.dp(); }
   // ---- IF(second half)
   cudaGraph_t body_half;
-  if ((st = add_conditional(c, cc.s[2], h_half, cudaGraphCondTypeIf, &body_half))) return st;
-  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[3], body_half, nullptr, nullptr, 0,
+  if ((st = add_conditional(c, cc.s[4], h_half, cudaGraphCondTypeIf, &body_half))) return st;
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[5], body_half, nullptr, nullptr, 0,
                                              cudaStreamCaptureModeThreadLocal));
-  cc.capturing[3] = true;
-  c->stream = cc.s[3];
+  cc.capturing[5] = true;
+  c->stream = cc.s[5];
   cc.mark();
   if ((st = precond(c, U_(KV_S), V_(KV_S), U_(KV_SHAT), V_(KV_SHAT)))) return st;
   k_matvec<<<g2, block2d(), 0, c->stream>>>(o, U_(KV_SHAT), V_(KV_SHAT), U_(KV_T), V_(KV_T), U_(KV_S), V_(KV_S),
@@ -2339,13 +2367,13 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
   k_update_p<<<g2, block2d(), 0, c->stream>>>(d, c->scal, U_(KV_R), V_(KV_R), U_(KV_V), V_(KV_V), U_(KV_P), V_(KV_P)); c->launches++;
   c->fine_passes += 3.0;
   DIVA_LAUNCHED(c, "graph second half");
-  G.n_second = cc.dl(); G.p_second = cc.dp();
-  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[3], &body_half));
-  cc.capturing[3] = false;
-  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[2], &body_while));
-  cc.capturing[2] = false;
+  if (count) { G.n_second = cc.dl(); G.p_second = cc.dp(); }
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[5], &body_half));
+  cc.capturing[5] = false;
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[4], &body_while));
+  cc.capturing[4] = false;
   // ---- tail
-  c->stream = cc.s[1];
+  c->stream = cc.s[3];
   cc.mark();
   k_ctl_lin_finish<<<1, 1, 0, c->stream>>>(c->scal); c->launches++;
   k_fill_boundary<<<g2, block2d(), 0, c->stream>>>(d, c->bc, U_(KV_X), V_(KV_X)); c->launches++;
@@ -2353,14 +2381,46 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
   if ((st = launch_picard_update(c, u, v, U_(KV_X), V_(KV_X), diva))) return st;
   if ((st = launch_ctl_end(c, relmode))) return st;
   if ((st = launch_err_commit_pred(c))) return st;
-  G.n_tail = cc.dl(); G.p_tail = cc.dp();
-  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[1], &body_solve));
-  cc.capturing[1] = false;
+  if (count) { G.n_tail = cc.dl(); G.p_tail = cc.dp(); }
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[3], &body_solve));
+  cc.capturing[3] = false;
   // ---- post
-  c->stream = cc.s[0];
+  c->stream = top;
   cc.mark();
   if (diva && relmode && (st = launch_basal_pred(c))) return st;
-  G.n_post = cc.dl();
+  k_ctl_loop<<<1, 1, 0, c->stream>>>(c->scal, h_a, h_b, has_b, C.DIVA_visc_it_nit); c->launches++;
+  DIVA_LAUNCHED(c, "k_ctl_loop");
+  if (count) G.n_post = cc.dl();
+  return DIVA_OK;
+}
+
+// the loop graph starting from the viscosity buffer `parity`
+int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
+  cudaGraph_t graph;
+  DIVA_CUDA(c, cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle h_pic;
+  DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_pic, graph, 1, cudaGraphCondAssignDefault));
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[0], graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cc.capturing[0] = true;
+  G.visc_buf[parity] = c->f[DIVA_F_VISC_EFF_3D_A];
+  int st;
+  cudaGraph_t body_pic;
+  if ((st = add_conditional(c, cc.s[0], h_pic, cudaGraphCondTypeWhile, &body_pic))) return st;
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[1], body_pic, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cc.capturing[1] = true;
+  cudaGraphConditionalHandle h_odd;
+  DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_odd, body_pic, 0, cudaGraphCondAssignDefault));
+  // the first iteration of the pair (its buffer order is this graph's parity)
+  if ((st = capture_iteration(c, cc, cc.s[1], diva, G, parity == 0, h_pic, h_odd, 1))) return st;
+  cudaGraph_t body_odd;
+  if ((st = add_conditional(c, cc.s[1], h_odd, cudaGraphCondTypeIf, &body_odd))) return st;
+  DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[2], body_odd, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cc.capturing[2] = true;
+  if ((st = capture_iteration(c, cc, cc.s[2], diva, G, false, h_pic, h_pic, 0))) return st;
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[2], &body_odd));
+  cc.capturing[2] = false;
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[1], &body_pic));
+  cc.capturing[1] = false;
   DIVA_CUDA(c, cudaStreamEndCapture(cc.s[0], &graph));
   cc.capturing[0] = false;
   cudaGraphExec_t exec = nullptr;
@@ -2392,12 +2452,15 @@ int solver_build_picard_graphs(Ctx* c, bool diva) {
   void* visc0 = c->f[DIVA_F_VISC_EFF_3D_A];
   double* prev0 = c->visc_prev;
   int st = DIVA_OK;
-  for (int q = 0; q < 4 && !st; ++q)
+  for (int q = 0; q < 6 && !st; ++q)
     if (cudaStreamCreateWithFlags(&cc.s[q], cudaStreamNonBlocking) != cudaSuccess) st = DIVA_CUDA_ERROR;
-  // parity 0 starts from the current buffer, parity 1 from the other; the two
-  // captures swap the viscosity buffers twice, so the host state is unchanged
-  for (int parity = 0; parity < 2 && !st; ++parity) st = build_one(c, cc, diva, G, parity);
-  for (int q = 3; q >= 0; --q) {
+  // parity 0 starts from the current buffer, parity 1 from the other; each graph
+  // captures two iterations, which swap the viscosity buffers twice
+  for (int parity = 0; parity < 2 && !st; ++parity) {
+    if (parity == 1) std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
+    st = build_one(c, cc, diva, G, parity);
+  }
+  for (int q = 5; q >= 0; --q) {
     if (cc.capturing[q]) {
       cudaGraph_t junk = nullptr;
       cudaStreamEndCapture(cc.s[q], &junk);
@@ -2405,7 +2468,7 @@ int solver_build_picard_graphs(Ctx* c, bool diva) {
     }
   }
   cudaGetLastError();   // clear any capture error so the host path can proceed
-  for (int q = 0; q < 4; ++q)
+  for (int q = 0; q < 6; ++q)
     if (cc.s[q]) cudaStreamDestroy(cc.s[q]);
   c->stream = user;
   c->launches = launches0;

@@ -338,7 +338,7 @@ def solve_SSA(grid, ice, config=None, backend=None):
 
 def solve_DIVA_batch(contexts):
     """solve_DIVA for several contexts at once (diva_solve_diva_batch): each on its own
-    stream, one viscosity iteration of every unfinished member in flight, so small
+    stream, every member's graph-launched viscosity loop in flight at once, so small
     members share the GPU.  Returns the reports in order; raises DivaError naming the
     first member whose status is neither OK nor MAX_PICARD."""
     if not contexts:

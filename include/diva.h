@@ -196,8 +196,8 @@ int  diva_solve_ssa(diva_ctx_t* ctx, diva_report_t* rep);
 /* solve_DIVA (ice_velocity_module.f90:249-374); needs DIVA. */
 int  diva_solve_diva(diva_ctx_t* ctx, diva_report_t* rep);
 /* solve_DIVA for n contexts at once (an ensemble; no single routine of the reference:
- * its members would be separate solve_DIVA calls).  Each context runs on its own
- * stream and one viscosity iteration of every unfinished member is kept in flight,
+ * its members would be separate solve_DIVA calls).  Each context runs its
+ * graph-launched viscosity loop on its own stream, all members in flight at once,
  * so the iterations of different members overlap on the GPU.  reports[k] is the report
  * of ctxs[k] (its status included); returns DIVA_OK if every member is OK, else the
  * first other status.  Contexts must be distinct. */
