@@ -25,6 +25,8 @@ RHEO = {"uniform": 0, "Huybrechts1992": 1}
 STOP = {"resid_UV": 0, "relres": 1}
 PREC = {"fp64": 0, "mixed": 1}
 HBC = {"zero": 0, "infinite": 1, "periodic": 2, "fixed": 3, "none": 4}
+HEATCAP = {"uniform": 0, "Pounder1965": 1}
+CONDUCT = {"uniform": 0, "Ritz1987": 1}
 
 GRID_KINDS = ["A", "CX", "CY", "B", "A3", "CX3", "CY3", "B3"]
 
@@ -75,6 +77,12 @@ class Config(C.Structure):
         ("precision", C.c_int32),
         ("ice_thickness_west_BC", C.c_int32), ("ice_thickness_east_BC", C.c_int32),
         ("ice_thickness_south_BC", C.c_int32), ("ice_thickness_north_BC", C.c_int32),
+        ("dt_thermo", C.c_double),
+        ("choice_ice_heat_capacity", C.c_int32),
+        ("uniform_ice_heat_capacity", C.c_double),
+        ("choice_ice_thermal_conductivity", C.c_int32),
+        ("uniform_ice_thermal_conductivity", C.c_double),
+        ("T_ocean_mean_PD_ANT", C.c_double),
         ("reserved", C.c_int32 * 8),
     ]
 
@@ -106,6 +114,7 @@ ENUM_OPTIONS = {
     "choice_ice_rheology": RHEO, "picard_stop": STOP, "precision": PREC,
     "ice_thickness_west_BC": HBC, "ice_thickness_east_BC": HBC, "ice_thickness_south_BC": HBC,
     "ice_thickness_north_BC": HBC,
+    "choice_ice_heat_capacity": HEATCAP, "choice_ice_thermal_conductivity": CONDUCT,
 }
 
 
@@ -136,6 +145,7 @@ def bind(lib, prefix):
         "pc_predictor": (C.c_int, [vp, C.c_double, C.c_double]),
         "pc_corrector": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, dp]),
         "pc_finish": (C.c_int, [vp, C.c_double]),
+        "run_thermo_model": (C.c_int, [vp, i32, C.POINTER(C.c_int32)]),
         "last_error": (C.c_char_p, [vp]),
     }
     fns = {}

@@ -112,6 +112,10 @@ void config_defaults(diva_config_t* c) {
   c->do_ocean_floodfill = 1;
   c->lin_rtol = 1E-8; c->lin_maxit = 500;
   c->picard_stop = DIVA_STOP_RESID_UV; c->picard_relres_tol = 1E-6; c->lin_adaptive = 0; c->lin_adaptive_eta = 0.5;
+  c->dt_thermo = 10.0;                                   // configuration_module.f90:56, 427-430, 647
+  c->choice_ice_heat_capacity = DIVA_HEATCAP_POUNDER1965; c->uniform_ice_heat_capacity = 2009.0;
+  c->choice_ice_thermal_conductivity = DIVA_CONDUCT_RITZ1987; c->uniform_ice_thermal_conductivity = 6.626958E7;
+  c->T_ocean_mean_PD_ANT = -1.7;
   c->precision = DIVA_PREC_FP64;
 }
 

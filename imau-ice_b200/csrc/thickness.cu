@@ -388,6 +388,9 @@ int diva_pc_corrector(diva_ctx_t* h, double dt, double zeta, double eta_min, dou
 int diva_pc_finish(diva_ctx_t* h, double dt) {
   if (!h || !(dt >= 0.0)) return DIVA_BAD_INPUT;
   Ctx* c = &h->c;
+  // update_ice_thickness keeps the ice mask of the step for the thermodynamics (:446)
+  DIVA_CUDA(c, cudaMemcpyAsync(c->I(DIVA_F_MASK_ICE_A_PREV), c->I(DIVA_F_MASK_ICE_A), sizeof(int) * c->d.plane,
+                               cudaMemcpyDeviceToDevice, c->stream));
   k_pc_finish<<<G2T>>>(c->d, dt, c->D(DIVA_F_HI_A), c->D(DIVA_F_DHI_DT_A), c->D(DIVA_F_HI_TPLUSDT_A)); c->launches++;
   DIVA_LAUNCHED(c, "k_pc_finish");
   if (int st = launch_update_general_ice_model_data(c)) return st;

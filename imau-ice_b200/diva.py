@@ -257,6 +257,14 @@ class Context:
         """Hi_tplusdt_a and the thickness update of the step (:429-431, :435-648 in part)."""
         self._check(self.backend.fns["pc_finish"](self.h, float(dt)), "pc_finish")
 
+    def run_thermo_model(self, do_solve_heat_equation=True):
+        """run_thermo_model with the 3D heat equation (thermodynamics_module.f90:29-121);
+        returns the number of unstable columns replaced by the Robin solution."""
+        n = C.c_int32()
+        self._check(self.backend.fns["run_thermo_model"](self.h, int(bool(do_solve_heat_equation)), C.byref(n)),
+                    "run_thermo_model")
+        return n.value
+
     def state_save(self):
         self._check(self.backend.fns["state_save"](self.h), "state_save")
 

@@ -81,6 +81,8 @@ typedef enum { DIVA_STOP_RESID_UV = 0, DIVA_STOP_RELRES = 1 } diva_stop_t;
  * MIXED needs the tiled smoother (no periodic side) and a grid of at least 9 points in one
  * direction; otherwise the solve returns DIVA_UNSUPPORTED. */
 typedef enum { DIVA_PREC_FP64 = 0, DIVA_PREC_MIXED = 1 } diva_precision_t;
+typedef enum { DIVA_HEATCAP_UNIFORM = 0, DIVA_HEATCAP_POUNDER1965 = 1 } diva_heatcap_t;
+typedef enum { DIVA_CONDUCT_UNIFORM = 0, DIVA_CONDUCT_RITZ1987 = 1 } diva_conductivity_t;
 /* Ice thickness at the domain boundary (apply_ice_thickness_BC, ice_thickness_module.f90:728-931). */
 typedef enum { DIVA_HBC_ZERO = 0, DIVA_HBC_INFINITE = 1, DIVA_HBC_PERIODIC = 2, DIVA_HBC_FIXED = 3,
                DIVA_HBC_NONE = 4 } diva_hbc_t;
@@ -137,6 +139,14 @@ typedef struct {
   int32_t precision;                    /* diva_precision_t */
   /* ice thickness boundary conditions, diva_hbc_t (configuration_module.f90:325-328, default zero) */
   int32_t ice_thickness_west_BC, ice_thickness_east_BC, ice_thickness_south_BC, ice_thickness_north_BC;
+  /* thermodynamics (configuration_module.f90:56, 424-430, 647); the ocean model is 'none':
+   * the shelf base sits at T0 + T_ocean_mean_PD_ANT */
+  double  dt_thermo;                           /* :56, default 10 yr */
+  int32_t choice_ice_heat_capacity;            /* diva_heatcap_t, default Pounder1965 */
+  double  uniform_ice_heat_capacity;           /* :428, 2009 */
+  int32_t choice_ice_thermal_conductivity;     /* diva_conductivity_t, default Ritz1987 */
+  double  uniform_ice_thermal_conductivity;    /* :430, 6.626958E7 */
+  double  T_ocean_mean_PD_ANT;                 /* :647, -1.7 */
   int32_t reserved[8];
 } diva_config_t;
 
@@ -237,6 +247,17 @@ int  diva_pc_corrector(diva_ctx_t* ctx, double dt, double zeta, double eta_min, 
  * :435-648, without calving, fixed geometries or the no-ice mask) Hi_a = Hi_tplusdt_a,
  * update_general_ice_model_data and determine_floating_margin_fraction. */
 int  diva_pc_finish(diva_ctx_t* ctx, double dt);
+
+/* run_thermo_model with choice_thermo_model '3D_heat_equation' (thermodynamics_module.f90:
+ * 29-121): temperature of newly ice-covered columns from their upwind neighbour,
+ * frictional heating, heat capacity, conductivity, pressure melting point, then (when
+ * do_solve_heat_equation) solve_3D_heat_equation (:124-381: one implicit column solve
+ * per interior column over C%dt_thermo, unstable columns replaced by the Robin
+ * solution, :384-481), then calc_ice_rheology.  *n_unstable receives the number of
+ * unstable columns; more than 1 % of the grid returns DIVA_NAN_DETECTED (the reference
+ * crashes).  The column systems are solved by Gaussian elimination with partial
+ * pivoting in the order of LAPACK's dgtsv, which the reference calls. */
+int  diva_run_thermo_model(diva_ctx_t* ctx, int32_t do_solve_heat_equation, int32_t* n_unstable);
 
 /* FP64 nonlinear residual of the current (u_vav_cx, v_vav_cy): evaluates the
  * coefficients of the next viscosity iteration (A3-A7) and returns

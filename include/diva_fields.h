@@ -148,6 +148,21 @@
   X(DHIDT_HN_UN,          dHidt_Hn_un,          A,   D)      \
   X(DHIDT_HNM1_UNM1,      dHidt_Hnm1_unm1,      A,   D)      \
   X(DHIDT_HSTARNP1_UNP1,  dHidt_Hstarnp1_unp1,  A,   D)      \
-  X(PC_TAU,               pc_tau,               A,   D)
+  X(PC_TAU,               pc_tau,               A,   D)      \
+  X(MASK_ICE_A_PREV,      mask_ice_a_prev,      A,   I)      \
+  /* thermodynamics (thermodynamics_module.f90:29-608,   */ \
+  /*  derivatives_and_grids_module.f90:1892-2061);       */ \
+  /* T_surf_annual_a is SUM(climate%T2m)/12 and GHF_a    */ \
+  /* ice%GHF_a (J m-2 yr-1)                              */ \
+  X(T_SURF_ANNUAL_A,      T_surf_annual_a,      A,   D)      \
+  X(GHF_A,                GHF_a,                A,   D)      \
+  X(FRICTIONAL_HEATING_A, frictional_heating_a, A,   D)      \
+  X(CPI_A,                Cpi_a,                A3,  D)      \
+  X(KI_A,                 Ki_a,                 A3,  D)      \
+  X(DHS_DT_A,             dHs_dt_a,             A,   D)      \
+  X(DZETA_DT_A,           dzeta_dt_a,           A3,  D)      \
+  X(DZETA_DX_A,           dzeta_dx_a,           A3,  D)      \
+  X(DZETA_DY_A,           dzeta_dy_a,           A3,  D)      \
+  X(DZETA_DZ_A,           dzeta_dz_a,           A,   D)
 
 #endif /* DIVA_FIELDS_H */

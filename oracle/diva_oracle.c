@@ -2217,6 +2217,10 @@ void orc_config_defaults(diva_config_t* c) {
   c->do_ocean_floodfill = 1;
   c->lin_rtol = 1E-8; c->lin_maxit = 2000;
   c->picard_stop = DIVA_STOP_RESID_UV; c->picard_relres_tol = 1E-6; c->lin_adaptive = 0; c->lin_adaptive_eta = 0.5;
+  c->dt_thermo = 10.0;                                   /* configuration_module.f90:56, 427-430, 647 */
+  c->choice_ice_heat_capacity = DIVA_HEATCAP_POUNDER1965; c->uniform_ice_heat_capacity = 2009.0;
+  c->choice_ice_thermal_conductivity = DIVA_CONDUCT_RITZ1987; c->uniform_ice_thermal_conductivity = 6.626958E7;
+  c->T_ocean_mean_PD_ANT = -1.7;
   c->precision = DIVA_PREC_FP64;
 }
 
@@ -2539,11 +2543,269 @@ int orc_pc_finish(orc_ctx* c, double dt) {
   double *Hi = FD(c, HI_A), *Hn = FD(c, HI_TPLUSDT_A);
   const double* dH = FD(c, DHI_DT_A);
   for (size_t q = 0; q < n; ++q) Hn[q] = fmax(0.0, Hi[q] + dt * dH[q]);
+  memcpy(FI(c, MASK_ICE_A_PREV), FI(c, MASK_ICE_A), sizeof(int32_t) * n);   /* update_ice_thickness :446 */
   for (size_t q = 0; q < n; ++q) Hi[q] = fmax(0.0, Hn[q]);
   int st = orc_update_general_ice_model_data(c);
   if (st) return st;
   floating_margin_fraction(c);
   return DIVA_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Thermodynamics: run_thermo_model with the 3D heat equation                */
+
+#define SEC_PER_YEAR 31556943.36                 /* parameters_module.f90:12 */
+
+/* Gaussian elimination with partial pivoting for a tridiagonal system (the algorithm of
+ * LAPACK dgtsv, which tridiagonal_solve, utilities_module.f90:791-834, calls): dl, d, du
+ * are overwritten, b holds the solution.  Returns 0, or k+1 for a zero pivot in row k. */
+int orc_tridiagonal_solve(int n, double* dl, double* d, double* du, double* b) {
+  for (int i = 0; i < n - 1; ++i) {
+    if (fabs(d[i]) >= fabs(dl[i])) {
+      if (d[i] == 0.0) return i + 1;
+      const double fact = dl[i] / d[i];
+      d[i + 1] = d[i + 1] - fact * du[i];
+      b[i + 1] = b[i + 1] - fact * b[i];
+      if (i < n - 2) dl[i] = 0.0;
+    } else {
+      const double fact = d[i] / dl[i];
+      d[i] = dl[i];
+      const double t = d[i + 1];
+      d[i + 1] = du[i] - fact * t;
+      if (i < n - 2) {
+        dl[i] = du[i + 1];
+        du[i + 1] = -fact * dl[i];
+      }
+      du[i] = t;
+      const double tb = b[i];
+      b[i] = b[i + 1];
+      b[i + 1] = tb - fact * b[i + 1];
+    }
+  }
+  if (d[n - 1] == 0.0) return n;
+  b[n - 1] = b[n - 1] / d[n - 1];
+  if (n > 1) b[n - 2] = (b[n - 2] - du[n - 2] * b[n - 1]) / d[n - 2];
+  for (int i = n - 3; i >= 0; --i) b[i] = (b[i] - du[i] * b[i + 1] - dl[i] * b[i + 2]) / d[i];
+  return 0;
+}
+
+/* zeta coefficients of initialise_zeta_discretisation, derivatives_and_grids_module.f90:1930-2000 */
+struct zeta_coef { double a[64], b[64], c[64], aa[64], bb[64], cc[64]; };
+static void zeta_coefficients(const double* z, int nz, struct zeta_coef* q) {
+  for (int k = 1; k < nz - 1; ++k) {
+    const double ak = z[k] - z[k - 1], bk = z[k + 1] - z[k];
+    q->a[k] = -bk / (ak * (ak + bk));
+    q->b[k] = (bk - ak) / (ak * bk);
+    q->c[k] = ak / (bk * (ak + bk));
+    q->aa[k] = 2.0 / (ak * (ak + bk));
+    q->bb[k] = -2.0 / (ak * bk);
+    q->cc[k] = 2.0 / (bk * (ak + bk));
+  }
+}
+
+/* replace_Ti_with_robin_solution, thermodynamics_module.f90:384-481 (ocean model 'none';
+ * the shelf profile adds T0_C to T0_C + T_ocean_mean_PD_ANT, as written) */
+static void robin_column(orc_ctx* c, double* Tn, int i, int j) {
+  DECL_DIMS(c);
+  const double* z = c->g.zeta;
+  const size_t q = IA(j, i);
+  const double Hi = FD(c, HI_A)[q], ghf = FD(c, GHF_A)[q], smb = FD(c, SMB_A)[q];
+  const double* Tp = FD(c, TI_PMP_A);
+  const double K = 9.828 * SEC_PER_YEAR * exp(-0.0057 * T0_C);
+  const double kappa = K / (ICE_DENSITY * 2127.5);
+  const double grad = -ghf / K;
+  const double Ts = fmin(T0_C, FD(c, T_SURF_ANNUAL_A)[q]);
+  if (FI(c, MASK_SHEET_A)[q] == 1) {
+    if (smb > 0.0) {
+      const double L = sqrt(2.0 * kappa * Hi / smb);
+      for (int k = 0; k < nz; ++k) {
+        const double erf1 = erf((1.0 - z[k]) * Hi / L), erf2 = erf(Hi / L);
+        Tn[IA3(k, j, i)] = Ts + sqrt(PI_C) / 2.0 * L * grad * (erf1 - erf2);
+      }
+    } else {
+      for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = Ts + ((T0_C - CC_C * Hi) - Ts) * z[k];
+    }
+  } else if (FI(c, MASK_SHELF_A)[q] == 1) {
+    const double To = T0_C + c->c.T_ocean_mean_PD_ANT;
+    for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = Ts + z[k] * (T0_C + To - Ts);
+  } else {
+    for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = Ts;
+  }
+  for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = fmin(Tn[IA3(k, j, i)], Tp[IA3(k, j, i)]);
+}
+
+/* solve_3D_heat_equation, thermodynamics_module.f90:124-381; returns the number of
+ * unstable columns (-1 if they exceed 1 % of the grid) */
+static int solve_3d_heat_equation(orc_ctx* c) {
+  DECL_DIMS(c);
+  const double dx = c->dx, dt = c->c.dt_thermo;
+  const double* z = c->g.zeta;
+  const double *Hi = FD(c, HI_A), *Hs = FD(c, HS_A);
+  const int32_t *ice = FI(c, MASK_ICE_A), *shelf = FI(c, MASK_SHELF_A), *sheet = FI(c, MASK_SHEET_A);
+  double *Ti = FD(c, TI_A), *dHs_dt = FD(c, DHS_DT_A);
+  const double *dHi_dt = FD(c, DHI_DT_A), *dHb_dt = FD(c, DHB_DT_A);
+  double *zdt = FD(c, DZETA_DT_A), *zdx = FD(c, DZETA_DX_A), *zdy = FD(c, DZETA_DY_A), *zdz = FD(c, DZETA_DZ_A);
+  const double *dHs_dx = FD(c, DHS_DX_A), *dHs_dy = FD(c, DHS_DY_A), *dHi_dx = FD(c, DHI_DX_A), *dHi_dy = FD(c, DHI_DY_A);
+  const double *Ts = FD(c, T_SURF_ANNUAL_A), *ghf = FD(c, GHF_A), *fh = FD(c, FRICTIONAL_HEATING_A);
+  const double *Cp = FD(c, CPI_A), *Ki = FD(c, KI_A), *Tp = FD(c, TI_PMP_A);
+  const double *u3 = FD(c, U_3D_A), *v3 = FD(c, V_3D_A), *w3 = FD(c, W_3D_A);
+  const double *ucx = FD(c, U_3D_CX), *vcy = FD(c, V_3D_CY);
+  (void)Hs;
+  for (size_t q = 0; q < (size_t)nx * ny; ++q)
+    dHs_dt[q] = shelf[q] == 0 ? dHi_dt[q] + dHb_dt[q] : dHi_dt[q] * (1.0 - ICE_DENSITY / SW_DENSITY);
+  /* calculate_zeta_derivatives, derivatives_and_grids_module.f90:1892-1929 */
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const size_t q = IA(j, i);
+      const double inv = 1.0 / Hi[q];
+      zdz[q] = -inv;
+      for (int k = 0; k < nz; ++k) {
+        zdt[IA3(k, j, i)] = inv * (dHs_dt[q] - z[k] * dHi_dt[q]);
+        zdx[IA3(k, j, i)] = inv * (dHs_dx[q] - z[k] * dHi_dx[q]);
+        zdy[IA3(k, j, i)] = inv * (dHs_dy[q] - z[k] * dHi_dy[q]);
+      }
+    }
+  for (size_t q = 0; q < (size_t)nx * ny; ++q) Ti[q * nz] = fmin(T0_C, Ts[q]);   /* layer 1 */
+  const double T_ocean = T0_C + c->c.T_ocean_mean_PD_ANT;
+  struct zeta_coef zc;
+  zeta_coefficients(z, nz, &zc);
+  double* Tn = (double*)calloc((size_t)nx * ny * nz, sizeof(double));
+  unsigned char* unstable = (unsigned char*)calloc((size_t)nx * ny, 1);
+  int n_unstable = 0;
+  double dl[64], d[64], du[64], b[64];
+  for (int i = 1; i < nx - 1; ++i)
+    for (int j = 1; j < ny - 1; ++j) {
+      const size_t q = IA(j, i);
+      if (ice[q] == 0) {
+        for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = Ti[IA3(0, j, i)];
+        continue;
+      }
+      if (Hi[q] < 1.0) {
+        for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = fmin(T0_C, Ts[q]);
+        continue;
+      }
+      for (int k = 1; k < nz - 1; ++k) {
+        const size_t p = IA3(k, j, i);
+        double heat = 0.0;
+        if (sheet[q] == 1)
+          heat = ((-GRAV * z[k]) / Cp[p]) *
+                 ((zc.a[k] * u3[IA3(k - 1, j, i)] + zc.b[k] * u3[p] + zc.c[k] * u3[IA3(k + 1, j, i)]) * dHs_dx[q] +
+                  (zc.a[k] * v3[IA3(k - 1, j, i)] + zc.b[k] * v3[p] + zc.c[k] * v3[IA3(k + 1, j, i)]) * dHs_dy[q]);
+        double udx, vdy;
+        if (u3[p] > 0.0) udx = ucx[ICX3(k, j, i - 1)] * (Ti[p] - Ti[IA3(k, j, i - 1)]) / dx;
+        else udx = ucx[ICX3(k, j, i)] * (Ti[IA3(k, j, i + 1)] - Ti[p]) / dx;
+        if (v3[p] > 0.0) vdy = vcy[ICY3(k, j - 1, i)] * (Ti[p] - Ti[IA3(k, j - 1, i)]) / dx;
+        else vdy = vcy[ICY3(k, j, i)] * (Ti[IA3(k, j + 1, i)] - Ti[p]) / dx;
+        const double f1 = (Ki[p] * (zdz[q] * zdz[q])) / (ICE_DENSITY * Cp[p]);
+        const double f2 = zdt[p] + zdx[p] * u3[p] + zdy[p] * v3[p] + zdz[q] * w3[p];
+        const double f3 = heat + (udx + vdy) - Ti[p] / dt;
+        dl[k - 1] = f1 * zc.aa[k] - f2 * zc.a[k];
+        d[k] = f1 * zc.bb[k] - f2 * zc.b[k] - 1.0 / dt;
+        du[k] = f1 * zc.cc[k] - f2 * zc.c[k];
+        b[k] = f3;
+      }
+      d[0] = 1.0; du[0] = 0.0; b[0] = fmin(T0_C, Ts[q]);
+      const size_t pb = IA3(nz - 1, j, i);
+      if (shelf[q] == 1) {
+        dl[nz - 2] = 0.0; d[nz - 1] = 1.0; b[nz - 1] = fmin(T0_C, fmin(Tp[pb], T_ocean));
+      } else if (Ti[pb] >= Tp[pb]) {
+        dl[nz - 2] = 0.0; d[nz - 1] = 1.0; b[nz - 1] = Tp[pb];
+      } else {
+        dl[nz - 2] = 1.0; d[nz - 1] = -1.0;
+        b[nz - 1] = (z[nz - 1] - z[nz - 2]) * (ghf[q] + fh[q]) / (zdz[q] * Ki[pb]);
+      }
+      const int info = orc_tridiagonal_solve(nz, dl, d, du, b);
+      for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = info ? NAN : b[k];
+      for (int k = 0; k < nz - 1; ++k) Tn[IA3(k, j, i)] = fmin(Tn[IA3(k, j, i)], Tp[IA3(k, j, i)]);
+      if (Tn[pb] >= Tp[pb])
+        Tn[pb] = fmin(Tp[pb], Ti[IA3(nz - 2, j, i)] -
+                                  (z[nz - 1] - z[nz - 2]) * (ghf[q] + fh[q]) / (zdz[q] * Ki[pb]));
+      int bad = 0;
+      double mn = INFINITY;
+      for (int k = 0; k < nz; ++k) {
+        const double t = Tn[IA3(k, j, i)];
+        if (t != t) bad = 1;
+        mn = fmin(mn, t);
+      }
+      if (mn < 150.0 || bad) { unstable[q] = 1; ++n_unstable; }
+    }
+  /* Neumann_BC_a_3D, derivatives_and_grids_module.f90:2034-2061: rows, then columns */
+  for (int i = 0; i < nx; ++i)
+    for (int k = 0; k < nz; ++k) {
+      Tn[IA3(k, 0, i)] = Tn[IA3(k, 1, i)];
+      Tn[IA3(k, ny - 1, i)] = Tn[IA3(k, ny - 2, i)];
+    }
+  for (int j = 0; j < ny; ++j)
+    for (int k = 0; k < nz; ++k) {
+      Tn[IA3(k, j, 0)] = Tn[IA3(k, j, 1)];
+      Tn[IA3(k, j, nx - 1)] = Tn[IA3(k, j, nx - 2)];
+    }
+  const int limit = (int)ceil((double)(nx * ny) / 100.0);
+  if (n_unstable >= limit) {
+    free(Tn); free(unstable);
+    return -1;
+  }
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      if (unstable[IA(j, i)]) robin_column(c, Tn, i, j);
+  memcpy(Ti, Tn, sizeof(double) * (size_t)nx * ny * nz);
+  free(Tn); free(unstable);
+  return n_unstable;
+}
+
+/* run_thermo_model, thermodynamics_module.f90:29-121 */
+int orc_run_thermo_model(orc_ctx* c, int32_t do_solve, int32_t* n_unstable) {
+  DECL_DIMS(c);
+  const int32_t *ice = FI(c, MASK_ICE_A), *prev = FI(c, MASK_ICE_A_PREV);
+  const double *u = FD(c, U_VAV_CX), *v = FD(c, V_VAV_CY), *Ts = FD(c, T_SURF_ANNUAL_A);
+  double* Ti = FD(c, TI_A);
+  *n_unstable = 0;
+  /* newly ice-covered columns take the temperature of an upwind ice neighbour (:46-72) */
+  for (int i = 1; i < nx - 1; ++i)
+    for (int j = 1; j < ny - 1; ++j) {
+      if (!(ice[IA(j, i)] == 1 && prev[IA(j, i)] == 0)) continue;
+      int si = -1, sj = -1;
+      if (u[ICX(j, i - 1)] > 0.0 && prev[IA(j, i - 1)] == 1) { si = i - 1; sj = j; }
+      else if (u[ICX(j, i)] < 0.0 && prev[IA(j, i + 1)] == 1) { si = i + 1; sj = j; }
+      else if (v[ICY(j - 1, i)] > 0.0 && prev[IA(j - 1, i)] == 1) { si = i; sj = j - 1; }
+      else if (v[ICY(j, i)] < 0.0 && prev[IA(j + 1, i)] == 1) { si = i; sj = j + 1; }
+      for (int k = 0; k < nz; ++k)
+        Ti[IA3(k, j, i)] = si >= 0 ? Ti[IA3(k, sj, si)] : fmin(Ts[IA(j, i)], T0_C);
+    }
+  /* calc_bottom_frictional_heating (:484-522) */
+  double* fh = FD(c, FRICTIONAL_HEATING_A);
+  const int no_fric = c->c.choice_ice_dynamics == DIVA_DYN_SIA || c->c.choice_sliding_law == DIVA_SLIDING_NONE;
+  if (no_fric) {
+    for (size_t q = 0; q < (size_t)nx * ny; ++q) fh[q] = 0.0;
+  } else {
+    const double *beta = FD(c, BETA_A), *ub = FD(c, U_BASE_A), *vb = FD(c, V_BASE_A);
+    const int32_t* sheet = FI(c, MASK_SHEET_A);
+    for (int i = 1; i < nx - 1; ++i)
+      for (int j = 1; j < ny - 1; ++j) {
+        const size_t q = IA(j, i);
+        fh[q] = sheet[q] == 1 ? beta[q] * (ub[q] * ub[q] + vb[q] * vb[q]) : 0.0;
+      }
+  }
+  /* calc_heat_capacity, calc_thermal_conductivity (:523-608) */
+  double *Cp = FD(c, CPI_A), *Ki = FD(c, KI_A);
+  const size_t n3 = (size_t)nx * ny * nz;
+  for (size_t p = 0; p < n3; ++p) {
+    Cp[p] = c->c.choice_ice_heat_capacity == DIVA_HEATCAP_UNIFORM ? c->c.uniform_ice_heat_capacity
+                                                                   : 2115.3 + 7.79293 * (Ti[p] - T0_C);
+    Ki[p] = c->c.choice_ice_thermal_conductivity == DIVA_CONDUCT_UNIFORM ? c->c.uniform_ice_thermal_conductivity
+                                                                          : 3.101E+08 * exp(-0.0057 * Ti[p]);
+  }
+  orc_calc_pressure_melting_point(c);
+  if (do_solve) {
+    if (!(c->c.dt_thermo > 0.0)) return DIVA_BAD_INPUT;
+    const int nu = solve_3d_heat_equation(c);
+    if (nu < 0) {
+      snprintf(c->err, sizeof(c->err), "heat equation solver unstable for more than 1%% of grid cells");
+      return DIVA_NAN_DETECTED;
+    }
+    *n_unstable = nu;
+  }
+  return orc_calc_ice_rheology(c);
 }
 
 int orc_diva_coefficients(orc_ctx* c) {

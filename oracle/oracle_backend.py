@@ -46,6 +46,8 @@ def oracle_backend():
     lib.orc_vertical_average.argtypes = [dp, C.c_int, dp]
     lib.orc_vertical_average.restype = C.c_double
     lib.orc_vertical_integration_from_bottom_to_zeta.argtypes = [dp, C.c_int, dp, dp]
+    lib.orc_tridiagonal_solve.argtypes = [C.c_int, dp, dp, dp, dp]
+    lib.orc_tridiagonal_solve.restype = C.c_int
     lib.orc_num_threads.restype = C.c_int
     lib.orc_set_threads.argtypes = [C.c_void_p, C.c_int32]
     lib.orc_set_threads.restype = C.c_int
