@@ -9,9 +9,10 @@ exactly as in the reference, and every field operation is a call of the
 context (``pc_predictor``, ``solve_DIVA``, ``pc_corrector``, ``pc_finish``),
 so the geometry stays resident on the device between steps.
 
-Only the ice-dynamics event drives the clock here: thermodynamics, climate,
-SMB/BMB models, GIA, output and calving are outside the velocity path (SMB_a
-and BMB_a are input fields), and the start-up scaling of the linear-solver
+The ice-dynamics event and, with ``thermo=True``, the thermodynamics event
+(run_thermo_model every step, the heat equation every dt_thermo) drive the clock;
+climate, SMB/BMB models, GIA, output and calving are outside the velocity path
+(SMB_a, BMB_a, T_surf_annual_a and GHF_a are input fields), and the start-up scaling of the linear-solver
 tolerances (r_solver_acc, :279-290) has no counterpart because the velocity
 solver takes its tolerances from the configuration.
 """
@@ -22,7 +23,7 @@ class PCTimeStepper:
     478-545 and ice_dynamics_module.f90:987-996 for the initial values)."""
 
     def __init__(self, ctx, start_time, end_time, dt_min=0.01, dt_max=10.0, dt_startup_phase=10.0,
-                 pc_epsilon=0.5, pc_k_I=0.2, pc_k_p=0.2, pc_eta_min=1e-8):
+                 pc_epsilon=0.5, pc_k_I=0.2, pc_k_p=0.2, pc_eta_min=1e-8, thermo=False):
         self.ctx = ctx
         self.start_time, self.end_time = float(start_time), float(end_time)
         self.dt_min, self.dt_max, self.dt_startup_phase = float(dt_min), float(dt_max), float(dt_startup_phase)
@@ -37,6 +38,12 @@ class PCTimeStepper:
         self.pc_eta = pc_epsilon
         self.pc_eta_prev = pc_epsilon
         self.reports = []
+        # the thermodynamics event (IMAU_ICE_main_model.f90:545; dt_thermo of the context)
+        self.thermo = thermo
+        self.dt_thermo = float(ctx.cfg.dt_thermo)
+        self.t_next_thermo = self.start_time + self.dt_thermo
+        self.do_thermo = False
+        self.thermo_solves = 0
 
     def _dt_max_now(self):
         """The start-up / wind-down cap of the time step (ice_dynamics_module.f90:292-299)."""
@@ -70,13 +77,22 @@ class PCTimeStepper:
             self.pc_eta_prev = self.pc_eta
             self.pc_eta = ctx.pc_corrector(self.dt_crit_ice, self.pc_zeta, self.pc_eta_min)
         t_next = min(t_end, self.time + self.dt_max, self.t_next_DIVA)
+        if self.thermo:
+            self.do_thermo = self.time == self.t_next_thermo
+            if self.do_thermo:
+                self.t_next_thermo = self.time + self.dt_thermo
+            t_next = min(t_next, self.t_next_thermo)
         self.dt = t_next - self.time
 
     def step(self, t_end=None):
-        """One model time step: run_ice_dynamics_pc, then the thickness update at the end
-        of the step (update_ice_thickness) and the clock (IMAU_ICE_main_model.f90:117-207)."""
+        """One model time step: run_ice_dynamics_pc, [run_thermo_model, solving the heat
+        equation when its event is due], then the thickness update at the end of the step
+        (update_ice_thickness) and the clock (IMAU_ICE_main_model.f90:117-207)."""
         t_end = self.end_time if t_end is None else t_end
         self.run_ice_dynamics_pc(t_end)
+        if self.thermo:
+            self.ctx.run_thermo_model(self.do_thermo)
+            self.thermo_solves += int(self.do_thermo)
         self.ctx.pc_finish(self.dt)
         self.time = self.time + self.dt
         return self.dt

@@ -75,3 +75,35 @@ def test_slab_cases_match_the_oracle(cuda, oracle, case):
         ctx.close()
     assert n[0] == n[1]
     compare(out[0], out[1])
+
+
+def test_coupled_time_steps_match_the_oracle(cuda, oracle):
+    """Predictor/corrector steps with the thermodynamics event on both sides, each solving
+    its own velocities to the nonlinear rel-res 1e-8: time steps, thickness and
+    temperature agree to that tolerance."""
+    from imau_ice_b200 import dynamics
+    g, cfg, f = synth.marine_channel(dx=20e3)
+    f = dict(f)
+    ny, nx = f["Hi_a"].shape
+    for k, v in (("SMB_a", 0.3), ("BMB_a", 0.0), ("T_surf_annual_a", 243.0), ("GHF_a", 1.7e6)):
+        f[k] = np.asfortranarray(np.full((ny, nx), v))
+    f["mask_ice_a_prev"] = np.ones((ny, nx), dtype=np.int32, order="F")
+    cfg = dict(cfg, lin_rtol=1e-12, picard_stop="relres", picard_relres_tol=1e-8, DIVA_visc_it_nit=500,
+               dt_thermo=0.02, ice_thickness_west_BC="infinite", ice_thickness_east_BC="zero",
+               ice_thickness_south_BC="infinite", ice_thickness_north_BC="infinite")
+    res = []
+    for be in (cuda, oracle):
+        ctx = diva.Context(diva.Grid(**g), cfg, be)
+        if be is oracle:
+            ob.set_linear_solver(ctx, ob.LIN_GMRES_WARM, 1e-12, 0.0)
+        helpers.prepare(ctx, f)
+        ctx.determine_floating_margin_fraction()
+        pc = dynamics.PCTimeStepper(ctx, 0.0, 1000.0, thermo=True)
+        dts = [pc.step() for _ in range(4)]
+        res.append((dts, pc.thermo_solves, ctx.download(["Hi_a", "Ti_a"])))
+        ctx.close()
+    (d0, n0, o0), (d1, n1, o1) = res
+    assert n0 == n1 >= 1
+    np.testing.assert_allclose(d0, d1, rtol=1e-9)
+    assert helpers.rel_l2(o0["Hi_a"], o1["Hi_a"]) <= 1e-5
+    assert helpers.rel_l2(o0["Ti_a"], o1["Ti_a"]) <= 1e-9

@@ -125,3 +125,28 @@ def test_heat_equation_after_a_velocity_solve():
     np.testing.assert_allclose(o["Ki_a"], 3.101e8 * np.exp(-0.0057 * T_before), rtol=1e-14)
     np.testing.assert_allclose(o["Cpi_a"], 2115.3 + 7.79293 * (T_before - T0), rtol=1e-14)
     assert np.abs(o["Ti_a"] - T_before).max() > 1e-3                  # the step changed the temperatures
+
+
+def test_time_steps_with_thermodynamics():
+    """Predictor/corrector steps with the thermodynamics event: the heat equation runs when
+    its clock is due (dt_thermo), the rheology follows the new temperatures."""
+    from imau_ice_b200 import dynamics
+    g, cfg, f = synth.marine_channel(dx=20e3)
+    f = dict(f)
+    ny, nx = f["Hi_a"].shape
+    for k, v in (("SMB_a", 0.3), ("BMB_a", 0.0), ("T_surf_annual_a", 243.0), ("GHF_a", 1.7e6)):
+        f[k] = np.asfortranarray(np.full((ny, nx), v))
+    f["mask_ice_a_prev"] = np.ones((ny, nx), dtype=np.int32, order="F")
+    cfg = dict(cfg, lin_rtol=1e-10, dt_thermo=0.02, ice_thickness_west_BC="infinite", ice_thickness_east_BC="zero",
+               ice_thickness_south_BC="infinite", ice_thickness_north_BC="infinite")
+    ctx = diva.Context(diva.Grid(**g), cfg, ob.oracle_backend())
+    ob.set_linear_solver(ctx, ob.LIN_GMRES_WARM, 1e-10, 0.0)
+    helpers.prepare(ctx, f)
+    ctx.determine_floating_margin_fraction()
+    T0_field = ctx.download(["Ti_a", "A_flow_3D_a"])
+    pc = dynamics.PCTimeStepper(ctx, 0.0, 1000.0, thermo=True)
+    pc.run(max_steps=4)
+    o = ctx.download(["Ti_a", "A_flow_3D_a"])
+    assert pc.thermo_solves >= 1
+    assert np.abs(o["Ti_a"] - T0_field["Ti_a"]).max() > 1e-3
+    assert not np.array_equal(o["A_flow_3D_a"], T0_field["A_flow_3D_a"])
