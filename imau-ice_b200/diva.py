@@ -193,6 +193,31 @@ class Context:
             res[name] = a
         return res
 
+    # ---- restart files ----------------------------------------------------------
+    def save_restart(self, path, names=None):
+        """Write the grid, the configuration and the fields (all by default) to an .npz
+        file: a restart of the whole device state, velocities and viscosity included
+        (the reference's restart file, netcdf_module.f90:31-127, holds the geometry and
+        temperature but not the velocity-solver state)."""
+        arrays = self.download(names)
+        meta = {"_grid": np.array([self.grid.nx, self.grid.ny], dtype=np.int64),
+                "_grid_f": np.array([self.grid.dx, self.grid.xmin, self.grid.ymin]),
+                "_zeta": self.grid.zeta,
+                "_config": np.frombuffer(bytes(self.cfg), dtype=np.uint8)}
+        np.savez(path, **arrays, **meta)
+
+    @classmethod
+    def load_restart(cls, path, backend=None):
+        """A new context with the grid, configuration and fields of a restart file."""
+        z = np.load(path)
+        nx, ny = (int(v) for v in z["_grid"])
+        dx, xmin, ymin = (float(v) for v in z["_grid_f"])
+        grid = Grid(nx, ny, dx, zeta=z["_zeta"], xmin=xmin, ymin=ymin)
+        cfg = _abi.Config.from_buffer_copy(z["_config"].tobytes())
+        ctx = cls(grid, cfg, backend)
+        ctx.upload({k: np.asfortranarray(z[k]) for k in z.files if not k.startswith("_")})
+        return ctx
+
     # ---- the reference's routines ---------------------------------------------
     def update_general_ice_model_data(self):
         self._check(self.backend.fns["update_general_ice_model_data"](self.h), "update_general_ice_model_data")

@@ -274,3 +274,23 @@ def test_mixed_precision_matches_fp64(cuda, case):
     b = np.concatenate([o32["u_vav_cx"].ravel(), o32["v_vav_cy"].ravel()])
     assert helpers.rel_l2(b, a) <= 1e-5
     assert abs(r32["picard_iterations"] - r64["picard_iterations"]) <= 0.1 * r64["picard_iterations"] + 2
+
+
+def test_restart_file_continues_bit_for_bit(cuda, tmp_path):
+    """save_restart / load_restart of a GPU context: the reloaded context's next solve is
+    the original context's, bit for bit."""
+    g, cfg, f = small()
+    ctx = diva.Context(g, cfg, cuda)
+    helpers.prepare(ctx, f)
+    ctx.solve_DIVA()
+    path = tmp_path / "restart.npz"
+    ctx.save_restart(path)
+    ctx2 = diva.Context.load_restart(path, cuda)
+    r1, r2 = ctx.solve_DIVA(), ctx2.solve_DIVA()
+    assert r1["picard_iterations"] == r2["picard_iterations"]
+    a, b = ctx.download(["u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "u_3D_cx"]), ctx2.download(
+        ["u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "u_3D_cx"])
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    ctx.close()
+    ctx2.close()

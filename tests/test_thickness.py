@@ -186,3 +186,28 @@ def test_predictor_corrector_steps_on_the_oracle():
     assert np.all(o["Hi_a"][:, -2:] == 0.0)                        # the 'zero' east edge (two columns, DIVA)
     assert 0.0 < change[2:-2, 2:-2].max() < 50.0                    # a few years of flow inside
     assert pc.pc_eta >= pc.pc_eta_min and np.isfinite(pc.pc_eta)
+
+
+def test_restart_file_continues_the_run(tmp_path):
+    """A restart written after a solve and a time step, read into a new context, continues
+    exactly as the original context does."""
+    g, cfg, f = synth.marine_channel(dx=20e3)
+    f = dict(f)
+    f["SMB_a"] = np.asfortranarray(np.full_like(f["Hi_a"], 0.3))
+    cfg = dict(cfg, lin_rtol=1e-10, ice_thickness_west_BC="infinite", ice_thickness_east_BC="zero",
+               ice_thickness_south_BC="infinite", ice_thickness_north_BC="infinite")
+    ctx = diva.Context(diva.Grid(**g), cfg, ob.oracle_backend())
+    ob.set_linear_solver(ctx, ob.LIN_GMRES_WARM, 1e-10, 0.0)
+    helpers.prepare(ctx, f)
+    ctx.determine_floating_margin_fraction()
+    pc = dynamics.PCTimeStepper(ctx, 0.0, 1000.0)
+    pc.step()
+    path = tmp_path / "restart.npz"
+    ctx.save_restart(path)
+    ctx2 = diva.Context.load_restart(path, ob.oracle_backend())
+    ob.set_linear_solver(ctx2, ob.LIN_GMRES_WARM, 1e-10, 0.0)
+    r1, r2 = ctx.solve_DIVA(), ctx2.solve_DIVA()
+    a, b = ctx.download(), ctx2.download()
+    assert r1["picard_iterations"] == r2["picard_iterations"]
+    for k in a:
+        assert np.array_equal(a[k], b[k], equal_nan=True), k
