@@ -27,6 +27,7 @@ PREC = {"fp64": 0, "mixed": 1}
 HBC = {"zero": 0, "infinite": 1, "periodic": 2, "fixed": 3, "none": 4}
 HEATCAP = {"uniform": 0, "Pounder1965": 1}
 CONDUCT = {"uniform": 0, "Ritz1987": 1}
+INTEGRATION = {"explicit": 0, "semi-implicit": 1, "none": 2}
 
 GRID_KINDS = ["A", "CX", "CY", "B", "A3", "CX3", "CY3", "B3"]
 
@@ -83,6 +84,9 @@ class Config(C.Structure):
         ("choice_ice_thermal_conductivity", C.c_int32),
         ("uniform_ice_thermal_conductivity", C.c_double),
         ("T_ocean_mean_PD_ANT", C.c_double),
+        ("choice_ice_integration_method", C.c_int32),
+        ("dHi_rtol", C.c_double),
+        ("dHi_maxit", C.c_int32),
         ("reserved", C.c_int32 * 8),
     ]
 
@@ -115,6 +119,7 @@ ENUM_OPTIONS = {
     "ice_thickness_west_BC": HBC, "ice_thickness_east_BC": HBC, "ice_thickness_south_BC": HBC,
     "ice_thickness_north_BC": HBC,
     "choice_ice_heat_capacity": HEATCAP, "choice_ice_thermal_conductivity": CONDUCT,
+    "choice_ice_integration_method": INTEGRATION,
 }
 
 

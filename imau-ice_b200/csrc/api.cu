@@ -116,6 +116,7 @@ void config_defaults(diva_config_t* c) {
   c->choice_ice_heat_capacity = DIVA_HEATCAP_POUNDER1965; c->uniform_ice_heat_capacity = 2009.0;
   c->choice_ice_thermal_conductivity = DIVA_CONDUCT_RITZ1987; c->uniform_ice_thermal_conductivity = 6.626958E7;
   c->T_ocean_mean_PD_ANT = -1.7;
+  c->choice_ice_integration_method = DIVA_INTEGRATION_EXPLICIT; c->dHi_rtol = 1E-10; c->dHi_maxit = 1000;
   c->precision = DIVA_PREC_FP64;
 }
 

@@ -11,6 +11,7 @@
 // place in loop order, but a face is rescaled only by its upwind cell and a cell's
 // factor depends only on its own outfluxes, so one launch per stage reproduces it.
 #include <cmath>
+#include <cstdio>
 #include "ctx.hpp"
 
 namespace diva {
@@ -259,6 +260,164 @@ __global__ void k_pc_finish(Dims d, double dt, double* Hi, const double* dH, dou
   Hi[q] = max_ref(0.0, Hn[q]);
 }
 
+// ---- the semi-implicit scheme (calc_dHi_dt_semiimplicit, :302-727) ---------------------
+// Per cell a row of the implicit system: identity (mass-balance-only or explicit cells)
+// or the over-implicit upwind row (fs = 2.5).  The matrix is column diagonally dominant
+// (the 1/dt term), and is solved by BiCGStab with a Jacobi preconditioner.
+struct HSI {
+  double *d, *cw, *ce, *cs, *cn, *b, *x;
+};
+__global__ void k_hsi_rows(Dims dm, double dt, const double* Hi, const double* u, const double* v, const double* smb,
+                           const double* bmb, const double* fmf, const int* ice, const int* shelf, const int* ocean,
+                           const int* cf, HSI h) {
+  IDX2D
+  if (j >= dm.ny || i >= dm.nx) return;
+  const int nx = dm.nx, ny = dm.ny;
+  const double fs = 2.5, dx = dm.dx;
+  const int im1 = i > 0 ? i - 1 : 0, ip1 = i < nx - 1 ? i + 1 : nx - 1;
+  const int jm1 = j > 0 ? j - 1 : 0, jp1 = j < ny - 1 ? j + 1 : ny - 1;
+  const long long q = dm.at(j, i), qw = dm.at(j, im1), qe = dm.at(j, ip1), qs = dm.at(jm1, i), qn = dm.at(jp1, i);
+  int scheme;
+  if (ice[q] == 0 && ice[qw] == 0 && ice[qe] == 0 && ice[qs] == 0 && ice[qn] == 0) scheme = 0;
+  else if (shelf[q] == 1 && ((ocean[qw] == 1 && ice[qw] == 0) || (ocean[qe] == 1 && ice[qe] == 0) ||
+                             (ocean[qs] == 1 && ice[qs] == 0) || (ocean[qn] == 1 && ice[qn] == 0))) scheme = 1;
+  else if (ocean[q] == 1 && ice[q] == 0 && (shelf[qw] == 1 || shelf[qe] == 1 || shelf[qs] == 1 || shelf[qn] == 1))
+    scheme = 1;
+  else scheme = 2;
+  double mb;
+  if (cf[q] == 1 && shelf[q] == 1) mb = (smb[q] + bmb[q]) * fmf[q];
+  else if (ocean[q] == 1 && shelf[q] == 0) mb = 0.0;
+  else mb = smb[q] + bmb[q];
+  bool cut_w = false, cut_e = false, cut_s = false, cut_n = false;
+  if (i > 0) {
+    if (shelf[q] == 1 && ocean[qw] == 1 && ice[qw] == 0) cut_w = fmf[q] < 1.0;
+    else if (shelf[qw] == 1 && ocean[q] == 1 && ice[q] == 0) cut_w = fmf[qw] < 1.0;
+  }
+  if (i < nx - 1) {
+    if (shelf[q] == 1 && ocean[qe] == 1 && ice[qe] == 0) cut_e = fmf[q] < 1.0;
+    else if (shelf[qe] == 1 && ocean[q] == 1 && ice[q] == 0) cut_e = fmf[qe] < 1.0;
+  }
+  if (j > 0) {
+    if (shelf[q] == 1 && ocean[qs] == 1 && ice[qs] == 0) cut_s = fmf[q] < 1.0;
+    else if (shelf[qs] == 1 && ocean[q] == 1 && ice[q] == 0) cut_s = fmf[qs] < 1.0;
+  }
+  if (j < ny - 1) {
+    if (shelf[q] == 1 && ocean[qn] == 1 && ice[qn] == 0) cut_n = fmf[q] < 1.0;
+    else if (shelf[qn] == 1 && ocean[q] == 1 && ice[q] == 0) cut_n = fmf[qn] < 1.0;
+  }
+  double d = 1.0, cw = 0.0, ce = 0.0, cs = 0.0, cn = 0.0, b, x0;
+  if (scheme == 0) {
+    b = max_ref(0.0, Hi[q] + (mb * dt));
+    x0 = b;
+  } else if (scheme == 1) {
+    double Qw = 0.0, Qe = 0.0, Qs = 0.0, Qn = 0.0;
+    if (i > 0) { const double uu = u[dm.at(j, i - 1)]; Qw = uu * (uu > 0.0 ? Hi[qw] : Hi[q]) / dx; }
+    if (i < nx - 1) { const double uu = u[q]; Qe = -uu * (uu > 0.0 ? Hi[q] : Hi[qe]) / dx; }
+    if (j > 0) { const double vv = v[dm.at(j - 1, i)]; Qs = vv * (vv > 0.0 ? Hi[qs] : Hi[q]) / dx; }
+    if (j < ny - 1) { const double vv = v[q]; Qn = -vv * (vv > 0.0 ? Hi[q] : Hi[qn]) / dx; }
+    if (cut_w) Qw = 0.0;
+    if (cut_e) Qe = 0.0;
+    if (cut_s) Qs = 0.0;
+    if (cut_n) Qn = 0.0;
+    b = max_ref(0.0, Hi[q] + dt * (mb + Qw + Qe + Qs + Qn));
+    x0 = b;
+  } else {
+    const double uw = (i > 0 && !cut_w) ? u[dm.at(j, i - 1)] : 0.0, ue = (i < nx - 1 && !cut_e) ? u[q] : 0.0;
+    const double vs = (j > 0 && !cut_s) ? v[dm.at(j - 1, i)] : 0.0, vn = (j < ny - 1 && !cut_n) ? v[q] : 0.0;
+    d = 1.0 / dt;
+    if (i > 0) d = d - (fs / dx) * min_ref(uw, 0.0);
+    if (i < nx - 1) d = d + (fs / dx) * max_ref(ue, 0.0);
+    if (j > 0) d = d - (fs / dx) * min_ref(vs, 0.0);
+    if (j < ny - 1) d = d + (fs / dx) * max_ref(vn, 0.0);
+    if (i > 0) cw = (-fs / dx) * max_ref(uw, 0.0);
+    if (i < nx - 1) ce = (fs / dx) * min_ref(ue, 0.0);
+    if (j > 0) cs = (-fs / dx) * max_ref(vs, 0.0);
+    if (j < ny - 1) cn = (fs / dx) * min_ref(vn, 0.0);
+    double r = mb + Hi[q] / dt;
+    if (i > 0) r = r + Hi[q] * (1.0 - fs) / dx * min_ref(uw, 0.0) + Hi[qw] * (1.0 - fs) / dx * max_ref(uw, 0.0);
+    if (i < nx - 1) r = r - Hi[q] * (1.0 - fs) / dx * max_ref(ue, 0.0) - Hi[qe] * (1.0 - fs) / dx * min_ref(ue, 0.0);
+    if (j > 0) r = r + Hi[q] * (1.0 - fs) / dx * min_ref(vs, 0.0) + Hi[qs] * (1.0 - fs) / dx * max_ref(vs, 0.0);
+    if (j < ny - 1) r = r - Hi[q] * (1.0 - fs) / dx * max_ref(vn, 0.0) - Hi[qn] * (1.0 - fs) / dx * min_ref(vn, 0.0);
+    b = r;
+    x0 = Hi[q];
+  }
+  h.d[q] = d; h.cw[q] = cw; h.ce[q] = ce; h.cs[q] = cs; h.cn[q] = cn; h.b[q] = b; h.x[q] = x0;
+}
+
+__device__ __forceinline__ double hsi_apply(const Dims& dm, const HSI& h, const double* x, int j, int i) {
+  const long long q = dm.at(j, i);
+  double y = h.d[q] * x[q];
+  if (i > 0) y = y + h.cw[q] * x[dm.at(j, i - 1)];
+  if (i < dm.nx - 1) y = y + h.ce[q] * x[dm.at(j, i + 1)];
+  if (j > 0) y = y + h.cs[q] * x[dm.at(j - 1, i)];
+  if (j < dm.ny - 1) y = y + h.cn[q] * x[dm.at(j + 1, i)];
+  return y;
+}
+
+// out = A x (or b - A x when b is given); block partials of (w, out) and (out, out)
+__global__ void k_hsi_op(Dims dm, HSI h, const double* x, const double* b, const double* w, double* out,
+                         double* part) {
+  IDX2D
+  double acc[2] = {0.0, 0.0};
+  if (j < dm.ny && i < dm.nx) {
+    const long long q = dm.at(j, i);
+    double y = hsi_apply(dm, h, x, j, i);
+    if (b) y = b[q] - y;
+    out[q] = y;
+    acc[0] = (w ? w[q] : y) * y;
+    acc[1] = y * y;
+  }
+  block_sum<2>(acc);
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+    part[2 * blk] = acc[0];
+    part[2 * blk + 1] = acc[1];
+  }
+}
+
+// out = a x + c y + e z (null arrays count as zero); optional division by the diagonal;
+// block partials of (w, out) and (out, out)
+__global__ void k_hsi_comb(Dims dm, double a, const double* x, double cc, const double* y, double e, const double* z,
+                           const double* diag, const double* w, double* out, double* part) {
+  IDX2D
+  double acc[2] = {0.0, 0.0};
+  if (j < dm.ny && i < dm.nx) {
+    const long long q = dm.at(j, i);
+    double r = a * x[q];
+    if (y) r = r + cc * y[q];
+    if (z) r = r + e * z[q];
+    if (diag) r = r / diag[q];
+    out[q] = r;
+    acc[0] = (w ? w[q] : r) * r;
+    acc[1] = r * r;
+  }
+  block_sum<2>(acc);
+  if (part && threadIdx.x == 0 && threadIdx.y == 0) {
+    const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+    part[2 * blk] = acc[0];
+    part[2 * blk + 1] = acc[1];
+  }
+}
+
+__global__ void k_hsi_sum(const double* part, int nb, double* out) {
+  if (threadIdx.x != 0) return;
+  double s0 = 0.0, s1 = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    s0 += part[2 * b];
+    s1 += part[2 * b + 1];
+  }
+  out[0] = s0;
+  out[1] = s1;
+}
+
+__global__ void k_hsi_finish(Dims dm, double dt, const double* Hi, const double* x, double* dH, double* Hn) {
+  IDX2D
+  if (j >= dm.ny || i >= dm.nx) return;
+  const long long q = dm.at(j, i);
+  Hn[q] = max_ref(0.0, x[q]);
+  dH[q] = (Hn[q] - Hi[q]) / dt;
+}
+
 }  // namespace
 
 int launch_floating_margin_fraction(Ctx* c) {
@@ -269,8 +428,100 @@ int launch_floating_margin_fraction(Ctx* c) {
   return DIVA_OK;
 }
 
+int launch_thickness_bc(Ctx* c, double dt);
+
+// the two sums of the last reduction, read on the host
+static int hsi_read(Ctx* c, int nb, double* s0, double* s1) {
+  k_hsi_sum<<<1, 32, 0, c->stream>>>(c->partials, nb, c->scal + SC_TMP0); c->launches++;
+  DIVA_CUDA(c, cudaMemcpyAsync(c->h_scal, c->scal + SC_TMP0, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  *s0 = c->h_scal[0];
+  *s1 = c->h_scal[1];
+  return DIVA_OK;
+}
+
+// calc_dHi_dt_semiimplicit: rows, then BiCGStab with a Jacobi preconditioner to dHi_rtol
+static int launch_semiimplicit(Ctx* c, double dt) {
+  const Dims d = c->d;
+  HSI h;
+  h.d = c->kv[KV_X][1]; h.cw = c->kv[KV_B][1]; h.ce = c->kv[KV_R][1]; h.cs = c->kv[KV_RHAT][1];
+  h.cn = c->kv[KV_P][1]; h.b = c->kv[KV_PHAT][1]; h.x = c->kv[KV_V][1];
+  double *r = c->kv[KV_S][1], *rh = c->kv[KV_SHAT][1], *p = c->kv[KV_T][1];
+  double *v = c->kv[KV_X][0], *ph = c->kv[KV_B][0], *s = c->kv[KV_R][0], *sh = c->kv[KV_RHAT][0], *t = c->kv[KV_P][0];
+  const dim3 g = grid2d(d.ny, d.nx);
+  const int nb = g.x * g.y;
+  k_hsi_rows<<<g, block2d(), 0, c->stream>>>(d, dt, c->D(DIVA_F_HI_A), c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY),
+                                             c->D(DIVA_F_SMB_A), c->D(DIVA_F_BMB_A), c->D(DIVA_F_FLOAT_MARGIN_FRAC_A),
+                                             c->I(DIVA_F_MASK_ICE_A), c->I(DIVA_F_MASK_SHELF_A),
+                                             c->I(DIVA_F_MASK_OCEAN_A), c->I(DIVA_F_MASK_CF_A), h); c->launches++;
+  double s0, s1;
+  // ||b||, then r = b - A x0 (copied to rhat and p)
+  k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, h.b, 0.0, nullptr, 0.0, nullptr, nullptr, nullptr, ph,
+                                             c->partials); c->launches++;
+  if (int st = hsi_read(c, nb, &s0, &s1)) return st;
+  const double target = c->c.dHi_rtol * std::sqrt(s1);
+  k_hsi_op<<<g, block2d(), 0, c->stream>>>(d, h, h.x, h.b, nullptr, r, c->partials); c->launches++;
+  if (int st = hsi_read(c, nb, &s0, &s1)) return st;
+  DIVA_CUDA(c, cudaMemcpyAsync(rh, r, sizeof(double) * d.plane, cudaMemcpyDeviceToDevice, c->stream));
+  DIVA_CUDA(c, cudaMemsetAsync(p, 0, sizeof(double) * d.plane, c->stream));
+  DIVA_CUDA(c, cudaMemsetAsync(v, 0, sizeof(double) * d.plane, c->stream));
+  double rnorm = std::sqrt(s1), rho = 1.0, alpha = 1.0, omega = 1.0;
+  int it = 0;
+  while (rnorm > target && it < c->c.dHi_maxit) {
+    ++it;
+    // rho_new = (rhat, r) and p = r + beta (p - omega v); phat = p / diag
+    k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, r, 0.0, nullptr, 0.0, nullptr, nullptr, rh, s, c->partials);
+    c->launches++;
+    if (int st = hsi_read(c, nb, &s0, &s1)) return st;
+    const double rho_new = s0;
+    if (!(std::fabs(rho_new) > 0.0) || !std::isfinite(rho_new)) break;
+    const double beta = (rho_new / rho) * (alpha / omega);
+    k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, r, beta, p, -beta * omega, v, nullptr, nullptr, p, nullptr);
+    k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, p, 0.0, nullptr, 0.0, nullptr, h.d, nullptr, ph, nullptr);
+    k_hsi_op<<<g, block2d(), 0, c->stream>>>(d, h, ph, nullptr, rh, v, c->partials); c->launches += 3;
+    if (int st = hsi_read(c, nb, &s0, &s1)) return st;
+    alpha = rho_new / s0;
+    // s = r - alpha v
+    k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, r, -alpha, v, 0.0, nullptr, nullptr, nullptr, s, c->partials);
+    c->launches++;
+    if (int st = hsi_read(c, nb, &s0, &s1)) return st;
+    if (std::sqrt(s1) <= target) {
+      k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, h.x, alpha, ph, 0.0, nullptr, nullptr, nullptr, h.x, nullptr);
+      c->launches++;
+      rnorm = std::sqrt(s1);
+      break;
+    }
+    k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, s, 0.0, nullptr, 0.0, nullptr, h.d, nullptr, sh, nullptr);
+    k_hsi_op<<<g, block2d(), 0, c->stream>>>(d, h, sh, nullptr, s, t, c->partials); c->launches += 2;
+    if (int st = hsi_read(c, nb, &s0, &s1)) return st;
+    omega = s1 > 0.0 ? s0 / s1 : 0.0;
+    k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, h.x, alpha, ph, omega, sh, nullptr, nullptr, h.x, nullptr);
+    k_hsi_comb<<<g, block2d(), 0, c->stream>>>(d, 1.0, s, -omega, t, 0.0, nullptr, nullptr, nullptr, r, c->partials);
+    c->launches += 2;
+    if (int st = hsi_read(c, nb, &s0, &s1)) return st;
+    rnorm = std::sqrt(s1);
+    rho = rho_new;
+    if (omega == 0.0) break;
+  }
+  DIVA_LAUNCHED(c, "semi-implicit thickness solve");
+  if (!(rnorm <= target))
+    return set_error(c, DIVA_LINEAR_NOT_CONVERGED, "semi-implicit thickness solve did not reach dHi_rtol");
+  k_hsi_finish<<<g, block2d(), 0, c->stream>>>(d, dt, c->D(DIVA_F_HI_A), h.x, c->D(DIVA_F_DHI_DT_A),
+                                               c->D(DIVA_F_HI_TPLUSDT_A)); c->launches++;
+  DIVA_LAUNCHED(c, "k_hsi_finish");
+  return DIVA_OK;
+}
+
 int launch_calc_dHi_dt(Ctx* c, double dt) {
   const Dims d = c->d;
+  if (c->c.choice_ice_integration_method == DIVA_INTEGRATION_SEMIIMPLICIT) {
+    if (int st = launch_semiimplicit(c, dt)) return st;
+    return launch_thickness_bc(c, dt);
+  }
+  if (c->c.choice_ice_integration_method == DIVA_INTEGRATION_NONE) {
+    DIVA_CUDA(c, cudaMemsetAsync(c->D(DIVA_F_DHI_DT_A), 0, sizeof(double) * d.plane, c->stream));
+    return launch_thickness_bc(c, dt);
+  }
   double *Qx = c->D(DIVA_F_QX_CX), *Qy = c->D(DIVA_F_QY_CY);
   double *mb = c->quad[0], *rf = c->quad[1];   // scratch planes (grounded-fraction work space)
   k_fluxes<<<G2T>>>(d, dt, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), c->D(DIVA_F_HI_A), Qx, Qy); c->launches++;
@@ -280,6 +531,12 @@ int launch_calc_dHi_dt(Ctx* c, double dt) {
   k_rescale_faces<<<G2T>>>(d, rf, Qx, Qy); c->launches++;
   k_dhdt<<<G2T>>>(d, dt, c->D(DIVA_F_HI_A), mb, Qx, Qy, c->D(DIVA_F_DHI_DT_A), c->D(DIVA_F_HI_TPLUSDT_A));
   c->launches++;
+  return launch_thickness_bc(c, dt);
+}
+
+// apply_ice_thickness_BC (:728-931)
+int launch_thickness_bc(Ctx* c, double dt) {
+  const Dims d = c->d;
   HBC b;
   b.side[0] = c->c.ice_thickness_west_BC;
   b.side[1] = c->c.ice_thickness_east_BC;

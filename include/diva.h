@@ -81,6 +81,8 @@ typedef enum { DIVA_STOP_RESID_UV = 0, DIVA_STOP_RELRES = 1 } diva_stop_t;
  * MIXED needs the tiled smoother (no periodic side) and a grid of at least 9 points in one
  * direction; otherwise the solve returns DIVA_UNSUPPORTED. */
 typedef enum { DIVA_PREC_FP64 = 0, DIVA_PREC_MIXED = 1 } diva_precision_t;
+typedef enum { DIVA_INTEGRATION_EXPLICIT = 0, DIVA_INTEGRATION_SEMIIMPLICIT = 1,
+               DIVA_INTEGRATION_NONE = 2 } diva_integration_t;
 typedef enum { DIVA_HEATCAP_UNIFORM = 0, DIVA_HEATCAP_POUNDER1965 = 1 } diva_heatcap_t;
 typedef enum { DIVA_CONDUCT_UNIFORM = 0, DIVA_CONDUCT_RITZ1987 = 1 } diva_conductivity_t;
 /* Ice thickness at the domain boundary (apply_ice_thickness_BC, ice_thickness_module.f90:728-931). */
@@ -147,6 +149,12 @@ typedef struct {
   int32_t choice_ice_thermal_conductivity;     /* diva_conductivity_t, default Ritz1987 */
   double  uniform_ice_thermal_conductivity;    /* :430, 6.626958E7 */
   double  T_ocean_mean_PD_ANT;                 /* :647, -1.7 */
+  /* ice-thickness integration (configuration_module.f90:308-314): diva_integration_t, and
+   * for 'semi-implicit' the relative residual and iteration cap of its linear solve
+   * (replacing dHi_SOR_* / dHi_PETSc_*) */
+  int32_t choice_ice_integration_method;
+  double  dHi_rtol;
+  int32_t dHi_maxit;
   int32_t reserved[8];
 } diva_config_t;
 
@@ -223,11 +231,13 @@ int  diva_calc_sia_3d_velocities(diva_ctx_t* ctx);
 /* determine_floating_margin_fraction (general_ice_model_data_module.f90:784-865):
  * float_margin_frac_a and Hi_eff_cf_a of rows 2..ny-1 from Hi_a and the masks. */
 int  diva_determine_floating_margin_fraction(diva_ctx_t* ctx);
-/* calc_dHi_dt with choice_ice_integration_method 'explicit' (ice_thickness_module.f90:
- * 26-300): upwind fluxes Qx_cx/Qy_cy of u_vav, mass balance SMB_a + BMB_a (the floating
- * fraction at calving fronts, none on open ocean), outfluxes rescaled so no cell goes
- * negative, dHi_dt_a and Hi_tplusdt_a = Hi_a + dt dHi_dt_a, then
- * apply_ice_thickness_BC (:728-931; west, east, south, north in that order). */
+/* calc_dHi_dt (ice_thickness_module.f90:26-63) with choice_ice_integration_method
+ * 'explicit' (:65-300: upwind fluxes Qx_cx/Qy_cy of u_vav, mass balance SMB_a + BMB_a with
+ * the floating fraction at calving fronts and none on open ocean, outfluxes rescaled so
+ * no cell goes negative, dHi_dt_a and Hi_tplusdt_a = Hi_a + dt dHi_dt_a), 'semi-implicit'
+ * (:302-727: per cell a mass-balance-only, explicit or over-implicit upwind row, fs = 2.5,
+ * solved to dHi_rtol by BiCGStab with a Jacobi preconditioner) or 'none' (dHi_dt_a = 0),
+ * then apply_ice_thickness_BC (:728-931; west, east, south, north in that order). */
 int  diva_calc_dHi_dt(diva_ctx_t* ctx, double dt);
 /* calc_critical_timestep_adv (ice_dynamics_module.f90:726-762):
  * min(dt_max, 0.9 min over interior a-points of dx / (|u_vav_cx| + |v_vav_cy|)). */

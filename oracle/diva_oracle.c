@@ -2221,6 +2221,7 @@ void orc_config_defaults(diva_config_t* c) {
   c->choice_ice_heat_capacity = DIVA_HEATCAP_POUNDER1965; c->uniform_ice_heat_capacity = 2009.0;
   c->choice_ice_thermal_conductivity = DIVA_CONDUCT_RITZ1987; c->uniform_ice_thermal_conductivity = 6.626958E7;
   c->T_ocean_mean_PD_ANT = -1.7;
+  c->choice_ice_integration_method = DIVA_INTEGRATION_EXPLICIT; c->dHi_rtol = 1E-10; c->dHi_maxit = 1000;
   c->precision = DIVA_PREC_FP64;
 }
 
@@ -2405,8 +2406,153 @@ static void apply_ice_thickness_bc(orc_ctx* c, double dt) {
   }
 }
 
-/* calc_dHi_dt with 'explicit' integration, ice_thickness_module.f90:26-300 */
-static void calc_dHi_dt(orc_ctx* c, double dt) {
+/* The rows of calc_dHi_dt_semiimplicit (ice_thickness_module.f90:302-727) for cell (j,i):
+ * *ident = 1 for a mass-balance-only or explicit row (x = b), else the over-implicit row
+ * diag x + cw x_W + ce x_E + cs x_S + cn x_N = b; *x0 the first guess. */
+static void semiimplicit_row(orc_ctx* c, double dt, int i, int j, int* ident, double* diag, double* cw,
+                             double* ce, double* cs, double* cn, double* b, double* x0) {
+  DECL_DIMS(c);
+  const double fs = 2.5, dx = c->dx;
+  const double *Hi = FD(c, HI_A), *u = FD(c, U_VAV_CX), *v = FD(c, V_VAV_CY);
+  const double *smb = FD(c, SMB_A), *bmb = FD(c, BMB_A), *fmf = FD(c, FLOAT_MARGIN_FRAC_A);
+  const int32_t *ice = FI(c, MASK_ICE_A), *shelf = FI(c, MASK_SHELF_A), *ocean = FI(c, MASK_OCEAN_A);
+  const int32_t* cf = FI(c, MASK_CF_A);
+  const int im1 = i > 0 ? i - 1 : 0, ip1 = i < nx - 1 ? i + 1 : nx - 1;
+  const int jm1 = j > 0 ? j - 1 : 0, jp1 = j < ny - 1 ? j + 1 : ny - 1;
+  const size_t q = IA(j, i), qw = IA(j, im1), qe = IA(j, ip1), qs = IA(jm1, i), qn = IA(jp1, i);
+  int scheme;   /* 0 MB-only, 1 explicit, 2 semi-implicit (:327-347) */
+  if (ice[q] == 0 && ice[qw] == 0 && ice[qe] == 0 && ice[qs] == 0 && ice[qn] == 0) scheme = 0;
+  else if (shelf[q] == 1 && ((ocean[qw] == 1 && ice[qw] == 0) || (ocean[qe] == 1 && ice[qe] == 0) ||
+                             (ocean[qs] == 1 && ice[qs] == 0) || (ocean[qn] == 1 && ice[qn] == 0))) scheme = 1;
+  else if (ocean[q] == 1 && ice[q] == 0 && (shelf[qw] == 1 || shelf[qe] == 1 || shelf[qs] == 1 || shelf[qn] == 1))
+    scheme = 1;
+  else scheme = 2;
+  double mb;
+  if (cf[q] == 1 && shelf[q] == 1) mb = (smb[q] + bmb[q]) * fmf[q];
+  else if (ocean[q] == 1 && shelf[q] == 0) mb = 0.0;
+  else mb = smb[q] + bmb[q];
+  /* a face between a shelf cell and open ocean carries nothing until the shelf cell is
+   * full (float_margin_frac_a < 1), :501-531 and :573-620 */
+  int cut_w = 0, cut_e = 0, cut_s = 0, cut_n = 0;
+  if (i > 0) {
+    if (shelf[q] == 1 && ocean[qw] == 1 && ice[qw] == 0) cut_w = fmf[q] < 1.0;
+    else if (shelf[qw] == 1 && ocean[q] == 1 && ice[q] == 0) cut_w = fmf[qw] < 1.0;
+  }
+  if (i < nx - 1) {
+    if (shelf[q] == 1 && ocean[qe] == 1 && ice[qe] == 0) cut_e = fmf[q] < 1.0;
+    else if (shelf[qe] == 1 && ocean[q] == 1 && ice[q] == 0) cut_e = fmf[qe] < 1.0;
+  }
+  if (j > 0) {
+    if (shelf[q] == 1 && ocean[qs] == 1 && ice[qs] == 0) cut_s = fmf[q] < 1.0;
+    else if (shelf[qs] == 1 && ocean[q] == 1 && ice[q] == 0) cut_s = fmf[qs] < 1.0;
+  }
+  if (j < ny - 1) {
+    if (shelf[q] == 1 && ocean[qn] == 1 && ice[qn] == 0) cut_n = fmf[q] < 1.0;
+    else if (shelf[qn] == 1 && ocean[q] == 1 && ice[q] == 0) cut_n = fmf[qn] < 1.0;
+  }
+  *diag = 1.0; *cw = *ce = *cs = *cn = 0.0;
+  if (scheme == 0) {
+    *ident = 1;
+    *b = fmax(0.0, Hi[q] + (mb * dt));
+    *x0 = *b;
+    return;
+  }
+  if (scheme == 1) {   /* :441-548 */
+    double Qw = 0.0, Qe = 0.0, Qs = 0.0, Qn = 0.0;
+    if (i > 0) { const double uu = u[ICX(j, i - 1)]; Qw = uu * (uu > 0.0 ? Hi[qw] : Hi[q]) / dx; }
+    if (i < nx - 1) { const double uu = u[ICX(j, i)]; Qe = -uu * (uu > 0.0 ? Hi[q] : Hi[qe]) / dx; }
+    if (j > 0) { const double vv = v[ICY(j - 1, i)]; Qs = vv * (vv > 0.0 ? Hi[qs] : Hi[q]) / dx; }
+    if (j < ny - 1) { const double vv = v[ICY(j, i)]; Qn = -vv * (vv > 0.0 ? Hi[q] : Hi[qn]) / dx; }
+    if (cut_w) Qw = 0.0;
+    if (cut_e) Qe = 0.0;
+    if (cut_s) Qs = 0.0;
+    if (cut_n) Qn = 0.0;
+    *ident = 1;
+    *b = fmax(0.0, Hi[q] + dt * (mb + Qw + Qe + Qs + Qn));
+    *x0 = *b;
+    return;
+  }
+  /* :549-727 */
+  const double uw = (i > 0 && !cut_w) ? u[ICX(j, i - 1)] : 0.0, ue = (i < nx - 1 && !cut_e) ? u[ICX(j, i)] : 0.0;
+  const double vs = (j > 0 && !cut_s) ? v[ICY(j - 1, i)] : 0.0, vn = (j < ny - 1 && !cut_n) ? v[ICY(j, i)] : 0.0;
+  double d = 1.0 / dt;
+  if (i > 0) d = d - (fs / dx) * fmin(uw, 0.0);
+  if (i < nx - 1) d = d + (fs / dx) * fmax(ue, 0.0);
+  if (j > 0) d = d - (fs / dx) * fmin(vs, 0.0);
+  if (j < ny - 1) d = d + (fs / dx) * fmax(vn, 0.0);
+  *diag = d;
+  if (i > 0) *cw = (-fs / dx) * fmax(uw, 0.0);
+  if (i < nx - 1) *ce = (fs / dx) * fmin(ue, 0.0);
+  if (j > 0) *cs = (-fs / dx) * fmax(vs, 0.0);
+  if (j < ny - 1) *cn = (fs / dx) * fmin(vn, 0.0);
+  double r = mb + Hi[q] / dt;
+  if (i > 0) r = r + Hi[q] * (1.0 - fs) / dx * fmin(uw, 0.0) + Hi[qw] * (1.0 - fs) / dx * fmax(uw, 0.0);
+  if (i < nx - 1) r = r - Hi[q] * (1.0 - fs) / dx * fmax(ue, 0.0) - Hi[qe] * (1.0 - fs) / dx * fmin(ue, 0.0);
+  if (j > 0) r = r + Hi[q] * (1.0 - fs) / dx * fmin(vs, 0.0) + Hi[qs] * (1.0 - fs) / dx * fmax(vs, 0.0);
+  if (j < ny - 1) r = r - Hi[q] * (1.0 - fs) / dx * fmax(vn, 0.0) - Hi[qn] * (1.0 - fs) / dx * fmin(vn, 0.0);
+  *ident = 0;
+  *b = r;
+  *x0 = Hi[q];
+}
+
+/* calc_dHi_dt_semiimplicit, ice_thickness_module.f90:302-440: the rows above, solved
+ * exactly (banded elimination in the cell order i outer, j inner; the matrix is
+ * column diagonally dominant, so no pivoting is needed) */
+static int calc_dHi_dt_semiimplicit(orc_ctx* c, double dt) {
+  DECL_DIMS(c);
+  const int n = nx * ny, bw = ny;
+  const double* Hi = FD(c, HI_A);
+  double *dH = FD(c, DHI_DT_A), *Hn = FD(c, HI_TPLUSDT_A);
+  const int W = 2 * bw + 1;
+  double* band = (double*)calloc((size_t)n * W, sizeof(double));
+  double* x = (double*)malloc(sizeof(double) * n);
+  if (!band || !x) { free(band); free(x); return DIVA_BAD_INPUT; }
+#define BAND(r, col) band[(size_t)(r) * W + ((col) - (r) + bw)]
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const int r = i * ny + j;
+      int ident;
+      double d, cw, ce, cs, cn, b, x0;
+      semiimplicit_row(c, dt, i, j, &ident, &d, &cw, &ce, &cs, &cn, &b, &x0);
+      BAND(r, r) = ident ? 1.0 : d;
+      if (!ident) {
+        if (i > 0) BAND(r, r - ny) += cw;
+        if (i < nx - 1) BAND(r, r + ny) += ce;
+        if (j > 0) BAND(r, r - 1) += cs;
+        if (j < ny - 1) BAND(r, r + 1) += cn;
+      }
+      x[r] = b;
+    }
+  for (int col = 0; col < n; ++col) {
+    const double p = BAND(col, col);
+    if (p == 0.0) { free(band); free(x); return DIVA_LINEAR_NOT_CONVERGED; }
+    const int last = col + bw < n - 1 ? col + bw : n - 1;
+    for (int r = col + 1; r <= last; ++r) {
+      const double f = BAND(r, col) / p;
+      if (f == 0.0) continue;
+      for (int cc = col; cc <= last; ++cc) BAND(r, cc) -= f * BAND(col, cc);
+      x[r] -= f * x[col];
+    }
+  }
+  for (int r = n - 1; r >= 0; --r) {
+    double s = x[r];
+    const int last = r + bw < n - 1 ? r + bw : n - 1;
+    for (int cc = r + 1; cc <= last; ++cc) s -= BAND(r, cc) * x[cc];
+    x[r] = s / BAND(r, r);
+  }
+#undef BAND
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const size_t q = IA(j, i);
+      Hn[q] = fmax(0.0, x[i * ny + j]);
+      dH[q] = (Hn[q] - Hi[q]) / dt;
+    }
+  free(band); free(x);
+  return DIVA_OK;
+}
+
+/* calc_dHi_dt_explicit, ice_thickness_module.f90:65-300 */
+static void calc_dHi_dt_explicit(orc_ctx* c, double dt) {
   DECL_DIMS(c);
   const double dx = c->dx;
   const double *u = FD(c, U_VAV_CX), *v = FD(c, V_VAV_CY), *Hi = FD(c, HI_A);
@@ -2462,14 +2608,27 @@ static void calc_dHi_dt(orc_ctx* c, double dt) {
       Hn[q] = Hi[q] + d * dt;
     }
   free(mb);
+}
+
+/* calc_dHi_dt, ice_thickness_module.f90:26-63: the integration method, then the boundary conditions */
+static int calc_dHi_dt(orc_ctx* c, double dt) {
+  DECL_DIMS(c);
+  int st = DIVA_OK;
+  if (c->c.choice_ice_integration_method == DIVA_INTEGRATION_SEMIIMPLICIT) st = calc_dHi_dt_semiimplicit(c, dt);
+  else if (c->c.choice_ice_integration_method == DIVA_INTEGRATION_NONE)
+    memset(FD(c, DHI_DT_A), 0, sizeof(double) * (size_t)nx * ny);
+  else calc_dHi_dt_explicit(c, dt);
+  if (st) return st;
   apply_ice_thickness_bc(c, dt);
+  return DIVA_OK;
 }
 
 int orc_determine_floating_margin_fraction(orc_ctx* c) { floating_margin_fraction(c); return DIVA_OK; }
 
 int orc_calc_dHi_dt(orc_ctx* c, double dt) {
   if (!(dt > 0.0)) return DIVA_BAD_INPUT;
-  calc_dHi_dt(c, dt);
+  int st = calc_dHi_dt(c, dt);
+  if (st) return st;
   DECL_DIMS(c);
   if (check_nan(c, FD(c, DHI_DT_A), (size_t)nx * ny)) return DIVA_NAN_DETECTED;
   return DIVA_OK;
@@ -2492,7 +2651,8 @@ int orc_pc_predictor(orc_ctx* c, double dt, double zeta) {
   const size_t n = (size_t)nx * ny;
   if (!(dt > 0.0)) return DIVA_BAD_INPUT;
   memcpy(FD(c, DHIDT_HNM1_UNM1), FD(c, DHIDT_HN_UN), sizeof(double) * n);
-  calc_dHi_dt(c, dt);
+  int st0 = calc_dHi_dt(c, dt);
+  if (st0) return st0;
   memcpy(FD(c, DHIDT_HN_UN), FD(c, DHI_DT_A), sizeof(double) * n);
   double *Hi = FD(c, HI_A), *pred = FD(c, HI_PRED), *old = FD(c, HI_OLD);
   const double *hn = FD(c, DHIDT_HN_UN), *hm = FD(c, DHIDT_HNM1_UNM1);
@@ -2508,7 +2668,8 @@ int orc_pc_corrector(orc_ctx* c, double dt, double zeta, double eta_min, double*
   DECL_DIMS(c);
   const size_t n = (size_t)nx * ny;
   if (!(dt > 0.0)) return DIVA_BAD_INPUT;
-  calc_dHi_dt(c, dt);
+  int st0 = calc_dHi_dt(c, dt);
+  if (st0) return st0;
   memcpy(FD(c, DHIDT_HSTARNP1_UNP1), FD(c, DHI_DT_A), sizeof(double) * n);
   double *Hi = FD(c, HI_A), *old = FD(c, HI_OLD), *corr = FD(c, HI_CORR), *dH = FD(c, DHI_DT_A);
   memcpy(Hi, old, sizeof(double) * n);

@@ -102,3 +102,26 @@ def test_time_steps_against_the_oracle(cuda, oracle):
     assert helpers.rel_l2(o0["Hi_a"], o1["Hi_a"]) <= 1e-5
     assert helpers.rel_l2(np.concatenate([o0["u_vav_cx"].ravel(), o0["v_vav_cy"].ravel()]),
                           np.concatenate([o1["u_vav_cx"].ravel(), o1["v_vav_cy"].ravel()])) <= 1e-5
+
+
+@pytest.mark.parametrize("case", ["grounded", "shelf"])
+def test_semiimplicit_matches_the_oracle(cuda, oracle, case):
+    """The semi-implicit thickness solve: the oracle eliminates exactly, the GPU runs
+    BiCGStab to dHi_rtol = 1e-13; all row types (mass-balance-only, explicit next to the
+    calving front, over-implicit) on the shelf case."""
+    import test_thickness
+    out = []
+    for be in (cuda, oracle):
+        if case == "grounded":
+            ctx, g = test_thickness.grounded_case(be, "semi-implicit")
+        else:
+            ctx = random_case(be, 6, ("none", "none", "none", "none"))
+            ctx.set_config({"choice_ice_integration_method": "semi-implicit", "dHi_rtol": 1e-13,
+                            "choice_ice_dynamics": "DIVA", "ice_thickness_west_BC": "none",
+                            "ice_thickness_east_BC": "none", "ice_thickness_south_BC": "none",
+                            "ice_thickness_north_BC": "none"})
+        ctx.calc_dHi_dt(20.0)
+        out.append(ctx.download(["Hi_tplusdt_a", "dHi_dt_a"]))
+        ctx.close()
+    np.testing.assert_allclose(out[0]["Hi_tplusdt_a"], out[1]["Hi_tplusdt_a"], rtol=1e-10, atol=1e-8)
+    np.testing.assert_allclose(out[0]["dHi_dt_a"], out[1]["dHi_dt_a"], rtol=1e-9, atol=1e-9)

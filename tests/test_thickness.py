@@ -211,3 +211,56 @@ def test_restart_file_continues_the_run(tmp_path):
     assert r1["picard_iterations"] == r2["picard_iterations"]
     for k in a:
         assert np.array_equal(a[k], b[k], equal_nan=True), k
+
+
+def grounded_case(backend, method, seed=7, nx=13, ny=11, dx=10e3):
+    rng = np.random.default_rng(seed)
+    g = diva.Grid(nx, ny, dx)
+    f = {"Hi_a": rng.uniform(500.0, 1500.0, (ny, nx)), "Hb_a": np.full((ny, nx), 200.0), "SL_a": np.zeros((ny, nx)),
+         "Ti_a": np.full((g.nz, ny, nx), 260.0), "SMB_a": rng.uniform(-1.0, 1.0, (ny, nx)),
+         "BMB_a": np.zeros((ny, nx)), "u_vav_cx": rng.uniform(-300.0, 300.0, (ny, nx - 1)),
+         "v_vav_cy": rng.uniform(-300.0, 300.0, (ny - 1, nx))}
+    cfg = {"choice_ice_integration_method": method, "dHi_rtol": 1e-13}
+    for side in ("west", "east", "south", "north"):
+        cfg[f"ice_thickness_{side}_BC"] = "none"
+    ctx = diva.Context(g, cfg, backend)
+    ctx.upload({k: np.asfortranarray(v) for k, v in f.items()})
+    ctx.update_general_ice_model_data()
+    ctx.determine_floating_margin_fraction()
+    return ctx, g
+
+
+def test_semiimplicit_conserves_mass_and_reduces_to_the_mass_balance():
+    ctx, g = grounded_case(ob.oracle_backend(), "semi-implicit")
+    dt = 20.0
+    ctx.calc_dHi_dt(dt)
+    o = ctx.download(["Hi_a", "Hi_tplusdt_a", "SMB_a", "dHi_dt_a"])
+    # every cell is an over-implicit row and the fluxes are conservative across faces
+    assert np.isclose((o["Hi_tplusdt_a"] - o["Hi_a"]).sum(), dt * o["SMB_a"].sum(), rtol=1e-10, atol=1e-6)
+    np.testing.assert_allclose(o["dHi_dt_a"], (o["Hi_tplusdt_a"] - o["Hi_a"]) / dt, rtol=1e-14)
+    # with the ice at rest the row is (1/dt) x = MB + H/dt
+    ctx.upload({"u_vav_cx": np.zeros((g.ny, g.nx - 1)), "v_vav_cy": np.zeros((g.ny - 1, g.nx))})
+    ctx.calc_dHi_dt(dt)
+    o = ctx.download(["Hi_a", "Hi_tplusdt_a", "SMB_a"])
+    np.testing.assert_allclose(o["Hi_tplusdt_a"], o["Hi_a"] + o["SMB_a"] * dt, rtol=1e-13)
+
+
+def test_semiimplicit_approaches_the_explicit_scheme_for_small_steps():
+    out = {}
+    for m in ("explicit", "semi-implicit"):
+        ctx, g = grounded_case(ob.oracle_backend(), m)
+        ctx.calc_dHi_dt(1e-3)
+        out[m] = ctx.download(["dHi_dt_a"])["dHi_dt_a"]
+    np.testing.assert_allclose(out["semi-implicit"], out["explicit"], rtol=1e-3, atol=1e-3)
+
+
+def test_semiimplicit_row_types_on_a_shelf():
+    """Mass-balance-only cells (no ice nearby), explicit cells (shelf next to open ocean and
+    open ocean next to the shelf) and over-implicit cells side by side."""
+    ctx, g = small_case(4, bc="none")
+    ctx.set_config({"choice_ice_integration_method": "semi-implicit", "choice_ice_dynamics": "DIVA",
+                    "ice_thickness_west_BC": "none", "ice_thickness_east_BC": "none",
+                    "ice_thickness_south_BC": "none", "ice_thickness_north_BC": "none"})
+    ctx.calc_dHi_dt(5.0)
+    o = ctx.download(["Hi_tplusdt_a", "dHi_dt_a", "mask_ice_a"])
+    assert np.isfinite(o["Hi_tplusdt_a"]).all() and o["Hi_tplusdt_a"].min() >= 0.0
