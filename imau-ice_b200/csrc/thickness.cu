@@ -260,6 +260,60 @@ __global__ void k_pc_finish(Dims d, double dt, double* Hi, const double* dH, dou
   Hi[q] = max_ref(0.0, Hn[q]);
 }
 
+// ---- remove_unconnected_shelves (:932-1044) -----------------------------------------
+// The reference searches depth-first from the interior shelf cells next to sheet ice
+// through 4-connected shelf cells; the reached set is that connected component, which
+// label propagation gives the same: seeds, then repeated spreading (iterated inside a
+// block over its tile, relaunched until nothing changes), then the removal.
+constexpr int kSX = 32, kSY = 8;
+__global__ void k_shelf_seed(Dims d, const int* shelf, const int* sheet, int* reach) {
+  IDX2D
+  if (j >= d.ny || i >= d.nx) return;
+  const long long q = d.at(j, i);
+  int r = 0;
+  if (j >= 1 && j <= d.ny - 2 && i >= 1 && i <= d.nx - 2 && shelf[q] == 1)
+    r = (sheet[d.at(j, i + 1)] == 1 || sheet[d.at(j, i - 1)] == 1 || sheet[d.at(j + 1, i)] == 1 ||
+         sheet[d.at(j - 1, i)] == 1) ? 1 : 0;
+  reach[q] = r;
+}
+__global__ void k_shelf_spread(Dims d, const int* shelf, int* reach, int* changed) {
+  __shared__ int sr[kSY + 2][kSX + 2];
+  __shared__ int ss[kSY + 2][kSX + 2];
+  const int j0 = blockIdx.x * kSX, i0 = blockIdx.y * kSY;
+  for (int t = threadIdx.y * kSX + threadIdx.x; t < (kSX + 2) * (kSY + 2); t += kSX * kSY) {
+    const int lj = t % (kSX + 2), li = t / (kSX + 2);
+    const int j = j0 + lj - 1, i = i0 + li - 1;
+    const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
+    // a reached cell spreads only if it is shelf itself
+    sr[li][lj] = in ? (reach[d.at(j, i)] && shelf[d.at(j, i)] == 1) : 0;
+    ss[li][lj] = in ? (shelf[d.at(j, i)] == 1) : 0;
+  }
+  __syncthreads();
+  const int lj = threadIdx.x + 1, li = threadIdx.y + 1;
+  const int j = j0 + threadIdx.x, i = i0 + threadIdx.y;
+  const bool mine = j < d.ny && i < d.nx;
+  int any = 0;
+  for (int it = 0; it < kSX * kSY + 4; ++it) {
+    int ch = 0;
+    if (mine && ss[li][lj] && !sr[li][lj] && (sr[li - 1][lj] | sr[li + 1][lj] | sr[li][lj - 1] | sr[li][lj + 1])) ch = 1;
+    __syncthreads();
+    if (ch) sr[li][lj] = 1;
+    any |= ch;
+    if (!__syncthreads_or(ch)) break;
+  }
+  if (mine && any) {
+    reach[d.at(j, i)] = 1;
+    atomicOr(changed, 1);
+  }
+}
+__global__ void k_shelf_remove(Dims d, const int* shelf, const int* reach, const int* noice, double* Hi) {
+  IDX2D
+  if (j >= d.ny || i >= d.nx) return;
+  const long long q = d.at(j, i);
+  if (shelf[q] == 1 && !reach[q]) Hi[q] = 0.0;
+  if (noice[q] == 1) Hi[q] = 0.0;
+}
+
 // ---- the semi-implicit scheme (calc_dHi_dt_semiimplicit, :302-727) ---------------------
 // Per cell a row of the implicit system: identity (mass-balance-only or explicit cells)
 // or the over-implicit upwind row (fs = 2.5).  The matrix is column diagonally dominant
@@ -645,13 +699,32 @@ int diva_pc_corrector(diva_ctx_t* h, double dt, double zeta, double eta_min, dou
 int diva_pc_finish(diva_ctx_t* h, double dt) {
   if (!h || !(dt >= 0.0)) return DIVA_BAD_INPUT;
   Ctx* c = &h->c;
+  const Dims d = c->d;
   // update_ice_thickness keeps the ice mask of the step for the thermodynamics (:446)
-  DIVA_CUDA(c, cudaMemcpyAsync(c->I(DIVA_F_MASK_ICE_A_PREV), c->I(DIVA_F_MASK_ICE_A), sizeof(int) * c->d.plane,
+  DIVA_CUDA(c, cudaMemcpyAsync(c->I(DIVA_F_MASK_ICE_A_PREV), c->I(DIVA_F_MASK_ICE_A), sizeof(int) * d.plane,
                                cudaMemcpyDeviceToDevice, c->stream));
-  k_pc_finish<<<G2T>>>(c->d, dt, c->D(DIVA_F_HI_A), c->D(DIVA_F_DHI_DT_A), c->D(DIVA_F_HI_TPLUSDT_A)); c->launches++;
+  k_pc_finish<<<G2T>>>(d, dt, c->D(DIVA_F_HI_A), c->D(DIVA_F_DHI_DT_A), c->D(DIVA_F_HI_TPLUSDT_A)); c->launches++;
   DIVA_LAUNCHED(c, "k_pc_finish");
   if (int st = launch_update_general_ice_model_data(c)) return st;
   if (int st = launch_floating_margin_fraction(c)) return st;
+  // remove_unconnected_shelves (:932-1044), then the no-ice mask (:586-592)
+  int* reach = c->col_flags;   // per-column scratch
+  const int* shelf = c->I(DIVA_F_MASK_SHELF_A);
+  k_shelf_seed<<<G2T>>>(d, shelf, c->I(DIVA_F_MASK_SHEET_A), reach); c->launches++;
+  const dim3 gs((d.ny + kSX - 1) / kSX, (d.nx + kSY - 1) / kSY), bs(kSX, kSY);
+  for (long long pass = 0;; ++pass) {
+    if (pass > (long long)d.nx * d.ny) return set_error(c, DIVA_TIMEOUT, "remove_unconnected_shelves did not settle");
+    DIVA_CUDA(c, cudaMemsetAsync(c->ff_flag, 0, sizeof(int), c->stream));
+    k_shelf_spread<<<gs, bs, 0, c->stream>>>(d, shelf, reach, c->ff_flag); c->launches++;
+    DIVA_LAUNCHED(c, "k_shelf_spread");
+    int changed = 0;
+    DIVA_CUDA(c, cudaMemcpyAsync(&changed, c->ff_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!changed) break;
+  }
+  k_shelf_remove<<<G2T>>>(d, shelf, reach, c->I(DIVA_F_MASK_NOICE_A), c->D(DIVA_F_HI_A)); c->launches++;
+  DIVA_LAUNCHED(c, "k_shelf_remove");
+  if (int st = launch_update_general_ice_model_data(c)) return st;
   DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
   return DIVA_OK;
 }

@@ -253,9 +253,13 @@ int  diva_pc_predictor(diva_ctx_t* ctx, double dt, double zeta);
  * dHi_dt_a = (Hi_corr - Hi) / dt; pc_tau and *eta = max(eta_min, pc_tau over interior
  * sheet cells with no grounding line in their 3 x 3 neighbourhood). */
 int  diva_pc_corrector(diva_ctx_t* ctx, double dt, double zeta, double eta_min, double* eta);
-/* Hi_tplusdt_a = max(0, Hi_a + dt dHi_dt_a) (:429-431), then (update_ice_thickness,
- * :435-648, without calving, fixed geometries or the no-ice mask) Hi_a = Hi_tplusdt_a,
- * update_general_ice_model_data and determine_floating_margin_fraction. */
+/* Hi_tplusdt_a = max(0, Hi_a + dt dHi_dt_a) (:429-431), then update_ice_thickness
+ * (:435-648) on its default path (choice_calving_law 'none', no fixed geometries, no
+ * shelf removal): mask_ice_a_prev = mask_ice_a; Hi_a = max(0, Hi_tplusdt_a); masks;
+ * determine_floating_margin_fraction; remove_unconnected_shelves (ice_thickness_module.f90:
+ * 932-1044: shelf cells not 4-connected through shelf to a shelf cell next to sheet ice
+ * lose their ice); Hi_a = 0 where mask_noice_a (region%mask_noice); and
+ * update_general_ice_model_data. */
 int  diva_pc_finish(diva_ctx_t* ctx, double dt);
 
 /* run_thermo_model with choice_thermo_model '3D_heat_equation' (thermodynamics_module.f90:

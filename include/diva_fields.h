@@ -150,6 +150,7 @@
   X(DHIDT_HSTARNP1_UNP1,  dHidt_Hstarnp1_unp1,  A,   D)      \
   X(PC_TAU,               pc_tau,               A,   D)      \
   X(MASK_ICE_A_PREV,      mask_ice_a_prev,      A,   I)      \
+  X(MASK_NOICE_A,         mask_noice_a,         A,   I)      \
   /* thermodynamics (thermodynamics_module.f90:29-608,   */ \
   /*  derivatives_and_grids_module.f90:1892-2061);       */ \
   /* T_surf_annual_a is SUM(climate%T2m)/12 and GHF_a    */ \

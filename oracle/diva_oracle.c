@@ -2696,20 +2696,57 @@ int orc_pc_corrector(orc_ctx* c, double dt, double zeta, double eta_min, double*
   return DIVA_OK;
 }
 
-/* Hi_tplusdt_a (:429-431) and the geometry update of update_ice_thickness (:435-648
- * without calving, fixed geometries, shelf removal or the no-ice mask) */
+/* remove_unconnected_shelves, ice_thickness_module.f90:932-1044: a depth-first search
+ * from the interior shelf cells next to sheet ice through 4-connected shelf cells; the
+ * shelf cells it never reaches lose their ice */
+static void remove_unconnected_shelves(orc_ctx* c) {
+  DECL_DIMS(c);
+  const int32_t *shelf = FI(c, MASK_SHELF_A), *sheet = FI(c, MASK_SHEET_A);
+  double* Hi = FD(c, HI_A);
+  unsigned char* map = (unsigned char*)calloc((size_t)nx * ny, 1);
+  int* stack = (int*)malloc(sizeof(int) * 2 * (size_t)nx * ny);
+  size_t top = 0;
+  for (int i = 1; i < nx - 1; ++i)
+    for (int j = 1; j < ny - 1; ++j)
+      if (shelf[IA(j, i)] == 1 && (sheet[IA(j, i + 1)] == 1 || sheet[IA(j, i - 1)] == 1 || sheet[IA(j + 1, i)] == 1 ||
+                                   sheet[IA(j - 1, i)] == 1)) {
+        stack[2 * top] = i; stack[2 * top + 1] = j; ++top;
+        map[IA(j, i)] = 1;
+      }
+  while (top > 0) {
+    --top;
+    const int i = stack[2 * top], j = stack[2 * top + 1];
+    if (shelf[IA(j, i)] != 1) continue;
+    map[IA(j, i)] = 2;
+    const int ni[4] = {i - 1, i + 1, i, i}, nj[4] = {j, j, j - 1, j + 1};
+    for (int k = 0; k < 4; ++k) {
+      if (ni[k] < 0 || ni[k] >= nx || nj[k] < 0 || nj[k] >= ny || map[IA(nj[k], ni[k])] != 0) continue;
+      map[IA(nj[k], ni[k])] = 1;
+      stack[2 * top] = ni[k]; stack[2 * top + 1] = nj[k]; ++top;
+    }
+  }
+  for (size_t q = 0; q < (size_t)nx * ny; ++q)
+    if (shelf[q] == 1 && map[q] == 0) Hi[q] = 0.0;
+  free(map); free(stack);
+}
+
+/* Hi_tplusdt_a (:429-431) and update_ice_thickness (:435-648) on its default path */
 int orc_pc_finish(orc_ctx* c, double dt) {
   DECL_DIMS(c);
   const size_t n = (size_t)nx * ny;
   double *Hi = FD(c, HI_A), *Hn = FD(c, HI_TPLUSDT_A);
   const double* dH = FD(c, DHI_DT_A);
   for (size_t q = 0; q < n; ++q) Hn[q] = fmax(0.0, Hi[q] + dt * dH[q]);
-  memcpy(FI(c, MASK_ICE_A_PREV), FI(c, MASK_ICE_A), sizeof(int32_t) * n);   /* update_ice_thickness :446 */
+  memcpy(FI(c, MASK_ICE_A_PREV), FI(c, MASK_ICE_A), sizeof(int32_t) * n);   /* :446 */
   for (size_t q = 0; q < n; ++q) Hi[q] = fmax(0.0, Hn[q]);
-  int st = orc_update_general_ice_model_data(c);
+  int st = orc_update_general_ice_model_data(c);                            /* the masks of :556-570 */
   if (st) return st;
   floating_margin_fraction(c);
-  return DIVA_OK;
+  remove_unconnected_shelves(c);
+  const int32_t* noice = FI(c, MASK_NOICE_A);
+  for (size_t q = 0; q < n; ++q)
+    if (noice[q] == 1) Hi[q] = 0.0;                                          /* :586-592 */
+  return orc_update_general_ice_model_data(c);
 }
 
 /* ------------------------------------------------------------------------ */

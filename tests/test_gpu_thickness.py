@@ -125,3 +125,15 @@ def test_semiimplicit_matches_the_oracle(cuda, oracle, case):
         ctx.close()
     np.testing.assert_allclose(out[0]["Hi_tplusdt_a"], out[1]["Hi_tplusdt_a"], rtol=1e-10, atol=1e-8)
     np.testing.assert_allclose(out[0]["dHi_dt_a"], out[1]["dHi_dt_a"], rtol=1e-9, atol=1e-9)
+
+
+def test_unconnected_shelves_match_the_oracle(cuda, oracle):
+    import test_thickness
+    out = []
+    for be in (cuda, oracle):
+        ctx, _ = test_thickness.island_case(be)
+        ctx.pc_finish(1.0)
+        out.append(ctx.download(["Hi_a", "mask_ice_a", "mask_shelf_a", "mask_ice_a_prev", "float_margin_frac_a"]))
+        ctx.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k

@@ -264,3 +264,35 @@ def test_semiimplicit_row_types_on_a_shelf():
     ctx.calc_dHi_dt(5.0)
     o = ctx.download(["Hi_tplusdt_a", "dHi_dt_a", "mask_ice_a"])
     assert np.isfinite(o["Hi_tplusdt_a"]).all() and o["Hi_tplusdt_a"].min() >= 0.0
+
+
+def island_case(backend):
+    """Grounded ice in the west, a shelf attached to it, and a floating island (not
+    4-connected to the attached shelf) in the east; a no-ice patch on the grounded part."""
+    ny, nx = 15, 21
+    g = diva.Grid(nx, ny, 10e3)
+    Hb = np.full((ny, nx), -800.0)
+    Hb[:, :6] = 300.0
+    H = np.zeros((ny, nx))
+    H[2:-2, :10] = 400.0                 # sheet (x < 6) and the shelf attached to it
+    H[5:9, 13:17] = 300.0                # the floating island
+    H[6:8, 10:13] = 0.0
+    noice = np.zeros((ny, nx), dtype=np.int32)
+    noice[3, 2] = 1
+    f = {"Hi_a": H, "Hb_a": Hb, "SL_a": np.zeros((ny, nx)), "Ti_a": np.full((g.nz, ny, nx), 260.0),
+         "mask_noice_a": noice}
+    ctx = diva.Context(g, {}, backend)
+    ctx.upload({k: np.asfortranarray(v) for k, v in f.items()})
+    ctx.update_general_ice_model_data()
+    ctx.determine_floating_margin_fraction()
+    return ctx, H
+
+
+def test_unconnected_shelves_and_the_no_ice_mask_lose_their_ice():
+    ctx, H = island_case(ob.oracle_backend())
+    ctx.pc_finish(1.0)                                # dHi_dt_a = 0: only the geometry clean-up acts
+    o = ctx.download(["Hi_a", "mask_ice_a_prev"])
+    assert np.all(o["Hi_a"][5:9, 13:17] == 0.0)     # the island is gone
+    assert np.all(o["Hi_a"][2:-2, 6:10][H[2:-2, 6:10] > 0] == 400.0)   # the attached shelf stays
+    assert o["Hi_a"][3, 2] == 0.0 and o["Hi_a"][4, 2] == 400.0         # the no-ice mask
+    assert o["mask_ice_a_prev"][6, 14] == 1                             # the step's ice mask kept
