@@ -470,6 +470,62 @@ def run_ensemble(args):
     return 0
 
 
+def run_timestep(args):
+    """Time-step workload: the ice cap (321 x 561 x 15) advanced by predictor/corrector
+    steps with DIVA velocities, the explicit thickness update and the 3D heat equation,
+    all resident on the device (host arithmetic only for the step control).  Each step
+    is a warm-started solve from the previous step's state.  Metric: time steps/s,
+    device-synchronised wall clock (the step control reads scalars on the host)."""
+    import numpy as np
+    import torch
+    load_package()
+    from imau_ice_b200 import build, diva, dynamics
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    build.build()
+    g, cfg, fields = workload()
+    cfg = dict(cfg, dt_thermo=0.05)
+    grid = diva.Grid(**g)
+    ctx = diva.Context(grid, cfg)
+    ny, nx = fields["Hi_a"].shape
+    f = dict(fields)
+    f["SMB_a"] = np.asfortranarray(np.full((ny, nx), 0.2))
+    f["T_surf_annual_a"] = np.asfortranarray(np.asarray(fields["Ti_a"])[0])
+    f["GHF_a"] = np.asfortranarray(np.full((ny, nx), 1.7e6))
+    ctx.upload(f)
+    ctx.update_general_ice_model_data()
+    ctx.calc_pressure_melting_point()
+    ctx.calc_ice_rheology()
+    ctx.update_general_ice_model_data()
+    ctx.upload({"mask_ice_a_prev": ctx.download(["mask_ice_a"])["mask_ice_a"]})
+    ctx.determine_floating_margin_fraction()
+    pc = dynamics.PCTimeStepper(ctx, 0.0, 1e5, thermo=True)
+    for _ in range(args.warmup):
+        pc.step()
+    n0, t_model0 = len(pc.reports), pc.time
+    clocks = ClockSampler(0)
+    clocks.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pc.step()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    clk = clocks.stop()
+    its = [r["picard_iterations"] for r in pc.reports[n0:]]
+    print(json.dumps({
+        "metric": "ice-dynamics time steps/s at 321x561x15 (PC + DIVA + thickness + heat equation)",
+        "value": args.steps / dt, "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded ice cap, SMB 0.2 m/yr, GHF 1.7e6 J/m2/yr)",
+        "config": {"workload": "predictor/corrector time steps of the synthetic ice cap 1600x2800 km @5 km",
+                   "viscosity_iterations_per_solve": its, "model_years": pc.time - t_model0,
+                   "thermo_solves": pc.thermo_solves,
+                   "timing": "device-synchronised wall clock around the host-controlled steps"},
+        "clocks": clk}))
+    ctx.close()
+    return 0
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--gpus", type=int, default=1)
@@ -479,8 +535,9 @@ def main():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true",
                    help="timed solves only (no roofline, e2e or CPU legs): the command profiled with ncu")
-    p.add_argument("--workload", choices=["icecap", "ensemble"], default="icecap",
-                   help="icecap: the headline solve (default); ensemble: --members perturbed members")
+    p.add_argument("--workload", choices=["icecap", "ensemble", "timestep"], default="icecap",
+                   help="icecap: the headline solve (default); ensemble: --members perturbed members; "
+                        "timestep: predictor/corrector steps with thickness and heat equation")
     p.add_argument("--members", type=int, default=64)
     p.add_argument("--ensemble-sizes", default="channel,icecap",
                    help="member kinds drawn from: channel (129x17), icecap (321x561), sheet (1501x1501)")
@@ -489,6 +546,8 @@ def main():
     args = p.parse_args()
     if args.impl == "b200" and args.workload == "ensemble":
         return run_ensemble(args)
+    if args.impl == "b200" and args.workload == "timestep":
+        return run_timestep(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)
