@@ -44,7 +44,7 @@ CASES = {
     "icecap_40km": (2, 40e3, {"lin_rtol": 1e-12}),
     "channel_5km_relres": (1, None, {"picard_stop": "relres", "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 300,
                                      "lin_rtol": 1e-12}),
-    # SURVEY config 3: FP32 finest-level smoother inside the FP64 Krylov solve, against the FP64 oracle
+    # precision 'mixed': FP32 finest-level smoother inside the FP64 Krylov solve, against the FP64 oracle
     "channel_5km_mixed": (1, None, {"lin_rtol": 1e-12, "precision": "mixed"}),
     # calving fronts with the 'BC' margin rows (stress boundary condition, shelf-next-to-land identities)
     "channel_front_BC_relres": (1, None, {"choice_ice_margin": "BC", "picard_stop": "relres",
