@@ -18,9 +18,9 @@ import time
 
 from . import diva
 
-# device bytes of one context per grid column (nz = 15, every 2D/3D field and
-# solver level resident): measured 14 GB for 1501 x 1501
-BYTES_PER_COLUMN = 6.5e3
+# device bytes of one context per grid column (nz = 15: the 127 fields, the solver's
+# work space and the state snapshot taken before each solve), ~18 GB at 1501 x 1501
+BYTES_PER_COLUMN = 8.5e3
 # viscosity iterations to rel-res 1e-6 observed per member kind (the cost model's
 # second factor; only the ratios matter)
 EXPECTED_ITERATIONS = {"channel": 90, "icecap": 80, "sheet": 400}
