@@ -87,6 +87,9 @@ class Config(C.Structure):
         ("choice_ice_integration_method", C.c_int32),
         ("dHi_rtol", C.c_double),
         ("dHi_maxit", C.c_int32),
+        ("fixed_shelf_geometry", C.c_int32), ("fixed_sheet_geometry", C.c_int32),
+        ("fixed_grounding_line", C.c_int32), ("do_remove_shelves", C.c_int32),
+        ("ocean_temperature_input", C.c_int32),
         ("reserved", C.c_int32 * 8),
     ]
 

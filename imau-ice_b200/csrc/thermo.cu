@@ -24,7 +24,9 @@ constexpr double kSecPerYear = 31556943.36;   // parameters_module.f90:12
 struct ThermoArgs {
   Dims d;
   Zeta zt;
-  double dt, T_ocean;
+  double dt, T_ocean;        // the shelf-base ocean temperature with ocean model 'none'
+  int ocean_input;           // 1: T_ocean_base_a (deg C) instead
+  const double* To_in;
   int heatcap, conduct;
   double cp_uniform, k_uniform;
   int no_friction;
@@ -167,9 +169,10 @@ __global__ void k_heat_columns(ThermoArgs a) {
   const long long pb = (long long)(nz - 1) * P + q;
   const double bed = (z[nz - 1] - z[nz - 2]) * (a.ghf[q] + a.fh[q]) / (zdz * a.Ki[pb]);
   if (a.shelf[q] == 1) {
+    const double To = a.ocean_input ? a.To_in[q] + kT0 : a.T_ocean;
     dl[nz - 2] = 0.0;
     dg[nz - 1] = 1.0;
-    b[nz - 1] = min_ref(kT0, min_ref(a.Tp[pb], a.T_ocean));
+    b[nz - 1] = min_ref(kT0, min_ref(a.Tp[pb], To));
   } else if (a.Ti[pb] >= a.Tp[pb]) {
     dl[nz - 2] = 0.0;
     dg[nz - 1] = 1.0;
@@ -245,7 +248,10 @@ __global__ void k_robin(ThermoArgs a) {
       for (int k = 0; k < d.nz; ++k) a.Tn[k * P + q] = Ts + ((kT0 - kCC * Hi) - Ts) * z[k];
     }
   } else if (a.shelf[q] == 1) {
-    for (int k = 0; k < d.nz; ++k) a.Tn[k * P + q] = Ts + z[k] * (kT0 + a.T_ocean - Ts);
+    // the Robin profile adds T0 to its ocean temperature, which with ocean model 'none' is
+    // already T0 + T_ocean_mean_PD_ANT (:455-465, as written)
+    const double To = a.ocean_input ? a.To_in[q] : a.T_ocean;
+    for (int k = 0; k < d.nz; ++k) a.Tn[k * P + q] = Ts + z[k] * (kT0 + To - Ts);
   } else {
     for (int k = 0; k < d.nz; ++k) a.Tn[k * P + q] = Ts;
   }
@@ -269,6 +275,8 @@ extern "C" int diva_run_thermo_model(diva_ctx_t* h, int32_t do_solve, int32_t* n
   a.zt = c->zt;
   a.dt = c->c.dt_thermo;
   a.T_ocean = kT0 + c->c.T_ocean_mean_PD_ANT;
+  a.ocean_input = c->c.ocean_temperature_input;
+  a.To_in = c->D(DIVA_F_T_OCEAN_BASE_A);
   a.heatcap = c->c.choice_ice_heat_capacity;
   a.conduct = c->c.choice_ice_thermal_conductivity;
   a.cp_uniform = c->c.uniform_ice_heat_capacity;

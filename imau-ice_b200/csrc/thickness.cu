@@ -252,12 +252,32 @@ __global__ void k_pc_tau(Dims d, double dt, double zeta, double eta_min, const d
   block_extreme(e, 1, &part[blockIdx.y * gridDim.x + blockIdx.x]);
 }
 
-__global__ void k_pc_finish(Dims d, double dt, double* Hi, const double* dH, double* Hn) {
+// Hi_tplusdt_a, the fixed-geometry options of update_ice_thickness (:449-540: a cell keeps
+// its thickness when it is shelf / sheet / grounding line by the 3 x 3 mask test), then
+// Hi_a = max(0, Hi_tplusdt_a)
+struct FixFlags {
+  int shelf, sheet, gl;
+};
+__global__ void k_pc_finish(Dims d, double dt, double* Hi, const double* dH, double* Hn, FixFlags fx,
+                            const int* shelf, const int* sheet) {
   IDX2D
   if (j >= d.ny || i >= d.nx) return;
   const long long q = d.at(j, i);
-  Hn[q] = max_ref(0.0, Hi[q] + dt * dH[q]);
-  Hi[q] = max_ref(0.0, Hn[q]);
+  double hn = max_ref(0.0, Hi[q] + dt * dH[q]);
+  if (fx.shelf | fx.sheet | fx.gl) {
+    bool nb_shelf = false, nb_sheet = false;
+    for (int ii = (i > 0 ? i - 1 : 0); ii <= (i < d.nx - 1 ? i + 1 : d.nx - 1); ++ii)
+      for (int jj = (j > 0 ? j - 1 : 0); jj <= (j < d.ny - 1 ? j + 1 : d.ny - 1); ++jj) {
+        nb_shelf = nb_shelf || shelf[d.at(jj, ii)] == 1;
+        nb_sheet = nb_sheet || sheet[d.at(jj, ii)] == 1;
+      }
+    const bool sh = shelf[q] == 1, sg = sheet[q] == 1;
+    if (fx.shelf && (sh || (sg && nb_shelf))) hn = Hi[q];
+    if (fx.sheet && (sg || (sh && nb_sheet))) hn = Hi[q];
+    if (fx.gl && ((sg && nb_shelf) || (sh && nb_sheet))) hn = Hi[q];
+  }
+  Hn[q] = hn;
+  Hi[q] = max_ref(0.0, hn);
 }
 
 // ---- remove_unconnected_shelves (:932-1044) -----------------------------------------
@@ -306,12 +326,15 @@ __global__ void k_shelf_spread(Dims d, const int* shelf, int* reach, int* change
     atomicOr(changed, 1);
   }
 }
-__global__ void k_shelf_remove(Dims d, const int* shelf, const int* reach, const int* noice, double* Hi) {
+// then the no-ice mask (:586-592) and, with do_remove_shelves, all floating ice (:600-608)
+__global__ void k_shelf_remove(Dims d, const int* shelf, const int* reach, const int* noice, int remove_floating,
+                               const double* Hb, const double* SL, double* Hi) {
   IDX2D
   if (j >= d.ny || i >= d.nx) return;
   const long long q = d.at(j, i);
   if (shelf[q] == 1 && !reach[q]) Hi[q] = 0.0;
   if (noice[q] == 1) Hi[q] = 0.0;
+  if (remove_floating && Hi[q] < (SL[q] - Hb[q]) * kRhoSW / kRhoI) Hi[q] = 0.0;
 }
 
 // ---- the semi-implicit scheme (calc_dHi_dt_semiimplicit, :302-727) ---------------------
@@ -703,7 +726,9 @@ int diva_pc_finish(diva_ctx_t* h, double dt) {
   // update_ice_thickness keeps the ice mask of the step for the thermodynamics (:446)
   DIVA_CUDA(c, cudaMemcpyAsync(c->I(DIVA_F_MASK_ICE_A_PREV), c->I(DIVA_F_MASK_ICE_A), sizeof(int) * d.plane,
                                cudaMemcpyDeviceToDevice, c->stream));
-  k_pc_finish<<<G2T>>>(d, dt, c->D(DIVA_F_HI_A), c->D(DIVA_F_DHI_DT_A), c->D(DIVA_F_HI_TPLUSDT_A)); c->launches++;
+  const FixFlags fx{c->c.fixed_shelf_geometry, c->c.fixed_sheet_geometry, c->c.fixed_grounding_line};
+  k_pc_finish<<<G2T>>>(d, dt, c->D(DIVA_F_HI_A), c->D(DIVA_F_DHI_DT_A), c->D(DIVA_F_HI_TPLUSDT_A), fx,
+                       c->I(DIVA_F_MASK_SHELF_A), c->I(DIVA_F_MASK_SHEET_A)); c->launches++;
   DIVA_LAUNCHED(c, "k_pc_finish");
   if (int st = launch_update_general_ice_model_data(c)) return st;
   if (int st = launch_floating_margin_fraction(c)) return st;
@@ -722,7 +747,8 @@ int diva_pc_finish(diva_ctx_t* h, double dt) {
     DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
     if (!changed) break;
   }
-  k_shelf_remove<<<G2T>>>(d, shelf, reach, c->I(DIVA_F_MASK_NOICE_A), c->D(DIVA_F_HI_A)); c->launches++;
+  k_shelf_remove<<<G2T>>>(d, shelf, reach, c->I(DIVA_F_MASK_NOICE_A), c->c.do_remove_shelves, c->D(DIVA_F_HB_A),
+                          c->D(DIVA_F_SL_A), c->D(DIVA_F_HI_A)); c->launches++;
   DIVA_LAUNCHED(c, "k_shelf_remove");
   if (int st = launch_update_general_ice_model_data(c)) return st;
   DIVA_CUDA(c, cudaStreamSynchronize(c->stream));

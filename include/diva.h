@@ -155,6 +155,12 @@ typedef struct {
   int32_t choice_ice_integration_method;
   double  dHi_rtol;
   int32_t dHi_maxit;
+  /* update_ice_thickness options (configuration_module.f90:335-337, 414), default off */
+  int32_t fixed_shelf_geometry, fixed_sheet_geometry, fixed_grounding_line, do_remove_shelves;
+  /* 1: the heat equation takes the ocean temperature at the shelf base (deg C, what
+   * interpolate_ocean_depth gives an ocean model) from T_ocean_base_a; 0: ocean model
+   * 'none', T_ocean_mean_PD_ANT everywhere */
+  int32_t ocean_temperature_input;
   int32_t reserved[8];
 } diva_config_t;
 
@@ -255,11 +261,13 @@ int  diva_pc_predictor(diva_ctx_t* ctx, double dt, double zeta);
 int  diva_pc_corrector(diva_ctx_t* ctx, double dt, double zeta, double eta_min, double* eta);
 /* Hi_tplusdt_a = max(0, Hi_a + dt dHi_dt_a) (:429-431), then update_ice_thickness
  * (:435-648) on its default path (choice_calving_law 'none', no fixed geometries, no
- * shelf removal): mask_ice_a_prev = mask_ice_a; Hi_a = max(0, Hi_tplusdt_a); masks;
+ * shelf removal flags unless set): mask_ice_a_prev = mask_ice_a; [fixed_shelf_geometry,
+ * fixed_sheet_geometry, fixed_grounding_line keep Hi_tplusdt_a = Hi_a on shelf / sheet /
+ * grounding-line cells]; Hi_a = max(0, Hi_tplusdt_a); masks;
  * determine_floating_margin_fraction; remove_unconnected_shelves (ice_thickness_module.f90:
  * 932-1044: shelf cells not 4-connected through shelf to a shelf cell next to sheet ice
- * lose their ice); Hi_a = 0 where mask_noice_a (region%mask_noice); and
- * update_general_ice_model_data. */
+ * lose their ice); Hi_a = 0 where mask_noice_a (region%mask_noice); [do_remove_shelves:
+ * Hi_a = 0 on floating cells]; and update_general_ice_model_data. */
 int  diva_pc_finish(diva_ctx_t* ctx, double dt);
 
 /* run_thermo_model with choice_thermo_model '3D_heat_equation' (thermodynamics_module.f90:

@@ -157,6 +157,7 @@
   /* ice%GHF_a (J m-2 yr-1)                              */ \
   X(T_SURF_ANNUAL_A,      T_surf_annual_a,      A,   D)      \
   X(GHF_A,                GHF_a,                A,   D)      \
+  X(T_OCEAN_BASE_A,       T_ocean_base_a,       A,   D)      \
   X(FRICTIONAL_HEATING_A, frictional_heating_a, A,   D)      \
   X(CPI_A,                Cpi_a,                A3,  D)      \
   X(KI_A,                 Ki_a,                 A3,  D)      \

@@ -2738,6 +2738,27 @@ int orc_pc_finish(orc_ctx* c, double dt) {
   const double* dH = FD(c, DHI_DT_A);
   for (size_t q = 0; q < n; ++q) Hn[q] = fmax(0.0, Hi[q] + dt * dH[q]);
   memcpy(FI(c, MASK_ICE_A_PREV), FI(c, MASK_ICE_A), sizeof(int32_t) * n);   /* :446 */
+  /* fixed shelf / sheet / grounding-line geometry, :449-540 */
+  const int32_t *shelf = FI(c, MASK_SHELF_A), *sheet = FI(c, MASK_SHEET_A);
+  const int fix[3] = {c->c.fixed_shelf_geometry, c->c.fixed_sheet_geometry, c->c.fixed_grounding_line};
+  for (int f = 0; f < 3; ++f) {
+    if (!fix[f]) continue;
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) {
+        const size_t q = IA(j, i);
+        int nb_shelf = 0, nb_sheet = 0;
+        for (int ii = (i > 0 ? i - 1 : 0); ii <= (i < nx - 1 ? i + 1 : nx - 1); ++ii)
+          for (int jj = (j > 0 ? j - 1 : 0); jj <= (j < ny - 1 ? j + 1 : ny - 1); ++jj) {
+            nb_shelf |= shelf[IA(jj, ii)] == 1;
+            nb_sheet |= sheet[IA(jj, ii)] == 1;
+          }
+        int keep;
+        if (f == 0) keep = shelf[q] == 1 || (sheet[q] == 1 && nb_shelf);
+        else if (f == 1) keep = sheet[q] == 1 || (shelf[q] == 1 && nb_sheet);
+        else keep = (sheet[q] == 1 && nb_shelf) || (shelf[q] == 1 && nb_sheet);
+        if (keep) Hn[q] = Hi[q];
+      }
+  }
   for (size_t q = 0; q < n; ++q) Hi[q] = fmax(0.0, Hn[q]);
   int st = orc_update_general_ice_model_data(c);                            /* the masks of :556-570 */
   if (st) return st;
@@ -2746,6 +2767,11 @@ int orc_pc_finish(orc_ctx* c, double dt) {
   const int32_t* noice = FI(c, MASK_NOICE_A);
   for (size_t q = 0; q < n; ++q)
     if (noice[q] == 1) Hi[q] = 0.0;                                          /* :586-592 */
+  if (c->c.do_remove_shelves) {                                              /* :600-608 */
+    const double *Hb = FD(c, HB_A), *SL = FD(c, SL_A);
+    for (size_t q = 0; q < n; ++q)
+      if (is_floating(Hi[q], Hb[q], SL[q])) Hi[q] = 0.0;
+  }
   return orc_update_general_ice_model_data(c);
 }
 
@@ -2824,7 +2850,9 @@ static void robin_column(orc_ctx* c, double* Tn, int i, int j) {
       for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = Ts + ((T0_C - CC_C * Hi) - Ts) * z[k];
     }
   } else if (FI(c, MASK_SHELF_A)[q] == 1) {
-    const double To = T0_C + c->c.T_ocean_mean_PD_ANT;
+    /* the Robin profile adds T0 to its ocean temperature, which with ocean model 'none' is
+     * already T0 + T_ocean_mean_PD_ANT (:455-465, as written) */
+    const double To = c->c.ocean_temperature_input ? FD(c, T_OCEAN_BASE_A)[q] : T0_C + c->c.T_ocean_mean_PD_ANT;
     for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = Ts + z[k] * (T0_C + To - Ts);
   } else {
     for (int k = 0; k < nz; ++k) Tn[IA3(k, j, i)] = Ts;
@@ -2864,7 +2892,7 @@ static int solve_3d_heat_equation(orc_ctx* c) {
       }
     }
   for (size_t q = 0; q < (size_t)nx * ny; ++q) Ti[q * nz] = fmin(T0_C, Ts[q]);   /* layer 1 */
-  const double T_ocean = T0_C + c->c.T_ocean_mean_PD_ANT;
+  const double* To_in = FD(c, T_OCEAN_BASE_A);   /* ocean_temperature_input: T0 added as at :209 */
   struct zeta_coef zc;
   zeta_coefficients(z, nz, &zc);
   double* Tn = (double*)calloc((size_t)nx * ny * nz, sizeof(double));
@@ -2905,6 +2933,7 @@ static int solve_3d_heat_equation(orc_ctx* c) {
       d[0] = 1.0; du[0] = 0.0; b[0] = fmin(T0_C, Ts[q]);
       const size_t pb = IA3(nz - 1, j, i);
       if (shelf[q] == 1) {
+        const double T_ocean = c->c.ocean_temperature_input ? To_in[q] + T0_C : T0_C + c->c.T_ocean_mean_PD_ANT;
         dl[nz - 2] = 0.0; d[nz - 1] = 1.0; b[nz - 1] = fmin(T0_C, fmin(Tp[pb], T_ocean));
       } else if (Ti[pb] >= Tp[pb]) {
         dl[nz - 2] = 0.0; d[nz - 1] = 1.0; b[nz - 1] = Tp[pb];

@@ -51,7 +51,7 @@ def test_heat_equation_after_a_solve_matches_the_oracle(cuda, oracle):
     compare(og, oo)
 
 
-@pytest.mark.parametrize("case", ["steady", "robin", "new_ice"])
+@pytest.mark.parametrize("case", ["steady", "robin", "new_ice", "shelf_ocean_input"])
 def test_slab_cases_match_the_oracle(cuda, oracle, case):
     g, f = test_thermo.slab()
     cfg = {"choice_ice_heat_capacity": "uniform", "choice_ice_thermal_conductivity": "uniform",
@@ -63,6 +63,11 @@ def test_slab_cases_match_the_oracle(cuda, oracle, case):
         f["mask_ice_a_prev"][4, 5] = 0
         f["Ti_a"][:, 4, 4] = np.linspace(250.0, 260.0, g.nz)
         cfg.update(choice_ice_heat_capacity="Pounder1965", choice_ice_thermal_conductivity="Ritz1987")
+    if case == "shelf_ocean_input":                   # a floating slab, the shelf-base temperature
+        f["Hb_a"] = np.full(f["Hi_a"].shape, -3000.0)  # from T_ocean_base_a, one Robin column on it
+        f["T_ocean_base_a"] = np.random.default_rng(7).uniform(-3.0, -2.0, f["Hi_a"].shape)
+        f["T_surf_annual_a"][7, 8] = 100.0
+        cfg.update(ocean_temperature_input=1)
     out, n = [], []
     for be in (cuda, oracle):
         ctx = diva.Context(g, cfg, be)

@@ -137,3 +137,12 @@ def test_unconnected_shelves_match_the_oracle(cuda, oracle):
         ctx.close()
     for k in out[0]:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("flag", ["fixed_shelf_geometry", "fixed_sheet_geometry", "fixed_grounding_line",
+                                  "do_remove_shelves"])
+def test_update_ice_thickness_options_bit_exact(cuda, oracle, flag):
+    import test_thickness
+    out = [test_thickness.options_case(be, flag)[1] for be in (cuda, oracle)]
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k

@@ -150,3 +150,21 @@ def test_time_steps_with_thermodynamics():
     assert pc.thermo_solves >= 1
     assert np.abs(o["Ti_a"] - T0_field["Ti_a"]).max() > 1e-3
     assert not np.array_equal(o["A_flow_3D_a"], T0_field["A_flow_3D_a"])
+
+
+def test_shelf_base_takes_the_ocean_input():
+    """ocean_temperature_input: the shelf-base temperature is T0 + T_ocean_base_a instead of
+    T0 + T_ocean_mean_PD_ANT (thermodynamics_module.f90:189-218, :296-300). Both stay below
+    the pressure melting point of the 2000 m slab (T0 - 1.74), which would otherwise take
+    the base to the basal-gradient value (:323-326)."""
+    g, f = slab()
+    f["Hb_a"] = np.full(f["Hi_a"].shape, -3000.0)         # a floating slab
+    f["T_ocean_base_a"] = np.full(f["Hi_a"].shape, -2.5)
+    base = {}
+    for flag in (0, 1):
+        ctx = thermo_ctx(g, f, ocean_temperature_input=flag, T_ocean_mean_PD_ANT=-3.0)
+        assert ctx.run_thermo_model(True) == 0
+        o = ctx.download(["Ti_a", "mask_shelf_a"])
+        assert o["mask_shelf_a"][10, 10] == 1
+        base[flag] = o["Ti_a"][-1, 10, 10]
+    assert base[0] == T0 - 3.0 and base[1] == -2.5 + T0

@@ -296,3 +296,47 @@ def test_unconnected_shelves_and_the_no_ice_mask_lose_their_ice():
     assert np.all(o["Hi_a"][2:-2, 6:10][H[2:-2, 6:10] > 0] == 400.0)   # the attached shelf stays
     assert o["Hi_a"][3, 2] == 0.0 and o["Hi_a"][4, 2] == 400.0         # the no-ice mask
     assert o["mask_ice_a_prev"][6, 14] == 1                             # the step's ice mask kept
+
+
+OPTIONS = ["fixed_shelf_geometry", "fixed_sheet_geometry", "fixed_grounding_line", "do_remove_shelves"]
+
+
+def options_case(backend, flag):
+    """The island case with dHi_dt_a = 1 m/yr everywhere and one option of
+    update_ice_thickness (ice_dynamics_module.f90:449-608) switched on; returns the
+    masks and thickness before pc_finish(1.0) and the thickness after it."""
+    ctx, H = island_case(backend)
+    ctx.set_config({flag: 1})
+    g = ctx.grid
+    ctx.upload({"dHi_dt_a": np.ones((g.ny, g.nx))})
+    before = ctx.download(["mask_shelf_a", "mask_sheet_a", "Hi_a"])
+    ctx.pc_finish(1.0)
+    after = ctx.download(["Hi_a", "mask_ice_a", "mask_shelf_a", "mask_sheet_a", "mask_gl_a",
+                          "float_margin_frac_a"])
+    ctx.close()
+    return before, after
+
+
+@pytest.mark.parametrize("flag", OPTIONS)
+def test_update_ice_thickness_options(flag):
+    """Fixed shelf / sheet / grounding-line geometry keep Hi_a (ice_dynamics_module.f90:
+    465-530: the masked cells and their 8-neighbours across the grounding line); the
+    others take dHi_dt_a; do_remove_shelves zeroes every floating cell (:600-606)."""
+    from scipy.ndimage import binary_dilation
+    before, o = options_case(ob.oracle_backend(), flag)
+    shelf, sheet, H0 = before["mask_shelf_a"] == 1, before["mask_sheet_a"] == 1, before["Hi_a"]
+    near_shelf = binary_dilation(shelf, np.ones((3, 3), bool))
+    near_sheet = binary_dilation(sheet, np.ones((3, 3), bool))
+    kept = {"fixed_shelf_geometry": shelf | (sheet & near_shelf),
+            "fixed_sheet_geometry": sheet | (shelf & near_sheet),
+            "fixed_grounding_line": (sheet & near_shelf) | (shelf & near_sheet),
+            "do_remove_shelves": np.zeros_like(shelf)}[flag]
+    grounded = sheet & (H0 > 0)
+    grounded[3, 2] = False                                # the no-ice cell
+    assert o["Hi_a"][3, 2] == 0.0
+    if flag == "do_remove_shelves":
+        assert np.all(o["Hi_a"][shelf] == 0.0)
+        np.testing.assert_array_equal(o["Hi_a"][grounded], H0[grounded] + 1.0)
+        return
+    np.testing.assert_array_equal(o["Hi_a"][grounded & kept], H0[grounded & kept])
+    np.testing.assert_array_equal(o["Hi_a"][grounded & ~kept], H0[grounded & ~kept] + 1.0)
