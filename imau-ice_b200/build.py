@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
           "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 SOURCES = {"api.cu": [], "geometry.cu": ["--fmad=false"], "picard.cu": [], "solver.cu": [], "noalloc.cu": [],
-           "thickness.cu": ["--fmad=false"], "thermo.cu": ["--fmad=false"]}
+           "thickness.cu": ["--fmad=false"], "thermo.cu": ["--fmad=false"], "cnn.cu": []}
 
 
 def _nvcc():

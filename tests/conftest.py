@@ -27,6 +27,8 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); runs the libdiva_b200.so kernels")
+    config.addinivalue_line("markers", "gpu_pending: needs a CUDA GPU (B200); kernels whose first GPU run is "
+                                       "pending, selected with -m gpu_pending")
 
 
 @pytest.fixture(scope="session")

@@ -14,9 +14,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_functions():
-    src = open(os.path.join(ROOT, "include", "diva.h")).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:int|void|int64_t|const char\*)\s+(diva_\w+)\s*\(", src, flags=re.M)))
+    names = set()
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"^\s*(?:int|int32_t|void|int64_t|const char\*)\s+(diva_\w+)\s*\(", src,
+                                flags=re.M))
+    return sorted(names)
 
 
 @pytest.fixture(scope="module")
