@@ -145,6 +145,7 @@ def bind(lib, prefix):
         "solve_diva": (C.c_int, [vp, C.POINTER(Report)]),
         "calc_sia_3d_velocities": (C.c_int, [vp]),
         "nonlinear_residual": (C.c_int, [vp, dp]),
+        "complete_state": (C.c_int, [vp, i32]),
         "state_save": (C.c_int, [vp]),
         "state_restore": (C.c_int, [vp]),
         "determine_floating_margin_fraction": (C.c_int, [vp]),

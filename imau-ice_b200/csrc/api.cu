@@ -774,6 +774,22 @@ int diva_nonlinear_residual(diva_ctx_t* h, double* relres) {
   return solver_relres(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), relres);
 }
 
+int diva_complete_state(diva_ctx_t* h, int32_t sweeps) {
+  if (!h || sweeps < 0 || sweeps > 10000) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  int st;
+  if ((st = launch_driving_stress(c))) return st;
+  if ((st = launch_basal_conditions(c))) return st;
+  if ((st = launch_grounded_fractions(c))) return st;
+  if ((st = launch_prepare_afac(c))) return st;
+  for (int s = 0; s < sweeps; ++s) {
+    if ((st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true))) return st;
+    if ((st = launch_basal_stress_velocities(c))) return st;
+  }
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
 int diva_state_save(diva_ctx_t* h) {
   if (!h) return DIVA_BAD_INPUT;
   Ctx* c = &h->c;

@@ -245,6 +245,12 @@ class Context:
     def calc_sia_3d_velocities(self):
         self._check(self.backend.fns["calc_sia_3d_velocities"](self.h), "calc_sia_3d_velocities")
 
+    def complete_state(self, sweeps=30):
+        """diva_complete_state: the viscosity iteration's carried state (viscosity,
+        beta_eff, basal stress) for the current u_vav_cx / v_vav_cy, by ``sweeps``
+        column-local passes without a linear solve."""
+        self._check(self.backend.fns["complete_state"](self.h, int(sweeps)), "complete_state")
+
     def nonlinear_residual(self):
         r = C.c_double()
         self._check(self.backend.fns["nonlinear_residual"](self.h, C.byref(r)), "nonlinear_residual")

@@ -287,6 +287,19 @@ int  diva_run_thermo_model(diva_ctx_t* ctx, int32_t do_solve_heat_equation, int3
  * except for the coefficient fields. */
 int  diva_nonlinear_residual(diva_ctx_t* ctx, double* relres);
 
+/* Complete the state the DIVA viscosity iteration carries from given velocities:
+ * `sweeps` passes of the column-local stages of one viscosity iteration -- vertical
+ * shear strain rates, effective viscosity, beta, F2, beta_eff (A3-A7,
+ * ice_velocity_module.f90:664-1086) -- and the basal stress and velocities
+ * (:1087-1199), with u_vav_cx / v_vav_cy held fixed and no linear solve.  The
+ * first of those stages reads the previous viscosity and basal stress
+ * (calc_vertical_shear_strain_rates, :664-721), so a context given only velocities
+ * (a restart without viscosity, an observation, a predicted guess) starts
+ * diva_solve_diva as far from its fixed point as a cold start; completing the state
+ * first lets it start from the velocities' own.  No reference counterpart.
+ * 0 <= sweeps <= 10000. */
+int  diva_complete_state(diva_ctx_t* ctx, int32_t sweeps);
+
 /* Snapshot / restore of the Picard state that persists across calls
  * (velocities, visc_eff_3D_a, taub, u_3D_a, v_3D_a, u_3D_cx, v_3D_cy ...):
  * a device-side checkpoint, replacing a cold restart from u = 0. */

@@ -2197,6 +2197,25 @@ int orc_nonlinear_residual(orc_ctx* c, double* relres) {
   return DIVA_OK;
 }
 
+/* The column-local stages of one DIVA viscosity iteration (A3-A7,
+ * ice_velocity_module.f90:664-1086) and the basal stress and velocities
+ * (:1087-1199), `sweeps` times with u_vav held fixed and no linear solve: the
+ * iteration state that belongs to the given velocities.  Test infrastructure: the
+ * restatement the device's diva_complete_state is checked against. */
+int orc_diva_coefficients(orc_ctx* c);
+int orc_complete_state(orc_ctx* c, int32_t sweeps) {
+  if (sweeps < 0 || sweeps > 10000) return DIVA_BAD_INPUT;
+  calc_driving_stress(c);
+  calc_basal_conditions(c);
+  determine_grounded_fractions(c);
+  for (int s = 0; s < sweeps; ++s) {
+    orc_diva_coefficients(c);
+    calc_basal_stress(c);
+    calc_basal_velocities(c);
+  }
+  return DIVA_OK;
+}
+
 /* ------------------------------------------------------------------------ */
 /* context, I/O and configuration                                            */
 

@@ -89,3 +89,25 @@ def test_the_iteration_warm_starts_from_its_whole_state():
     uv, _ = run({k: s[k] for k in ("u_vav_cx", "v_vav_cy")})
     full, _ = run(s)
     assert cold > 20 and uv >= 0.8 * cold and full <= 2
+
+
+def test_complete_state_lets_velocities_alone_warm_start():
+    """diva_complete_state on the oracle: the converged velocities plus 30 column-local
+    sweeps start solve_DIVA at its fixed point."""
+    g, cfg, f = synth.ice_cap(seed=310, dx=20e3)
+    f = dict(f)
+    f["beta_sq_a"] = np.asfortranarray(f["beta_sq_a"] * 4.0)
+    cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
+               lin_rtol=1e-10)
+    its, uv = [], None
+    for sweeps in (None, 30):
+        ctx = diva.Context(diva.Grid(**g), cfg, ob.oracle_backend())
+        ob.set_linear_solver(ctx, ob.LIN_GMRES_WARM, rtol=1e-10, abstol=0.0)
+        helpers.prepare(ctx, f)
+        if uv is not None:
+            ctx.upload(uv)
+            ctx.complete_state(sweeps)
+        its.append(ctx.solve_DIVA()["picard_iterations"])
+        uv = ctx.download(["u_vav_cx", "v_vav_cy"])
+        ctx.close()
+    assert its[0] > 20 and its[1] <= 2, its

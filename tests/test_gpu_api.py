@@ -294,3 +294,37 @@ def test_restart_file_continues_bit_for_bit(cuda, tmp_path):
         assert np.array_equal(a[k], b[k]), k
     ctx.close()
     ctx2.close()
+
+
+def test_complete_state_matches_the_oracle_and_warm_starts(cuda, oracle):
+    """diva_complete_state from the oracle's converged velocities: the completed
+    viscosity, beta_eff and basal stress agree with the oracle's, and solve_DIVA
+    started from them stops within a few iterations (a cold start needs > 20)."""
+    import oracle_backend as ob
+    from imau_ice_b200 import synth
+    g, cfg, f = synth.ice_cap(seed=310, dx=20e3)
+    f = dict(f)
+    f["beta_sq_a"] = np.asfortranarray(f["beta_sq_a"] * 4.0)
+    cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
+               lin_rtol=1e-10)
+    grid = diva.Grid(**g)
+    ctx = diva.Context(grid, cfg, oracle)
+    ob.set_linear_solver(ctx, ob.LIN_GMRES_WARM, rtol=1e-10, abstol=0.0)
+    helpers.prepare(ctx, f)
+    cold = ctx.solve_DIVA()["picard_iterations"]
+    uv = ctx.download(["u_vav_cx", "v_vav_cy"])
+    ctx.close()
+    names = ["visc_eff_3D_a", "beta_eff_cx", "beta_eff_cy", "taub_cx", "taub_cy", "u_base_cx", "v_base_cy"]
+    out = []
+    for be in (cuda, oracle):
+        ctx = diva.Context(grid, cfg, be)
+        helpers.prepare(ctx, f)
+        ctx.upload(uv)
+        ctx.complete_state(30)
+        out.append(ctx.download(names))
+        if be is cuda:
+            rep = ctx.solve_DIVA()
+        ctx.close()
+    for k in names:
+        assert helpers.rel_l2(out[0][k], out[1][k]) <= 1e-9, k
+    assert cold > 20 and rep["status"] == 0 and rep["picard_iterations"] <= 3, (cold, rep)
