@@ -713,19 +713,17 @@ __global__ void k_targets(Dims d, StatePtrs s, float* tgt, int Hp, int Wp) {
   for (int o = 0; o < kOut; ++o) tgt[((long)y * Wp + x) * kOut + o] = t[o];
 }
 
-__global__ void k_apply(Dims d, const float* pred, StatePtrs s, int Wp) {
+// the predicted state into the context's fields; velocities_only: u_vav_cx and v_vav_cy
+__global__ void k_apply(Dims d, const float* pred, StatePtrs s, int Wp, int velocities_only) {
   const int y = blockIdx.x * blockDim.x + threadIdx.x;
   const int x = blockIdx.y * blockDim.y + threadIdx.y;
   if (y >= d.ny || x >= d.nx) return;
   const float* q = pred + ((long)y * Wp + x) * kOut;
-  if (x < d.nx - 1) {
-    s.ucx[d.at(y, x)] = kVelScale * sinh((double)q[0]);
-    s.tbx[d.at(y, x)] = kTauScale * sinh((double)q[2]);
-  }
-  if (y < d.ny - 1) {
-    s.vcy[d.at(y, x)] = kVelScale * sinh((double)q[1]);
-    s.tby[d.at(y, x)] = kTauScale * sinh((double)q[3]);
-  }
+  if (x < d.nx - 1) s.ucx[d.at(y, x)] = kVelScale * sinh((double)q[0]);
+  if (y < d.ny - 1) s.vcy[d.at(y, x)] = kVelScale * sinh((double)q[1]);
+  if (velocities_only) return;
+  if (x < d.nx - 1) s.tbx[d.at(y, x)] = kTauScale * sinh((double)q[2]);
+  if (y < d.ny - 1) s.tby[d.at(y, x)] = kTauScale * sinh((double)q[3]);
   for (int k = 0; k < d.nz; ++k) s.visc[k * d.plane + d.at(y, x)] = pow(10.0, (double)q[4 + k] + kViscShift);
 }
 
@@ -1182,18 +1180,20 @@ int32_t diva_cnn_add_sample(diva_cnn_t* N, diva_ctx_t* ctx) {
   return DIVA_OK;
 }
 
-int32_t diva_cnn_predict(diva_cnn_t* N, diva_ctx_t* ctx) {
-  if (!N || !ctx) return DIVA_BAD_INPUT;
+int32_t diva_cnn_predict(diva_cnn_t* N, diva_ctx_t* ctx, int32_t complete_sweeps) {
+  if (!N || !ctx || complete_sweeps < 0 || complete_sweeps > 10000) return DIVA_BAD_INPUT;
   Ctx* c = &ctx->c;
   if (c->d.ny != N->ny || c->d.nx != N->nx || c->d.nz != N->nz) return DIVA_BAD_INPUT;
   CK(cudaStreamSynchronize(N->stream));
   k_features<<<img_grid(N->Hp, N->Wp), block2d(), 0, c->stream>>>(c->d, field_ptrs(c), N->act[T_IN], N->Hp,
                                                                    N->Wp);
   RET(forward(N, N->act[T_IN], N->out, 1, c->stream));
-  k_apply<<<img_grid(N->ny, N->nx), block2d(), 0, c->stream>>>(c->d, N->out, state_ptrs(c), N->Wp);
+  k_apply<<<img_grid(N->ny, N->nx), block2d(), 0, c->stream>>>(c->d, N->out, state_ptrs(c), N->Wp,
+                                                                complete_sweeps > 0);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
-  return check_err(N);
+  RET(check_err(N));
+  return complete_sweeps > 0 ? diva_complete_state(ctx, complete_sweeps) : DIVA_OK;
 }
 
 int32_t diva_cnn_forward(diva_cnn_t* N, const void* feat, float* out, int32_t n) {

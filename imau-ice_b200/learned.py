@@ -3,8 +3,9 @@
 ``WarmStartNet`` owns one network for one grid size: it collects training samples
 from contexts after converged solves (``add_sample``), trains on them on the device
 (``train``: BF16 tensor-core convolutions with FP32 accumulation, Adam on FP32 master
-weights), and writes its prediction of the iteration state -- u_vav_cx, v_vav_cy,
-taub_cx, taub_cy and visc_eff_3D_a -- into a context before its solve (``predict``).
+weights), and warm-starts a context before its solve (``predict``): the predicted
+velocities with the viscosity and basal stress completed from them, or the whole
+predicted state (u_vav_cx, v_vav_cy, taub_cx, taub_cy, visc_eff_3D_a).
 The viscosity iteration then runs to its own tolerance from there, so the prediction
 changes the iteration count, not the converged velocities.
 
@@ -46,7 +47,7 @@ def _bind(lib):
         "add_sample": [vp, vp],
         "num_samples": [vp, C.POINTER(i32)],
         "train": [vp, i32, C.c_float, C.c_uint64, f32p],
-        "predict": [vp, vp],
+        "predict": [vp, vp, i32],
         "padded_shape": [vp, C.POINTER(i32), C.POINTER(i32)],
         "forward": [vp, vp, vp, i32],
         "train_step": [vp, vp, vp, i32, C.c_float, f32p],
@@ -137,9 +138,10 @@ class WarmStartNet:
         self._check(self._f["train"](self._h, int(epochs), float(lr), C.c_uint64(seed), C.byref(loss)), "train")
         return loss.value
 
-    def predict(self, ctx):
-        """Write the predicted iteration state into ``ctx`` (call before solve_DIVA)."""
-        self._check(self._f["predict"](self._h, ctx.h), "predict")
+    def predict(self, ctx, complete_sweeps=30):
+        """Warm-start ``ctx`` (call before solve_DIVA): the predicted velocities plus
+        ``complete_sweeps`` state-completion sweeps, or with 0 the whole predicted state."""
+        self._check(self._f["predict"](self._h, ctx.h, int(complete_sweeps)), "predict")
 
     # device-buffer forms (pointers to device memory) ----------------------------
     def forward(self, feat_ptr, out_ptr, n):

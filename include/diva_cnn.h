@@ -12,7 +12,9 @@
  * vertical shear (calc_vertical_shear_strain_rates, :664-721) is computed from the
  * previous viscosity and basal stress, so a context given the converged velocities
  * but a cold viscosity and stress iterates as long as a cold start.  diva_cnn_predict
- * writes all five fields of a context; a caller places it before diva_solve_diva.
+ * writes the predicted velocities and completes the rest of the state from them
+ * (diva_complete_state), or writes all five fields; a caller places it before
+ * diva_solve_diva.
  *
  * Network (one instance per grid size; all sizes in cells of the a-grid):
  *   input  16 channels on the a-grid padded to multiples of 4 (8 used, see below)
@@ -76,10 +78,15 @@ int32_t diva_cnn_num_samples(const diva_cnn_t* net, int32_t* n);
  * error of the last epoch. */
 int32_t diva_cnn_train(diva_cnn_t* net, int32_t epochs, float lr, uint64_t seed, float* loss);
 
-/* Set the context's u_vav_cx, v_vav_cy, taub_cx, taub_cy and visc_eff_3D_a from the
- * network's prediction for its current fields (on the context's stream, synchronised
- * before return). */
-int32_t diva_cnn_predict(diva_cnn_t* net, diva_ctx_t* ctx);
+/* Warm-start the context from the network's prediction for its current fields.
+ * complete_sweeps > 0: set u_vav_cx and v_vav_cy from the prediction, then derive the
+ * viscosity and basal stress that belong to them with diva_complete_state(ctx,
+ * complete_sweeps) (the more robust choice: measured on 20 km ice caps with the
+ * oracle, 30 sweeps after a predicted velocity field cut the viscosity iterations by
+ * a fifth and lengthened one case of twenty).  complete_sweeps = 0: set all five
+ * state fields from the prediction.  On the context's stream, synchronised before
+ * return. */
+int32_t diva_cnn_predict(diva_cnn_t* net, diva_ctx_t* ctx, int32_t complete_sweeps);
 
 /* Device-buffer forms for tests and callers with their own data (pointers are device
  * memory; n <= batch).  feat: [n][Hp][Wp][16] BF16 with Hp, Wp = ny, nx rounded up to
