@@ -526,6 +526,93 @@ def run_timestep(args):
     return 0
 
 
+def run_learned(args):
+    """Learned warm start workload (the ice cap 321 x 561 x 15, seeded geometries):
+    solve --members training caps (seeds 0..) with the plain FP64 path and keep them
+    on the device, train the warm-start network on them, then time --steps held-out
+    caps (seeds 10000..) both ways -- cold FP64, and network prediction + state
+    completion + solve at --precision -- each to rel-res 1e-6.  value = learned
+    solves/s; the cold FP64 rate and the iteration counts ride along.  Device-
+    synchronised wall clock around each whole solve call (inputs already resident)."""
+    import numpy as np
+    import torch
+    load_package()
+    from imau_ice_b200 import build, diva, learned, synth
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    build.build()
+
+    def case(seed, precision):
+        g, cfg, f = synth.ice_cap(seed=seed)
+        cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
+                   lin_rtol=1e-10, precision=precision)
+        return diva.Grid(**g), cfg, f
+
+    def prepared(seed, precision):
+        grid, cfg, f = case(seed, precision)
+        ctx = diva.Context(grid, cfg)
+        ctx.upload(f)
+        ctx.update_general_ice_model_data()
+        ctx.calc_pressure_melting_point()
+        ctx.calc_ice_rheology()
+        ctx.update_general_ice_model_data()
+        return ctx
+
+    grid = case(0, "fp64")[0]
+    net = learned.WarmStartNet(grid, batch=8, capacity=args.members, seed=0)
+    t0 = time.perf_counter()
+    seed = 0
+    while net.num_samples < args.members and seed < 4 * args.members:
+        ctx = prepared(seed, "fp64")
+        if ctx.solve_DIVA()["status"] == 0:
+            net.add_sample(ctx)
+        ctx.close()
+        seed += 1
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss = net.train(args.epochs, lr=1e-3, seed=1)
+    t_train = time.perf_counter() - t0
+
+    def timed(seed, use_net):
+        ctx = prepared(seed, args.precision if use_net else "fp64")
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        if use_net:
+            net.predict(ctx, complete_sweeps=30)
+        rep = ctx.solve_DIVA()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+        ctx.close()
+        return dt, rep
+
+    for k in range(args.warmup):
+        timed(20000 + k, False)
+        timed(20000 + k, True)
+    clocks = ClockSampler(0)
+    clocks.start()
+    cold = [timed(10000 + k, False) for k in range(args.steps)]
+    warm = [timed(10000 + k, True) for k in range(args.steps)]
+    clk = clocks.stop()
+    t_cold, t_warm = sum(d for d, _ in cold), sum(d for d, _ in warm)
+    print(json.dumps({
+        "metric": "DIVA solves/s at 321x561x15 to rel-res 1e-6: learned warm start" +
+                  (" + FP32 smoother" if args.precision == "mixed" else "") + " vs plain FP64 GPU",
+        "value": args.steps / t_warm, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * t_warm / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+        "data": "synthetic (seeded ice caps; training seeds 0.., held-out seeds 10000..)",
+        "config": {"workload": "held-out ice caps 1600x2800 km @5 km, network warm start + 30 completion sweeps",
+                   "plain_fp64_solves_per_s": args.steps / t_cold,
+                   "iterations_cold": [r["picard_iterations"] for _, r in cold],
+                   "iterations_learned": [r["picard_iterations"] for _, r in warm],
+                   "status_learned": [r["status"] for _, r in warm],
+                   "training_samples": net.num_samples, "epochs": args.epochs, "final_loss": loss,
+                   "data_generation_s": t_data, "training_s": t_train,
+                   "timing": "device-synchronised wall clock around predict + solve (inputs resident)"},
+        "clocks": clk}))
+    net.close()
+    return 0
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--gpus", type=int, default=1)
@@ -535,9 +622,11 @@ def main():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true",
                    help="timed solves only (no roofline, e2e or CPU legs): the command profiled with ncu")
-    p.add_argument("--workload", choices=["icecap", "ensemble", "timestep"], default="icecap",
+    p.add_argument("--workload", choices=["icecap", "ensemble", "timestep", "learned"], default="icecap",
                    help="icecap: the headline solve (default); ensemble: --members perturbed members; "
-                        "timestep: predictor/corrector steps with thickness and heat equation")
+                        "timestep: predictor/corrector steps with thickness and heat equation; "
+                        "learned: --members training caps, then held-out solves cold vs warm-started")
+    p.add_argument("--epochs", type=int, default=60, help="training epochs of the learned workload")
     p.add_argument("--members", type=int, default=64)
     p.add_argument("--ensemble-sizes", default="channel,icecap",
                    help="member kinds drawn from: channel (129x17), icecap (321x561), sheet (1501x1501)")
@@ -548,6 +637,8 @@ def main():
         return run_ensemble(args)
     if args.impl == "b200" and args.workload == "timestep":
         return run_timestep(args)
+    if args.impl == "b200" and args.workload == "learned":
+        return run_learned(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)
