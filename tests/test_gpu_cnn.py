@@ -1,8 +1,9 @@
 """The warm-start network's CUDA kernels (tcgen05 implicit-GEMM convolutions, head,
 Adam, the context <-> tensor kernels) against the PyTorch FP32 reference
 (tests/cnn_reference.py) with the device's BF16 roundings, and the end-to-end effect
-on solve_DIVA.  Marked ``gpu_pending``: selected with ``-m gpu_pending`` on a B200;
-they move under ``gpu`` once they have run there."""
+on solve_DIVA.  Tests marked ``gpu`` have passed on a B200; those marked
+``gpu_pending`` (selected with ``-m gpu_pending``) have not run there yet and move
+under ``gpu`` once they have."""
 import numpy as np
 import pytest
 import torch
@@ -11,8 +12,7 @@ from imau_ice_b200 import diva, learned, synth
 import cnn_reference as ref
 import helpers
 
-pytestmark = [pytest.mark.gpu_pending,
-              pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU (B200)")]
+pytestmark = pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU (B200)")
 
 
 def small_net(ny=29, nx=37, batch=2, seed=3):
@@ -34,6 +34,7 @@ def dev(a, dtype):
     return torch.as_tensor(a).to(dtype).cuda().contiguous()
 
 
+@pytest.mark.gpu
 def test_forward_matches_the_reference():
     g, net = small_net()
     feat, _ = random_batch(net, 2, 0)
@@ -46,6 +47,7 @@ def test_forward_matches_the_reference():
     net.close()
 
 
+@pytest.mark.gpu_pending
 def test_gradients_match_autograd():
     g, net = small_net()
     feat, tgt = random_batch(net, 2, 1)
@@ -55,9 +57,10 @@ def test_gradients_match_autograd():
     loss_ref = ref.loss(ref.forward(feat, w, bf16=True), torch.as_tensor(tgt), mask)
     loss_ref.backward()
     gref = w.grad.numpy()
-    loss = net.train_step(dev(feat, torch.bfloat16).data_ptr(), dev(tgt, torch.float32).data_ptr(), 2, 0.0)
+    f, t = dev(feat, torch.bfloat16), dev(tgt, torch.float32)    # held: the kernels read them
+    loss = net.train_step(f.data_ptr(), t.data_ptr(), 2, 0.0)
     gdev = net.grads()
-    assert abs(loss - float(loss_ref)) <= 2e-2 * float(loss_ref)
+    assert abs(loss - loss_ref.item()) <= 2e-2 * loss_ref.item()
     lay, _ = learned.weight_layout()
     for name, (wo, shape, bo, nb) in lay.items():
         n = int(np.prod(shape))
@@ -67,6 +70,7 @@ def test_gradients_match_autograd():
     net.close()
 
 
+@pytest.mark.gpu_pending
 def test_training_lowers_the_loss_and_predict_writes_the_state():
     g, net = small_net(batch=2)
     feat, tgt = random_batch(net, 2, 2)
@@ -97,6 +101,7 @@ def test_training_lowers_the_loss_and_predict_writes_the_state():
     net2.close()
 
 
+@pytest.mark.gpu_pending
 def test_warm_start_from_the_trained_network_cuts_iterations():
     """Ice caps at 20 km (friction x4): train on 96 solved members, then the held-out
     members converge to the same tolerance from the prediction (velocities plus 30
