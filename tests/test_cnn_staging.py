@@ -57,7 +57,7 @@ def conv_kernel(x, gate, w, bias, KC, NO, dgrad, n, H, W):
                 sm[base:base + 8] = v
             for k in range(KC // 16):
                 A = canon_read(sm, 2 * k * 2048, 2048, 128, 128)
-                B = canon_read(sm, A_BYTES + 2 * k * (NO * 16), NO * 16, 128, NO, 16)
+                B = canon_read(sm, A_BYTES + 2 * k * (NO * 16), NO * 16, 128, NO)
                 D += A @ B.T
         for tid in range(128):
             p = blk * 128 + tid
@@ -104,7 +104,7 @@ def wgrad_kernel(x, dy_, gate, CI, CO, n, H, W, nsplit, PIX=64):
                         sm[(A_BYTES + (kk >> 3) * (CI * 16) + (nc * 8 + q) * 16 + (kk & 7) * 2) // 2] = v[q]
                 for k in range(PIX // 16):
                     A = canon_read(sm, 2 * k * 2048, 2048, 128, 128)
-                    B = canon_read(sm, A_BYTES + 2 * k * (CI * 16), CI * 16, 128, CI, 16)
+                    B = canon_read(sm, A_BYTES + 2 * k * (CI * 16), CI * 16, 128, CI)
                     D += A @ B.T
             part[split, t] = D[:CO]
     return part.sum(0)   # [9][CO][CI]
