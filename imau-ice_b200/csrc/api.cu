@@ -813,6 +813,23 @@ int diva_state_restore(diva_ctx_t* h) {
   return DIVA_OK;
 }
 
+int diva_get_tile_edges(diva_ctx_t* h, int32_t* edges, int32_t n, int32_t* nlev) {
+  if (!h || !edges || !nlev || n < 0) return DIVA_BAD_INPUT;
+  *nlev = solver_tile_edges(&h->c, edges, n < kMaxLevels ? n : kMaxLevels);
+  for (int l = kMaxLevels; l < n; ++l) edges[l] = 0;
+  return DIVA_OK;
+}
+
+int diva_set_tile_edges(diva_ctx_t* h, const int32_t* edges, int32_t n) {
+  if (!h || (n > 0 && !edges) || n < 0 || n > kMaxLevels) return DIVA_BAD_INPUT;
+  for (int l = 0; l < n; ++l)
+    if (edges[l] != 0 && edges[l] != 16 && edges[l] != 32) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  for (int l = 0; l < kMaxLevels; ++l) c->tile_override[l] = l < n ? edges[l] : 0;
+  solver_destroy_graphs(c);   // captured launches carry the tile shapes
+  return DIVA_OK;
+}
+
 int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, double* bytes) {
   if (!h || !ms || !bytes || reps < 1 || which < 0 || which > 5) return DIVA_BAD_INPUT;
   Ctx* c = &h->c;

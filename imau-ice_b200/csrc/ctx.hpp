@@ -113,6 +113,7 @@ struct Ctx {
   bool graphs_disabled = false;         // set if graph construction failed: host-driven loop
   bool tiled = false;                   // large levels smoothed by the tiled kernels
   bool tiles_disabled = false;          // per-colour kernels on every level
+  int tile_override[kMaxLevels] = {};   // tile edge of a tiled level: 0 by its size, else 16 or 32
   // counters of the last solve
   long lin_iters = 0, mg_cycles = 0;
   long long launches = 0;            // kernels launched since create
@@ -180,6 +181,9 @@ int solver_subcycle(Ctx* c, int reps);
 double solver_vcycle_bytes(const Ctx* c);
 int solver_build_picard_graphs(Ctx* c, bool diva);
 void solver_destroy_graphs(Ctx* c);
+// tile edge (16 or 32) of each level's smoothing kernels, 0 for levels not smoothed by
+// the tiled kernels; returns the number of levels
+int solver_tile_edges(const Ctx* c, int32_t* edges, int n);
 
 }  // namespace diva
 

@@ -1764,8 +1764,10 @@ static int sub_first_level(const Ctx* c) {
 static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
                   const Restriction& rs);
 
-// tile edge of level l's smoothing kernels: 32 x 32 while that still fills the GPU, else 16 x 16
+// tile edge of level l's smoothing kernels: 32 x 32 while that still fills the GPU, else
+// 16 x 16, unless the caller chose one (diva_set_tile_edges, e.g. from an autotuner)
 static int tile_edge(const Ctx* c, int l) {
+  if (c->tile_override[l] == 16 || c->tile_override[l] == 32) return c->tile_override[l];
   const Dims& d = c->lv[l].d;
   const long long b32 = (long long)((d.ny + 31) / 32) * ((d.nx + 31) / 32);
   return b32 >= 148 ? 32 : 16;
@@ -2431,6 +2433,13 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
 }
 
 }  // namespace
+
+int solver_tile_edges(const Ctx* c, int32_t* edges, int n) {
+  const int first = sub_first_level(c);
+  for (int l = 0; l < n; ++l)
+    edges[l] = (l < c->nlev && c->tiled && c->nlev > 1 && l < first) ? tile_edge(c, l) : 0;
+  return c->nlev;
+}
 
 void solver_destroy_graphs(Ctx* c) {
   for (auto& G : c->graphs) {

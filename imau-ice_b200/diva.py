@@ -316,6 +316,21 @@ class Context:
         f.restype = C.c_int64
         return int(f(self.h))
 
+    def get_tile_edges(self):
+        """(edge of each multigrid level's tiled smoother, 0 where untiled; level count)."""
+        f = self.backend.lib.diva_get_tile_edges
+        f.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]
+        e, n = (C.c_int32 * 12)(), C.c_int32()
+        self._check(f(self.h, e, 12, C.byref(n)), "get_tile_edges")
+        return [int(e[k]) for k in range(n.value)]
+
+    def set_tile_edges(self, edges):
+        """Fix the tile edge (16, 32, or 0 for the default) of levels 0..len(edges)-1."""
+        f = self.backend.lib.diva_set_tile_edges
+        f.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int32]
+        e = (C.c_int32 * max(1, len(edges)))(*[int(v) for v in edges])
+        self._check(f(self.h, e, len(edges)), "set_tile_edges")
+
     def profile_kernel(self, which, reps=20):
         """(ms per launch, algorithmic bytes per launch) of one hot kernel (diva_profile_kernel)."""
         f = self.backend.lib.diva_profile_kernel

@@ -300,6 +300,17 @@ int  diva_nonlinear_residual(diva_ctx_t* ctx, double* relres);
  * 0 <= sweeps <= 10000. */
 int  diva_complete_state(diva_ctx_t* ctx, int32_t sweeps);
 
+/* Tile shapes of the multigrid smoother.  The levels above the one-block sub-cycle
+ * are smoothed by tiled kernels of edge 16 or 32; by default a level takes 32 while
+ * its 32 x 32 tiles still fill the GPU.  diva_get_tile_edges writes each level's
+ * edge (0 for levels not smoothed by tiles) into edges[0..n) and the level count
+ * into *nlev; diva_set_tile_edges fixes the edge of levels 0..n-1 (16, 32, or 0 for
+ * the default) until the next call, e.g. from an autotuner that times candidates
+ * with diva_profile_kernel.  The solution does not depend on the edge, only the
+ * time per V-cycle. */
+int  diva_get_tile_edges(diva_ctx_t* ctx, int32_t* edges, int32_t n, int32_t* nlev);
+int  diva_set_tile_edges(diva_ctx_t* ctx, const int32_t* edges, int32_t n);
+
 /* Snapshot / restore of the Picard state that persists across calls
  * (velocities, visc_eff_3D_a, taub, u_3D_a, v_3D_a, u_3D_cx, v_3D_cy ...):
  * a device-side checkpoint, replacing a cold restart from u = 0. */
