@@ -33,7 +33,10 @@ def candidates(edges):
 
 
 def tune_tile_edges(ctx, reps=20, trials=3, cache=None):
-    """Pick and set the fastest tile edges for ``ctx``; returns (edges, {edges: ms})."""
+    """Pick and set the fastest tile edges for ``ctx``; returns (edges, {edges: ms}).
+    Contexts of other backends than the CUDA library have no tiles: ([], {})."""
+    if getattr(getattr(ctx, "backend", None), "name", "cuda") != "cuda":
+        return [], {}
     key = cache_key(ctx)
     if cache and os.path.exists(cache):
         with open(cache) as f:

@@ -79,10 +79,14 @@ def _prepare(ctx, fields):
     ctx.update_general_ice_model_data()
 
 
-def solve_members(members, indices, backend, budget_bytes=40e9, outputs=("u_vav_cx", "v_vav_cy")):
+def solve_members(members, indices, backend, budget_bytes=40e9, outputs=("u_vav_cx", "v_vav_cy"),
+                  tile_cache=None):
     """Solve members ``indices`` on this process's device, group by group.  Returns
     {index: {"name", "report", "seconds", <outputs>}}; a member whose solve fails
-    carries its status and message in the report instead of outputs."""
+    carries its status and message in the report instead of outputs.  With
+    ``tile_cache`` (a JSON path) each member's smoother tile shapes come from the
+    autotuner, which times each grid shape once and caches the choice there; the
+    results are the same bit for bit, only the time per V-cycle changes."""
     res = {}
     batched = getattr(backend.lib, backend.prefix + "solve_diva_batch", None) is not None
     for grp in groups(members, indices, budget_bytes):
@@ -93,6 +97,9 @@ def solve_members(members, indices, backend, budget_bytes=40e9, outputs=("u_vav_
                 c = diva.Context(_grid(grid), cfg, backend)
                 ctxs.append(c)
                 _prepare(c, fields)
+                if tile_cache:
+                    from . import autotune
+                    autotune.tune_tile_edges(c, cache=tile_cache)
                 c.state_save()
             t0 = time.perf_counter()
             if batched:
@@ -123,13 +130,13 @@ def solve_members(members, indices, backend, budget_bytes=40e9, outputs=("u_vav_
 
 
 def solve_ensemble(members, backend, rank=0, world=1, group=None, budget_bytes=40e9,
-                   outputs=("u_vav_cx", "v_vav_cy"), gather=True):
+                   outputs=("u_vav_cx", "v_vav_cy"), gather=True, tile_cache=None):
     """Solve an ensemble with ``world`` processes: this rank solves its share of the
     longest-processing-time partition.  With ``gather`` (and world > 1) every rank
     returns the results of all members (host all-gather through torch.distributed on
     ``group``); otherwise only its own."""
     parts = partition([member_cost(m) for m in members], world)
-    mine = solve_members(members, parts[rank], backend, budget_bytes, outputs)
+    mine = solve_members(members, parts[rank], backend, budget_bytes, outputs, tile_cache)
     if not gather or world == 1:
         return mine, parts
     import torch.distributed as dist

@@ -43,3 +43,9 @@ def test_tuner_picks_the_fastest_and_caches_it(tmp_path):
     ctx2 = FakeCtx()
     best2, t2 = autotune.tune_tile_edges(ctx2, cache=cache)
     assert best2 == best and ctx2.calls == 0 and ctx2.edges == best
+
+
+def test_other_backends_are_left_alone():
+    ctx = FakeCtx()
+    ctx.backend = type("B", (), {"name": "oracle"})()
+    assert autotune.tune_tile_edges(ctx) == ([], {}) and ctx.calls == 0 and ctx.edges == []
