@@ -28,6 +28,7 @@ HBC = {"zero": 0, "infinite": 1, "periodic": 2, "fixed": 3, "none": 4}
 HEATCAP = {"uniform": 0, "Pounder1965": 1}
 CONDUCT = {"uniform": 0, "Ritz1987": 1}
 INTEGRATION = {"explicit": 0, "semi-implicit": 1, "none": 2}
+CALVING = {"none": 0, "threshold_thickness": 1}
 
 GRID_KINDS = ["A", "CX", "CY", "B", "A3", "CX3", "CY3", "B3"]
 
@@ -90,6 +91,8 @@ class Config(C.Structure):
         ("fixed_shelf_geometry", C.c_int32), ("fixed_sheet_geometry", C.c_int32),
         ("fixed_grounding_line", C.c_int32), ("do_remove_shelves", C.c_int32),
         ("ocean_temperature_input", C.c_int32),
+        ("choice_calving_law", C.c_int32),
+        ("calving_threshold_thickness", C.c_double),
         ("reserved", C.c_int32 * 8),
     ]
 
@@ -123,6 +126,7 @@ ENUM_OPTIONS = {
     "ice_thickness_north_BC": HBC,
     "choice_ice_heat_capacity": HEATCAP, "choice_ice_thermal_conductivity": CONDUCT,
     "choice_ice_integration_method": INTEGRATION,
+    "choice_calving_law": CALVING,
 }
 
 

@@ -327,6 +327,15 @@ __global__ void k_shelf_spread(Dims d, const int* shelf, int* reach, int* change
   }
 }
 // then the no-ice mask (:586-592) and, with do_remove_shelves, all floating ice (:600-608)
+// threshold_thickness_calving (calving_module.f90:62-91): calving-front cells whose
+// effective thickness is below the threshold lose their ice
+__global__ void k_calve_threshold(Dims d, const int* cf, const double* Heff, double thr, double* Hi) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= d.ny || i >= d.nx) return;
+  const long long q = d.at(j, i);
+  if (cf[q] == 1 && Heff[q] < thr) Hi[q] = 0.0;
+}
+
 __global__ void k_shelf_remove(Dims d, const int* shelf, const int* reach, const int* noice, int remove_floating,
                                const double* Hb, const double* SL, double* Hi) {
   IDX2D
@@ -732,6 +741,18 @@ int diva_pc_finish(diva_ctx_t* h, double dt) {
   DIVA_LAUNCHED(c, "k_pc_finish");
   if (int st = launch_update_general_ice_model_data(c)) return st;
   if (int st = launch_floating_margin_fraction(c)) return st;
+  if (c->c.choice_calving_law == DIVA_CALVING_THRESHOLD_THICKNESS) {
+    // threshold_thickness_calving (calving_module.f90:62-91), twice so that the calving
+    // front may retreat by more than one cell (ice_dynamics_module.f90:562-583)
+    for (int pass = 0; pass < 2; ++pass) {
+      k_calve_threshold<<<G2T>>>(d, c->I(DIVA_F_MASK_CF_A), c->D(DIVA_F_HI_EFF_CF_A),
+                                 c->c.calving_threshold_thickness, c->D(DIVA_F_HI_A)); c->launches++;
+      DIVA_LAUNCHED(c, "k_calve_threshold");
+      if (int st = launch_update_general_ice_model_data(c)) return st;
+      if (pass == 0)
+        if (int st = launch_floating_margin_fraction(c)) return st;
+    }
+  }
   // remove_unconnected_shelves (:932-1044), then the no-ice mask (:586-592)
   int* reach = c->col_flags;   // per-column scratch
   const int* shelf = c->I(DIVA_F_MASK_SHELF_A);

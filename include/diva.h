@@ -84,6 +84,8 @@ typedef enum { DIVA_PREC_FP64 = 0, DIVA_PREC_MIXED = 1 } diva_precision_t;
 typedef enum { DIVA_INTEGRATION_EXPLICIT = 0, DIVA_INTEGRATION_SEMIIMPLICIT = 1,
                DIVA_INTEGRATION_NONE = 2 } diva_integration_t;
 typedef enum { DIVA_HEATCAP_UNIFORM = 0, DIVA_HEATCAP_POUNDER1965 = 1 } diva_heatcap_t;
+/* Calving law of update_ice_thickness (calving_module.f90:30-91). */
+typedef enum { DIVA_CALVING_NONE = 0, DIVA_CALVING_THRESHOLD_THICKNESS = 1 } diva_calving_t;
 typedef enum { DIVA_CONDUCT_UNIFORM = 0, DIVA_CONDUCT_RITZ1987 = 1 } diva_conductivity_t;
 /* Ice thickness at the domain boundary (apply_ice_thickness_BC, ice_thickness_module.f90:728-931). */
 typedef enum { DIVA_HBC_ZERO = 0, DIVA_HBC_INFINITE = 1, DIVA_HBC_PERIODIC = 2, DIVA_HBC_FIXED = 3,
@@ -161,6 +163,10 @@ typedef struct {
    * interpolate_ocean_depth gives an ocean model) from T_ocean_base_a; 0: ocean model
    * 'none', T_ocean_mean_PD_ANT everywhere */
   int32_t ocean_temperature_input;
+  /* calving law (configuration_module.f90:412-413): diva_calving_t, default
+   * 'threshold_thickness' with 200 m, as in the reference */
+  int32_t choice_calving_law;
+  double  calving_threshold_thickness;
   int32_t reserved[8];
 } diva_config_t;
 
@@ -260,11 +266,13 @@ int  diva_pc_predictor(diva_ctx_t* ctx, double dt, double zeta);
  * sheet cells with no grounding line in their 3 x 3 neighbourhood). */
 int  diva_pc_corrector(diva_ctx_t* ctx, double dt, double zeta, double eta_min, double* eta);
 /* Hi_tplusdt_a = max(0, Hi_a + dt dHi_dt_a) (:429-431), then update_ice_thickness
- * (:435-648) on its default path (choice_calving_law 'none', no fixed geometries, no
- * shelf removal flags unless set): mask_ice_a_prev = mask_ice_a; [fixed_shelf_geometry,
- * fixed_sheet_geometry, fixed_grounding_line keep Hi_tplusdt_a = Hi_a on shelf / sheet /
- * grounding-line cells]; Hi_a = max(0, Hi_tplusdt_a); masks;
- * determine_floating_margin_fraction; remove_unconnected_shelves (ice_thickness_module.f90:
+ * (:435-648): mask_ice_a_prev = mask_ice_a; [fixed_shelf_geometry, fixed_sheet_geometry,
+ * fixed_grounding_line keep Hi_tplusdt_a = Hi_a on shelf / sheet / grounding-line
+ * cells]; Hi_a = max(0, Hi_tplusdt_a); masks; determine_floating_margin_fraction;
+ * [choice_calving_law 'threshold_thickness' (the default): twice, Hi_a = 0 on
+ * calving-front cells with Hi_eff_cf_a < calving_threshold_thickness, then masks (and
+ * the floating margin fraction after the first pass) (:562-583, calving_module.f90:
+ * 62-91)]; remove_unconnected_shelves (ice_thickness_module.f90:
  * 932-1044: shelf cells not 4-connected through shelf to a shelf cell next to sheet ice
  * lose their ice); Hi_a = 0 where mask_noice_a (region%mask_noice); [do_remove_shelves:
  * Hi_a = 0 on floating cells]; and update_general_ice_model_data. */

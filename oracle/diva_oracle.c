@@ -2241,6 +2241,7 @@ void orc_config_defaults(diva_config_t* c) {
   c->choice_ice_thermal_conductivity = DIVA_CONDUCT_RITZ1987; c->uniform_ice_thermal_conductivity = 6.626958E7;
   c->T_ocean_mean_PD_ANT = -1.7;
   c->choice_ice_integration_method = DIVA_INTEGRATION_EXPLICIT; c->dHi_rtol = 1E-10; c->dHi_maxit = 1000;
+  c->choice_calving_law = DIVA_CALVING_THRESHOLD_THICKNESS; c->calving_threshold_thickness = 200.0;
   c->precision = DIVA_PREC_FP64;
 }
 
@@ -2779,9 +2780,21 @@ int orc_pc_finish(orc_ctx* c, double dt) {
       }
   }
   for (size_t q = 0; q < n; ++q) Hi[q] = fmax(0.0, Hn[q]);
-  int st = orc_update_general_ice_model_data(c);                            /* the masks of :556-570 */
+  int st = orc_update_general_ice_model_data(c);                            /* the masks of :556-590 */
   if (st) return st;
   floating_margin_fraction(c);
+  if (c->c.choice_calving_law == DIVA_CALVING_THRESHOLD_THICKNESS) {
+    /* threshold_thickness_calving (calving_module.f90:62-91), twice so that the calving
+     * front may retreat by more than one cell (ice_dynamics_module.f90:562-583) */
+    for (int pass = 0; pass < 2; ++pass) {
+      const int32_t* cf = FI(c, MASK_CF_A);
+      const double* He = FD(c, HI_EFF_CF_A);
+      for (size_t q = 0; q < n; ++q)
+        if (cf[q] == 1 && He[q] < c->c.calving_threshold_thickness) Hi[q] = 0.0;
+      if ((st = orc_update_general_ice_model_data(c))) return st;
+      if (pass == 0) floating_margin_fraction(c);
+    }
+  }
   remove_unconnected_shelves(c);
   const int32_t* noice = FI(c, MASK_NOICE_A);
   for (size_t q = 0; q < n; ++q)

@@ -146,3 +146,16 @@ def test_update_ice_thickness_options_bit_exact(cuda, oracle, flag):
     out = [test_thickness.options_case(be, flag)[1] for be in (cuda, oracle)]
     for k in out[0]:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("law", ["none", "threshold_thickness"])
+def test_calving_bit_exact(cuda, oracle, law):
+    import test_thickness
+    out = []
+    for be in (cuda, oracle):
+        ctx, _ = test_thickness.calving_case(be, law)
+        ctx.pc_finish(1.0)
+        out.append(ctx.download(["Hi_a", "mask_ice_a", "mask_cf_a", "Hi_eff_cf_a", "float_margin_frac_a"]))
+        ctx.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k

@@ -340,3 +340,41 @@ def test_update_ice_thickness_options(flag):
         return
     np.testing.assert_array_equal(o["Hi_a"][grounded & kept], H0[grounded & kept])
     np.testing.assert_array_equal(o["Hi_a"][grounded & ~kept], H0[grounded & ~kept] + 1.0)
+
+
+def calving_case(backend, law):
+    """A grounded sheet (x < 5), a 400 m shelf thinning to 180 / 150 / 120 m over its
+    last three columns, open ocean beyond; dHi_dt_a = 0."""
+    ny, nx = 7, 20
+    g = diva.Grid(nx, ny, 10e3)
+    Hb = np.full((ny, nx), -800.0)
+    Hb[:, :5] = 300.0
+    H = np.zeros((ny, nx))
+    H[:, :14] = np.where(np.arange(14) < 5, 600.0, 400.0)
+    H[:, 14], H[:, 15], H[:, 16] = 180.0, 150.0, 120.0
+    f = {"Hi_a": H, "Hb_a": Hb, "SL_a": np.zeros((ny, nx)), "Ti_a": np.full((g.nz, ny, nx), 260.0)}
+    ctx = diva.Context(g, {"choice_calving_law": law}, backend)
+    ctx.upload({k: np.asfortranarray(v) for k, v in f.items()})
+    ctx.update_general_ice_model_data()
+    ctx.determine_floating_margin_fraction()
+    return ctx, H
+
+
+def test_threshold_thickness_calving_retreats_the_front_two_cells():
+    """threshold_thickness_calving (calving_module.f90:62-91) applied twice per update
+    (ice_dynamics_module.f90:562-583): the 120 m front column goes (its effective
+    thickness is its 150 m neighbour's), then the 150 m column (effective 180 m); the
+    180 m column waits for the next update.  The domain's edge rows are never calving
+    front (the masks leave the border out), so they keep their ice.  With law 'none'
+    nothing calves."""
+    out = {}
+    for law in ("none", "threshold_thickness"):
+        ctx, H = calving_case(ob.oracle_backend(), law)
+        ctx.pc_finish(1.0)
+        out[law] = ctx.download(["Hi_a"])["Hi_a"]
+        ctx.close()
+    np.testing.assert_array_equal(out["none"], H)
+    c = out["threshold_thickness"]
+    assert np.all(c[1:-1, 15:] == 0.0)
+    np.testing.assert_array_equal(c[1:-1, :15], H[1:-1, :15])
+    np.testing.assert_array_equal(c[[0, -1]], H[[0, -1]])
