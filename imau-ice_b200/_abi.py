@@ -93,6 +93,8 @@ class Config(C.Structure):
         ("ocean_temperature_input", C.c_int32),
         ("choice_calving_law", C.c_int32),
         ("calving_threshold_thickness", C.c_double),
+        ("remove_shelves_larger_than_PD", C.c_int32), ("continental_shelf_calving", C.c_int32),
+        ("continental_shelf_min_height", C.c_double),
         ("reserved", C.c_int32 * 8),
     ]
 

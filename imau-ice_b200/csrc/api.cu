@@ -118,6 +118,7 @@ void config_defaults(diva_config_t* c) {
   c->T_ocean_mean_PD_ANT = -1.7;
   c->choice_ice_integration_method = DIVA_INTEGRATION_EXPLICIT; c->dHi_rtol = 1E-10; c->dHi_maxit = 1000;
   c->choice_calving_law = DIVA_CALVING_THRESHOLD_THICKNESS; c->calving_threshold_thickness = 200.0;
+  c->continental_shelf_min_height = -2000.0;
   c->precision = DIVA_PREC_FP64;
 }
 

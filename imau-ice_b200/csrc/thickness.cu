@@ -336,14 +336,23 @@ __global__ void k_calve_threshold(Dims d, const int* cf, const double* Heff, dou
   if (cf[q] == 1 && Heff[q] < thr) Hi[q] = 0.0;
 }
 
+// the removal options of update_ice_thickness with reference geometries (:613-635)
+struct RefGeo {
+  int larger_than_pd, shelf_edge;
+  double shelf_min_height;
+  const double *Hi_pd, *Hb_pd, *Hi_eq, *Hb_eq;
+};
+
 __global__ void k_shelf_remove(Dims d, const int* shelf, const int* reach, const int* noice, int remove_floating,
-                               const double* Hb, const double* SL, double* Hi) {
+                               const double* Hb, const double* SL, RefGeo rg, double* Hi) {
   IDX2D
   if (j >= d.ny || i >= d.nx) return;
   const long long q = d.at(j, i);
   if (shelf[q] == 1 && !reach[q]) Hi[q] = 0.0;
   if (noice[q] == 1) Hi[q] = 0.0;
   if (remove_floating && Hi[q] < (SL[q] - Hb[q]) * kRhoSW / kRhoI) Hi[q] = 0.0;
+  if (rg.larger_than_pd && rg.Hi_pd[q] == 0.0 && rg.Hb_pd[q] < 0.0) Hi[q] = 0.0;
+  if (rg.shelf_edge && rg.Hi_eq[q] == 0.0 && rg.Hb_eq[q] < rg.shelf_min_height) Hi[q] = 0.0;
 }
 
 // ---- the semi-implicit scheme (calc_dHi_dt_semiimplicit, :302-727) ---------------------
@@ -768,8 +777,11 @@ int diva_pc_finish(diva_ctx_t* h, double dt) {
     DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
     if (!changed) break;
   }
+  const RefGeo rg{c->c.remove_shelves_larger_than_PD, c->c.continental_shelf_calving,
+                  c->c.continental_shelf_min_height, c->D(DIVA_F_HI_PD_A), c->D(DIVA_F_HB_PD_A),
+                  c->D(DIVA_F_HI_GIAEQ_A), c->D(DIVA_F_HB_GIAEQ_A)};
   k_shelf_remove<<<G2T>>>(d, shelf, reach, c->I(DIVA_F_MASK_NOICE_A), c->c.do_remove_shelves, c->D(DIVA_F_HB_A),
-                          c->D(DIVA_F_SL_A), c->D(DIVA_F_HI_A)); c->launches++;
+                          c->D(DIVA_F_SL_A), rg, c->D(DIVA_F_HI_A)); c->launches++;
   DIVA_LAUNCHED(c, "k_shelf_remove");
   if (int st = launch_update_general_ice_model_data(c)) return st;
   DIVA_CUDA(c, cudaStreamSynchronize(c->stream));

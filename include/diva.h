@@ -167,6 +167,12 @@ typedef struct {
    * 'threshold_thickness' with 200 m, as in the reference */
   int32_t choice_calving_law;
   double  calving_threshold_thickness;
+  /* remove floating ice where the present-day geometry (Hi_PD_a, Hb_PD_a) has open
+   * ocean; remove ice where the GIA-equilibrium geometry (Hi_GIAeq_a, Hb_GIAeq_a) has
+   * no ice on a bed deeper than continental_shelf_min_height (configuration_module.f90:
+   * 415-417; default off, -2000 m) */
+  int32_t remove_shelves_larger_than_PD, continental_shelf_calving;
+  double  continental_shelf_min_height;
   int32_t reserved[8];
 } diva_config_t;
 
@@ -275,7 +281,10 @@ int  diva_pc_corrector(diva_ctx_t* ctx, double dt, double zeta, double eta_min, 
  * 62-91)]; remove_unconnected_shelves (ice_thickness_module.f90:
  * 932-1044: shelf cells not 4-connected through shelf to a shelf cell next to sheet ice
  * lose their ice); Hi_a = 0 where mask_noice_a (region%mask_noice); [do_remove_shelves:
- * Hi_a = 0 on floating cells]; and update_general_ice_model_data. */
+ * Hi_a = 0 on floating cells]; [remove_shelves_larger_than_PD: Hi_a = 0 where Hi_PD_a = 0
+ * and Hb_PD_a < 0]; [continental_shelf_calving: Hi_a = 0 where Hi_GIAeq_a = 0 and
+ * Hb_GIAeq_a < continental_shelf_min_height] (:600-635); and
+ * update_general_ice_model_data. */
 int  diva_pc_finish(diva_ctx_t* ctx, double dt);
 
 /* run_thermo_model with choice_thermo_model '3D_heat_equation' (thermodynamics_module.f90:

@@ -151,6 +151,13 @@
   X(PC_TAU,               pc_tau,               A,   D)      \
   X(MASK_ICE_A_PREV,      mask_ice_a_prev,      A,   I)      \
   X(MASK_NOICE_A,         mask_noice_a,         A,   I)      \
+  /* reference geometries read by update_ice_thickness's  */ \
+  /* remove_shelves_larger_than_PD / continental_shelf_   */ \
+  /* calving (refgeo_PD, refgeo_GIAeq: Hi and Hb)          */ \
+  X(HI_PD_A,              Hi_PD_a,              A,   D)      \
+  X(HB_PD_A,              Hb_PD_a,              A,   D)      \
+  X(HI_GIAEQ_A,           Hi_GIAeq_a,           A,   D)      \
+  X(HB_GIAEQ_A,           Hb_GIAeq_a,           A,   D)      \
   /* thermodynamics (thermodynamics_module.f90:29-608,   */ \
   /*  derivatives_and_grids_module.f90:1892-2061);       */ \
   /* T_surf_annual_a is SUM(climate%T2m)/12 and GHF_a    */ \

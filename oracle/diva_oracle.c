@@ -2242,6 +2242,7 @@ void orc_config_defaults(diva_config_t* c) {
   c->T_ocean_mean_PD_ANT = -1.7;
   c->choice_ice_integration_method = DIVA_INTEGRATION_EXPLICIT; c->dHi_rtol = 1E-10; c->dHi_maxit = 1000;
   c->choice_calving_law = DIVA_CALVING_THRESHOLD_THICKNESS; c->calving_threshold_thickness = 200.0;
+  c->continental_shelf_min_height = -2000.0;
   c->precision = DIVA_PREC_FP64;
 }
 
@@ -2803,6 +2804,16 @@ int orc_pc_finish(orc_ctx* c, double dt) {
     const double *Hb = FD(c, HB_A), *SL = FD(c, SL_A);
     for (size_t q = 0; q < n; ++q)
       if (is_floating(Hi[q], Hb[q], SL[q])) Hi[q] = 0.0;
+  }
+  if (c->c.remove_shelves_larger_than_PD) {                                  /* :613-622 */
+    const double *Hp = FD(c, HI_PD_A), *Bp = FD(c, HB_PD_A);
+    for (size_t q = 0; q < n; ++q)
+      if (Hp[q] == 0.0 && Bp[q] < 0.0) Hi[q] = 0.0;
+  }
+  if (c->c.continental_shelf_calving) {                                      /* :625-635 */
+    const double *Hg = FD(c, HI_GIAEQ_A), *Bg = FD(c, HB_GIAEQ_A);
+    for (size_t q = 0; q < n; ++q)
+      if (Hg[q] == 0.0 && Bg[q] < c->c.continental_shelf_min_height) Hi[q] = 0.0;
   }
   return orc_update_general_ice_model_data(c);
 }

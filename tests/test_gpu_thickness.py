@@ -159,3 +159,16 @@ def test_calving_bit_exact(cuda, oracle, law):
         ctx.close()
     for k in out[0]:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("flag", ["remove_shelves_larger_than_PD", "continental_shelf_calving"])
+def test_reference_geometry_removal_bit_exact(cuda, oracle, flag):
+    import test_thickness
+    out = []
+    for be in (cuda, oracle):
+        ctx, _ = test_thickness.refgeo_case(be, flag)
+        ctx.pc_finish(1.0)
+        out.append(ctx.download(["Hi_a", "mask_ice_a", "mask_shelf_a"]))
+        ctx.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k

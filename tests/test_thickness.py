@@ -378,3 +378,30 @@ def test_threshold_thickness_calving_retreats_the_front_two_cells():
     assert np.all(c[1:-1, 15:] == 0.0)
     np.testing.assert_array_equal(c[1:-1, :15], H[1:-1, :15])
     np.testing.assert_array_equal(c[[0, -1]], H[[0, -1]])
+
+
+def refgeo_case(backend, flag):
+    ctx, H = calving_case(backend, "none")
+    ny, nx = H.shape
+    Hpd, Bpd = H.copy(), np.full((ny, nx), -800.0)
+    Hpd[:, 10:] = 0.0                                  # the present-day front at x = 10
+    Heq, Beq = H.copy(), np.full((ny, nx), -800.0)
+    Heq[:, 12:] = 0.0
+    Beq[:, 12:] = -2500.0                              # beyond the shelf edge from x = 12
+    ctx.upload({k: np.asfortranarray(v) for k, v in
+                {"Hi_PD_a": Hpd, "Hb_PD_a": Bpd, "Hi_GIAeq_a": Heq, "Hb_GIAeq_a": Beq}.items()})
+    ctx.set_config({"choice_calving_law": "none", flag: 1})
+    return ctx, H
+
+
+@pytest.mark.parametrize("flag,edge", [("remove_shelves_larger_than_PD", 10), ("continental_shelf_calving", 12)])
+def test_reference_geometry_removal(flag, edge):
+    """remove_shelves_larger_than_PD / continental_shelf_calving (ice_dynamics_module.f90:
+    613-635): ice goes where the reference geometry has open ocean (PD) or no ice on a bed
+    below continental_shelf_min_height (GIA equilibrium)."""
+    ctx, H = refgeo_case(ob.oracle_backend(), flag)
+    ctx.pc_finish(1.0)
+    o = ctx.download(["Hi_a"])["Hi_a"]
+    ctx.close()
+    assert np.all(o[:, edge:] == 0.0)
+    np.testing.assert_array_equal(o[:, :edge], H[:, :edge])
