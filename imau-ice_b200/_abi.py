@@ -160,6 +160,7 @@ def bind(lib, prefix):
         "pc_predictor": (C.c_int, [vp, C.c_double, C.c_double]),
         "pc_corrector": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, dp]),
         "pc_finish": (C.c_int, [vp, C.c_double]),
+        "apply_prescribed_retreat_mask": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
         "run_thermo_model": (C.c_int, [vp, i32, C.POINTER(C.c_int32)]),
         "last_error": (C.c_char_p, [vp]),
     }

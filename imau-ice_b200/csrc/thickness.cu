@@ -327,6 +327,27 @@ __global__ void k_shelf_spread(Dims d, const int* shelf, int* reach, int* change
   }
 }
 // then the no-ice mask (:586-592) and, with do_remove_shelves, all floating ice (:600-608)
+// apply_prescribed_retreat_mask (calving_module.f90:125-136): the mask at the model time
+__global__ void k_retreat_interp(Dims d, double wt0, const double* m0, const double* m1, double* m) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= d.ny || i >= d.nx) return;
+  const long long q = d.at(j, i);
+  m[q] = (wt0 * m0[q]) + ((1.0 - wt0) * m1[q]);
+}
+
+// (:139-164): cap the thickness where the mask has retreat, and at interior cells next to it
+__global__ void k_retreat_apply(Dims d, const double* m, const double* Href, double* Hi) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= d.ny || i >= d.nx) return;
+  const long long q = d.at(j, i);
+  bool cap = m[q] < 0.999;
+  if (!cap && i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1)
+    for (int di = -1; di <= 1; ++di)
+      for (int dj = -1; dj <= 1; ++dj)
+        if ((di || dj) && m[d.at(j + dj, i + di)] < 0.999) cap = true;
+  if (cap) Hi[q] = fmin(Hi[q], Href[q] * m[q]);
+}
+
 // threshold_thickness_calving (calving_module.f90:62-91): calving-front cells whose
 // effective thickness is below the threshold lose their ice
 __global__ void k_calve_threshold(Dims d, const int* cf, const double* Heff, double thr, double* Hi) {
@@ -783,6 +804,21 @@ int diva_pc_finish(diva_ctx_t* h, double dt) {
   k_shelf_remove<<<G2T>>>(d, shelf, reach, c->I(DIVA_F_MASK_NOICE_A), c->c.do_remove_shelves, c->D(DIVA_F_HB_A),
                           c->D(DIVA_F_SL_A), rg, c->D(DIVA_F_HI_A)); c->launches++;
   DIVA_LAUNCHED(c, "k_shelf_remove");
+  if (int st = launch_update_general_ice_model_data(c)) return st;
+  DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DIVA_OK;
+}
+
+int diva_apply_prescribed_retreat_mask(diva_ctx_t* h, double time, double t0, double t1) {
+  if (!h || !(t1 > t0)) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  const double wt0 = fmax(0.0, fmin(1.0, (t1 - time) / (t1 - t0)));
+  k_retreat_interp<<<G2T>>>(c->d, wt0, c->D(DIVA_F_RETREAT_MASK0_A), c->D(DIVA_F_RETREAT_MASK1_A),
+                            c->D(DIVA_F_RETREAT_MASK_A)); c->launches++;
+  DIVA_LAUNCHED(c, "k_retreat_interp");
+  k_retreat_apply<<<G2T>>>(c->d, c->D(DIVA_F_RETREAT_MASK_A), c->D(DIVA_F_RETREAT_MASK_HI_REF_A),
+                           c->D(DIVA_F_HI_A)); c->launches++;
+  DIVA_LAUNCHED(c, "k_retreat_apply");
   if (int st = launch_update_general_ice_model_data(c)) return st;
   DIVA_CUDA(c, cudaStreamSynchronize(c->stream));
   return DIVA_OK;

@@ -288,6 +288,12 @@ class Context:
         """Hi_tplusdt_a and the thickness update of the step (:429-431, :435-648 in part)."""
         self._check(self.backend.fns["pc_finish"](self.h, float(dt)), "pc_finish")
 
+    def apply_prescribed_retreat_mask(self, time, t0, t1):
+        """apply_prescribed_retreat_mask (calving_module.f90:96-169) at model ``time``
+        between the uploaded frames at t0 and t1; call after pc_finish."""
+        self._check(self.backend.fns["apply_prescribed_retreat_mask"](self.h, float(time), float(t0), float(t1)),
+                    "apply_prescribed_retreat_mask")
+
     def run_thermo_model(self, do_solve_heat_equation=True):
         """run_thermo_model with the 3D heat equation (thermodynamics_module.f90:29-121);
         returns the number of unstable columns replaced by the Robin solution."""

@@ -23,7 +23,7 @@ class PCTimeStepper:
     478-545 and ice_dynamics_module.f90:987-996 for the initial values)."""
 
     def __init__(self, ctx, start_time, end_time, dt_min=0.01, dt_max=10.0, dt_startup_phase=10.0,
-                 pc_epsilon=0.5, pc_k_I=0.2, pc_k_p=0.2, pc_eta_min=1e-8, thermo=False):
+                 pc_epsilon=0.5, pc_k_I=0.2, pc_k_p=0.2, pc_eta_min=1e-8, thermo=False, retreat_frames=None):
         self.ctx = ctx
         self.start_time, self.end_time = float(start_time), float(end_time)
         self.dt_min, self.dt_max, self.dt_startup_phase = float(dt_min), float(dt_max), float(dt_startup_phase)
@@ -44,6 +44,9 @@ class PCTimeStepper:
         self.t_next_thermo = self.start_time + self.dt_thermo
         self.do_thermo = False
         self.thermo_solves = 0
+        # do_apply_prescribed_retreat_mask: the times (t0, t1) of the two mask frames the
+        # caller has uploaded (it replaces them and this pair as the model time moves on)
+        self.retreat_frames = retreat_frames
 
     def _dt_max_now(self):
         """The start-up / wind-down cap of the time step (ice_dynamics_module.f90:292-299)."""
@@ -94,6 +97,8 @@ class PCTimeStepper:
             self.ctx.run_thermo_model(self.do_thermo)
             self.thermo_solves += int(self.do_thermo)
         self.ctx.pc_finish(self.dt)
+        if self.retreat_frames is not None:            # the end of update_ice_thickness (:637-640)
+            self.ctx.apply_prescribed_retreat_mask(self.time, *self.retreat_frames)
         self.time = self.time + self.dt
         return self.dt
 

@@ -287,6 +287,17 @@ int  diva_pc_corrector(diva_ctx_t* ctx, double dt, double zeta, double eta_min, 
  * update_general_ice_model_data. */
 int  diva_pc_finish(diva_ctx_t* ctx, double dt);
 
+/* apply_prescribed_retreat_mask (calving_module.f90:96-169), the last removal step of
+ * update_ice_thickness when do_apply_prescribed_retreat_mask is set; call it after
+ * diva_pc_finish.  The caller reads the mask's time frames (NetCDF in the reference)
+ * and uploads them as ice_fraction_retreat_mask0_a / _mask1_a with the reference
+ * thickness retreat_mask_Hi_ref_a; t0 < t1 are the frames' times.  On the device:
+ * ice_fraction_retreat_mask_a = wt0 mask0 + (1 - wt0) mask1 with wt0 = clamp((t1 -
+ * time) / (t1 - t0), 0, 1); Hi_a = min(Hi_a, Hi_ref * mask) where the mask is below
+ * 0.999, and also at interior cells whose mask is not but a neighbour's is (3 x 3);
+ * then update_general_ice_model_data. */
+int  diva_apply_prescribed_retreat_mask(diva_ctx_t* ctx, double time, double t0, double t1);
+
 /* run_thermo_model with choice_thermo_model '3D_heat_equation' (thermodynamics_module.f90:
  * 29-121): temperature of newly ice-covered columns from their upwind neighbour,
  * frictional heating, heat capacity, conductivity, pressure melting point, then (when

@@ -158,6 +158,13 @@
   X(HB_PD_A,              Hb_PD_a,              A,   D)      \
   X(HI_GIAEQ_A,           Hi_GIAeq_a,           A,   D)      \
   X(HB_GIAEQ_A,           Hb_GIAeq_a,           A,   D)      \
+  /* prescribed retreat mask (calving_module.f90:96-169): */ \
+  /* the two time frames, the reference thickness, and   */ \
+  /* the mask interpolated to the model time (output)    */ \
+  X(RETREAT_MASK0_A,      ice_fraction_retreat_mask0_a, A, D)  \
+  X(RETREAT_MASK1_A,      ice_fraction_retreat_mask1_a, A, D)  \
+  X(RETREAT_MASK_HI_REF_A, retreat_mask_Hi_ref_a,       A, D)  \
+  X(RETREAT_MASK_A,       ice_fraction_retreat_mask_a,  A, D)  \
   /* thermodynamics (thermodynamics_module.f90:29-608,   */ \
   /*  derivatives_and_grids_module.f90:1892-2061);       */ \
   /* T_surf_annual_a is SUM(climate%T2m)/12 and GHF_a    */ \

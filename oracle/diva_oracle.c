@@ -2818,6 +2818,30 @@ int orc_pc_finish(orc_ctx* c, double dt) {
   return orc_update_general_ice_model_data(c);
 }
 
+/* apply_prescribed_retreat_mask, calving_module.f90:96-169 (frames read by the caller) */
+int orc_apply_prescribed_retreat_mask(orc_ctx* c, double time, double t0, double t1) {
+  DECL_DIMS(c);
+  if (!(t1 > t0)) return DIVA_BAD_INPUT;
+  const double wt0 = fmax(0.0, fmin(1.0, (t1 - time) / (t1 - t0))), wt1 = 1.0 - wt0;
+  const double *m0 = FD(c, RETREAT_MASK0_A), *m1 = FD(c, RETREAT_MASK1_A), *Href = FD(c, RETREAT_MASK_HI_REF_A);
+  double *m = FD(c, RETREAT_MASK_A), *Hi = FD(c, HI_A);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) m[IA(j, i)] = (wt0 * m0[IA(j, i)]) + (wt1 * m1[IA(j, i)]);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const size_t q = IA(j, i);
+      if (m[q] < 0.999) Hi[q] = fmin(Hi[q], Href[q] * m[q]);
+      if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && m[q] >= 0.999) {
+        int any = 0;
+        for (int di = -1; di <= 1; ++di)
+          for (int dj = -1; dj <= 1; ++dj)
+            if ((di || dj) && m[IA(j + dj, i + di)] < 0.999) any = 1;
+        if (any) Hi[q] = fmin(Hi[q], Href[q] * m[q]);
+      }
+    }
+  return orc_update_general_ice_model_data(c);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Thermodynamics: run_thermo_model with the 3D heat equation                */
 

@@ -172,3 +172,15 @@ def test_reference_geometry_removal_bit_exact(cuda, oracle, flag):
         ctx.close()
     for k in out[0]:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_prescribed_retreat_mask_bit_exact(cuda, oracle):
+    import test_thickness
+    out = []
+    for be in (cuda, oracle):
+        ctx = test_thickness.retreat_case(be)[0]
+        ctx.apply_prescribed_retreat_mask(25.0, 0.0, 100.0)
+        out.append(ctx.download(["Hi_a", "ice_fraction_retreat_mask_a", "mask_ice_a"]))
+        ctx.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k

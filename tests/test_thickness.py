@@ -405,3 +405,39 @@ def test_reference_geometry_removal(flag, edge):
     ctx.close()
     assert np.all(o[:, edge:] == 0.0)
     np.testing.assert_array_equal(o[:, :edge], H[:, :edge])
+
+
+def retreat_case(backend):
+    ctx, H = calving_case(backend, "none")
+    ny, nx = H.shape
+    m0, m1 = np.ones((ny, nx)), np.ones((ny, nx))
+    m1[:, 12:] = 0.0                                   # the later frame has retreated to x = 12
+    m1[:, 11] = 0.5
+    Href = np.full((ny, nx), 300.0)
+    ctx.upload({k: np.asfortranarray(v) for k, v in {"ice_fraction_retreat_mask0_a": m0,
+                                                      "ice_fraction_retreat_mask1_a": m1,
+                                                      "retreat_mask_Hi_ref_a": Href}.items()})
+    return ctx, H, m0, m1, Href
+
+
+def test_prescribed_retreat_mask_caps_the_thickness():
+    """apply_prescribed_retreat_mask (calving_module.f90:96-169) a quarter of the way from
+    the frame at t0 = 0 to the one at t1 = 100: mask = 0.75 m0 + 0.25 m1; thickness
+    capped at Href * mask where the mask is below 0.999 and at interior cells next to
+    such a cell; elsewhere untouched."""
+    ctx, H, m0, m1, Href = retreat_case(ob.oracle_backend())
+    ctx.apply_prescribed_retreat_mask(25.0, 0.0, 100.0)
+    o = ctx.download(["Hi_a", "ice_fraction_retreat_mask_a"])
+    ctx.close()
+    m = 0.75 * m0 + 0.25 * m1
+    np.testing.assert_array_equal(o["ice_fraction_retreat_mask_a"], m)
+    ny, nx = H.shape
+    low = m < 0.999
+    near = np.zeros_like(low)
+    for dj in (-1, 0, 1):
+        for di in (-1, 0, 1):
+            near[1:-1, 1:-1] |= np.roll(np.roll(low, dj, 0), di, 1)[1:-1, 1:-1]
+    capped = low | near
+    want = np.where(capped, np.minimum(H, Href * m), H)
+    np.testing.assert_array_equal(o["Hi_a"], want)
+    assert capped[3, 10] and not capped[3, 9] and o["Hi_a"][3, 10] == 300.0
