@@ -713,18 +713,30 @@ __global__ void k_targets(Dims d, StatePtrs s, float* tgt, int Hp, int Wp) {
   for (int o = 0; o < kOut; ++o) tgt[((long)y * Wp + x) * kOut + o] = t[o];
 }
 
-// the predicted state into the context's fields; velocities_only: u_vav_cx and v_vav_cy
-__global__ void k_apply(Dims d, const float* pred, StatePtrs s, int Wp, int velocities_only) {
+// an output clamped to [-lim, lim]; a non-finite one becomes 0
+__device__ __forceinline__ double clamp_out(float v, double lim) {
+  const double x = (double)v;
+  return x == x ? fmax(-lim, fmin(lim, x)) : 0.0;
+}
+
+// the predicted state into the context's fields, within physical bounds (velocities
+// within the solver's DIVA_vel_max, |taub| <= 1e7 Pa, viscosity in [1e3, 1e18]) so that
+// a poorly trained network cannot hand the solve an overflow; velocities_only: u, v
+__global__ void k_apply(Dims d, const float* pred, StatePtrs s, int Wp, int velocities_only, double vmax) {
   const int y = blockIdx.x * blockDim.x + threadIdx.x;
   const int x = blockIdx.y * blockDim.y + threadIdx.y;
   if (y >= d.ny || x >= d.nx) return;
   const float* q = pred + ((long)y * Wp + x) * kOut;
-  if (x < d.nx - 1) s.ucx[d.at(y, x)] = kVelScale * sinh((double)q[0]);
-  if (y < d.ny - 1) s.vcy[d.at(y, x)] = kVelScale * sinh((double)q[1]);
+  const double ulim = asinh(vmax / kVelScale), tlim = asinh(1e7 / kTauScale);
+  if (x < d.nx - 1) s.ucx[d.at(y, x)] = kVelScale * sinh(clamp_out(q[0], ulim));
+  if (y < d.ny - 1) s.vcy[d.at(y, x)] = kVelScale * sinh(clamp_out(q[1], ulim));
   if (velocities_only) return;
-  if (x < d.nx - 1) s.tbx[d.at(y, x)] = kTauScale * sinh((double)q[2]);
-  if (y < d.ny - 1) s.tby[d.at(y, x)] = kTauScale * sinh((double)q[3]);
-  for (int k = 0; k < d.nz; ++k) s.visc[k * d.plane + d.at(y, x)] = pow(10.0, (double)q[4 + k] + kViscShift);
+  if (x < d.nx - 1) s.tbx[d.at(y, x)] = kTauScale * sinh(clamp_out(q[2], tlim));
+  if (y < d.ny - 1) s.tby[d.at(y, x)] = kTauScale * sinh(clamp_out(q[3], tlim));
+  for (int k = 0; k < d.nz; ++k) {
+    const double l = fmax(3.0 - kViscShift, fmin(18.0 - kViscShift, clamp_out(q[4 + k], 1e30)));
+    s.visc[k * d.plane + d.at(y, x)] = pow(10.0, l + kViscShift);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1189,7 +1201,7 @@ int32_t diva_cnn_predict(diva_cnn_t* N, diva_ctx_t* ctx, int32_t complete_sweeps
                                                                    N->Wp);
   RET(forward(N, N->act[T_IN], N->out, 1, c->stream));
   k_apply<<<img_grid(N->ny, N->nx), block2d(), 0, c->stream>>>(c->d, N->out, state_ptrs(c), N->Wp,
-                                                                complete_sweeps > 0);
+                                                                complete_sweeps > 0, c->c.DIVA_vel_max);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   RET(check_err(N));
@@ -1252,6 +1264,10 @@ int32_t diva_cnn_train(diva_cnn_t* N, int32_t epochs, float lr, uint64_t seed, f
     double sum = 0.0;
     for (int b = 0; b < nb; ++b) sum += batch_loss[b];
     last = sum / (double)N->valid(N->nsamples);
+    if (!(last == last) || std::isinf(last)) {   // diverged: the weights are no longer usable
+      if (loss) *loss = (float)last;
+      return DIVA_NAN_DETECTED;
+    }
   }
   if (loss) *loss = (float)last;
   return DIVA_OK;

@@ -75,7 +75,8 @@ int32_t diva_cnn_num_samples(const diva_cnn_t* net, int32_t* n);
 
 /* `epochs` passes of Adam (lr, beta1 0.9, beta2 0.999, eps 1e-8) over the training
  * set in minibatches, the order shuffled from `seed`; *loss = mean masked squared
- * error of the last epoch. */
+ * error of the last epoch.  DIVA_NAN_DETECTED if an epoch's loss is not finite
+ * (training diverged; reset the weights with diva_cnn_weights before using them). */
 int32_t diva_cnn_train(diva_cnn_t* net, int32_t epochs, float lr, uint64_t seed, float* loss);
 
 /* Warm-start the context from the network's prediction for its current fields.
