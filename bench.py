@@ -559,6 +559,7 @@ def run_learned(args):
 
     grid = case(0, "fp64")[0]
     net = learned.WarmStartNet(grid, batch=8, capacity=args.members, seed=0)
+    net.velocities_only()                  # predict below completes the rest of the state
     t0 = time.perf_counter()
     seed = 0
     while net.num_samples < args.members and seed < 4 * args.members:

@@ -559,9 +559,13 @@ __device__ __forceinline__ bool out_valid(int o, int x, int y, int nx, int ny, i
   if (o == 1 || o == 3) return y < ny - 1 && x < nx;
   return o < 4 + nz && x < nx && y < ny;
 }
+struct LossWeights {
+  float w[kOut];
+};
+
 __global__ void __launch_bounds__(128) k_head(const bf16* d1, const float* wh, const float* bh, float* out,
                                               const float* tgt, float* dout, bf16* gd1, float* part, int n, int H,
-                                              int W, int ny, int nx, int nz, float inv_count) {
+                                              int W, int ny, int nx, int nz, float inv_count, LossWeights lw) {
   __shared__ float red[4];
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long npix = (long)n * H * W;
@@ -595,8 +599,8 @@ __global__ void __launch_bounds__(128) k_head(const bf16* d1, const float* wh, c
 #pragma unroll
       for (int j = 0; j < kOut; ++j) {
         const float e = out_valid(j, x, y, nx, ny, nz) ? o[j] - tgt[p * kOut + j] : 0.0f;
-        const float g = 2.0f * e * inv_count;
-        se += e * e;
+        const float g = 2.0f * lw.w[j] * e * inv_count;
+        se += lw.w[j] * e * e;
         dout[p * kOut + j] = g;
 #pragma unroll
         for (int c = 0; c < kHeadC; ++c) gd[c] = fmaf(g, wh[j * kHeadC + c], gd[c]);
@@ -842,6 +846,7 @@ struct diva_cnn {
   float* ds_tgt = nullptr;
   int* err = nullptr;
   long adam_t = 0;
+  LossWeights lw{};
 
   // valid output entries of n samples (the loss is their mean squared error)
   long valid(int n) const {
@@ -909,7 +914,8 @@ int forward(diva_cnn_t* N, const bf16* in, float* out, int n, cudaStream_t st) {
   if (out) {
     const long npix = (long)n * N->Hp * N->Wp;
     k_head<<<nblk(npix, 128), 128, 0, st>>>(N->act[T_D1], N->w + N->head_w, N->w + N->head_b, out, nullptr,
-                                            nullptr, nullptr, nullptr, n, N->Hp, N->Wp, N->ny, N->nx, N->nz, 0.0f);
+                                            nullptr, nullptr, nullptr, n, N->Hp, N->Wp, N->ny, N->nx, N->nz, 0.0f,
+                                            N->lw);
   }
   CK(cudaGetLastError());
   return DIVA_OK;
@@ -922,7 +928,7 @@ int backward(diva_cnn_t* N, const bf16* in, const float* tgt, int n, cudaStream_
   if ((long)hb > N->part_floats - 128 || (long)kHeadBlocks * kHeadGrad > N->part_floats - 128) return DIVA_BAD_INPUT;
   k_head<<<hb, 128, 0, st>>>(N->act[T_D1], N->w + N->head_w, N->w + N->head_b, nullptr, tgt, N->dout,
                              N->grad[T_D1], N->part, n, N->Hp, N->Wp, N->ny, N->nx, N->nz,
-                             1.0f / (float)N->valid(n));
+                             1.0f / (float)N->valid(n), N->lw);
   k_sum_rows<<<1, 32, 0, st>>>(N->part, (int)hb, 1, loss_dst);
   k_head_wgrad<<<kHeadBlocks, kHeadGrad, 0, st>>>(N->dout, N->act[T_D1], npix0, kHeadBlocks, N->part);
   k_sum_rows<<<nblk(kHeadGrad, 256), 256, 0, st>>>(N->part, kHeadBlocks, kHeadGrad, N->g + N->head_w);
@@ -1029,6 +1035,7 @@ int32_t diva_cnn_create(diva_cnn_t** out, int32_t ny, int32_t nx, int32_t nz, in
   N->Wp = (nx + 3) / 4 * 4;
   N->batch = batch;
   N->capacity = capacity;
+  for (int o = 0; o < kOut; ++o) N->lw.w[o] = 1.0f;
   long off = 0;
   for (int l = 0; l < kNL; ++l) {
     Layer& ly = N->L[l];
@@ -1172,6 +1179,15 @@ int32_t diva_cnn_grads(diva_cnn_t* N, float* host, int64_t n) {
   if (!N || !host || n != N->nw) return DIVA_BAD_INPUT;
   CK(cudaStreamSynchronize(N->stream));
   CK(cudaMemcpy(host, N->g, n * 4, cudaMemcpyDeviceToHost));
+  return DIVA_OK;
+}
+
+int32_t diva_cnn_set_loss_weights(diva_cnn_t* N, const float* w, int32_t n) {
+  if (!N || !w || n != kOut) return DIVA_BAD_INPUT;
+  for (int o = 0; o < kOut; ++o)
+    if (!(w[o] >= 0.0f) || std::isinf(w[o])) return DIVA_BAD_INPUT;
+  CK(cudaStreamSynchronize(N->stream));
+  for (int o = 0; o < kOut; ++o) N->lw.w[o] = w[o];
   return DIVA_OK;
 }
 

@@ -52,6 +52,7 @@ def _bind(lib):
         "forward": [vp, vp, vp, i32],
         "train_step": [vp, vp, vp, i32, C.c_float, f32p],
         "grads": [vp, f32p, i64],
+        "set_loss_weights": [vp, f32p, i32],
     }
     fns = {}
     for name, args in sig.items():
@@ -131,6 +132,18 @@ class WarmStartNet:
         n = C.c_int32()
         self._check(self._f["num_samples"](self._h, C.byref(n)), "num_samples")
         return n.value
+
+    def set_loss_weights(self, w):
+        """Loss weight of each of the N_OUT output channels (>= 0)."""
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(self._f["set_loss_weights"](self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size),
+                    "set_loss_weights")
+
+    def velocities_only(self):
+        """Train on the velocity channels alone (what predict's default mode uses)."""
+        w = np.zeros(N_OUT, np.float32)
+        w[:2] = 1.0
+        self.set_loss_weights(w)
 
     def train(self, epochs, lr=1e-3, seed=0):
         """Adam over the training set; returns the last epoch's mean squared error."""

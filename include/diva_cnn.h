@@ -30,7 +30,7 @@
  * 2 asinh(taub_cx(j,i) / 1000 Pa) for i < nx-1; 1 asinh(v_vav_cy(j,i) / 10 m/yr) and
  * 3 asinh(taub_cy(j,i) / 1000 Pa) for j < ny-1; 4+k log10(visc_eff_3D_a(k,j,i)) - 8 for
  * the nz <= 16 layers; the remaining channels are unused.  The training loss is the
- * mean squared error over the valid entries.
+ * weighted sum of squared errors over the valid entries divided by their number.
  *
  * Arithmetic: BF16 activations and weights, FP32 accumulation in tensor memory
  * (tcgen05.mma, kind::f16), FP32 master weights and Adam moments.
@@ -72,6 +72,12 @@ int32_t diva_cnn_weights(diva_cnn_t* net, float* host, int64_t n, int32_t direct
  * grid size. */
 int32_t diva_cnn_add_sample(diva_cnn_t* net, diva_ctx_t* ctx);
 int32_t diva_cnn_num_samples(const diva_cnn_t* net, int32_t* n);
+
+/* Weights of the 20 output channels in the training loss (default 1 each; >= 0).  The
+ * default predict mode uses only channels 0 and 1 (the velocities, the rest of the
+ * state completed from them), so weights {1, 1, 0, ...} spend the network's capacity
+ * on those. */
+int32_t diva_cnn_set_loss_weights(diva_cnn_t* net, const float* w, int32_t n);
 
 /* `epochs` passes of Adam (lr, beta1 0.9, beta2 0.999, eps 1e-8) over the training
  * set in minibatches, the order shuffled from `seed`; *loss = mean masked squared

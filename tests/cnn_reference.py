@@ -62,9 +62,12 @@ def valid_mask(Hp, Wp, ny, nx, nz):
     return m
 
 
-def loss(out, tgt, mask):
-    e = (out - tgt) * torch.as_tensor(np.array(mask), dtype=out.dtype)
-    return (e * e).sum() / float(mask.sum())
+def loss(out, tgt, mask, weights=None):
+    """sum over valid entries of w_channel (out - tgt)^2, divided by the number of valid entries."""
+    m = torch.as_tensor(np.array(mask), dtype=out.dtype)
+    w = torch.ones(out.shape[-1]) if weights is None else torch.as_tensor(np.asarray(weights, np.float32))
+    e = (out - tgt) * m
+    return (w * e * e).sum() / float(mask.sum())
 
 
 def features(f, Hp, Wp):

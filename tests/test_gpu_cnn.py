@@ -48,13 +48,18 @@ def test_forward_matches_the_reference():
 
 
 @pytest.mark.gpu_pending
-def test_gradients_match_autograd():
+@pytest.mark.parametrize("velocities_only", [False, True])
+def test_gradients_match_autograd(velocities_only):
     g, net = small_net()
     feat, tgt = random_batch(net, 2, 1)
+    lw = np.ones(learned.N_OUT, np.float32)
+    if velocities_only:
+        net.velocities_only()
+        lw[2:] = 0.0
     w = torch.as_tensor(net.get_weights()).requires_grad_(True)
     mask = ref.valid_mask(*net.padded_shape, g.ny, g.nx, g.nz)
     mask = np.broadcast_to(mask, (2,) + mask.shape)
-    loss_ref = ref.loss(ref.forward(feat, w, bf16=True), torch.as_tensor(tgt), mask)
+    loss_ref = ref.loss(ref.forward(feat, w, bf16=True), torch.as_tensor(tgt), mask, lw)
     loss_ref.backward()
     gref = w.grad.numpy()
     f, t = dev(feat, torch.bfloat16), dev(tgt, torch.float32)    # held: the kernels read them
@@ -117,6 +122,7 @@ def test_warm_start_from_the_trained_network_cuts_iterations():
 
     grid = case(0)[0]
     net = learned.WarmStartNet(grid, batch=8, capacity=96, seed=0)
+    net.velocities_only()                   # predict's default mode completes the rest
     seed = 0
     while net.num_samples < 96:
         _, cfg, fl = case(seed)
