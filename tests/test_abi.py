@@ -48,22 +48,28 @@ def test_struct_layout_matches_ctypes(tmp_path):
 #include <stdio.h>
 #include <stddef.h>
 #include "diva.h"
+#include "diva_cnn.h"
 int main(void) {
   printf("%zu %zu %zu %zu\n", sizeof(diva_grid_t), sizeof(diva_config_t), sizeof(diva_report_t), sizeof(diva_fields_t));
   printf("%zu %zu %zu %zu\n", offsetof(diva_config_t, lin_rtol), offsetof(diva_config_t, precision),
          offsetof(diva_config_t, prescribed_tauc), offsetof(diva_report_t, elapsed_ms));
   printf("%d\n", (int)DIVA_NUM_FIELDS);
+  printf("%zu %zu %zu\n", offsetof(diva_config_t, calving_threshold_thickness),
+         offsetof(diva_config_t, continental_shelf_min_height), offsetof(diva_config_t, reserved));
   return 0;
 }
 ''')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
-    a, b, n = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")[:3]
+    a, b, n, tail = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")[:4]
     sizes = [int(x) for x in a.split()]
     offs = [int(x) for x in b.split()]
     assert sizes[:3] == [C.sizeof(_abi.Grid), C.sizeof(_abi.Config), C.sizeof(_abi.Report)]
     assert offs == [_abi.Config.lin_rtol.offset, _abi.Config.precision.offset, _abi.Config.prescribed_tauc.offset,
                     _abi.Report.elapsed_ms.offset]
+    assert [int(x) for x in tail.split()] == [_abi.Config.calving_threshold_thickness.offset,
+                                              _abi.Config.continental_shelf_min_height.offset,
+                                              _abi.Config.reserved.offset]
     assert sizes[3] == int(n) * C.sizeof(C.c_void_p)
 
 
