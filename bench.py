@@ -530,8 +530,8 @@ def run_learned(args):
     """Learned warm start workload (the ice cap 321 x 561 x 15, seeded geometries):
     solve --members training caps (seeds 0..) with the plain FP64 path and keep them
     on the device, train the warm-start network on them, then time --steps held-out
-    caps (seeds 10000..) both ways -- cold FP64, and network prediction + state
-    completion + solve at --precision -- each to rel-res 1e-6.  value = learned
+    caps (seeds 10000..) both ways -- cold FP64, and network prediction + 10 state-
+    completion sweeps + solve at --precision -- each to rel-res 1e-6.  value = learned
     solves/s; the cold FP64 rate and the iteration counts ride along.  Device-
     synchronised wall clock around each whole solve call (inputs already resident)."""
     import numpy as np
@@ -578,7 +578,7 @@ def run_learned(args):
         torch.cuda.synchronize()
         t = time.perf_counter()
         if use_net:
-            net.predict(ctx, complete_sweeps=30)
+            net.predict(ctx, complete_sweeps=10)
         rep = ctx.solve_DIVA()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t
@@ -601,7 +601,7 @@ def run_learned(args):
         "warmup": args.warmup, "ms_per_step": 1000.0 * t_warm / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
         "data": "synthetic (seeded ice caps; training seeds 0.., held-out seeds 10000..)",
-        "config": {"workload": "held-out ice caps 1600x2800 km @5 km, network warm start + 30 completion sweeps",
+        "config": {"workload": "held-out ice caps 1600x2800 km @5 km, network warm start + 10 completion sweeps",
                    "plain_fp64_solves_per_s": args.steps / t_cold,
                    "iterations_cold": [r["picard_iterations"] for _, r in cold],
                    "iterations_learned": [r["picard_iterations"] for _, r in warm],

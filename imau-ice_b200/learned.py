@@ -151,7 +151,7 @@ class WarmStartNet:
         self._check(self._f["train"](self._h, int(epochs), float(lr), C.c_uint64(seed), C.byref(loss)), "train")
         return loss.value
 
-    def predict(self, ctx, complete_sweeps=30):
+    def predict(self, ctx, complete_sweeps=10):
         """Warm-start ``ctx`` (call before solve_DIVA): the predicted velocities plus
         ``complete_sweeps`` state-completion sweeps, or with 0 the whole predicted state."""
         self._check(self._f["predict"](self._h, ctx.h, int(complete_sweeps)), "predict")

@@ -89,8 +89,9 @@ int32_t diva_cnn_train(diva_cnn_t* net, int32_t epochs, float lr, uint64_t seed,
  * complete_sweeps > 0: set u_vav_cx and v_vav_cy from the prediction, then derive the
  * viscosity and basal stress that belong to them with diva_complete_state(ctx,
  * complete_sweeps) (the more robust choice: measured on 20 km ice caps with the
- * oracle, 30 sweeps after a predicted velocity field cut the viscosity iterations by
- * a fifth and lengthened one case of twenty).  complete_sweeps = 0: set all five
+ * oracle, 10 sweeps after a predicted velocity field cut the viscosity iterations by
+ * a fifth and lengthened one case of twenty; 30 or 60 sweeps gained one iteration
+ * more, because the guess's own error dominates).  complete_sweeps = 0: set all five
  * state fields from the prediction.  On the context's stream, synchronised before
  * return. */
 int32_t diva_cnn_predict(diva_cnn_t* net, diva_ctx_t* ctx, int32_t complete_sweeps);

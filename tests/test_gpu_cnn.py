@@ -109,7 +109,7 @@ def test_training_lowers_the_loss_and_predict_writes_the_state():
 @pytest.mark.gpu_pending
 def test_warm_start_from_the_trained_network_cuts_iterations():
     """Ice caps at 20 km (friction x4): train on 96 solved members, then the held-out
-    members converge to the same tolerance from the prediction (velocities plus 30
+    members converge to the same tolerance from the prediction (velocities plus 10
     state-completion sweeps) in fewer viscosity iterations than from cold, to the same
     velocities."""
     def case(seed):
