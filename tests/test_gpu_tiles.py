@@ -17,6 +17,7 @@ def solve(edges=None, tune=False):
                                                         "DIVA_visc_it_nit": 300, "lin_adaptive": 1})
     ctx = diva.Context(g, cfg)
     helpers.prepare(ctx, f)
+    ctx.nonlinear_residual()        # what the tuner does first: every run starts from the same state
     if edges is not None:
         ctx.set_tile_edges(edges)
     chosen = autotune.tune_tile_edges(ctx, reps=5, trials=1)[0] if tune else ctx.get_tile_edges()
