@@ -441,3 +441,17 @@ def test_prescribed_retreat_mask_caps_the_thickness():
     want = np.where(capped, np.minimum(H, Href * m), H)
     np.testing.assert_array_equal(o["Hi_a"], want)
     assert capped[3, 10] and not capped[3, 9] and o["Hi_a"][3, 10] == 300.0
+
+
+def test_bad_arguments_are_rejected_on_the_host():
+    """Invalid calls return DIVA_BAD_INPUT before any work: a retreat-mask frame
+    interval that is empty or reversed, a negative number of completion sweeps."""
+    ctx, _ = calving_case(ob.oracle_backend(), "none")
+    for t0, t1 in ((0.0, 0.0), (10.0, 5.0)):
+        with pytest.raises(diva.DivaError) as e:
+            ctx.apply_prescribed_retreat_mask(1.0, t0, t1)
+        assert e.value.status == 4
+    with pytest.raises(diva.DivaError) as e:
+        ctx.complete_state(-1)
+    assert e.value.status == 4
+    ctx.close()
