@@ -152,7 +152,7 @@ __host__ constexpr int smem_floor(int ncols) { return ncols >= 128 ? 47 * 1024 :
 struct ConvArgs {
   const bf16* x;     // [n][H][W][KC]: forward input, or dY of the layer (dgrad)
   const bf16* gate;  // dgrad: the layer's forward output [n][H][W][KC]
-  const bf16* w;     // [9][COUT][CIN]
+  const bf16* w;     // forward: W [9][COUT][CIN]; dgrad: W^T [9][CIN][COUT]
   const float* bias; // forward: [COUT]
   bf16* y;           // [n][H][W][NO]
   int n, H, W, relu;
@@ -218,17 +218,11 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs a) {
       }
       *reinterpret_cast<uint4*>(As + kc * 2048 + tid * 16) = v;
     }
+    // B(n, k) = w[t][n][k]: forward, W[t][cout][cin]; dgrad, the transposed copy
+    // W^T[t][cin][cout] (k_transpose_w), so both stage contiguous 16-byte rows
     for (int c = tid; c < NO * (KC / 8); c += 128) {
       const int n = c % NO, kc = c / NO;
-      uint4 v;
-      if (!DGRAD) {  // B(n = cout, k = cin) = W[t][n][k]
-        v = *reinterpret_cast<const uint4*>(a.w + ((long)t * NO + n) * KC + kc * 8);
-      } else {       // B(n = cin, k = cout) = W[t][k][n]; W is [9][KC][NO]
-        __align__(16) bf16 e[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) e[q] = a.w[((long)t * KC + kc * 8 + q) * NO + n];
-        v = *reinterpret_cast<const uint4*>(e);
-      }
+      const uint4 v = *reinterpret_cast<const uint4*>(a.w + ((long)t * NO + n) * KC + kc * 8);
       *reinterpret_cast<uint4*>(Bs + kc * (NO * 16) + n * 16) = v;
     }
     fence_async_smem();
@@ -658,6 +652,16 @@ __global__ void k_to_bf16(const float* w, bf16* wb, long n) {
   if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
 }
 
+// W^T[t][ci][co] = bf16(W[t][co][ci]) of one 3x3 layer: the dgrad operand
+__global__ void k_transpose_w(const float* w, bf16* wt, int cin, int cout) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 9L * cin * cout) return;
+  const int co = (int)(i % cout);
+  const long r = i / cout;
+  const int ci = (int)(r % cin), t = (int)(r / cin);
+  wt[i] = __float2bfloat16_rn(w[((long)t * cout + co) * cin + ci]);
+}
+
 // ---------------------------------------------------------------------------
 // the context's fields <-> network tensors
 // ---------------------------------------------------------------------------
@@ -838,6 +842,7 @@ struct diva_cnn {
   void* arena = nullptr;
   float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
   bf16* wb = nullptr;
+  bf16* wbt = nullptr;   // per-layer transposed BF16 weights (dgrad)
   bf16* act[T_N] = {};
   bf16* grad[T_N] = {};
   float *out = nullptr, *tgt = nullptr, *dout = nullptr, *part = nullptr, *loss = nullptr, *loss_hist = nullptr;
@@ -949,7 +954,7 @@ int backward(diva_cnn_t* N, const bf16* in, const float* tgt, int n, cudaStream_
     k_bias_part<<<nb, 128, 0, st>>>(N->grad[ly.out], N->act[ly.out], npix, ly.cout, nb, N->part);
     k_sum_rows<<<1, 128, 0, st>>>(N->part, nb, ly.cout, N->g + ly.boff);
     if (dgrad) {
-      ConvArgs a{N->grad[ly.out], N->act[ly.out], N->wb + ly.woff, nullptr, N->grad[ly.in], n, H, W, 0, N->err};
+      ConvArgs a{N->grad[ly.out], N->act[ly.out], N->wbt + ly.woff, nullptr, N->grad[ly.in], n, H, W, 0, N->err};
       RET(conv_dgrad(ly.cin, ly.cout, a, st));
     }
     return DIVA_OK;
@@ -985,10 +990,19 @@ int backward(diva_cnn_t* N, const bf16* in, const float* tgt, int n, cudaStream_
   return DIVA_OK;
 }
 
+void transpose_weights(diva_cnn_t* N, cudaStream_t st) {
+  for (int l = 0; l < kNL; ++l) {
+    const Layer& ly = N->L[l];
+    k_transpose_w<<<nblk(9L * ly.cin * ly.cout, 256), 256, 0, st>>>(N->w + ly.woff, N->wbt + ly.woff, ly.cin,
+                                                                    ly.cout);
+  }
+}
+
 int adam(diva_cnn_t* N, float lr, cudaStream_t st) {
   N->adam_t += 1;
   const float c1 = 1.0f - powf(0.9f, (float)N->adam_t), c2 = 1.0f - powf(0.999f, (float)N->adam_t);
   k_adam<<<nblk(N->nw, 256), 256, 0, st>>>(N->w, N->g, N->m, N->v, N->wb, N->nw, lr, c1, c2);
+  transpose_weights(N, st);
   CK(cudaGetLastError());
   return DIVA_OK;
 }
@@ -1070,7 +1084,7 @@ int32_t diva_cnn_create(diva_cnn_t** out, int32_t ny, int32_t nx, int32_t nz, in
     return o;
   };
   const size_t o_w = carve(N->nw * 4), o_g = carve(N->nw * 4), o_m = carve(N->nw * 4), o_v = carve(N->nw * 4);
-  const size_t o_wb = carve(N->nw * 2);
+  const size_t o_wb = carve(N->nw * 2), o_wbt = carve(N->nw * 2);
   size_t o_act[T_N], o_grad[T_N];
   for (int t = 0; t < T_N; ++t) {
     o_act[t] = carve((size_t)batch * N->tsize(t) * 2);
@@ -1091,6 +1105,7 @@ int32_t diva_cnn_create(diva_cnn_t** out, int32_t ny, int32_t nx, int32_t nz, in
   N->m = reinterpret_cast<float*>(base + o_m);
   N->v = reinterpret_cast<float*>(base + o_v);
   N->wb = reinterpret_cast<bf16*>(base + o_wb);
+  N->wbt = reinterpret_cast<bf16*>(base + o_wbt);
   for (int t = 0; t < T_N; ++t) {
     N->act[t] = reinterpret_cast<bf16*>(base + o_act[t]);
     N->grad[t] = t == T_IN ? nullptr : reinterpret_cast<bf16*>(base + o_grad[t]);
@@ -1170,6 +1185,7 @@ int32_t diva_cnn_weights(diva_cnn_t* N, float* host, int64_t n, int32_t directio
   CK(cudaMemset(N->v, 0, n * 4));
   N->adam_t = 0;
   k_to_bf16<<<nblk(n, 256), 256, 0, N->stream>>>(N->w, N->wb, n);
+  transpose_weights(N, N->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(N->stream));
   return DIVA_OK;

@@ -24,7 +24,8 @@ def canon_read(smem, start, lbo, sbo, rows):
 
 
 def conv_kernel(x, gate, w, bias, KC, NO, dgrad, n, H, W):
-    """k_conv3x3<KC, NO, dgrad>: x [n][H][W][KC]; w [9][COUT][CIN]; y [n][H][W][NO]
+    """k_conv3x3<KC, NO, dgrad>: x [n][H][W][KC]; w [9][NO][KC] (forward: W [9][COUT][CIN],
+    dgrad: W^T [9][CIN][COUT] as k_transpose_w writes it); y [n][H][W][NO]
     (FP32 throughout: the BF16 roundings are not what this checks)."""
     npix = n * H * W
     y = np.zeros((npix, NO), np.float32)
@@ -51,8 +52,7 @@ def conv_kernel(x, gate, w, bias, KC, NO, dgrad, n, H, W):
             Bs = A_BYTES // 2
             for c in range(NO * (KC // 8)):
                 nn_, kc = c % NO, c // NO
-                if not dgrad: v = w[t, nn_, kc * 8:kc * 8 + 8]
-                else: v = np.array([w[t, kc * 8 + q, nn_] for q in range(8)])
+                v = w[t, nn_, kc * 8:kc * 8 + 8]          # forward: W; dgrad: the transposed copy
                 base = Bs + (kc * (NO * 16) + nn_ * 16) // 2
                 sm[base:base + 8] = v
             for k in range(KC // 16):
@@ -125,7 +125,8 @@ def test_staging_reproduces_forward_dgrad_and_wgrad():
     y = conv_kernel(x, None, w, b, CI, CO, False, n, H, W)
     np.testing.assert_allclose(y, yt.detach().permute(0, 2, 3, 1).numpy(), atol=1e-4)
     g = gy.permute(0, 2, 3, 1).numpy()
-    dx = conv_kernel(g, y, w, None, CO, CI, True, n, H, W)
+    w_tr = np.ascontiguousarray(w.transpose(0, 2, 1))      # k_transpose_w
+    dx = conv_kernel(g, y, w_tr, None, CO, CI, True, n, H, W)
     np.testing.assert_allclose(dx, xt.grad.permute(0, 2, 3, 1).numpy(), atol=1e-4)
     dw = wgrad_kernel(x, g, y, CI, CO, n, H, W, nsplit=3, PIX=64)
     np.testing.assert_allclose(dw, wt.grad.reshape(CO, CI, 9).permute(2, 0, 1).numpy(), atol=1e-4)
