@@ -3,7 +3,6 @@ the PyTorch reference, and the finding the network's output channels rest on -- 
 viscosity iteration warm-starts from its whole carried state (velocities, basal
 stress, viscosity), not from the velocities alone (oracle, no GPU)."""
 import numpy as np
-import pytest
 import torch
 import torch.nn.functional as F
 
