@@ -157,6 +157,7 @@ def bind(lib, prefix):
         "determine_floating_margin_fraction": (C.c_int, [vp]),
         "calc_dHi_dt": (C.c_int, [vp, C.c_double]),
         "calc_critical_timestep_adv": (C.c_int, [vp, C.c_double, dp]),
+        "calc_critical_timestep_sia": (C.c_int, [vp, C.c_double, dp]),
         "pc_predictor": (C.c_int, [vp, C.c_double, C.c_double]),
         "pc_corrector": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, dp]),
         "pc_finish": (C.c_int, [vp, C.c_double]),

@@ -210,6 +210,46 @@ __global__ void k_crit_adv(Dims d, double init, const double* u, const double* v
   }
   block_extreme(m, -1, &part[blockIdx.y * gridDim.x + blockIdx.x]);
 }
+// calc_critical_timestep_SIA (ice_dynamics_module.f90:651-725): the diffusive limit
+// dx^2 / (6 D_SIA) from the depth-averaged SIA velocities of sheet faces, and the 3D
+// advective limit dx / (|u| + |v|) of every layer, per-block minima
+struct SiaDt {
+  Dims d;
+  Zeta zt;
+  double init;
+  const int* sheet;
+  const double *us, *vs, *Hcx, *Hcy, *sx, *sy, *u3, *v3;
+};
+__device__ __forceinline__ double vavg_layers(const Zeta& zt, const double* f, long long stride) {
+  double s = 0.0;   // vertical_average, utilities_module.f90:97-123
+  for (int k = 0; k < zt.nz - 1; ++k) s = s + 0.5 * (f[(k + 1) * stride] + f[k * stride]) * (zt.z[k + 1] - zt.z[k]);
+  return s;
+}
+__global__ void k_crit_sia(SiaDt a, double* part) {
+  IDX2D
+  const Dims& d = a.d;
+  double m = a.init;
+  if (j < d.ny && i < d.nx) {
+    const long long q = d.at(j, i), P = d.plane;
+    double D = 1E-9;
+    if (i < d.nx - 1 && a.sheet[q] == 1 && a.sheet[d.at(j, i + 1)] == 1)
+      D = max_ref(D, fabs(vavg_layers(a.zt, a.us + q, P) * a.Hcx[q] / a.sx[q]));
+    if (j < d.ny - 1 && a.sheet[q] == 1 && a.sheet[d.at(j + 1, i)] == 1)
+      D = max_ref(D, fabs(vavg_layers(a.zt, a.vs + q, P) * a.Hcy[q] / a.sy[q]));
+    m = min_ref(m, d.dx * d.dx / (6.0 * D));
+    for (int k = 0; k < d.nz; ++k) {
+      const double* u = a.u3 + k * P;
+      const double* v = a.v3 + k * P;
+      const double ua = i == 0 ? fabs(u[d.at(j, 0)]) : i == d.nx - 1 ? fabs(u[d.at(j, d.nx - 2)])
+                                                                     : max_ref(fabs(u[d.at(j, i - 1)]), fabs(u[q]));
+      const double va = j == 0 ? fabs(v[d.at(0, i)]) : j == d.ny - 1 ? fabs(v[d.at(d.ny - 2, i)])
+                                                                     : max_ref(fabs(v[d.at(j - 1, i)]), fabs(v[q]));
+      m = min_ref(m, d.dx / (ua + va));
+    }
+  }
+  block_extreme(m, -1, &part[blockIdx.y * gridDim.x + blockIdx.x]);
+}
+
 __global__ void k_extreme_final(const double* part, int nb, double init, int sign, double* out) {
   double m = init;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) m = pick(m, part[b], sign);
@@ -715,6 +755,23 @@ int diva_calc_critical_timestep_adv(diva_ctx_t* h, double dt_max, double* dt_cri
   double m;
   if (int st = read_scalar(c, c->scal + SC_TMP0, &m)) return st;
   *dt_crit_adv = min_ref(dt_max, m * 0.9);
+  return DIVA_OK;
+}
+
+int diva_calc_critical_timestep_sia(diva_ctx_t* h, double dt_max, double* dt_crit_sia) {
+  if (!h || !dt_crit_sia) return DIVA_BAD_INPUT;
+  Ctx* c = &h->c;
+  const dim3 g = grid2d(c->d.ny, c->d.nx);
+  const int nb = g.x * g.y;
+  SiaDt a{c->d, c->zt, dt_max, c->I(DIVA_F_MASK_SHEET_A), c->D(DIVA_F_U_3D_SIA_CX), c->D(DIVA_F_V_3D_SIA_CY),
+          c->D(DIVA_F_HI_CX), c->D(DIVA_F_HI_CY), c->D(DIVA_F_DHS_DX_CX), c->D(DIVA_F_DHS_DY_CY),
+          c->D(DIVA_F_U_3D_CX), c->D(DIVA_F_V_3D_CY)};
+  k_crit_sia<<<g, block2d(), 0, c->stream>>>(a, c->partials); c->launches++;
+  k_extreme_final<<<1, 256, 0, c->stream>>>(c->partials, nb, dt_max, -1, c->scal + SC_TMP0); c->launches++;
+  DIVA_LAUNCHED(c, "k_crit_sia");
+  double m;
+  if (int st = read_scalar(c, c->scal + SC_TMP0, &m)) return st;
+  *dt_crit_sia = m * 0.9;
   return DIVA_OK;
 }
 

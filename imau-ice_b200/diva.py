@@ -266,6 +266,13 @@ class Context:
         """ice_thickness_module.f90:26-300 ('explicit') with apply_ice_thickness_BC."""
         self._check(self.backend.fns["calc_dHi_dt"](self.h, float(dt)), "calc_dHi_dt")
 
+    def calc_critical_timestep_SIA(self, dt_max):
+        """calc_critical_timestep_SIA (ice_dynamics_module.f90:651-725)."""
+        r = C.c_double()
+        self._check(self.backend.fns["calc_critical_timestep_sia"](self.h, float(dt_max), C.byref(r)),
+                    "calc_critical_timestep_sia")
+        return r.value
+
     def calc_critical_timestep_adv(self, dt_max):
         """ice_dynamics_module.f90:726-762; returns dt_crit_adv."""
         r = C.c_double()

@@ -110,3 +110,60 @@ class PCTimeStepper:
             self.step(t_end)
             n += 1
         return n
+
+
+class DirectTimeStepper:
+    """The direct time stepping of SIA, SSA and SIA/SSA dynamics (run_ice_dynamics_direct,
+    ice_dynamics_module.f90:63-242, with the dynamics events of
+    determine_timesteps_and_actions :817-941): each velocity solve when its event is due,
+    its critical time step (calc_critical_timestep_SIA for SIA, _adv for SSA) bounded by
+    dt_min and the start-up / wind-down cap, then calc_dHi_dt over the step and the
+    thickness update at its end (update_ice_thickness).  The reference refuses DIVA here;
+    so does this class."""
+
+    def __init__(self, ctx, start_time, end_time, dt_min=0.01, dt_max=10.0, dt_startup_phase=10.0):
+        dyn = _abi_name(ctx, "choice_ice_dynamics")
+        if dyn not in ("SIA", "SSA", "SIA/SSA"):
+            raise ValueError(f'"direct" time stepping works only with SIA, SSA or SIA/SSA dynamics, not {dyn}')
+        self.ctx, self.dyn = ctx, dyn
+        self.start_time, self.end_time = float(start_time), float(end_time)
+        self.dt_min, self.dt_max, self.dt_startup_phase = float(dt_min), float(dt_max), float(dt_startup_phase)
+        self.time = self.start_time
+        self.t_next_SIA = self.t_next_SSA = self.start_time
+        self.dt_crit_SIA = self.dt_crit_SSA = self.dt_min
+        self.dt = 0.0
+        self.reports = []
+
+    _dt_max_now = PCTimeStepper._dt_max_now
+
+    def run_ice_dynamics_direct(self, t_end):
+        ctx, dt_max = self.ctx, self._dt_max_now()
+        if self.dyn in ("SIA", "SIA/SSA") and self.time == self.t_next_SIA:
+            self.reports.append(ctx.solve_SIA())
+            self.dt_crit_SIA = max(self.dt_min, min(dt_max, ctx.calc_critical_timestep_SIA(self.dt_max)))
+            self.t_next_SIA = self.time + self.dt_crit_SIA
+        if self.dyn in ("SSA", "SIA/SSA") and self.time == self.t_next_SSA:
+            self.reports.append(ctx.solve_SSA())
+            self.dt_crit_SSA = max(self.dt_min, min(dt_max, ctx.calc_critical_timestep_adv(self.dt_max)))
+            self.t_next_SSA = self.time + self.dt_crit_SSA
+        t_next = min(t_end, self.time + self.dt_max)
+        if self.dyn in ("SIA", "SIA/SSA"):
+            t_next = min(t_next, self.t_next_SIA)
+        if self.dyn in ("SSA", "SIA/SSA"):
+            t_next = min(t_next, self.t_next_SSA)
+        self.dt = t_next - self.time
+        ctx.calc_dHi_dt(self.dt)
+
+    def step(self, t_end=None):
+        t_end = self.end_time if t_end is None else t_end
+        self.run_ice_dynamics_direct(t_end)
+        self.ctx.pc_finish(self.dt)
+        self.time = self.time + self.dt
+        return self.dt
+
+
+def _abi_name(ctx, field):
+    """The configuration's choice as its reference name."""
+    from . import _abi
+    value = getattr(ctx.cfg, field)
+    return {v: k for k, v in _abi.ENUM_OPTIONS[field].items()}.get(value, value)

@@ -260,6 +260,12 @@ int  diva_calc_dHi_dt(diva_ctx_t* ctx, double dt);
 /* calc_critical_timestep_adv (ice_dynamics_module.f90:726-762):
  * min(dt_max, 0.9 min over interior a-points of dx / (|u_vav_cx| + |v_vav_cy|)). */
 int  diva_calc_critical_timestep_adv(diva_ctx_t* ctx, double dt_max, double* dt_crit_adv);
+/* calc_critical_timestep_SIA (ice_dynamics_module.f90:651-725), for the direct time
+ * stepping of SIA and SIA/SSA dynamics: 0.9 x min(dt_max, dx^2 / (6 D_SIA) over sheet
+ * faces with D_SIA = max(1e-9, |vertical average of u_3D_SIA x Hi / dHs_dx| on the
+ * face), dx / (|u_3D| + |v_3D|) of every layer and cell) -- reads u_3D_SIA_cx,
+ * v_3D_SIA_cy (solve_SIA) and u_3D_cx, v_3D_cy. */
+int  diva_calc_critical_timestep_sia(diva_ctx_t* ctx, double dt_max, double* dt_crit_sia);
 /* The predictor of run_ice_dynamics_pc (:360-377): dHidt_Hnm1_unm1 = dHidt_Hn_un;
  * calc_dHi_dt(dt); dHidt_Hn_un = dHi_dt_a; Hi_pred = max(0, Hi + dt ((1 + zeta/2)
  * dHidt_Hn_un - zeta/2 dHidt_Hnm1_unm1)); Hi_old = Hi; Hi = Hi_pred;

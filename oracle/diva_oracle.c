@@ -2666,6 +2666,33 @@ int orc_calc_critical_timestep_adv(orc_ctx* c, double dt_max, double* dt_crit_ad
   return DIVA_OK;
 }
 
+/* calc_critical_timestep_SIA, ice_dynamics_module.f90:651-725 */
+int orc_calc_critical_timestep_sia(orc_ctx* c, double dt_max, double* dt_crit_sia) {
+  DECL_DIMS(c);
+  const int32_t* sheet = FI(c, MASK_SHEET_A);
+  const double *us = FD(c, U_3D_SIA_CX), *vs = FD(c, V_3D_SIA_CY), *Hcx = FD(c, HI_CX), *Hcy = FD(c, HI_CY);
+  const double *sx = FD(c, DHS_DX_CX), *sy = FD(c, DHS_DY_CY), *u3 = FD(c, U_3D_CX), *v3 = FD(c, V_3D_CY);
+  double dtc = dt_max;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      double D = 1E-9;
+      if (i < nx - 1 && sheet[IA(j, i)] == 1 && sheet[IA(j, i + 1)] == 1)
+        D = fmax(D, fabs(vavg(c->g.zeta, nz, &us[ICX3(0, j, i)]) * Hcx[ICX(j, i)] / sx[ICX(j, i)]));
+      if (j < ny - 1 && sheet[IA(j, i)] == 1 && sheet[IA(j + 1, i)] == 1)
+        D = fmax(D, fabs(vavg(c->g.zeta, nz, &vs[ICY3(0, j, i)]) * Hcy[ICY(j, i)] / sy[ICY(j, i)]));
+      dtc = fmin(dtc, c->dx * c->dx / (6.0 * D));
+      for (int k = 0; k < nz; ++k) {
+        const double ua = i == 0 ? fabs(u3[ICX3(k, j, 0)]) : i == nx - 1 ? fabs(u3[ICX3(k, j, nx - 2)])
+                                 : fmax(fabs(u3[ICX3(k, j, i - 1)]), fabs(u3[ICX3(k, j, i)]));
+        const double va = j == 0 ? fabs(v3[ICY3(k, 0, i)]) : j == ny - 1 ? fabs(v3[ICY3(k, ny - 2, i)])
+                                 : fmax(fabs(v3[ICY3(k, j - 1, i)]), fabs(v3[ICY3(k, j, i)]));
+        dtc = fmin(dtc, c->dx / (ua + va));
+      }
+    }
+  *dt_crit_sia = dtc * 0.9;
+  return DIVA_OK;
+}
+
 /* the predictor of run_ice_dynamics_pc, ice_dynamics_module.f90:360-377 */
 int orc_pc_predictor(orc_ctx* c, double dt, double zeta) {
   DECL_DIMS(c);

@@ -184,3 +184,21 @@ def test_prescribed_retreat_mask_bit_exact(cuda, oracle):
         ctx.close()
     for k in out[0]:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_critical_timestep_sia_bit_exact(cuda, oracle):
+    """From the oracle's state after solve_SIA, both sides' calc_critical_timestep_SIA
+    agree exactly (same vertical averages in the same order, no FMA contraction)."""
+    g, cfg, f = synth.ice_cap(dx=40e3)
+    cfg = dict(cfg, choice_ice_dynamics="SIA")
+    ctx = diva.Context(diva.Grid(**g), cfg, oracle)
+    helpers.prepare(ctx, f)
+    ctx.solve_SIA()
+    state = ctx.download()
+    dts = [ctx.calc_critical_timestep_SIA(10.0)]
+    ctx.close()
+    ctx = diva.Context(diva.Grid(**g), cfg, cuda)
+    ctx.upload(state)
+    dts.append(ctx.calc_critical_timestep_SIA(10.0))
+    ctx.close()
+    assert dts[0] == dts[1] and 0.0 < dts[0] <= 9.0

@@ -455,3 +455,49 @@ def test_bad_arguments_are_rejected_on_the_host():
         ctx.complete_state(-1)
     assert e.value.status == 4
     ctx.close()
+
+
+def test_critical_timestep_sia_known_answer():
+    """calc_critical_timestep_SIA (ice_dynamics_module.f90:651-725) on a sheet with a
+    uniform SIA velocity profile: D = |u_vav Hi / dHs_dx| on the x faces, the 3D
+    advective limit from u_3D, times 0.9."""
+    ny, nx = 9, 11
+    g = diva.Grid(nx, ny, 10e3)
+    ctx = diva.Context(g, {"choice_ice_dynamics": "SIA"}, ob.oracle_backend())
+    f = {"Hi_a": np.full((ny, nx), 1000.0), "Hb_a": np.full((ny, nx), 100.0), "SL_a": np.zeros((ny, nx)),
+         "Ti_a": np.full((g.nz, ny, nx), 260.0)}
+    ctx.upload({k: np.asfortranarray(v) for k, v in f.items()})
+    ctx.update_general_ice_model_data()
+    u = np.full((g.nz, ny, nx - 1), 50.0)
+    ctx.upload({"u_3D_SIA_cx": np.asfortranarray(u), "v_3D_SIA_cy": np.zeros((g.nz, ny - 1, nx)),
+                "dHs_dx_cx": np.full((ny, nx - 1), -2e-3), "dHs_dy_cy": np.full((ny - 1, nx), 1.0),
+                "Hi_cx": np.full((ny, nx - 1), 1000.0), "Hi_cy": np.full((ny - 1, nx), 1000.0),
+                "u_3D_cx": np.full((g.nz, ny, nx - 1), 20.0), "v_3D_cy": np.full((g.nz, ny - 1, nx), 5.0)})
+    dt = ctx.calc_critical_timestep_SIA(100.0)
+    D = 50.0 * 1000.0 / 2e-3
+    assert dt == pytest.approx(0.9 * min(100.0, 1e8 / (6.0 * D), 1e4 / 25.0), rel=1e-12)
+    ctx.close()
+
+
+def test_direct_time_stepping_of_sia():
+    """run_ice_dynamics_direct with SIA: the SIA solve when its event is due, the step
+    bounded by the SIA critical time step and the start-up cap, thickness changing."""
+    from imau_ice_b200 import dynamics
+    g, cfg, f = synth.ice_cap(dx=80e3)
+    cfg = dict(cfg, choice_ice_dynamics="SIA")
+    f = dict(f)
+    f["SMB_a"] = np.asfortranarray(np.full(f["Hi_a"].shape, 0.3))
+    ctx = diva.Context(diva.Grid(**g), cfg, ob.oracle_backend())
+    helpers.prepare(ctx, f)
+    H0 = ctx.download(["Hi_a"])["Hi_a"]
+    st = dynamics.DirectTimeStepper(ctx, 0.0, 1000.0, dt_min=0.1, dt_max=10.0, dt_startup_phase=10.0)
+    dts = [st.step() for _ in range(4)]
+    H1 = ctx.download(["Hi_a"])["Hi_a"]
+    ctx.close()
+    assert len(st.reports) >= 2 and all(r["status"] == 0 for r in st.reports)
+    assert all(0.0 < d <= 10.0 for d in dts) and st.time == pytest.approx(sum(dts))
+    assert dts[0] == pytest.approx(0.1)           # the start-up cap at t = 0 is dt_min
+    assert np.abs(H1 - H0).max() > 0.0
+    with pytest.raises(ValueError):
+        dynamics.DirectTimeStepper(diva.Context(diva.Grid(**g), dict(cfg, choice_ice_dynamics="DIVA"),
+                                                ob.oracle_backend()), 0.0, 10.0)
