@@ -479,12 +479,14 @@ def test_critical_timestep_sia_known_answer():
     ctx.close()
 
 
-def test_direct_time_stepping_of_sia():
-    """run_ice_dynamics_direct with SIA: the SIA solve when its event is due, the step
-    bounded by the SIA critical time step and the start-up cap, thickness changing."""
+@pytest.mark.parametrize("dyn", ["SIA", "SIA/SSA"])
+def test_direct_time_stepping(dyn):
+    """run_ice_dynamics_direct with SIA or hybrid SIA/SSA: each solve when its event is
+    due, the step bounded by the critical time steps and the start-up cap, thickness
+    changing."""
     from imau_ice_b200 import dynamics
     g, cfg, f = synth.ice_cap(dx=80e3)
-    cfg = dict(cfg, choice_ice_dynamics="SIA")
+    cfg = dict(cfg, choice_ice_dynamics=dyn)
     f = dict(f)
     f["SMB_a"] = np.asfortranarray(np.full(f["Hi_a"].shape, 0.3))
     ctx = diva.Context(diva.Grid(**g), cfg, ob.oracle_backend())
