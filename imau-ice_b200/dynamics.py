@@ -121,7 +121,7 @@ class DirectTimeStepper:
     thickness update at its end (update_ice_thickness).  The reference refuses DIVA here;
     so does this class."""
 
-    def __init__(self, ctx, start_time, end_time, dt_min=0.01, dt_max=10.0, dt_startup_phase=10.0):
+    def __init__(self, ctx, start_time, end_time, dt_min=0.01, dt_max=10.0, dt_startup_phase=10.0, thermo=False):
         dyn = _abi_name(ctx, "choice_ice_dynamics")
         if dyn not in ("SIA", "SSA", "SIA/SSA"):
             raise ValueError(f'"direct" time stepping works only with SIA, SSA or SIA/SSA dynamics, not {dyn}')
@@ -133,6 +133,11 @@ class DirectTimeStepper:
         self.dt_crit_SIA = self.dt_crit_SSA = self.dt_min
         self.dt = 0.0
         self.reports = []
+        self.thermo = thermo                     # the thermodynamics event, as in PCTimeStepper
+        self.dt_thermo = float(ctx.cfg.dt_thermo)
+        self.t_next_thermo = self.start_time + self.dt_thermo
+        self.do_thermo = False
+        self.thermo_solves = 0
 
     _dt_max_now = PCTimeStepper._dt_max_now
 
@@ -151,12 +156,22 @@ class DirectTimeStepper:
             t_next = min(t_next, self.t_next_SIA)
         if self.dyn in ("SSA", "SIA/SSA"):
             t_next = min(t_next, self.t_next_SSA)
+        if self.thermo:
+            self.do_thermo = self.time == self.t_next_thermo
+            if self.do_thermo:
+                self.t_next_thermo = self.time + self.dt_thermo
+            t_next = min(t_next, self.t_next_thermo)
         self.dt = t_next - self.time
         ctx.calc_dHi_dt(self.dt)
 
     def step(self, t_end=None):
+        """One model time step: run_ice_dynamics_direct, [run_thermo_model], then the
+        thickness update at the end of the step (IMAU_ICE_main_model.f90:117-207)."""
         t_end = self.end_time if t_end is None else t_end
         self.run_ice_dynamics_direct(t_end)
+        if self.thermo:
+            self.ctx.run_thermo_model(self.do_thermo)
+            self.thermo_solves += int(self.do_thermo)
         self.ctx.pc_finish(self.dt)
         self.time = self.time + self.dt
         return self.dt
