@@ -503,3 +503,28 @@ def test_direct_time_stepping(dyn):
     with pytest.raises(ValueError):
         dynamics.DirectTimeStepper(diva.Context(diva.Grid(**g), dict(cfg, choice_ice_dynamics="DIVA"),
                                                 ob.oracle_backend()), 0.0, 10.0)
+
+
+def test_direct_time_stepping_with_the_heat_equation():
+    """The thermodynamics event of the direct scheme: run_thermo_model every step, the
+    heat equation when dt_thermo has elapsed, and the step cut at that event."""
+    from imau_ice_b200 import dynamics
+    g, cfg, f = synth.ice_cap(dx=80e3)
+    cfg = dict(cfg, choice_ice_dynamics="SIA", dt_thermo=0.25)
+    f = dict(f)
+    ny, nx = f["Hi_a"].shape
+    for k, v in (("SMB_a", 0.3), ("T_surf_annual_a", 245.0), ("GHF_a", 1.7e6)):
+        f[k] = np.asfortranarray(np.full((ny, nx), v))
+    f["mask_ice_a_prev"] = np.ones((ny, nx), dtype=np.int32, order="F")
+    ctx = diva.Context(diva.Grid(**g), cfg, ob.oracle_backend())
+    helpers.prepare(ctx, f)
+    T0 = ctx.download(["Ti_a"])["Ti_a"]
+    st = dynamics.DirectTimeStepper(ctx, 0.0, 1000.0, dt_min=0.1, dt_max=10.0, dt_startup_phase=10.0, thermo=True)
+    times = []
+    for _ in range(6):
+        st.step()
+        times.append(st.time)
+    T1 = ctx.download(["Ti_a"])["Ti_a"]
+    ctx.close()
+    assert st.thermo_solves >= 1 and np.abs(T1 - T0).max() > 0.0
+    assert any(abs(t - 0.25) < 1e-12 or abs(t - 0.5) < 1e-12 for t in times)   # steps end on the event
