@@ -199,11 +199,13 @@ class Context:
         file: a restart of the whole device state, velocities and viscosity included
         (the reference's restart file, netcdf_module.f90:31-127, holds the geometry and
         temperature but not the velocity-solver state)."""
+        import json
         arrays = self.download(names)
+        cfg = {name: getattr(self.cfg, name) for name, _ in _abi.Config._fields_ if name != "reserved"}
         meta = {"_grid": np.array([self.grid.nx, self.grid.ny], dtype=np.int64),
                 "_grid_f": np.array([self.grid.dx, self.grid.xmin, self.grid.ymin]),
                 "_zeta": self.grid.zeta,
-                "_config": np.frombuffer(bytes(self.cfg), dtype=np.uint8)}
+                "_config_json": np.array(json.dumps(cfg))}
         np.savez(path, **arrays, **meta)
 
     @classmethod
@@ -213,8 +215,21 @@ class Context:
         nx, ny = (int(v) for v in z["_grid"])
         dx, xmin, ymin = (float(v) for v in z["_grid_f"])
         grid = Grid(nx, ny, dx, zeta=z["_zeta"], xmin=xmin, ymin=ymin)
-        cfg = _abi.Config.from_buffer_copy(z["_config"].tobytes())
-        ctx = cls(grid, cfg, backend)
+        be = backend or cuda_backend()
+        if "_config_json" in z.files:
+            # by field name onto the library's defaults: files stay readable when
+            # configuration fields are added
+            import json
+            cfg = be.default_config()
+            for name, value in json.loads(str(z["_config_json"])).items():
+                if hasattr(cfg, name):
+                    setattr(cfg, name, value)
+        else:
+            raw = z["_config"].tobytes()
+            if len(raw) != C.sizeof(_abi.Config):
+                raise DivaError(_abi.BAD_INPUT, "restart file written with another configuration layout")
+            cfg = _abi.Config.from_buffer_copy(raw)
+        ctx = cls(grid, cfg, be)
         ctx.upload({k: np.asfortranarray(z[k]) for k in z.files if not k.startswith("_")})
         return ctx
 
