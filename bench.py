@@ -406,7 +406,7 @@ def run_ensemble(args):
     budget = 0.7 * torch.cuda.mem_get_info()[0]
     clocks = ClockSampler(local)
     clocks.start()
-    t_total, launches, last = 0.0, 0, {}
+    t_total, launches, last, group_seconds = 0.0, 0, {}, []
     for grp in ensemble.groups(members, parts[rank], budget):
         ctxs = []
         for k in grp:
@@ -435,6 +435,7 @@ def run_ensemble(args):
         for _ in range(args.steps):
             reps = step()
         torch.cuda.synchronize()
+        group_seconds.append((time.perf_counter() - t0) / args.steps)
         t_total += time.perf_counter() - t0
         launches += sum(c.kernel_launches() for c in ctxs) - l0
         last.update({k: r for k, r in zip(grp, reps)})
@@ -446,6 +447,8 @@ def run_ensemble(args):
         dist.all_reduce(dt, op=dist.ReduceOp.MAX)
     t_max = float(dt.item())
     its = [last[k]["picard_iterations"] for k in sorted(last)]
+    cycles = [last[k]["mg_cycles"] for k in sorted(last)]
+    member_ms = [round(last[k]["elapsed_ms"], 3) for k in sorted(last)]
     converged = sum(1 for k in last if last[k]["status"] == 0)
     if rank == 0:
         print(json.dumps({
@@ -457,6 +460,9 @@ def run_ensemble(args):
                                    "U_log[0.3,3], flow factor x U_log[0.5,2]",
                        "members_per_rank": [len(p) for p in parts],
                        "picard_iterations_rank0": its,
+                       "mg_cycles_rank0": cycles,
+                       "member_elapsed_ms_rank0": member_ms,
+                       "group_seconds_rank0": [round(x, 4) for x in group_seconds],
                        "rank0_members_converged": converged,
                        "rank0_members_at_iteration_cap": len(last) - converged,
                        "note": "members with low friction reach the 5000 m/yr velocity limit of the "
