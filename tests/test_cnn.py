@@ -110,3 +110,9 @@ def test_complete_state_lets_velocities_alone_warm_start():
         uv = ctx.download(["u_vav_cx", "v_vav_cy"])
         ctx.close()
     assert its[0] > 20 and its[1] <= 2, its
+
+
+def test_the_network_needs_the_cuda_library():
+    """No host implementation of the network: another backend is refused up front."""
+    with np.testing.assert_raises(diva.DivaError):
+        learned.WarmStartNet(diva.Grid(37, 29, 10e3), backend=ob.oracle_backend())
