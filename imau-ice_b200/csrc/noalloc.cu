@@ -13,6 +13,7 @@
 // overlap on the GPU (different streams, or host threads) race on it; serialise
 // them.  Each call writes every partial it later reads, so nothing has to be
 // cleared between calls.
+#include <cuda.h>   // CUcontext and CUresult, for the context id of the set-up
 #include <mutex>
 #include "common.cuh"
 
@@ -77,19 +78,57 @@ __global__ void k_resid_final(const double* partials, int nblocks, double* out) 
   }
 }
 
-// device address of the scratch array, looked up once per device with that device current
+// Device address of the scratch array, set up by the first call in each CUDA context:
+// cudaGetSymbolAddress with the device current, checked, and cached with the context's
+// unique id (cuCtxGetId, never reused within a process).  A cudaDeviceReset, or a caller
+// that makes another context current on the same device, gives a new id, and the next
+// call sets up again (the module, and with it the array, may sit at a new address).
+// The driver calls are resolved through the runtime, so the library needs no link
+// against the driver library.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+
+// id of the context current on this thread; 0 if none is current yet
+int current_context_id(unsigned long long* id) {
+  if (!g_ctx_current || !g_ctx_id) {
+    void* f0 = nullptr;
+    void* f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0, q1;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) != cudaSuccess ||
+        q0 != cudaDriverEntryPointSuccess || !f0)
+      return DIVA_CUDA_ERROR;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || !f1)
+      return DIVA_CUDA_ERROR;
+    g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+    g_ctx_id = reinterpret_cast<CtxGetIdFn>(f1);
+  }
+  CUcontext ctx = nullptr;
+  if (g_ctx_current(&ctx) != CUDA_SUCCESS) return DIVA_CUDA_ERROR;
+  *id = 0;
+  if (ctx && g_ctx_id(ctx, id) != CUDA_SUCCESS) return DIVA_CUDA_ERROR;
+  return DIVA_OK;
+}
 
 int scratch_for_current_device(double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return DIVA_CUDA_ERROR;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_ptr[dev]) {
+  unsigned long long id = 0;
+  int st = current_context_id(&id);
+  if (st) return st;
+  if (id == 0 || id != g_scratch_ctx[dev] || !g_scratch_ptr[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_resid_scratch) != cudaSuccess || !p) return DIVA_CUDA_ERROR;
+    if ((st = current_context_id(&id))) return st;   // the look-up made the primary context current
     g_scratch_ptr[dev] = static_cast<double*>(p);
+    g_scratch_ctx[dev] = id;
   }
   *out = g_scratch_ptr[dev];
   return DIVA_OK;

@@ -62,3 +62,46 @@ def test_noalloc_rejects_grids_beyond_its_scratch(cuda):
     # ceil(3000/32) * ceil(3000/8) = 94 * 375 blocks > 16384: rejected before any launch
     assert fn(3000, 3000, p, p, 3000, p, p, 2999, p, None) == _abi.BAD_INPUT
     assert fn(1, 5, p, p, 5, p, p, 4, p, None) == _abi.BAD_INPUT
+
+
+def test_noalloc_padded_rows_on_a_side_stream_allocates_nothing(cuda):
+    """Caller arrays with padded leading dimensions (ld_cx = ny + 3, ld_cy = ny + 2) on a
+    stream of the caller's own: the same norm as unpadded arrays on the default stream, and
+    the device's free memory does not move over repeated calls (the entry point allocates
+    nothing; the first call may load the library's device code, so it is made before)."""
+    import torch
+    fn = _fn(cuda.lib)
+    rng = np.random.default_rng(7)
+    ny, nx = 45, 37
+    u, up = rng.normal(0, 100, (2, ny, nx - 1))
+    v, vp = rng.normal(0, 100, (2, ny - 1, nx))
+    u[3:9, 4:7] = 0.0                      # points below the velocity tolerance are left out
+
+    def dev(a, ld):
+        t = torch.zeros((a.shape[1], ld), dtype=torch.float64)
+        t[:, :a.shape[0]] = torch.from_numpy(a.T.copy())
+        return t.cuda()
+
+    out0 = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    out1 = torch.full((1,), -2.0, dtype=torch.float64, device="cuda")
+    plain = [dev(a, a.shape[0]) for a in (u, up, v, vp)]
+    padded = [dev(u, ny + 3), dev(up, ny + 3), dev(v, ny + 2), dev(vp, ny + 2)]
+    assert fn(nx, ny, plain[0].data_ptr(), plain[1].data_ptr(), ny, plain[2].data_ptr(), plain[3].data_ptr(),
+              ny - 1, out0.data_ptr(), None) == _abi.OK
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        st = fn(nx, ny, padded[0].data_ptr(), padded[1].data_ptr(), ny + 3, padded[2].data_ptr(),
+                padded[3].data_ptr(), ny + 2, out1.data_ptr(), C.c_void_p(side.cuda_stream))
+        assert st == _abi.OK
+    side.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    m = np.abs(u) > 1e-6
+    mv = np.abs(v) > 1e-6
+    r1 = np.sum((u - up)[m] ** 2) + np.sum((v - vp)[mv] ** 2)
+    r2 = np.sum((u + up)[m] ** 2) + np.sum((v + vp)[mv] ** 2)
+    want = 2.0 * np.sqrt(r1) / max(np.sqrt(r2), 1e-8)
+    assert out1.item() == pytest.approx(out0.item(), rel=1e-12)
+    assert out1.item() == pytest.approx(want, rel=1e-12)
+
