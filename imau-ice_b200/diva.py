@@ -16,7 +16,7 @@ settings from the global ``C%``.  This module keeps that shape:
 
 For repeated solves on one grid, ``Context`` keeps the whole state resident on
 the GPU between calls (upload once, solve many times, download on request),
-which is how the Fortran shim in INTEGRATION.md drives the library.
+which is how a Fortran shim over the C ABI drives the library.
 
 The product backend is ``libdiva_b200.so`` (CUDA, sm_100a).  There is no CPU
 fallback: if the library or a GPU is missing, creating a context raises.
