@@ -95,7 +95,8 @@ class Config(C.Structure):
         ("calving_threshold_thickness", C.c_double),
         ("remove_shelves_larger_than_PD", C.c_int32), ("continental_shelf_calving", C.c_int32),
         ("continental_shelf_min_height", C.c_double),
-        ("reserved", C.c_int32 * 8),
+        ("picard_anderson_m", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 

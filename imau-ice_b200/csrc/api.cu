@@ -133,6 +133,10 @@ int validate_config(Ctx* c, const diva_config_t* cfg) {
     return set_error(c, DIVA_BAD_INPUT, "precision must be DIVA_PREC_FP64 or DIVA_PREC_MIXED");
   if (cfg->lin_adaptive && !(cfg->lin_adaptive_eta > 0.0 && cfg->lin_adaptive_eta < 1.0))
     return set_error(c, DIVA_BAD_INPUT, "lin_adaptive_eta must lie in (0, 1)");
+  if (cfg->picard_anderson_m < 0 || cfg->picard_anderson_m > kAAMax)
+    return set_error(c, DIVA_BAD_INPUT, "picard_anderson_m must lie in 0..5");
+  if (cfg->picard_anderson_m > 0 && cfg->picard_stop != DIVA_STOP_RELRES)
+    return set_error(c, DIVA_BAD_INPUT, "picard_anderson_m > 0 needs picard_stop = DIVA_STOP_RELRES");
   const int bcs[8] = {cfg->BC_u_west, cfg->BC_u_east, cfg->BC_u_south, cfg->BC_u_north,
                       cfg->BC_v_west, cfg->BC_v_east, cfg->BC_v_south, cfg->BC_v_north};
   for (int b : bcs)
@@ -193,9 +197,17 @@ size_t carve(Ctx* c, Carver& cv) {
   c->sub_tab = (uint16_t*)cv.take(sizeof(uint16_t) * (solver_table_entries(c) + 8));
   const dim3 g = grid2d(d.ny, d.nx);
   c->max_blocks = g.x * g.y;
-  c->partials = (double*)cv.take(sizeof(double) * 4 * c->max_blocks);
+  c->partials = (double*)cv.take(sizeof(double) * (kAAPartials > 4 ? kAAPartials : 4) * c->max_blocks);
   for (int k = 0; k < KV_COUNT; ++k)
     for (int q = 0; q < 2; ++q) c->kv[k][q] = (double*)cv.take(sizeof(double) * d.plane);
+  for (int q = 0; q < 2; ++q) {
+    for (int k = 0; k < kAAMax; ++k) {
+      c->aa_dF[k][q] = (double*)cv.take(sizeof(double) * d.plane);
+      c->aa_dG[k][q] = (double*)cv.take(sizeof(double) * d.plane);
+    }
+    c->aa_f[q] = (double*)cv.take(sizeof(double) * d.plane);
+    c->aa_g[q] = (double*)cv.take(sizeof(double) * d.plane);
+  }
   for (int l = 0; l < c->nlev; ++l) {
     Level& L = c->lv[l];
     const size_t pb = sizeof(double) * L.d.plane;
@@ -260,7 +272,7 @@ int graph_loop_begin(Ctx* c, GraphLoop& L) {
   init[SC_ETA - SC_TARGET2] = c->c.lin_adaptive_eta;
   DIVA_CUDA(c, cudaMemcpyAsync(c->scal + SC_TARGET2, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
   L.it = 0; L.resid = 0.0; L.relres = -1.0; L.by_relres = false; L.done = false;
-  return DIVA_OK;
+  return anderson_reset(c);
 }
 
 // enqueue the whole viscosity loop (one graph launch) and the copy of its status block
@@ -338,6 +350,11 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
   const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
   int it = 0, st = DIVA_OK, lin_fail = 0;
   double resid = 0.0, relres = -1.0, eta = C.lin_adaptive_eta, relres_prev = 0.0;
+  if (C.picard_anderson_m > 0) {
+    double init[SC_COUNT - SC_AA_N] = {};
+    DIVA_CUDA(c, cudaMemcpyAsync(c->scal + SC_AA_N, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+    if ((st = anderson_reset(c))) return st;
+  }
   for (;;) {
     ++it;
     if ((st = launch_diva_coefficients(c, u, v, diva))) return st;
@@ -360,6 +377,11 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
       ++lin_fail;   // the reference does not check PETSc/SOR convergence either; keep iterating
     } else if (st) {
       return st;
+    }
+    if (C.picard_anderson_m > 0) {
+      // the mixing step reads this iteration's nonlinear residual from the device scalars
+      DIVA_CUDA(c, cudaMemcpyAsync(c->scal + SC_RELRES, &relres, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      if ((st = launch_anderson_prepare(c, u, v, c->kv[KV_X][0], c->kv[KV_X][1]))) return st;
     }
     if ((st = launch_picard_update(c, u, v, c->kv[KV_X][0], c->kv[KV_X][1], diva))) return st;
     DIVA_CUDA(c, cudaMemcpyAsync(c->h_scal + SC_RES1, c->scal + SC_RES1, 3 * sizeof(double), cudaMemcpyDeviceToHost,

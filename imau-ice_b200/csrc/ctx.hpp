@@ -2,6 +2,7 @@
 // the translation units of libdiva_b200.so.
 #pragma once
 #include <cuda_runtime.h>
+#include <cmath>
 #include <string>
 #include "common.cuh"
 
@@ -51,8 +52,99 @@ enum {
   SC_RELRES, SC_NAN, SC_SOLVED, SC_HALFDONE,
   SC_ETA, SC_RELRES_PREV,   // adaptive linear tolerance factor and the previous nonlinear residual
   SC_SUM_LIN, SC_SUM_FULL, SC_N_SOLVED,   // totals of a graph-launched viscosity loop
-  SC_COUNT = 40
+  // Anderson mixing of the viscosity iteration (picard_anderson_m > 0): history columns held,
+  // the ring slot the next one goes to, whether the previous map value is stored, the
+  // nonlinear residual the last mixing step saw, the Gram matrix of the residual
+  // differences, its right-hand side and the mixing coefficients
+  SC_AA_N, SC_AA_HEAD, SC_AA_HAVE, SC_AA_RPREV, SC_AA_RESTARTS,
+  SC_AA_G, SC_AA_RHS = SC_AA_G + 25, SC_AA_GAMMA = SC_AA_RHS + 5,
+  SC_COUNT = SC_AA_GAMMA + 5
 };
+constexpr int kAAMax = 5;             // largest Anderson depth
+constexpr int kAAPartials = 2 * kAAMax;   // block partials of one mixing step
+
+// One Anderson mixing step's coefficients from the inner products of the newest residual
+// difference dF_s with every history column (dots[0..m)) and of the residual f with them
+// (dots[kAAMax..kAAMax+m)), on the device scalars SC_AA_*.  The first call of a solve only
+// records that a map value exists (gamma = 0: the plain step g).  A nonlinear residual
+// more than 10 x the one the previous step saw drops the older columns.  gamma solves the
+// normal equations of the least-squares problem over the n most recent columns, scaled to
+// unit diagonal and regularised by 1e-10; when the Cholesky factorisation meets a pivot
+// below 1e-12 the oldest column is dropped and the solve repeated (down to none).
+__host__ __device__ inline void aa_coefficients(double* sc, int m, const double* dots) {
+  double* G = sc + SC_AA_G;
+  double* rhs = sc + SC_AA_RHS;
+  double* gam = sc + SC_AA_GAMMA;
+  const double relres = sc[SC_RELRES], rprev = sc[SC_AA_RPREV];
+  for (int k = 0; k < kAAMax; ++k) gam[k] = 0.0;
+  sc[SC_AA_RPREV] = relres;
+  if (sc[SC_AA_HAVE] == 0.0) {
+    sc[SC_AA_HAVE] = 1.0;
+    sc[SC_AA_N] = 0.0;
+    sc[SC_AA_HEAD] = 0.0;
+    return;
+  }
+  const int s = (int)sc[SC_AA_HEAD];
+  int n = (int)sc[SC_AA_N];
+  if (rprev > 0.0 && relres > 10.0 * rprev) {
+    n = 0;
+    sc[SC_AA_RESTARTS] += 1.0;
+  }
+  for (int i = 0; i < m; ++i) {
+    G[s * kAAMax + i] = dots[i];
+    G[i * kAAMax + s] = dots[i];
+    rhs[i] = dots[kAAMax + i];
+  }
+  n = n + 1 < m ? n + 1 : m;
+  sc[SC_AA_HEAD] = (double)((s + 1) % m);
+  int idx[kAAMax];
+  for (int k = 0; k < n; ++k) idx[k] = (s - k + m) % m;   // newest first
+  for (int nn = n; nn > 0; --nn) {
+    double A[kAAMax][kAAMax], b[kAAMax], dk[kAAMax];
+    bool ok = true;
+    for (int k = 0; k < nn && ok; ++k) {
+      dk[k] = sqrt(G[idx[k] * kAAMax + idx[k]]);
+      ok = dk[k] > 0.0 && dk[k] < 1e300;
+    }
+    if (!ok) continue;
+    for (int k = 0; k < nn; ++k) {
+      for (int l = 0; l < nn; ++l) A[k][l] = G[idx[k] * kAAMax + idx[l]] / (dk[k] * dk[l]);
+      A[k][k] += 1e-10;
+      b[k] = rhs[idx[k]] / dk[k];
+    }
+    // Cholesky A = L L^T in the lower triangle
+    for (int k = 0; k < nn && ok; ++k) {
+      double p = A[k][k];
+      for (int l = 0; l < k; ++l) p -= A[k][l] * A[k][l];
+      if (!(p > 1e-12)) { ok = false; break; }
+      const double r = sqrt(p);
+      A[k][k] = r;
+      for (int i = k + 1; i < nn; ++i) {
+        double t = A[i][k];
+        for (int l = 0; l < k; ++l) t -= A[i][l] * A[k][l];
+        A[i][k] = t / r;
+      }
+    }
+    if (!ok) continue;
+    double y[kAAMax];
+    for (int k = 0; k < nn; ++k) {
+      double t = b[k];
+      for (int l = 0; l < k; ++l) t -= A[k][l] * y[l];
+      y[k] = t / A[k][k];
+    }
+    for (int k = nn - 1; k >= 0; --k) {
+      double t = y[k];
+      for (int l = k + 1; l < nn; ++l) t -= A[l][k] * y[l];
+      y[k] = t / A[k][k];
+    }
+    for (int k = 0; k < nn; ++k) ok = ok && (y[k] == y[k]) && fabs(y[k]) < 1e300;
+    if (!ok) continue;
+    for (int k = 0; k < nn; ++k) gam[idx[k]] = y[k] / dk[k];
+    sc[SC_AA_N] = (double)nn;
+    return;
+  }
+  sc[SC_AA_N] = 0.0;
+}
 
 // The graph-launched viscosity loop: one instantiated graph per starting buffer of
 // the viscosity double buffer; the launch and pass counts of each captured region of
@@ -96,6 +188,12 @@ struct Ctx {
   double* partials = nullptr;         // block partial sums
   int max_blocks = 0;
   double* kv[KV_COUNT][2] = {};       // Krylov vectors (u,v)
+  // Anderson mixing history (u,v plane pairs): ring of residual differences dF and map
+  // differences dG, and the previous residual f = g - u and map value g
+  double* aa_dF[kAAMax][2] = {};
+  double* aa_dG[kAAMax][2] = {};
+  double* aa_f[2] = {};
+  double* aa_g[2] = {};
   Level lv[kMaxLevels];
   int nlev = 0;
   // inverse of the coarsest level's reduced matrix (when it has few enough unknowns)
@@ -152,6 +250,12 @@ int launch_sico_masks(Ctx* c);
 int launch_prepare_afac(Ctx* c);
 int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva, bool layer_only = false);
 int launch_picard_update(Ctx* c, double* u, double* v, const double* xu, const double* xv, bool diva);
+// Anderson mixing step before launch_picard_update (picard_anderson_m > 0): the map value
+// g = velocity-limited linear solution, its residual f = g - u, the new history columns
+// and the mixing coefficients (device scalars); launch_picard_update then forms the
+// mixed iterate g - sum gamma_i dG_i in place of the relaxation.
+int launch_anderson_prepare(Ctx* c, const double* u, const double* v, const double* xu, const double* xv);
+int anderson_reset(Ctx* c);   // empty history at the start of a solve (zeroed columns)
 int launch_commit_err(Ctx* c);
 int launch_basal_stress_velocities(Ctx* c);
 int launch_visc_b_output(Ctx* c);

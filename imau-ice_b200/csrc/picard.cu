@@ -379,12 +379,130 @@ __global__ void k_afac(Dims d, double n_flow, const double* A, double* afac) {
   }
 }
 
+// apply_velocity_limits (:1432-1498) of the linear solution at a cx point: |u| with v mapped
+// to the cx grid (map_cy_to_cx_2D :1757-1797), scaled down to vmax
+__device__ __forceinline__ double limited_u(const Dims& d, const double* xu, const double* xv, double vmax, int j,
+                                            int i) {
+  const int ny = d.ny;
+  auto XV = [&](int jj, int ii) { return xv[d.at(jj, ii)]; };
+  double vcx;
+  if (j > 0 && j < ny - 1) vcx = (XV(j - 1, i) + XV(j - 1, i + 1) + XV(j, i) + XV(j, i + 1)) / 4.0;
+  else if (j == 0) vcx = (XV(0, i) + XV(0, i + 1)) / 2.0;
+  else vcx = (XV(ny - 2, i) + XV(ny - 2, i + 1)) / 2.0;
+  double un = xu[d.at(j, i)];
+  const double uabs = sqrt(un * un + vcx * vcx);
+  if (uabs > vmax) un = un * vmax / uabs;
+  return un;
+}
+// the same at a cy point, u mapped to the cy grid (map_cx_to_cy_2D :1718-1756)
+__device__ __forceinline__ double limited_v(const Dims& d, const double* xu, const double* xv, double vmax, int j,
+                                            int i) {
+  const int nx = d.nx;
+  auto XU = [&](int jj, int ii) { return xu[d.at(jj, ii)]; };
+  double ucy;
+  if (i > 0 && i < nx - 1) ucy = (XU(j, i - 1) + XU(j, i) + XU(j + 1, i - 1) + XU(j + 1, i)) / 4.0;
+  else if (i == 0) ucy = (XU(j, 0) + XU(j + 1, 0)) / 2.0;
+  else ucy = (XU(j, nx - 2) + XU(j + 1, nx - 2)) / 2.0;
+  double vn = xv[d.at(j, i)];
+  const double vabs = sqrt(ucy * ucy + vn * vn);
+  if (vabs > vmax) vn = vn * vmax / vabs;
+  return vn;
+}
+
+// ---- Anderson mixing of the viscosity iteration (picard_anderson_m > 0) --------------
+// No counterpart in the reference, whose update is the relaxation :1499-1529.  The map is
+// one unrelaxed Picard step, g(u) = velocity-limited solution of A(u) x = b(u); with the
+// residual f = g(u) - u and the differences dF_i = f_i+1 - f_i, dG_i = g_i+1 - g_i of the
+// last m iterations, the next iterate is g - sum_i gamma_i dG_i, gamma the least-squares
+// minimiser of |f - sum_i gamma_i dF_i| (u on the cx points and v on the cy points make
+// one vector).  k_aa_prepare writes g, f and the newest difference columns and reduces
+// the inner products of the newest dF and of f with every history column; k_aa_solve
+// updates the Gram matrix and solves for gamma on one thread; k_picard_update mixes.
+struct AAArgs {
+  Dims d;
+  int m, nblk_x;
+  double vmax;
+  const double *u, *v, *xu, *xv;
+  double *dFu[kAAMax], *dFv[kAAMax], *dGu[kAAMax], *dGv[kAAMax];
+  double *fu, *fv, *gu, *gv;   // previous f, g on entry; this iteration's on exit
+  const double* sc;
+  double* partials;            // kAAPartials per block: dF_i . dF_new, then dF_i . f
+};
+
+__global__ void __launch_bounds__(256) k_aa_prepare(AAArgs a) {
+  const Dims d = a.d;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  const bool have = a.sc[SC_AA_HAVE] != 0.0;
+  const int s = (int)a.sc[SC_AA_HEAD];
+  double acc[kAAPartials];
+#pragma unroll
+  for (int k = 0; k < kAAPartials; ++k) acc[k] = 0.0;
+  if (j < d.ny && i < d.nx) {
+    const long long q = d.at(j, i);
+    auto point = [&](double g, double x, double* fp, double* gp, double* const* dF, double* const* dG) {
+      const double f = g - x;
+      if (have) {
+        const double df = f - fp[q];
+        dF[s][q] = df;
+        dG[s][q] = g - gp[q];
+        for (int k = 0; k < a.m; ++k) {
+          const double c = (k == s) ? df : dF[k][q];
+          acc[k] += c * df;
+          acc[kAAMax + k] += c * f;
+        }
+      }
+      fp[q] = f;
+      gp[q] = g;
+    };
+    if (i < d.nx - 1) point(limited_u(d, a.xu, a.xv, a.vmax, j, i), a.u[q], a.fu, a.gu, a.dFu, a.dGu);
+    if (j < d.ny - 1) point(limited_v(d, a.xu, a.xv, a.vmax, j, i), a.v[q], a.fv, a.gv, a.dFv, a.dGv);
+  }
+  // block sums in groups of at most four values (block_sum keeps one shared array per width)
+  double* out = a.partials + (long long)kAAPartials * (blockIdx.y * a.nblk_x + blockIdx.x);
+  for (int base = 0; base < kAAPartials; base += 4) {
+    double v4[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v4[k] = base + k < kAAPartials ? acc[base + k] : 0.0;
+    block_sum<4>(v4);
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+      for (int k = 0; k < 4 && base + k < kAAPartials; ++k) out[base + k] = v4[k];
+    __syncthreads();
+  }
+}
+
+// One thread: fixed-order sums of the partials, the Gram matrix update and the mixing
+// coefficients.  Shared with the oracle's restatement (aa_coefficients).
+__global__ void k_aa_solve(const double* partials, int nblocks, int m, double* sc) {
+  __shared__ double sh[kAAPartials][256];
+  double t[kAAPartials];
+#pragma unroll
+  for (int k = 0; k < kAAPartials; ++k) t[k] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int k = 0; k < kAAPartials; ++k) t[k] += partials[(long long)kAAPartials * b + k];
+  for (int k = 0; k < kAAPartials; ++k) sh[k][threadIdx.x] = t[k];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < kAAPartials; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  double dots[kAAPartials];
+  for (int k = 0; k < kAAPartials; ++k) dots[k] = sh[k][0];
+  aa_coefficients(sc, m, dots);
+}
+
 struct UpdArgs {
   Dims d;
   int diva, sliding_none, basal_freezing, nblk_x;
   double vmax, rel, dT_freeze;
   const double *xu, *xv;           // linear solution
   double *u, *v, *up, *vp;         // velocities (relaxed in place) and the previous iterate
+  // Anderson mixing (aa_m > 0): the iterate is g - sum gamma_i dG_i instead of the relaxation
+  int aa_m;
+  const double* sc;
+  const double *gu, *gv;
+  const double *dGu[kAAMax], *dGv[kAAMax];
   const double *uchk, *vchk;       // fields tested by estimate_visc_iter_UV_errors
   double *errx, *erry;             // DIVA_err candidates
   const double *bex, *bey, *F2, *Hi, *Ti, *Tpmp;
@@ -399,23 +517,21 @@ __global__ void __launch_bounds__(256) k_picard_update(UpdArgs a) {
   if (j < d.ny && i < d.nx) {
     const int nx = d.nx, ny = d.ny;
     const long long q = d.at(j, i);
-    auto XU = [&](int jj, int ii) { return a.xu[d.at(jj, ii)]; };
-    auto XV = [&](int jj, int ii) { return a.xv[d.at(jj, ii)]; };
     bool frozen = false;
     if (a.diva && a.basal_freezing) {
       const long long ob = (long long)(d.nz - 1) * d.plane + q;
       frozen = a.Tpmp[ob] - a.Ti[ob] > a.dT_freeze;
     }
     if (i < nx - 1) {
-      double vcx;   // map_cy_to_cx_2D :1757-1797
-      if (j > 0 && j < ny - 1) vcx = (XV(j - 1, i) + XV(j - 1, i + 1) + XV(j, i) + XV(j, i + 1)) / 4.0;
-      else if (j == 0) vcx = (XV(0, i) + XV(0, i + 1)) / 2.0;
-      else vcx = (XV(ny - 2, i) + XV(ny - 2, i + 1)) / 2.0;
-      double un = XU(j, i);
-      const double uabs = sqrt(un * un + vcx * vcx);
-      if (uabs > a.vmax) un = un * a.vmax / uabs;
       const double uo = a.u[q];
-      un = a.rel * un + (1.0 - a.rel) * uo;
+      double un;
+      if (a.aa_m > 0) {
+        un = a.gu[q];
+        for (int k = 0; k < a.aa_m; ++k) un -= a.sc[SC_AA_GAMMA + k] * a.dGu[k][q];
+      } else {
+        un = limited_u(d, a.xu, a.xv, a.vmax, j, i);
+        un = a.rel * un + (1.0 - a.rel) * uo;
+      }
       a.up[q] = uo;
       a.u[q] = un;
       if (fabs(un) > kVelTol) {
@@ -437,15 +553,15 @@ __global__ void __launch_bounds__(256) k_picard_update(UpdArgs a) {
       }
     }
     if (j < ny - 1) {
-      double ucy;   // map_cx_to_cy_2D :1718-1756
-      if (i > 0 && i < nx - 1) ucy = (XU(j, i - 1) + XU(j, i) + XU(j + 1, i - 1) + XU(j + 1, i)) / 4.0;
-      else if (i == 0) ucy = (XU(j, 0) + XU(j + 1, 0)) / 2.0;
-      else ucy = (XU(j, nx - 2) + XU(j + 1, nx - 2)) / 2.0;
-      double vn = XV(j, i);
-      const double vabs = sqrt(ucy * ucy + vn * vn);
-      if (vabs > a.vmax) vn = vn * a.vmax / vabs;
       const double vo = a.v[q];
-      vn = a.rel * vn + (1.0 - a.rel) * vo;
+      double vn;
+      if (a.aa_m > 0) {
+        vn = a.gv[q];
+        for (int k = 0; k < a.aa_m; ++k) vn -= a.sc[SC_AA_GAMMA + k] * a.dGv[k][q];
+      } else {
+        vn = limited_v(d, a.xu, a.xv, a.vmax, j, i);
+        vn = a.rel * vn + (1.0 - a.rel) * vo;
+      }
       a.vp[q] = vo;
       a.v[q] = vn;
       if (fabs(vn) > kVelTol) {
@@ -919,10 +1035,48 @@ int launch_picard_update(Ctx* c, double* u, double* v, const double* xu, const d
   a.taubx = c->D(DIVA_F_TAUB_CX); a.tauby = c->D(DIVA_F_TAUB_CY);
   a.ubx = c->D(DIVA_F_U_BASE_CX); a.vby = c->D(DIVA_F_V_BASE_CY);
   a.partials = c->partials;
+  a.aa_m = C.picard_anderson_m;
+  a.sc = c->scal;
+  a.gu = c->aa_g[0]; a.gv = c->aa_g[1];
+  for (int k = 0; k < kAAMax; ++k) { a.dGu[k] = c->aa_dG[k][0]; a.dGv[k] = c->aa_dG[k][1]; }
   k_picard_update<<<g, block2d(), 0, c->stream>>>(a); c->launches++;
   DIVA_LAUNCHED(c, "k_picard_update");
   k_sum_partials<<<1, 256, 0, c->stream>>>(c->partials, (int)(g.x * g.y), 3, c->scal + SC_RES1); c->launches++;
   DIVA_LAUNCHED(c, "k_sum_partials");
+  return DIVA_OK;
+}
+
+int launch_anderson_prepare(Ctx* c, const double* u, const double* v, const double* xu, const double* xv) {
+  const diva_config_t& C = c->c;
+  AAArgs a{};
+  a.d = c->d;
+  a.m = C.picard_anderson_m;
+  const dim3 g = grid2d(c->d.ny, c->d.nx);
+  a.nblk_x = g.x;
+  a.vmax = C.DIVA_vel_max;
+  a.u = u; a.v = v; a.xu = xu; a.xv = xv;
+  for (int k = 0; k < kAAMax; ++k) {
+    a.dFu[k] = c->aa_dF[k][0]; a.dFv[k] = c->aa_dF[k][1];
+    a.dGu[k] = c->aa_dG[k][0]; a.dGv[k] = c->aa_dG[k][1];
+  }
+  a.fu = c->aa_f[0]; a.fv = c->aa_f[1]; a.gu = c->aa_g[0]; a.gv = c->aa_g[1];
+  a.sc = c->scal;
+  a.partials = c->partials;
+  k_aa_prepare<<<g, block2d(), 0, c->stream>>>(a); c->launches++;
+  DIVA_LAUNCHED(c, "k_aa_prepare");
+  k_aa_solve<<<1, 256, 0, c->stream>>>(c->partials, (int)(g.x * g.y), a.m, c->scal); c->launches++;
+  DIVA_LAUNCHED(c, "k_aa_solve");
+  return DIVA_OK;
+}
+
+// start of a solve: empty history, zeroed columns (unused slots then mix in nothing)
+int anderson_reset(Ctx* c) {
+  if (c->c.picard_anderson_m <= 0) return DIVA_OK;
+  for (int q = 0; q < 2; ++q)
+    for (int k = 0; k < kAAMax; ++k) {
+      DIVA_CUDA(c, cudaMemsetAsync(c->aa_dF[k][q], 0, sizeof(double) * c->d.plane, c->stream));
+      DIVA_CUDA(c, cudaMemsetAsync(c->aa_dG[k][q], 0, sizeof(double) * c->d.plane, c->stream));
+    }
   return DIVA_OK;
 }
 

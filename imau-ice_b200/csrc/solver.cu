@@ -2380,6 +2380,7 @@ int capture_iteration(Ctx* c, CaptureCtx& cc, cudaStream_t top, bool diva, Picar
   k_ctl_lin_finish<<<1, 1, 0, c->stream>>>(c->scal); c->launches++;
   k_fill_boundary<<<g2, block2d(), 0, c->stream>>>(d, c->bc, U_(KV_X), V_(KV_X)); c->launches++;
   DIVA_LAUNCHED(c, "graph tail");
+  if (C.picard_anderson_m > 0 && (st = launch_anderson_prepare(c, u, v, U_(KV_X), V_(KV_X)))) return st;
   if ((st = launch_picard_update(c, u, v, U_(KV_X), V_(KV_X), diva))) return st;
   if ((st = launch_ctl_end(c, relmode))) return st;
   if ((st = launch_err_commit_pred(c))) return st;

@@ -173,7 +173,16 @@ typedef struct {
    * 415-417; default off, -2000 m) */
   int32_t remove_shelves_larger_than_PD, continental_shelf_calving;
   double  continental_shelf_min_height;
-  int32_t reserved[8];
+  /* Nonlinear iteration (no reference counterpart): 0 = the reference's relaxed Picard
+   * update u <- relax x + (1 - relax) u_prev (ice_velocity_module.f90:1499-1529); m in 1..5 =
+   * Anderson mixing of depth m on the unrelaxed Picard map g(u) (the velocity-limited
+   * linear solution): u <- g - sum_i gamma_i (g_i+1 - g_i), with gamma minimising
+   * || f - sum_i gamma_i (f_i+1 - f_i) ||_2 over the last m residuals f = g(u) - u
+   * (velocities on the cx and cy points).  Needs picard_stop = DIVA_STOP_RELRES: the
+   * stop test is the nonlinear residual, so the converged state solves the same equations
+   * as with the relaxed update; only the path there, and its length, change. */
+  int32_t picard_anderson_m;
+  int32_t reserved[7];
 } diva_config_t;
 
 /* ---- per-solve report --------------------------------------------------- */
@@ -383,8 +392,9 @@ int  diva_profile_kernel(diva_ctx_t* ctx, int32_t which, int32_t reps, double* m
  * every GPU loading the library holds until exit, enough for grids of at most
  * 16384 thread blocks of 32 x 8 columns, i.e. ceil(ny/32) * ceil(nx/8) <=
  * 16384 (2048 x 2048 fits); larger grids return DIVA_BAD_INPUT.  The first
- * call on a device looks up the scratch array's device address (with that
- * device current) and caches it, so make the first call before any stream
+ * call on a device (more exactly: in each CUDA context, so again after a
+ * cudaDeviceReset) looks up the scratch array's device address with that
+ * device current and caches it, so make that first call before any stream
  * capture.  All calls share the scratch array: calls that overlap on the GPU
  * race, so serialise them. */
 int  diva_visc_iter_uv_resid_noalloc(int32_t nx, int32_t ny, const double* u_cx, const double* u_cx_prev,

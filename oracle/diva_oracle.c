@@ -87,6 +87,12 @@ typedef struct orc_ctx {
   int threads;              /* threads of the timed CPU baseline (1: the sequential algorithm) */
   struct orc_pool* pool;    /* their workers (NULL with one thread) */
   long lin_iters_total;
+  /* Anderson mixing of the viscosity iteration (picard_anderson_m > 0): history columns of
+   * residual differences dF and map differences dG (u on cx points then v on cy points),
+   * the previous residual f and map value g, and the small least-squares state */
+  double *aa_dF[5], *aa_dG[5], *aa_f, *aa_g;
+  int aa_have, aa_n, aa_head, aa_restarts;
+  double aa_G[25], aa_rhs[5], aa_gamma[5], aa_rprev;
   char err[512];
 } orc_ctx;
 
@@ -2058,6 +2064,145 @@ static void fill_err(orc_ctx* c) {
   for (size_t q = 0; q < (size_t)(ny - 1) * nx; ++q) ey[q] = 1E5;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Anderson mixing of the viscosity iteration (picard_anderson_m > 0).  No counterpart in
+ * the reference, whose update is relax_DIVA_visc_iterations (:1499-1529): the oracle's own
+ * restatement of the GPU library's mixing step, to check it.  The map is one unrelaxed
+ * Picard step g(u) (the velocity-limited linear solution), f = g(u) - u, dF_i / dG_i the
+ * differences of consecutive residuals / map values; the next iterate is
+ * g - sum gamma_i dG_i with gamma minimising |f - sum gamma_i dF_i|_2 over the n <= m most
+ * recent columns (normal equations scaled to unit diagonal, + 1e-10; on a Cholesky pivot
+ * below 1e-12 the oldest column is dropped).  A nonlinear residual 10 x the previous
+ * step's drops the older columns. */
+#define AA_MAX 5
+
+static void aa_reset(orc_ctx* c) {
+  const size_t n = (size_t)c->ny * (c->nx - 1) + (size_t)(c->ny - 1) * c->nx;
+  for (int k = 0; k < AA_MAX; ++k) {
+    if (!c->aa_dF[k]) c->aa_dF[k] = (double*)malloc(sizeof(double) * n);
+    if (!c->aa_dG[k]) c->aa_dG[k] = (double*)malloc(sizeof(double) * n);
+    memset(c->aa_dF[k], 0, sizeof(double) * n);
+    memset(c->aa_dG[k], 0, sizeof(double) * n);
+  }
+  if (!c->aa_f) c->aa_f = (double*)malloc(sizeof(double) * n);
+  if (!c->aa_g) c->aa_g = (double*)malloc(sizeof(double) * n);
+  c->aa_have = 0; c->aa_n = 0; c->aa_head = 0; c->aa_restarts = 0; c->aa_rprev = 0.0;
+  memset(c->aa_G, 0, sizeof(c->aa_G));
+}
+
+/* gamma from dots[0..m) = dF_i . dF_new and dots[AA_MAX..AA_MAX+m) = dF_i . f */
+static void aa_coefficients(orc_ctx* c, int m, const double* dots, double relres) {
+  double* G = c->aa_G;
+  for (int k = 0; k < AA_MAX; ++k) c->aa_gamma[k] = 0.0;
+  const double rprev = c->aa_rprev;
+  c->aa_rprev = relres;
+  if (!c->aa_have) { c->aa_have = 1; c->aa_n = 0; c->aa_head = 0; return; }
+  const int s = c->aa_head;
+  int n = c->aa_n;
+  if (rprev > 0.0 && relres > 10.0 * rprev) { n = 0; c->aa_restarts++; }
+  for (int i = 0; i < m; ++i) {
+    G[s * AA_MAX + i] = dots[i];
+    G[i * AA_MAX + s] = dots[i];
+    c->aa_rhs[i] = dots[AA_MAX + i];
+  }
+  n = n + 1 < m ? n + 1 : m;
+  c->aa_head = (s + 1) % m;
+  int idx[AA_MAX];
+  for (int k = 0; k < n; ++k) idx[k] = (s - k + m) % m;
+  for (int nn = n; nn > 0; --nn) {
+    double A[AA_MAX][AA_MAX], b[AA_MAX], dk[AA_MAX], y[AA_MAX];
+    int ok = 1;
+    for (int k = 0; k < nn && ok; ++k) {
+      dk[k] = sqrt(G[idx[k] * AA_MAX + idx[k]]);
+      ok = dk[k] > 0.0 && dk[k] < 1e300;
+    }
+    if (!ok) continue;
+    for (int k = 0; k < nn; ++k) {
+      for (int l = 0; l < nn; ++l) A[k][l] = G[idx[k] * AA_MAX + idx[l]] / (dk[k] * dk[l]);
+      A[k][k] += 1e-10;
+      b[k] = c->aa_rhs[idx[k]] / dk[k];
+    }
+    for (int k = 0; k < nn && ok; ++k) {
+      double p = A[k][k];
+      for (int l = 0; l < k; ++l) p -= A[k][l] * A[k][l];
+      if (!(p > 1e-12)) { ok = 0; break; }
+      const double r = sqrt(p);
+      A[k][k] = r;
+      for (int i = k + 1; i < nn; ++i) {
+        double t = A[i][k];
+        for (int l = 0; l < k; ++l) t -= A[i][l] * A[k][l];
+        A[i][k] = t / r;
+      }
+    }
+    if (!ok) continue;
+    for (int k = 0; k < nn; ++k) {
+      double t = b[k];
+      for (int l = 0; l < k; ++l) t -= A[k][l] * y[l];
+      y[k] = t / A[k][k];
+    }
+    for (int k = nn - 1; k >= 0; --k) {
+      double t = y[k];
+      for (int l = k + 1; l < nn; ++l) t -= A[l][k] * y[l];
+      y[k] = t / A[k][k];
+    }
+    for (int k = 0; k < nn; ++k) ok = ok && isfinite(y[k]);
+    if (!ok) continue;
+    for (int k = 0; k < nn; ++k) c->aa_gamma[idx[k]] = y[k] / dk[k];
+    c->aa_n = nn;
+    return;
+  }
+  c->aa_n = 0;
+}
+
+/* on entry u, v hold the map value g and U_CX_PREV / V_CY_PREV the iterate; on exit u, v
+ * hold the mixed iterate */
+static void anderson_mix(orc_ctx* c, double* u, double* v, double relres) {
+  DECL_DIMS(c);
+  const int m = c->c.picard_anderson_m;
+  const double *up = FD(c, U_CX_PREV), *vp = FD(c, V_CY_PREV);
+  const size_t ncx = (size_t)ny * (nx - 1);
+  const int s = c->aa_head, have = c->aa_have;
+  double dots[2 * AA_MAX] = {0};
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      for (int comp = 0; comp < 2; ++comp) {
+        size_t q;
+        double g, x;
+        if (comp == 0) { if (i >= nx - 1) continue; q = ICX(j, i); g = u[q]; x = up[q]; }
+        else { if (j >= ny - 1) continue; q = ncx + ICY(j, i); g = v[ICY(j, i)]; x = vp[ICY(j, i)]; }
+        const double f = g - x;
+        if (have) {
+          const double df = f - c->aa_f[q];
+          c->aa_dF[s][q] = df;
+          c->aa_dG[s][q] = g - c->aa_g[q];
+          for (int k = 0; k < m; ++k) {
+            const double col = (k == s) ? df : c->aa_dF[k][q];
+            dots[k] += col * df;
+            dots[AA_MAX + k] += col * f;
+          }
+        }
+        c->aa_f[q] = f;
+        c->aa_g[q] = g;
+      }
+    }
+  aa_coefficients(c, m, dots, relres);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      if (i < nx - 1) {
+        const size_t q = ICX(j, i);
+        double w = c->aa_g[q];
+        for (int k = 0; k < m; ++k) w -= c->aa_gamma[k] * c->aa_dG[k][q];
+        u[q] = w;
+      }
+      if (j < ny - 1) {
+        const size_t q = ncx + ICY(j, i);
+        double w = c->aa_g[q];
+        for (int k = 0; k < m; ++k) w -= c->aa_gamma[k] * c->aa_dG[k][q];
+        v[ICY(j, i)] = w;
+      }
+    }
+}
+
 /* shared Picard loop of solve_SSA (:180-240) and solve_DIVA (:307-363) */
 static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep) {
   DECL_DIMS(c);
@@ -2069,6 +2214,8 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
   const int relmode = (C->picard_stop == DIVA_STOP_RELRES);
   int exited_by_relres = 0;
   double eta = C->lin_adaptive_eta, relres_prev = 0.0;
+  const int aa = relmode && C->picard_anderson_m > 0;
+  if (aa) aa_reset(c);
   for (;;) {
     ++it;
     if (diva) calc_vertical_shear_strain_rates(c);
@@ -2113,7 +2260,8 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
     c->true_residual = 0;
     if (st != DIVA_OK) status = st;
     apply_velocity_limits(c, u, v);
-    relax_visc_iterations(c, u, v, C->DIVA_visc_it_relax);
+    if (aa) anderson_mix(c, u, v, relres);
+    else relax_visc_iterations(c, u, v, C->DIVA_visc_it_relax);
     resid = calc_visc_iter_UV_resid(c, u, v);
     int converged = 0;
     if (!relmode && resid < C->DIVA_visc_it_norm_dUV_tol) converged = 1;
@@ -2296,6 +2444,8 @@ int orc_destroy(orc_ctx* c) {
   for (int f = 0; f < DIVA_NUM_FIELDS; ++f) { free(c->F[f]); free(c->S[f]); }
   free(c->ij2n_u); free(c->ij2n_v); free(c->n2ij);
   free(c->m.ptr); free(c->m.idx); free(c->m.val); free(c->m.b); free(c->m.x);
+  for (int k = 0; k < AA_MAX; ++k) { free(c->aa_dF[k]); free(c->aa_dG[k]); }
+  free(c->aa_f); free(c->aa_g);
   pool_destroy(c->pool);
   free(c);
   return DIVA_OK;

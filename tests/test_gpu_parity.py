@@ -53,6 +53,14 @@ CASES = {
     "channel_2.5km_front_BC_relres": (1, 2.5e3, {"choice_ice_margin": "BC", "picard_stop": "relres",
                                                  "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 300,
                                                  "lin_rtol": 1e-12}, {"calving_front": True}),
+    # Anderson mixing of depth 3 in place of the relaxation (picard_anderson_m), exact linear
+    # solves on both sides: the GPU's mixing step against the oracle's restatement of it
+    "channel_5km_anderson_relres": (1, None, {"picard_stop": "relres", "picard_relres_tol": 1e-6,
+                                              "DIVA_visc_it_nit": 300, "lin_rtol": 1e-12,
+                                              "picard_anderson_m": 3}),
+    "icecap_40km_anderson_relres": (2, 40e3, {"picard_stop": "relres", "picard_relres_tol": 1e-6,
+                                              "DIVA_visc_it_nit": 300, "lin_rtol": 1e-12,
+                                              "picard_anderson_m": 3}),
 }
 
 
@@ -146,29 +154,62 @@ def test_ssa_schoof_icestream(cuda, oracle):
     assert helpers.rel_l2(og["u_SSA_cx"], oo["u_SSA_cx"]) <= 1e-6
 
 
-def test_full_size_icecap_against_the_oracle(cuda, oracle):
-    """321 x 561 x 15: masks bit-exact, SIA velocities to 1e-12, and the GPU's converged
-    DIVA state satisfies the oracle's own nonlinear equations to rel-res 1e-6."""
-    g, cfg, f = helpers.make_case(2, overrides={"picard_stop": "relres", "picard_relres_tol": 1e-6,
-                                                "DIVA_visc_it_nit": 400, "lin_adaptive": 1, "lin_rtol": 1e-10})
+def _oracle_threads():
+    import os
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    return max(1, min(n, 32))
+
+
+FULL_SIZE = {
+    # SURVEY config 2 as specified: Picard stop on the reference's step norm (tol 1e-3), every
+    # linear solve to 1e-12 (exact for the fixed point: the oracle's solutions at 1e-10 and
+    # 1e-12 differ by 9e-10 relative L2)
+    "icecap321x561_reference_stop": {"lin_rtol": 1e-12},
+    # the headline stop rule, rel-res 1e-6, with exact linear solves on both sides
+    "icecap321x561_relres": {"picard_stop": "relres", "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 400,
+                             "lin_adaptive": 0, "lin_rtol": 1e-12},
+    # the same with Anderson mixing of depth 3 in place of the relaxation
+    "icecap321x561_anderson_relres": {"picard_stop": "relres", "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 400,
+                                      "lin_adaptive": 0, "lin_rtol": 1e-12, "picard_anderson_m": 3},
+}
+
+
+@pytest.fixture(scope="module", params=list(FULL_SIZE))
+def full_pair(request, cuda, oracle):
+    g, cfg, f = helpers.make_case(2, overrides=FULL_SIZE[request.param])
     ctx = diva.Context(g, cfg, cuda)
     helpers.prepare(ctx, f)
     ctx.calc_sia_3d_velocities()
-    rep = ctx.solve_DIVA()
-    gpu = ctx.download()
+    rg = ctx.solve_DIVA()
+    og = ctx.download()
     ctx.close()
-    assert rep["status"] == 0 and rep["relres"] <= 1e-6
     octx = diva.Context(g, cfg, oracle)
+    ob.set_linear_solver(octx, ob.LIN_GMRES_WARM, 1e-12, 0.0)
+    ob.set_threads(octx, _oracle_threads())
     helpers.prepare(octx, f)
     octx.calc_sia_3d_velocities()
-    oracle.lib.orc_prepare_diva(octx.h)      # driving stress, basal conditions, grounded fractions
-    ref = octx.download()
-    for m in MASKS[:10]:
-        assert np.array_equal(gpu[m], ref[m]), m
-    for k in ("u_3D_SIA_cx", "v_3D_SIA_cy", "f_grnd_cx", "A_flow_3D_a"):
-        assert helpers.rel_l2(gpu[k], ref[k]) <= 1e-12, k
-    # hand the GPU state to the oracle and evaluate the reference equations there
-    octx.upload({k: gpu[k] for k in ("u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "taub_cx", "taub_cy")})
-    r = octx.nonlinear_residual()
+    ro = octx.solve_DIVA()
+    oo = octx.download()
     octx.close()
-    assert r <= 2e-6
+    return request.param, rg, og, ro, oo
+
+
+def test_full_size_icecap_velocities_within_1e6(full_pair):
+    """321 x 561 x 15, the GPU's converged DIVA solve against the oracle's on the same seeded
+    inputs: masks bit-exact, SIA velocities to 1e-12, the same number of viscosity iterations,
+    u and v together within relative L2 1e-6 (and the 3D and basal velocities)."""
+    name, rg, og, ro, oo = full_pair
+    for m in MASKS:
+        assert np.array_equal(og[m], oo[m]), m
+    for k in ("u_3D_SIA_cx", "v_3D_SIA_cy", "f_grnd_cx", "A_flow_3D_a"):
+        assert helpers.rel_l2(og[k], oo[k]) <= 1e-12, k
+    assert rg["status"] == 0 and ro["status"] == 0, (rg, ro)
+    assert rg["picard_iterations"] == ro["picard_iterations"], (rg, ro)
+    assert uv_rel(og, oo) <= 1e-6, uv_rel(og, oo)
+    for k in VELOCITY_3D:
+        assert helpers.rel_l2(og[k], oo[k]) <= 1e-6, k
+    if "relres" in name:
+        assert 0 <= rg["relres"] <= 1e-6 and 0 <= ro["relres"] <= 1e-6
