@@ -51,27 +51,42 @@ UNIT = "solves/s"
 INPUT_FIELDS = ["Hi_a", "Hb_a", "SL_a", "dHb_dt_a", "Ti_a", "beta_sq_a"]
 STATE_FIELDS = ["u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "taub_cx", "taub_cy", "u_3D_a", "v_3D_a"]
 OUTPUT_FIELDS = ["u_vav_cx", "v_vav_cy", "u_3D_cx", "v_3D_cy", "w_3D_a", "u_3D_SIA_cx", "v_3D_SIA_cy"]
-KERNEL_NAMES = {0: "column coefficients (k_column_prep, k_layer_viscosity, k_column_integrals, k_face_coefficients)", 1: "k_smooth_down+k_smooth_up (fine level)", 2: "k_matvec",
+KERNEL_NAMES = {0: "K1 column coefficients (all launches of one viscosity iteration)",
+                1: "k_smooth_down+k_smooth_up (fine level)", 2: "k_matvec",
                 3: "V-cycle (all levels)", 4: "k_subcycle (coarse levels, one block)",
                 5: "k_layer_viscosity"}
-TRAFFIC_KEYS = {5: "k_layer_viscosity_icecap321x561", 1: "k_smooth_down_icecap321x561",
-                4: "k_subcycle_icecap321x561"}
+# committed ncu summaries holding the DRAM bytes of one launch of each part
+TRAFFIC_KEYS = {0: "k1_icecap321x561", 3: "vcycle_icecap321x561"}
 
 
-def workload(seed=2, precision="fp64"):
+def workload(seed=2, precision="fp64", anderson=0, eta=None):
+    """The ice cap, solved cold to rel-res 1e-6.  anderson = 0: the reference's relaxed
+    Picard update with the adaptive linear tolerance 0.5 min(1, rel-res); anderson = m > 0:
+    Anderson mixing of depth m, linear tolerance factor 0.1 unless eta is given."""
     from imau_ice_b200 import synth
     g, cfg, fields = synth.ice_cap(seed=seed)
     cfg = dict(cfg)
     cfg.update(picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1, lin_rtol=1e-10,
-               precision=precision)
+               precision=precision, picard_anderson_m=anderson,
+               lin_adaptive_eta=eta if eta is not None else (0.1 if anderson else 0.5))
     return g, cfg, fields
+
+
+def nonlinear_json(cfg):
+    m = cfg.get("picard_anderson_m", 0)
+    it = (f"Anderson mixing of depth {m} on the unrelaxed Picard map" if m else
+          f"the reference's relaxed Picard update (relax {cfg.get('DIVA_visc_it_relax', 0.4)})")
+    return {"nonlinear_iteration": it,
+            "linear_solver": "BiCGStab + geometric multigrid V(2,2), adaptive tolerance "
+                             f"{cfg['lin_adaptive_eta']:g} min(1, rel-res)"}
 
 
 def config_json(g, extra=None):
     c = {"workload": "DIVA+SIA cold-start solve, synthetic ice cap 1600x2800 km @5 km",
          "nx": g["nx"], "ny": g["ny"], "nz": len(g["zeta"]), "stop": "nonlinear rel-res <= 1e-6",
-         "linear_solver": "BiCGStab + geometric multigrid V(2,2), adaptive tolerance 0.5 min(1, rel-res)",
-         "l2": "inputs larger than L2 (working set ~0.6 GB > 126 MB)"}
+         "l2": "inputs larger than L2: each step is a whole solve over ~0.6 GB of device state; the 3D "
+               "fields (21.6 MB each) stream from HBM every viscosity iteration, the 2D multigrid "
+               "levels (~17 MB at level 0) stay L2-resident within a solve; no flush"}
     c.update(extra or {})
     return c
 
@@ -196,7 +211,10 @@ def run_reference(args):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ice cap)",
            "config": config_json(g, {"parallelism": f"CPU oracle port on {threads} host threads (block-Jacobi "
-                                                     f"ILU(0) over {threads} row blocks, column loops split)"}),
+                                                     f"ILU(0) over {threads} row blocks, column loops split)",
+                                     "nonlinear_iteration": "the reference's relaxed Picard update (relax 0.4)",
+                                     "linear_solver": "GMRES(30) + ILU(0) from the current iterate, adaptive "
+                                                      "tolerance 0.5 min(1, rel-res)"}),
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                             "sample": "each step " + last["sample"]},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -220,7 +238,7 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     build.build()
 
-    g, cfg, fields = workload(precision=args.precision)
+    g, cfg, fields = workload(precision=args.precision, anderson=args.anderson, eta=args.eta)
     grid = diva.Grid(**g)
     ctx = diva.Context(grid, cfg)
     stream = torch.cuda.Stream()
@@ -273,19 +291,17 @@ def run_b200(args):
     picard = [r["picard_iterations"] for r in reps]
     mg = [r["mg_cycles"] for r in reps]
 
-    # roofline of the dominant kernel: time share = launches per solve x time per launch
+    # roofline of the dominant part of the solve, by device time per solve = time per launch
+    # (CUDA events on the solve's stream, the part run alone on the converged state) x launches
+    # per solve.  Candidates: the column coefficients K1 (four launches per viscosity iteration,
+    # 480 B per column: (3 nz + 15) x 8) and one multigrid V-cycle (all levels; per level the
+    # smoothing sweeps, residual and transfers, weighted by its points); sub-parts of the
+    # V-cycle ride along in other_kernels.
     prof = {}
     for which in (0, 1, 2, 3, 4, 5):
         prof[which] = ctx.profile_kernel(which, reps=30 if which else 10)
-    # device time per solve of each part, from its in-situ time per launch x launches per solve
-    per_solve = {0: prof[0][0] * statistics.mean(picard),
-                 # tiled grids: one pre/post kernel pair per V-cycle (24 values per column), else
-                 # V(2,2) as four per-colour sweeps (10 values per column each)
-                 1: prof[1][0] * statistics.mean(mg) * (1 if prof[1][1] >= 20 * 8 * g["nx"] * g["ny"] else 4),
-                 4: prof[4][0] * statistics.mean(mg)}
+    per_solve = {0: prof[0][0] * statistics.mean(picard), 3: prof[3][0] * statistics.mean(mg)}
     dom = max(per_solve, key=per_solve.get)
-    if dom == 0:   # the column coefficients are four launches: report their largest, the layer step
-        dom = 5
     ms_l, bytes_l = prof[dom]
     hbm_peak = None
     peak_src = "fallback 6650 GB/s"
@@ -295,16 +311,14 @@ def run_b200(args):
     except Exception:
         hbm_peak = 6650.0
     achieved = bytes_l / (ms_l * 1e-3) / 1e9
-    traffic_key = TRAFFIC_KEYS[dom]
     roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": read_traffic(traffic_key),
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": read_traffic(TRAFFIC_KEYS[dom]),
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": bytes_l, "ms_per_launch": ms_l,
-                "other_kernels": {KERNEL_NAMES[w]: {"ms_per_launch": prof[w][0],
+                "launches_per_solve": statistics.mean(picard) if dom == 0 else statistics.mean(mg),
+                "other_kernels": {KERNEL_NAMES[w]: {"ms_per_launch": prof[w][0], "algorithmic_bytes": prof[w][1],
                                                     "GB/s": prof[w][1] / (prof[w][0] * 1e-3) / 1e9}
                                   for w in prof},
-                "ms_per_solve": {KERNEL_NAMES[w]: per_solve[w] for w in per_solve} |
-                                {KERNEL_NAMES[3]: prof[3][0] * statistics.mean(mg),
-                                 KERNEL_NAMES[5]: prof[5][0] * statistics.mean(picard)}}
+                "ms_per_solve": {KERNEL_NAMES[w]: per_solve[w] for w in per_solve}}
 
     # end to end through the public API with pinned host buffers
     def pinned(a):
@@ -330,7 +344,7 @@ def run_b200(args):
         h, t_ = pinned(ctx.empty(n))
         host_out[n] = h
         keep.append(t_)
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = args.steps
 
     def e2e_step():
         ctx.upload(host_in)
@@ -362,7 +376,7 @@ def run_b200(args):
                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ice cap)",
                "config": config_json(g, {"parallelism": f"replicas x{world} (a single solve does not shard)",
-                                         "precision": args.precision,
+                                         "precision": args.precision, **nonlinear_json(cfg),
                                          "picard_iterations": picard, "mg_cycles": mg,
                                          "relres": [r["relres"] for r in reps]}),
                "roofline": roofline, "clocks": clk,
@@ -547,14 +561,15 @@ def run_learned(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     build.build()
 
-    def case(seed, precision):
+    def case(seed, precision, anderson=0):
         g, cfg, f = synth.ice_cap(seed=seed)
         cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
-                   lin_rtol=1e-10, precision=precision)
+                   lin_rtol=1e-10, precision=precision, picard_anderson_m=anderson,
+                   lin_adaptive_eta=args.eta if args.eta is not None else (0.1 if anderson else 0.5))
         return diva.Grid(**g), cfg, f
 
-    def prepared(seed, precision):
-        grid, cfg, f = case(seed, precision)
+    def prepared(seed, precision, anderson=0):
+        grid, cfg, f = case(seed, precision, anderson)
         ctx = diva.Context(grid, cfg)
         ctx.upload(f)
         ctx.update_general_ice_model_data()
@@ -579,8 +594,8 @@ def run_learned(args):
     loss = net.train(args.epochs, lr=1e-3, seed=1)
     t_train = time.perf_counter() - t0
 
-    def timed(seed, use_net):
-        ctx = prepared(seed, args.precision if use_net else "fp64")
+    def timed(seed, use_net, precision="fp64", anderson=0):
+        ctx = prepared(seed, precision, anderson)
         torch.cuda.synchronize()
         t = time.perf_counter()
         if use_net:
@@ -591,27 +606,37 @@ def run_learned(args):
         ctx.close()
         return dt, rep
 
+    arms = {"plain": (False, "fp64", 0), "learned": (True, args.precision, args.anderson),
+            "accelerated_cold": (False, args.precision, args.anderson)}
     for k in range(args.warmup):
-        timed(20000 + k, False)
-        timed(20000 + k, True)
+        for a in arms.values():
+            timed(20000 + k, *a)
     clocks = ClockSampler(0)
     clocks.start()
-    cold = [timed(10000 + k, False) for k in range(args.steps)]
-    warm = [timed(10000 + k, True) for k in range(args.steps)]
+    res = {name: [timed(10000 + k, *a) for k in range(args.steps)] for name, a in arms.items()}
     clk = clocks.stop()
+    cold, warm = res["plain"], res["learned"]
     t_cold, t_warm = sum(d for d, _ in cold), sum(d for d, _ in warm)
+    t_acc = sum(d for d, _ in res["accelerated_cold"])
+    parts = ["learned warm start"] + (["FP32 smoother"] if args.precision == "mixed" else []) + \
+            ([f"Anderson({args.anderson})"] if args.anderson else [])
     print(json.dumps({
-        "metric": "DIVA solves/s at 321x561x15 to rel-res 1e-6: learned warm start" +
-                  (" + FP32 smoother" if args.precision == "mixed" else "") + " vs plain FP64 GPU",
+        "metric": "DIVA solves/s at 321x561x15 to rel-res 1e-6: " + " + ".join(parts) + " vs plain FP64 GPU",
         "value": args.steps / t_warm, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * t_warm / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
         "data": "synthetic (seeded ice caps; training seeds 0.., held-out seeds 10000..)",
         "config": {"workload": "held-out ice caps 1600x2800 km @5 km, network warm start + 10 completion sweeps",
                    "plain_fp64_solves_per_s": args.steps / t_cold,
+                   "ratio_vs_plain_fp64": t_cold / t_warm,
+                   "same_method_cold_solves_per_s": args.steps / t_acc,
                    "iterations_cold": [r["picard_iterations"] for _, r in cold],
                    "iterations_learned": [r["picard_iterations"] for _, r in warm],
+                   "iterations_same_method_cold": [r["picard_iterations"] for _, r in res["accelerated_cold"]],
+                   "mg_cycles_cold": [r["mg_cycles"] for _, r in cold],
+                   "mg_cycles_learned": [r["mg_cycles"] for _, r in warm],
                    "status_learned": [r["status"] for _, r in warm],
+                   "relres_learned": [r["relres"] for _, r in warm],
                    "training_samples": net.num_samples, "epochs": args.epochs, "final_loss": loss,
                    "data_generation_s": t_data, "training_s": t_train,
                    "timing": "device-synchronised wall clock around predict + solve (inputs resident)"},
@@ -639,6 +664,10 @@ def main():
                    help="member kinds drawn from: channel (129x17), icecap (321x561), sheet (1501x1501)")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                    help="mixed: FP32 finest-level smoother inside the FP64 Krylov solve (not the default line)")
+    p.add_argument("--anderson", type=int, default=0,
+                   help="Anderson mixing depth of the viscosity iteration (0: the reference's relaxation)")
+    p.add_argument("--eta", type=float, default=None,
+                   help="adaptive linear tolerance factor (default 0.5, or 0.1 with --anderson)")
     args = p.parse_args()
     if args.impl == "b200" and args.workload == "ensemble":
         return run_ensemble(args)

@@ -1,6 +1,5 @@
 """Tile shapes of the multigrid smoother on the GPU: any per-level choice of 16 / 32
-gives the bit-identical solve, and the autotuner sets a valid choice.  Marked
-``gpu_pending`` until it has run on a B200 (``-m gpu_pending``)."""
+gives the bit-identical solve, and the autotuner sets a valid choice."""
 import numpy as np
 import pytest
 import torch
@@ -8,7 +7,7 @@ import torch
 from imau_ice_b200 import autotune, diva
 import helpers
 
-pytestmark = [pytest.mark.gpu_pending,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU (B200)")]
 
 
