@@ -193,6 +193,61 @@ def cpu_baseline(threads=None):
                        f"iterations) plus SIA, {t:.1f} s on {threads} threads")}
 
 
+def run_cpu_variants(args):
+    """The CPU port's variants of the linear solve on the ice cap (321 x 561 x 15), each one
+    full cold solve_DIVA plus SIA on the host threads: (i) the reference's defaults (Picard
+    step-norm tolerance 1e-2, at most 50 viscosity iterations, PETSc KSP rtol 1e-2 / abstol
+    2.5, petsc_module.F90:49-69), (ii) the configuration's tolerances (step norm 1e-3, linear
+    1e-8), (iii) SOR as utilities_module.f90:644-718 (omega 1.3, max |res/diag| <= 2.5,
+    sweep cap 10000; one thread, it is sequential) at the configuration's step-norm tolerance,
+    and (iv) the bench's rel-res 1e-6 stop with the adaptive tolerance (the cpu_baseline leg).
+    Reported only: one JSON line with each variant's time, iterations and final rel-res."""
+    load_package()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_backend as ob
+    from imau_ice_b200 import diva
+    threads = min(host_threads(), 64)
+    orc = ob.oracle_backend()
+    g, base, fields = workload()
+    grid = diva.Grid(**g)
+    ref_stop = dict(base, picard_stop="resid_UV", lin_adaptive=0)
+    variants = {
+        "reference_defaults_gmres": (dict(ref_stop, DIVA_visc_it_norm_dUV_tol=1e-2, DIVA_visc_it_nit=50),
+                                     (ob.LIN_GMRES_WARM, 1e-2, 2.5), threads),
+        "config_tolerances_gmres": (dict(ref_stop, DIVA_visc_it_norm_dUV_tol=1e-3, DIVA_visc_it_nit=200,
+                                         lin_rtol=1e-8), (ob.LIN_GMRES_WARM, 1e-8, 0.0), threads),
+        "config_tolerances_sor": (dict(ref_stop, DIVA_visc_it_norm_dUV_tol=1e-3, DIVA_visc_it_nit=200),
+                                  (ob.LIN_SOR, 0.0, 0.0), 1),
+        "relres_1e-6_adaptive_gmres": (base, (ob.LIN_GMRES_WARM, 1e-10, 0.0), threads),
+    }
+    out = {}
+    for name, (cfg, solver, thr) in variants.items():
+        ctx = diva.Context(grid, cfg, orc)
+        if solver[0] == ob.LIN_SOR:
+            ob.set_linear_solver(ctx, ob.LIN_SOR, sor_nit=10000, sor_tol=2.5, sor_omega=1.3)
+        else:
+            ob.set_linear_solver(ctx, solver[0], rtol=solver[1], abstol=solver[2])
+        ob.set_threads(ctx, thr)
+        ctx.upload(fields)
+        ctx.update_general_ice_model_data()
+        ctx.calc_pressure_melting_point()
+        ctx.calc_ice_rheology()
+        ctx.update_general_ice_model_data()
+        t0 = time.perf_counter()
+        rep = ctx.solve_DIVA()
+        ctx.calc_sia_3d_velocities()
+        t = time.perf_counter() - t0
+        rr = ctx.nonlinear_residual()
+        ctx.close()
+        out[name] = {"seconds": round(t, 3), "solves_per_s": 1.0 / t, "threads": thr,
+                     "viscosity_iterations": rep["picard_iterations"], "linear_iterations": rep["linear_iterations"],
+                     "status": rep["status"], "final_relres": rr}
+        print(name, out[name], file=sys.stderr, flush=True)
+    print(json.dumps({"workload": "CPU port variants, synthetic ice cap 321x561x15, one cold solve_DIVA + SIA each",
+                      "host_threads": threads, "variants": out}))
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -600,7 +655,10 @@ def run_learned(args):
         t = time.perf_counter()
         if use_net:
             net.predict(ctx, complete_sweeps=10)
-        rep = ctx.solve_DIVA()
+        try:
+            rep = ctx.solve_DIVA()
+        except diva.DivaError as e:     # reported in the line, not fatal to the run
+            rep = {"status": e.status, "picard_iterations": -1, "mg_cycles": -1, "relres": -1.0, "error": str(e)}
         torch.cuda.synchronize()
         dt = time.perf_counter() - t
         ctx.close()
@@ -636,6 +694,7 @@ def run_learned(args):
                    "mg_cycles_cold": [r["mg_cycles"] for _, r in cold],
                    "mg_cycles_learned": [r["mg_cycles"] for _, r in warm],
                    "status_learned": [r["status"] for _, r in warm],
+                   "status_same_method_cold": [r["status"] for _, r in res["accelerated_cold"]],
                    "relres_learned": [r["relres"] for _, r in warm],
                    "training_samples": net.num_samples, "epochs": args.epochs, "final_loss": loss,
                    "data_generation_s": t_data, "training_s": t_train,
@@ -654,7 +713,8 @@ def main():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true",
                    help="timed solves only (no roofline, e2e or CPU legs): the command profiled with ncu")
-    p.add_argument("--workload", choices=["icecap", "ensemble", "timestep", "learned"], default="icecap",
+    p.add_argument("--workload", choices=["icecap", "ensemble", "timestep", "learned", "cpu-variants"],
+                   default="icecap",
                    help="icecap: the headline solve (default); ensemble: --members perturbed members; "
                         "timestep: predictor/corrector steps with thickness and heat equation; "
                         "learned: --members training caps, then held-out solves cold vs warm-started")
@@ -675,6 +735,8 @@ def main():
         return run_timestep(args)
     if args.impl == "b200" and args.workload == "learned":
         return run_learned(args)
+    if args.workload == "cpu-variants":
+        return run_cpu_variants(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

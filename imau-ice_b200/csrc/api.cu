@@ -185,6 +185,7 @@ size_t carve(Ctx* c, Carver& cv) {
   c->staging = (double*)cv.take(sizeof(double) * d.nz * d.plane);
   c->col_eps = (double*)cv.take(sizeof(double) * d.plane);
   c->col_flags = (int*)cv.take(sizeof(int) * d.plane);
+  for (int q = 0; q < 2; ++q) c->taub_seen[q] = (double*)cv.take(sizeof(double) * d.plane);
   for (int k = 0; k < 6; ++k) c->f32[k] = (float*)cv.take(sizeof(float) * d.plane);
   c->rtu = (int8_t*)cv.take(d.plane);
   c->rtv = (int8_t*)cv.take(d.plane);
@@ -357,8 +358,8 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
   }
   for (;;) {
     ++it;
-    if ((st = launch_diva_coefficients(c, u, v, diva))) return st;
-    if ((st = solver_setup(c))) return st;
+    if ((st = launch_diva_coefficients(c, u, v, diva, K1_LOOP))) return st;
+    if ((st = solver_setup(c, coarse_inverse_due(it) ? 0 : 2))) return st;
     if (relmode) {
       if ((st = solver_relres(c, u, v, &relres))) return st;
       eta = eta_after(eta, relres, relres_prev, C.picard_relres_tol);   // as the graph's k_ctl_relres does
@@ -862,12 +863,12 @@ int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, 
   DIVA_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   for (int r = 0; r < reps && !st; ++r) {
     switch (which) {
-      case 0: st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true); break;
+      case 0: st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true, K1_LOOP); break;
       case 1: st = solver_smooth_fine(c, 1); break;
       case 2: st = solver_matvec_fine(c, 1); break;
       case 3: st = solver_vcycle_fine(c, 1); break;
       case 4: st = solver_subcycle(c, 1); break;
-      case 5: st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true, true); break;
+      case 5: st = launch_diva_coefficients(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true, K1_COLUMNS_ONLY); break;
     }
   }
   if (st) return st;
@@ -884,10 +885,10 @@ int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, 
   //  3: one V-cycle: per level 4 sweeps, a residual and the transfers, weighted by its points
   //  4: the one-block coarse levels of a V-cycle (latency-bound; bytes as for 3 over those levels)
   const double per_col[3] = {(3 * nz + 15) * w, solver_smooth_fine_values(c) * w, 8 * w};
-  //  5: the layer-parallel viscosity step alone: previous viscosity and A-factor read, viscosity
-  //     and the two shear fields written (5 nz)
+  //  5: the column kernel of 0 alone (without the b-grid faces): A-factor and previous viscosity
+  //     read, viscosity written (3 nz), with the 2D fields it reads and writes (12)
   *bytes = which < 3 ? per_col[which] * nc
-                     : (which == 3 ? solver_vcycle_bytes(c) : (which == 5 ? 5 * nz * w * nc : 0.0));
+                     : (which == 3 ? solver_vcycle_bytes(c) : (which == 5 ? (3 * nz + 12) * w * nc : 0.0));
   return DIVA_OK;
 }
 

@@ -62,6 +62,7 @@ enum {
 };
 constexpr int kAAMax = 5;             // largest Anderson depth
 constexpr int kAAPartials = 2 * kAAMax;   // block partials of one mixing step
+constexpr double kAAGammaMax = 20.0;      // largest sum of |gamma_i| a mixing step accepts
 
 // One Anderson mixing step's coefficients from the inner products of the newest residual
 // difference dF_s with every history column (dots[0..m)) and of the residual f with them
@@ -70,7 +71,9 @@ constexpr int kAAPartials = 2 * kAAMax;   // block partials of one mixing step
 // more than 10 x the one the previous step saw drops the older columns.  gamma solves the
 // normal equations of the least-squares problem over the n most recent columns, scaled to
 // unit diagonal and regularised by 1e-10; when the Cholesky factorisation meets a pivot
-// below 1e-12 the oldest column is dropped and the solve repeated (down to none).
+// below 1e-12, or the coefficients sum to more than kAAGammaMax in magnitude (an
+// extrapolation far outside the history), the oldest column is dropped and the solve
+// repeated (down to none: the plain step).
 __host__ __device__ inline void aa_coefficients(double* sc, int m, const double* dots) {
   double* G = sc + SC_AA_G;
   double* rhs = sc + SC_AA_RHS;
@@ -137,9 +140,14 @@ __host__ __device__ inline void aa_coefficients(double* sc, int m, const double*
       for (int l = k + 1; l < nn; ++l) t -= A[l][k] * y[l];
       y[k] = t / A[k][k];
     }
-    for (int k = 0; k < nn; ++k) ok = ok && (y[k] == y[k]) && fabs(y[k]) < 1e300;
-    if (!ok) continue;
-    for (int k = 0; k < nn; ++k) gam[idx[k]] = y[k] / dk[k];
+    double gsum = 0.0;
+    for (int k = 0; k < nn; ++k) {
+      y[k] = y[k] / dk[k];
+      ok = ok && (y[k] == y[k]) && fabs(y[k]) < 1e300;
+      gsum += fabs(y[k]);
+    }
+    if (!ok || !(gsum <= kAAGammaMax)) continue;
+    for (int k = 0; k < nn; ++k) gam[idx[k]] = y[k];
     sc[SC_AA_N] = (double)nn;
     return;
   }
@@ -178,6 +186,7 @@ struct Ctx {
   double* staging = nullptr;          // upload/download staging (largest field)
   double* col_eps = nullptr;          // column coefficients: mean-flow strain rate per column
   int* col_flags = nullptr;           // column coefficients: shear faces with ice
+  double* taub_seen[2] = {};          // basal stress (cx, cy) the last K1 of the viscosity loop read
   float* f32[6] = {};                 // float copies of the finest level (F32_*, precision 'mixed')
   int8_t* rtu = nullptr;              // finest-level row types ('BC' ice margins)
   int8_t* rtv = nullptr;
@@ -248,7 +257,12 @@ int launch_sico_masks(Ctx* c);
 
 // picard.cu
 int launch_prepare_afac(Ctx* c);
-int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva, bool layer_only = false);
+// K1: the coefficients of one viscosity iteration from (u, v), the previous viscosity and
+// the basal stress.  K1_WRITE_SHEAR also writes du_dz_3D_cx / dv_dz_3D_cy; K1_LOOP (the
+// viscosity loop) keeps what it needs to write them after the loop instead
+// (launch_visc_b_output); K1_COLUMNS_ONLY launches the column kernel alone (timing).
+enum { K1_WRITE_SHEAR = 0, K1_LOOP = 1, K1_COLUMNS_ONLY = 2 };
+int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva, int what = K1_WRITE_SHEAR);
 int launch_picard_update(Ctx* c, double* u, double* v, const double* xu, const double* xv, bool diva);
 // Anderson mixing step before launch_picard_update (picard_anderson_m > 0): the map value
 // g = velocity-limited linear solution, its residual f = g - u, the new history columns
@@ -258,7 +272,7 @@ int launch_anderson_prepare(Ctx* c, const double* u, const double* v, const doub
 int anderson_reset(Ctx* c);   // empty history at the start of a solve (zeroed columns)
 int launch_commit_err(Ctx* c);
 int launch_basal_stress_velocities(Ctx* c);
-int launch_visc_b_output(Ctx* c);
+int launch_visc_b_output(Ctx* c);   // after the viscosity loop: visc_eff_3D_b and the shear strain rates
 int launch_3d_horizontal_velocities(Ctx* c);
 int launch_secondary_velocities(Ctx* c);
 int launch_sia(Ctx* c);
@@ -272,7 +286,16 @@ int launch_any_sheet(Ctx* c, int* result);
 // solver.cu
 int solver_init(Ctx* c);
 size_t solver_table_entries(const Ctx* c);   // uint16 entries of the sub-cycle row tables      // per-context solver choices (after the configuration is known)
-int solver_setup(Ctx* c);     // coefficients of all levels from N_a, N_b, beta_eff, taud
+// Coefficients of all levels from N_a, N_b, beta_eff, taud.  The inverse of the coarsest
+// level's matrix (the coarse step of the V-cycle preconditioner) is formed when inv_when is
+// 0; with 1 only in the viscosity iterations coarse_inverse_due() picks (the device
+// iteration counter of the graph-launched loop), with 2 not at all (an older inverse stays).
+// The operator itself, and so the converged answer, is always current.
+int solver_setup(Ctx* c, int inv_when = 0);
+// Viscosity iterations that refresh the coarse inverse: the first three, then every fourth.
+// Its one-block Gauss-Jordan elimination costs as much as a fifth of an iteration's V-cycle,
+// while the coarsest grid's coefficients change slowly once the iteration has settled.
+__host__ __device__ inline bool coarse_inverse_due(int it) { return it <= 3 || (it - 1) % 4 == 0; }
 int solver_solve(Ctx* c, const double* u0, const double* v0, double rtol, int maxit, int* iters, double* relres0);
 int solver_relres(Ctx* c, const double* u, const double* v, double* relres);
 int solver_fill_boundary(Ctx* c, double* u, double* v);

@@ -1,7 +1,7 @@
 // picard.cu -- the per-iteration physics of solve_DIVA / solve_SSA and the
 // velocity fields computed after the viscosity iteration.
 //
-//   K1 k_column_prep, k_layer_viscosity, k_column_integrals
+//   K1 k_column_coefficients (+ k_shear_rates once per solve)
 //                             calc_vertical_shear_strain_rates   ice_velocity_module.f90:664-721
 //                             calc_effective_viscosity (a-grid)   :722-818
 //                             calc_sliding_term_beta + laws       :900-959, basal_conditions_and_sliding_module.f90:908-1236
@@ -44,6 +44,9 @@ struct CoefArgs {
   // per-column scratch between the three launches
   double* col_eps;
   int* col_flags;
+  // the basal stress each column read (the fused kernel keeps a copy, so that the shear
+  // strain rates of the last viscosity iteration can be written after the loop)
+  double *taub_seen_cx, *taub_seen_cy;
 };
 
 // strain rates of the depth-averaged velocity on the a-grid,
@@ -114,18 +117,10 @@ __device__ __forceinline__ double sliding_beta(const CoefArgs& a, long long q, d
   return CUDART_NAN;
 }
 
-// K1 in three launches.  (a) k_column_prep, one thread per column: the strain rates
-// of the depth-averaged flow and which of the column's four shear faces have ice.
-// (b) k_layer_viscosity, one thread per (column, layer), a warp over 32 neighbouring
-// rows j of one grid column i and one layer: the shear of the column's own east and
-// north faces (written), the west face, and the south face as the north face of the
-// lane below (shuffle), then the viscosity of the layer.  (c) k_column_integrals, one
-// thread per column: the vertical integrals in layer order (as the sequential
-// quadrature does), N_a, the sliding law, F2 and beta_eff.  The split costs one more
-// read of the viscosity and buys a layer-parallel, dependency-free middle step.
+// Block shape of the layer-parallel k_shear_rates: a warp over 32 rows, 4 grid columns.
 constexpr int kColLanes = 32, kColRows = 4;
 
-// Per-column decisions of the layer step, packed by k_column_prep:
+// Per-column decisions of K1, packed by k_column_coefficients (and kept for k_shear_rates):
 //   bits 0-3   the E, W, N, S shear face carries ice (FACE_*)
 //   bits 4-11  per face, which side the staggered viscosity takes (calc_staggered_margin
 //              :1300-1319): 0 the mean of both, 1 the first (west/south) side, 2 the second
@@ -145,111 +140,101 @@ __device__ __forceinline__ double stag_mode(int mode, double v0, double v1) {
   return mode == 1 ? v0 : (mode == 2 ? v1 : 0.5 * (v0 + v1));
 }
 
-__global__ void __launch_bounds__(256) k_column_prep(CoefArgs a) {
+// K1 fused: one thread per a-grid column, a warp over 32 neighbouring rows j of one grid
+// column i, the zeta layers walked in order.  Per column: the strain rates of the
+// depth-averaged flow and which of the four shear faces carry ice, then per layer the
+// face shears -- the south face is the north face of the lane below (shuffle) -- and the
+// viscosity, accumulating the vertical integrals in layer order (as the sequential
+// quadrature does), then N_a, the sliding law, F2 and beta_eff.  Per column it reads the A-factor and the previous viscosity and writes
+// the new viscosity once: (3 nz + 15) x 8 bytes with the 2D fields.  The shear strain
+// rates du/dz, dv/dz (:664-721) are written only with WRITE_SHEAR; the loop instead keeps
+// the flags and the basal stress it read, from which k_shear_rates writes the last
+// iteration's shear after the loop.
+template <bool WRITE_SHEAR>
+__global__ void __launch_bounds__(kBX * kBY) k_column_coefficients(CoefArgs a) {
   const Dims d = a.d;
+  const int lane = threadIdx.x;
   const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
-  if (j >= d.ny || i >= d.nx) return;
-  const int nx = d.nx, ny = d.ny;
-  const long long q = d.at(j, i);
+  if (i >= d.nx) return;        // whole warps: i is uniform across a warp
+  const bool col = j < d.ny;    // lanes past the last row stay for the shuffle
+  const int nx = d.nx, ny = d.ny, ld = d.ld, nz = d.nz;
+  const int jc = col ? j : ny - 1;
+  const long long q = d.at(jc, i);
   const int* __restrict__ mask = a.mask_ice;
   const double* __restrict__ Hi = a.Hi;
+  const double H = Hi[q];
   const bool ice = mask[q] == 1;
-  const bool skip_visc = a.bc_margin && !ice;  // BC margins: no viscosity outside the ice (:759-764)
-  // strain rates of the depth-averaged flow (calc_effective_viscosity :751-754)
+  const bool skip_visc = a.bc_margin && !ice;   // BC margins: no viscosity outside the ice (:759-764)
   double eps_h = 0.0;
-  if (!skip_visc) {
-    const double du_dx = ddx_cx_to_a(d, a.u, j, i), dv_dy = ddy_cy_to_a(d, a.v, j, i);
-    const double du_dy = ddy_cx_to_a(d, a.u, j, i), dv_dx = ddx_cy_to_a(d, a.v, j, i);
+  if (!skip_visc) {   // calc_effective_viscosity :751-754
+    const double du_dx = ddx_cx_to_a(d, a.u, jc, i), dv_dy = ddy_cy_to_a(d, a.v, jc, i);
+    const double du_dy = ddy_cx_to_a(d, a.u, jc, i), dv_dx = ddx_cy_to_a(d, a.v, jc, i);
     eps_h = du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((du_dy + dv_dx) * (du_dy + dv_dx));
   }
-  const double H = Hi[q];
   int flags = skip_visc ? COL_SKIP : 0;
   auto face = [&](int bit, int f, long long p0, long long p1) {
-    // a face carries shear if either side has ice (calc_vertical_shear_strain_rates :685-695)
     if (a.diva && !(mask[p0] == 0 && mask[p1] == 0)) flags |= bit;
     flags |= margin_mode(Hi[p0], Hi[p1]) << (kModeShift + 2 * f);
   };
-  if (i < nx - 1) face(FACE_E, 0, q, d.at(j, i + 1));
-  if (i > 0) face(FACE_W, 1, d.at(j, i - 1), q);
-  if (j < ny - 1) face(FACE_N, 2, q, d.at(j + 1, i));
-  if (j > 0) face(FACE_S, 3, d.at(j - 1, i), q);
-  // a-grid staggering of the face values: first column/row the east/north face alone (2),
-  // last column/row the west/south face alone (1), else the margin rule
-  const int mx = i == 0 ? 2 : (i == nx - 1 ? 1 : margin_mode(Hi[d.at(j, i - 1)], H));
-  const int my = j == 0 ? 2 : (j == ny - 1 ? 1 : margin_mode(Hi[d.at(j - 1, i)], H));
+  if (i < nx - 1) face(FACE_E, 0, q, d.at(jc, i + 1));
+  if (i > 0) face(FACE_W, 1, d.at(jc, i - 1), q);
+  if (jc < ny - 1) face(FACE_N, 2, q, d.at(jc + 1, i));
+  if (jc > 0) face(FACE_S, 3, d.at(jc - 1, i), q);
+  const int mx = i == 0 ? 2 : (i == nx - 1 ? 1 : margin_mode(Hi[d.at(jc, i - 1)], H));
+  const int my = jc == 0 ? 2 : (jc == ny - 1 ? 1 : margin_mode(Hi[d.at(jc - 1, i)], H));
   flags |= (mx << kStagXShift) | (my << kStagYShift);
-  a.col_eps[q] = eps_h;
-  a.col_flags[q] = flags;
-}
-
-__global__ void __launch_bounds__(kColLanes * kColRows) k_layer_viscosity(CoefArgs a) {
-  const Dims d = a.d;
-  const int lane = threadIdx.x;
-  // the layer is the fastest grid index: blocks running together share their columns'
-  // 2D inputs in L1/L2 instead of streaming them once per layer
-  const int k = blockIdx.x, j = blockIdx.y * kColLanes + lane, i = blockIdx.z * kColRows + threadIdx.y;
-  if (i >= d.nx) return;       // whole warps: i is uniform across a warp
-  const bool col = j < d.ny;   // lanes past the last row stay for the shuffle
-  const int nx = d.nx, ny = d.ny, ld = d.ld;
-  const int q = i * ld + (col ? j : ny - 1);   // plane index (planes hold < 2^31 points)
-  const long long off = (long long)k * d.plane;
-  const double* __restrict__ vp = a.visc_prev + off;
-  const double zk = a.zt.z[k];
-  const int flags = a.col_flags[q];
   const bool has_e = col && i < nx - 1, has_w = col && i > 0, has_n = col && j < ny - 1, has_s = col && j > 0;
   auto mode = [&](int f) { return (flags >> (kModeShift + 2 * f)) & 3; };
-  double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0, dudz_w = 0.0;
+  double tbe = 0.0, tbw = 0.0, tbn = 0.0, tbs = 0.0;
   if (a.diva) {
-    const double vq = vp[q];
-    if (has_e) {
-      if (flags & FACE_E) dudz_e = (a.taub_cx[q] / stag_mode(mode(0), vq, vp[q + ld])) * zk;
-      a.dudz[off + q] = dudz_e;
-    }
-    if (has_n) {
-      if (flags & FACE_N) dvdz_n = (a.taub_cy[q] / stag_mode(mode(2), vq, vp[q + 1])) * zk;
-      a.dvdz[off + q] = dvdz_n;
-    }
-    if (has_w && (flags & FACE_W)) dudz_w = (a.taub_cx[q - ld] / stag_mode(mode(1), vp[q - ld], vq)) * zk;
-    dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
-    if (lane == 0 && has_s)
-      dvdz_s = (flags & FACE_S) ? (a.taub_cy[q - 1] / stag_mode(mode(3), vp[q - 1], vq)) * zk : 0.0;
+    if (has_e) tbe = a.taub_cx[q];
+    if (has_w) tbw = a.taub_cx[q - ld];
+    if (has_n) tbn = a.taub_cy[q];
+    if (has_s && lane == 0) tbs = a.taub_cy[q - 1];
   }
-  if (!col) return;
-  double eta = 0.0;
-  if (!(flags & COL_SKIP)) {
-    const int mx = (flags >> kStagXShift) & 3, my = (flags >> kStagYShift) & 3;
-    double du_dz_a, dv_dz_a;
-    if (a.diva) {
-      du_dz_a = stag_mode(mx, dudz_w, dudz_e);
-      dv_dz_a = stag_mode(my, dvdz_s, dvdz_n);
-    } else {
-      // solve_SSA calls calc_effective_viscosity without refreshing du/dz: use the stored fields
-      const double* dudz = a.dudz + off;
-      const double* dvdz = a.dvdz + off;
-      du_dz_a = stag_mode(mx, i > 0 ? dudz[q - ld] : 0.0, i < nx - 1 ? dudz[q] : 0.0);
-      dv_dz_a = stag_mode(my, j > 0 ? dvdz[q - 1] : 0.0, j < ny - 1 ? dvdz[q] : 0.0);
+  if (col) {
+    a.col_flags[q] = flags;
+    if (a.diva && !WRITE_SHEAR) {
+      if (has_e) a.taub_seen_cx[q] = tbe;
+      if (has_n) a.taub_seen_cy[q] = tbn;
     }
-    const double eps_sq = a.col_eps[q] + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
-    const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
-    eta = max_ref(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
   }
-  a.visc[off + q] = eta;
-}
-
-__global__ void __launch_bounds__(256) k_column_integrals(CoefArgs a) {
-  const Dims d = a.d;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
-  if (j >= d.ny || i >= d.nx) return;
-  const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const long long q = d.at(j, i);
-  const double H = a.Hi[q];
-  const bool ice = a.mask_ice[q] == 1;
-  const bool skip_visc = a.bc_margin && !ice;
-  const double* __restrict__ visc = a.visc;
+  const double* __restrict__ vp = a.visc_prev;
   double vint = 0.0, fint = 0.0, vprev = 0.0, fprev = 0.0;
   for (int k = 0; k < nz; ++k) {
-    const double eta = visc[(long long)k * d.plane + q];
+    const long long off = (long long)k * d.plane;
     const double zk = a.zt.z[k];
+    double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0, dudz_w = 0.0;
+    if (a.diva) {
+      const double vq = vp[off + q];
+      if (has_e && (flags & FACE_E)) dudz_e = (tbe / stag_mode(mode(0), vq, vp[off + q + ld])) * zk;
+      if (has_n && (flags & FACE_N)) dvdz_n = (tbn / stag_mode(mode(2), vq, vp[off + q + 1])) * zk;
+      if (has_w && (flags & FACE_W)) dudz_w = (tbw / stag_mode(mode(1), vp[off + q - ld], vq)) * zk;
+      dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
+      if (lane == 0 && has_s) dvdz_s = (flags & FACE_S) ? (tbs / stag_mode(mode(3), vp[off + q - 1], vq)) * zk : 0.0;
+      if (WRITE_SHEAR) {
+        if (has_e) a.dudz[off + q] = dudz_e;
+        if (has_n) a.dvdz[off + q] = dvdz_n;
+      }
+    }
+    double eta = 0.0;
+    if (!skip_visc) {
+      double du_dz_a, dv_dz_a;
+      if (a.diva) {
+        du_dz_a = stag_mode(mx, dudz_w, dudz_e);
+        dv_dz_a = stag_mode(my, dvdz_s, dvdz_n);
+      } else {
+        // solve_SSA calls calc_effective_viscosity without refreshing du/dz: the stored fields
+        const double* dudz = a.dudz + off;
+        const double* dvdz = a.dvdz + off;
+        du_dz_a = stag_mode(mx, i > 0 ? dudz[q - ld] : 0.0, i < nx - 1 ? dudz[q] : 0.0);
+        dv_dz_a = stag_mode(my, jc > 0 ? dvdz[q - 1] : 0.0, jc < ny - 1 ? dvdz[q] : 0.0);
+      }
+      const double eps_sq = eps_h + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
+      const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
+      eta = max_ref(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
+    }
+    if (col) a.visc[off + q] = eta;
     if (k > 0) vint = vint + 0.5 * (eta + vprev) * (zk - a.zt.z[k - 1]);
     vprev = eta;
     if (a.diva) {
@@ -258,6 +243,7 @@ __global__ void __launch_bounds__(256) k_column_integrals(CoefArgs a) {
       fprev = fk;
     }
   }
+  if (!col) return;
   if (!skip_visc) {
     a.visc_int[q] = vint;
     a.Na[q] = a.bc_margin ? vint * H : vint * max_ref(0.1, H);
@@ -291,6 +277,33 @@ __global__ void __launch_bounds__(256) k_column_integrals(CoefArgs a) {
     a.beta_eff[q] = be;
   } else {
     a.beta_eff[q] = beta;   // solve_SSA :193
+  }
+}
+
+// The shear strain rates du/dz, dv/dz (calc_vertical_shear_strain_rates :664-721) of the last
+// viscosity iteration, from the flags and basal stress its fused K1 kept and the viscosity
+// it read: the values a K1 that writes them would have left.  Layer-parallel.
+__global__ void __launch_bounds__(kColLanes * kColRows) k_shear_rates(CoefArgs a) {
+  const Dims d = a.d;
+  const int lane = threadIdx.x;
+  const int k = blockIdx.x, j = blockIdx.y * kColLanes + lane, i = blockIdx.z * kColRows + threadIdx.y;
+  if (i >= d.nx) return;
+  const bool col = j < d.ny;
+  const int nx = d.nx, ny = d.ny, ld = d.ld;
+  const long long q = d.at(col ? j : ny - 1, i);
+  const long long off = (long long)k * d.plane;
+  const double* __restrict__ vp = a.visc_prev + off;
+  const double zk = a.zt.z[k];
+  const int flags = a.col_flags[q];
+  auto mode = [&](int f) { return (flags >> (kModeShift + 2 * f)) & 3; };
+  if (!col) return;
+  if (i < nx - 1) {
+    const double s = (flags & FACE_E) ? (a.taub_seen_cx[q] / stag_mode(mode(0), vp[q], vp[q + ld])) * zk : 0.0;
+    a.dudz[off + q] = s;
+  }
+  if (j < ny - 1) {
+    const double s = (flags & FACE_N) ? (a.taub_seen_cy[q] / stag_mode(mode(2), vp[q], vp[q + 1])) * zk : 0.0;
+    a.dvdz[off + q] = s;
   }
 }
 
@@ -443,12 +456,19 @@ __global__ void __launch_bounds__(256) k_aa_prepare(AAArgs a) {
       const double f = g - x;
       if (have) {
         const double df = f - fp[q];
-        dF[s][q] = df;
-        dG[s][q] = g - gp[q];
-        for (int k = 0; k < a.m; ++k) {
-          const double c = (k == s) ? df : dF[k][q];
-          acc[k] += c * df;
-          acc[kAAMax + k] += c * f;
+#pragma unroll
+        for (int k = 0; k < kAAMax; ++k)
+          if (k == s) {
+            dF[k][q] = df;
+            dG[k][q] = g - gp[q];
+          }
+#pragma unroll
+        for (int k = 0; k < kAAMax; ++k) {
+          if (k < a.m) {
+            const double c = (k == s) ? df : dF[k][q];
+            acc[k] += c * df;
+            acc[kAAMax + k] += c * f;
+          }
         }
       }
       fp[q] = f;
@@ -928,11 +948,8 @@ int launch_prepare_afac(Ctx* c) {
   return DIVA_OK;
 }
 
-int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva, bool layer_only) {
+static void fill_coef_args(Ctx* c, CoefArgs& a, const double* u, const double* v, bool diva) {
   const diva_config_t& C = c->c;
-  // Picard double buffering of visc_eff_3D_a: read the previous, write the new
-  std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
-  CoefArgs a{};
   a.d = c->d;
   a.zt = c->zt;
   a.diva = diva;
@@ -974,27 +991,31 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
   a.visc = c->D(DIVA_F_VISC_EFF_3D_A); a.visc_int = c->D(DIVA_F_VISC_EFF_INT_A); a.Na = c->D(DIVA_F_N_A);
   a.beta = c->D(DIVA_F_BETA_A); a.F2 = c->D(DIVA_F_F2_A); a.beta_eff = c->D(DIVA_F_BETA_EFF_A);
   a.tauc = c->D(DIVA_F_TAUC_A);
+  a.col_eps = c->col_eps;
+  a.col_flags = c->col_flags;
+  a.taub_seen_cx = c->taub_seen[0];
+  a.taub_seen_cy = c->taub_seen[1];
+}
+
+int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva, int what) {
+  const diva_config_t& C = c->c;
+  // Picard double buffering of visc_eff_3D_a: read the previous, write the new
+  std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
+  CoefArgs a{};
+  fill_coef_args(c, a, u, v, diva);
   if (C.choice_ice_margin == DIVA_MARGIN_BC) {
     // BC margins keep visc_eff_int_a / N_a of ice-free points from before: the
     // previous buffer's content is not carried over by the swap, so copy it.
     DIVA_CUDA(c, cudaMemcpyAsync(c->D(DIVA_F_VISC_EFF_3D_A), c->visc_prev, sizeof(double) * c->d.plane * c->d.nz,
                                  cudaMemcpyDeviceToDevice, c->stream));
   }
-  a.col_eps = c->col_eps;
-  a.col_flags = c->col_flags;
-  if (!layer_only) {
-    k_column_prep<<<G2>>>(a); c->launches++;
-  }
-  {
-    const dim3 block(kColLanes, kColRows);
-    const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
-    k_layer_viscosity<<<grid, block, 0, c->stream>>>(a); c->launches++;
-  }
-  if (layer_only) {   // timing of the layer step alone (diva_profile_kernel), per-column data of the last call
-    DIVA_LAUNCHED(c, "k_layer_viscosity");
+  if (what == K1_WRITE_SHEAR) k_column_coefficients<true><<<G2>>>(a);
+  else k_column_coefficients<false><<<G2>>>(a);
+  c->launches++;
+  if (what == K1_COLUMNS_ONLY) {   // timing of the column kernel alone (diva_profile_kernel)
+    DIVA_LAUNCHED(c, "k_column_coefficients");
     return DIVA_OK;
   }
-  k_column_integrals<<<G2>>>(a); c->launches++;
   DIVA_LAUNCHED(c, "column coefficients");
   FaceArgs fa{};
   fa.d = c->d;
@@ -1146,7 +1167,20 @@ int launch_err_commit_pred(Ctx* c) {
   return DIVA_OK;
 }
 
+int launch_shear_rates(Ctx* c) {
+  CoefArgs a{};
+  fill_coef_args(c, a, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true);
+  const dim3 block(kColLanes, kColRows);
+  const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
+  k_shear_rates<<<grid, block, 0, c->stream>>>(a); c->launches++;
+  DIVA_LAUNCHED(c, "k_shear_rates");
+  return DIVA_OK;
+}
+
 int launch_visc_b_output(Ctx* c) {
+  // the shear strain rates the last viscosity iteration's K1 saw (the loop does not write them)
+  int st;
+  if ((st = launch_shear_rates(c))) return st;
   k_visc_b<<<G2>>>(c->d, c->c.choice_ice_margin == DIVA_MARGIN_BC, c->D(DIVA_F_VISC_EFF_3D_A),
                    c->I(DIVA_F_MASK_ICE_A), c->D(DIVA_F_VISC_EFF_3D_B)); c->launches++;
   DIVA_LAUNCHED(c, "k_visc_b");

@@ -1228,6 +1228,10 @@ __global__ void k_level_setup(Op o, int coarsen, Dims dc, int fx, int fy, double
 struct SmallSetup {
   int first, last;           // the levels handled
   int direct;                // assemble and invert the coarsest level's matrix
+  // when: 0 every launch; 1 in the viscosity iterations coarse_inverse_due() picks, read from
+  // the device iteration counter (graph-launched loop); 2 not in this launch
+  int inv_when;
+  const double* sc;
   CoarseMap map;
   const uint16_t* tab;       // the coarsest level's row table
   double* Ainv;
@@ -1254,7 +1258,8 @@ __global__ void __launch_bounds__(kInvThreads) k_small_setup(SmallSetup a) {
     }
     __syncthreads();
   }
-  if (a.direct) coarse_setup_block(a.o[a.last], a.map, a.tab, a.Ainv, a.singular);
+  const bool inv = a.inv_when == 0 || (a.inv_when == 1 && coarse_inverse_due((int)a.sc[SC_PIC_IT]));
+  if (a.direct && inv) coarse_setup_block(a.o[a.last], a.map, a.tab, a.Ainv, a.singular);
 }
 
 // ---- Krylov kernels (fine level) --------------------------------------------------
@@ -1647,7 +1652,7 @@ static CoarseMap coarse_map(const Ctx* c) {
 
 static int sub_first_level(const Ctx* c);
 
-int solver_setup(Ctx* c) {
+int solver_setup(Ctx* c, int inv_when) {
   const diva_config_t& C = c->c;
   // the 'BC' front rows live on the finest level only; a grid too small to coarsen
   // would hand that level to the coarse direct solve, whose matrix has no front rows
@@ -1697,6 +1702,8 @@ int solver_setup(Ctx* c) {
   a.tab = c->sub_tab + c->sub_tab_off[c->nlev - 1];
   a.Ainv = c->coarse_inv;
   a.singular = c->coarse_singular;
+  a.inv_when = inv_when;
+  a.sc = c->scal;
   for (int l = a.first < a.last ? a.first : a.last; l <= a.last; ++l) {   // (first > last on a one-level grid)
     a.o[l] = make_op(c, l);
     a.idu[l] = c->lv[l].idu;
@@ -2301,8 +2308,8 @@ int capture_iteration(Ctx* c, CaptureCtx& cc, cudaStream_t top, bool diva, Picar
   // ---- pre
   cc.mark();
   k_ctl_begin<<<1, 1, 0, c->stream>>>(c->scal); c->launches++;
-  if ((st = launch_diva_coefficients(c, u, v, diva))) return st;   // swaps the viscosity buffers
-  if ((st = solver_setup(c))) return st;
+  if ((st = launch_diva_coefficients(c, u, v, diva, K1_LOOP))) return st;   // swaps the viscosity buffers
+  if ((st = solver_setup(c, 1))) return st;
   if (relmode) {
     k_relres<<<g2, block2d(), 0, c->stream>>>(o, u, v, U_(KV_B), V_(KV_B), c->partials, g2.x); c->launches++;
     k_ctl_relres<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, h_solve, C.picard_relres_tol); c->launches++;

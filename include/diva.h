@@ -178,7 +178,9 @@ typedef struct {
    * Anderson mixing of depth m on the unrelaxed Picard map g(u) (the velocity-limited
    * linear solution): u <- g - sum_i gamma_i (g_i+1 - g_i), with gamma minimising
    * || f - sum_i gamma_i (f_i+1 - f_i) ||_2 over the last m residuals f = g(u) - u
-   * (velocities on the cx and cy points).  Needs picard_stop = DIVA_STOP_RELRES: the
+   * (velocities on the cx and cy points); safeguards: columns are dropped while the
+ * coefficients' magnitudes sum to more than 20, and all but the newest when the
+ * nonlinear residual grows tenfold.  Needs picard_stop = DIVA_STOP_RELRES: the
    * stop test is the nonlinear residual, so the converged state solves the same equations
    * as with the relaxed update; only the path there, and its length, change. */
   int32_t picard_anderson_m;
@@ -361,12 +363,13 @@ int  diva_state_save(diva_ctx_t* ctx);
 int  diva_state_restore(diva_ctx_t* ctx);
 
 /* Time one hot kernel of the current state in isolation: `which` selects
- *   0  the fused column-coefficient kernel (viscosity, F2, beta, beta_eff) + face kernel
+ *   0  the column coefficients of one viscosity iteration: the fused column kernel (viscosity,
+ *      F2, beta, beta_eff) + the b-grid face kernel
  *   1  one full Gauss-Seidel sweep (4 colours) of the fine-level operator
  *   2  one fine-level operator application (matrix-free A x with dot products)
  *   3  one multigrid V-cycle (the preconditioner of one Krylov half-step)
  *   4  the one-block coarse-level part of a V-cycle alone
- *   5  the layer-parallel viscosity step of 0 alone (k_layer_viscosity)
+ *   5  the fused column kernel of 0 alone (k_column_coefficients)
  * `reps` launches are bracketed by CUDA events on the context's stream;
  * returns the mean device time per launch and the algorithmic bytes one launch
  * must move.  Needs a context that has completed a solve; kind 0 leaves the

@@ -2072,9 +2072,10 @@ static void fill_err(orc_ctx* c) {
  * differences of consecutive residuals / map values; the next iterate is
  * g - sum gamma_i dG_i with gamma minimising |f - sum gamma_i dF_i|_2 over the n <= m most
  * recent columns (normal equations scaled to unit diagonal, + 1e-10; on a Cholesky pivot
- * below 1e-12 the oldest column is dropped).  A nonlinear residual 10 x the previous
- * step's drops the older columns. */
+ * below 1e-12, or when the coefficients' magnitudes sum to more than 20, the oldest column
+ * is dropped).  A nonlinear residual 10 x the previous step's drops the older columns. */
 #define AA_MAX 5
+#define AA_GAMMA_MAX 20.0   /* largest sum of |gamma_i| a mixing step accepts, else drop columns */
 
 static void aa_reset(orc_ctx* c) {
   const size_t n = (size_t)c->ny * (c->nx - 1) + (size_t)(c->ny - 1) * c->nx;
@@ -2145,9 +2146,14 @@ static void aa_coefficients(orc_ctx* c, int m, const double* dots, double relres
       for (int l = k + 1; l < nn; ++l) t -= A[l][k] * y[l];
       y[k] = t / A[k][k];
     }
-    for (int k = 0; k < nn; ++k) ok = ok && isfinite(y[k]);
-    if (!ok) continue;
-    for (int k = 0; k < nn; ++k) c->aa_gamma[idx[k]] = y[k] / dk[k];
+    double gsum = 0.0;
+    for (int k = 0; k < nn; ++k) {
+      y[k] = y[k] / dk[k];
+      ok = ok && isfinite(y[k]);
+      gsum += fabs(y[k]);
+    }
+    if (!ok || !(gsum <= AA_GAMMA_MAX)) continue;
+    for (int k = 0; k < nn; ++k) c->aa_gamma[idx[k]] = y[k];
     c->aa_n = nn;
     return;
   }
