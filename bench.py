@@ -54,7 +54,7 @@ OUTPUT_FIELDS = ["u_vav_cx", "v_vav_cy", "u_3D_cx", "v_3D_cy", "w_3D_a", "u_3D_S
 KERNEL_NAMES = {0: "K1 column coefficients (all launches of one viscosity iteration)",
                 1: "k_smooth_down+k_smooth_up (fine level)", 2: "k_matvec",
                 3: "V-cycle (all levels)", 4: "k_subcycle (coarse levels, one block)",
-                5: "k_layer_viscosity"}
+                5: "K1 column launches (without the b-grid faces)"}
 # committed ncu summaries holding the DRAM bytes of one launch of each part
 TRAFFIC_KEYS = {0: "k1_icecap321x561", 3: "vcycle_icecap321x561"}
 

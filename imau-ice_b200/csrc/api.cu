@@ -885,8 +885,8 @@ int diva_profile_kernel(diva_ctx_t* h, int32_t which, int32_t reps, double* ms, 
   //  3: one V-cycle: per level 4 sweeps, a residual and the transfers, weighted by its points
   //  4: the one-block coarse levels of a V-cycle (latency-bound; bytes as for 3 over those levels)
   const double per_col[3] = {(3 * nz + 15) * w, solver_smooth_fine_values(c) * w, 8 * w};
-  //  5: the column kernel of 0 alone (without the b-grid faces): A-factor and previous viscosity
-  //     read, viscosity written (3 nz), with the 2D fields it reads and writes (12)
+  //  5: the column launches of 0 without the b-grid faces: A-factor and previous viscosity
+  //     read, viscosity written (3 nz), with the 2D fields they read and write (12)
   *bytes = which < 3 ? per_col[which] * nc
                      : (which == 3 ? solver_vcycle_bytes(c) : (which == 5 ? (3 * nz + 12) * w * nc : 0.0));
   return DIVA_OK;

@@ -1,7 +1,7 @@
 // picard.cu -- the per-iteration physics of solve_DIVA / solve_SSA and the
 // velocity fields computed after the viscosity iteration.
 //
-//   K1 k_column_coefficients (+ k_shear_rates once per solve)
+//   K1 k_column_prep, k_layer_viscosity, k_column_integrals (+ k_shear_rates once per solve)
 //                             calc_vertical_shear_strain_rates   ice_velocity_module.f90:664-721
 //                             calc_effective_viscosity (a-grid)   :722-818
 //                             calc_sliding_term_beta + laws       :900-959, basal_conditions_and_sliding_module.f90:908-1236
@@ -44,8 +44,9 @@ struct CoefArgs {
   // per-column scratch between the three launches
   double* col_eps;
   int* col_flags;
-  // the basal stress each column read (the fused kernel keeps a copy, so that the shear
-  // strain rates of the last viscosity iteration can be written after the loop)
+  // the basal stress each column's shear read, kept (keep_seen) so that the shear strain
+  // rates of the viscosity loop's last iteration can be written after the loop
+  int keep_seen;
   double *taub_seen_cx, *taub_seen_cy;
 };
 
@@ -117,10 +118,10 @@ __device__ __forceinline__ double sliding_beta(const CoefArgs& a, long long q, d
   return CUDART_NAN;
 }
 
-// Block shape of the layer-parallel k_shear_rates: a warp over 32 rows, 4 grid columns.
+// Block shape of the layer-parallel kernels: a warp over 32 rows, 4 grid columns.
 constexpr int kColLanes = 32, kColRows = 4;
 
-// Per-column decisions of K1, packed by k_column_coefficients (and kept for k_shear_rates):
+// Per-column decisions of the layer step, packed by k_column_prep (and kept for k_shear_rates):
 //   bits 0-3   the E, W, N, S shear face carries ice (FACE_*)
 //   bits 4-11  per face, which side the staggered viscosity takes (calc_staggered_margin
 //              :1300-1319): 0 the mean of both, 1 the first (west/south) side, 2 the second
@@ -140,101 +141,134 @@ __device__ __forceinline__ double stag_mode(int mode, double v0, double v1) {
   return mode == 1 ? v0 : (mode == 2 ? v1 : 0.5 * (v0 + v1));
 }
 
-// K1 fused: one thread per a-grid column, a warp over 32 neighbouring rows j of one grid
-// column i, the zeta layers walked in order.  Per column: the strain rates of the
-// depth-averaged flow and which of the four shear faces carry ice, then per layer the
-// face shears -- the south face is the north face of the lane below (shuffle) -- and the
-// viscosity, accumulating the vertical integrals in layer order (as the sequential
-// quadrature does), then N_a, the sliding law, F2 and beta_eff.  Per column it reads the A-factor and the previous viscosity and writes
-// the new viscosity once: (3 nz + 15) x 8 bytes with the 2D fields.  The shear strain
-// rates du/dz, dv/dz (:664-721) are written only with WRITE_SHEAR; the loop instead keeps
-// the flags and the basal stress it read, from which k_shear_rates writes the last
-// iteration's shear after the loop.
-template <bool WRITE_SHEAR>
-__global__ void __launch_bounds__(kBX * kBY) k_column_coefficients(CoefArgs a) {
+// K1 in three launches.  (a) k_column_prep, one thread per column: the strain rates
+// of the depth-averaged flow and which of the column's four shear faces have ice.
+// (b) k_layer_viscosity, one thread per (column, layer), a warp over 32 neighbouring
+// rows j of one grid column i and one layer: the shear of the column's own east and
+// north faces, the west face, and the south face as the north face of the lane below
+// (shuffle), then the viscosity of the layer.  (c) k_column_integrals, one thread per
+// column: the vertical integrals in layer order (as the sequential quadrature does), N_a,
+// the sliding law, F2 and beta_eff.  The middle step is layer-parallel (15 x the threads
+// of a column kernel): a single column kernel walking the layers, measured, took 104 us
+// per iteration on the 321 x 561 ice cap against 75 us for the three launches, whose extra
+// read of the viscosity is cheaper than the lost parallelism.  The shear strain rates
+// du/dz, dv/dz (:664-721) are written by the layer step only with WRITE_SHEAR; inside the
+// viscosity loop (K1_LOOP) k_column_prep keeps the basal stress it saw instead, and
+// k_shear_rates writes the last iteration's shear once after the loop.
+__global__ void __launch_bounds__(256) k_column_prep(CoefArgs a) {
   const Dims d = a.d;
-  const int lane = threadIdx.x;
   const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= d.nx) return;        // whole warps: i is uniform across a warp
-  const bool col = j < d.ny;    // lanes past the last row stay for the shuffle
-  const int nx = d.nx, ny = d.ny, ld = d.ld, nz = d.nz;
-  const int jc = col ? j : ny - 1;
-  const long long q = d.at(jc, i);
+  if (j >= d.ny || i >= d.nx) return;
+  const int nx = d.nx, ny = d.ny;
+  const long long q = d.at(j, i);
   const int* __restrict__ mask = a.mask_ice;
   const double* __restrict__ Hi = a.Hi;
-  const double H = Hi[q];
   const bool ice = mask[q] == 1;
-  const bool skip_visc = a.bc_margin && !ice;   // BC margins: no viscosity outside the ice (:759-764)
+  const bool skip_visc = a.bc_margin && !ice;  // BC margins: no viscosity outside the ice (:759-764)
+  // strain rates of the depth-averaged flow (calc_effective_viscosity :751-754)
   double eps_h = 0.0;
-  if (!skip_visc) {   // calc_effective_viscosity :751-754
-    const double du_dx = ddx_cx_to_a(d, a.u, jc, i), dv_dy = ddy_cy_to_a(d, a.v, jc, i);
-    const double du_dy = ddy_cx_to_a(d, a.u, jc, i), dv_dx = ddx_cy_to_a(d, a.v, jc, i);
+  if (!skip_visc) {
+    const double du_dx = ddx_cx_to_a(d, a.u, j, i), dv_dy = ddy_cy_to_a(d, a.v, j, i);
+    const double du_dy = ddy_cx_to_a(d, a.u, j, i), dv_dx = ddx_cy_to_a(d, a.v, j, i);
     eps_h = du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((du_dy + dv_dx) * (du_dy + dv_dx));
   }
+  const double H = Hi[q];
   int flags = skip_visc ? COL_SKIP : 0;
   auto face = [&](int bit, int f, long long p0, long long p1) {
+    // a face carries shear if either side has ice (calc_vertical_shear_strain_rates :685-695)
     if (a.diva && !(mask[p0] == 0 && mask[p1] == 0)) flags |= bit;
     flags |= margin_mode(Hi[p0], Hi[p1]) << (kModeShift + 2 * f);
   };
-  if (i < nx - 1) face(FACE_E, 0, q, d.at(jc, i + 1));
-  if (i > 0) face(FACE_W, 1, d.at(jc, i - 1), q);
-  if (jc < ny - 1) face(FACE_N, 2, q, d.at(jc + 1, i));
-  if (jc > 0) face(FACE_S, 3, d.at(jc - 1, i), q);
-  const int mx = i == 0 ? 2 : (i == nx - 1 ? 1 : margin_mode(Hi[d.at(jc, i - 1)], H));
-  const int my = jc == 0 ? 2 : (jc == ny - 1 ? 1 : margin_mode(Hi[d.at(jc - 1, i)], H));
+  if (i < nx - 1) face(FACE_E, 0, q, d.at(j, i + 1));
+  if (i > 0) face(FACE_W, 1, d.at(j, i - 1), q);
+  if (j < ny - 1) face(FACE_N, 2, q, d.at(j + 1, i));
+  if (j > 0) face(FACE_S, 3, d.at(j - 1, i), q);
+  // a-grid staggering of the face values: first column/row the east/north face alone (2),
+  // last column/row the west/south face alone (1), else the margin rule
+  const int mx = i == 0 ? 2 : (i == nx - 1 ? 1 : margin_mode(Hi[d.at(j, i - 1)], H));
+  const int my = j == 0 ? 2 : (j == ny - 1 ? 1 : margin_mode(Hi[d.at(j - 1, i)], H));
   flags |= (mx << kStagXShift) | (my << kStagYShift);
+  a.col_eps[q] = eps_h;
+  a.col_flags[q] = flags;
+  if (a.keep_seen && a.diva) {   // the basal stress this iteration's shear reads (k_shear_rates)
+    if (i < nx - 1) a.taub_seen_cx[q] = a.taub_cx[q];
+    if (j < ny - 1) a.taub_seen_cy[q] = a.taub_cy[q];
+  }
+}
+
+template <bool WRITE_SHEAR>
+__global__ void __launch_bounds__(kColLanes * kColRows) k_layer_viscosity(CoefArgs a) {
+  const Dims d = a.d;
+  const int lane = threadIdx.x;
+  // the layer is the fastest grid index: blocks running together share their columns'
+  // 2D inputs in L1/L2 instead of streaming them once per layer
+  const int k = blockIdx.x, j = blockIdx.y * kColLanes + lane, i = blockIdx.z * kColRows + threadIdx.y;
+  if (i >= d.nx) return;       // whole warps: i is uniform across a warp
+  const bool col = j < d.ny;   // lanes past the last row stay for the shuffle
+  const int nx = d.nx, ny = d.ny, ld = d.ld;
+  const int q = i * ld + (col ? j : ny - 1);   // plane index (planes hold < 2^31 points)
+  const long long off = (long long)k * d.plane;
+  const double* __restrict__ vp = a.visc_prev + off;
+  const double zk = a.zt.z[k];
+  const int flags = a.col_flags[q];
   const bool has_e = col && i < nx - 1, has_w = col && i > 0, has_n = col && j < ny - 1, has_s = col && j > 0;
   auto mode = [&](int f) { return (flags >> (kModeShift + 2 * f)) & 3; };
-  double tbe = 0.0, tbw = 0.0, tbn = 0.0, tbs = 0.0;
+  double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0, dudz_w = 0.0;
   if (a.diva) {
-    if (has_e) tbe = a.taub_cx[q];
-    if (has_w) tbw = a.taub_cx[q - ld];
-    if (has_n) tbn = a.taub_cy[q];
-    if (has_s && lane == 0) tbs = a.taub_cy[q - 1];
-  }
-  if (col) {
-    a.col_flags[q] = flags;
-    if (a.diva && !WRITE_SHEAR) {
-      if (has_e) a.taub_seen_cx[q] = tbe;
-      if (has_n) a.taub_seen_cy[q] = tbn;
+    const double vq = vp[q];
+    if (has_e) {
+      if (flags & FACE_E) dudz_e = (a.taub_cx[q] / stag_mode(mode(0), vq, vp[q + ld])) * zk;
+      if (WRITE_SHEAR) a.dudz[off + q] = dudz_e;
     }
+    if (has_n) {
+      if (flags & FACE_N) dvdz_n = (a.taub_cy[q] / stag_mode(mode(2), vq, vp[q + 1])) * zk;
+      if (WRITE_SHEAR) a.dvdz[off + q] = dvdz_n;
+    }
+    if (has_w && (flags & FACE_W)) dudz_w = (a.taub_cx[q - ld] / stag_mode(mode(1), vp[q - ld], vq)) * zk;
+    dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
+    if (lane == 0 && has_s)
+      dvdz_s = (flags & FACE_S) ? (a.taub_cy[q - 1] / stag_mode(mode(3), vp[q - 1], vq)) * zk : 0.0;
   }
-  const double* __restrict__ vp = a.visc_prev;
-  double vint = 0.0, fint = 0.0, vprev = 0.0, fprev = 0.0;
-  for (int k = 0; k < nz; ++k) {
-    const long long off = (long long)k * d.plane;
-    const double zk = a.zt.z[k];
-    double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0, dudz_w = 0.0;
+  if (!col) return;
+  double eta = 0.0;
+  if (!(flags & COL_SKIP)) {
+    const int mx = (flags >> kStagXShift) & 3, my = (flags >> kStagYShift) & 3;
+    double du_dz_a, dv_dz_a;
     if (a.diva) {
-      const double vq = vp[off + q];
-      if (has_e && (flags & FACE_E)) dudz_e = (tbe / stag_mode(mode(0), vq, vp[off + q + ld])) * zk;
-      if (has_n && (flags & FACE_N)) dvdz_n = (tbn / stag_mode(mode(2), vq, vp[off + q + 1])) * zk;
-      if (has_w && (flags & FACE_W)) dudz_w = (tbw / stag_mode(mode(1), vp[off + q - ld], vq)) * zk;
-      dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
-      if (lane == 0 && has_s) dvdz_s = (flags & FACE_S) ? (tbs / stag_mode(mode(3), vp[off + q - 1], vq)) * zk : 0.0;
-      if (WRITE_SHEAR) {
-        if (has_e) a.dudz[off + q] = dudz_e;
-        if (has_n) a.dvdz[off + q] = dvdz_n;
-      }
+      du_dz_a = stag_mode(mx, dudz_w, dudz_e);
+      dv_dz_a = stag_mode(my, dvdz_s, dvdz_n);
+    } else {
+      // solve_SSA calls calc_effective_viscosity without refreshing du/dz: use the stored fields
+      const double* dudz = a.dudz + off;
+      const double* dvdz = a.dvdz + off;
+      du_dz_a = stag_mode(mx, i > 0 ? dudz[q - ld] : 0.0, i < nx - 1 ? dudz[q] : 0.0);
+      dv_dz_a = stag_mode(my, j > 0 ? dvdz[q - 1] : 0.0, j < ny - 1 ? dvdz[q] : 0.0);
     }
-    double eta = 0.0;
-    if (!skip_visc) {
-      double du_dz_a, dv_dz_a;
-      if (a.diva) {
-        du_dz_a = stag_mode(mx, dudz_w, dudz_e);
-        dv_dz_a = stag_mode(my, dvdz_s, dvdz_n);
-      } else {
-        // solve_SSA calls calc_effective_viscosity without refreshing du/dz: the stored fields
-        const double* dudz = a.dudz + off;
-        const double* dvdz = a.dvdz + off;
-        du_dz_a = stag_mode(mx, i > 0 ? dudz[q - ld] : 0.0, i < nx - 1 ? dudz[q] : 0.0);
-        dv_dz_a = stag_mode(my, jc > 0 ? dvdz[q - 1] : 0.0, jc < ny - 1 ? dvdz[q] : 0.0);
-      }
-      const double eps_sq = eps_h + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
-      const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
-      eta = max_ref(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
-    }
-    if (col) a.visc[off + q] = eta;
+    const double eps_sq = a.col_eps[q] + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
+    const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
+    eta = max_ref(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
+  }
+  a.visc[off + q] = eta;
+}
+
+// NZ > 0: the layer count known at compile time (the default 15 layers), so the loop is
+// unrolled and every layer's load is in flight at once; NZ = 0: any layer count.
+template <int NZ>
+__global__ void __launch_bounds__(256) k_column_integrals(CoefArgs a) {
+  const Dims d = a.d;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= d.ny || i >= d.nx) return;
+  const int nx = d.nx, ny = d.ny, nz = NZ > 0 ? NZ : d.nz;
+  const long long q = d.at(j, i);
+  const double H = a.Hi[q];
+  const bool ice = a.mask_ice[q] == 1;
+  const bool skip_visc = a.bc_margin && !ice;
+  const double* __restrict__ visc = a.visc;
+  double vint = 0.0, fint = 0.0, vprev = 0.0, fprev = 0.0;
+#pragma unroll
+  for (int k = 0; k < nz; ++k) {
+    const double eta = visc[(long long)k * d.plane + q];
+    const double zk = a.zt.z[k];
     if (k > 0) vint = vint + 0.5 * (eta + vprev) * (zk - a.zt.z[k - 1]);
     vprev = eta;
     if (a.diva) {
@@ -243,7 +277,6 @@ __global__ void __launch_bounds__(kBX * kBY) k_column_coefficients(CoefArgs a) {
       fprev = fk;
     }
   }
-  if (!col) return;
   if (!skip_visc) {
     a.visc_int[q] = vint;
     a.Na[q] = a.bc_margin ? vint * H : vint * max_ref(0.1, H);
@@ -279,6 +312,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_column_coefficients(CoefArgs a) {
     a.beta_eff[q] = beta;   // solve_SSA :193
   }
 }
+
 
 // The shear strain rates du/dz, dv/dz (calc_vertical_shear_strain_rates :664-721) of the last
 // viscosity iteration, from the flags and basal stress its fused K1 kept and the viscosity
@@ -1009,11 +1043,20 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
     DIVA_CUDA(c, cudaMemcpyAsync(c->D(DIVA_F_VISC_EFF_3D_A), c->visc_prev, sizeof(double) * c->d.plane * c->d.nz,
                                  cudaMemcpyDeviceToDevice, c->stream));
   }
-  if (what == K1_WRITE_SHEAR) k_column_coefficients<true><<<G2>>>(a);
-  else k_column_coefficients<false><<<G2>>>(a);
+  a.keep_seen = what != K1_WRITE_SHEAR;
+  k_column_prep<<<G2>>>(a); c->launches++;
+  {
+    const dim3 block(kColLanes, kColRows);
+    const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
+    if (what == K1_WRITE_SHEAR) k_layer_viscosity<true><<<grid, block, 0, c->stream>>>(a);
+    else k_layer_viscosity<false><<<grid, block, 0, c->stream>>>(a);
+    c->launches++;
+  }
+  if (c->d.nz == 15) k_column_integrals<15><<<G2>>>(a);
+  else k_column_integrals<0><<<G2>>>(a);
   c->launches++;
-  if (what == K1_COLUMNS_ONLY) {   // timing of the column kernel alone (diva_profile_kernel)
-    DIVA_LAUNCHED(c, "k_column_coefficients");
+  if (what == K1_COLUMNS_ONLY) {   // timing of the column launches alone (diva_profile_kernel)
+    DIVA_LAUNCHED(c, "column coefficients");
     return DIVA_OK;
   }
   DIVA_LAUNCHED(c, "column coefficients");

@@ -1956,9 +1956,17 @@ int solver_init(Ctx* c) {
 
 // One V-cycle from level l down, entered with x = 0.  b is given in bu/bv, or (rs.on)
 // restricted from the finer level's residual by the level's first kernel.
+// Gauss-Seidel sweeps before and after the coarse correction: on the finest level, and on
+// every coarser level (the tiled levels and the one-block sub-cycle).
+#ifndef DIVA_MG_NU_FINE
+#define DIVA_MG_NU_FINE 2
+#endif
+#ifndef DIVA_MG_NU_COARSE
+#define DIVA_MG_NU_COARSE 2
+#endif
 static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
                   const Restriction& rs) {
-  const int nu1 = 2, nu2 = 2, coarse_sweeps = 64;
+  const int nu1 = l == 0 ? DIVA_MG_NU_FINE : DIVA_MG_NU_COARSE, nu2 = nu1, coarse_sweeps = 64;
   if (l == sub_first_level(c)) {
     SubCycle sc;
     sc.first = l;

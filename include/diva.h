@@ -363,13 +363,13 @@ int  diva_state_save(diva_ctx_t* ctx);
 int  diva_state_restore(diva_ctx_t* ctx);
 
 /* Time one hot kernel of the current state in isolation: `which` selects
- *   0  the column coefficients of one viscosity iteration: the fused column kernel (viscosity,
- *      F2, beta, beta_eff) + the b-grid face kernel
+ *   0  the column coefficients of one viscosity iteration: column prep, layer viscosity and
+ *      column integrals (viscosity, F2, beta, beta_eff) + the b-grid face kernel
  *   1  one full Gauss-Seidel sweep (4 colours) of the fine-level operator
  *   2  one fine-level operator application (matrix-free A x with dot products)
  *   3  one multigrid V-cycle (the preconditioner of one Krylov half-step)
  *   4  the one-block coarse-level part of a V-cycle alone
- *   5  the fused column kernel of 0 alone (k_column_coefficients)
+ *   5  the column launches of 0 without the b-grid face kernel
  * `reps` launches are bracketed by CUDA events on the context's stream;
  * returns the mean device time per launch and the algorithmic bytes one launch
  * must move.  Needs a context that has completed a solve; kind 0 leaves the
