@@ -1,25 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the B200 DIVA velocity solver.
 
-Metric: DIVA solves/s on the 321 x 561 x 15 synthetic ice cap (the 1600 x 2800 km,
-5 km configuration), each solve a cold start run to a relative nonlinear
-residual of 1e-6, followed by the SIA 3D velocities ("DIVA plus SIA").
+Metric: DIVA solves/s at 321 x 561 x 15 to rel-res 1e-6, learned + FP32 vs plain FP64 GPU:
+cold-start DIVA + SIA solves of synthetic ice caps (1600 x 2800 km at 5 km, 15 layers), each
+run to a relative nonlinear residual of 1e-6.  Before the timed region the warm-start network
+is trained on plain FP64 solutions of --members seeded caps (seeds 0..) by the library's own
+tcgen05 kernels; timed step k solves the held-out cap of seed 10000 + k.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...]
 
-One process per GPU (torchrun for N > 1).  A single solve does not shard:
-each rank runs an independent replica of the workload, so per-GPU work is
-fixed as N grows ("scaling": "weak") and there is no data-path collective;
-the only collectives are the timing barrier and the max over ranks.
+One process per GPU (torchrun for N > 1).  A single solve does not shard: each rank runs an
+independent replica of the workload, so per-GPU work is fixed as N grows ("scaling": "weak")
+and there is no data-path collective; the only collectives are the timing barrier and the
+max over ranks.
 
-value : solves/s of the whole job, device-timed with CUDA events on the
-        library's stream, inputs (geometry, masks, rheology) resident in HBM;
-        each step restores the cold-start state (device copy), solves and
-        computes the SIA velocities.
-e2e   : the same through the public API with host buffers: every step uploads
-        the inputs and the cold-start state from pinned host memory, prepares
-        them on the GPU (update_general_ice_model_data, rheology), solves, and
-        downloads the velocity fields.
+value : learned-path solves/s of the whole job -- network warm start (prediction plus 10
+        state-completion sweeps), FP32 finest-level smoother inside the FP64 BiCGStab,
+        Anderson mixing of the viscosity iteration -- device-timed with CUDA events on the
+        solve's stream around predict + solve + SIA, inputs resident in HBM.  The plain FP64
+        path (the reference's relaxed Picard update) on the same geometries is reported in
+        config as the denominator of the learned + FP32 vs plain FP64 ratio.
+e2e   : the learned path through the public API with host buffers: every step uploads the
+        geometry's inputs and the cold-start state from pinned host memory, prepares them on
+        the GPU (update_general_ice_model_data, rheology), predicts, solves, computes the SIA
+        velocities and downloads the velocity fields.
+--impl reference : the CPU port of the reference path on the host threads, one full cold
+        solve of the same geometries per step.
 """
 import argparse
 import json
@@ -59,12 +65,12 @@ KERNEL_NAMES = {0: "K1 column coefficients (all launches of one viscosity iterat
 TRAFFIC_KEYS = {0: "k1_icecap321x561", 3: "vcycle_icecap321x561"}
 
 
-def workload(seed=2, precision="fp64", anderson=0, eta=None):
+def workload(seed=2, precision="fp64", anderson=0, eta=None, dx=None):
     """The ice cap, solved cold to rel-res 1e-6.  anderson = 0: the reference's relaxed
     Picard update with the adaptive linear tolerance 0.5 min(1, rel-res); anderson = m > 0:
     Anderson mixing of depth m, linear tolerance factor 0.1 unless eta is given."""
     from imau_ice_b200 import synth
-    g, cfg, fields = synth.ice_cap(seed=seed)
+    g, cfg, fields = synth.ice_cap(seed=seed, **({"dx": dx} if dx else {}))
     cfg = dict(cfg)
     cfg.update(picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1, lin_rtol=1e-10,
                precision=precision, picard_anderson_m=anderson,
@@ -160,7 +166,7 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def cpu_baseline(threads=None):
+def cpu_baseline(threads=None, seed=2, dx=None):
     """The oracle (a CPU port of the reference path) on the same workload: one full cold
     solve to rel-res 1e-6 plus the SIA velocities, timed.  Linear solves: GMRES(30) +
     ILU(0) from the current iterate, right-preconditioned so that it tests the true
@@ -172,7 +178,7 @@ def cpu_baseline(threads=None):
     import oracle_backend
     from imau_ice_b200 import diva
     orc = oracle_backend.oracle_backend()
-    g, cfg, fields = workload()
+    g, cfg, fields = workload(seed=seed, dx=dx)
     grid = diva.Grid(**g)
     ctx = diva.Context(grid, cfg, orc)
     oracle_backend.set_linear_solver(ctx, oracle_backend.LIN_GMRES_WARM, rtol=1e-10, abstol=0.0)
@@ -188,7 +194,7 @@ def cpu_baseline(threads=None):
     t = time.perf_counter() - t0
     ctx.close()
     return {"value": 1.0 / t, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": (f"one full cold solve at 321x561x15 to rel-res {rep['relres']:.2e} "
+            "sample": (f"one full cold solve of ice cap seed {seed} at 321x561x15 to rel-res {rep['relres']:.2e} "
                        f"({rep['picard_iterations']} viscosity iterations, {rep['linear_iterations']} GMRES "
                        f"iterations) plus SIA, {t:.1f} s on {threads} threads")}
 
@@ -249,29 +255,42 @@ def run_cpu_variants(args):
 
 
 def run_reference(args):
+    """The reference arm: the CPU port of the reference path (relaxed Picard update, GMRES +
+    ILU(0)) on all host threads, one full cold solve per step of the same workload as the
+    default line (the headline: held-out ice-cap seed 10000 + k at step k; --workload icecap:
+    the fixed seed-2 cap).  Warm-up steps solve the 40 km ice cap (81 x 141) so they stay
+    short.  Rank 0 alone runs and prints."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     load_package()
+    headline = args.workload == "headline"
     g, _, _ = workload()
-    vals = []
+    secs = []
     threads = min(host_threads(), 64)
     for _ in range(args.warmup):
-        cpu_baseline(threads)
-    for _ in range(args.steps):
-        last = cpu_baseline(threads)
-        vals.append(last["value"])
-    v = statistics.mean(vals)
-    out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        cpu_baseline(threads, seed=2, dx=40e3)
+    last = None
+    for k in range(args.steps):
+        last = cpu_baseline(threads, seed=held_out_seed(k) if headline else 2)
+        secs.append(1.0 / last["value"])
+    v = args.steps / sum(secs)
+    out = {"metric": HEADLINE_METRIC if headline else METRIC, "value": v, "unit": UNIT, "impl": "reference",
+           "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ice cap)",
-           "config": config_json(g, {"parallelism": f"CPU oracle port on {threads} host threads (block-Jacobi "
+           "config": config_json(g, {**({"workload": "DIVA+SIA cold-start solves of held-out synthetic ice caps "
+                                                     "1600x2800 km @5 km, one geometry per step",
+                                         "seeds": [held_out_seed(k) for k in range(args.steps)]} if headline else {}),
+                                     "parallelism": f"CPU oracle port on {threads} host threads (block-Jacobi "
                                                      f"ILU(0) over {threads} row blocks, column loops split)",
                                      "nonlinear_iteration": "the reference's relaxed Picard update (relax 0.4)",
                                      "linear_solver": "GMRES(30) + ILU(0) from the current iterate, adaptive "
                                                       "tolerance 0.5 min(1, rel-res)"}),
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                            "sample": "each step " + last["sample"]},
+                            "sample": ("each step one full cold solve of the step's geometry (held-out ice-cap seeds "
+                                       f"10000..{held_out_seed(args.steps - 1)})" if headline else "each step " +
+                                       last["sample"])},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -445,6 +464,263 @@ def run_b200(args):
                 res["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
         print(json.dumps(res))
     ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+HEADLINE_METRIC = "DIVA solves/s at 321x561x15 to rel-res 1e-6: learned+FP32 vs plain FP64 GPU"
+
+
+def held_out_seed(k):
+    """Geometry of timed step k: held-out ice caps, never in the training set (seeds 0..)."""
+    return 10000 + k
+
+
+def headline_case(seed, learned_path, anderson=3, eta=0.1):
+    """The seeded ice cap and its solve settings: the learned path (FP32 smoother, Anderson
+    mixing, tighter adaptive linear tolerance) or the plain FP64 path (the reference's
+    relaxed Picard update)."""
+    from imau_ice_b200 import synth
+    g, cfg, f = synth.ice_cap(seed=seed)
+    cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
+               lin_rtol=1e-10)
+    if learned_path:
+        cfg.update(precision="mixed", picard_anderson_m=anderson, lin_adaptive_eta=eta)
+    else:
+        cfg.update(precision="fp64", picard_anderson_m=0, lin_adaptive_eta=0.5)
+    return g, cfg, f
+
+
+def train_warm_start(grid, members, epochs):
+    """The warm-start network trained on `members` plain FP64 solutions (seeds 0..) by the
+    library's own tcgen05 forward and backward kernels; returns (net, loss, seconds)."""
+    from imau_ice_b200 import diva, learned
+    net = learned.WarmStartNet(grid, batch=8, capacity=members, seed=0)
+    net.velocities_only()                  # predict completes the rest of the state
+    t0 = time.perf_counter()
+    seed = 0
+    while net.num_samples < members and seed < 4 * members:
+        g, cfg, f = headline_case(seed, False)
+        ctx = diva.Context(diva.Grid(**g), cfg)
+        ctx.upload(f)
+        ctx.update_general_ice_model_data()
+        ctx.calc_pressure_melting_point()
+        ctx.calc_ice_rheology()
+        ctx.update_general_ice_model_data()
+        if ctx.solve_DIVA()["status"] == 0:
+            net.add_sample(ctx)
+        ctx.close()
+        seed += 1
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss = net.train(epochs, lr=1e-3, seed=1)
+    return net, loss, t_data, time.perf_counter() - t0
+
+
+def run_headline(args):
+    """The headline line: DIVA + SIA solves of held-out 321 x 561 x 15 ice caps to rel-res
+    1e-6 through the learned path (network warm start, FP32 finest-level smoother, Anderson
+    mixing), with the plain FP64 GPU path on the same geometries as its denominator.
+    value: learned-path solves/s, device-timed with CUDA events around predict + solve +
+    SIA on the solve's stream (inputs resident); e2e: the same through the public API with
+    host buffers (upload, data-model update, predict, solve, SIA, download)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    load_package()
+    from imau_ice_b200 import build, diva
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    build.build()
+    g0 = headline_case(0, True)[0]
+    grid = diva.Grid(**g0)
+    net, loss, t_data, t_train = train_warm_start(grid, args.members, args.epochs)
+    stream = torch.cuda.Stream()
+
+    def prepared(seed, learned_path):
+        g, cfg, f = headline_case(seed, learned_path, args.anderson or 3, args.eta or 0.1)
+        ctx = diva.Context(grid, cfg)
+        ctx.set_stream(stream.cuda_stream)
+        ctx.upload(f)
+        ctx.update_general_ice_model_data()
+        ctx.calc_pressure_melting_point()
+        ctx.calc_ice_rheology()
+        ctx.update_general_ice_model_data()
+        return ctx
+
+    def device_solve(seed, learned_path, keep=False):
+        ctx = prepared(seed, learned_path)
+        torch.cuda.synchronize()
+        l0 = ctx.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if learned_path:
+            net.predict(ctx, complete_sweeps=10)
+        try:
+            rep = ctx.solve_DIVA()
+        except diva.DivaError as e:
+            rep = {"status": e.status, "picard_iterations": -1, "mg_cycles": -1, "relres": -1.0}
+        ctx.calc_sia_3d_velocities()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = ctx.kernel_launches() - l0
+        if keep:
+            return e0.elapsed_time(e1), rep, launches, ctx
+        ctx.close()
+        return e0.elapsed_time(e1), rep, launches
+
+    for k in range(args.warmup):
+        device_solve(20000 + k, True)
+        device_solve(20000 + k, False)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    learned_runs = [device_solve(held_out_seed(k), True) for k in range(args.steps)]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    plain_runs = [device_solve(held_out_seed(k), False) for k in range(args.steps)]
+    t = torch.tensor([sum(r[0] for r in learned_runs), sum(r[0] for r in plain_runs)], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_learned, ms_plain = float(t[0]), float(t[1])
+    value = world * args.steps / (ms_learned / 1000.0)
+    plain_value = world * args.steps / (ms_plain / 1000.0)
+
+    # roofline: the dominant part of a learned-path solve, timed alone on its converged state
+    _, rep_k, _, ctx = device_solve(held_out_seed(0), True, keep=True)
+    prof = {w: ctx.profile_kernel(w, reps=30 if w else 10) for w in (0, 1, 2, 3, 4, 5)}
+    ctx.close()
+    its = statistics.mean(r[1]["picard_iterations"] for r in learned_runs)
+    cyc = statistics.mean(r[1]["mg_cycles"] for r in learned_runs)
+    per_solve = {0: prof[0][0] * its, 3: prof[3][0] * cyc}
+    dom = max(per_solve, key=per_solve.get)
+    ms_l, bytes_l = prof[dom]
+    try:
+        hbm_peak, peak_src = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"], \
+            "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        hbm_peak, peak_src = 6650.0, "fallback 6650 GB/s"
+    achieved = bytes_l / (ms_l * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": read_traffic(TRAFFIC_KEYS[dom]), "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": bytes_l, "ms_per_launch": ms_l,
+                "launches_per_solve": its if dom == 0 else cyc,
+                "other_kernels": {KERNEL_NAMES[w]: {"ms_per_launch": prof[w][0], "algorithmic_bytes": prof[w][1],
+                                                    "GB/s": prof[w][1] / (prof[w][0] * 1e-3) / 1e9} for w in prof},
+                "ms_per_solve": {KERNEL_NAMES[w]: per_solve[w] for w in per_solve}}
+
+    # end to end through the public API: pinned host inputs of every step's geometry, the
+    # cold-start state, and pinned outputs
+    def pinned(a):
+        t_ = torch.empty(a.shape[::-1], dtype=torch.float64 if a.dtype == np.float64 else torch.int32,
+                         pin_memory=True)
+        h = t_.numpy().T
+        h[...] = a
+        return h, t_
+
+    keep = []
+    host_inputs = []
+    for k in range(args.steps):
+        f = headline_case(held_out_seed(k), True)[2]
+        hk = {}
+        for n in INPUT_FIELDS:
+            h, t_ = pinned(np.asarray(f[n]))
+            hk[n] = h
+            keep.append(t_)
+        host_inputs.append(hk)
+    ectx = prepared(held_out_seed(0), True)
+    host_state, host_out = {}, {}
+    for n in STATE_FIELDS:
+        h, t_ = pinned(np.zeros_like(ectx.empty(n)))
+        host_state[n] = h
+        keep.append(t_)
+    for n in OUTPUT_FIELDS:
+        h, t_ = pinned(ectx.empty(n))
+        host_out[n] = h
+        keep.append(t_)
+    h2d = sum(a.nbytes for a in host_inputs[0].values()) + sum(a.nbytes for a in host_state.values())
+    d2h = sum(a.nbytes for a in host_out.values())
+
+    def e2e_step(k):
+        ectx.upload(host_inputs[k])
+        ectx.upload(host_state)
+        ectx.update_general_ice_model_data()
+        ectx.calc_pressure_melting_point()
+        ectx.calc_ice_rheology()
+        ectx.update_general_ice_model_data()
+        net.predict(ectx, complete_sweeps=10)
+        try:
+            ectx.solve_DIVA()
+        except diva.DivaError:
+            pass
+        ectx.calc_sia_3d_velocities()
+        return ectx.download(OUTPUT_FIELDS, out=host_out)
+
+    e2e_step(0)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        e2e_step(k)
+    torch.cuda.synchronize()
+    te = torch.tensor([time.perf_counter() - t0], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    e2e_val = world * args.steps / float(te.item())
+    ectx.close()
+
+    if rank == 0:
+        res = {"metric": HEADLINE_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_learned / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+               "data": "synthetic (seeded ice caps; network trained on seeds 0.., timed on held-out seeds 10000..)",
+               "config": {
+                   "workload": "DIVA+SIA cold-start solves of held-out synthetic ice caps 1600x2800 km @5 km, "
+                               "one geometry per step",
+                   "nx": grid.nx, "ny": grid.ny, "nz": grid.nz, "stop": "nonlinear rel-res <= 1e-6",
+                   "learned_path": "warm start by the trained network (10 state-completion sweeps), FP32 "
+                                   "finest-level smoother in the FP64 BiCGStab, Anderson mixing of depth "
+                                   f"{args.anderson or 3}, adaptive linear tolerance {args.eta or 0.1:g} min(1, rel-res)",
+                   "plain_path": "FP64 throughout, the reference's relaxed Picard update (relax 0.4), adaptive "
+                                 "linear tolerance 0.5 min(1, rel-res)",
+                   "plain_fp64_solves_per_s": plain_value,
+                   "ratio_learned_vs_plain_fp64": value / plain_value,
+                   "seeds": [held_out_seed(k) for k in range(args.steps)],
+                   "iterations_learned": [r[1]["picard_iterations"] for r in learned_runs],
+                   "iterations_plain": [r[1]["picard_iterations"] for r in plain_runs],
+                   "mg_cycles_learned": [r[1]["mg_cycles"] for r in learned_runs],
+                   "mg_cycles_plain": [r[1]["mg_cycles"] for r in plain_runs],
+                   "status_learned": [r[1]["status"] for r in learned_runs],
+                   "relres_learned": [r[1]["relres"] for r in learned_runs],
+                   "training": {"samples": net.num_samples, "epochs": args.epochs, "final_loss": loss,
+                                "data_generation_s": round(t_data, 2), "training_s": round(t_train, 2)},
+                   "parallelism": f"replicas x{world} (a single solve does not shard)",
+                   "l2": "inputs larger than L2: each step is a whole solve over ~0.6 GB of device state; the 3D "
+                         "fields (21.6 MB each) stream from HBM every viscosity iteration, the 2D multigrid "
+                         "levels (~17 MB at level 0) stay L2-resident within a solve; no flush"},
+               "roofline": roofline, "clocks": clk,
+               "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                       "timing": "host wall clock with device synchronisation, max over ranks"},
+               "gpu_launches": int(sum(r[2] for r in learned_runs))}
+        if not args.no_cpu_baseline:
+            try:
+                res["cpu_baseline"] = cpu_baseline(seed=held_out_seed(0))
+            except Exception as ex:   # the baseline is reported, never required
+                res["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
+        print(json.dumps(res))
+    net.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
@@ -713,9 +989,11 @@ def main():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true",
                    help="timed solves only (no roofline, e2e or CPU legs): the command profiled with ncu")
-    p.add_argument("--workload", choices=["icecap", "ensemble", "timestep", "learned", "cpu-variants"],
-                   default="icecap",
-                   help="icecap: the headline solve (default); ensemble: --members perturbed members; "
+    p.add_argument("--workload", choices=["headline", "icecap", "ensemble", "timestep", "learned", "cpu-variants"],
+                   default="headline",
+                   help="headline (default): held-out ice caps through the learned path (trained network, "
+                        "FP32 smoother, Anderson mixing) against the plain FP64 path; icecap: the plain FP64 solve "
+                        "of one fixed ice cap; ensemble: --members perturbed members; "
                         "timestep: predictor/corrector steps with thickness and heat equation; "
                         "learned: --members training caps, then held-out solves cold vs warm-started")
     p.add_argument("--epochs", type=int, default=60, help="training epochs of the learned workload")
@@ -739,6 +1017,8 @@ def main():
         return run_cpu_variants(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "headline":
+        return run_headline(args)
     return run_b200(args)
 
 

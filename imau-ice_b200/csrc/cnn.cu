@@ -1234,6 +1234,9 @@ int32_t diva_cnn_predict(diva_cnn_t* N, diva_ctx_t* ctx, int32_t complete_sweeps
   RET(forward(N, N->act[T_IN], N->out, 1, c->stream));
   k_apply<<<img_grid(N->ny, N->nx), block2d(), 0, c->stream>>>(c->d, N->out, state_ptrs(c), N->Wp,
                                                                 complete_sweeps > 0, c->c.DIVA_vel_max);
+  // the context's launch count includes the network's kernels run on its stream: features,
+  // 10 convolutions, 2 pools, 2 up-concatenations, the head and the state write
+  c->launches += 17;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   RET(check_err(N));
