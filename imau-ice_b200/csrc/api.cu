@@ -186,7 +186,8 @@ size_t carve(Ctx* c, Carver& cv) {
   c->col_eps = (double*)cv.take(sizeof(double) * d.plane);
   c->col_flags = (int*)cv.take(sizeof(int) * d.plane);
   for (int q = 0; q < 2; ++q) c->taub_seen[q] = (double*)cv.take(sizeof(double) * d.plane);
-  for (int k = 0; k < 6; ++k) c->f32[k] = (float*)cv.take(sizeof(float) * d.plane);
+  for (int l = 0; l < c->nlev; ++l)
+    for (int k = 0; k < 6; ++k) c->f32[l][k] = (float*)cv.take(sizeof(float) * c->lv[l].d.plane);
   c->rtu = (int8_t*)cv.take(d.plane);
   c->rtv = (int8_t*)cv.take(d.plane);
   c->ff_ocean = (int*)cv.take(sizeof(int) * 2 * d.plane);

@@ -37,7 +37,7 @@ struct BCs {
   int uW, uE, uS, uN, vW, vE, vS, vN;
 };
 
-// Float planes of the finest level for the mixed-precision preconditioner.
+// Float planes of each tiled level for the mixed-precision preconditioner.
 enum { F32_NA = 0, F32_NB, F32_BX, F32_BY, F32_IDU, F32_IDV };
 
 // Krylov vectors on the fine level, each a (u,v) pair of planes.
@@ -187,7 +187,7 @@ struct Ctx {
   double* col_eps = nullptr;          // column coefficients: mean-flow strain rate per column
   int* col_flags = nullptr;           // column coefficients: shear faces with ice
   double* taub_seen[2] = {};          // basal stress (cx, cy) the last K1 of the viscosity loop read
-  float* f32[6] = {};                 // float copies of the finest level (F32_*, precision 'mixed')
+  float* f32[kMaxLevels][6] = {};     // float copies of each tiled level (F32_*, precision 'mixed')
   int8_t* rtu = nullptr;              // finest-level row types ('BC' ice margins)
   int8_t* rtv = nullptr;
   int* ff_ocean = nullptr;            // flood-fill state

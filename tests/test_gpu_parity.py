@@ -44,8 +44,6 @@ CASES = {
     "icecap_40km": (2, 40e3, {"lin_rtol": 1e-12}),
     "channel_5km_relres": (1, None, {"picard_stop": "relres", "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 300,
                                      "lin_rtol": 1e-12}),
-    # precision 'mixed': FP32 finest-level smoother inside the FP64 Krylov solve, against the FP64 oracle
-    "channel_5km_mixed": (1, None, {"lin_rtol": 1e-12, "precision": "mixed"}),
     # calving fronts with the 'BC' margin rows (stress boundary condition, shelf-next-to-land identities)
     "channel_front_BC_relres": (1, None, {"choice_ice_margin": "BC", "picard_stop": "relres",
                                           "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 300, "lin_rtol": 1e-12},
@@ -235,3 +233,28 @@ def test_full_size_icecap_velocities_within_1e6(full_pair):
         assert helpers.rel_l2(og[k], oo[k]) <= 1e-6, k
     if "relres" in name:
         assert 0 <= rg["relres"] <= 1e-6 and 0 <= ro["relres"] <= 1e-6
+
+
+@pytest.mark.parametrize("stop", ["reference_stop", "relres"])
+def test_mixed_precision_error_against_the_fp64_oracle(cuda, oracle, stop):
+    """Precision 'mixed' (SURVEY config 3: the viscosity of the linearisation and the
+    multigrid smoothing in FP32, the Krylov solve, nonlinear residual, update and Picard
+    norms in FP64) on the marine channel, against the FP64 oracle: the error the FP32
+    viscosity leaves in the converged velocities, relative L2 and max |du| in m/yr."""
+    ov = {"lin_rtol": 1e-12, "DIVA_visc_it_nit": 300}
+    if stop == "relres":
+        ov.update(picard_stop="relres", picard_relres_tol=1e-6)
+    g, cfg, f = helpers.make_case(1, overrides=ov)
+    rg, og = helpers.run(cuda, g, dict(cfg, precision="mixed"), f)
+    ro, oo = helpers.run(oracle, g, cfg, f, oracle_solver=ORACLE_SOLVER)
+    for m in MASKS:
+        assert np.array_equal(og[m], oo[m]), m
+    assert rg["status"] == 0 and ro["status"] == 0, (rg, ro)
+    a = np.concatenate([og["u_vav_cx"].ravel(), og["v_vav_cy"].ravel()])
+    b = np.concatenate([oo["u_vav_cx"].ravel(), oo["v_vav_cy"].ravel()])
+    rel, dmax = helpers.rel_l2(a, b), float(np.abs(a - b).max())
+    print(f"mixed vs FP64 oracle ({stop}): rel-L2 {rel:.3e}, max |du| {dmax:.3e} m/yr, "
+          f"iterations {rg['picard_iterations']} / {ro['picard_iterations']}")
+    assert rel <= 1e-5, rel
+    assert abs(rg["picard_iterations"] - ro["picard_iterations"]) <= 2
+
