@@ -5,7 +5,7 @@ Metric: DIVA solves/s at 321 x 561 x 15 to rel-res 1e-6, learned + FP32 vs plain
 cold-start DIVA + SIA solves of synthetic ice caps (1600 x 2800 km at 5 km, 15 layers), each
 run to a relative nonlinear residual of 1e-6.  Before the timed region the warm-start network
 is trained on plain FP64 solutions of --members seeded caps (seeds 0..) by the library's own
-tcgen05 kernels; timed step k solves the held-out cap of seed 10000 + k.
+tcgen05 kernels; timed step k solves held-out cap HELD_OUT_SEEDS[k] (seeds from 10000 on).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...]
 
@@ -288,8 +288,8 @@ def run_reference(args):
                                      "linear_solver": "GMRES(30) + ILU(0) from the current iterate, adaptive "
                                                       "tolerance 0.5 min(1, rel-res)"}),
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                            "sample": ("each step one full cold solve of the step's geometry (held-out ice-cap seeds "
-                                       f"10000..{held_out_seed(args.steps - 1)})" if headline else "each step " +
+                            "sample": ("each step one full cold solve of the step's geometry (the first "
+                                       f"{args.steps} held-out ice-cap seeds of the list)" if headline else "each step " +
                                        last["sample"])},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -472,9 +472,25 @@ def run_b200(args):
 HEADLINE_METRIC = "DIVA solves/s at 321x561x15 to rel-res 1e-6: learned+FP32 vs plain FP64 GPU"
 
 
+# Held-out ice caps of the headline line: the seeds from 10000 on whose plain FP64 solve
+# reaches rel-res 1e-6 within 500 viscosity iterations.  Of seeds 10000-10099, 29 do not:
+# their fastest ice runs into the reference's 5000 m/yr velocity limit (apply_velocity_limits,
+# ice_velocity_module.f90:1432-1498), and the fixed point of the limited iteration does not
+# solve the unlimited equations, so no method reaches rel-res 1e-6 there.  The list was taken
+# from one scan of those 100 seeds with the plain FP64 path on a B200 (76-267 iterations for
+# the 71 that converge) and is fixed here, so both arms of the bench time the same geometries.
+HELD_OUT_SEEDS = [
+    10000, 10001, 10002, 10003, 10004, 10005, 10010, 10011, 10012, 10014, 10015, 10016, 10017, 10018,
+    10019, 10021, 10023, 10024, 10026, 10027, 10028, 10029, 10031, 10034, 10036, 10038, 10040, 10041,
+    10042, 10043, 10049, 10050, 10051, 10052, 10053, 10054, 10056, 10057, 10058, 10059, 10060, 10061,
+    10062, 10063, 10064, 10065, 10066, 10067, 10068, 10069, 10070, 10071, 10073, 10074, 10079, 10080,
+    10081, 10083, 10084, 10085, 10086, 10088, 10089, 10090, 10091, 10093, 10094, 10096, 10097, 10098,
+    10099]
+
+
 def held_out_seed(k):
     """Geometry of timed step k: held-out ice caps, never in the training set (seeds 0..)."""
-    return 10000 + k
+    return HELD_OUT_SEEDS[k % len(HELD_OUT_SEEDS)]
 
 
 def headline_case(seed, learned_path, anderson=3, eta=0.1):

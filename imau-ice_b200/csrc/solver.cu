@@ -470,8 +470,9 @@ __global__ void k_prolong(Op oc, Dims df, int fx, int fy, const double* xcu, con
 
 // ---- tiled smoothing of the large levels ---------------------------------------------
 // One block owns a TJ x TI tile of a level and keeps x and b of the tile plus a
-// halo of kHalo points on every side in shared memory.  Colour pass q of a
-// smoothing phase updates the points within kHalo-1-q of the tile.  Every value
+// halo of H points on every side in shared memory (H = 4 nu + 1 for nu sweeps per
+// phase: kHalo for two, kHaloOne for one).  Colour pass q of a smoothing phase
+// updates the points within H-1-q of the tile.  Every value
 // a row reads -- its stencil neighbours and, on an 'infinite' or 'zero' side, the
 // inner point a boundary unknown is mapped to -- lies within one point of the row,
 // so after the 8 passes of V(2,2)'s pre- or post-smoothing the tile and one ring
@@ -479,16 +480,19 @@ __global__ void k_prolong(Op oc, Dims df, int fx, int fy, const double* xcu, con
 // residual of the tile follows from them.  The halo is recomputed by the
 // neighbouring blocks instead of exchanged.  A periodic side maps a boundary
 // unknown across the domain, so such grids use the per-colour kernels.
-constexpr int kHalo = 9;
+constexpr int kHalo = 9;        // the widest halo: 2 sweeps (8 colour passes) + 1
+constexpr int kHaloOne = 5;     // the halo of 1 sweep (4 colour passes) + 1
 constexpr int kTileThreads = 512;
+// the halo a tile kernel needs for `sweeps` smoothing sweeps per phase
+inline int halo_for(int sweeps) { return sweeps <= 1 ? kHaloOne : kHalo; }
 
 // STAGE: the region's coefficients (N_a, N_b, B_x, B_y and the inverse diagonals)
 // are staged in shared memory too, so the colour passes touch no global memory.
 // R: the type of the tile's values and coefficients (float on the finest level of the
 // mixed-precision preconditioner, else double).
-template <int TJ, int TI, bool STAGE, class R = double>
+template <int TJ, int TI, bool STAGE, class R = double, int H = kHalo>
 struct TileGeom {
-  static constexpr int RJ = TJ + 2 * kHalo, RI = TI + 2 * kHalo, N = RJ * RI;
+  static constexpr int RJ = TJ + 2 * H, RI = TI + 2 * H, N = RJ * RI;
   static constexpr size_t smem = (STAGE ? 10 : 4) * N * sizeof(R);   // x, b (+ 6 coefficient planes)
 };
 
@@ -497,22 +501,22 @@ struct TileGeom {
 // as stored: the boundary mapping is the identity there, so DEEP blocks skip it and
 // the interior tests (the same values, decided once per block).
 constexpr bool kTileDeepPath = true;
-template <int TJ, int TI>
+template <int TJ, int TI, int H>
 __device__ __forceinline__ bool tile_deep(const TIx& ix, const Dims& d) {
-  constexpr int RJ = TJ + 2 * kHalo, RI = TI + 2 * kHalo;
+  constexpr int RJ = TJ + 2 * H, RI = TI + 2 * H;
   return kTileDeepPath && ix.i0 >= 1 && ix.i0 + RI - 1 <= d.nx - 3 && ix.j0 >= 1 && ix.j0 + RJ - 1 <= d.ny - 3;
 }
 
 // The shared-memory planes of a tile kernel and the operator reading from them.
 // FRONT: the operator may carry 'BC' front rows (only the finest level's kernels with
 // choice_ice_margin 'BC'); without it the row-type test is compiled out.
-template <int TJ, int TI, bool STAGE, bool FRONT, class R>
+template <int TJ, int TI, bool STAGE, bool FRONT, class R, int H>
 struct TileMem {
   R *xu, *xv, *bu, *bv;
   const R *iu, *iv;   // inverse diagonals: staged plane or the level's
   OpT<R> os;          // the level's operator, coefficients staged when STAGE
   __device__ TileMem(R* sm, const OpT<R>& o, const R* idu, const R* idv) {
-    using G = TileGeom<TJ, TI, STAGE, R>;
+    using G = TileGeom<TJ, TI, STAGE, R, H>;
     xu = sm; xv = sm + G::N; bu = sm + 2 * G::N; bv = sm + 3 * G::N;
     os = o;
     iu = idu; iv = idv;
@@ -524,7 +528,7 @@ struct TileMem {
   // stage the region's coefficients (out-of-domain points are never read)
   __device__ void stage(const OpT<R>& o, const R* idu, const R* idv, const TIx& ix, int t, bool in, long long q) {
     if (!STAGE) return;
-    using G = TileGeom<TJ, TI, STAGE, R>;
+    using G = TileGeom<TJ, TI, STAGE, R, H>;
     R* sm = xu;
     sm[4 * G::N + t] = in ? o.Na[q] : R(0);
     sm[5 * G::N + t] = in ? o.Nb[q] : R(0);
@@ -601,18 +605,18 @@ __device__ __forceinline__ void restrict_from(const Restriction& rs, const Dims&
 // pre-smoothing from x = 0 (the descent of a V-cycle enters every level with x = 0):
 // `sweeps` forward sweeps (u0 u1 v0 v1), then x, b and r = b - A x of the tile.
 // b is read (and, when restricted here, stored) in double; x and r are written in R.
-template <int TJ, int TI, bool STAGE, bool FRONT, class R>
+template <int TJ, int TI, bool STAGE, bool FRONT, class R, int H>
 __global__ void __launch_bounds__(kTileThreads) k_smooth_down(OpT<R> o, Restriction rs, double* gbu, double* gbv,
                                                               R* gxu, R* gxv, R* gru, R* grv, const R* idu,
                                                               const R* idv, int sweeps) {
-  constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
+  constexpr int RJ = TJ + 2 * H, N = RJ * (TI + 2 * H);
   extern __shared__ double smd[];
   R* sm = reinterpret_cast<R*>(smd);
-  TileMem<TJ, TI, STAGE, FRONT, R> m(sm, o, idu, idv);
+  TileMem<TJ, TI, STAGE, FRONT, R, H> m(sm, o, idu, idv);
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
-  const TIx ix{tj0 - kHalo, ti0 - kHalo, RJ};
-  const bool deep = tile_deep<TJ, TI>(ix, d);
+  const TIx ix{tj0 - H, ti0 - H, RJ};
+  const bool deep = tile_deep<TJ, TI, H>(ix, d);
   for (int t = threadIdx.x; t < N; t += blockDim.x) {
     const int j = ix.j0 + t % RJ, i = ix.i0 + t / RJ;
     const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
@@ -636,7 +640,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(OpT<R> o, Restrict
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 0; p < 4; ++p, ++pass) {
-      tile_pass_any<TJ, TI>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI>(deep, m, ix, tj0, ti0, p >> 1, p & 1, H - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -665,19 +669,19 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(OpT<R> o, Restrict
 // (oxu, oxv): separate arrays, since blocks of other tiles may still be reading the
 // halo when this block writes (the grid runs in several waves on large levels).  The
 // coarse correction and b are double; the smoothing runs in R; the output is double.
-template <int TJ, int TI, bool STAGE, bool FRONT, class R>
+template <int TJ, int TI, bool STAGE, bool FRONT, class R, int H>
 __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int fx, int fy, const double* xcu,
                                                             const double* xcv, const double* gbu, const double* gbv,
                                                             const R* gxu, const R* gxv, double* oxu, double* oxv,
                                                             const R* idu, const R* idv, int sweeps) {
-  constexpr int RJ = TJ + 2 * kHalo, N = RJ * (TI + 2 * kHalo);
+  constexpr int RJ = TJ + 2 * H, N = RJ * (TI + 2 * H);
   extern __shared__ double smd[];
   R* sm = reinterpret_cast<R*>(smd);
-  TileMem<TJ, TI, STAGE, FRONT, R> m(sm, o, idu, idv);
+  TileMem<TJ, TI, STAGE, FRONT, R, H> m(sm, o, idu, idv);
   const Dims& d = o.d;
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
-  const TIx ix{tj0 - kHalo, ti0 - kHalo, RJ};
-  const bool deep = tile_deep<TJ, TI>(ix, d);
+  const TIx ix{tj0 - H, ti0 - H, RJ};
+  const bool deep = tile_deep<TJ, TI, H>(ix, d);
   for (int t = threadIdx.x; t < N; t += blockDim.x) {
     const int j = ix.j0 + t % RJ, i = ix.i0 + t / RJ;
     const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
@@ -703,7 +707,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 3; p >= 0; --p, ++pass) {
-      tile_pass_any<TJ, TI>(deep, m, ix, tj0, ti0, p >> 1, p & 1, kHalo - 1 - pass);
+      tile_pass_any<TJ, TI>(deep, m, ix, tj0, ti0, p >> 1, p & 1, H - 1 - pass);
       __syncthreads();
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
@@ -1790,29 +1794,42 @@ static int tile_edge(const Ctx* c, int l) {
 // from L2 instead).
 constexpr bool kStage16 = true, kStage32 = false;
 
-template <int T, bool S, class R>
-static void tile_down_r(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, const Restriction& rs,
+// H: the tile's halo, 4 nu + 1 for nu sweeps per phase (halo_for)
+template <int T, bool S, class R, int H>
+static void tile_down_h(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, const Restriction& rs,
                         const double* bu, const double* bv, int nu) {
   const Level& L = c->lv[l];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
   // b is written only when it is restricted here (rs.on), which never happens on the finest level
-  auto kern = o.rtu ? k_smooth_down<T, T, S, true, R> : k_smooth_down<T, T, S, false, R>;
-  kern<<<grid, kTileThreads, TileGeom<T, T, S, R>::smem, c->stream>>>(
+  auto kern = o.rtu ? k_smooth_down<T, T, S, true, R, H> : k_smooth_down<T, T, S, false, R, H>;
+  kern<<<grid, kTileThreads, TileGeom<T, T, S, R, H>::smem, c->stream>>>(
       o, rs, const_cast<double*>(bu), const_cast<double*>(bv), reinterpret_cast<R*>(L.tu),
       reinterpret_cast<R*>(L.tv), reinterpret_cast<R*>(L.ru), reinterpret_cast<R*>(L.rv), idu, idv, nu);
   c->launches++;
 }
-template <int T, bool S, class R>
-static void tile_up_r(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, int fx, int fy, const double* bu,
+template <int T, bool S, class R, int H>
+static void tile_up_h(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, int fx, int fy, const double* bu,
                       const double* bv, double* xu, double* xv, int nu) {
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
-  auto kern = o.rtu ? k_smooth_up<T, T, S, true, R> : k_smooth_up<T, T, S, false, R>;
-  kern<<<grid, kTileThreads, TileGeom<T, T, S, R>::smem, c->stream>>>(
+  auto kern = o.rtu ? k_smooth_up<T, T, S, true, R, H> : k_smooth_up<T, T, S, false, R, H>;
+  kern<<<grid, kTileThreads, TileGeom<T, T, S, R, H>::smem, c->stream>>>(
       o, make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, reinterpret_cast<const R*>(L.tu),
       reinterpret_cast<const R*>(L.tv), xu, xv, idu, idv, nu);
   c->launches++;
+}
+template <int T, bool S, class R>
+static void tile_down_r(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, const Restriction& rs,
+                        const double* bu, const double* bv, int nu) {
+  if (halo_for(nu) == kHaloOne) tile_down_h<T, S, R, kHaloOne>(c, l, o, idu, idv, rs, bu, bv, nu);
+  else tile_down_h<T, S, R, kHalo>(c, l, o, idu, idv, rs, bu, bv, nu);
+}
+template <int T, bool S, class R>
+static void tile_up_r(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, int fx, int fy, const double* bu,
+                      const double* bv, double* xu, double* xv, int nu) {
+  if (halo_for(nu) == kHaloOne) tile_up_h<T, S, R, kHaloOne>(c, l, o, idu, idv, fx, fy, bu, bv, xu, xv, nu);
+  else tile_up_h<T, S, R, kHalo>(c, l, o, idu, idv, fx, fy, bu, bv, xu, xv, nu);
 }
 static int tile_down(Ctx* c, int l, const Restriction& rs, const double* bu, const double* bv, double* xu,
                      double* xv, int nu) {
@@ -1853,7 +1870,8 @@ static int tile_up(Ctx* c, int l, int fx, int fy, const double* bu, const double
 // restriction instead of 4 per sweep and 2 more
 static int vcycle_tiled(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
                         const Restriction& rs, int nu1, int nu2) {
-  if (4 * nu1 > kHalo - 1 || 4 * nu2 > kHalo - 1) return set_error(c, DIVA_UNSUPPORTED, "tiled smoothing depth");
+  if (4 * nu1 > halo_for(nu1) - 1 || 4 * nu2 > halo_for(nu2) - 1)
+    return set_error(c, DIVA_UNSUPPORTED, "tiled smoothing depth");
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
   int st = tile_down(c, l, rs, bu, bv, xu, xv, nu1);
@@ -1919,6 +1937,17 @@ static int build_sub_tables(Ctx* c) {
 
 size_t solver_table_entries(const Ctx* c) { return sub_tab_entries(c, sub_first_fit(c)); }
 
+// dynamic shared memory of the four tile kernels (down/up, with/without front rows) of one shape
+template <int T, bool S, class R, int H>
+static int tile_attrs(Ctx* c) {
+  const void* k[4] = {(const void*)k_smooth_down<T, T, S, false, R, H>, (const void*)k_smooth_down<T, T, S, true, R, H>,
+                      (const void*)k_smooth_up<T, T, S, false, R, H>, (const void*)k_smooth_up<T, T, S, true, R, H>};
+  for (int q = 0; q < 4; ++q)
+    DIVA_CUDA(c, cudaFuncSetAttribute(k[q], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)TileGeom<T, T, S, R, H>::smem));
+  return DIVA_OK;
+}
+
 int solver_init(Ctx* c) {
   if (sub_bytes(c, c->nlev - 1) > kSubSmemBudget)
     return set_error(c, DIVA_UNSUPPORTED, "coarsest multigrid level too large for the one-block sub-cycle");
@@ -1926,32 +1955,14 @@ int solver_init(Ctx* c) {
   DIVA_CUDA(c, cudaFuncSetAttribute(k_small_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
-  const void* tile32[4] = {(const void*)k_smooth_down<32, 32, kStage32, false, double>,
-                           (const void*)k_smooth_down<32, 32, kStage32, true, double>,
-                           (const void*)k_smooth_up<32, 32, kStage32, false, double>,
-                           (const void*)k_smooth_up<32, 32, kStage32, true, double>};
-  const void* tile16[4] = {(const void*)k_smooth_down<16, 16, kStage16, false, double>,
-                           (const void*)k_smooth_down<16, 16, kStage16, true, double>,
-                           (const void*)k_smooth_up<16, 16, kStage16, false, double>,
-                           (const void*)k_smooth_up<16, 16, kStage16, true, double>};
-  const void* f32t32[4] = {(const void*)k_smooth_down<32, 32, true, false, float>,
-                           (const void*)k_smooth_down<32, 32, true, true, float>,
-                           (const void*)k_smooth_up<32, 32, true, false, float>,
-                           (const void*)k_smooth_up<32, 32, true, true, float>};
-  const void* f32t16[4] = {(const void*)k_smooth_down<16, 16, true, false, float>,
-                           (const void*)k_smooth_down<16, 16, true, true, float>,
-                           (const void*)k_smooth_up<16, 16, true, false, float>,
-                           (const void*)k_smooth_up<16, 16, true, true, float>};
-  for (int k = 0; k < 4; ++k) {
-    DIVA_CUDA(c, cudaFuncSetAttribute(tile32[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)TileGeom<32, 32, kStage32>::smem));
-    DIVA_CUDA(c, cudaFuncSetAttribute(tile16[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)TileGeom<16, 16, kStage16>::smem));
-    DIVA_CUDA(c, cudaFuncSetAttribute(f32t32[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)TileGeom<32, 32, true, float>::smem));
-    DIVA_CUDA(c, cudaFuncSetAttribute(f32t16[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)TileGeom<16, 16, true, float>::smem));
-  }
+  if (int st = tile_attrs<32, kStage32, double, kHalo>(c)) return st;
+  if (int st = tile_attrs<16, kStage16, double, kHalo>(c)) return st;
+  if (int st = tile_attrs<32, true, float, kHalo>(c)) return st;
+  if (int st = tile_attrs<16, true, float, kHalo>(c)) return st;
+  if (int st = tile_attrs<32, kStage32, double, kHaloOne>(c)) return st;
+  if (int st = tile_attrs<16, kStage16, double, kHaloOne>(c)) return st;
+  if (int st = tile_attrs<32, true, float, kHaloOne>(c)) return st;
+  if (int st = tile_attrs<16, true, float, kHaloOne>(c)) return st;
   const BCs& b = c->bc;
   const int all[8] = {b.uW, b.uE, b.uS, b.uN, b.vW, b.vE, b.vS, b.vN};
   bool periodic = false;
