@@ -749,6 +749,7 @@ def run_ensemble(args):
     prepared (untimed), then warm-up and timed batched solves run, each from the prepared
     cold state.  Solves/s of the whole ensemble: members x steps over the max over ranks of
     the per-rank sum of the groups' device-synchronised wall times."""
+    import numpy as np
     import torch
     import torch.distributed as dist
     load_package()
@@ -768,12 +769,21 @@ def run_ensemble(args):
     clocks = ClockSampler(local)
     clocks.start()
     t_total, launches, last, group_seconds = 0.0, 0, {}, []
+    fp64_err = {}
+
+    def member_cfg(cfg, accelerated=True):
+        cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
+                   lin_rtol=1e-10, picard_stall_tol=args.stall_tol)
+        if accelerated:
+            cfg.update(picard_anderson_m=args.anderson, precision=args.precision,
+                       lin_adaptive_eta=args.eta if args.eta is not None else (0.1 if args.anderson else 0.5))
+        return cfg
+
     for grp in ensemble.groups(members, parts[rank], budget):
         ctxs = []
         for k in grp:
             name, g, cfg, f = members[k]
-            cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
-                       lin_rtol=1e-10)
+            cfg = member_cfg(cfg)
             c = diva.Context(diva.Grid(**g) if isinstance(g, dict) else g, cfg)
             c.upload(f)
             c.update_general_ice_model_data()
@@ -800,6 +810,23 @@ def run_ensemble(args):
         t_total += time.perf_counter() - t0
         launches += sum(c.kernel_launches() for c in ctxs) - l0
         last.update({k: r for k, r in zip(grp, reps)})
+        if args.anderson or args.precision != "fp64":
+            # each member's error against the plain FP64 path (untimed): the same member
+            # solved again from its cold state with the reference's relaxation in FP64
+            for k, c in zip(grp, ctxs):
+                a = c.download(["u_vav_cx", "v_vav_cy"])
+                c.set_config(member_cfg(members[k][2], accelerated=False))
+                c.state_restore()
+                try:
+                    r64 = c.solve_DIVA()
+                except diva.DivaError:
+                    r64 = {"status": -1}
+                b = c.download(["u_vav_cx", "v_vav_cy"])
+                x = np.concatenate([a["u_vav_cx"].ravel(), a["v_vav_cy"].ravel()])
+                y = np.concatenate([b["u_vav_cx"].ravel(), b["v_vav_cy"].ravel()])
+                den = float(np.linalg.norm(y))
+                fp64_err[k] = (float(np.linalg.norm(x - y)) / den if den > 0 else 0.0,
+                               float(np.abs(x - y).max()), r64["status"])
         for c in ctxs:
             c.close()
     clk = clocks.stop()
@@ -811,6 +838,8 @@ def run_ensemble(args):
     cycles = [last[k]["mg_cycles"] for k in sorted(last)]
     member_ms = [round(last[k]["elapsed_ms"], 3) for k in sorted(last)]
     converged = sum(1 for k in last if last[k]["status"] == 0)
+    stalled = sum(1 for k in last if last[k].get("stalled"))
+    kinds = [members[k][0] for k in sorted(last)]
     if rank == 0:
         print(json.dumps({
             "metric": f"DIVA ensemble solves/s ({args.members} members) to rel-res 1e-6", "value":
@@ -820,16 +849,27 @@ def run_ensemble(args):
             "config": {"workload": f"{args.members}-member ensemble, sizes {'/'.join(sizes)}, beta_sq x "
                                    "U_log[0.3,3], flow factor x U_log[0.5,2]",
                        "members_per_rank": [len(p) for p in parts],
+                       "member_kinds_rank0": kinds,
                        "picard_iterations_rank0": its,
                        "mg_cycles_rank0": cycles,
-                       "member_elapsed_ms_rank0": member_ms,
+                       "member_stream_span_ms_rank0": member_ms,
                        "group_seconds_rank0": [round(x, 4) for x in group_seconds],
                        "rank0_members_converged": converged,
-                       "rank0_members_at_iteration_cap": len(last) - converged,
-                       "note": "members with low friction reach the 5000 m/yr velocity limit of the "
-                               "reference's Picard update and stall above rel-res 1e-6 until the cap",
+                       "rank0_members_stalled": stalled,
+                       "rank0_members_at_iteration_cap": len(last) - converged - stalled,
+                       "solver": (f"Anderson({args.anderson}) " if args.anderson else "relaxed Picard ") +
+                                 f"precision {args.precision}, stall tolerance {args.stall_tol:g}",
+                       "error_vs_plain_fp64_rank0": {"rel_l2": [round(fp64_err[k][0], 9) for k in sorted(fp64_err)],
+                                                     "max_abs_m_per_yr": [round(fp64_err[k][1], 6)
+                                                                          for k in sorted(fp64_err)],
+                                                     "fp64_status": [fp64_err[k][2] for k in sorted(fp64_err)]}
+                       if fp64_err else None,
+                       "note": "members with low friction reach the 5000 m/yr velocity limit of the reference's "
+                               "Picard update: the limited iteration has a fixed point above rel-res 1e-6; with a "
+                               "stall tolerance they stop there (status MAX_PICARD), without one at the cap",
                        "timing": "device-synchronised wall clock of the batched solves (members on their own "
-                                 "streams), summed over memory-bounded groups, max over ranks",
+                                 "streams), summed over memory-bounded groups, max over ranks; a member's stream "
+                                 "span is its events' span while it shares the GPU with the group's others",
                        "parallelism": f"members partitioned over {world} GPU(s), no data-path collective"},
             "clocks": clk, "gpu_launches": int(launches)}))
     if world > 1:
@@ -1022,6 +1062,9 @@ def main():
                    help="Anderson mixing depth of the viscosity iteration (0: the reference's relaxation)")
     p.add_argument("--eta", type=float, default=None,
                    help="adaptive linear tolerance factor (default 0.5, or 0.1 with --anderson)")
+    p.add_argument("--stall-tol", type=float, default=0.0,
+                   help="ensemble: stop a member whose step norm falls below this while rel-res stays above "
+                        "its tolerance (a fixed point of the velocity-limited iteration); 0 = off")
     args = p.parse_args()
     if args.impl == "b200" and args.workload == "ensemble":
         return run_ensemble(args)

@@ -57,6 +57,7 @@ enum {
   // nonlinear residual the last mixing step saw, the Gram matrix of the residual
   // differences, its right-hand side and the mixing coefficients
   SC_AA_N, SC_AA_HEAD, SC_AA_HAVE, SC_AA_RPREV, SC_AA_RESTARTS,
+  SC_STALLED,   // the rel-res iteration stopped on picard_stall_tol
   SC_AA_G, SC_AA_RHS = SC_AA_G + 25, SC_AA_GAMMA = SC_AA_RHS + 5,
   SC_COUNT = SC_AA_GAMMA + 5
 };

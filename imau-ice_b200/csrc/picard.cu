@@ -118,8 +118,8 @@ __device__ __forceinline__ double sliding_beta(const CoefArgs& a, long long q, d
   return CUDART_NAN;
 }
 
-// Block shape of the layer-parallel kernels: a warp over 32 rows, 4 grid columns.
-constexpr int kColLanes = 32, kColRows = 4;
+// Block shape of the layer-parallel kernels: a warp over 32 rows, 8 grid columns.
+constexpr int kColLanes = 32, kColRows = 8;
 
 // Per-column decisions of the layer step, packed by k_column_prep (and kept for k_shear_rates):
 //   bits 0-3   the E, W, N, S shear face carries ice (FACE_*)
@@ -215,10 +215,10 @@ __global__ void __launch_bounds__(kColLanes * kColRows) k_layer_viscosity(CoefAr
   // the layer is the fastest grid index: blocks running together share their columns'
   // 2D inputs in L1/L2 instead of streaming them once per layer
   const int k = blockIdx.x, j = blockIdx.y * kColLanes + lane, i = blockIdx.z * kColRows + threadIdx.y;
-  if (i >= d.nx) return;       // whole warps: i is uniform across a warp
-  const bool col = j < d.ny;   // lanes past the last row stay for the shuffle
+  const bool row = i < d.nx;   // whole warps: i is uniform across a warp; idle warps stay for the barrier
+  const bool col = row && j < d.ny;   // lanes past the last row stay for the shuffle
   const int nx = d.nx, ny = d.ny, ld = d.ld;
-  const int q = i * ld + (col ? j : ny - 1);   // plane index (planes hold < 2^31 points)
+  const int q = (row ? i : nx - 1) * ld + (j < ny ? j : ny - 1);   // plane index (planes hold < 2^31 points)
   const long long off = (long long)k * d.plane;
   const double* __restrict__ vp = a.visc_prev + off;
   const R zk = (R)a.zt.z[k];
@@ -226,6 +226,9 @@ __global__ void __launch_bounds__(kColLanes * kColRows) k_layer_viscosity(CoefAr
   const bool has_e = col && i < nx - 1, has_w = col && i > 0, has_n = col && j < ny - 1, has_s = col && j > 0;
   auto mode = [&](int f) { return (flags >> (kModeShift + 2 * f)) & 3; };
   auto shear = [&](double tb, double v0, double v1, int m) { return ((R)tb / stag_mode_t<R>(m, (R)v0, (R)v1)) * zk; };
+  // the west face of column i is the east face of column i-1: the warp below in the block
+  // computed it (the same operands, so the same value), the block's first warp computes it
+  __shared__ R east[kColRows][kColLanes];
   R dudz_e = R(0), dvdz_n = R(0), dvdz_s = R(0), dudz_w = R(0);
   if (a.diva) {
     const double vq = vp[q];
@@ -233,13 +236,16 @@ __global__ void __launch_bounds__(kColLanes * kColRows) k_layer_viscosity(CoefAr
       if (flags & FACE_E) dudz_e = shear(a.taub_cx[q], vq, vp[q + ld], mode(0));
       if (WRITE_SHEAR) a.dudz[off + q] = (double)dudz_e;
     }
+    east[threadIdx.y][lane] = dudz_e;
     if (has_n) {
       if (flags & FACE_N) dvdz_n = shear(a.taub_cy[q], vq, vp[q + 1], mode(2));
       if (WRITE_SHEAR) a.dvdz[off + q] = (double)dvdz_n;
     }
-    if (has_w && (flags & FACE_W)) dudz_w = shear(a.taub_cx[q - ld], vp[q - ld], vq, mode(1));
     dvdz_s = __shfl_up_sync(0xffffffffu, dvdz_n, 1);   // north face of row j-1
     if (lane == 0 && has_s) dvdz_s = (flags & FACE_S) ? shear(a.taub_cy[q - 1], vp[q - 1], vq, mode(3)) : R(0);
+    __syncthreads();
+    if (has_w && (flags & FACE_W))
+      dudz_w = threadIdx.y > 0 ? east[threadIdx.y - 1][lane] : shear(a.taub_cx[q - ld], vp[q - ld], vq, mode(1));
   }
   if (!col) return;
   R eta = R(0);
@@ -1195,7 +1201,7 @@ int launch_basal_pred(Ctx* c) {
 
 // end of a graph-launched viscosity iteration: the step norm from the summed
 // partials (calc_visc_iter_UV_resid :1588-1596) and the stop test (:346-351)
-__global__ void k_ctl_end(double* sc, int relmode, double tol, int nit) {
+__global__ void k_ctl_end(double* sc, int relmode, double tol, int nit, double stall_tol) {
   const double r1 = sc[SC_RES1], r2 = sc[SC_RES2], cnt = sc[SC_RES1 + 2];
   if (!isfinite(r1) || !isfinite(r2)) sc[SC_NAN] = 1.0;
   const double resid = (cnt > 0.0) ? 2.0 * sqrt(r1) / max_ref(sqrt(r2), 1E-8) : 0.0;
@@ -1203,6 +1209,10 @@ __global__ void k_ctl_end(double* sc, int relmode, double tol, int nit) {
   bool conv = false;
   if (!relmode && resid < tol) conv = true;
   else if (sc[SC_PIC_IT] >= (double)nit) conv = true;
+  else if (relmode && stall_tol > 0.0 && resid < stall_tol) {   // a stalled rel-res iteration
+    conv = true;
+    sc[SC_STALLED] = 1.0;
+  }
   sc[SC_CONVERGED] = conv ? 1.0 : 0.0;
 }
 
@@ -1217,7 +1227,8 @@ __global__ void k_err_commit(Dims d, const double* sc, const double* cx, const d
 }
 
 int launch_ctl_end(Ctx* c, bool relmode) {
-  k_ctl_end<<<1, 1, 0, c->stream>>>(c->scal, relmode, c->c.DIVA_visc_it_norm_dUV_tol, c->c.DIVA_visc_it_nit); c->launches++;
+  k_ctl_end<<<1, 1, 0, c->stream>>>(c->scal, relmode, c->c.DIVA_visc_it_norm_dUV_tol, c->c.DIVA_visc_it_nit,
+                                    c->c.picard_stall_tol); c->launches++;
   DIVA_LAUNCHED(c, "k_ctl_end");
   return DIVA_OK;
 }

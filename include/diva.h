@@ -184,7 +184,15 @@ typedef struct {
    * stop test is the nonlinear residual, so the converged state solves the same equations
    * as with the relaxed update; only the path there, and its length, change. */
   int32_t picard_anderson_m;
-  int32_t reserved[7];
+  /* Stop a rel-res iteration that has stalled (no reference counterpart): with
+   * picard_stop = DIVA_STOP_RELRES and picard_stall_tol > 0, an iteration whose step norm
+   * resid_UV falls below picard_stall_tol while rel-res is still above its tolerance ends
+   * the loop with DIVA_MAX_PICARD.  This is the case when the velocity limit DIVA_vel_max
+   * (apply_velocity_limits, ice_velocity_module.f90:1432-1498) is active: the limited
+   * iteration has a fixed point that does not solve the unlimited equations, and further
+   * iterations change nothing.  0 (the default) keeps iterating to DIVA_visc_it_nit. */
+  double  picard_stall_tol;
+  int32_t reserved[6];
 } diva_config_t;
 
 /* ---- per-solve report --------------------------------------------------- */

@@ -2221,6 +2221,7 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
   int exited_by_relres = 0;
   double eta = C->lin_adaptive_eta, relres_prev = 0.0;
   const int aa = relmode && C->picard_anderson_m > 0;
+  int stalled = 0;   /* a rel-res loop stopped on picard_stall_tol (the GPU library's rule) */
   if (aa) aa_reset(c);
   for (;;) {
     ++it;
@@ -2272,11 +2273,13 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
     int converged = 0;
     if (!relmode && resid < C->DIVA_visc_it_norm_dUV_tol) converged = 1;
     else if (it >= C->DIVA_visc_it_nit) converged = 1;
+    else if (relmode && C->picard_stall_tol > 0.0 && resid < C->picard_stall_tol) converged = stalled = 1;
     if (!converged) estimate_visc_iter_UV_errors(c, u, v);
     if (diva) { calc_basal_stress(c); calc_basal_velocities(c); }
     if (check_nan(c, u, ncx) || check_nan(c, v, ncy)) { status = DIVA_NAN_DETECTED; break; }
     if (converged) {
-      if (it >= C->DIVA_visc_it_nit && (relmode || resid >= C->DIVA_visc_it_norm_dUV_tol) && status == DIVA_OK)
+      if ((it >= C->DIVA_visc_it_nit || stalled) && (relmode || resid >= C->DIVA_visc_it_norm_dUV_tol) &&
+          status == DIVA_OK)
         status = DIVA_MAX_PICARD;
       break;
     }
@@ -2287,6 +2290,7 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
     rep->resid_UV = resid;
     rep->relres = relres;
     rep->status = status;
+    rep->reserved[2] = stalled;
   }
   return status;
 }
