@@ -796,7 +796,7 @@ def run_ensemble(args):
         def step():
             for c in ctxs:
                 c.state_restore()
-            return diva.solve_DIVA_batch(ctxs)
+            return diva.solve_DIVA_batch(ctxs, raise_on_error=False)
 
         for _ in range(args.warmup):
             step()
@@ -839,6 +839,7 @@ def run_ensemble(args):
     member_ms = [round(last[k]["elapsed_ms"], 3) for k in sorted(last)]
     converged = sum(1 for k in last if last[k]["status"] == 0)
     stalled = sum(1 for k in last if last[k].get("stalled"))
+    failed = {k: last[k]["status"] for k in sorted(last) if last[k]["status"] not in (0, 1)}
     kinds = [members[k][0] for k in sorted(last)]
     if rank == 0:
         print(json.dumps({
@@ -856,7 +857,8 @@ def run_ensemble(args):
                        "group_seconds_rank0": [round(x, 4) for x in group_seconds],
                        "rank0_members_converged": converged,
                        "rank0_members_stalled": stalled,
-                       "rank0_members_at_iteration_cap": len(last) - converged - stalled,
+                       "rank0_members_at_iteration_cap": len(last) - converged - stalled - len(failed),
+                       "rank0_members_failed": failed,
                        "solver": (f"Anderson({args.anderson}) " if args.anderson else "relaxed Picard ") +
                                  f"precision {args.precision}, stall tolerance {args.stall_tol:g}",
                        "error_vs_plain_fp64_rank0": {"rel_l2": [round(fp64_err[k][0], 9) for k in sorted(fp64_err)],

@@ -990,6 +990,12 @@ __global__ void k_zero_uv(Dims d, double* u, double* v) {
 
 #define G2 grid2d(c->d.ny, c->d.nx), block2d(), 0, c->stream
 
+// Whether K1 computes the viscosity of the linearisation in FP32 (precision 'mixed').
+#ifndef DIVA_K1_FP32
+#define DIVA_K1_FP32 1
+#endif
+static bool k1_fp32(const diva_config_t& C) { return DIVA_K1_FP32 && C.precision == DIVA_PREC_MIXED; }
+
 int launch_prepare_afac(Ctx* c) {
   k_afac<<<G2>>>(c->d, c->c.n_flow, c->D(DIVA_F_A_FLOW_3D_A), c->afac); c->launches++;
   DIVA_LAUNCHED(c, "k_afac");
@@ -1062,7 +1068,7 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
   {
     const dim3 block(kColLanes, kColRows);
     const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
-    const bool f32 = C.precision == DIVA_PREC_MIXED;
+    const bool f32 = k1_fp32(C);
     if (what == K1_WRITE_SHEAR) {
       if (f32) k_layer_viscosity<true, float><<<grid, block, 0, c->stream>>>(a);
       else k_layer_viscosity<true, double><<<grid, block, 0, c->stream>>>(a);
@@ -1072,7 +1078,7 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
     }
     c->launches++;
   }
-  if (C.precision == DIVA_PREC_MIXED) {
+  if (k1_fp32(C)) {
     if (c->d.nz == 15) k_column_integrals<15, float><<<G2>>>(a);
     else k_column_integrals<0, float><<<G2>>>(a);
   } else {
@@ -1245,7 +1251,7 @@ int launch_shear_rates(Ctx* c) {
   fill_coef_args(c, a, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY), true);
   const dim3 block(kColLanes, kColRows);
   const dim3 grid(c->d.nz, (c->d.ny + kColLanes - 1) / kColLanes, (c->d.nx + kColRows - 1) / kColRows);
-  if (c->c.precision == DIVA_PREC_MIXED) k_shear_rates<float><<<grid, block, 0, c->stream>>>(a);
+  if (k1_fp32(c->c)) k_shear_rates<float><<<grid, block, 0, c->stream>>>(a);
   else k_shear_rates<double><<<grid, block, 0, c->stream>>>(a);
   c->launches++;
   DIVA_LAUNCHED(c, "k_shear_rates");

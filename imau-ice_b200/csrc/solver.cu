@@ -1973,21 +1973,23 @@ int solver_init(Ctx* c) {
 
 // One V-cycle from level l down, entered with x = 0.  b is given in bu/bv, or (rs.on)
 // restricted from the finer level's residual by the level's first kernel.
-// Gauss-Seidel sweeps before and after the coarse correction: on the finest level, and on
-// every coarser level (the tiled levels and the one-block sub-cycle).  Measured on the
-// 321 x 561 ice cap (one B200, solves to rel-res 1e-6): V(2,2) on the finest level with
-// V(1,1) below it keeps the V-cycle count of V(2,2) everywhere (79 with the relaxed update,
-// 43 with Anderson mixing) at 8-13 % less time per solve; V(1,1) everywhere needs 2-3 x the
-// cycles.
-#ifndef DIVA_MG_NU_FINE
-#define DIVA_MG_NU_FINE 2
+// Gauss-Seidel sweeps before and after the coarse correction.  The finest level and every
+// coarser level of at least DIVA_MG_NU2_POINTS points take two (V(2,2)); smaller levels,
+// whose kernels are bound by the latency of their barrier-separated colour passes rather
+// than by their points, take one (V(1,1)), and so does the one-block sub-cycle.  Measured
+// on one B200, solves to rel-res 1e-6: on the 321 x 561 ice cap one sweep below the finest
+// level keeps the V-cycle count of V(2,2) everywhere (79 relaxed, 43 with Anderson mixing)
+// at 8-13 % less time per solve; on the 1501 x 1501 sheet one sweep on its large coarse
+// levels (751 x 751, 376 x 376) doubled the V-cycles per viscosity iteration.
+#ifndef DIVA_MG_NU2_POINTS
+#define DIVA_MG_NU2_POINTS 100000
 #endif
-#ifndef DIVA_MG_NU_COARSE
-#define DIVA_MG_NU_COARSE 1
-#endif
+static int level_nu(const Ctx* c, int l) {
+  return (l == 0 || (long long)c->lv[l].d.nx * c->lv[l].d.ny >= DIVA_MG_NU2_POINTS) ? 2 : 1;
+}
 static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const double* bv,
                   const Restriction& rs) {
-  const int nu1 = l == 0 ? DIVA_MG_NU_FINE : DIVA_MG_NU_COARSE, nu2 = nu1, coarse_sweeps = 64;
+  const int nu1 = level_nu(c, l), nu2 = nu1, coarse_sweeps = 64;
   if (l == sub_first_level(c)) {
     SubCycle sc;
     sc.first = l;

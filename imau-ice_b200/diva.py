@@ -418,11 +418,12 @@ def solve_SSA(grid, ice, config=None, backend=None):
     return _run(grid, ice, config, backend, "solve_SSA", OUT_SSA)
 
 
-def solve_DIVA_batch(contexts):
+def solve_DIVA_batch(contexts, raise_on_error=True):
     """solve_DIVA for several contexts at once (diva_solve_diva_batch): each on its own
     stream, every member's graph-launched viscosity loop in flight at once, so small
     members share the GPU.  Returns the reports in order; raises DivaError naming the
-    first member whose status is neither OK nor MAX_PICARD."""
+    first member whose status is neither OK nor MAX_PICARD, unless raise_on_error is
+    False (then each report's status says how its member ended)."""
     if not contexts:
         return []
     be = contexts[0].backend
@@ -442,7 +443,7 @@ def solve_DIVA_batch(contexts):
         err = be.fns["last_error"](contexts[0].h)   # rejected before any member ran
         raise DivaError(st, f"solve_DIVA_batch: {err.decode() if err else ''}")
     for k, (c, r) in enumerate(zip(contexts, out)):
-        if r["status"] not in (0, _abi.MAX_PICARD):
+        if raise_on_error and r["status"] not in (0, _abi.MAX_PICARD):
             err = be.fns["last_error"](c.h)
             raise DivaError(r["status"], f"solve_DIVA_batch member {k}: {err.decode() if err else ''}")
     return out
