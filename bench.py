@@ -773,7 +773,7 @@ def run_ensemble(args):
 
     def member_cfg(cfg, accelerated=True):
         cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
-                   lin_rtol=1e-10, picard_stall_tol=args.stall_tol)
+                   lin_rtol=1e-10, picard_stall_its=args.stall_its)
         if accelerated:
             cfg.update(picard_anderson_m=args.anderson, precision=args.precision,
                        lin_adaptive_eta=args.eta if args.eta is not None else (0.1 if args.anderson else 0.5))
@@ -860,15 +860,16 @@ def run_ensemble(args):
                        "rank0_members_at_iteration_cap": len(last) - converged - stalled - len(failed),
                        "rank0_members_failed": failed,
                        "solver": (f"Anderson({args.anderson}) " if args.anderson else "relaxed Picard ") +
-                                 f"precision {args.precision}, stall tolerance {args.stall_tol:g}",
+                                 f"precision {args.precision}, stall window {args.stall_its} iterations",
                        "error_vs_plain_fp64_rank0": {"rel_l2": [round(fp64_err[k][0], 9) for k in sorted(fp64_err)],
                                                      "max_abs_m_per_yr": [round(fp64_err[k][1], 6)
                                                                           for k in sorted(fp64_err)],
                                                      "fp64_status": [fp64_err[k][2] for k in sorted(fp64_err)]}
                        if fp64_err else None,
                        "note": "members with low friction reach the 5000 m/yr velocity limit of the reference's "
-                               "Picard update: the limited iteration has a fixed point above rel-res 1e-6; with a "
-                               "stall tolerance they stop there (status MAX_PICARD), without one at the cap",
+                               "Picard update: the limited iteration settles on or cycles around states above "
+                               "rel-res 1e-6; with a stall window they stop once rel-res has not fallen by 10 % "
+                               "for that many iterations (status MAX_PICARD), without one at the cap",
                        "timing": "device-synchronised wall clock of the batched solves (members on their own "
                                  "streams), summed over memory-bounded groups, max over ranks; a member's stream "
                                  "span is its events' span while it shares the GPU with the group's others",
@@ -1064,9 +1065,9 @@ def main():
                    help="Anderson mixing depth of the viscosity iteration (0: the reference's relaxation)")
     p.add_argument("--eta", type=float, default=None,
                    help="adaptive linear tolerance factor (default 0.5, or 0.1 with --anderson)")
-    p.add_argument("--stall-tol", type=float, default=0.0,
-                   help="ensemble: stop a member whose step norm falls below this while rel-res stays above "
-                        "its tolerance (a fixed point of the velocity-limited iteration); 0 = off")
+    p.add_argument("--stall-its", type=int, default=0,
+                   help="ensemble: stop a member whose rel-res has not fallen by 10 %% for this many viscosity "
+                        "iterations (a velocity-limited member that cannot reach the tolerance); 0 = off")
     args = p.parse_args()
     if args.impl == "b200" and args.workload == "ensemble":
         return run_ensemble(args)

@@ -96,8 +96,8 @@ class Config(C.Structure):
         ("remove_shelves_larger_than_PD", C.c_int32), ("continental_shelf_calving", C.c_int32),
         ("continental_shelf_min_height", C.c_double),
         ("picard_anderson_m", C.c_int32),
-        ("picard_stall_tol", C.c_double),
-        ("reserved", C.c_int32 * 6),
+        ("picard_stall_its", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -112,7 +112,7 @@ class Report(C.Structure):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
         d["linear_not_converged"] = self.reserved[0]   # linear solves that missed their tolerance
         d["graph_launched"] = self.reserved[1]         # 1 if the iterations ran as CUDA graphs
-        d["stalled"] = self.reserved[2]                # 1 if a rel-res loop stopped on picard_stall_tol
+        d["stalled"] = self.reserved[2]                # 1 if a rel-res loop stopped on picard_stall_its
         return d
 
 

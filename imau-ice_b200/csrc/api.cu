@@ -137,7 +137,7 @@ int validate_config(Ctx* c, const diva_config_t* cfg) {
     return set_error(c, DIVA_BAD_INPUT, "picard_anderson_m must lie in 0..5");
   if (cfg->picard_anderson_m > 0 && cfg->picard_stop != DIVA_STOP_RELRES)
     return set_error(c, DIVA_BAD_INPUT, "picard_anderson_m > 0 needs picard_stop = DIVA_STOP_RELRES");
-  if (!(cfg->picard_stall_tol >= 0.0)) return set_error(c, DIVA_BAD_INPUT, "picard_stall_tol must be >= 0");
+  if (cfg->picard_stall_its < 0) return set_error(c, DIVA_BAD_INPUT, "picard_stall_its must be >= 0");
   const int bcs[8] = {cfg->BC_u_west, cfg->BC_u_east, cfg->BC_u_south, cfg->BC_u_north,
                       cfg->BC_v_west, cfg->BC_v_east, cfg->BC_v_south, cfg->BC_v_north};
   for (int b : bcs)
@@ -320,10 +320,10 @@ int graph_loop_end(Ctx* c, const GraphLoop& L, diva_report_t* rep) {
   const diva_config_t& C = c->c;
   const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
   int status = DIVA_OK;
-  // a rel-res loop that ended on anything but its tolerance (the iteration cap, or a stall
-  // on picard_stall_tol) has not converged; the step-norm loop only at the cap
-  if (!L.by_relres && (relmode || (L.it >= C.DIVA_visc_it_nit && L.resid >= C.DIVA_visc_it_norm_dUV_tol)))
+  const bool stalled = c->h_scal[SC_STALLED] != 0.0;
+  if (!L.by_relres && L.it >= C.DIVA_visc_it_nit && (relmode || L.resid >= C.DIVA_visc_it_norm_dUV_tol))
     status = DIVA_MAX_PICARD;
+  if (stalled) status = DIVA_MAX_PICARD;   // stopped on picard_stall_its short of the tolerance
   if (rep) {
     rep->picard_iterations = L.it;
     rep->resid_UV = L.resid;
@@ -331,7 +331,7 @@ int graph_loop_end(Ctx* c, const GraphLoop& L, diva_report_t* rep) {
     rep->status = status;
     rep->reserved[0] = (int32_t)c->h_scal[SC_LIN_FAILED];
     rep->reserved[1] = 1;   // graph-launched
-    rep->reserved[2] = c->h_scal[SC_STALLED] != 0.0 ? 1 : 0;
+    rep->reserved[2] = stalled ? 1 : 0;
   }
   return status;
 }
@@ -356,6 +356,7 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
   const bool relmode = C.picard_stop == DIVA_STOP_RELRES;
   int it = 0, st = DIVA_OK, lin_fail = 0;
   bool stalled_exit = false;
+  double stall_best = 0.0, stall_since = 0.0;
   double resid = 0.0, relres = -1.0, eta = C.lin_adaptive_eta, relres_prev = 0.0;
   if (C.picard_anderson_m > 0) {
     double init[SC_COUNT - SC_AA_N] = {};
@@ -371,7 +372,10 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
       eta = eta_after(eta, relres, relres_prev, C.picard_relres_tol);   // as the graph's k_ctl_relres does
       relres_prev = relres;
       if (!std::isfinite(relres)) return set_error(c, DIVA_NAN_DETECTED, "NaN in the nonlinear residual");
-      if (relres <= C.picard_relres_tol) {
+      const bool stop_stall = relres > C.picard_relres_tol &&
+                              stall_after(relres, &stall_best, &stall_since, C.picard_stall_its);
+      if (relres <= C.picard_relres_tol || stop_stall) {
+        stalled_exit = stop_stall;
         if (diva && (st = launch_basal_stress_velocities(c))) return st;
         break;
       }
@@ -397,21 +401,18 @@ int picard(Ctx* c, bool diva, double* u, double* v, diva_report_t* rep) {
     const double r1 = c->h_scal[SC_RES1], r2 = c->h_scal[SC_RES2], cnt = c->h_scal[SC_RES1 + 2];
     if (!std::isfinite(r1) || !std::isfinite(r2)) return set_error(c, DIVA_NAN_DETECTED, "NaN in the velocities");
     resid = (cnt > 0.0) ? 2.0 * sqrt(r1) / std::max(sqrt(r2), 1E-8) : 0.0;
-    bool converged = false, stalled = false;
+    bool converged = false;
     if (!relmode && resid < C.DIVA_visc_it_norm_dUV_tol) converged = true;
     else if (it >= C.DIVA_visc_it_nit) converged = true;
-    else if (relmode && C.picard_stall_tol > 0.0 && resid < C.picard_stall_tol) converged = stalled = true;
     if (!converged) launch_commit_err(c);
-    if (converged) {
-      stalled_exit = stalled;
-      break;
-    }
+    if (converged) break;
   }
   int status = DIVA_OK;
   if ((it >= C.DIVA_visc_it_nit || stalled_exit) &&
       ((relmode && !(relres >= 0.0 && relres <= C.picard_relres_tol)) ||
        (!relmode && resid >= C.DIVA_visc_it_norm_dUV_tol)))
     status = DIVA_MAX_PICARD;
+  if (stalled_exit) status = DIVA_MAX_PICARD;
   if (rep) {
     rep->picard_iterations = it;
     rep->resid_UV = resid;

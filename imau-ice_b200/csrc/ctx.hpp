@@ -57,13 +57,15 @@ enum {
   // nonlinear residual the last mixing step saw, the Gram matrix of the residual
   // differences, its right-hand side and the mixing coefficients
   SC_AA_N, SC_AA_HEAD, SC_AA_HAVE, SC_AA_RPREV, SC_AA_RESTARTS,
-  SC_STALLED,   // the rel-res iteration stopped on picard_stall_tol
+  SC_STALLED, SC_STALL_BEST, SC_STALL_SINCE,   // stagnation stop: flag, lowest rel-res, iterations since
+  SC_AA_OFF, SC_AA_BEST, SC_AA_SINCE,   // mixing given up; best rel-res so far; steps since it improved
   SC_AA_G, SC_AA_RHS = SC_AA_G + 25, SC_AA_GAMMA = SC_AA_RHS + 5,
   SC_COUNT = SC_AA_GAMMA + 5
 };
 constexpr int kAAMax = 5;             // largest Anderson depth
 constexpr int kAAPartials = 2 * kAAMax;   // block partials of one mixing step
 constexpr double kAAGammaMax = 20.0;      // largest sum of |gamma_i| a mixing step accepts
+constexpr int kAAPatience = 20;           // steps without a 10 % better rel-res before mixing is given up
 
 // One Anderson mixing step's coefficients from the inner products of the newest residual
 // difference dF_s with every history column (dots[0..m)) and of the residual f with them
@@ -82,6 +84,18 @@ __host__ __device__ inline void aa_coefficients(double* sc, int m, const double*
   const double relres = sc[SC_RELRES], rprev = sc[SC_AA_RPREV];
   for (int k = 0; k < kAAMax; ++k) gam[k] = 0.0;
   sc[SC_AA_RPREV] = relres;
+  // Mixing that has not lowered rel-res by 10 % in kAAPatience steps is given up for the
+  // rest of the solve and the reference's relaxation takes over (launch_picard_update reads
+  // SC_AA_OFF): where the velocity limit is active the limited map is not smooth, the mixed
+  // iteration wanders, while the relaxed one settles on the limited fixed point.
+  if (sc[SC_AA_OFF] != 0.0) return;
+  if (sc[SC_AA_BEST] == 0.0 || relres < 0.9 * sc[SC_AA_BEST]) {
+    sc[SC_AA_BEST] = relres;
+    sc[SC_AA_SINCE] = 0.0;
+  } else if ((sc[SC_AA_SINCE] += 1.0) >= (double)kAAPatience) {
+    sc[SC_AA_OFF] = 1.0;
+    return;
+  }
   if (sc[SC_AA_HAVE] == 0.0) {
     sc[SC_AA_HAVE] = 1.0;
     sc[SC_AA_N] = 0.0;
@@ -297,6 +311,18 @@ int solver_setup(Ctx* c, int inv_when = 0);
 // Its one-block Gauss-Jordan elimination costs as much as a fifth of an iteration's V-cycle,
 // while the coarsest grid's coefficients change slowly once the iteration has settled.
 __host__ __device__ inline bool coarse_inverse_due(int it) { return it <= 3 || (it - 1) % 4 == 0; }
+// The stagnation stop of a rel-res loop (picard_stall_its): track the lowest rel-res and the
+// iterations since it last fell by 10 %; true once that count reaches stall_its.
+__host__ __device__ inline bool stall_after(double relres, double* best, double* since, int stall_its) {
+  if (stall_its <= 0) return false;
+  if (*best == 0.0 || relres < 0.9 * *best) {
+    *best = relres;
+    *since = 0.0;
+    return false;
+  }
+  *since += 1.0;
+  return *since >= (double)stall_its;
+}
 int solver_solve(Ctx* c, const double* u0, const double* v0, double rtol, int maxit, int* iters, double* relres0);
 int solver_relres(Ctx* c, const double* u, const double* v, double* relres);
 int solver_fill_boundary(Ctx* c, double* u, double* v);

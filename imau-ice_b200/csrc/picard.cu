@@ -593,7 +593,9 @@ __global__ void __launch_bounds__(256) k_picard_update(UpdArgs a) {
     if (i < nx - 1) {
       const double uo = a.u[q];
       double un;
-      if (a.aa_m > 0) {
+      if (a.aa_m > 0 && a.sc[SC_AA_OFF] != 0.0) {
+        un = a.rel * a.gu[q] + (1.0 - a.rel) * uo;   // mixing given up: the relaxation of g
+      } else if (a.aa_m > 0) {
         un = a.gu[q];
         for (int k = 0; k < a.aa_m; ++k) un -= a.sc[SC_AA_GAMMA + k] * a.dGu[k][q];
       } else {
@@ -623,7 +625,9 @@ __global__ void __launch_bounds__(256) k_picard_update(UpdArgs a) {
     if (j < ny - 1) {
       const double vo = a.v[q];
       double vn;
-      if (a.aa_m > 0) {
+      if (a.aa_m > 0 && a.sc[SC_AA_OFF] != 0.0) {
+        vn = a.rel * a.gv[q] + (1.0 - a.rel) * vo;
+      } else if (a.aa_m > 0) {
         vn = a.gv[q];
         for (int k = 0; k < a.aa_m; ++k) vn -= a.sc[SC_AA_GAMMA + k] * a.dGv[k][q];
       } else {
@@ -1207,7 +1211,7 @@ int launch_basal_pred(Ctx* c) {
 
 // end of a graph-launched viscosity iteration: the step norm from the summed
 // partials (calc_visc_iter_UV_resid :1588-1596) and the stop test (:346-351)
-__global__ void k_ctl_end(double* sc, int relmode, double tol, int nit, double stall_tol) {
+__global__ void k_ctl_end(double* sc, int relmode, double tol, int nit) {
   const double r1 = sc[SC_RES1], r2 = sc[SC_RES2], cnt = sc[SC_RES1 + 2];
   if (!isfinite(r1) || !isfinite(r2)) sc[SC_NAN] = 1.0;
   const double resid = (cnt > 0.0) ? 2.0 * sqrt(r1) / max_ref(sqrt(r2), 1E-8) : 0.0;
@@ -1215,10 +1219,6 @@ __global__ void k_ctl_end(double* sc, int relmode, double tol, int nit, double s
   bool conv = false;
   if (!relmode && resid < tol) conv = true;
   else if (sc[SC_PIC_IT] >= (double)nit) conv = true;
-  else if (relmode && stall_tol > 0.0 && resid < stall_tol) {   // a stalled rel-res iteration
-    conv = true;
-    sc[SC_STALLED] = 1.0;
-  }
   sc[SC_CONVERGED] = conv ? 1.0 : 0.0;
 }
 
@@ -1233,8 +1233,7 @@ __global__ void k_err_commit(Dims d, const double* sc, const double* cx, const d
 }
 
 int launch_ctl_end(Ctx* c, bool relmode) {
-  k_ctl_end<<<1, 1, 0, c->stream>>>(c->scal, relmode, c->c.DIVA_visc_it_norm_dUV_tol, c->c.DIVA_visc_it_nit,
-                                    c->c.picard_stall_tol); c->launches++;
+  k_ctl_end<<<1, 1, 0, c->stream>>>(c->scal, relmode, c->c.DIVA_visc_it_norm_dUV_tol, c->c.DIVA_visc_it_nit); c->launches++;
   DIVA_LAUNCHED(c, "k_ctl_end");
   return DIVA_OK;
 }

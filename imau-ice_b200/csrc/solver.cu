@@ -1500,7 +1500,7 @@ __global__ void k_ctl_begin(double* sc) {
 
 // nonlinear residual of the current iterate; skip the solve when it meets the tolerance
 __global__ void k_ctl_relres(const double* partials, int nblocks, double* sc, cudaGraphConditionalHandle h_solve,
-                             double tol) {
+                             double tol, int stall_its) {
   double v[kPW];
   sum_partials4(partials, nblocks, v);
   if (threadIdx.x != 0) return;
@@ -1512,6 +1512,11 @@ __global__ void k_ctl_relres(const double* partials, int nblocks, double* sc, cu
   bool stop = false;
   if (!isfinite(relres)) { sc[SC_NAN] = 1.0; stop = true; }
   else if (relres <= tol) { sc[SC_EXIT_RELRES] = 1.0; stop = true; }
+  else if (stall_after(relres, sc + SC_STALL_BEST, sc + SC_STALL_SINCE, stall_its)) {
+    sc[SC_EXIT_RELRES] = 1.0;   // ends like a converged one (basal stress at this state), flagged
+    sc[SC_STALLED] = 1.0;
+    stop = true;
+  }
   cudaGraphSetConditional(h_solve, stop ? 0u : 1u);
 }
 
@@ -2343,7 +2348,8 @@ int capture_iteration(Ctx* c, CaptureCtx& cc, cudaStream_t top, bool diva, Picar
   if ((st = solver_setup(c, 1))) return st;
   if (relmode) {
     k_relres<<<g2, block2d(), 0, c->stream>>>(o, u, v, U_(KV_B), V_(KV_B), c->partials, g2.x); c->launches++;
-    k_ctl_relres<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, h_solve, C.picard_relres_tol); c->launches++;
+    k_ctl_relres<<<1, 256, 0, c->stream>>>(c->partials, nb, c->scal, h_solve, C.picard_relres_tol,
+                                           C.picard_stall_its); c->launches++;
     c->fine_passes += 1.0;
   }
   DIVA_LAUNCHED(c, "graph pre");

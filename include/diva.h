@@ -179,20 +179,23 @@ typedef struct {
    * linear solution): u <- g - sum_i gamma_i (g_i+1 - g_i), with gamma minimising
    * || f - sum_i gamma_i (f_i+1 - f_i) ||_2 over the last m residuals f = g(u) - u
    * (velocities on the cx and cy points); safeguards: columns are dropped while the
- * coefficients' magnitudes sum to more than 20, and all but the newest when the
- * nonlinear residual grows tenfold.  Needs picard_stop = DIVA_STOP_RELRES: the
+ * coefficients' magnitudes sum to more than 20, all but the newest when the nonlinear
+ * residual grows tenfold, and mixing that has not lowered the nonlinear residual by 10 %
+ * in 20 steps hands over to the relaxation for the rest of the solve (where the
+ * velocity limit is active the mixed iteration wanders, the relaxed one settles).
+ * Needs picard_stop = DIVA_STOP_RELRES: the
    * stop test is the nonlinear residual, so the converged state solves the same equations
    * as with the relaxed update; only the path there, and its length, change. */
   int32_t picard_anderson_m;
-  /* Stop a rel-res iteration that has stalled (no reference counterpart): with
-   * picard_stop = DIVA_STOP_RELRES and picard_stall_tol > 0, an iteration whose step norm
-   * resid_UV falls below picard_stall_tol while rel-res is still above its tolerance ends
-   * the loop with DIVA_MAX_PICARD.  This is the case when the velocity limit DIVA_vel_max
-   * (apply_velocity_limits, ice_velocity_module.f90:1432-1498) is active: the limited
-   * iteration has a fixed point that does not solve the unlimited equations, and further
-   * iterations change nothing.  0 (the default) keeps iterating to DIVA_visc_it_nit. */
-  double  picard_stall_tol;
-  int32_t reserved[6];
+  /* Stop a rel-res iteration that has stopped making progress (no reference counterpart):
+   * with picard_stop = DIVA_STOP_RELRES and picard_stall_its = K > 0, the loop ends with
+   * DIVA_MAX_PICARD once the nonlinear residual has not fallen below 0.9 x its lowest value
+   * so far for K viscosity iterations in a row.  This is the case where the velocity limit
+   * DIVA_vel_max (apply_velocity_limits, ice_velocity_module.f90:1432-1498) is active: the
+   * limited iteration settles on, or cycles around, states that do not solve the unlimited
+   * equations.  0 (the default) keeps iterating to DIVA_visc_it_nit. */
+  int32_t picard_stall_its;
+  int32_t reserved[7];
 } diva_config_t;
 
 /* ---- per-solve report --------------------------------------------------- */

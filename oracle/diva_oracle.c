@@ -91,8 +91,8 @@ typedef struct orc_ctx {
    * residual differences dF and map differences dG (u on cx points then v on cy points),
    * the previous residual f and map value g, and the small least-squares state */
   double *aa_dF[5], *aa_dG[5], *aa_f, *aa_g;
-  int aa_have, aa_n, aa_head, aa_restarts;
-  double aa_G[25], aa_rhs[5], aa_gamma[5], aa_rprev;
+  int aa_have, aa_n, aa_head, aa_restarts, aa_off, aa_since;
+  double aa_G[25], aa_rhs[5], aa_gamma[5], aa_rprev, aa_best;
   char err[512];
 } orc_ctx;
 
@@ -2088,6 +2088,7 @@ static void aa_reset(orc_ctx* c) {
   if (!c->aa_f) c->aa_f = (double*)malloc(sizeof(double) * n);
   if (!c->aa_g) c->aa_g = (double*)malloc(sizeof(double) * n);
   c->aa_have = 0; c->aa_n = 0; c->aa_head = 0; c->aa_restarts = 0; c->aa_rprev = 0.0;
+  c->aa_off = 0; c->aa_since = 0; c->aa_best = 0.0;
   memset(c->aa_G, 0, sizeof(c->aa_G));
 }
 
@@ -2097,6 +2098,10 @@ static void aa_coefficients(orc_ctx* c, int m, const double* dots, double relres
   for (int k = 0; k < AA_MAX; ++k) c->aa_gamma[k] = 0.0;
   const double rprev = c->aa_rprev;
   c->aa_rprev = relres;
+  /* mixing that has not lowered rel-res by 10 % in 20 steps is given up: relaxation */
+  if (c->aa_off) return;
+  if (c->aa_best == 0.0 || relres < 0.9 * c->aa_best) { c->aa_best = relres; c->aa_since = 0; }
+  else if (++c->aa_since >= 20) { c->aa_off = 1; return; }
   if (!c->aa_have) { c->aa_have = 1; c->aa_n = 0; c->aa_head = 0; return; }
   const int s = c->aa_head;
   int n = c->aa_n;
@@ -2192,6 +2197,15 @@ static void anderson_mix(orc_ctx* c, double* u, double* v, double relres) {
       }
     }
   aa_coefficients(c, m, dots, relres);
+  if (c->aa_off) {   /* mixing given up: the relaxation of the map value */
+    const double rel = c->c.DIVA_visc_it_relax;
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) {
+        if (i < nx - 1) u[ICX(j, i)] = rel * c->aa_g[ICX(j, i)] + (1.0 - rel) * up[ICX(j, i)];
+        if (j < ny - 1) v[ICY(j, i)] = rel * c->aa_g[ncx + ICY(j, i)] + (1.0 - rel) * vp[ICY(j, i)];
+      }
+    return;
+  }
   for (int i = 0; i < nx; ++i)
     for (int j = 0; j < ny; ++j) {
       if (i < nx - 1) {
@@ -2221,7 +2235,9 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
   int exited_by_relres = 0;
   double eta = C->lin_adaptive_eta, relres_prev = 0.0;
   const int aa = relmode && C->picard_anderson_m > 0;
-  int stalled = 0;   /* a rel-res loop stopped on picard_stall_tol (the GPU library's rule) */
+  int stalled = 0;   /* a rel-res loop stopped on picard_stall_its (the GPU library's rule) */
+  double stall_best = 0.0;
+  int stall_since = 0;
   if (aa) aa_reset(c);
   for (;;) {
     ++it;
@@ -2251,6 +2267,11 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
         eta = fmax(0.05, 0.5 * eta);
       relres_prev = relres;
       if (relres <= C->picard_relres_tol) { exited_by_relres = 1; }
+      else if (C->picard_stall_its > 0) {
+        /* stagnation: rel-res not below 0.9 x its lowest for picard_stall_its iterations */
+        if (stall_best == 0.0 || relres < 0.9 * stall_best) { stall_best = relres; stall_since = 0; }
+        else if (++stall_since >= C->picard_stall_its) { exited_by_relres = 1; stalled = 1; }
+      }
     }
     if (exited_by_relres) {
       if (diva) { calc_basal_stress(c); calc_basal_velocities(c); }
@@ -2273,17 +2294,17 @@ static int picard(orc_ctx* c, int diva, double* u, double* v, diva_report_t* rep
     int converged = 0;
     if (!relmode && resid < C->DIVA_visc_it_norm_dUV_tol) converged = 1;
     else if (it >= C->DIVA_visc_it_nit) converged = 1;
-    else if (relmode && C->picard_stall_tol > 0.0 && resid < C->picard_stall_tol) converged = stalled = 1;
+
     if (!converged) estimate_visc_iter_UV_errors(c, u, v);
     if (diva) { calc_basal_stress(c); calc_basal_velocities(c); }
     if (check_nan(c, u, ncx) || check_nan(c, v, ncy)) { status = DIVA_NAN_DETECTED; break; }
     if (converged) {
-      if ((it >= C->DIVA_visc_it_nit || stalled) && (relmode || resid >= C->DIVA_visc_it_norm_dUV_tol) &&
-          status == DIVA_OK)
+      if (it >= C->DIVA_visc_it_nit && (relmode || resid >= C->DIVA_visc_it_norm_dUV_tol) && status == DIVA_OK)
         status = DIVA_MAX_PICARD;
       break;
     }
   }
+  if (stalled && status == DIVA_OK) status = DIVA_MAX_PICARD;
   if (rep) {
     rep->picard_iterations = it;
     rep->linear_iterations = (int32_t)(c->lin_iters_total - lin0);

@@ -60,12 +60,12 @@ CASES = {
                                               "DIVA_visc_it_nit": 300, "lin_rtol": 1e-12,
                                               "picard_anderson_m": 3}),
     # the 20 km cap's fastest ice runs into the 5000 m/yr velocity limit: the limited
-    # iteration settles at rel-res 7e-3 and stops on picard_stall_tol (status MAX_PICARD)
+    # iteration settles at rel-res 7e-3 and stops on picard_stall_its (status MAX_PICARD)
     "icecap_20km_stall_relres": (2, 20e3, {"picard_stop": "relres", "picard_relres_tol": 1e-6,
-                                           "DIVA_visc_it_nit": 300, "lin_rtol": 1e-12, "picard_stall_tol": 1e-9}),
+                                           "DIVA_visc_it_nit": 300, "lin_rtol": 1e-12, "picard_stall_its": 30}),
     "icecap_20km_stall_anderson_relres": (2, 20e3, {"picard_stop": "relres", "picard_relres_tol": 1e-6,
                                                     "DIVA_visc_it_nit": 300, "lin_rtol": 1e-12,
-                                                    "picard_stall_tol": 1e-9, "picard_anderson_m": 3}),
+                                                    "picard_stall_its": 30, "picard_anderson_m": 3}),
 }
 # the sliding laws beside Weertman (basal_conditions_and_sliding_module.f90:1083 regularised
 # Coulomb, :1131 Tsai 2015, :1182-1183 Schoof 2005, :1223 Zoet-Iverson), with seeded till
