@@ -774,6 +774,141 @@ int diva_solve_diva_batch(diva_ctx_t** hs, int32_t n, diva_report_t* reports) {
   return DIVA_OK;
 }
 
+// ---- persistent batches: every member's viscosity loop in one graph launch ----------
+}  // extern "C"
+
+struct diva_batch {
+  std::vector<diva_ctx_t*> members;
+  std::vector<void*> bufs;            // the viscosity buffer each member's captured loop starts from
+  std::vector<diva_config_t> cfgs;    // the configurations the loops were captured with
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t stream = nullptr;      // the batch graph's launch stream
+  cudaEvent_t done = nullptr;
+  std::vector<cudaEvent_t> ready;     // one per member: its prelude has been enqueued
+};
+
+namespace {
+void batch_free(diva_batch* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (cudaEvent_t e : b->ready)
+    if (e) cudaEventDestroy(e);
+  if (b->done) cudaEventDestroy(b->done);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+}  // namespace
+
+extern "C" {
+
+int diva_batch_create(diva_ctx_t** hs, int32_t n, diva_batch_t** out) {
+  if (!hs || n < 1 || !out) return DIVA_BAD_INPUT;
+  *out = nullptr;
+  for (int k = 0; k < n; ++k) {
+    if (!hs[k]) return DIVA_BAD_INPUT;
+    for (int m = 0; m < k; ++m)
+      if (hs[m] == hs[k]) return set_error(&hs[0]->c, DIVA_BAD_INPUT, "a context appears twice in the batch");
+    if (hs[k]->c.c.choice_ice_dynamics != DIVA_DYN_DIVA)
+      return set_error(&hs[k]->c, DIVA_BAD_INPUT, "batch members must have choice_ice_dynamics DIVA");
+  }
+  std::vector<Ctx*> cs(n);
+  for (int k = 0; k < n; ++k) {
+    cs[k] = &hs[k]->c;
+    if (cs[k]->graphs_disabled) return set_error(cs[k], DIVA_UNSUPPORTED, "member without graph-launched loops");
+    if (int st = solver_build_picard_graphs(cs[k], true)) return st;
+  }
+  diva_batch* b = new diva_batch;
+  b->members.assign(hs, hs + n);
+  b->bufs.resize(n);
+  b->ready.resize(n, nullptr);
+  for (int k = 0; k < n; ++k) b->cfgs.push_back(cs[k]->c);
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+  for (int k = 0; k < n && ok; ++k) ok = cudaEventCreateWithFlags(&b->ready[k], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    batch_free(b);
+    return set_error(cs[0], DIVA_CUDA_ERROR, "batch stream or events");
+  }
+  if (int st = solver_build_batch_graph(cs.data(), n, &b->exec, b->bufs.data())) {
+    batch_free(b);
+    return st;
+  }
+  *out = b;
+  return DIVA_OK;
+}
+
+int diva_batch_destroy(diva_batch_t* b) {
+  batch_free(b);
+  return DIVA_OK;
+}
+
+int diva_batch_solve_diva(diva_batch_t* b, diva_report_t* reports) {
+  if (!b || !reports) return DIVA_BAD_INPUT;
+  const int n = (int)b->members.size();
+  std::vector<GraphLoop> loops(n);
+  std::vector<int> status(n, DIVA_OK), any(n, 1);
+  // preludes on the members' streams (each as solve_DIVA's before its loop)
+  for (int k = 0; k < n; ++k) {
+    Ctx* c = &b->members[k]->c;
+    diva_report_t* rep = &reports[k];
+    memset(rep, 0, sizeof(*rep));
+    rep->relres = -1.0;
+    if (memcmp(&c->c, &b->cfgs[k], sizeof(diva_config_t)) != 0 || !c->graphs[1].valid)
+      return set_error(c, DIVA_BAD_INPUT, "batch member reconfigured since diva_batch_create");
+    int st;
+    if ((st = begin(c)) || (st = launch_any_sheet(c, &any[k]))) return st;
+    if (any[k] && (st = prepare_velocity_solve(c))) return st;
+    loops[k].diva = true;
+    if ((st = graph_loop_begin(c, loops[k]))) return st;
+    // the captured loop reads the viscosity from the buffer it was captured with
+    if (c->f[DIVA_F_VISC_EFF_3D_A] != b->bufs[k]) {
+      DIVA_CUDA(c, cudaMemcpyAsync(b->bufs[k], c->f[DIVA_F_VISC_EFF_3D_A], sizeof(double) * c->d.nz * c->d.plane,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+      c->visc_prev = static_cast<double*>(c->f[DIVA_F_VISC_EFF_3D_A]);
+      c->f[DIVA_F_VISC_EFF_3D_A] = b->bufs[k];
+    }
+    DIVA_CUDA(c, cudaEventRecord(b->ready[k], c->stream));
+    DIVA_CUDA(c, cudaStreamWaitEvent(b->stream, b->ready[k], 0));
+  }
+  // one launch runs every member's viscosity loop
+  Ctx* c0 = &b->members[0]->c;
+  DIVA_CUDA(c0, cudaGraphLaunch(b->exec, b->stream));
+  DIVA_CUDA(c0, cudaEventRecord(b->done, b->stream));
+  for (int k = 0; k < n; ++k) {
+    Ctx* c = &b->members[k]->c;
+    DIVA_CUDA(c, cudaStreamWaitEvent(c->stream, b->done, 0));
+    DIVA_CUDA(c, cudaMemcpyAsync(c->h_scal + SC_TARGET2, c->scal + SC_TARGET2,
+                                 sizeof(double) * (SC_COUNT - SC_TARGET2), cudaMemcpyDeviceToHost, c->stream));
+  }
+  // accounting and the solves' tails on the members' streams
+  int first_bad = DIVA_OK;
+  for (int k = 0; k < n; ++k) {
+    Ctx* c = &b->members[k]->c;
+    int st = graph_loop_collect(c, loops[k]);   // also mirrors the loop's viscosity buffer swaps
+    if (!any[k]) {
+      // no sheet ice: solve_DIVA sets the velocities to zero and solves nothing (:276-285);
+      // the member's captured loop ran all the same, and its outcome is dropped
+      st = launch_zero_velocities(c, c->D(DIVA_F_U_VAV_CX), c->D(DIVA_F_V_VAV_CY));
+      c->err.clear();
+      if (!st) st = finish(c, &reports[k]);
+      reports[k].picard_iterations = 0;
+    } else {
+      if (!st) st = graph_loop_end(c, loops[k], &reports[k]);
+      if (st == DIVA_OK || st == DIVA_MAX_PICARD) {
+        int s2 = launch_visc_b_output(c);
+        if (!s2) s2 = launch_3d_horizontal_velocities(c);
+        if (!s2) s2 = launch_secondary_velocities(c);
+        if (!s2) s2 = finish(c, &reports[k]);
+        if (s2) st = s2;
+      }
+    }
+    status[k] = st;
+    reports[k].status = st;
+    if (st != DIVA_OK && first_bad == DIVA_OK) first_bad = st;
+  }
+  return first_bad;
+}
+
 int diva_solve_ssa(diva_ctx_t* h, diva_report_t* rep) {
   if (!h) return DIVA_BAD_INPUT;
   Ctx* c = &h->c;

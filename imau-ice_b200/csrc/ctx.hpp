@@ -334,6 +334,8 @@ int solver_vcycle_fine(Ctx* c, int reps);
 int solver_subcycle(Ctx* c, int reps);
 double solver_vcycle_bytes(const Ctx* c);
 int solver_build_picard_graphs(Ctx* c, bool diva);
+// the viscosity loops of n contexts (solve_DIVA) side by side in one instantiated graph
+int solver_build_batch_graph(Ctx* const* cs, int n, cudaGraphExec_t* exec, void** bufs);
 void solver_destroy_graphs(Ctx* c);
 // tile edge (16 or 32) of each level's smoothing kernels, 0 for levels not smoothed by
 // the tiled kernels; returns the number of levels

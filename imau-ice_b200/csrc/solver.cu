@@ -2441,10 +2441,10 @@ int capture_iteration(Ctx* c, CaptureCtx& cc, cudaStream_t top, bool diva, Picar
   return DIVA_OK;
 }
 
-// the loop graph starting from the viscosity buffer `parity`
-int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
-  cudaGraph_t graph;
-  DIVA_CUDA(c, cudaGraphCreate(&graph, 0));
+// The whole viscosity loop of one context, WHILE(picard) { ITER(parity); IF(odd) { ITER(1 -
+// parity) } }, appended to `graph` as a root node (no dependencies): on its own the graph of
+// build_one, several of them side by side the graph of a batch (solver_build_batch_graph).
+int capture_loop(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity, cudaGraph_t graph, bool count) {
   cudaGraphConditionalHandle h_pic;
   DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_pic, graph, 1, cudaGraphCondAssignDefault));
   DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[0], graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -2458,7 +2458,7 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
   cudaGraphConditionalHandle h_odd;
   DIVA_CUDA(c, cudaGraphConditionalHandleCreate(&h_odd, body_pic, 0, cudaGraphCondAssignDefault));
   // the first iteration of the pair (its buffer order is this graph's parity)
-  if ((st = capture_iteration(c, cc, cc.s[1], diva, G, parity == 0, h_pic, h_odd, 1))) return st;
+  if ((st = capture_iteration(c, cc, cc.s[1], diva, G, count, h_pic, h_odd, 1))) return st;
   cudaGraph_t body_odd;
   if ((st = add_conditional(c, cc.s[1], h_odd, cudaGraphCondTypeIf, &body_odd))) return st;
   DIVA_CUDA(c, cudaStreamBeginCaptureToGraph(cc.s[2], body_odd, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -2468,13 +2468,40 @@ int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
   cc.capturing[2] = false;
   DIVA_CUDA(c, cudaStreamEndCapture(cc.s[1], &body_pic));
   cc.capturing[1] = false;
-  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[0], &graph));
+  cudaGraph_t top = nullptr;
+  DIVA_CUDA(c, cudaStreamEndCapture(cc.s[0], &top));
   cc.capturing[0] = false;
+  return DIVA_OK;
+}
+
+// the loop graph starting from the viscosity buffer `parity`
+int build_one(Ctx* c, CaptureCtx& cc, bool diva, PicardGraphs& G, int parity) {
+  cudaGraph_t graph;
+  DIVA_CUDA(c, cudaGraphCreate(&graph, 0));
+  int st = capture_loop(c, cc, diva, G, parity, graph, parity == 0);
+  if (st) {
+    cudaGraphDestroy(graph);
+    return st;
+  }
   cudaGraphExec_t exec = nullptr;
-  DIVA_CUDA(c, cudaGraphInstantiate(&exec, graph, 0));
+  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
+  DIVA_CUDA(c, e);
   G.exec[parity] = exec;
   return DIVA_OK;
+}
+
+// end every capture a failed build left open, and forget the error it left behind
+void close_captures(CaptureCtx& cc) {
+  for (int q = 5; q >= 0; --q) {
+    if (cc.capturing[q]) {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(cc.s[q], &junk);
+      if (junk) cudaGraphDestroy(junk);
+      cc.capturing[q] = false;
+    }
+  }
+  cudaGetLastError();
 }
 
 }  // namespace
@@ -2514,14 +2541,7 @@ int solver_build_picard_graphs(Ctx* c, bool diva) {
     if (parity == 1) std::swap(c->f[DIVA_F_VISC_EFF_3D_A], *reinterpret_cast<void**>(&c->visc_prev));
     st = build_one(c, cc, diva, G, parity);
   }
-  for (int q = 5; q >= 0; --q) {
-    if (cc.capturing[q]) {
-      cudaGraph_t junk = nullptr;
-      cudaStreamEndCapture(cc.s[q], &junk);
-      if (junk) cudaGraphDestroy(junk);
-    }
-  }
-  cudaGetLastError();   // clear any capture error so the host path can proceed
+  close_captures(cc);   // and clear any capture error so the host path can proceed
   for (int q = 0; q < 6; ++q)
     if (cc.s[q]) cudaStreamDestroy(cc.s[q]);
   c->stream = user;
@@ -2537,6 +2557,52 @@ int solver_build_picard_graphs(Ctx* c, bool diva) {
   }
   G.valid = true;
   return DIVA_OK;
+}
+
+// One graph holding the viscosity loops of n contexts side by side (a batch, diva_batch_create):
+// each member's loop is captured as it stands now (its viscosity buffer order, its
+// configuration) into one parent graph, instantiated once.  bufs[k] receives the buffer
+// member k's loop starts from.  Every member's own loop graphs must exist already (their
+// launch and pass counts account for the batch's iterations).
+int solver_build_batch_graph(Ctx* const* cs, int n, cudaGraphExec_t* exec, void** bufs) {
+  Ctx* c0 = cs[0];
+  *exec = nullptr;
+  cudaGraph_t parent = nullptr;
+  DIVA_CUDA(c0, cudaGraphCreate(&parent, 0));
+  CaptureCtx cc;
+  int st = DIVA_OK;
+  for (int q = 0; q < 6 && !st; ++q)
+    if (cudaStreamCreateWithFlags(&cc.s[q], cudaStreamNonBlocking) != cudaSuccess) st = DIVA_CUDA_ERROR;
+  for (int k = 0; k < n && !st; ++k) {
+    Ctx* c = cs[k];
+    cc.c = c;
+    PicardGraphs scratch;   // the loop's counts are the member's own graphs'
+    cudaStream_t user = c->stream;
+    const long long launches0 = c->launches;
+    const double passes0 = c->fine_passes;
+    const long mg0 = c->mg_cycles;
+    void* visc0 = c->f[DIVA_F_VISC_EFF_3D_A];
+    double* prev0 = c->visc_prev;
+    bufs[k] = visc0;
+    st = capture_loop(c, cc, true, scratch, 0, parent, false);
+    c->stream = user;
+    c->launches = launches0;
+    c->fine_passes = passes0;
+    c->mg_cycles = mg0;
+    c->f[DIVA_F_VISC_EFF_3D_A] = visc0;   // the capture swaps these without running anything
+    c->visc_prev = prev0;
+    if (st) set_error(c0, st, "batch graph: capture of member " + std::to_string(k) + " failed: " + c->err);
+  }
+  close_captures(cc);
+  for (int q = 0; q < 6; ++q)
+    if (cc.s[q]) cudaStreamDestroy(cc.s[q]);
+  if (!st && cudaGraphInstantiate(exec, parent, 0) != cudaSuccess) {
+    *exec = nullptr;
+    cudaGetLastError();
+    st = set_error(c0, DIVA_CUDA_ERROR, "batch graph: instantiation failed");
+  }
+  cudaGraphDestroy(parent);
+  return st;
 }
 
 }  // namespace diva

@@ -418,6 +418,64 @@ def solve_SSA(grid, ice, config=None, backend=None):
     return _run(grid, ice, config, backend, "solve_SSA", OUT_SSA)
 
 
+class Batch:
+    """A persistent batch (diva_batch_create): the viscosity loops of ``contexts`` captured
+    into one CUDA graph once; every ``solve_DIVA()`` is solve_DIVA for all members with a
+    single graph launch for their iterations.  The contexts must stay open and keep their
+    configuration while the batch lives."""
+
+    def __init__(self, contexts):
+        if not contexts:
+            raise DivaError(_abi.BAD_INPUT, "a batch needs at least one context")
+        self.contexts = list(contexts)
+        be = self.contexts[0].backend
+        if be.name != "cuda" or any(c.backend is not be for c in self.contexts):
+            raise DivaError(_abi.UNSUPPORTED, "batches run on the CUDA library, all members on it")
+        lib = be.lib
+        self._create = lib.diva_batch_create
+        self._create.restype = C.c_int
+        self._create.argtypes = [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]
+        self._solve = lib.diva_batch_solve_diva
+        self._solve.restype = C.c_int
+        self._solve.argtypes = [C.c_void_p, C.POINTER(_abi.Report)]
+        self._destroy = lib.diva_batch_destroy
+        self._destroy.restype = C.c_int
+        self._destroy.argtypes = [C.c_void_p]
+        self.h = C.c_void_p()
+        n = len(self.contexts)
+        hs = (C.c_void_p * n)(*[c.h for c in self.contexts])
+        st = self._create(hs, n, C.byref(self.h))
+        if st != 0:
+            err = be.fns["last_error"](self.contexts[0].h)
+            raise DivaError(st, f"diva_batch_create: {err.decode() if err else ''}")
+
+    def solve_DIVA(self, raise_on_error=True):
+        n = len(self.contexts)
+        reps = (_abi.Report * n)()
+        st = self._solve(self.h, reps)
+        out = [r.as_dict() for r in reps]
+        if raise_on_error:
+            for k, (c, r) in enumerate(zip(self.contexts, out)):
+                if r["status"] not in (0, _abi.MAX_PICARD):
+                    err = c.backend.fns["last_error"](c.h)
+                    raise DivaError(r["status"], f"batch member {k}: {err.decode() if err else ''}")
+            if st not in (0, _abi.MAX_PICARD) and all(r["status"] in (0, _abi.MAX_PICARD) for r in out):
+                err = self.contexts[0].backend.fns["last_error"](self.contexts[0].h)
+                raise DivaError(st, f"diva_batch_solve_diva: {err.decode() if err else ''}")
+        return out
+
+    def close(self):
+        if self.h:
+            self._destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def solve_DIVA_batch(contexts, raise_on_error=True):
     """solve_DIVA for several contexts at once (diva_solve_diva_batch): each on its own
     stream, every member's graph-launched viscosity loop in flight at once, so small

@@ -260,6 +260,22 @@ int  diva_solve_diva(diva_ctx_t* ctx, diva_report_t* rep);
  * of ctxs[k] (its status included); returns DIVA_OK if every member is OK, else the
  * first other status.  Contexts must be distinct. */
 int  diva_solve_diva_batch(diva_ctx_t** ctxs, int32_t n, diva_report_t* reports);
+/* A persistent batch: the viscosity loops of n contexts (an ensemble's members) captured
+ * side by side in ONE CUDA graph, instantiated once by diva_batch_create and replayed by
+ * every diva_batch_solve_diva, which is solve_DIVA for all members with a single graph
+ * launch for all their viscosity iterations (each member's loop still ends on its own test;
+ * the launch ends when the last member's has).  The members' preludes and tails (driving
+ * stress, basal conditions, grounded fractions before; 3D and secondary velocities after)
+ * run on the members' own streams around it.  reports[k] is member k's report; returns
+ * DIVA_OK if every member is OK, else the first other status.  The members must stay
+ * alive and unconfigured for the batch's lifetime (a diva_set_config on a member makes
+ * the next solve return DIVA_BAD_INPUT); a member with no sheet ice gets zero velocities,
+ * as from solve_DIVA, after its captured loop has run regardless.  No single routine of
+ * the reference: its members would be separate solve_DIVA calls. */
+typedef struct diva_batch diva_batch_t;
+int  diva_batch_create(diva_ctx_t** ctxs, int32_t n, diva_batch_t** batch);
+int  diva_batch_solve_diva(diva_batch_t* batch, diva_report_t* reports);
+int  diva_batch_destroy(diva_batch_t* batch);
 /* The SIA 3D velocity loop of solve_SIA (ice_velocity_module.f90:60-105) alone,
  * in any dynamics mode (used for "DIVA plus SIA" diagnostics). */
 int  diva_calc_sia_3d_velocities(diva_ctx_t* ctx);

@@ -221,6 +221,46 @@ def test_batch_solve_matches_individual_solves(cuda):
     assert reps[2]["status"] == _abi.MAX_PICARD   # the capped member ends like the lone solve
 
 
+def test_persistent_batch_graph_matches_individual_solves(cuda):
+    """diva_batch_create captures every member's viscosity loop into one CUDA graph;
+    diva_batch_solve_diva replays it as one launch.  Each member's result is bit-identical
+    to solving it alone, on the first replay and on a second one from the same cold
+    states (the members' viscosity buffers then start in another order, which the batch
+    restores before its launch), and a member reconfigured after capture is refused."""
+    ov = {"picard_stop": "relres", "picard_relres_tol": 1e-6, "DIVA_visc_it_nit": 300, "lin_adaptive": 1}
+    cases = [helpers.make_case(1, overrides=ov), helpers.make_case(2, dx=40e3, overrides=ov),
+             helpers.make_case(2, dx=20e3, overrides=dict(ov, picard_anderson_m=3, lin_adaptive_eta=0.1,
+                                                          picard_stall_its=30)),
+             helpers.make_case(2, dx=10e3, overrides=dict(ov, DIVA_visc_it_nit=40, precision="mixed"))]
+    names = ("u_vav_cx", "v_vav_cy", "visc_eff_3D_a", "u_3D_cx", "w_3D_a")
+    alone = [helpers.run(cuda, g, cfg, f) for g, cfg, f in cases]
+    ctxs = []
+    for g, cfg, f in cases:
+        ctx = diva.Context(g, cfg, cuda)
+        helpers.prepare(ctx, f)
+        ctx.state_save()
+        ctxs.append(ctx)
+    batch = diva.Batch(ctxs)
+    for replay in range(2):
+        for ctx in ctxs:
+            ctx.state_restore()
+        reps = batch.solve_DIVA()
+        outs = [ctx.download(list(names)) for ctx in ctxs]
+        for (ra, oa), rb, ob in zip(alone, reps, outs):
+            assert ra["status"] == rb["status"] and ra["picard_iterations"] == rb["picard_iterations"], replay
+            assert ra["mg_cycles"] == rb["mg_cycles"] and ra["stalled"] == rb["stalled"], replay
+            for k in names:
+                assert np.array_equal(oa[k], ob[k]), (replay, k)
+    assert reps[2]["stalled"] == 1 and reps[3]["status"] == _abi.MAX_PICARD
+    ctxs[1].set_config(dict(cases[1][1], lin_adaptive_eta=0.3))
+    with pytest.raises(diva.DivaError) as e:
+        batch.solve_DIVA()
+    assert e.value.status == _abi.BAD_INPUT
+    batch.close()
+    for ctx in ctxs:
+        ctx.close()
+
+
 def test_batch_solve_rejects_repeated_context(cuda):
     g, cfg, f = helpers.make_case(2, dx=40e3)
     ctx = diva.Context(g, cfg, cuda)
