@@ -254,6 +254,68 @@ def run_cpu_variants(args):
     return 0
 
 
+def run_cnn(args):
+    """The warm-start network's tensor-core kernels alone at the headline grid: one forward
+    pass (inference) and one training step (forward, dgrad, wgrad, Adam) on a batch of 8
+    321 x 561 samples, device-synchronised wall clock per call (each call synchronises).
+    FLOPs: 2 x 9 x Cin x Cout per pixel of each 3x3 convolution at its level's resolution
+    (175 kFLOP per pixel of the padded grid forward; a training step counts three times
+    the forward's convolution FLOPs); the tensor roofline is the measured dense BF16 GEMM
+    rate (MEASURED_PEAKS.json)."""
+    import numpy as np
+    import torch
+    load_package()
+    from imau_ice_b200 import build, diva, learned
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    build.build()
+    g = headline_case(0, True)[0]
+    grid = diva.Grid(**g)
+    batch = 8
+    net = learned.WarmStartNet(grid, batch=batch, capacity=0, seed=0)
+    Hp, Wp = net.padded_shape
+    rng = np.random.default_rng(0)
+    feat = torch.as_tensor(rng.normal(0, 1, (batch, Hp, Wp, learned.IN_C)).astype(np.float32)).to(torch.bfloat16).cuda()
+    tgt = torch.as_tensor(rng.normal(0, 1, (batch, Hp, Wp, learned.N_OUT)).astype(np.float32)).cuda()
+    out = torch.zeros(batch, Hp, Wp, learned.N_OUT, device="cuda")
+    level_px = [Hp * Wp, (Hp // 2) * (Wp // 2), (Hp // 4) * (Wp // 4)]
+    lvl = {"e1a": 0, "e1b": 0, "e2a": 1, "e2b": 1, "ba": 2, "bb": 2, "d2a": 1, "d2b": 1, "d1a": 0, "d1b": 0}
+    flop_fwd = batch * sum(2.0 * 9 * ci * co * level_px[lvl[name]] for name, ci, co in learned.LAYERS)
+
+    def timed(fn, reps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    t_fwd = timed(lambda: net.forward(feat.data_ptr(), out.data_ptr(), batch), args.steps)
+    t_train = timed(lambda: net.train_step(feat.data_ptr(), tgt.data_ptr(), batch, 1e-4), args.steps)
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
+        src = "measured (MEASURED_PEAKS.json bf16_tflops)"
+    except Exception:
+        peak, src = 1590.0, "fallback 1590 TFLOP/s"
+    fwd_tf = flop_fwd / t_fwd / 1e12
+    train_tf = 3 * flop_fwd / t_train / 1e12
+    print(json.dumps({
+        "metric": "warm-start network forward passes/s (batch of 8 samples of 321x561)", "value": 1.0 / t_fwd,
+        "unit": "passes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_fwd,
+        "higher_is_better": True, "dtype": "bf16 (fp32 accumulation)", "data": "synthetic (random features)",
+        "config": {"workload": "U-Net of 10 3x3 convolutions (16-128 channels) on the padded a-grid "
+                               f"{Hp}x{Wp}, batch {batch}", "training_step_ms": 1000 * t_train,
+                   "training_steps_per_s": 1.0 / t_train,
+                   "timing": "device-synchronised wall clock per call"},
+        "roofline": {"bound": "tensor", "kernel": "k_conv3x3 (all convolutions of one pass)",
+                     "achieved": fwd_tf, "peak": peak, "unit": "TFLOP/s", "frac": fwd_tf / peak,
+                     "flop_per_pass": flop_fwd, "peak_source": src,
+                     "training_step": {"achieved": train_tf, "frac": train_tf / peak}}}))
+    net.close()
+    return 0
+
+
 def run_reference(args):
     """The reference arm: the CPU port of the reference path (relaxed Picard update, GMRES +
     ILU(0)) on all host threads, one full cold solve per step of the same workload as the
@@ -773,7 +835,7 @@ def run_ensemble(args):
 
     def member_cfg(cfg, accelerated=True):
         cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
-                   lin_rtol=1e-10, picard_stall_its=args.stall_its)
+                   lin_rtol=1e-10, picard_stall_its=args.stall_its, lin_maxit=args.lin_maxit)
         if accelerated:
             cfg.update(picard_anderson_m=args.anderson, precision=args.precision,
                        lin_adaptive_eta=args.eta if args.eta is not None else (0.1 if args.anderson else 0.5))
@@ -843,6 +905,8 @@ def run_ensemble(args):
     converged = sum(1 for k in last if last[k]["status"] == 0)
     stalled = sum(1 for k in last if last[k].get("stalled"))
     failed = {k: last[k]["status"] for k in sorted(last) if last[k]["status"] not in (0, 1)}
+    # members that reached rel-res 1e-6 on both paths: the error the accelerated path leaves
+    both = [fp64_err[k][0] for k in sorted(fp64_err) if last[k]["status"] == 0 and fp64_err[k][2] == 0]
     kinds = [members[k][0] for k in sorted(last)]
     if rank == 0:
         print(json.dumps({
@@ -864,6 +928,10 @@ def run_ensemble(args):
                        "rank0_members_failed": failed,
                        "solver": (f"Anderson({args.anderson}) " if args.anderson else "relaxed Picard ") +
                                  f"precision {args.precision}, stall window {args.stall_its} iterations",
+                       "error_vs_plain_fp64_summary": ({"members_both_converged": len(both),
+                                                        "rel_l2_median": float(np.median(both)) if both else None,
+                                                        "rel_l2_max": float(np.max(both)) if both else None}
+                                                       if fp64_err else None),
                        "error_vs_plain_fp64_rank0": {"rel_l2": [round(fp64_err[k][0], 9) for k in sorted(fp64_err)],
                                                      "max_abs_m_per_yr": [round(fp64_err[k][1], 6)
                                                                           for k in sorted(fp64_err)],
@@ -1052,7 +1120,8 @@ def main():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true",
                    help="timed solves only (no roofline, e2e or CPU legs): the command profiled with ncu")
-    p.add_argument("--workload", choices=["headline", "icecap", "ensemble", "timestep", "learned", "cpu-variants"],
+    p.add_argument("--workload", choices=["headline", "icecap", "ensemble", "timestep", "learned", "cpu-variants",
+                                          "cnn"],
                    default="headline",
                    help="headline (default): held-out ice caps through the learned path (trained network, "
                         "FP32 smoother, Anderson mixing) against the plain FP64 path; icecap: the plain FP64 solve "
@@ -1069,6 +1138,8 @@ def main():
                    help="Anderson mixing depth of the viscosity iteration (0: the reference's relaxation)")
     p.add_argument("--eta", type=float, default=None,
                    help="adaptive linear tolerance factor (default 0.5, or 0.1 with --anderson)")
+    p.add_argument("--lin-maxit", type=int, default=500,
+                   help="ensemble: Krylov iteration cap of each linear solve")
     p.add_argument("--stall-its", type=int, default=0,
                    help="ensemble: stop a member whose rel-res has not fallen by 10 %% for this many viscosity "
                         "iterations (a velocity-limited member that cannot reach the tolerance); 0 = off")
@@ -1081,6 +1152,8 @@ def main():
         return run_learned(args)
     if args.workload == "cpu-variants":
         return run_cpu_variants(args)
+    if args.impl == "b200" and args.workload == "cnn":
+        return run_cnn(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "headline":
