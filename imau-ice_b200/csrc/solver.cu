@@ -36,7 +36,10 @@
 namespace diva {
 namespace {
 
-constexpr int kSubThreads = 1024;       // threads of the one-block coarse-level kernel
+#ifndef DIVA_SUB_THREADS
+#define DIVA_SUB_THREADS 1024
+#endif
+constexpr int kSubThreads = DIVA_SUB_THREADS;   // threads of the one-block coarse-level kernel
 
 // A level's operator.  R is the type of its coefficients and of the x values it is
 // applied to: double everywhere, float for the finest level's smoother copies of the
