@@ -596,6 +596,48 @@ def train_warm_start(grid, members, epochs):
     return net, loss, t_data, time.perf_counter() - t0
 
 
+def train_member_net(kind, samples, epochs):
+    """A warm-start network for the ensemble's members of one size: trained, by the library's
+    tcgen05 kernels, on plain FP64 solutions of that size's generator at seeds 0.. (the
+    ensemble's members use seeds 1000 and up), with friction and flow factors drawn from
+    the ensemble's distributions.  Returns (net, loss, data seconds, training seconds)."""
+    import numpy as np
+    from imau_ice_b200 import diva, learned, synth
+    gen = {"channel": synth.marine_channel, "icecap": synth.ice_cap}[kind]
+    grid = diva.Grid(**gen(seed=0)[0])
+    net = learned.WarmStartNet(grid, batch=8, capacity=samples, seed=0)
+    net.velocities_only()
+    rng = np.random.default_rng(7)
+    t0 = time.perf_counter()
+    seed = 0
+    while net.num_samples < samples and seed < 4 * samples:
+        g, cfg, f = gen(seed=seed)
+        fb = float(np.exp(rng.uniform(np.log(0.3), np.log(3.0))))
+        fa = float(np.exp(rng.uniform(np.log(0.5), np.log(2.0))))
+        f = dict(f)
+        if "beta_sq_a" in f:
+            f["beta_sq_a"] = np.asfortranarray(f["beta_sq_a"] * fb)
+        cfg = dict(cfg, m_enh_sheet=fa, m_enh_shelf=fa, picard_stop="relres", picard_relres_tol=1e-6,
+                   DIVA_visc_it_nit=500, lin_adaptive=1, lin_rtol=1e-10, lin_adaptive_eta=0.5)
+        ctx = diva.Context(diva.Grid(**g), cfg)
+        ctx.upload(f)
+        ctx.update_general_ice_model_data()
+        ctx.calc_pressure_melting_point()
+        ctx.calc_ice_rheology()
+        ctx.update_general_ice_model_data()
+        try:
+            if ctx.solve_DIVA()["status"] == 0:
+                net.add_sample(ctx)
+        except diva.DivaError:
+            pass
+        ctx.close()
+        seed += 1
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss = net.train(epochs, lr=1e-3, seed=1)
+    return net, loss, t_data, time.perf_counter() - t0
+
+
 def run_headline(args):
     """The headline line: DIVA + SIA solves of held-out 321 x 561 x 15 ice caps to rel-res
     1e-6 through the learned path (network warm start, FP32 finest-level smoother, Anderson
@@ -832,6 +874,18 @@ def run_ensemble(args):
     clocks.start()
     t_total, launches, last, group_seconds = 0.0, 0, {}, []
     fp64_err = {}
+    nets, net_info = {}, {}
+    if args.learned:
+        # one network per member size; the 1501 x 1501 sheet has none (one training sample
+        # of it is ~250 MB of device memory), its members start cold
+        for kind in sizes:
+            if kind == "sheet":
+                net_info[kind] = "none: members start cold"
+                continue
+            net, loss, t_data, t_train = train_member_net(kind, args.learned_samples, args.epochs)
+            nets[kind] = net
+            net_info[kind] = {"samples": net.num_samples, "epochs": args.epochs, "final_loss": loss,
+                              "data_generation_s": round(t_data, 2), "training_s": round(t_train, 2)}
 
     def member_cfg(cfg, accelerated=True):
         cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
@@ -856,10 +910,13 @@ def run_ensemble(args):
             ctxs.append(c)
 
         batch = diva.Batch(ctxs)   # every member's viscosity loop in one graph, captured once
+        kinds_grp = [members[k][0].split("-")[0] for k in grp]
 
         def step():
-            for c in ctxs:
+            for c, kind in zip(ctxs, kinds_grp):
                 c.state_restore()
+                if kind in nets:   # the warm start is part of the timed solve
+                    nets[kind].predict(c, complete_sweeps=10)
             return batch.solve_DIVA(raise_on_error=False)
 
         for _ in range(args.warmup):
@@ -894,6 +951,8 @@ def run_ensemble(args):
                                float(np.abs(x - y).max()), r64["status"])
         for c in ctxs:
             c.close()
+    for net in nets.values():
+        net.close()
     clk = clocks.stop()
     dt = torch.tensor([t_total], device="cuda")
     if world > 1:
@@ -927,7 +986,9 @@ def run_ensemble(args):
                        "rank0_members_at_iteration_cap": len(last) - converged - stalled - len(failed),
                        "rank0_members_failed": failed,
                        "solver": (f"Anderson({args.anderson}) " if args.anderson else "relaxed Picard ") +
-                                 f"precision {args.precision}, stall window {args.stall_its} iterations",
+                                 f"precision {args.precision}, stall window {args.stall_its} iterations" +
+                                 (", learned warm start" if args.learned else ""),
+                       "warm_start": net_info or None,
                        "error_vs_plain_fp64_summary": ({"members_both_converged": len(both),
                                                         "rel_l2_median": float(np.median(both)) if both else None,
                                                         "rel_l2_max": float(np.max(both)) if both else None}
@@ -1130,6 +1191,9 @@ def main():
                         "learned: --members training caps, then held-out solves cold vs warm-started")
     p.add_argument("--epochs", type=int, default=60, help="training epochs of the learned workload")
     p.add_argument("--members", type=int, default=64)
+    p.add_argument("--learned", action="store_true",
+                   help="ensemble: warm-start the channel and ice-cap members with a trained network each")
+    p.add_argument("--learned-samples", type=int, default=64, help="training solutions per network (ensemble)")
     p.add_argument("--ensemble-sizes", default="channel,icecap",
                    help="member kinds drawn from: channel (129x17), icecap (321x561), sheet (1501x1501)")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",

@@ -357,9 +357,8 @@ __global__ void __launch_bounds__(kColLanes * kColRows) k_shear_rates(CoefArgs a
 
 struct FaceArgs {
   Dims d;
-  Zeta zt;
   int bc_margin, apply_fgrnd, crossterms;
-  const double *visc, *Hb_i, *beta_eff, *fcx, *fcy, *Na;
+  const double *vint, *Hb_i, *beta_eff, *fcx, *fcy, *Na;
   const int* mask_ice;
   double *visc_int_b, *Nb, *bex, *bey, *Ncx, *Ncy;
   double *lvBx, *lvBy, *lvNa, *lvNb;   // level-0 operator coefficients (Bx = beta_eff_cx * dx^2)
@@ -372,30 +371,23 @@ __global__ void __launch_bounds__(256) k_face_coefficients(FaceArgs a) {
   const long long q = d.at(j, i);
   const double dx2 = d.dx * d.dx;
   if (i < d.nx - 1 && j < d.ny - 1) {
-    // stagger the 3D viscosity to the b-grid and integrate (:820-874)
+    // the 3D viscosity staggered to the b-grid and integrated over the column (:820-874).
+    // The staggering is a fixed weighting of the four corner columns and the trapezoid rule
+    // is linear, so the integral is the same weighting of the corners' integrals (equal up
+    // to rounding): the 3D viscosity is not read again.
     const long long q1 = d.at(j, i + 1), q2 = d.at(j + 1, i), q3 = d.at(j + 1, i + 1);
-    double w = 0.0;
-    int m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+    double s;
     if (a.bc_margin) {
-      m0 = a.mask_ice[q] == 1; m1 = a.mask_ice[q1] == 1; m2 = a.mask_ice[q2] == 1; m3 = a.mask_ice[q3] == 1;
-      w = (double)m0 + (double)m1 + (double)m2 + (double)m3;
-    }
-    double s = 0.0, prev = 0.0;
-    for (int k = 0; k < d.nz; ++k) {
-      const long long o = (long long)k * d.plane;
-      double vb;
-      if (a.bc_margin) {
-        vb = 0.0;
-        if (m0) vb = vb + a.visc[o + q];
-        if (m1) vb = vb + a.visc[o + q1];
-        if (m2) vb = vb + a.visc[o + q2];
-        if (m3) vb = vb + a.visc[o + q3];
-        if (w > 0.0) vb = vb / w;
-      } else {
-        vb = (a.visc[o + q] + a.visc[o + q1] + a.visc[o + q2] + a.visc[o + q3]) / 4.0;
-      }
-      if (k > 0) s = s + 0.5 * (vb + prev) * (a.zt.z[k] - a.zt.z[k - 1]);
-      prev = vb;
+      const int m0 = a.mask_ice[q] == 1, m1 = a.mask_ice[q1] == 1, m2 = a.mask_ice[q2] == 1, m3 = a.mask_ice[q3] == 1;
+      const double w = (double)m0 + (double)m1 + (double)m2 + (double)m3;
+      double vb = 0.0;
+      if (m0) vb = vb + a.vint[q];
+      if (m1) vb = vb + a.vint[q1];
+      if (m2) vb = vb + a.vint[q2];
+      if (m3) vb = vb + a.vint[q3];
+      s = w > 0.0 ? vb / w : 0.0;
+    } else {
+      s = (a.vint[q] + a.vint[q1] + a.vint[q2] + a.vint[q3]) / 4.0;
     }
     a.visc_int_b[q] = s;
     const double nb = a.bc_margin ? s * a.Hb_i[q] : s * max_ref(0.1, a.Hb_i[q]);
@@ -1097,11 +1089,10 @@ int launch_diva_coefficients(Ctx* c, const double* u, const double* v, bool diva
   DIVA_LAUNCHED(c, "column coefficients");
   FaceArgs fa{};
   fa.d = c->d;
-  fa.zt = c->zt;
   fa.bc_margin = a.bc_margin;
   fa.apply_fgrnd = diva ? C.do_GL_subgrid_friction : 1;   // solve_SSA always applies f_grnd^2 (:200-205)
   fa.crossterms = C.include_SSADIVA_crossterms;
-  fa.visc = c->D(DIVA_F_VISC_EFF_3D_A); fa.Hb_i = c->D(DIVA_F_HI_B); fa.beta_eff = c->D(DIVA_F_BETA_EFF_A);
+  fa.vint = c->D(DIVA_F_VISC_EFF_INT_A); fa.Hb_i = c->D(DIVA_F_HI_B); fa.beta_eff = c->D(DIVA_F_BETA_EFF_A);
   fa.fcx = c->D(DIVA_F_F_GRND_CX); fa.fcy = c->D(DIVA_F_F_GRND_CY); fa.Na = c->D(DIVA_F_N_A);
   fa.mask_ice = c->I(DIVA_F_MASK_ICE_A);
   fa.visc_int_b = c->D(DIVA_F_VISC_EFF_INT_B); fa.Nb = c->D(DIVA_F_N_B);

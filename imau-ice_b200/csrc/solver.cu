@@ -293,14 +293,16 @@ __device__ __forceinline__ double diag_v(const Op& o, int j, int i) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;                   \
   const int i = blockIdx.y * blockDim.y + threadIdx.y;
 
-// Gauss-Seidel update of one point of one component (comp 0 = u, 1 = v)
+// Gauss-Seidel update of one point of one component (comp 0 = u, 1 = v).  Every smoother
+// (these per-colour kernels, the tiles, the sub-cycle) forms x + (b - A x) / diag as one
+// explicit fused multiply-add, so all of them round alike.
 __device__ __forceinline__ void gs_point(const Op& o, double* xu, double* xv, const double* bu, const double* bv,
                                          const double* idu, const double* idv, int comp, int j, int i) {
   const long long q = o.d.at(j, i);
   if (comp == 0) {
-    if (u_int(o.d, j, i)) xu[q] += (bu[q] - Au(o, xu, xv, j, i)) * idu[q];
+    if (u_int(o.d, j, i)) xu[q] = fma(bu[q] - Au(o, xu, xv, j, i), idu[q], xu[q]);
   } else {
-    if (v_int(o.d, j, i)) xv[q] += (bv[q] - Av(o, xu, xv, j, i)) * idv[q];
+    if (v_int(o.d, j, i)) xv[q] = fma(bv[q] - Av(o, xu, xv, j, i), idv[q], xv[q]);
   }
 }
 
@@ -358,31 +360,35 @@ __global__ void k_residual(Op o, const double* xu, const double* xv, const doubl
 }
 
 // 1D transfer weights.  "cell" direction: u along x, v along y; "node": u along y, v along x.
-// Gather form of the restriction: coarse C collects fine f with weight w.
-__device__ __forceinline__ int gather_cell(int C, int f2, int* f, double* w) {
-  if (f2 == 1) { f[0] = C; w[0] = 1.0; return 1; }
-  f[0] = 2 * C - 1; w[0] = 0.25; f[1] = 2 * C; w[1] = 0.75; f[2] = 2 * C + 1; w[2] = 0.75; f[3] = 2 * C + 2; w[3] = 0.25;
-  return 4;
+// Gather form of the restriction: coarse C collects fine f with weight w; tap k of at most
+// 4 (cell) or 3 (node), or the single tap f = C, w = 1 where the level is not coarsened
+// along that direction (f2 = 1).  The taps are formed in registers, one at a time, and
+// summed with explicit fused multiply-adds (the weights' products are exact), so every
+// kernel that restricts or prolongs rounds alike.
+__device__ __forceinline__ int gather_cell_n(int f2) { return f2 == 1 ? 1 : 4; }
+__device__ __forceinline__ int gather_node_n(int f2) { return f2 == 1 ? 1 : 3; }
+__device__ __forceinline__ void gather_cell(int C, int f2, int k, int& f, double& w) {
+  if (f2 == 1) { f = C; w = 1.0; return; }
+  f = 2 * C - 1 + k; w = (k == 0 || k == 3) ? 0.25 : 0.75;
 }
-__device__ __forceinline__ int gather_node(int C, int f2, int* f, double* w) {
-  if (f2 == 1) { f[0] = C; w[0] = 1.0; return 1; }
-  f[0] = 2 * C - 1; w[0] = 0.5; f[1] = 2 * C; w[1] = 1.0; f[2] = 2 * C + 1; w[2] = 0.5;
-  return 3;
+__device__ __forceinline__ void gather_node(int C, int f2, int k, int& f, double& w) {
+  if (f2 == 1) { f = C; w = 1.0; return; }
+  f = 2 * C - 1 + k; w = k == 1 ? 1.0 : 0.5;
 }
-// Scatter form (prolongation): fine f takes coarse C with weight w.
-__device__ __forceinline__ int scatter_cell(int f, int f2, int* C, double* w) {
-  if (f2 == 1) { C[0] = f; w[0] = 1.0; return 1; }
+// Scatter form (prolongation): fine f takes coarse C with weight w; tap k of at most 2.
+__device__ __forceinline__ int scatter_cell_n(int f, int f2) { return f2 == 1 ? 1 : 2; }
+__device__ __forceinline__ int scatter_node_n(int f, int f2) { return f2 == 1 ? 1 : ((f & 1) == 0 ? 1 : 2); }
+__device__ __forceinline__ void scatter_cell(int f, int f2, int k, int& C, double& w) {
+  if (f2 == 1) { C = f; w = 1.0; return; }
   const int c = f >> 1;
-  if ((f & 1) == 0) { C[0] = c; w[0] = 0.75; C[1] = c - 1; w[1] = 0.25; }
-  else { C[0] = c; w[0] = 0.75; C[1] = c + 1; w[1] = 0.25; }
-  return 2;
+  C = k == 0 ? c : ((f & 1) == 0 ? c - 1 : c + 1);
+  w = k == 0 ? 0.75 : 0.25;
 }
-__device__ __forceinline__ int scatter_node(int f, int f2, int* C, double* w) {
-  if (f2 == 1) { C[0] = f; w[0] = 1.0; return 1; }
+__device__ __forceinline__ void scatter_node(int f, int f2, int k, int& C, double& w) {
+  if (f2 == 1) { C = f; w = 1.0; return; }
   const int c = f >> 1;
-  if ((f & 1) == 0) { C[0] = c; w[0] = 1.0; return 1; }
-  C[0] = c; w[0] = 0.5; C[1] = c + 1; w[1] = 0.5;
-  return 2;
+  if ((f & 1) == 0) { C = c; w = 1.0; return; }
+  C = c + k; w = 0.5;
 }
 
 // b_c = P^T r_f on coarse interior points; x_c = 0
@@ -390,22 +396,40 @@ __device__ __forceinline__ int scatter_node(int f, int f2, int* C, double* w) {
 template <class RR>
 __device__ __forceinline__ void restrict_values(const Dims& df, const Dims& dc, int fx, int fy, const RR* ru,
                                                 const RR* rv, int j, int i, double& bu, double& bv) {
-  int fi[4], fj[4];
-  double wi[4], wj[4];
   double s = 0.0;
   if (u_int(dc, j, i)) {
-    const int ni = gather_cell(i, fx, fi, wi), nj = gather_node(j, fy, fj, wj);
-    for (int a = 0; a < nj; ++a)
-      for (int b = 0; b < ni; ++b)
-        if (u_int(df, fj[a], fi[b])) s += wj[a] * wi[b] * (double)ru[df.at(fj[a], fi[b])];
+    const int ni = gather_cell_n(fx), nj = gather_node_n(fy);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (a >= nj) break;
+      int fj; double wj;
+      gather_node(j, fy, a, fj, wj);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        if (b >= ni) break;
+        int fi; double wi;
+        gather_cell(i, fx, b, fi, wi);
+        if (u_int(df, fj, fi)) s = fma(wj * wi, (double)ru[df.at(fj, fi)], s);
+      }
+    }
   }
   bu = s;
   s = 0.0;
   if (v_int(dc, j, i)) {
-    const int ni = gather_node(i, fx, fi, wi), nj = gather_cell(j, fy, fj, wj);
-    for (int a = 0; a < nj; ++a)
-      for (int b = 0; b < ni; ++b)
-        if (v_int(df, fj[a], fi[b])) s += wj[a] * wi[b] * (double)rv[df.at(fj[a], fi[b])];
+    const int ni = gather_node_n(fx), nj = gather_cell_n(fy);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      if (a >= nj) break;
+      int fj; double wj;
+      gather_cell(j, fy, a, fj, wj);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        if (b >= ni) break;
+        int fi; double wi;
+        gather_node(i, fx, b, fi, wi);
+        if (v_int(df, fj, fi)) s = fma(wj * wi, (double)rv[df.at(fj, fi)], s);
+      }
+    }
   }
   bv = s;
 }
@@ -429,29 +453,45 @@ __global__ void k_restrict(Dims df, Dims dc, int fx, int fy, const double* ru, c
 // coarse boundary mapping); zero off the fine interior
 __device__ __forceinline__ void prolong_delta(const Op& oc, const Dims& df, int fx, int fy, const double* xcu,
                                               const double* xcv, int j, int i, double& du, double& dv) {
-  int Ci[2], Cj[2];
-  double wi[2], wj[2];
   const Dims& dc = oc.d;
   du = 0.0;
   dv = 0.0;
   if (u_int(df, j, i)) {
-    const int ni = scatter_cell(i, fx, Ci, wi), nj = scatter_node(j, fy, Cj, wj);
+    const int ni = scatter_cell_n(i, fx), nj = scatter_node_n(j, fy);
     double s = 0.0;
-    for (int a = 0; a < nj; ++a)
-      for (int b = 0; b < ni; ++b) {
-        const int J = min(max(Cj[a], 0), dc.ny - 1), I = min(max(Ci[b], 0), dc.nx - 2);
-        s += wj[a] * wi[b] * LU(oc, xcu, J, I);
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      if (a >= nj) break;
+      int Cj; double wj;
+      scatter_node(j, fy, a, Cj, wj);
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        if (b >= ni) break;
+        int Ci; double wi;
+        scatter_cell(i, fx, b, Ci, wi);
+        const int J = min(max(Cj, 0), dc.ny - 1), I = min(max(Ci, 0), dc.nx - 2);
+        s = fma(wj * wi, LU(oc, xcu, J, I), s);
       }
+    }
     du = s;
   }
   if (v_int(df, j, i)) {
-    const int ni = scatter_node(i, fx, Ci, wi), nj = scatter_cell(j, fy, Cj, wj);
+    const int ni = scatter_node_n(i, fx), nj = scatter_cell_n(j, fy);
     double s = 0.0;
-    for (int a = 0; a < nj; ++a)
-      for (int b = 0; b < ni; ++b) {
-        const int J = min(max(Cj[a], 0), dc.ny - 2), I = min(max(Ci[b], 0), dc.nx - 1);
-        s += wj[a] * wi[b] * LV(oc, xcv, J, I);
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      if (a >= nj) break;
+      int Cj; double wj;
+      scatter_cell(j, fy, a, Cj, wj);
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        if (b >= ni) break;
+        int Ci; double wi;
+        scatter_node(i, fx, b, Ci, wi);
+        const int J = min(max(Cj, 0), dc.ny - 2), I = min(max(Ci, 0), dc.nx - 1);
+        s = fma(wj * wi, LV(oc, xcv, J, I), s);
       }
+    }
     dv = s;
   }
 }
@@ -556,6 +596,56 @@ struct TileMem {
   __device__ __forceinline__ R idv(const TIx& ix, int j, int i) const {
     return STAGE ? iv[ix(j, i)] : iv[os.d.at(j, i)];
   }
+  // Boundary unknowns in the tile ("ghosts").  A u or v value outside its component's
+  // interior is read, by the rows next to it, through the boundary elimination (u_src,
+  // v_src): as the value of its source point, or as zero.  The tile keeps each such value
+  // in its own slot, equal to its source's current value, so every row of a block reads
+  // its whole stencil as stored, at the domain's edge too: a ghost takes its source's
+  // value in the staging and again whenever the source is updated (ghosts_u, ghosts_v).
+  // The elimination maps a row's outside same-component neighbours back to the row
+  // itself, and cross-component ghosts are read only in the other component's passes, so
+  // no pass reads a ghost that it rewrites.  (Periodic sides, whose sources lie across the
+  // domain, do not use the tiles.)
+  __device__ __forceinline__ bool in_region(const TIx& ix, int j, int i) const {
+    using G = TileGeom<TJ, TI, STAGE, R, H>;
+    return j >= ix.j0 && j < ix.j0 + G::RJ && i >= ix.i0 && i < ix.i0 + G::RI;
+  }
+  // The new value of the interior u point (j,i) into the ghosts whose source it is: by
+  // u_src's rule, the edge point beyond it on an 'infinite' side and the corner beyond it
+  // where two such sides meet.
+  __device__ __forceinline__ void ghosts_u(const TIx& ix, int j, int i, R val) {
+    const Dims& d = os.d;
+    const BCs& b = os.bc;
+    const bool W = i == 1, E = i == d.nx - 3, S = j == 1, N = j == d.ny - 2;
+    if (!(W || E || S || N)) return;
+    auto put = [&](int jg, int ig) { if (in_region(ix, jg, ig)) xu[ix(jg, ig)] = val; };
+    constexpr int INF = DIVA_BC_INFINITE;
+    if (W && b.uW == INF) put(j, 0);
+    if (E && b.uE == INF) put(j, d.nx - 2);
+    if (S && b.uS == INF) put(0, i);
+    if (N && b.uN == INF) put(d.ny - 1, i);
+    if (W && S && bc_pick(b.uS, b.uW) == INF) put(0, 0);
+    if (E && S && bc_pick(b.uS, b.uE) == INF) put(0, d.nx - 2);
+    if (W && N && bc_pick(b.uN, b.uW) == INF) put(d.ny - 1, 0);
+    if (E && N && bc_pick(b.uN, b.uE) == INF) put(d.ny - 1, d.nx - 2);
+  }
+  // the same for the interior v point (j,i) (v_src's rule)
+  __device__ __forceinline__ void ghosts_v(const TIx& ix, int j, int i, R val) {
+    const Dims& d = os.d;
+    const BCs& b = os.bc;
+    const bool W = i == 1, E = i == d.nx - 2, S = j == 1, N = j == d.ny - 3;
+    if (!(W || E || S || N)) return;
+    auto put = [&](int jg, int ig) { if (in_region(ix, jg, ig)) xv[ix(jg, ig)] = val; };
+    constexpr int INF = DIVA_BC_INFINITE;
+    if (W && b.vW == INF) put(j, 0);
+    if (E && b.vE == INF) put(j, d.nx - 1);
+    if (S && b.vS == INF) put(0, i);
+    if (N && b.vN == INF) put(d.ny - 2, i);
+    if (W && S && bc_pick(b.vS, b.vW) == INF) put(0, 0);
+    if (E && S && bc_pick(b.vS, b.vE) == INF) put(0, d.nx - 1);
+    if (W && N && bc_pick(b.vN, b.vW) == INF) put(d.ny - 2, 0);
+    if (E && N && bc_pick(b.vN, b.vE) == INF) put(d.ny - 2, d.nx - 1);
+  }
 };
 
 // one colour pass over the region points within `reach` of the tile
@@ -572,10 +662,20 @@ __device__ __forceinline__ void tile_pass(M& m, const TIx& ix, int TJ, int TI, i
     if (j >= bj0 + BJ) continue;
     if (!DEEP && (j < 0 || j >= d.ny || i < 0 || i >= d.nx)) continue;
     const int k = ix(j, i);
+    // every stencil value is read as stored: at the domain's edge the ghosts hold what
+    // the boundary elimination would read
     if (comp == 0) {
-      if (DEEP || u_int(d, j, i)) m.xu[k] += (m.bu[k] - m.template Au<DEEP>(ix, j, i)) * m.idu(ix, j, i);
+      if (DEEP || u_int(d, j, i)) {
+        const auto val = fma_r(m.bu[k] - m.template Au<true>(ix, j, i), m.idu(ix, j, i), m.xu[k]);
+        m.xu[k] = val;
+        if (!DEEP) m.ghosts_u(ix, j, i, val);
+      }
     } else {
-      if (DEEP || v_int(d, j, i)) m.xv[k] += (m.bv[k] - m.template Av<DEEP>(ix, j, i)) * m.idv(ix, j, i);
+      if (DEEP || v_int(d, j, i)) {
+        const auto val = fma_r(m.bv[k] - m.template Av<true>(ix, j, i), m.idv(ix, j, i), m.xv[k]);
+        m.xv[k] = val;
+        if (!DEEP) m.ghosts_v(ix, j, i, val);
+      }
     }
   }
 }
@@ -661,8 +761,9 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(OpT<R> o, Restrict
       gru[q] = m.bu[k] - m.template Au<true>(ix, j, i);
       grv[q] = m.bv[k] - m.template Av<true>(ix, j, i);
     } else {
-      gru[q] = u_int(d, j, i) ? m.bu[k] - m.template Au<false>(ix, j, i) : R(0);
-      grv[q] = v_int(d, j, i) ? m.bv[k] - m.template Av<false>(ix, j, i) : R(0);
+      // the ghosts hold the boundary values: stored reads
+      gru[q] = u_int(d, j, i) ? m.bu[k] - m.template Au<true>(ix, j, i) : R(0);
+      grv[q] = v_int(d, j, i) ? m.bv[k] - m.template Av<true>(ix, j, i) : R(0);
     }
   }
 }
@@ -699,6 +800,25 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
       if (v_int(d, j, i)) xb += dv;
       ba = gbu[q];
       bb = gbv[q];
+      if (!deep) {   // a ghost: its source's staged value, formed as the source forms it
+        int js, is;
+        if (j <= d.ny - 1 && i <= d.nx - 2 && !u_int(d, j, i)) {
+          xa = 0.0;
+          if (u_src(d, o.bc, j, i, js, is)) {
+            double a0, a1;
+            prolong_delta(oc, d, fx, fy, xcu, xcv, js, is, a0, a1);
+            xa = gxu[d.at(js, is)] + a0;
+          }
+        }
+        if (j <= d.ny - 2 && i <= d.nx - 1 && !v_int(d, j, i)) {
+          xb = 0.0;
+          if (v_src(d, o.bc, j, i, js, is)) {
+            double a0, a1;
+            prolong_delta(oc, d, fx, fy, xcu, xcv, js, is, a0, a1);
+            xb = gxv[d.at(js, is)] + a1;
+          }
+        }
+      }
     }
     m.xu[t] = R(xa);
     m.xv[t] = R(xb);
@@ -718,8 +838,8 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
     if (j >= d.ny || i >= d.nx) continue;
     const long long q = d.at(j, i);
     const int k = ix(j, i);
-    oxu[q] = m.xu[k];
-    oxv[q] = m.xv[k];
+    oxu[q] = (deep || u_int(d, j, i)) ? (double)m.xu[k] : 0.0;   // no ghost values out
+    oxv[q] = (deep || v_int(d, j, i)) ? (double)m.xv[k] : 0.0;
   }
 }
 
@@ -735,7 +855,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
 // relaxes instead.
 struct CoarseMap {
   int ny, nu, nv;
-  __device__ __forceinline__ int n() const { return nu + nv; }
+  __host__ __device__ __forceinline__ int n() const { return nu + nv; }
   __device__ __forceinline__ void point(int r, int& comp, int& j, int& i) const {
     if (r < nu) { comp = 0; i = 1 + r / (ny - 2); j = 1 + r % (ny - 2); }
     else { const int q = r - nu; comp = 1; i = 1 + q / (ny - 3); j = 1 + q % (ny - 3); }
@@ -860,8 +980,11 @@ __device__ __forceinline__ void coarse_setup_block(const Op& o, const CoarseMap&
 }
 
 
-// x += Ainv (b - A x) on the coarsest level, by one block (the caller synchronises)
-__device__ __forceinline__ void block_coarse_direct(const Op& o, const CoarseMap& m, const double* Ainv, double* xu,
+// x = Ainv b on the coarsest level, by one block (the caller synchronises).  The descent
+// enters the coarsest level with x = 0, so its residual is b itself.  AinvT is the
+// inverse transposed (AinvT[c * n + r] = Ainv[r][c]), in shared memory, so the threads of
+// a warp read consecutive elements; the sums run over c in ascending order.
+__device__ __forceinline__ void block_coarse_direct(const Op& o, const CoarseMap& m, const double* AinvT, double* xu,
                                                     double* xv, const double* bu, const double* bv) {
   __shared__ double sr[kCoarseDirectMax];
   const int n = m.n();
@@ -869,15 +992,15 @@ __device__ __forceinline__ void block_coarse_direct(const Op& o, const CoarseMap
     int comp, j, i;
     m.point(r, comp, j, i);
     const long long q = o.d.at(j, i);
-    sr[r] = comp == 0 ? bu[q] - Au(o, xu, xv, j, i) : bv[q] - Av(o, xu, xv, j, i);
+    sr[r] = comp == 0 ? bu[q] : bv[q];
   }
   __syncthreads();
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
     double s = 0.0;
-    for (int c = 0; c < n; ++c) s += Ainv[r * n + c] * sr[c];
+    for (int c = 0; c < n; ++c) s += AinvT[c * n + r] * sr[c];
     int comp, j, i;
     m.point(r, comp, j, i);
-    (comp == 0 ? xu : xv)[o.d.at(j, i)] += s;
+    (comp == 0 ? xu : xv)[o.d.at(j, i)] = s;
   }
 }
 
@@ -917,6 +1040,8 @@ struct SubCycle {
   const int* singular;
   Restriction rs;              // b of the first level: given, or restricted from the finer residual
   int dbl;                     // doubles of all levels' planes (the table area follows)
+  int ainv_off;                // offset (doubles) of the staged, transposed inverse, after the tables
+  int tab16;                   // 16-byte vectors of all levels' row tables
   SubLevel L[kMaxLevels];
 };
 
@@ -952,6 +1077,10 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
   extern __shared__ double sm[];
   __shared__ Op so[kMaxLevels];   // operators of the staged levels
   uint16_t* tabs = reinterpret_cast<uint16_t*>(sm + sc.dbl);
+  double* AinvT = sm + sc.ainv_off;
+  // whether the coarsest level is solved with its inverse (read before the staging, so
+  // that the flag's load overlaps it)
+  const bool direct = sc.direct && *sc.singular == 0;
   if (threadIdx.x == 0)
     for (int l = sc.first; l <= sc.last; ++l) {
       Op o = sc.L[l].o;
@@ -965,18 +1094,25 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
       o.By = a + SA_BY * P1;
       so[l] = o;
     }
-  for (int l = sc.first; l <= sc.last; ++l) {
-    const SubLevel& L = sc.L[l];
-    const Dims& g = L.o.d;
-    const int P = g.nx * g.ny, P1 = P + 1;
-    double* a = sm + L.soff;
-    for (int t = threadIdx.x; t < P1; t += blockDim.x) {
+  // the staging: one pass over the points of all levels (their loads independent of one
+  // another), then the row tables and the coarsest level's inverse
+  {
+    int total = 0;
+    for (int l = sc.first; l <= sc.last; ++l) total += sc.L[l].o.d.nx * sc.L[l].o.d.ny + 1;
+    for (int t0 = threadIdx.x; t0 < total; t0 += blockDim.x) {
+      int l = sc.first, t = t0;
+      while (t >= sc.L[l].o.d.nx * sc.L[l].o.d.ny + 1) { t -= sc.L[l].o.d.nx * sc.L[l].o.d.ny + 1; ++l; }
+      const SubLevel& L = sc.L[l];
+      const Dims& g = L.o.d;
+      const int P = g.nx * g.ny, P1 = P + 1;
+      double* a = sm + L.soff;
       if (t == P) {   // the zero element read by 'zero' boundary sides
         a[SA_XU * P1 + t] = 0.0;
         a[SA_XV * P1 + t] = 0.0;
         continue;
       }
-      const long long q = g.at(t % g.ny, t / g.ny);
+      const int jj = t % g.ny, ii = t / g.ny;
+      const long long q = g.at(jj, ii);
       a[SA_NA * P1 + t] = L.o.Na[q];
       a[SA_NB * P1 + t] = L.o.Nb[q];
       a[SA_BX * P1 + t] = L.o.Bx[q];
@@ -986,7 +1122,7 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
       if (l == sc.first) {   // entered with x = 0
         double b0, b1;
         if (sc.rs.on) {
-          restrict_from(sc.rs, g, t % g.ny, t / g.ny, b0, b1);
+          restrict_from(sc.rs, g, jj, ii, b0, b1);
         } else {
           b0 = bu0[q];
           b1 = bv0[q];
@@ -997,7 +1133,15 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
         a[SA_BV * P1 + t] = b1;
       }
     }
-    for (int t = threadIdx.x; t < kTabCols * L.rows; t += blockDim.x) tabs[L.toff + t] = L.gtab[t];
+    {   // the levels' tables are contiguous and padded to 16 bytes in both places
+      const uint4* g = reinterpret_cast<const uint4*>(sc.L[sc.first].gtab);
+      uint4* t = reinterpret_cast<uint4*>(tabs);
+      for (int e = threadIdx.x; e < sc.tab16; e += blockDim.x) t[e] = g[e];
+    }
+    if (direct) {
+      const int n = sc.map.n();
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) AinvT[(e % n) * n + e / n] = sc.Ainv[e];
+    }
   }
   __syncthreads();
   auto arr = [&](int l, int k) { return sm + sc.L[l].soff + k * (sc.L[l].o.d.nx * sc.L[l].o.d.ny + 1); };
@@ -1015,8 +1159,8 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
       int q;
       const double Ax = table_row_apply(tab, L.rows, r, urow, ny, o.ax, o.ay, a + SA_NA * P1, a + SA_NB * P1,
                                         a + SA_BX * P1, a + SA_BY * P1, xu, xv, q);
-      if (urow) xu[q] += (a[SA_BU * P1 + q] - Ax) * a[SA_IDU * P1 + q];
-      else xv[q] += (a[SA_BV * P1 + q] - Ax) * a[SA_IDV * P1 + q];
+      if (urow) xu[q] = fma(a[SA_BU * P1 + q] - Ax, a[SA_IDU * P1 + q], xu[q]);
+      else xv[q] = fma(a[SA_BV * P1 + q] - Ax, a[SA_IDV * P1 + q], xv[q]);
     }
   };
   // descend
@@ -1025,8 +1169,8 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
     double *xu = arr(l, SA_XU), *xv = arr(l, SA_XV), *bu = arr(l, SA_BU), *bv = arr(l, SA_BV);
     const double *idu = arr(l, SA_IDU), *idv = arr(l, SA_IDV);
     if (l == sc.last) {
-      if (sc.direct && *sc.singular == 0) {
-        block_coarse_direct(o, sc.map, sc.Ainv, xu, xv, bu, bv);
+      if (direct) {
+        block_coarse_direct(o, sc.map, AinvT, xu, xv, bu, bv);
         __syncthreads();
       } else {
         block_coarse_relax(o, xu, xv, bu, bv, idu, idv, sc.coarse_sweeps);
@@ -1665,6 +1809,11 @@ static CoarseMap coarse_map(const Ctx* c) {
   return m;
 }
 
+static int coarse_direct_n(const Ctx* c) {
+  const int n = coarse_map(c).n();
+  return n > 0 && n <= kCoarseDirectMax ? n : 0;
+}
+
 static int sub_first_level(const Ctx* c);
 
 int solver_setup(Ctx* c, int inv_when) {
@@ -1758,13 +1907,22 @@ static size_t sub_dbl(const Ctx* c, int l) {
   for (int q = l; q < c->nlev; ++q) n += (size_t)kSubArrays * ((size_t)c->lv[q].d.nx * c->lv[q].d.ny + 1);
   return n;
 }
+// entries of one level's row table, padded to 8 (16 bytes) so that every level's table
+// starts 16-byte aligned and the sub-cycle copies the tables as 16-byte vectors
+static size_t level_tab_entries(const Dims& d) { return ((size_t)kTabCols * level_rows(d) + 7) / 8 * 8; }
 static size_t sub_tab_entries(const Ctx* c, int l) {
   size_t n = 0;
-  for (int q = l; q < c->nlev; ++q) n += (size_t)kTabCols * level_rows(c->lv[q].d);
+  for (int q = l; q < c->nlev; ++q) n += level_tab_entries(c->lv[q].d);
   return n;
 }
+// the coarsest level's unknowns when it is solved with its inverse, else 0
+static int coarse_direct_n(const Ctx* c);
+// doubles of the sub-cycle's table area (16-byte aligned), between the planes and the inverse
+static size_t sub_tab_dbl(const Ctx* c, int l) { return ((sub_tab_entries(c, l) * sizeof(uint16_t) + 15) / 16) * 2; }
+// dynamic shared memory of the sub-cycle from level l: planes, row tables, the inverse
 static size_t sub_bytes(const Ctx* c, int l) {
-  return sub_dbl(c, l) * sizeof(double) + ((sub_tab_entries(c, l) * sizeof(uint16_t) + 15) / 16) * 16;
+  const size_t n = (size_t)coarse_direct_n(c);
+  return (sub_dbl(c, l) + sub_tab_dbl(c, l) + n * n) * sizeof(double);
 }
 
 // the largest level whose levels all fit in the sub-cycle's shared memory (the row
@@ -1936,7 +2094,7 @@ static int build_sub_tables(Ctx* c) {
     }
     c->sub_cls[l][4] = r;
     if (r != R) return set_error(c, DIVA_CUDA_ERROR, "sub-cycle row table size");
-    off += (size_t)kTabCols * R;
+    off += level_tab_entries(c->lv[l].d);
   }
   if (!tab.empty())
     DIVA_CUDA(c, cudaMemcpy(c->sub_tab, tab.data(), tab.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
@@ -2023,9 +2181,11 @@ static int vcycle(Ctx* c, int l, double* xu, double* xv, const double* bu, const
       for (int k = 0; k < 5; ++k) S.cls[k] = c->sub_cls[q][k];
       S.toff = toff;
       S.gtab = c->sub_tab + c->sub_tab_off[q];
-      toff += kTabCols * S.rows;
+      toff += (int)level_tab_entries(L.d);
     }
     sc.dbl = soff;
+    sc.ainv_off = soff + (int)sub_tab_dbl(c, l);
+    sc.tab16 = toff / 8;
     sc.rs = rs;
     k_subcycle<<<1, kSubThreads, sub_bytes(c, l), c->stream>>>(sc, xu, xv, bu, bv); c->launches++;
     DIVA_LAUNCHED(c, "k_subcycle");
