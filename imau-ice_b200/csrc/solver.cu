@@ -629,6 +629,35 @@ struct TileMem {
     if (W && N && bc_pick(b.uN, b.uW) == INF) put(d.ny - 1, 0);
     if (E && N && bc_pick(b.uN, b.uE) == INF) put(d.ny - 1, d.nx - 2);
   }
+  // Every source point of the region (the interior points on the lines i = 1, the last
+  // interior column, j = 1 and the last interior row of each component) writes its current
+  // value into its ghosts; one point per thread.
+  __device__ __forceinline__ void ghost_refresh(const TIx& ix) {
+    using G = TileGeom<TJ, TI, STAGE, R, H>;
+    const Dims& d = os.d;
+    // the four lines of each component, clipped to the region: 2 vertical (RJ points each)
+    // and 2 horizontal (RI points each)
+    const int per = 2 * G::RJ + 2 * G::RI;
+    for (int t = threadIdx.x; t < 2 * per; t += blockDim.x) {
+      const bool ucomp = t < per;
+      const int e = ucomp ? t : t - per;
+      int j, i;
+      if (e < 2 * G::RJ) {   // a column line: i = 1 or the last interior column
+        j = ix.j0 + e % G::RJ;
+        i = e < G::RJ ? 1 : (ucomp ? d.nx - 3 : d.nx - 2);
+      } else {               // a row line: j = 1 or the last interior row
+        const int f = e - 2 * G::RJ;
+        i = ix.i0 + f % G::RI;
+        j = f < G::RI ? 1 : (ucomp ? d.ny - 2 : d.ny - 3);
+      }
+      if (!in_region(ix, j, i)) continue;
+      if (ucomp) {
+        if (u_int(d, j, i)) ghosts_u(ix, j, i, xu[ix(j, i)]);
+      } else {
+        if (v_int(d, j, i)) ghosts_v(ix, j, i, xv[ix(j, i)]);
+      }
+    }
+  }
   // the same for the interior v point (j,i) (v_src's rule)
   __device__ __forceinline__ void ghosts_v(const TIx& ix, int j, int i, R val) {
     const Dims& d = os.d;
@@ -800,25 +829,6 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
       if (v_int(d, j, i)) xb += dv;
       ba = gbu[q];
       bb = gbv[q];
-      if (!deep) {   // a ghost: its source's staged value, formed as the source forms it
-        int js, is;
-        if (j <= d.ny - 1 && i <= d.nx - 2 && !u_int(d, j, i)) {
-          xa = 0.0;
-          if (u_src(d, o.bc, j, i, js, is)) {
-            double a0, a1;
-            prolong_delta(oc, d, fx, fy, xcu, xcv, js, is, a0, a1);
-            xa = gxu[d.at(js, is)] + a0;
-          }
-        }
-        if (j <= d.ny - 2 && i <= d.nx - 1 && !v_int(d, j, i)) {
-          xb = 0.0;
-          if (v_src(d, o.bc, j, i, js, is)) {
-            double a0, a1;
-            prolong_delta(oc, d, fx, fy, xcu, xcv, js, is, a0, a1);
-            xb = gxv[d.at(js, is)] + a1;
-          }
-        }
-      }
     }
     m.xu[t] = R(xa);
     m.xv[t] = R(xb);
@@ -827,6 +837,13 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
     m.stage(o, idu, idv, ix, t, in, q);
   }
   __syncthreads();
+  if (!deep) {
+    // The ghosts take their sources' staged values: every interior point on the lines next
+    // to the domain's edge writes its own ghosts (the rule of the passes), so only those
+    // lines are visited.  A 'zero' ghost holds 0 already (the pre-smoothing left it so).
+    m.ghost_refresh(ix);
+    __syncthreads();
+  }
   int pass = 0;
   for (int s = 0; s < sweeps; ++s)
     for (int p = 3; p >= 0; --p, ++pass) {
