@@ -1219,8 +1219,11 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
     const Op& k = so[l + 1];
     double *kxu = arr(l + 1, SA_XU), *kxv = arr(l + 1, SA_XV), *kbu = arr(l + 1, SA_BU), *kbv = arr(l + 1, SA_BV);
     const int fx = sc.L[l].fx, fy = sc.L[l].fy;
-    block_for_points(k.d, [&](int j, int i) {
-      restrict_point(o.d, k.d, fx, fy, ru, rv, kbu, kbv, kxu, kxv, j, i);
+    // the two levels' dimensions in registers for the transfer (not re-read from shared
+    // memory for every tap)
+    const Dims df = o.d, dc = k.d;
+    block_for_points(dc, [&](int j, int i) {
+      restrict_point(df, dc, fx, fy, ru, rv, kbu, kbv, kxu, kxv, j, i);
     });
     __syncthreads();
   }
@@ -1231,7 +1234,13 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
     double *xu = arr(l, SA_XU), *xv = arr(l, SA_XV);
     const double *kxu = arr(l + 1, SA_XU), *kxv = arr(l + 1, SA_XV);
     const int fx = sc.L[l].fx, fy = sc.L[l].fy;
-    block_for_points(o.d, [&](int j, int i) { prolong_point(k, o.d, fx, fy, kxu, kxv, xu, xv, j, i); });
+    // the coarse level's dimensions and sides in registers for the transfer (the
+    // prolongation reads them for every tap through the boundary mapping)
+    Op kr{};
+    kr.d = k.d;
+    kr.bc = k.bc;
+    const Dims df = o.d;
+    block_for_points(df, [&](int j, int i) { prolong_point(kr, df, fx, fy, kxu, kxv, xu, xv, j, i); });
     __syncthreads();
     for (int s = 0; s < sc.nu2; ++s)
       for (int p = 3; p >= 0; --p) {
