@@ -495,6 +495,51 @@ __device__ __forceinline__ void prolong_delta(const Op& oc, const Dims& df, int 
     dv = s;
   }
 }
+// P x_c at the fine point (j,i) of a level coarsened by 2 in both directions, from the
+// coarse correction staged in shared memory: cu/cv hold, for the coarse region whose
+// origin is (CJ0,CI0) (CRJ rows per column), the values prolong_delta reads (the clamped
+// position read through the coarse boundary mapping).  The same taps, weights and order.
+__device__ __forceinline__ void prolong_delta_staged(const Dims& df, const double* cu, const double* cv, int CJ0,
+                                                     int CI0, int CRJ, int j, int i, double& du, double& dv) {
+  du = 0.0;
+  dv = 0.0;
+  if (u_int(df, j, i)) {
+    const int ni = scatter_cell_n(i, 2), nj = scatter_node_n(j, 2);
+    double s = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      if (a >= nj) break;
+      int Cj; double wj;
+      scatter_node(j, 2, a, Cj, wj);
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        if (b >= ni) break;
+        int Ci; double wi;
+        scatter_cell(i, 2, b, Ci, wi);
+        s = fma(wj * wi, cu[(Ci - CI0) * CRJ + (Cj - CJ0)], s);
+      }
+    }
+    du = s;
+  }
+  if (v_int(df, j, i)) {
+    const int ni = scatter_node_n(i, 2), nj = scatter_cell_n(j, 2);
+    double s = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      if (a >= nj) break;
+      int Cj; double wj;
+      scatter_cell(j, 2, a, Cj, wj);
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        if (b >= ni) break;
+        int Ci; double wi;
+        scatter_node(i, 2, b, Ci, wi);
+        s = fma(wj * wi, cv[(Ci - CI0) * CRJ + (Cj - CJ0)], s);
+      }
+    }
+    dv = s;
+  }
+}
 // x_f += P x_c on fine interior points
 __device__ __forceinline__ void prolong_point(const Op& oc, const Dims& df, int fx, int fy, const double* xcu,
                                               const double* xcv, double* xu, double* xv, int j, int i) {
@@ -537,6 +582,11 @@ template <int TJ, int TI, bool STAGE, class R = double, int H = kHalo>
 struct TileGeom {
   static constexpr int RJ = TJ + 2 * H, RI = TI + 2 * H, N = RJ * RI;
   static constexpr size_t smem = (STAGE ? 10 : 4) * N * sizeof(R);   // x, b (+ 6 coefficient planes)
+  // the post-smoothing kernel also stages the coarse correction under its region (a
+  // level coarsened by 2 in both directions): CRJ x CRI coarse points, u and v, in double
+  static constexpr int CRJ = RJ / 2 + 3, CRI = RI / 2 + 3;
+  static constexpr size_t coarse_off = (smem + 7) / 8;   // in doubles
+  static constexpr size_t smem_up = (coarse_off + 2 * CRJ * CRI) * sizeof(double);
 };
 
 // A block whose whole region lies in the interior of both components (u: 1 <= i <=
@@ -815,6 +865,23 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
   const int tj0 = blockIdx.x * TJ, ti0 = blockIdx.y * TI;
   const TIx ix{tj0 - H, ti0 - H, RJ};
   const bool deep = tile_deep<TJ, TI, H>(ix, d);
+  // The coarse correction under the region, staged once (a level coarsened by 2 in both
+  // directions): each coarse value is read from L2 once per block instead of by every
+  // fine point that takes it (up to 8 reads per fine point).
+  using G = TileGeom<TJ, TI, STAGE, R, H>;
+  const bool staged = fx == 2 && fy == 2;
+  const int CJ0 = (ix.j0 >> 1) - 1, CI0 = (ix.i0 >> 1) - 1;
+  double* cu = smd + G::coarse_off;
+  double* cv = cu + G::CRJ * G::CRI;
+  if (staged) {
+    const Dims& dc = oc.d;
+    for (int t = threadIdx.x; t < G::CRJ * G::CRI; t += blockDim.x) {
+      const int J = CJ0 + t % G::CRJ, I = CI0 + t / G::CRJ;
+      cu[t] = LU(oc, xcu, min(max(J, 0), dc.ny - 1), min(max(I, 0), dc.nx - 2));
+      cv[t] = LV(oc, xcv, min(max(J, 0), dc.ny - 2), min(max(I, 0), dc.nx - 1));
+    }
+    __syncthreads();
+  }
   for (int t = threadIdx.x; t < N; t += blockDim.x) {
     const int j = ix.j0 + t % RJ, i = ix.i0 + t / RJ;
     const bool in = j >= 0 && j < d.ny && i >= 0 && i < d.nx;
@@ -822,7 +889,8 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
     double xa = 0.0, xb = 0.0, ba = 0.0, bb = 0.0;
     if (in) {
       double du, dv;
-      prolong_delta(oc, d, fx, fy, xcu, xcv, j, i, du, dv);
+      if (staged) prolong_delta_staged(d, cu, cv, CJ0, CI0, G::CRJ, j, i, du, dv);
+      else prolong_delta(oc, d, fx, fy, xcu, xcv, j, i, du, dv);
       xa = gxu[q];
       xb = gxv[q];
       if (u_int(d, j, i)) xa += du;
@@ -2006,7 +2074,7 @@ static void tile_up_h(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv
   const Level& K = c->lv[l + 1];
   const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
   auto kern = o.rtu ? k_smooth_up<T, T, S, true, R, H> : k_smooth_up<T, T, S, false, R, H>;
-  kern<<<grid, kTileThreads, TileGeom<T, T, S, R, H>::smem, c->stream>>>(
+  kern<<<grid, kTileThreads, TileGeom<T, T, S, R, H>::smem_up, c->stream>>>(
       o, make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, reinterpret_cast<const R*>(L.tu),
       reinterpret_cast<const R*>(L.tv), xu, xv, idu, idv, nu);
   c->launches++;
@@ -2134,9 +2202,9 @@ template <int T, bool S, class R, int H>
 static int tile_attrs(Ctx* c) {
   const void* k[4] = {(const void*)k_smooth_down<T, T, S, false, R, H>, (const void*)k_smooth_down<T, T, S, true, R, H>,
                       (const void*)k_smooth_up<T, T, S, false, R, H>, (const void*)k_smooth_up<T, T, S, true, R, H>};
-  for (int q = 0; q < 4; ++q)
+  for (int q = 0; q < 4; ++q)   // the up kernels (2, 3) also stage the coarse correction
     DIVA_CUDA(c, cudaFuncSetAttribute(k[q], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)TileGeom<T, T, S, R, H>::smem));
+                                      (int)(q < 2 ? TileGeom<T, T, S, R, H>::smem : TileGeom<T, T, S, R, H>::smem_up)));
   return DIVA_OK;
 }
 
