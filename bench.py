@@ -887,19 +887,20 @@ def run_ensemble(args):
             net_info[kind] = {"samples": net.num_samples, "epochs": args.epochs, "final_loss": loss,
                               "data_generation_s": round(t_data, 2), "training_s": round(t_train, 2)}
 
-    def member_cfg(cfg, accelerated=True):
+    def member_cfg(cfg, accelerated=True, kind=None):
         cfg = dict(cfg, picard_stop="relres", picard_relres_tol=1e-6, DIVA_visc_it_nit=500, lin_adaptive=1,
                    lin_rtol=1e-10, picard_stall_its=args.stall_its, lin_maxit=args.lin_maxit)
         if accelerated:
-            cfg.update(picard_anderson_m=args.anderson, precision=args.precision,
-                       lin_adaptive_eta=args.eta if args.eta is not None else (0.1 if args.anderson else 0.5))
+            m = args.anderson_sheet if (kind == "sheet" and args.anderson_sheet is not None) else args.anderson
+            cfg.update(picard_anderson_m=m, precision=args.precision,
+                       lin_adaptive_eta=args.eta if args.eta is not None else (0.1 if m else 0.5))
         return cfg
 
     for grp in ensemble.groups(members, parts[rank], budget):
         ctxs = []
         for k in grp:
             name, g, cfg, f = members[k]
-            cfg = member_cfg(cfg)
+            cfg = member_cfg(cfg, kind=name.split("-")[0])
             c = diva.Context(diva.Grid(**g) if isinstance(g, dict) else g, cfg)
             c.upload(f)
             c.update_general_ice_model_data()
@@ -986,6 +987,8 @@ def run_ensemble(args):
                        "rank0_members_at_iteration_cap": len(last) - converged - stalled - len(failed),
                        "rank0_members_failed": failed,
                        "solver": (f"Anderson({args.anderson}) " if args.anderson else "relaxed Picard ") +
+                                 (f"(sheets: Anderson({args.anderson_sheet})) " if args.anderson_sheet else
+                                  "(sheets: relaxed) " if args.anderson_sheet == 0 else "") +
                                  f"precision {args.precision}, stall window {args.stall_its} iterations" +
                                  (", learned warm start" if args.learned else ""),
                        "warm_start": net_info or None,
@@ -1191,6 +1194,8 @@ def main():
                         "learned: --members training caps, then held-out solves cold vs warm-started")
     p.add_argument("--epochs", type=int, default=60, help="training epochs of the learned workload")
     p.add_argument("--members", type=int, default=64)
+    p.add_argument("--anderson-sheet", type=int, default=None,
+                   help="ensemble: Anderson depth for the 1501 x 1501 members (default: --anderson)")
     p.add_argument("--learned", action="store_true",
                    help="ensemble: warm-start the channel and ice-cap members with a trained network each")
     p.add_argument("--learned-samples", type=int, default=64, help="training solutions per network (ensemble)")
