@@ -376,15 +376,15 @@ __device__ __forceinline__ void gather_node(int C, int f2, int k, int& f, double
   f = 2 * C - 1 + k; w = k == 1 ? 1.0 : 0.5;
 }
 // Scatter form (prolongation): fine f takes coarse C with weight w; tap k of at most 2.
-__device__ __forceinline__ int scatter_cell_n(int f, int f2) { return f2 == 1 ? 1 : 2; }
-__device__ __forceinline__ int scatter_node_n(int f, int f2) { return f2 == 1 ? 1 : ((f & 1) == 0 ? 1 : 2); }
-__device__ __forceinline__ void scatter_cell(int f, int f2, int k, int& C, double& w) {
+__host__ __device__ __forceinline__ int scatter_cell_n(int f, int f2) { return f2 == 1 ? 1 : 2; }
+__host__ __device__ __forceinline__ int scatter_node_n(int f, int f2) { return f2 == 1 ? 1 : ((f & 1) == 0 ? 1 : 2); }
+__host__ __device__ __forceinline__ void scatter_cell(int f, int f2, int k, int& C, double& w) {
   if (f2 == 1) { C = f; w = 1.0; return; }
   const int c = f >> 1;
   C = k == 0 ? c : ((f & 1) == 0 ? c - 1 : c + 1);
   w = k == 0 ? 0.75 : 0.25;
 }
-__device__ __forceinline__ void scatter_node(int f, int f2, int k, int& C, double& w) {
+__host__ __device__ __forceinline__ void scatter_node(int f, int f2, int k, int& C, double& w) {
   if (f2 == 1) { C = f; w = 1.0; return; }
   const int c = f >> 1;
   if ((f & 1) == 0) { C = c; w = 1.0; return; }
@@ -1106,6 +1106,7 @@ __device__ __forceinline__ void block_coarse_direct(const Op& o, const CoarseMap
 enum { SA_NA, SA_NB, SA_BX, SA_BY, SA_IDU, SA_IDV, SA_XU, SA_XV, SA_BU, SA_BV, SA_RU, SA_RV, kSubArrays };
 constexpr size_t kSubSmemBudget = 200 * 1024;   // dynamic shared memory of the sub-cycle
 constexpr int kTabCols = 9;                      // a row's position and its eight mapped reads
+constexpr int kTabProlong = 4;                   // then the row's prolongation taps (coarse positions)
 
 struct SubLevel {
   Op o;                      // global-memory operator of the level
@@ -1297,18 +1298,41 @@ __global__ void __launch_bounds__(kSubThreads) k_subcycle(SubCycle sc, double* x
   }
   // ascend
   for (int l = sc.last - 1; l >= sc.first; --l) {
-    const Op& o = so[l];
-    const Op& k = so[l + 1];
     double *xu = arr(l, SA_XU), *xv = arr(l, SA_XV);
     const double *kxu = arr(l + 1, SA_XU), *kxv = arr(l + 1, SA_XV);
-    const int fx = sc.L[l].fx, fy = sc.L[l].fy;
-    // the coarse level's dimensions and sides in registers for the transfer (the
-    // prolongation reads them for every tap through the boundary mapping)
-    Op kr{};
-    kr.d = k.d;
-    kr.bc = k.bc;
-    const Dims df = o.d;
-    block_for_points(df, [&](int j, int i) { prolong_point(kr, df, fx, fy, kxu, kxv, xu, xv, j, i); });
+    {   // x += P x_c on the interior rows, from the rows' prolongation taps (coarse positions
+        // mapped on the host; the weights formed here, in prolong_delta's order)
+      const SubLevel& L = sc.L[l];
+      const int fx = L.fx, fy = L.fy, ny = L.o.d.ny, R = L.rows;
+      const uint16_t* tab = tabs + L.toff;
+      const uint16_t* ptab = tab + kTabCols * R;
+      for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const int q = tab[r], j = q % ny, i = q / ny;
+        double s = 0.0, wj, wi;
+        int k = 0, C;
+        if (r < L.cls[2]) {
+          const int nj = scatter_node_n(j, fy), ni = scatter_cell_n(i, fx);
+          for (int a = 0; a < nj; ++a) {
+            scatter_node(j, fy, a, C, wj);
+            for (int b = 0; b < ni; ++b, ++k) {
+              scatter_cell(i, fx, b, C, wi);
+              s = fma(wj * wi, kxu[ptab[k * R + r]], s);
+            }
+          }
+          xu[q] += s;
+        } else {
+          const int nj = scatter_cell_n(j, fy), ni = scatter_node_n(i, fx);
+          for (int a = 0; a < nj; ++a) {
+            scatter_cell(j, fy, a, C, wj);
+            for (int b = 0; b < ni; ++b, ++k) {
+              scatter_node(i, fx, b, C, wi);
+              s = fma(wj * wi, kxv[ptab[k * R + r]], s);
+            }
+          }
+          xv[q] += s;
+        }
+      }
+    }
     __syncthreads();
     for (int s = 0; s < sc.nu2; ++s)
       for (int p = 3; p >= 0; --p) {
@@ -2003,7 +2027,7 @@ static size_t sub_dbl(const Ctx* c, int l) {
 }
 // entries of one level's row table, padded to 8 (16 bytes) so that every level's table
 // starts 16-byte aligned and the sub-cycle copies the tables as 16-byte vectors
-static size_t level_tab_entries(const Dims& d) { return ((size_t)kTabCols * level_rows(d) + 7) / 8 * 8; }
+static size_t level_tab_entries(const Dims& d) { return ((size_t)(kTabCols + kTabProlong) * level_rows(d) + 7) / 8 * 8; }
 static size_t sub_tab_entries(const Ctx* c, int l) {
   size_t n = 0;
   for (int q = l; q < c->nlev; ++q) n += level_tab_entries(c->lv[q].d);
@@ -2176,6 +2200,37 @@ static int build_sub_tables(Ctx* c) {
         tab[off + (size_t)(1 + k) * R + r] = on ? (uint16_t)d.at(js, is) : (uint16_t)P;
         const bool on2 = urow ? v_src(d, c->bc, jc_[k], ic_[k], js, is) : u_src(d, c->bc, jc_[k], ic_[k], js, is);
         tab[off + (size_t)(5 + k) * R + r] = on2 ? (uint16_t)d.at(js, is) : (uint16_t)P;
+      }
+      // the prolongation taps of the row from the next level (prolong_delta's taps in its
+      // order, each clamped and read through the coarse level's boundary mapping; the
+      // coarse plane's zero element for a 'zero' side or a tap the row does not have)
+      if (l + 1 < c->nlev) {
+        Dims dc = c->lv[l + 1].d;
+        dc.ld = dc.ny;
+        const int Pc = dc.nx * dc.ny;
+        int fx, fy;
+        factors(c, l, &fx, &fy);
+        int k = 0, js, is, Cj, Ci;
+        double w;
+        auto clampi = [](int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); };
+        if (urow) {
+          for (int a = 0; a < scatter_node_n(j, fy); ++a)
+            for (int b = 0; b < scatter_cell_n(i, fx); ++b, ++k) {
+              scatter_node(j, fy, a, Cj, w);
+              scatter_cell(i, fx, b, Ci, w);
+              const bool on = u_src(dc, c->bc, clampi(Cj, 0, dc.ny - 1), clampi(Ci, 0, dc.nx - 2), js, is);
+              tab[off + (size_t)(kTabCols + k) * R + r] = on ? (uint16_t)dc.at(js, is) : (uint16_t)Pc;
+            }
+        } else {
+          for (int a = 0; a < scatter_cell_n(j, fy); ++a)
+            for (int b = 0; b < scatter_node_n(i, fx); ++b, ++k) {
+              scatter_cell(j, fy, a, Cj, w);
+              scatter_node(i, fx, b, Ci, w);
+              const bool on = v_src(dc, c->bc, clampi(Cj, 0, dc.ny - 2), clampi(Ci, 0, dc.nx - 1), js, is);
+              tab[off + (size_t)(kTabCols + k) * R + r] = on ? (uint16_t)dc.at(js, is) : (uint16_t)Pc;
+            }
+        }
+        for (; k < kTabProlong; ++k) tab[off + (size_t)(kTabCols + k) * R + r] = (uint16_t)Pc;
       }
       ++r;
     };
