@@ -2071,6 +2071,19 @@ static int tile_edge(const Ctx* c, int l) {
   const long long b32 = (long long)((d.ny + 31) / 32) * ((d.nx + 31) / 32);
   return b32 >= 148 ? 32 : 16;
 }
+constexpr int kSMs = 148;   // B200
+// Whether level l's tiles are 1.5x wider along i (T x 3T/2): when square tiles give a little
+// more than one block per SM (e.g. 198 on the 321 x 561 ice cap's finest level, where 50 SMs
+// would run two blocks each and set the kernel's length) and the wider ones fit in one
+// block per SM, with less halo per point.  Not when the caller chose the edge.
+static bool tile_wide(const Ctx* c, int l) {
+  if (c->tile_override[l] == 16 || c->tile_override[l] == 32) return false;
+  const Dims& d = c->lv[l].d;
+  const int T = tile_edge(c, l), W = 3 * T / 2;
+  const long long sq = (long long)((d.ny + T - 1) / T) * ((d.nx + T - 1) / T);
+  const long long wide = (long long)((d.ny + T - 1) / T) * ((d.nx + W - 1) / W);
+  return sq > kSMs && wide <= kSMs;
+}
 
 // Which tile kernels a level uses: the edge (tile_edge), and whether the region's
 // coefficients are staged in shared memory (16 x 16 tiles: 92 KB, two blocks per SM;
@@ -2078,56 +2091,59 @@ static int tile_edge(const Ctx* c, int l) {
 // from L2 instead).
 constexpr bool kStage16 = true, kStage32 = false;
 
-// H: the tile's halo, 4 nu + 1 for nu sweeps per phase (halo_for)
-template <int T, bool S, class R, int H>
+// H: the tile's halo, 4 nu + 1 for nu sweeps per phase (halo_for); tiles of TJ rows (j)
+// by TI columns (i)
+template <int TJ, int TI, bool S, class R, int H>
 static void tile_down_h(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, const Restriction& rs,
                         const double* bu, const double* bv, int nu) {
   const Level& L = c->lv[l];
-  const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
+  const dim3 grid((L.d.ny + TJ - 1) / TJ, (L.d.nx + TI - 1) / TI);
   // b is written only when it is restricted here (rs.on), which never happens on the finest level
-  auto kern = o.rtu ? k_smooth_down<T, T, S, true, R, H> : k_smooth_down<T, T, S, false, R, H>;
-  kern<<<grid, kTileThreads, TileGeom<T, T, S, R, H>::smem, c->stream>>>(
+  auto kern = o.rtu ? k_smooth_down<TJ, TI, S, true, R, H> : k_smooth_down<TJ, TI, S, false, R, H>;
+  kern<<<grid, kTileThreads, TileGeom<TJ, TI, S, R, H>::smem, c->stream>>>(
       o, rs, const_cast<double*>(bu), const_cast<double*>(bv), reinterpret_cast<R*>(L.tu),
       reinterpret_cast<R*>(L.tv), reinterpret_cast<R*>(L.ru), reinterpret_cast<R*>(L.rv), idu, idv, nu);
   c->launches++;
 }
-template <int T, bool S, class R, int H>
+template <int TJ, int TI, bool S, class R, int H>
 static void tile_up_h(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, int fx, int fy, const double* bu,
                       const double* bv, double* xu, double* xv, int nu) {
   const Level& L = c->lv[l];
   const Level& K = c->lv[l + 1];
-  const dim3 grid((L.d.ny + T - 1) / T, (L.d.nx + T - 1) / T);
-  auto kern = o.rtu ? k_smooth_up<T, T, S, true, R, H> : k_smooth_up<T, T, S, false, R, H>;
-  kern<<<grid, kTileThreads, TileGeom<T, T, S, R, H>::smem_up, c->stream>>>(
+  const dim3 grid((L.d.ny + TJ - 1) / TJ, (L.d.nx + TI - 1) / TI);
+  auto kern = o.rtu ? k_smooth_up<TJ, TI, S, true, R, H> : k_smooth_up<TJ, TI, S, false, R, H>;
+  kern<<<grid, kTileThreads, TileGeom<TJ, TI, S, R, H>::smem_up, c->stream>>>(
       o, make_op(c, l + 1), fx, fy, K.xu, K.xv, bu, bv, reinterpret_cast<const R*>(L.tu),
       reinterpret_cast<const R*>(L.tv), xu, xv, idu, idv, nu);
   c->launches++;
 }
-template <int T, bool S, class R>
+template <int TJ, int TI, bool S, class R>
 static void tile_down_r(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, const Restriction& rs,
                         const double* bu, const double* bv, int nu) {
-  if (halo_for(nu) == kHaloOne) tile_down_h<T, S, R, kHaloOne>(c, l, o, idu, idv, rs, bu, bv, nu);
-  else tile_down_h<T, S, R, kHalo>(c, l, o, idu, idv, rs, bu, bv, nu);
+  if (halo_for(nu) == kHaloOne) tile_down_h<TJ, TI, S, R, kHaloOne>(c, l, o, idu, idv, rs, bu, bv, nu);
+  else tile_down_h<TJ, TI, S, R, kHalo>(c, l, o, idu, idv, rs, bu, bv, nu);
 }
-template <int T, bool S, class R>
+template <int TJ, int TI, bool S, class R>
 static void tile_up_r(Ctx* c, int l, const OpT<R>& o, const R* idu, const R* idv, int fx, int fy, const double* bu,
                       const double* bv, double* xu, double* xv, int nu) {
-  if (halo_for(nu) == kHaloOne) tile_up_h<T, S, R, kHaloOne>(c, l, o, idu, idv, fx, fy, bu, bv, xu, xv, nu);
-  else tile_up_h<T, S, R, kHalo>(c, l, o, idu, idv, fx, fy, bu, bv, xu, xv, nu);
+  if (halo_for(nu) == kHaloOne) tile_up_h<TJ, TI, S, R, kHaloOne>(c, l, o, idu, idv, fx, fy, bu, bv, xu, xv, nu);
+  else tile_up_h<TJ, TI, S, R, kHalo>(c, l, o, idu, idv, fx, fy, bu, bv, xu, xv, nu);
 }
 static int tile_down(Ctx* c, int l, const Restriction& rs, const double* bu, const double* bv, double* xu,
                      double* xv, int nu) {
   const Level& L = c->lv[l];
-  if (level_fp32(c, l)) {   // float tiles stage their coefficients at both edges (100 KB at 32 x 32)
+  const int T = tile_edge(c, l);
+  const bool W = tile_wide(c, l);
+  if (level_fp32(c, l)) {   // float tiles stage their coefficients at every shape (100 KB at 32 x 32)
     const OpT<float> o = make_op32(c, l);
     const float *iu = c->f32[l][F32_IDU], *iv = c->f32[l][F32_IDV];
-    if (tile_edge(c, l) == 32) tile_down_r<32, true>(c, l, o, iu, iv, rs, bu, bv, nu);
-    else tile_down_r<16, true>(c, l, o, iu, iv, rs, bu, bv, nu);
+    if (T == 32) W ? tile_down_r<32, 48, true>(c, l, o, iu, iv, rs, bu, bv, nu) : tile_down_r<32, 32, true>(c, l, o, iu, iv, rs, bu, bv, nu);
+    else W ? tile_down_r<16, 24, true>(c, l, o, iu, iv, rs, bu, bv, nu) : tile_down_r<16, 16, true>(c, l, o, iu, iv, rs, bu, bv, nu);
   } else {
     const Op o = make_op(c, l);
     const double *iu = L.idu, *iv = L.idv;
-    if (tile_edge(c, l) == 32) tile_down_r<32, kStage32>(c, l, o, iu, iv, rs, bu, bv, nu);
-    else tile_down_r<16, kStage16>(c, l, o, iu, iv, rs, bu, bv, nu);
+    if (T == 32) W ? tile_down_r<32, 48, kStage32>(c, l, o, iu, iv, rs, bu, bv, nu) : tile_down_r<32, 32, kStage32>(c, l, o, iu, iv, rs, bu, bv, nu);
+    else W ? tile_down_r<16, 24, kStage16>(c, l, o, iu, iv, rs, bu, bv, nu) : tile_down_r<16, 16, kStage16>(c, l, o, iu, iv, rs, bu, bv, nu);
   }
   DIVA_LAUNCHED(c, "k_smooth_down");
   return DIVA_OK;
@@ -2135,16 +2151,18 @@ static int tile_down(Ctx* c, int l, const Restriction& rs, const double* bu, con
 static int tile_up(Ctx* c, int l, int fx, int fy, const double* bu, const double* bv, double* xu, double* xv,
                    int nu) {
   const Level& L = c->lv[l];
+  const int T = tile_edge(c, l);
+  const bool W = tile_wide(c, l);
   if (level_fp32(c, l)) {
     const OpT<float> o = make_op32(c, l);
     const float *iu = c->f32[l][F32_IDU], *iv = c->f32[l][F32_IDV];
-    if (tile_edge(c, l) == 32) tile_up_r<32, true>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
-    else tile_up_r<16, true>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
+    if (T == 32) W ? tile_up_r<32, 48, true>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu) : tile_up_r<32, 32, true>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
+    else W ? tile_up_r<16, 24, true>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu) : tile_up_r<16, 16, true>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
   } else {
     const Op o = make_op(c, l);
     const double *iu = L.idu, *iv = L.idv;
-    if (tile_edge(c, l) == 32) tile_up_r<32, kStage32>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
-    else tile_up_r<16, kStage16>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
+    if (T == 32) W ? tile_up_r<32, 48, kStage32>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu) : tile_up_r<32, 32, kStage32>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
+    else W ? tile_up_r<16, 24, kStage16>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu) : tile_up_r<16, 16, kStage16>(c, l, o, iu, iv, fx, fy, bu, bv, xu, xv, nu);
   }
   DIVA_LAUNCHED(c, "k_smooth_up");
   return DIVA_OK;
@@ -2253,13 +2271,24 @@ static int build_sub_tables(Ctx* c) {
 size_t solver_table_entries(const Ctx* c) { return sub_tab_entries(c, sub_first_fit(c)); }
 
 // dynamic shared memory of the four tile kernels (down/up, with/without front rows) of one shape
-template <int T, bool S, class R, int H>
+template <int TJ, int TI, bool S, class R, int H>
 static int tile_attrs(Ctx* c) {
-  const void* k[4] = {(const void*)k_smooth_down<T, T, S, false, R, H>, (const void*)k_smooth_down<T, T, S, true, R, H>,
-                      (const void*)k_smooth_up<T, T, S, false, R, H>, (const void*)k_smooth_up<T, T, S, true, R, H>};
+  using G = TileGeom<TJ, TI, S, R, H>;
+  const void* k[4] = {(const void*)k_smooth_down<TJ, TI, S, false, R, H>, (const void*)k_smooth_down<TJ, TI, S, true, R, H>,
+                      (const void*)k_smooth_up<TJ, TI, S, false, R, H>, (const void*)k_smooth_up<TJ, TI, S, true, R, H>};
   for (int q = 0; q < 4; ++q)   // the up kernels (2, 3) also stage the coarse correction
     DIVA_CUDA(c, cudaFuncSetAttribute(k[q], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(q < 2 ? TileGeom<T, T, S, R, H>::smem : TileGeom<T, T, S, R, H>::smem_up)));
+                                      (int)(q < 2 ? G::smem : G::smem_up)));
+  return DIVA_OK;
+}
+// every tile shape (square, and 1.5x wider along i) of both edges, both types, both halos
+template <int TJ, int TI>
+static int tile_attrs_shape(Ctx* c) {
+  constexpr bool S = TJ == 16 ? kStage16 : kStage32;
+  if (int st = tile_attrs<TJ, TI, S, double, kHalo>(c)) return st;
+  if (int st = tile_attrs<TJ, TI, true, float, kHalo>(c)) return st;
+  if (int st = tile_attrs<TJ, TI, S, double, kHaloOne>(c)) return st;
+  if (int st = tile_attrs<TJ, TI, true, float, kHaloOne>(c)) return st;
   return DIVA_OK;
 }
 
@@ -2270,14 +2299,10 @@ int solver_init(Ctx* c) {
   DIVA_CUDA(c, cudaFuncSetAttribute(k_small_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
   DIVA_CUDA(c, cudaFuncSetAttribute(k_subcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kSubSmemBudget));
-  if (int st = tile_attrs<32, kStage32, double, kHalo>(c)) return st;
-  if (int st = tile_attrs<16, kStage16, double, kHalo>(c)) return st;
-  if (int st = tile_attrs<32, true, float, kHalo>(c)) return st;
-  if (int st = tile_attrs<16, true, float, kHalo>(c)) return st;
-  if (int st = tile_attrs<32, kStage32, double, kHaloOne>(c)) return st;
-  if (int st = tile_attrs<16, kStage16, double, kHaloOne>(c)) return st;
-  if (int st = tile_attrs<32, true, float, kHaloOne>(c)) return st;
-  if (int st = tile_attrs<16, true, float, kHaloOne>(c)) return st;
+  if (int st = tile_attrs_shape<32, 32>(c)) return st;
+  if (int st = tile_attrs_shape<16, 16>(c)) return st;
+  if (int st = tile_attrs_shape<32, 48>(c)) return st;
+  if (int st = tile_attrs_shape<16, 24>(c)) return st;
   const BCs& b = c->bc;
   const int all[8] = {b.uW, b.uE, b.uS, b.uN, b.vW, b.vE, b.vS, b.vN};
   bool periodic = false;
