@@ -649,12 +649,13 @@ struct TileMem {
   // Boundary unknowns in the tile ("ghosts").  A u or v value outside its component's
   // interior is read, by the rows next to it, through the boundary elimination (u_src,
   // v_src): as the value of its source point, or as zero.  The tile keeps each such value
-  // in its own slot, equal to its source's current value, so every row of a block reads
-  // its whole stencil as stored, at the domain's edge too: a ghost takes its source's
-  // value in the staging and again whenever the source is updated (ghosts_u, ghosts_v).
-  // The elimination maps a row's outside same-component neighbours back to the row
-  // itself, and cross-component ghosts are read only in the other component's passes, so
-  // no pass reads a ghost that it rewrites.  (Periodic sides, whose sources lie across the
+  // in its own slot, equal to its source's value, so every row of a block reads its whole
+  // stencil as stored, at the domain's edge too.  The elimination maps a row's outside
+  // same-component neighbours back to the row itself (read before the row's own update),
+  // and cross-component ghosts are read only in the other component's passes, so a
+  // component's ghosts are refreshed from their sources (ghost_refresh) after the staging
+  // and after each pair of that component's colour passes: every read then sees the value
+  // the elimination would read.  (Periodic sides, whose sources lie across the
   // domain, do not use the tiles.)
   __device__ __forceinline__ bool in_region(const TIx& ix, int j, int i) const {
     using G = TileGeom<TJ, TI, STAGE, R, H>;
@@ -682,13 +683,14 @@ struct TileMem {
   // Every source point of the region (the interior points on the lines i = 1, the last
   // interior column, j = 1 and the last interior row of each component) writes its current
   // value into its ghosts; one point per thread.
-  __device__ __forceinline__ void ghost_refresh(const TIx& ix) {
+  __device__ __forceinline__ void ghost_refresh(const TIx& ix, int comps = 3) {   // bit 0: u, bit 1: v
     using G = TileGeom<TJ, TI, STAGE, R, H>;
     const Dims& d = os.d;
     // the four lines of each component, clipped to the region: 2 vertical (RJ points each)
     // and 2 horizontal (RI points each)
     const int per = 2 * G::RJ + 2 * G::RI;
-    for (int t = threadIdx.x; t < 2 * per; t += blockDim.x) {
+    const int t0 = (comps & 1) ? 0 : per, t1 = (comps & 2) ? 2 * per : per;
+    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
       const bool ucomp = t < per;
       const int e = ucomp ? t : t - per;
       int j, i;
@@ -744,17 +746,9 @@ __device__ __forceinline__ void tile_pass(M& m, const TIx& ix, int TJ, int TI, i
     // every stencil value is read as stored: at the domain's edge the ghosts hold what
     // the boundary elimination would read
     if (comp == 0) {
-      if (DEEP || u_int(d, j, i)) {
-        const auto val = fma_r(m.bu[k] - m.template Au<true>(ix, j, i), m.idu(ix, j, i), m.xu[k]);
-        m.xu[k] = val;
-        if (!DEEP) m.ghosts_u(ix, j, i, val);
-      }
+      if (DEEP || u_int(d, j, i)) m.xu[k] = fma_r(m.bu[k] - m.template Au<true>(ix, j, i), m.idu(ix, j, i), m.xu[k]);
     } else {
-      if (DEEP || v_int(d, j, i)) {
-        const auto val = fma_r(m.bv[k] - m.template Av<true>(ix, j, i), m.idv(ix, j, i), m.xv[k]);
-        m.xv[k] = val;
-        if (!DEEP) m.ghosts_v(ix, j, i, val);
-      }
+      if (DEEP || v_int(d, j, i)) m.xv[k] = fma_r(m.bv[k] - m.template Av<true>(ix, j, i), m.idv(ix, j, i), m.xv[k]);
     }
   }
 }
@@ -824,6 +818,10 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_down(OpT<R> o, Restrict
     for (int p = 0; p < 4; ++p, ++pass) {
       tile_pass_any<TJ, TI>(deep, m, ix, tj0, ti0, p >> 1, p & 1, H - 1 - pass);
       __syncthreads();
+      if (!deep && (p & 1)) {   // a component's pair done: its ghosts from their sources
+        m.ghost_refresh(ix, 1 << (p >> 1));
+        __syncthreads();
+      }
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
     const int j = tj0 + t % TJ, i = ti0 + t / TJ;
@@ -917,6 +915,10 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
     for (int p = 3; p >= 0; --p, ++pass) {
       tile_pass_any<TJ, TI>(deep, m, ix, tj0, ti0, p >> 1, p & 1, H - 1 - pass);
       __syncthreads();
+      if (!deep && !(p & 1)) {   // a component's pair done: its ghosts from their sources
+        m.ghost_refresh(ix, 1 << (p >> 1));
+        __syncthreads();
+      }
     }
   for (int t = threadIdx.x; t < TJ * TI; t += blockDim.x) {
     const int j = tj0 + t % TJ, i = ti0 + t / TJ;
