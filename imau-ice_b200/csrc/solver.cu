@@ -905,7 +905,7 @@ __global__ void __launch_bounds__(kTileThreads) k_smooth_up(OpT<R> o, Op oc, int
   __syncthreads();
   if (!deep) {
     // The ghosts take their sources' staged values: every interior point on the lines next
-    // to the domain's edge writes its own ghosts (the rule of the passes), so only those
+    // to the domain's edge writes its own ghosts (ghosts_u/ghosts_v), so only those
     // lines are visited.  A 'zero' ghost holds 0 already (the pre-smoothing left it so).
     m.ghost_refresh(ix);
     __syncthreads();
