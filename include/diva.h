@@ -374,11 +374,13 @@ int  diva_complete_state(diva_ctx_t* ctx, int32_t sweeps);
 
 /* Tile shapes of the multigrid smoother.  The levels above the one-block sub-cycle
  * are smoothed by tiled kernels of edge 16 or 32; by default a level takes 32 while
- * its 32 x 32 tiles still fill the GPU.  diva_get_tile_edges writes each level's
- * edge (0 for levels not smoothed by tiles) into edges[0..n) and the level count
- * into *nlev; diva_set_tile_edges fixes the edge of levels 0..n-1 (16, 32, or 0 for
+ * its 32 x 32 tiles still fill the GPU, and tiles 1.5x as wide along i (32 x 48,
+ * 16 x 24) where the square ones give just over one block per SM and the wide ones
+ * fit in one.  diva_get_tile_edges writes each level's edge along j (0 for levels not
+ * smoothed by tiles) into edges[0..n) and the level count into *nlev;
+ * diva_set_tile_edges fixes the edge of levels 0..n-1 (16 or 32: square tiles; 0 for
  * the default) until the next call, e.g. from an autotuner that times candidates
- * with diva_profile_kernel.  The solution does not depend on the edge, only the
+ * with diva_profile_kernel.  The solution does not depend on the shape, only the
  * time per V-cycle. */
 int  diva_get_tile_edges(diva_ctx_t* ctx, int32_t* edges, int32_t n, int32_t* nlev);
 int  diva_set_tile_edges(diva_ctx_t* ctx, const int32_t* edges, int32_t n);
